@@ -1,0 +1,350 @@
+#!/usr/bin/env python3
+"""Benchmark of the path-tracing hot path (one JSON line on stdout, rank 0).
+
+A step is one full frame of the measured workload, rendered by the compat-mode kernel (the reference's
+semantics: per-pixel thrust::minstd_rand stream, mixture-PDF lambertian, floor(sqrt(spp))^2 samples):
+
+  spheres (default)  1280x720, 64 spp, depth 50, 488 spheres (ground r=1000, 22x22 grid of r=0.2, three
+                     r=1 feature spheres; 80/15/5 % lambertian/metal/dielectric), defocus aperture 0.1 at
+                     focus 10, sky-gradient background, one quad light; synthetic, seed 20261203.
+  cornell            256x256, 16 spp, depth 8 (the small Cornell box, reference host-build size).
+  meshes             1920x1080, 121 traced spp (128 requested), depth 16, 1,310,720 triangles, env map.
+
+value  = Mpaths/s of the whole job (all ranks; weak scaling, one replica frame per rank), device time
+         from CUDA events on the launching stream, L2 flushed (256 MiB write) between steps.
+e2e    = the same metric through the public C ABI with host buffers: per step rtc_scene_create
+         (flatten + SAH BVH + H2D upload) + rtc_render (kernel + D2H of the FP32 radiance) + destroy.
+roofline: algorithmic bytes of the render kernel per launch (BVH node visits x 64 B + primitive tests x
+         their record size + per-ray state), counted by an instrumented launch of the same frame, divided
+         by the mean event time of the timed launches, against the measured HBM copy bandwidth.
+cpu_baseline: the reference's own CPU code (oracle/_ref/libref_cpu.so: the reference's classes built
+         with g++) on all host cores, on a deterministic pixel subsample of the same frame.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--config spheres|cornell|meshes] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+from cortexraytracercuda_b200 import configs  # noqa: E402
+from cortexraytracercuda_b200.scene import DRAW_ORDER_DEVICE, DRAW_ORDER_HOST, MODE_CLEAN, MODE_COMPAT  # noqa: E402
+
+METRIC = "Mpaths/s"
+PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
+FALLBACK_HBM_GBS = 6650.0
+
+# bytes fetched per visit (ignoring caches) for the roofline's algorithmic traffic
+NODE_BYTES = 64          # BVH2 node: two child boxes + two child links (4 x float4)
+PRIM_BYTES = {"spheres": 16, "cornell": 48, "meshes": 48}   # dominant primitive record of each workload
+STATE_BYTES = 32 + 16 + 2 * 48   # ray read + hit write + path state read/write per traversal
+
+
+def workload(name):
+    mk, mp = configs.SCENES[name]
+    scene = mk()
+    params = mp()
+    params.mode = MODE_COMPAT
+    params.draw_order = DRAW_ORDER_DEVICE
+    return scene, params
+
+
+def describe(name, params, scene):
+    return {"workload": f"{name} {params.width}x{params.height} spp{params.spp} (traced {params.traced_spp}) "
+                        f"depth{params.max_depth}",
+            "primitives": scene.num_primitives, "mode": "compat (reference RNG stream and quirks)",
+            "l2": "flushed between steps (256 MiB write)", "seed": configs.DEFAULT_SEED}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled every 200 ms while running."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def hbm_peak():
+    try:
+        d = json.loads(PEAKS_FILE.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def cpu_reference_rate(scene, params, target_s=10.0, max_pixels=None):
+    """Times the reference's own CPU implementation on a deterministic pixel subsample.
+    Returns (Mpaths/s, Mrays/s, info)."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    import oracles
+    ref = oracles.ref_cpu()
+    kind = "reference"
+    threads = os.cpu_count() or 1
+    if ref is not None:
+        p = params.__class__(**{**params.__dict__, "draw_order": DRAW_ORDER_HOST})
+        rs = ref.scene(scene)
+        run = lambda pix: rs.render_pixels(p, pix, threads)   # noqa: E731
+    else:
+        kind = "port"
+        port = oracles.port()
+        ps = port.scene(scene)
+        p = params.__class__(**{**params.__dict__, "draw_order": DRAW_ORDER_HOST})
+        run = lambda pix: ps.render_pixels(p, pix, threads, trig=0)   # noqa: E731
+    npix = params.width * params.height
+    # calibration on 1/4096 of the frame, then a sample sized for ~target_s
+    stride = 4096
+    pix = np.arange(0, npix, stride, dtype=np.int64)
+    t = time.perf_counter()
+    run(pix)
+    dt = max(time.perf_counter() - t, 1e-6)
+    per_px = dt / pix.size
+    want = int(min(npix, max(pix.size, target_s / per_px)))
+    if max_pixels:
+        want = min(want, max_pixels)
+    stride = max(1, npix // want)
+    pix = np.arange(0, npix, stride, dtype=np.int64)
+    t = time.perf_counter()
+    _, rays = run(pix)
+    dt = time.perf_counter() - t
+    paths = pix.size * params.traced_spp
+    info = {"kind": kind, "cores": threads,
+            "sample": f"every {stride}th pixel of the frame ({pix.size} px x {params.traced_spp} paths), "
+                      f"{dt:.1f} s"}
+    return paths / dt / 1e6, rays / dt / 1e6, info
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    name = args.config
+    scene, params = workload(name)
+    vals = []
+    rays_rates = []
+    info = None
+    for it in range(args.warmup + args.steps):
+        v, r, info = cpu_reference_rate(scene, params, target_s=args.ref_step_s)
+        if it >= args.warmup:
+            vals.append(v)
+            rays_rates.append(r)
+    value = float(np.mean(vals))
+    line = {"metric": METRIC, "value": round(value, 4), "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic", "impl": "reference", "config": describe(name, params, scene),
+            "mrays_per_s": round(float(np.mean(rays_rates)), 4),
+            "cpu_baseline": {"value": round(value, 4), "unit": METRIC, **info},
+            "e2e": {"value": round(value, 4), "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--config", default="spheres", choices=["spheres", "cornell", "meshes"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--mode", default="compat", choices=["compat", "clean"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-baseline-s", type=float, default=12.0)
+    ap.add_argument("--ref-step-s", type=float, default=8.0)
+    ap.add_argument("--small", action="store_true", help="quarter-size frame, 16 spp (profiling captures)")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from cortexraytracercuda_b200.renderer import Context, DeviceScene
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    ctx = Context(local)
+    scene, params = workload(args.config)
+    if args.mode == "clean":
+        params.mode = MODE_CLEAN
+    if args.small:
+        params.width, params.height, params.spp = params.width // 4, params.height // 4, 16
+    ds = DeviceScene(ctx, scene)
+    info = ds.info()
+    W, H = params.width, params.height
+    out = torch.empty((H, W, 4), dtype=torch.float32, device="cuda")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    counters = torch.zeros(4, dtype=torch.int64, device="cuda")
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+
+    def launch(cnt=None):
+        ds.render_device(params, out.data_ptr(), None, cnt.data_ptr() if cnt is not None else None, sp)
+
+    # instrumented launch: algorithmic work counters (not timed)
+    counters.zero_()
+    launch(counters)
+    torch.cuda.synchronize()
+    rays, paths, nodes, prims = [int(x) for x in counters.tolist()]
+
+    for _ in range(args.warmup):
+        flush.fill_(1.0)
+        launch()
+    torch.cuda.synchronize()
+    barrier()
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    barrier()
+    torch.cuda.synchronize()
+    t_wall = time.perf_counter()
+    for k in range(args.steps):
+        flush.fill_(float(k))          # L2 flush between steps (outside the kernel's events)
+        ev[k][0].record(stream)
+        launch()
+        ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    t_wall = time.perf_counter() - t_wall
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    clk = clocks.stop()
+    kernel_ms = float(np.mean(step_ms))
+    total_ms = float(np.sum(step_ms))
+    if world > 1:
+        tt = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        total_ms = float(tt.item())
+    traced = W * H * params.traced_spp
+    value = traced * world * args.steps / (total_ms / 1e3) / 1e6
+    mrays = rays * world * args.steps / (total_ms / 1e3) / 1e6
+
+    # ---- end to end through the C ABI with host buffers ----------------------------------------
+    import ctypes as C
+    host_out = torch.empty((H, W, 4), dtype=torch.float32, pin_memory=True).numpy()
+    e2e_ms = []
+    for k in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ds2 = DeviceScene(ctx, scene)
+        p = params.to_c()
+        from cortexraytracercuda_b200._lib import check
+        check(ctx.lib.rtc_render(ctx.handle, ds2.handle, C.byref(p), host_out.ctypes.data, None))
+        ds2.close()
+        dt = (time.perf_counter() - t0) * 1e3
+        if k >= args.warmup:
+            e2e_ms.append(dt)
+    e2e_total = float(np.sum(e2e_ms))
+    if world > 1:
+        tt = torch.tensor([e2e_total], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_total = float(tt.item())
+    e2e_value = traced * world * args.steps / (e2e_total / 1e3) / 1e6
+
+    # ---- roofline -------------------------------------------------------------------------------
+    peak, peak_kind = hbm_peak()
+    prim_b = PRIM_BYTES[args.config]
+    alg_bytes = nodes * NODE_BYTES + prims * prim_b + rays * STATE_BYTES
+    achieved = alg_bytes / (kernel_ms / 1e3) / 1e9
+    roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "traffic": None, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+            "kernel": "rtc::rtc_render_compat<0>" if params.mode == MODE_COMPAT else "rtc::rtc_render_clean",
+            "alg_bytes_per_launch": int(alg_bytes), "kernel_ms": round(kernel_ms, 3),
+            "per_launch": {"rays": rays, "paths": paths, "node_visits": nodes, "prim_tests": prims},
+            "bytes_per_ray": round(alg_bytes / max(rays, 1), 1)}
+    prof = ROOT / "profiles" / f"traffic_{args.config}.json"
+    if prof.exists():
+        try:
+            roof["traffic"] = json.loads(prof.read_text()).get("dram_bytes_per_launch")
+        except Exception:
+            pass
+
+    line = {"metric": METRIC, "value": round(value, 3), "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {**describe(args.config, params, scene), "parallelism": f"replicas x{world}",
+                       "bvh_nodes": info["num_nodes"]},
+            "mrays_per_s": round(mrays, 3), "gpu_launches": args.steps,
+            "e2e": {"value": round(e2e_value, 3), "unit": METRIC, "h2d_bytes_per_step": int(info["device_bytes"]),
+                    "d2h_bytes_per_step": int(W * H * 16), "ms_per_step": round(e2e_total / args.steps, 3)},
+            "roofline": roof, "clocks": clk, "wall_s": round(t_wall, 3)}
+
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, r, inf = cpu_reference_rate(scene, params, target_s=args.cpu_baseline_s)
+        line["cpu_baseline"] = {"value": round(v, 4), "unit": METRIC, **inf, "mrays_per_s": round(r, 4)}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ds.close()
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

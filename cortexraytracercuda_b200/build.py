@@ -1,0 +1,96 @@
+"""Builds the in-tree shared library librtc_b200.so (sm_100a kernels + host C ABI).
+
+    python -m cortexraytracercuda_b200.build [--force] [--verbose]
+
+Compat-mode kernels are compiled with --fmad=false (reference float semantics), clean-mode kernels
+with FMA contraction; host sources with -ffp-contract=off.  Objects go to ``_build/`` beside this
+file, the library next to the package (``cortexraytracercuda_b200/librtc_b200.so``).
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+CSRC = PKG / "csrc"
+BUILD = PKG / "_build"
+LIB = PKG / "librtc_b200.so"
+INCLUDE = PKG.parent / "include"
+
+CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", str(CSRC), "-I", str(INCLUDE)] + ARCH
+CXX = os.environ.get("CXX", "g++")
+CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-Wall", "-Wno-unused-function",
+             "-I", str(CSRC), "-I", str(INCLUDE), "-I", os.path.join(CUDA_HOME, "include")]
+
+# (source, compiler, extra flags)
+SOURCES = [
+    ("render_compat.cu", "nvcc", ["--fmad=false"]),
+    ("render_clean.cu", "nvcc", ["--fmad=true"]),
+    ("rtc_api.cpp", "cxx", []),
+    ("bvh_build.cpp", "cxx", []),
+]
+HEADERS = ["rtc_dev.h", "rtc_math.cuh", "rtc_trace.cuh", "rtc_path.cuh", "rtc_kernels.h", "bvh_build.h"]
+
+
+def _newer(target: Path, deps) -> bool:
+    if not target.exists():
+        return True
+    t = target.stat().st_mtime
+    return any(Path(d).stat().st_mtime > t for d in deps)
+
+
+def _run(cmd, verbose):
+    if verbose:
+        print(" ".join(str(c) for c in cmd), flush=True)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError(f"build step failed: {' '.join(str(c) for c in cmd)}")
+    if verbose and (r.stdout or r.stderr):
+        sys.stderr.write(r.stdout + r.stderr)
+
+
+def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = False) -> Path:
+    if not os.path.exists(NVCC):
+        raise RuntimeError(f"nvcc not found at {NVCC}")
+    BUILD.mkdir(exist_ok=True)
+    headers = [CSRC / h for h in HEADERS] + [INCLUDE / "rtc.h"]
+    objs = []
+    for src, comp, extra in SOURCES:
+        s = CSRC / src
+        o = BUILD / (src + ".o")
+        objs.append(o)
+        if not force and not _newer(o, [s] + headers + [Path(__file__)]):
+            continue
+        if comp == "nvcc":
+            cmd = [NVCC] + NVCC_COMMON + extra + (["-Xptxas", "-v"] if ptxas_verbose else []) + ["-c", str(s), "-o", str(o)]
+        else:
+            cmd = [CXX] + CXX_FLAGS + extra + ["-c", str(s), "-o", str(o)]
+        _run(cmd, verbose or ptxas_verbose)
+    if force or _newer(LIB, objs):
+        tmp = LIB.with_suffix(".so.tmp")
+        cmd = [NVCC, "-shared"] + ARCH + ["-o", str(tmp)] + [str(o) for o in objs] + ["-cudart", "static", "-lpthread"]
+        _run(cmd, verbose)
+        os.replace(tmp, LIB)
+    return LIB
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--force", action="store_true")
+    ap.add_argument("--verbose", action="store_true")
+    ap.add_argument("--ptxas", action="store_true", help="print -Xptxas -v register/spill report")
+    a = ap.parse_args()
+    p = build(force=a.force, verbose=a.verbose, ptxas_verbose=a.ptxas)
+    print(p)
+
+
+if __name__ == "__main__":
+    main()

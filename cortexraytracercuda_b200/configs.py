@@ -1,0 +1,287 @@
+"""Synthetic scenes for the measured workloads and the parity cases.
+
+No public dataset is involved: every scene is generated from a seed (default 20261203).  The shapes,
+sizes and value distributions follow the workloads the library is measured on:
+
+* ``cornell``      - Cornell box: five 555-unit lambertian wall quads, a 130x105 ceiling quad light
+                     (emission 15), two white boxes of 12 triangles each (165^3 rotated +15 deg about y,
+                     165x330x165 rotated -18 deg), camera (278,278,-800) -> (278,278,0), vfov 40; 256^2,
+                     16 spp, depth 8.  Wall and light placement follow data/scenes/cornell_box.scene.
+* ``spheres``      - ground sphere r=1000, 22x22 grid of r=0.2 spheres at (a+0.9u, 0.2, b+0.9u'),
+                     80% lambertian (albedo U^3*U^3) / 15% metal (U(0.5,1)^3, fuzz U(0,0.5)) / 5%
+                     dielectric (1.5), three r=1 feature spheres; camera (13,2,3) -> 0, vfov 20,
+                     aperture 0.1, focus 10; 1280x720, 64 spp, depth 50; sky-gradient background; the
+                     quad light of data/scenes/random_spheres.scene so the lambertian mixture PDF has a
+                     light to sample (with an empty light list the reference's mixture PDF returns NaN
+                     for half the bounces, hittable_list.cuh:191-215).
+* ``meshes``       - an icosphere subdivided to 327,680 triangles, radially displaced by 3-octave value
+                     noise of amplitude 0.15, four instances (metal, dielectric, lambertian, lambertian
+                     checker) = 1,310,720 triangles; a checker ground quad with a 10-unit period; a
+                     2048x1024 FP32 equirectangular environment map (sky gradient + Gaussian sun lobe);
+                     1920x1080, 128 spp, depth 16.
+* ``textured``     - spheres and quads with checker and image textures (parity of the texture paths).
+* ``icosphere``    - a 1,280-triangle icosphere with lambertian, metal and dielectric instances.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from .scene import Camera, RenderParams, Scene
+
+DEFAULT_SEED = 20261203
+
+
+# -------------------------------------------------------------------------------------------------
+# geometry helpers
+# -------------------------------------------------------------------------------------------------
+def box_mesh(size, center, yaw_deg):
+    """12-triangle box of extent `size` centred at `center`, rotated by `yaw_deg` about +y."""
+    sx, sy, sz = (0.5 * float(s) for s in size)
+    corners = np.array([[x, y, z] for x in (-sx, sx) for y in (-sy, sy) for z in (-sz, sz)], dtype=np.float64)
+    th = math.radians(yaw_deg)
+    c, s = math.cos(th), math.sin(th)
+    rot = np.array([[c, 0.0, s], [0.0, 1.0, 0.0], [-s, 0.0, c]])
+    verts = corners @ rot.T + np.asarray(center, dtype=np.float64)
+    # corner index = 4*ix + 2*iy + iz
+    faces = [
+        (0, 1, 3), (0, 3, 2),   # x-
+        (4, 6, 7), (4, 7, 5),   # x+
+        (0, 4, 5), (0, 5, 1),   # y-
+        (2, 3, 7), (2, 7, 6),   # y+
+        (0, 2, 6), (0, 6, 4),   # z-
+        (1, 5, 7), (1, 7, 3),   # z+
+    ]
+    return verts.astype(np.float32), np.array(faces, dtype=np.uint32)
+
+
+def icosphere(level: int):
+    """Unit icosphere by repeated 4:1 edge-midpoint subdivision (20*4^level faces)."""
+    t = (1.0 + 5.0 ** 0.5) / 2.0
+    v = np.array([[-1, t, 0], [1, t, 0], [-1, -t, 0], [1, -t, 0], [0, -1, t], [0, 1, t], [0, -1, -t], [0, 1, -t],
+                  [t, 0, -1], [t, 0, 1], [-t, 0, -1], [-t, 0, 1]], dtype=np.float64)
+    f = np.array([[0, 11, 5], [0, 5, 1], [0, 1, 7], [0, 7, 10], [0, 10, 11], [1, 5, 9], [5, 11, 4], [11, 10, 2],
+                  [10, 7, 6], [7, 1, 8], [3, 9, 4], [3, 4, 2], [3, 2, 6], [3, 6, 8], [3, 8, 9], [4, 9, 5],
+                  [2, 4, 11], [6, 2, 10], [8, 6, 7], [9, 8, 1]], dtype=np.int64)
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    for _ in range(level):
+        e = np.concatenate([f[:, [0, 1]], f[:, [1, 2]], f[:, [2, 0]]], axis=0)
+        e.sort(axis=1)
+        uniq, inv = np.unique(e, axis=0, return_inverse=True)
+        inv = inv.reshape(-1)
+        mid = v[uniq[:, 0]] + v[uniq[:, 1]]
+        mid /= np.linalg.norm(mid, axis=1, keepdims=True)
+        base = v.shape[0]
+        v = np.concatenate([v, mid], axis=0)
+        nf = f.shape[0]
+        a = inv[:nf] + base
+        b = inv[nf:2 * nf] + base
+        c = inv[2 * nf:] + base
+        f = np.concatenate([np.stack([f[:, 0], a, c], 1), np.stack([f[:, 1], b, a], 1),
+                            np.stack([f[:, 2], c, b], 1), np.stack([a, b, c], 1)], axis=0)
+    return v, f.astype(np.uint32)
+
+
+def _lattice_hash(ix, iy, iz, seed):
+    h = (ix.astype(np.int64) * 73856093) ^ (iy.astype(np.int64) * 19349663) ^ (iz.astype(np.int64) * 83492791) ^ seed
+    h = (h ^ (h >> 13)) * 1274126177
+    h = h ^ (h >> 16)
+    return (h & 0xFFFFFF).astype(np.float64) / float(0xFFFFFF)
+
+
+def value_noise(p: np.ndarray, octaves=3, base_freq=2.0, seed=DEFAULT_SEED):
+    """Sum of `octaves` octaves of trilinear lattice value noise in [-1, 1] (amplitude halving)."""
+    out = np.zeros(p.shape[0])
+    amp, freq, norm = 1.0, base_freq, 0.0
+    for o in range(octaves):
+        q = p * freq
+        i0 = np.floor(q).astype(np.int64)
+        fr = q - i0
+        w = fr * fr * (3.0 - 2.0 * fr)
+        acc = np.zeros(p.shape[0])
+        for dx in (0, 1):
+            for dy in (0, 1):
+                for dz in (0, 1):
+                    val = _lattice_hash(i0[:, 0] + dx, i0[:, 1] + dy, i0[:, 2] + dz, seed + 7919 * o)
+                    wx = w[:, 0] if dx else 1.0 - w[:, 0]
+                    wy = w[:, 1] if dy else 1.0 - w[:, 1]
+                    wz = w[:, 2] if dz else 1.0 - w[:, 2]
+                    acc += wx * wy * wz * val
+        out += amp * (2.0 * acc - 1.0)
+        norm += amp
+        amp *= 0.5
+        freq *= 2.0
+    return out / norm
+
+
+def displaced_icosphere(level: int, amplitude=0.15, seed=DEFAULT_SEED):
+    v, f = icosphere(level)
+    r = 1.0 + amplitude * value_noise(v, seed=seed)
+    return (v * r[:, None]), f
+
+
+def procedural_image(w: int, h: int, seed=DEFAULT_SEED):
+    """Seeded RGB8 test image: smooth colour ramps plus a coarse random tile pattern."""
+    rng = np.random.default_rng(seed)
+    y, x = np.mgrid[0:h, 0:w]
+    tiles = rng.integers(0, 256, size=(8, 8, 3))
+    t = tiles[(y * 8) // h, (x * 8) // w]
+    img = np.stack([(x * 255) // max(1, w - 1), (y * 255) // max(1, h - 1), (x ^ y) & 255], axis=-1)
+    return ((img + t) // 2).astype(np.uint8)
+
+
+def sky_sun_envmap(w=2048, h=1024, sun_dir=(0.35, 0.6, -0.72), sun_sigma=0.04, sun_power=40.0):
+    """FP32 equirect map: sky gradient + Gaussian sun lobe, indexed as get_spherical_uv maps
+    directions (u = (atan2(-z, x) + pi) / 2pi, v = acos(-y) / pi; row 0 = v near 1, i.e. up)."""
+    j, i = np.mgrid[0:h, 0:w]
+    u = (i + 0.5) / w
+    v = 1.0 - (j + 0.5) / h
+    phi = u * 2.0 * np.pi - np.pi
+    theta = v * np.pi
+    dy = -np.cos(theta)
+    st = np.sin(theta)
+    dx = np.cos(phi) * st
+    dz = -np.sin(phi) * st
+    a = 0.5 * (dy + 1.0)
+    sky = (1.0 - a)[..., None] * np.array([1.0, 1.0, 1.0]) + a[..., None] * np.array([0.5, 0.7, 1.0])
+    sd = np.asarray(sun_dir, dtype=np.float64)
+    sd /= np.linalg.norm(sd)
+    cosang = np.clip(dx * sd[0] + dy * sd[1] + dz * sd[2], -1.0, 1.0)
+    ang = np.arccos(cosang)
+    sun = sun_power * np.exp(-0.5 * (ang / sun_sigma) ** 2)
+    env = sky + sun[..., None] * np.array([1.0, 0.95, 0.85])
+    return env.astype(np.float32)
+
+
+# -------------------------------------------------------------------------------------------------
+# scenes
+# -------------------------------------------------------------------------------------------------
+def cornell(light_intensity=1.0) -> Scene:
+    s = Scene(name="cornell")
+    red = s.lambertian((0.65, 0.05, 0.05))
+    green = s.lambertian((0.12, 0.45, 0.15))
+    white = s.lambertian((0.73, 0.73, 0.73))
+    s.dir_light((278.0, 554.0, 332.0), (-130.0, 0.0, 0.0), (0.0, 0.0, -105.0), (15.0, 15.0, 15.0),
+                intensity=light_intensity, invisible=True)
+    s.quad((555, 0, 0), (0, 555, 0), (0, 0, 555), green)
+    s.quad((0, 0, 0), (0, 555, 0), (0, 0, 555), red)
+    s.quad((0, 0, 0), (555, 0, 0), (0, 0, 555), white)
+    s.quad((555, 555, 555), (-555, 0, 0), (0, 0, -555), white)
+    s.quad((0, 0, 555), (555, 0, 0), (0, 555, 0), white)
+    v1, f1 = box_mesh((165, 165, 165), (212.5, 82.5, 147.5), 15.0)
+    v2, f2 = box_mesh((165, 330, 165), (347.5, 165.0, 377.5), -18.0)
+    s.mesh(v1, f1, white)
+    s.mesh(v2, f2, white)
+    s.camera = Camera(look_from=(278, 278, -800), look_at=(278, 278, 0), up=(0, 1, 0), vfov=40.0, aspect=1.0,
+                      aperture=0.0, focus=100.0)
+    s.set_background_constant((0.0, 0.0, 0.0))
+    return s
+
+
+def cornell_params(**kw) -> RenderParams:
+    p = dict(width=256, height=256, spp=16, max_depth=8)
+    p.update(kw)
+    return RenderParams(**p)
+
+
+def spheres(seed=DEFAULT_SEED, grid=11, light=True, sky=True) -> Scene:
+    rng = np.random.default_rng(seed)
+    s = Scene(name="spheres")
+    if light:
+        # data/scenes/random_spheres.scene:31-45
+        s.dir_light((0.0, 554.0, 147.0), (300.0, 0.0, 0.0), (0.0, 0.0, 265.0), (7.0, 7.0, 7.0), intensity=1.5,
+                    invisible=True)
+    ground = s.lambertian((0.5, 0.5, 0.5))
+    s.sphere((0.0, -1000.0, 0.0), 1000.0, ground)
+    s.sphere((0.0, 1.0, 0.0), 1.0, s.dielectric(1.5))
+    s.sphere((-4.0, 1.0, 0.0), 1.0, s.lambertian((0.4, 0.2, 0.1)))
+    s.sphere((4.0, 1.0, 0.0), 1.0, s.metal((0.7, 0.6, 0.5), 0.0))
+    for a in range(-grid, grid):
+        for b in range(-grid, grid):
+            choose = rng.random()
+            center = (a + 0.9 * rng.random(), 0.2, b + 0.9 * rng.random())
+            if choose < 0.8:
+                albedo = rng.random(3) * rng.random(3)
+                m = s.lambertian(tuple(albedo))
+            elif choose < 0.95:
+                albedo = 0.5 + 0.5 * rng.random(3)
+                m = s.metal(tuple(albedo), 0.5 * rng.random())
+            else:
+                m = s.dielectric(1.5)
+            s.sphere(center, 0.2, m)
+    s.camera = Camera(look_from=(13, 2, 3), look_at=(0, 0, 0), up=(0, 1, 0), vfov=20.0, aspect=16.0 / 9.0,
+                      aperture=0.1, focus=10.0)
+    if sky:
+        s.set_background_sky()
+    else:
+        s.set_background_constant((0.70, 0.80, 1.00))
+    return s
+
+
+def spheres_params(**kw) -> RenderParams:
+    p = dict(width=1280, height=720, spp=64, max_depth=50)
+    p.update(kw)
+    return RenderParams(**p)
+
+
+def meshes(level=7, seed=DEFAULT_SEED, env_size=(2048, 1024)) -> Scene:
+    s = Scene(name="meshes")
+    v, f = displaced_icosphere(level, 0.15, seed)
+    mats = [s.metal((0.8, 0.85, 0.9), 0.05), s.dielectric(1.5), s.lambertian((0.7, 0.3, 0.2)),
+            s.lambertian(s.checker_colors(0.25, (0.9, 0.9, 0.9), (0.1, 0.3, 0.6)))]
+    xs = (-3.3, -1.1, 1.1, 3.3)
+    for x, m in zip(xs, mats):
+        s.mesh((v + np.array([x, 1.0, 0.0])).astype(np.float32), f, m)
+    ground = s.lambertian(s.checker_colors(10.0, (0.2, 0.3, 0.1), (0.9, 0.9, 0.9)))
+    s.quad((-200.0, -0.15, -200.0), (400.0, 0.0, 0.0), (0.0, 0.0, 400.0), ground)
+    s.camera = Camera(look_from=(0.0, 2.5, 9.0), look_at=(0.0, 0.9, 0.0), up=(0, 1, 0), vfov=35.0,
+                      aspect=16.0 / 9.0, aperture=0.0, focus=9.0)
+    s.set_background_env(sky_sun_envmap(*env_size))
+    return s
+
+
+def meshes_params(**kw) -> RenderParams:
+    p = dict(width=1920, height=1080, spp=128, max_depth=16)
+    p.update(kw)
+    return RenderParams(**p)
+
+
+def textured(seed=DEFAULT_SEED) -> Scene:
+    """Checker and image textures on spheres and quads, lit by a quad light and a sky."""
+    s = Scene(name="textured")
+    s.dir_light((0.0, 8.0, 0.0), (4.0, 0.0, 0.0), (0.0, 0.0, 4.0), (6.0, 6.0, 6.0), intensity=1.0, invisible=True)
+    img = s.image(procedural_image(64, 48, seed))
+    chk = s.checker_colors(0.5, (0.2, 0.3, 0.1), (0.9, 0.9, 0.9))   # all_textures_spheres.scene scale style
+    s.quad((-6.0, 0.0, -6.0), (12.0, 0.0, 0.0), (0.0, 0.0, 12.0), s.lambertian(chk))
+    s.sphere((-1.6, 1.0, 0.0), 1.0, s.lambertian(img))
+    s.sphere((1.6, 1.0, 0.0), 1.0, s.lambertian(s.checker_colors(0.3, (0.8, 0.1, 0.1), (0.9, 0.9, 0.2))))
+    s.sphere((0.0, 0.6, 1.8), 0.6, s.metal((0.9, 0.9, 0.9), 0.2))
+    s.quad((-3.0, 0.0, -3.0), (6.0, 0.0, 0.0), (0.0, 3.0, 0.0), s.lambertian(img))
+    s.camera = Camera(look_from=(0.0, 3.0, 8.0), look_at=(0.0, 1.0, 0.0), up=(0, 1, 0), vfov=45.0, aspect=4.0 / 3.0,
+                      aperture=0.0, focus=8.0)
+    s.set_background_sky()
+    return s
+
+
+def icosphere_scene(level=3, seed=DEFAULT_SEED) -> Scene:
+    s = Scene(name="icosphere")
+    s.dir_light((0.0, 6.0, 0.0), (3.0, 0.0, 0.0), (0.0, 0.0, 3.0), (8.0, 8.0, 8.0), intensity=1.0, invisible=False)
+    v, f = displaced_icosphere(level, 0.15, seed)
+    mats = [s.lambertian((0.7, 0.3, 0.2)), s.metal((0.8, 0.8, 0.9), 0.1), s.dielectric(1.5)]
+    for x, m in zip((-2.2, 0.0, 2.2), mats):
+        s.mesh((v + np.array([x, 1.0, 0.0])).astype(np.float32), f, m)
+    s.quad((-10.0, -0.2, -10.0), (20.0, 0.0, 0.0), (0.0, 0.0, 20.0), s.lambertian((0.5, 0.5, 0.5)))
+    s.camera = Camera(look_from=(0.0, 2.5, 7.0), look_at=(0.0, 1.0, 0.0), up=(0, 1, 0), vfov=40.0, aspect=1.5,
+                      aperture=0.05, focus=7.0)
+    s.set_background_constant((0.3, 0.35, 0.45))
+    return s
+
+
+SCENES = {
+    "cornell": (cornell, cornell_params),
+    "spheres": (spheres, spheres_params),
+    "meshes": (meshes, meshes_params),
+    "textured": (textured, lambda **kw: RenderParams(**{**dict(width=160, height=120, spp=16, max_depth=10), **kw})),
+    "icosphere": (icosphere_scene, lambda **kw: RenderParams(**{**dict(width=150, height=100, spp=16, max_depth=12), **kw})),
+}

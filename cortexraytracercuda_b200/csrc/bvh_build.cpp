@@ -1,0 +1,226 @@
+// bvh_build.cpp - binned SAH BVH2 builder (host).  See bvh_build.h.
+#include "bvh_build.h"
+
+#include <algorithm>
+#include <atomic>
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <thread>
+
+#include "rtc_dev.h"
+
+namespace rtc {
+namespace {
+
+constexpr int NBINS = 32;
+constexpr int MAX_TREE_DEPTH = 56;   // < TRAVERSAL_STACK, leaves room for the root pair
+
+struct BNode {
+    Aabb box;
+    int32_t left = -1, right = -1;   // children (node ids) for inner nodes
+    uint32_t first = 0, count = 0;   // leaf range in the index array
+    bool leaf = false;
+};
+
+inline void grow(Aabb& a, const Aabb& b) {
+    for (int k = 0; k < 3; ++k) {
+        a.lo[k] = std::min(a.lo[k], b.lo[k]);
+        a.hi[k] = std::max(a.hi[k], b.hi[k]);
+    }
+}
+inline Aabb empty_box() {
+    Aabb a;
+    for (int k = 0; k < 3; ++k) { a.lo[k] = FLT_MAX; a.hi[k] = -FLT_MAX; }
+    return a;
+}
+inline double area(const Aabb& a) {
+    double dx = (double)a.hi[0] - a.lo[0], dy = (double)a.hi[1] - a.lo[1], dz = (double)a.hi[2] - a.lo[2];
+    if (dx < 0 || dy < 0 || dz < 0) return 0.0;
+    return 2.0 * (dx * dy + dy * dz + dz * dx);
+}
+
+struct Builder {
+    const std::vector<Aabb>& boxes;
+    std::vector<float> cen;          // 3 per primitive
+    std::vector<uint32_t> idx;
+    int max_leaf;
+    std::vector<BNode> nodes;        // per-builder (one per subtree task)
+
+    Builder(const std::vector<Aabb>& b, int ml) : boxes(b), max_leaf(ml) {}
+
+    int32_t build(uint32_t start, uint32_t end, int depth, uint32_t& max_depth) {
+        int32_t id = (int32_t)nodes.size();
+        nodes.emplace_back();
+        Aabb box = empty_box(), cb = empty_box();
+        for (uint32_t i = start; i < end; ++i) {
+            uint32_t p = idx[i];
+            grow(box, boxes[p]);
+            for (int k = 0; k < 3; ++k) {
+                cb.lo[k] = std::min(cb.lo[k], cen[3 * p + k]);
+                cb.hi[k] = std::max(cb.hi[k], cen[3 * p + k]);
+            }
+        }
+        nodes[id].box = box;
+        if ((uint32_t)depth > max_depth) max_depth = depth;
+        const uint32_t n = end - start;
+        auto make_leaf = [&]() {
+            nodes[id].leaf = true;
+            nodes[id].first = start;
+            nodes[id].count = n;
+            return id;
+        };
+        if (n <= 1) return make_leaf();
+
+        // best binned SAH split
+        int best_axis = -1, best_bin = -1;
+        double best_cost = DBL_MAX;
+        const double parea = std::max(area(box), 1e-30);
+        for (int ax = 0; ax < 3; ++ax) {
+            double ext = (double)cb.hi[ax] - cb.lo[ax];
+            if (!(ext > 0.0)) continue;
+            uint32_t cnt[NBINS] = {0};
+            Aabb bb[NBINS];
+            for (int b = 0; b < NBINS; ++b) bb[b] = empty_box();
+            const double scale = NBINS / ext;
+            for (uint32_t i = start; i < end; ++i) {
+                uint32_t p = idx[i];
+                int b = (int)(((double)cen[3 * p + ax] - cb.lo[ax]) * scale);
+                b = b < 0 ? 0 : (b >= NBINS ? NBINS - 1 : b);
+                cnt[b]++;
+                grow(bb[b], boxes[p]);
+            }
+            double la[NBINS];
+            uint32_t lc[NBINS];
+            Aabb acc = empty_box();
+            uint32_t c = 0;
+            for (int b = 0; b < NBINS - 1; ++b) {
+                grow(acc, bb[b]);
+                c += cnt[b];
+                la[b] = area(acc);
+                lc[b] = c;
+            }
+            acc = empty_box();
+            c = 0;
+            for (int b = NBINS - 1; b > 0; --b) {
+                grow(acc, bb[b]);
+                c += cnt[b];
+                uint32_t nl = lc[b - 1];
+                if (nl == 0 || c == 0) continue;
+                double cost = 1.0 + (la[b - 1] * nl + area(acc) * c) / parea;
+                if (cost < best_cost) { best_cost = cost; best_axis = ax; best_bin = b; }
+            }
+        }
+        const bool can_leaf = n <= (uint32_t)max_leaf;
+        if (can_leaf && (best_axis < 0 || (double)n <= best_cost)) return make_leaf();
+
+        uint32_t mid;
+        if (best_axis >= 0 && depth < MAX_TREE_DEPTH) {
+            const double ext = (double)cb.hi[best_axis] - cb.lo[best_axis];
+            const double scale = NBINS / ext;
+            auto it = std::partition(idx.begin() + start, idx.begin() + end, [&](uint32_t p) {
+                int b = (int)(((double)cen[3 * p + best_axis] - cb.lo[best_axis]) * scale);
+                b = b < 0 ? 0 : (b >= NBINS ? NBINS - 1 : b);
+                return b < best_bin;
+            });
+            mid = (uint32_t)(it - idx.begin());
+            if (mid == start || mid == end) mid = start + n / 2;
+        } else {
+            // median split on the widest centroid axis (also the fallback for coincident centroids)
+            int ax = 0;
+            for (int k = 1; k < 3; ++k)
+                if (cb.hi[k] - cb.lo[k] > cb.hi[ax] - cb.lo[ax]) ax = k;
+            mid = start + n / 2;
+            std::nth_element(idx.begin() + start, idx.begin() + mid, idx.begin() + end,
+                             [&](uint32_t a, uint32_t b) { return cen[3 * a + ax] < cen[3 * b + ax]; });
+        }
+        int32_t l = build(start, mid, depth + 1, max_depth);
+        int32_t r = build(mid, end, depth + 1, max_depth);
+        nodes[id].left = l;
+        nodes[id].right = r;
+        return id;
+    }
+};
+
+}  // namespace
+
+bool build_bvh(const BvhInput& in, int max_leaf, int threads, BvhOutput& out, const char** err) {
+    (void)threads;
+    const size_t n = in.boxes.size();
+    if (max_leaf < 1) max_leaf = 1;
+    if (max_leaf > MAX_LEAF) max_leaf = MAX_LEAF;
+    if (n >= (1u << 26)) { if (err) *err = "too many primitives for the leaf encoding (max 2^26)"; return false; }
+    Builder B(in.boxes, max_leaf);
+    B.cen.resize(3 * n);
+    B.idx.resize(n);
+    for (size_t p = 0; p < n; ++p) {
+        B.idx[p] = (uint32_t)p;
+        for (int k = 0; k < 3; ++k) B.cen[3 * p + k] = 0.5f * (in.boxes[p].lo[k] + in.boxes[p].hi[k]);
+    }
+    B.nodes.reserve(2 * n + 2);
+    uint32_t max_depth = 0;
+    int32_t root = n ? B.build(0, (uint32_t)n, 1, max_depth) : -1;
+
+    // Flatten: inner nodes in depth-first order, leaves folded into their parent's child slots.
+    out.nodes.clear();
+    out.order.clear();
+    out.max_leaf_seen = 0;
+    std::vector<int32_t> stack;
+    auto alloc_node = [&]() {
+        out.nodes.resize(out.nodes.size() + 16, 0.0f);
+        return (int32_t)(out.nodes.size() / 16 - 1);
+    };
+    auto encode_leaf = [&](const BNode& L) -> int32_t {
+        uint32_t first = (uint32_t)out.order.size();
+        for (uint32_t i = 0; i < L.count; ++i) out.order.push_back(B.idx[L.first + i]);
+        if (L.count > out.max_leaf_seen) out.max_leaf_seen = L.count;
+        return (int32_t)~((first << LEAF_COUNT_BITS) | L.count);
+    };
+    auto put_child = [&](int32_t slot, int side, const Aabb& bx, int32_t enc) {
+        float* f = &out.nodes[16 * (size_t)slot];
+        if (side == 0) {
+            f[0] = bx.lo[0]; f[1] = bx.hi[0]; f[2] = bx.lo[1]; f[3] = bx.hi[1];
+            f[8] = bx.lo[2]; f[9] = bx.hi[2];
+            std::memcpy(&f[12], &enc, 4);
+        } else {
+            f[4] = bx.lo[0]; f[5] = bx.hi[0]; f[6] = bx.lo[1]; f[7] = bx.hi[1];
+            f[10] = bx.lo[2]; f[11] = bx.hi[2];
+            std::memcpy(&f[13], &enc, 4);
+        }
+    };
+    // root slot 0: if the whole tree is one leaf, pair it with an empty leaf
+    struct Pending { int32_t bnode; int32_t slot; int side; };
+    std::vector<Pending> work;
+    int32_t slot0 = alloc_node();
+    Aabb none = empty_box();
+    if (root < 0) {
+        put_child(slot0, 0, none, (int32_t)~0u);
+        put_child(slot0, 1, none, (int32_t)~0u);
+    } else if (B.nodes[root].leaf) {
+        put_child(slot0, 0, B.nodes[root].box, encode_leaf(B.nodes[root]));
+        put_child(slot0, 1, none, (int32_t)~0u);
+    } else {
+        work.push_back({B.nodes[root].right, slot0, 1});
+        work.push_back({B.nodes[root].left, slot0, 0});
+        while (!work.empty()) {
+            Pending w = work.back();
+            work.pop_back();
+            const BNode& bn = B.nodes[w.bnode];
+            if (bn.leaf) {
+                put_child(w.slot, w.side, bn.box, encode_leaf(bn));
+            } else {
+                int32_t s = alloc_node();
+                put_child(w.slot, w.side, bn.box, s);
+                work.push_back({bn.right, s, 1});
+                work.push_back({bn.left, s, 0});
+            }
+        }
+    }
+    out.num_nodes = (uint32_t)(out.nodes.size() / 16);
+    out.max_depth = max_depth;
+    if (max_depth + 2 > (uint32_t)TRAVERSAL_STACK) { if (err) *err = "BVH too deep for the traversal stack"; return false; }
+    return true;
+}
+
+}  // namespace rtc

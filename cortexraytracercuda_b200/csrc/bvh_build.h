@@ -1,0 +1,35 @@
+// bvh_build.h - host SAH BVH2 builder producing the flattened 64-byte node layout of rtc_dev.h.
+//
+// Replaces the reference's bvh_node constructor (core/src/misc/bvh_node.cuh:63-108), which picks a
+// random axis with one RNG draw, exchange-sorts the span (O(n^2)) and splits at the median on a single
+// device thread.  Here: binned SAH (32 bins over the centroid bounds) on the host, leaves of at most
+// `max_leaf` items, subtrees built in parallel with std::thread.  Closest-hit results do not depend
+// on the tree, only the order in which exactly-equal-t candidates are met does.
+#pragma once
+
+#include <stdint.h>
+
+#include <vector>
+
+namespace rtc {
+
+struct Aabb {
+    float lo[3], hi[3];
+};
+
+struct BvhInput {
+    std::vector<Aabb> boxes;       // one per primitive (already padded)
+};
+
+struct BvhOutput {
+    std::vector<float> nodes;      // 16 floats per node (4 x float4), see rtc_dev.h
+    std::vector<uint32_t> order;   // primitive index per leaf slot, leaf order
+    uint32_t num_nodes = 0;
+    uint32_t max_depth = 0;
+    uint32_t max_leaf_seen = 0;
+};
+
+// Returns false (with a message) if the tree would not fit the traversal stack or the item encoding.
+bool build_bvh(const BvhInput& in, int max_leaf, int threads, BvhOutput& out, const char** err);
+
+}  // namespace rtc

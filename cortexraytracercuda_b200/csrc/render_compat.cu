@@ -1,0 +1,146 @@
+// render_compat.cu - compat-mode kernels (reference semantics, per-pixel minstd stream).
+//
+// Built with --fmad=false: every float expression restated from the reference is evaluated with
+// the reference's roundings (no FMA contraction), so the only differences left against a g++ build of
+// the reference are the last-ulp results of cos/sin/acos/atan2.  The BVH slab test uses explicit
+// __fmaf_rn, which is unaffected by the flag.
+//
+// Kernels:
+//   rtc_render_compat<ORDER>  one thread per pixel, all samples of the pixel in sequence
+//                             (the render kernel, core/src/gpu.cu:761-790), writes the FP32 sum;
+//   rtc_trace_closest         closest hit of arbitrary rays (hit-identity tests);
+//   rtc_quantize              prepare_pixel_color + 8-bit quantisation + row flip
+//                             (color.cuh:289-309, gpu.cu:792-799, 2098-2107).
+#include "rtc_kernels.h"
+#include "rtc_path.cuh"
+
+namespace rtc {
+
+__device__ __forceinline__ void flush_counters(unsigned long long* counters, uint32_t rays, uint32_t paths,
+                                               uint32_t nodes, uint32_t prims) {
+    if (!counters) return;
+    unsigned long long r = rays, p = paths, n = nodes, q = prims;
+    for (int off = 16; off > 0; off >>= 1) {
+        r += __shfl_down_sync(0xffffffffu, r, off);
+        p += __shfl_down_sync(0xffffffffu, p, off);
+        n += __shfl_down_sync(0xffffffffu, n, off);
+        q += __shfl_down_sync(0xffffffffu, q, off);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(counters + CNT_RAYS, r);
+        atomicAdd(counters + CNT_PATHS, p);
+        atomicAdd(counters + CNT_NODES, n);
+        atomicAdd(counters + CNT_PRIMS, q);
+    }
+}
+
+template <int ORDER>
+__global__ void __launch_bounds__(128) rtc_render_compat(DevScene S, DevParams P, float4* __restrict__ out,
+                                                         unsigned long long* counters, uint32_t* status_word) {
+    const int64_t pixel_index = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool active = pixel_index < P.num_pixels;
+    PathCounters pc{0, 0, 0};
+    uint32_t paths = 0, status = 0;
+    if (active) {
+        const int i = (int)(pixel_index % P.width);
+        const int j = (int)(pixel_index / P.width);
+        Minstd rng;
+        rng.seed(P.seed + (uint32_t)pixel_index);
+        const int sq = P.sqrt_spp;
+        float pr = 0.f, pg = 0.f, pb = 0.f;
+        for (int s_j = 0; s_j < sq; ++s_j) {
+            for (int s_i = 0; s_i < sq; ++s_i) {
+                float ur = rng.uniform();
+                float u = ((float)i + ((float)s_i + ur) / (float)sq) / (float)P.width;
+                float v = ((float)j + ((float)s_j + ur) / (float)sq) / (float)P.height;
+                Ray r = camera_ray<ORDER>(S.cam, u, v, rng);
+                RGB c = trace_sample<false, ORDER>(S, r, P.max_depth, rng, pc, status);
+                pr += c.r;
+                pg += c.g;
+                pb += c.b;
+                ++paths;
+            }
+        }
+        out[pixel_index] = make_float4(pr, pg, pb, 1.0f);
+    }
+    flush_counters(counters, pc.rays, paths, pc.nodes, pc.prims);
+    if (status) atomicOr(status_word, status);
+}
+
+__device__ __forceinline__ int32_t item_gid(const DevScene& S, uint32_t it) {
+    uint32_t kind = it >> 30, idx = it & 0x3fffffffu;
+    switch (kind) {
+    case ITEM_SPHERE: return __ldg(S.sph_aux + idx).y;
+    case ITEM_QUAD: return __float_as_int(__ldg(S.quad + 5 * (size_t)idx + 2).w);
+    case ITEM_LIGHT: return __float_as_int(__ldg(S.light + 6 * (size_t)idx + 2).w);
+    default: return __float_as_int(__ldg(S.tri + 3 * (size_t)idx + 1).w);
+    }
+}
+
+__global__ void __launch_bounds__(128) rtc_trace_closest(DevScene S, const float* __restrict__ rays, uint32_t n,
+                                                         int depth, int max_depth, int32_t* prim, float* tout,
+                                                         uint32_t* status_word) {
+    uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const float* R = rays + 8 * (size_t)k;
+    V3 o = v3(R[0], R[1], R[2]), d = v3(R[4], R[5], R[6]);
+    float t;
+    uint32_t item, status = 0;
+    TraceStats st{0, 0};
+    bool h = closest_hit(S, o, d, R[3], R[7], depth == max_depth, t, item, st, status);
+    if (prim) prim[k] = h ? item_gid(S, item) : -1;
+    if (tout) tout[k] = h ? t : INFINITY;
+    if (status) atomicOr(status_word, status);
+}
+
+// prepare_pixel_color (color.cuh:289-309): NaN -> 0, * (1/spp), sqrt; then
+// int(255.99 * clamp(c, 0, 0.999)) (gpu.cu:792-799) and the PNG row flip (gpu.cu:2098-2107).
+__global__ void rtc_quantize(const float4* __restrict__ sum, uint8_t* __restrict__ rgb8, int width, int height,
+                             int spp) {
+    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= (int64_t)width * height) return;
+    int i = (int)(p % width), j = (int)(p / width);
+    float4 c = sum[p];
+    float ch[3] = {c.x, c.y, c.z};
+    uint8_t* o = rgb8 + ((size_t)(height - j - 1) * width + i) * 3;
+    for (int k = 0; k < 3; ++k) {
+        float x = ch[k] != ch[k] ? 0.0f : ch[k];
+        if (spp > 0) x *= 1.0f / (float)spp;
+        x = sqrtf(x);
+        float cl = x < 0.0f ? 0.0f : (x > 0.999f ? 0.999f : x);
+        int q = (int)(255.99f * cl);
+        o[k] = (uint8_t)q;
+    }
+}
+
+}  // namespace rtc
+
+using namespace rtc;
+
+cudaError_t rtc_launch_render_compat(const DevScene& S, const DevParams& P, float4* out,
+                                     unsigned long long* counters, uint32_t* status, int block, cudaStream_t st) {
+    (void)block;
+    const int threads = 128;
+    const unsigned grid = (unsigned)((P.num_pixels + threads - 1) / threads);
+    if (P.draw_order == 1)
+        rtc_render_compat<1><<<grid, threads, 0, st>>>(S, P, out, counters, status);
+    else
+        rtc_render_compat<0><<<grid, threads, 0, st>>>(S, P, out, counters, status);
+    return cudaGetLastError();
+}
+
+cudaError_t rtc_launch_trace_closest(const DevScene& S, const float* rays, uint32_t n, int depth, int max_depth,
+                                     int32_t* prim, float* t, uint32_t* status, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    const int threads = 128;
+    rtc_trace_closest<<<(n + threads - 1) / threads, threads, 0, st>>>(S, rays, n, depth, max_depth, prim, t, status);
+    return cudaGetLastError();
+}
+
+cudaError_t rtc_launch_quantize(const float4* sum, uint8_t* rgb8, int width, int height, int spp, cudaStream_t st) {
+    int64_t n = (int64_t)width * height;
+    if (n == 0) return cudaSuccess;
+    const int threads = 256;
+    rtc_quantize<<<(unsigned)((n + threads - 1) / threads), threads, 0, st>>>(sum, rgb8, width, height, spp);
+    return cudaGetLastError();
+}

@@ -1,0 +1,729 @@
+// rtc_api.cpp - the C ABI (include/rtc.h): contexts, scene flattening + upload, render dispatch, PNG.
+//
+// Host float arithmetic that feeds the kernels (quad/light planes, triangle edges and normals, the
+// camera frame) restates the reference's constructors operation by operation and is compiled with
+// -ffp-contract=off, so the device sees bit-identical values to what a g++ build of the reference
+// computes.
+#include "../../include/rtc.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "bvh_build.h"
+#include "rtc_dev.h"
+#include "rtc_kernels.h"
+#include "rtc_math.cuh"
+
+using namespace rtc;
+
+namespace {
+thread_local std::string g_err;
+
+rtc_status fail(rtc_status s, const std::string& msg) {
+    g_err = msg;
+    return s;
+}
+rtc_status cuda_fail(cudaError_t e, const char* what) {
+    g_err = std::string(what) + ": " + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? RTC_ERR_OOM : RTC_ERR_CUDA;
+}
+#define RTC_CUDA(call)                                   \
+    do {                                                 \
+        cudaError_t _e = (call);                         \
+        if (_e != cudaSuccess) return cuda_fail(_e, #call); \
+    } while (0)
+
+bool finite3(const float* p) { return std::isfinite(p[0]) && std::isfinite(p[1]) && std::isfinite(p[2]); }
+
+}  // namespace
+
+struct rtc_context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    uint32_t* d_status = nullptr;
+    unsigned long long* d_counters = nullptr;
+    float4* d_out = nullptr;
+    size_t out_cap = 0;         // float4 elements
+    uint8_t* d_rgb8 = nullptr;
+    size_t rgb8_cap = 0;
+    std::mutex mu;
+};
+
+struct rtc_scene {
+    rtc_context* ctx = nullptr;   // creating context; not dereferenced after creation
+    int device = 0;
+    void* d_slab = nullptr;
+    size_t slab_bytes = 0;
+    DevScene dev{};
+    rtc_camera cam{};
+    rtc_scene_info info{};
+};
+
+extern "C" const char* rtc_last_error_string(void) { return g_err.c_str(); }
+
+extern "C" rtc_status rtc_context_create(int device, rtc_context** out) {
+    if (!out) return fail(RTC_ERR_INVALID_ARGUMENT, "out is null");
+    *out = nullptr;
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n <= 0) return fail(RTC_ERR_NO_DEVICE, "no CUDA device available");
+    if (device < 0 || device >= n) return fail(RTC_ERR_INVALID_ARGUMENT, "device index out of range");
+    cudaDeviceProp prop;
+    RTC_CUDA(cudaGetDeviceProperties(&prop, device));
+    if (prop.major < 10) return fail(RTC_ERR_NO_DEVICE, std::string("device is not sm_100: ") + prop.name);
+    RTC_CUDA(cudaSetDevice(device));
+    rtc_context* c = new (std::nothrow) rtc_context();
+    if (!c) return fail(RTC_ERR_OOM, "host allocation failed");
+    c->device = device;
+    cudaError_t e1 = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    cudaError_t e2 = cudaMalloc(&c->d_status, sizeof(uint32_t));
+    cudaError_t e3 = cudaMalloc(&c->d_counters, CNT_N * sizeof(unsigned long long));
+    if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess) {
+        cudaError_t e = e1 != cudaSuccess ? e1 : (e2 != cudaSuccess ? e2 : e3);
+        rtc_context_destroy(c);
+        return cuda_fail(e, "context setup");
+    }
+    *out = c;
+    return RTC_OK;
+}
+
+extern "C" rtc_status rtc_context_destroy(rtc_context* c) {
+    if (!c) return RTC_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    cudaFree(c->d_status);
+    cudaFree(c->d_counters);
+    cudaFree(c->d_out);
+    cudaFree(c->d_rgb8);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return RTC_OK;
+}
+
+// ---------------------------------------------------------------------------------------------------
+// scene flattening
+// ---------------------------------------------------------------------------------------------------
+namespace {
+
+struct PlanarPre {    // quad / directional light constants (quad.cuh:55-67, directional_light.cuh:45-58)
+    V3 n, normal, w;
+    float D, area;
+};
+PlanarPre planar_pre(V3 pos, V3 u, V3 v) {
+    PlanarPre p;
+    p.n = cross(u, v);
+    p.normal = unit(p.n);
+    p.D = dot(p.normal, pos);
+    p.w = divs(p.n, dot(p.n, p.n));
+    p.area = len(p.n);
+    return p;
+}
+
+Aabb pad_box(Aabb b) {
+    // conservative padding so the FMA slab test never culls a primitive its exact test accepts
+    for (int k = 0; k < 3; ++k) {
+        float m = std::max(std::fabs(b.lo[k]), std::fabs(b.hi[k]));
+        float e = 1e-5f * m + 1e-6f + 1e-5f * (b.hi[k] - b.lo[k]);
+        b.lo[k] -= e;
+        b.hi[k] += e;
+    }
+    return b;
+}
+Aabb box_of(const V3* pts, int n) {
+    Aabb b;
+    for (int k = 0; k < 3; ++k) { b.lo[k] = INFINITY; b.hi[k] = -INFINITY; }
+    for (int i = 0; i < n; ++i) {
+        const float c[3] = {pts[i].x, pts[i].y, pts[i].z};
+        for (int k = 0; k < 3; ++k) { b.lo[k] = std::min(b.lo[k], c[k]); b.hi[k] = std::max(b.hi[k], c[k]); }
+    }
+    return pad_box(b);
+}
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+}  // namespace
+
+extern "C" rtc_status rtc_scene_create(rtc_context* ctx, const rtc_scene_desc* d, rtc_scene** out) {
+    if (!ctx || !d || !out) return fail(RTC_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    auto t0 = std::chrono::steady_clock::now();
+    // ---- validation --------------------------------------------------------------------------
+    auto bad = [&](const std::string& m) { return fail(RTC_ERR_BAD_SCENE, m); };
+    if ((d->num_textures && !d->textures) || (d->num_images && !d->images) || (d->num_materials && !d->materials) ||
+        (d->num_dir_lights && !d->dir_lights) || (d->num_spheres && !d->spheres) || (d->num_quads && !d->quads) ||
+        (d->num_meshes && !d->meshes))
+        return bad("count > 0 with a null array");
+    for (uint32_t i = 0; i < d->num_images; ++i)
+        if (!d->images[i].rgb || d->images[i].width <= 0 || d->images[i].height <= 0) return bad("bad image " + std::to_string(i));
+    for (uint32_t i = 0; i < d->num_textures; ++i) {
+        const rtc_texture& t = d->textures[i];
+        if (t.kind == RTC_TEX_SOLID) continue;
+        if (t.kind == RTC_TEX_CHECKER) {
+            if (t.even < 0 || (uint32_t)t.even >= d->num_textures || t.odd < 0 || (uint32_t)t.odd >= d->num_textures)
+                return bad("checker texture " + std::to_string(i) + " references a missing texture");
+            if (!(t.scale != 0.0f) || !std::isfinite(t.scale)) return bad("checker texture with zero scale");
+            continue;
+        }
+        if (t.kind == RTC_TEX_IMAGE) {
+            if (t.image < 0 || (uint32_t)t.image >= d->num_images) return bad("image texture references a missing image");
+            continue;
+        }
+        return bad("unknown texture kind");
+    }
+    for (uint32_t i = 0; i < d->num_materials; ++i) {
+        const rtc_material& m = d->materials[i];
+        if (m.kind < 0 || m.kind > 3) return bad("unknown material kind");
+        if (m.kind != RTC_MAT_DIELECTRIC && (m.texture < 0 || (uint32_t)m.texture >= d->num_textures))
+            return bad("material " + std::to_string(i) + " references a missing texture");
+    }
+    auto mat_ok = [&](int32_t m) { return m >= 0 && (uint32_t)m < d->num_materials; };
+    uint64_t ntri = 0;
+    for (uint32_t i = 0; i < d->num_meshes; ++i) {
+        const rtc_mesh& M = d->meshes[i];
+        if (!mat_ok(M.material)) return bad("mesh " + std::to_string(i) + " has a bad material");
+        if (M.num_triangles && (!M.indices || !M.vertices)) return bad("mesh without vertices/indices");
+        ntri += M.num_triangles;
+    }
+    for (uint32_t i = 0; i < d->num_spheres; ++i)
+        if (!mat_ok(d->spheres[i].material) || !finite3(d->spheres[i].center) || !std::isfinite(d->spheres[i].radius))
+            return bad("sphere " + std::to_string(i) + " is invalid");
+    for (uint32_t i = 0; i < d->num_quads; ++i)
+        if (!mat_ok(d->quads[i].material) || !finite3(d->quads[i].q) || !finite3(d->quads[i].u) || !finite3(d->quads[i].v))
+            return bad("quad " + std::to_string(i) + " is invalid");
+    const uint64_t nprims = (uint64_t)d->num_dir_lights + d->num_spheres + d->num_quads + ntri;
+    if (nprims == 0) return bad("scene has no primitives");
+    if (nprims >= (1ull << 26)) return bad("scene has too many primitives (max 2^26)");
+    if (d->background.kind < 0 || d->background.kind > 2) return bad("unknown background kind");
+    if (d->background.kind == RTC_BG_ENV_MAP &&
+        (!d->background.env_rgb || d->background.env_width <= 0 || d->background.env_height <= 0))
+        return bad("environment map missing");
+
+    // ---- primitives in global order: lights, spheres, quads, triangles ------------------------
+    struct PrimRef { uint8_t kind; uint32_t src; };   // src: index within its own kind (mesh tris flattened)
+    std::vector<PrimRef> prims;
+    prims.reserve(nprims);
+    BvhInput bin;
+    bin.boxes.reserve(nprims);
+    for (uint32_t i = 0; i < d->num_dir_lights; ++i) {
+        const rtc_dir_light& L = d->dir_lights[i];
+        V3 P = v3(L.position), U = v3(L.u), Vv = v3(L.v);
+        V3 hu = mul(0.5f, U), hv = mul(0.5f, Vv);
+        V3 c[4] = {sub(sub(P, hu), hv), add(sub(P, hu), hv), sub(add(P, hu), hv), add(add(P, hu), hv)};
+        bin.boxes.push_back(box_of(c, 4));
+        prims.push_back({ITEM_LIGHT, i});
+    }
+    for (uint32_t i = 0; i < d->num_spheres; ++i) {
+        const rtc_sphere& S = d->spheres[i];
+        float r = std::fabs(S.radius);
+        V3 c[2] = {v3(S.center[0] - r, S.center[1] - r, S.center[2] - r), v3(S.center[0] + r, S.center[1] + r, S.center[2] + r)};
+        bin.boxes.push_back(box_of(c, 2));
+        prims.push_back({ITEM_SPHERE, i});
+    }
+    for (uint32_t i = 0; i < d->num_quads; ++i) {
+        const rtc_quad& Q = d->quads[i];
+        V3 q = v3(Q.q), u = v3(Q.u), v = v3(Q.v);
+        V3 c[4] = {q, add(q, u), add(q, v), add(add(q, u), v)};
+        bin.boxes.push_back(box_of(c, 4));
+        prims.push_back({ITEM_QUAD, i});
+    }
+    std::vector<uint32_t> tri_mesh;   // mesh of each flattened triangle
+    std::vector<uint32_t> tri_face;
+    tri_mesh.reserve(ntri);
+    tri_face.reserve(ntri);
+    {
+        uint32_t t = 0;
+        for (uint32_t m = 0; m < d->num_meshes; ++m) {
+            const rtc_mesh& M = d->meshes[m];
+            for (uint32_t f = 0; f < M.num_triangles; ++f, ++t) {
+                uint32_t ia = M.indices[3 * f], ib = M.indices[3 * f + 1], ic = M.indices[3 * f + 2];
+                if (ia >= M.num_vertices || ib >= M.num_vertices || ic >= M.num_vertices)
+                    return bad("mesh " + std::to_string(m) + " index out of range");
+                V3 c[3] = {v3(M.vertices + 3 * ia), v3(M.vertices + 3 * ib), v3(M.vertices + 3 * ic)};
+                if (!finite3(M.vertices + 3 * ia) || !finite3(M.vertices + 3 * ib) || !finite3(M.vertices + 3 * ic))
+                    return bad("mesh vertex is not finite");
+                bin.boxes.push_back(box_of(c, 3));
+                prims.push_back({ITEM_TRI, t});
+                tri_mesh.push_back(m);
+                tri_face.push_back(f);
+            }
+        }
+    }
+
+    // ---- BVH -----------------------------------------------------------------------------------
+    BvhOutput bvh;
+    const char* berr = nullptr;
+    if (!build_bvh(bin, 4, 0, bvh, &berr)) return bad(berr ? berr : "BVH build failed");
+    auto t1 = std::chrono::steady_clock::now();
+
+    // ---- materials / textures (directional lights get their own diffuse_light + solid texture) --
+    std::vector<int4> tex_i;
+    std::vector<float4> tex_f;
+    for (uint32_t i = 0; i < d->num_textures; ++i) {
+        const rtc_texture& t = d->textures[i];
+        tex_i.push_back(make_int4(t.kind, t.even, t.odd, t.image));
+        float inv = t.kind == RTC_TEX_CHECKER ? 1.0f / t.scale : 0.0f;   // checker_texture.cuh:23
+        tex_f.push_back(make_float4(t.color[0], t.color[1], t.color[2], inv));
+    }
+    std::vector<int4> mat_i;
+    std::vector<float4> mat_f;
+    for (uint32_t i = 0; i < d->num_materials; ++i) {
+        const rtc_material& m = d->materials[i];
+        float fuzz = m.fuzz < 1.0f ? m.fuzz : 1.0f;   // metal::metal (metal.cuh:52)
+        mat_i.push_back(make_int4(m.kind, m.texture, 0, 0));
+        mat_f.push_back(make_float4(fuzz, m.ior, m.intensity, m.directional ? 1.0f : 0.0f));
+    }
+    std::vector<int32_t> light_mat(d->num_dir_lights);
+    for (uint32_t i = 0; i < d->num_dir_lights; ++i) {
+        const rtc_dir_light& L = d->dir_lights[i];
+        int32_t tex = (int32_t)tex_i.size();
+        tex_i.push_back(make_int4(RTC_TEX_SOLID, 0, 0, 0));
+        tex_f.push_back(make_float4(L.color[0], L.color[1], L.color[2], 0.0f));
+        light_mat[i] = (int32_t)mat_i.size();
+        // directional_light: m_mat = new diffuse_light(m_color, intensity, true, invisible)
+        mat_i.push_back(make_int4(RTC_MAT_DIFFUSE_LIGHT, tex, 0, 0));
+        mat_f.push_back(make_float4(0.0f, 0.0f, L.intensity, 1.0f));
+    }
+    std::vector<int4> img_i;
+    std::vector<uint8_t> img_bytes;
+    for (uint32_t i = 0; i < d->num_images; ++i) {
+        const rtc_image& im = d->images[i];
+        size_t off = img_bytes.size();
+        size_t nb = (size_t)im.width * im.height * 3;
+        img_bytes.insert(img_bytes.end(), im.rgb, im.rgb + nb);
+        img_i.push_back(make_int4((int)off, im.width, im.height, 0));
+    }
+
+    // ---- per-kind arrays in leaf order ---------------------------------------------------------
+    std::vector<uint32_t> items(bvh.order.size());
+    std::vector<float4> sph, tri, tri_n, tri_vn, quad, light(6 * (size_t)d->num_dir_lights);
+    std::vector<int2> sph_aux;
+    // global id bases
+    const uint32_t base_sph = d->num_dir_lights, base_quad = base_sph + d->num_spheres, base_tri = base_quad + d->num_quads;
+    for (uint32_t i = 0; i < d->num_dir_lights; ++i) {   // lights keep light-list order (index = light id)
+        const rtc_dir_light& L = d->dir_lights[i];
+        V3 P = v3(L.position), U = v3(L.u), Vv = v3(L.v);
+        PlanarPre pp = planar_pre(P, U, Vv);
+        float4* q = &light[6 * (size_t)i];
+        q[0] = make_float4(pp.normal.x, pp.normal.y, pp.normal.z, pp.D);
+        q[1] = make_float4(P.x, P.y, P.z, ibits(light_mat[i]));
+        q[2] = make_float4(U.x, U.y, U.z, ibits((int32_t)i));
+        q[3] = make_float4(Vv.x, Vv.y, Vv.z, L.invisible ? 1.0f : 0.0f);
+        q[4] = make_float4(pp.w.x, pp.w.y, pp.w.z, pp.area);
+        q[5] = make_float4(L.color[0], L.color[1], L.color[2], L.intensity);
+    }
+    for (size_t k = 0; k < bvh.order.size(); ++k) {
+        const PrimRef& pr = prims[bvh.order[k]];
+        uint32_t typed = 0;
+        switch (pr.kind) {
+        case ITEM_LIGHT: typed = pr.src; break;
+        case ITEM_SPHERE: {
+            const rtc_sphere& S = d->spheres[pr.src];
+            typed = (uint32_t)sph.size();
+            sph.push_back(make_float4(S.center[0], S.center[1], S.center[2], S.radius));
+            sph_aux.push_back(make_int2(S.material, (int)(base_sph + pr.src)));
+        } break;
+        case ITEM_QUAD: {
+            const rtc_quad& Q = d->quads[pr.src];
+            V3 q0 = v3(Q.q), u = v3(Q.u), v = v3(Q.v);
+            PlanarPre pp = planar_pre(q0, u, v);
+            typed = (uint32_t)(quad.size() / 5);
+            quad.push_back(make_float4(pp.normal.x, pp.normal.y, pp.normal.z, pp.D));
+            quad.push_back(make_float4(q0.x, q0.y, q0.z, ibits(Q.material)));
+            quad.push_back(make_float4(u.x, u.y, u.z, ibits((int32_t)(base_quad + pr.src))));
+            quad.push_back(make_float4(v.x, v.y, v.z, 0.0f));
+            quad.push_back(make_float4(pp.w.x, pp.w.y, pp.w.z, 0.0f));
+        } break;
+        default: {
+            const rtc_mesh& M = d->meshes[tri_mesh[pr.src]];
+            uint32_t f = tri_face[pr.src];
+            uint32_t ia = M.indices[3 * f], ib = M.indices[3 * f + 1], ic = M.indices[3 * f + 2];
+            V3 a = v3(M.vertices + 3 * ia), b = v3(M.vertices + 3 * ib), c = v3(M.vertices + 3 * ic);
+            // triangle::triangle (triangle.cuh:87-123): v0_v1, v0_v2, middle_normal
+            V3 e1 = sub(b, a), e2 = sub(c, a);
+            V3 mn = unit(cross(sub(a, b), sub(a, c)));
+            typed = (uint32_t)(tri.size() / 3);
+            int32_t smooth_slot = -1;
+            if (M.smooth && M.normals) {
+                smooth_slot = (int32_t)(tri_vn.size() / 3);
+                for (uint32_t vi : {ia, ib, ic}) {
+                    V3 nn = unit(v3(M.normals + 3 * vi));
+                    tri_vn.push_back(make_float4(nn.x, nn.y, nn.z, 0.0f));
+                }
+            }
+            tri.push_back(make_float4(a.x, a.y, a.z, ibits(M.material)));
+            tri.push_back(make_float4(e1.x, e1.y, e1.z, ibits((int32_t)(base_tri + pr.src))));
+            tri.push_back(make_float4(e2.x, e2.y, e2.z, ibits(smooth_slot)));
+            tri_n.push_back(make_float4(mn.x, mn.y, mn.z, 0.0f));
+        } break;
+        }
+        items[k] = ((uint32_t)pr.kind << 30) | typed;
+    }
+
+    // ---- camera: perspective_camera::initialize (perspective_camera.cuh:41-108) -----------------
+    DevCamera cam{};
+    {
+        const rtc_camera& C = d->camera;
+        float theta = C.vfov * 3.14159265358979323846f / 180.0f;   // degrees_to_radians (math_utils.cuh)
+        float half_height = std::tan(theta / 2.0f);
+        float ratio = C.aspect;
+        float focus = C.focus;
+        V3 lookfrom = v3(C.look_from), lookat = v3(C.look_at), vup = v3(C.up);
+        V3 w = unit(sub(lookfrom, lookat));
+        V3 u = unit(cross(vup, w));
+        V3 v = cross(w, u);
+        float half_width = ratio * half_height;
+        V3 origin = lookfrom;
+        V3 llc = sub(sub(sub(origin, mul(half_width * focus, u)), mul(half_height * focus, v)), mul(focus, w));
+        V3 horizontal = mul(2.0f * half_width * focus, u);
+        V3 vertical = mul(2.0f * half_height * focus, v);
+        const V3 vals[6] = {origin, llc, horizontal, vertical, u, v};
+        float* dst[6] = {cam.origin, cam.llc, cam.horizontal, cam.vertical, cam.u, cam.v};
+        for (int k = 0; k < 6; ++k) { dst[k][0] = vals[k].x; dst[k][1] = vals[k].y; dst[k][2] = vals[k].z; }
+        cam.lens_radius = C.aperture / 2.0f;
+        cam.time0 = 0.0f;
+        cam.time1 = 1.0f;
+        if (!std::isfinite(cam.llc[0] + cam.llc[1] + cam.llc[2] + horizontal.x + vertical.y))
+            return bad("degenerate camera");
+    }
+
+    // ---- one device slab ----------------------------------------------------------------------
+    struct Chunk { const void* src; size_t bytes; size_t off; };
+    std::vector<Chunk> chunks;
+    size_t total = 0;
+    auto add_chunk = [&](const void* src, size_t bytes) {
+        size_t off = total;
+        chunks.push_back({src, bytes, off});
+        total = align256(total + std::max<size_t>(bytes, 16));
+        return off;
+    };
+    size_t o_nodes = add_chunk(bvh.nodes.data(), bvh.nodes.size() * sizeof(float));
+    size_t o_items = add_chunk(items.data(), items.size() * 4);
+    size_t o_sph = add_chunk(sph.data(), sph.size() * 16);
+    size_t o_sphx = add_chunk(sph_aux.data(), sph_aux.size() * 8);
+    size_t o_tri = add_chunk(tri.data(), tri.size() * 16);
+    size_t o_trin = add_chunk(tri_n.data(), tri_n.size() * 16);
+    size_t o_trivn = add_chunk(tri_vn.data(), tri_vn.size() * 16);
+    size_t o_quad = add_chunk(quad.data(), quad.size() * 16);
+    size_t o_light = add_chunk(light.data(), light.size() * 16);
+    size_t o_mi = add_chunk(mat_i.data(), mat_i.size() * 16);
+    size_t o_mf = add_chunk(mat_f.data(), mat_f.size() * 16);
+    size_t o_ti = add_chunk(tex_i.data(), tex_i.size() * 16);
+    size_t o_tf = add_chunk(tex_f.data(), tex_f.size() * 16);
+    size_t o_img = add_chunk(img_i.data(), img_i.size() * 16);
+    size_t o_imgb = add_chunk(img_bytes.data(), img_bytes.size());
+    size_t env_bytes = d->background.kind == RTC_BG_ENV_MAP
+                           ? (size_t)d->background.env_width * d->background.env_height * 3 * sizeof(float) : 0;
+    size_t o_env = add_chunk(env_bytes ? d->background.env_rgb : nullptr, env_bytes);
+
+    rtc_scene* s = new (std::nothrow) rtc_scene();
+    if (!s) return fail(RTC_ERR_OOM, "host allocation failed");
+    s->ctx = ctx;
+    s->device = ctx->device;
+    cudaSetDevice(ctx->device);
+    cudaError_t e = cudaMalloc(&s->d_slab, total);
+    if (e != cudaSuccess) { delete s; return cuda_fail(e, "cudaMalloc(scene)"); }
+    s->slab_bytes = total;
+    uint8_t* base = (uint8_t*)s->d_slab;
+    for (const Chunk& c : chunks) {
+        if (!c.src || !c.bytes) continue;
+        e = cudaMemcpyAsync(base + c.off, c.src, c.bytes, cudaMemcpyHostToDevice, ctx->stream);
+        if (e != cudaSuccess) { cudaFree(s->d_slab); delete s; return cuda_fail(e, "scene upload"); }
+    }
+    e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) { cudaFree(s->d_slab); delete s; return cuda_fail(e, "scene upload"); }
+
+    DevScene& D = s->dev;
+    D.nodes = (const float4*)(base + o_nodes);
+    D.items = (const uint32_t*)(base + o_items);
+    D.sph = (const float4*)(base + o_sph);
+    D.sph_aux = (const int2*)(base + o_sphx);
+    D.tri = (const float4*)(base + o_tri);
+    D.tri_n = (const float4*)(base + o_trin);
+    D.tri_vn = (const float4*)(base + o_trivn);
+    D.quad = (const float4*)(base + o_quad);
+    D.light = (const float4*)(base + o_light);
+    D.mat_i = (const int4*)(base + o_mi);
+    D.mat_f = (const float4*)(base + o_mf);
+    D.tex_i = (const int4*)(base + o_ti);
+    D.tex_f = (const float4*)(base + o_tf);
+    D.images = (const int4*)(base + o_img);
+    D.image_bytes = (const uint8_t*)(base + o_imgb);
+    D.num_nodes = bvh.num_nodes;
+    D.num_items = (uint32_t)items.size();
+    D.num_lights = d->num_dir_lights;
+    D.num_materials = (uint32_t)mat_i.size();
+    D.num_textures = (uint32_t)tex_i.size();
+    D.num_images = (uint32_t)img_i.size();
+    D.num_sph = (uint32_t)sph.size();
+    D.num_tri = (uint32_t)tri_n.size();
+    D.num_quad = (uint32_t)(quad.size() / 5);
+    D.cam = cam;
+    D.bg.kind = d->background.kind;
+    for (int k = 0; k < 3; ++k) { D.bg.color[k] = d->background.color[k]; D.bg.top[k] = d->background.top[k]; }
+    D.bg.env = env_bytes ? (const float*)(base + o_env) : nullptr;
+    D.bg.env_w = d->background.env_width;
+    D.bg.env_h = d->background.env_height;
+    s->cam = d->camera;
+    s->info.num_primitives = (uint32_t)nprims;
+    s->info.num_lights = d->num_dir_lights;
+    s->info.num_nodes = bvh.num_nodes;
+    s->info.max_leaf_size = bvh.max_leaf_seen;
+    s->info.device_bytes = total;
+    s->info.build_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    *out = s;
+    return RTC_OK;
+}
+
+extern "C" rtc_status rtc_scene_destroy(rtc_scene* s) {
+    // A scene may outlive its context: only its own device id is used here (cudaFree synchronises
+    // with the device before releasing the memory).
+    if (!s) return RTC_OK;
+    cudaSetDevice(s->device);
+    cudaFree(s->d_slab);
+    delete s;
+    return RTC_OK;
+}
+
+extern "C" rtc_status rtc_scene_get_info(const rtc_scene* s, rtc_scene_info* info) {
+    if (!s || !info) return fail(RTC_ERR_INVALID_ARGUMENT, "null argument");
+    *info = s->info;
+    return RTC_OK;
+}
+
+// ---------------------------------------------------------------------------------------------------
+// render
+// ---------------------------------------------------------------------------------------------------
+namespace {
+
+rtc_status check_params(const rtc_render_params* p) {
+    if (!p) return fail(RTC_ERR_INVALID_ARGUMENT, "params is null");
+    if (p->width <= 0 || p->height <= 0) return fail(RTC_ERR_INVALID_ARGUMENT, "width/height must be positive");
+    if ((int64_t)p->width * p->height > (1ll << 31)) return fail(RTC_ERR_INVALID_ARGUMENT, "image too large");
+    if (p->spp <= 0) return fail(RTC_ERR_INVALID_ARGUMENT, "spp must be positive");
+    if (p->max_depth <= 0 || p->max_depth > 100000) return fail(RTC_ERR_INVALID_ARGUMENT, "max_depth out of range");
+    if (p->mode != RTC_MODE_COMPAT && p->mode != RTC_MODE_CLEAN) return fail(RTC_ERR_INVALID_ARGUMENT, "unknown mode");
+    if (p->draw_order != RTC_DRAW_ORDER_DEVICE && p->draw_order != RTC_DRAW_ORDER_HOST)
+        return fail(RTC_ERR_INVALID_ARGUMENT, "unknown draw order");
+    return RTC_OK;
+}
+
+DevParams dev_params(const rtc_render_params* p) {
+    DevParams P;
+    P.width = p->width;
+    P.height = p->height;
+    P.spp = p->spp;
+    P.sqrt_spp = (int)std::sqrt((double)p->spp);   // gpu.cu:1989
+    P.max_depth = p->max_depth;
+    P.seed = p->seed;
+    P.draw_order = p->draw_order;
+    P.num_pixels = (int64_t)p->width * p->height;
+    return P;
+}
+
+rtc_status launch(rtc_context* c, const rtc_scene* s, const rtc_render_params* p, float4* d_out,
+                  unsigned long long* d_counters, cudaStream_t st) {
+    DevParams P = dev_params(p);
+    cudaError_t e = p->mode == RTC_MODE_COMPAT
+                        ? rtc_launch_render_compat(s->dev, P, d_out, d_counters, c->d_status, p->block_size, st)
+                        : rtc_launch_render_clean(s->dev, P, d_out, d_counters, c->d_status, p->block_size, st);
+    if (e != cudaSuccess) return cuda_fail(e, "render launch");
+    return RTC_OK;
+}
+
+rtc_status read_status(rtc_context* c) {
+    uint32_t st = 0;
+    RTC_CUDA(cudaMemcpyAsync(&st, c->d_status, 4, cudaMemcpyDeviceToHost, c->stream));
+    RTC_CUDA(cudaStreamSynchronize(c->stream));
+    if (st) {
+        char buf[128];
+        std::snprintf(buf, sizeof buf, "kernel status word 0x%x (1=stack 2=item 4=material 8=texture 16=timeout)", st);
+        return fail((st & STATUS_TIMEOUT) ? RTC_ERR_TIMEOUT : RTC_ERR_DEVICE_CHECK, buf);
+    }
+    return RTC_OK;
+}
+
+}  // namespace
+
+extern "C" rtc_status rtc_render(rtc_context* c, const rtc_scene* s, const rtc_render_params* p, float* radiance_sum,
+                                 uint8_t* rgb8) {
+    if (!c || !s) return fail(RTC_ERR_INVALID_ARGUMENT, "null context/scene");
+    rtc_status r = check_params(p);
+    if (r != RTC_OK) return r;
+    std::lock_guard<std::mutex> lk(c->mu);
+    RTC_CUDA(cudaSetDevice(c->device));
+    const size_t npix = (size_t)p->width * p->height;
+    if (c->out_cap < npix) {
+        cudaFree(c->d_out);
+        c->d_out = nullptr;
+        c->out_cap = 0;
+        RTC_CUDA(cudaMalloc(&c->d_out, npix * sizeof(float4)));
+        c->out_cap = npix;
+    }
+    if (rgb8 && c->rgb8_cap < npix * 3) {
+        cudaFree(c->d_rgb8);
+        c->d_rgb8 = nullptr;
+        c->rgb8_cap = 0;
+        RTC_CUDA(cudaMalloc(&c->d_rgb8, npix * 3));
+        c->rgb8_cap = npix * 3;
+    }
+    RTC_CUDA(cudaMemsetAsync(c->d_status, 0, 4, c->stream));
+    r = launch(c, s, p, c->d_out, nullptr, c->stream);
+    if (r != RTC_OK) return r;
+    if (rgb8) {
+        RTC_CUDA(rtc_launch_quantize(c->d_out, c->d_rgb8, p->width, p->height, p->spp, c->stream));
+        RTC_CUDA(cudaMemcpyAsync(rgb8, c->d_rgb8, npix * 3, cudaMemcpyDeviceToHost, c->stream));
+    }
+    if (radiance_sum)
+        RTC_CUDA(cudaMemcpyAsync(radiance_sum, c->d_out, npix * sizeof(float4), cudaMemcpyDeviceToHost, c->stream));
+    RTC_CUDA(cudaStreamSynchronize(c->stream));
+    return read_status(c);
+}
+
+extern "C" rtc_status rtc_render_device(rtc_context* c, const rtc_scene* s, const rtc_render_params* p,
+                                        float* d_radiance_sum, uint8_t* d_rgb8, unsigned long long* d_counters,
+                                        void* stream) {
+    if (!c || !s || !d_radiance_sum) return fail(RTC_ERR_INVALID_ARGUMENT, "null argument");
+    if (((uintptr_t)d_radiance_sum & 15u) != 0) return fail(RTC_ERR_INVALID_ARGUMENT, "radiance buffer must be 16-byte aligned");
+    rtc_status r = check_params(p);
+    if (r != RTC_OK) return r;
+    cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+    RTC_CUDA(cudaSetDevice(c->device));
+    r = launch(c, s, p, (float4*)d_radiance_sum, d_counters, st);
+    if (r != RTC_OK) return r;
+    if (d_rgb8) RTC_CUDA(rtc_launch_quantize((const float4*)d_radiance_sum, d_rgb8, p->width, p->height, p->spp, st));
+    return RTC_OK;
+}
+
+extern "C" rtc_status rtc_trace_closest(rtc_context* c, const rtc_scene* s, const float* rays, uint32_t n,
+                                        int32_t depth, int32_t max_depth, int32_t* prim, float* t) {
+    if (!c || !s || (n && !rays)) return fail(RTC_ERR_INVALID_ARGUMENT, "null argument");
+    if (n == 0) return RTC_OK;
+    std::lock_guard<std::mutex> lk(c->mu);
+    RTC_CUDA(cudaSetDevice(c->device));
+    float* d_rays = nullptr;
+    int32_t* d_prim = nullptr;
+    float* d_t = nullptr;
+    cudaError_t e = cudaMalloc(&d_rays, (size_t)n * 8 * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&d_prim, (size_t)n * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&d_t, (size_t)n * 4);
+    rtc_status r = RTC_OK;
+    if (e != cudaSuccess) r = cuda_fail(e, "cudaMalloc(trace)");
+    if (r == RTC_OK) {
+        e = cudaMemcpyAsync(d_rays, rays, (size_t)n * 8 * sizeof(float), cudaMemcpyHostToDevice, c->stream);
+        if (e == cudaSuccess) e = cudaMemsetAsync(c->d_status, 0, 4, c->stream);
+        if (e == cudaSuccess) e = rtc_launch_trace_closest(s->dev, d_rays, n, depth, max_depth, d_prim, d_t, c->d_status, c->stream);
+        if (e == cudaSuccess && prim) e = cudaMemcpyAsync(prim, d_prim, (size_t)n * 4, cudaMemcpyDeviceToHost, c->stream);
+        if (e == cudaSuccess && t) e = cudaMemcpyAsync(t, d_t, (size_t)n * 4, cudaMemcpyDeviceToHost, c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) r = cuda_fail(e, "trace_closest");
+    }
+    cudaFree(d_rays);
+    cudaFree(d_prim);
+    cudaFree(d_t);
+    if (r != RTC_OK) return r;
+    return read_status(c);
+}
+
+// ---------------------------------------------------------------------------------------------------
+// PNG (stored deflate blocks; the reference writes its PNG with stb_image_write, gpu.cu:2110)
+// ---------------------------------------------------------------------------------------------------
+namespace {
+uint32_t crc_table[256];
+std::once_flag crc_once;
+void crc_init() {
+    for (uint32_t n = 0; n < 256; ++n) {
+        uint32_t c = n;
+        for (int k = 0; k < 8; ++k) c = (c & 1) ? 0xedb88320u ^ (c >> 1) : c >> 1;
+        crc_table[n] = c;
+    }
+}
+uint32_t crc32(const uint8_t* p, size_t n, uint32_t c = 0xffffffffu) {
+    for (size_t i = 0; i < n; ++i) c = crc_table[(c ^ p[i]) & 0xff] ^ (c >> 8);
+    return c;
+}
+void put32(std::vector<uint8_t>& v, uint32_t x) {
+    v.push_back(x >> 24); v.push_back((x >> 16) & 0xff); v.push_back((x >> 8) & 0xff); v.push_back(x & 0xff);
+}
+void chunk(std::vector<uint8_t>& out, const char* type, const std::vector<uint8_t>& data) {
+    put32(out, (uint32_t)data.size());
+    size_t start = out.size();
+    out.insert(out.end(), type, type + 4);
+    out.insert(out.end(), data.begin(), data.end());
+    uint32_t c = crc32(out.data() + start, out.size() - start) ^ 0xffffffffu;
+    put32(out, c);
+}
+}  // namespace
+
+extern "C" rtc_status rtc_write_png(const char* path, const uint8_t* rgb8, int width, int height) {
+    if (!path || !rgb8 || width <= 0 || height <= 0) return fail(RTC_ERR_INVALID_ARGUMENT, "bad PNG arguments");
+    std::call_once(crc_once, crc_init);
+    std::vector<uint8_t> raw;
+    raw.reserve((size_t)height * (width * 3 + 1));
+    for (int y = 0; y < height; ++y) {
+        raw.push_back(0);   // filter: none
+        raw.insert(raw.end(), rgb8 + (size_t)y * width * 3, rgb8 + (size_t)(y + 1) * width * 3);
+    }
+    std::vector<uint8_t> z;
+    z.push_back(0x78);
+    z.push_back(0x01);
+    uint32_t a = 1, b = 0;
+    for (uint8_t x : raw) { a = (a + x) % 65521u; b = (b + a) % 65521u; }
+    size_t pos = 0;
+    do {
+        size_t n = std::min<size_t>(65535, raw.size() - pos);
+        bool last = pos + n == raw.size();
+        z.push_back(last ? 1 : 0);
+        z.push_back(n & 0xff); z.push_back(n >> 8);
+        z.push_back(~n & 0xff); z.push_back((~n >> 8) & 0xff);
+        z.insert(z.end(), raw.begin() + pos, raw.begin() + pos + n);
+        pos += n;
+    } while (pos < raw.size());
+    put32(z, (b << 16) | a);
+    std::vector<uint8_t> png = {0x89, 'P', 'N', 'G', '\r', '\n', 0x1a, '\n'};
+    std::vector<uint8_t> ihdr;
+    put32(ihdr, (uint32_t)width);
+    put32(ihdr, (uint32_t)height);
+    ihdr.insert(ihdr.end(), {8, 2, 0, 0, 0});
+    chunk(png, "IHDR", ihdr);
+    chunk(png, "IDAT", z);
+    chunk(png, "IEND", {});
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return fail(RTC_ERR_IO, std::string("cannot open ") + path);
+    size_t w = std::fwrite(png.data(), 1, png.size(), f);
+    int cl = std::fclose(f);
+    if (w != png.size() || cl != 0) return fail(RTC_ERR_IO, std::string("cannot write ") + path);
+    return RTC_OK;
+}
+
+extern "C" rtc_status rtc_launchGPU(const rtc_scene_desc* scene, int width, int height, int spp, int max_depth,
+                                    int tx, int ty, const char* filepath, int quiet_mode) {
+    (void)tx;
+    (void)ty;
+    if (!scene || !filepath) return fail(RTC_ERR_INVALID_ARGUMENT, "null argument");
+    rtc_context* c = nullptr;
+    rtc_status r = rtc_context_create(0, &c);
+    if (r != RTC_OK) return r;
+    rtc_scene* s = nullptr;
+    r = rtc_scene_create(c, scene, &s);
+    if (r == RTC_OK) {
+        rtc_render_params p{width, height, spp, max_depth, 2580u, RTC_MODE_COMPAT, RTC_DRAW_ORDER_DEVICE, 0};
+        std::vector<uint8_t> img((size_t)std::max(0, width) * std::max(0, height) * 3);
+        if (!quiet_mode) std::printf("[INFO] Rendering %dx%d %d samples > %s\n", width, height, spp, filepath);
+        r = rtc_render(c, s, &p, nullptr, img.data());
+        if (r == RTC_OK) r = rtc_write_png(filepath, img.data(), width, height);
+    }
+    std::string keep = g_err;
+    rtc_scene_destroy(s);
+    rtc_context_destroy(c);
+    g_err = keep;
+    return r;
+}

@@ -1,0 +1,103 @@
+// rtc_dev.h - device-resident scene layout (shared by the host builder and the kernels).
+//
+// HBM layout, all arrays 16-byte aligned float4/int4 so every fetch is one vectorised load:
+//
+//   nodes      BVH2, 4 x float4 = 64 B per node:
+//                n0 = (L.lo.x, L.hi.x, L.lo.y, L.hi.y)   n1 = (R.lo.x, R.hi.x, R.lo.y, R.hi.y)
+//                n2 = (L.lo.z, L.hi.z, R.lo.z, R.hi.z)   n3 = (child L, child R, -, -) as int bits
+//              child >= 0: inner node index; child < 0: leaf, ~child = (first_item << 5) | count.
+//   items      uint32 per leaf entry, leaf order: (kind << 30) | index into that kind's array.
+//   sph        float4 (center.xyz, radius)                      16 B / sphere  (leaf order)
+//   sph_aux    int2   (material, global id)
+//   tri        3 x float4: (v0.xyz, material bits) (v1-v0, gid bits) (v2-v0, smooth-normal slot or -1)
+//                                                               48 B / triangle test (leaf order)
+//   tri_n      float4 (middle_normal.xyz, -)                    fetched once per final hit only
+//   tri_vn     3 x float4 vertex normals (unit_vector'd) for smooth triangles
+//   quad       5 x float4: (n.xyz, D) (Q.xyz, mat) (u.xyz, gid) (v.xyz, -) (w.xyz, -)
+//   light      6 x float4: (n.xyz, D) (P.xyz, mat) (u.xyz, gid) (v.xyz, invisible) (w.xyz, area)
+//                          (emit.rgb * 1, intensity)       - directional lights in light-list order
+//   materials  int4 (kind, texture, -, -) + float4 (fuzz, ior, intensity, directional)
+//   textures   int4 (kind, even, odd, image) + float4 (color.rgb, inv_scale)
+//   images     int4 (byte offset, width, height, -) into image_bytes
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace rtc {
+
+enum ItemKind : uint32_t { ITEM_SPHERE = 0, ITEM_QUAD = 1, ITEM_TRI = 2, ITEM_LIGHT = 3 };
+constexpr int LEAF_COUNT_BITS = 5;
+constexpr int MAX_LEAF = 31;
+constexpr int TRAVERSAL_STACK = 64;
+
+// kernel status word bits (device -> host)
+enum StatusBits : uint32_t {
+    STATUS_STACK_OVERFLOW = 1u,
+    STATUS_BAD_ITEM = 2u,
+    STATUS_BAD_MATERIAL = 4u,
+    STATUS_BAD_TEXTURE = 8u,
+    STATUS_TIMEOUT = 16u,
+};
+
+struct DevCamera {
+    float origin[3];
+    float llc[3];
+    float horizontal[3];
+    float vertical[3];
+    float u[3];
+    float v[3];
+    float lens_radius;
+    float time0, time1;
+};
+
+struct DevBackground {
+    int kind;
+    float color[3];
+    float top[3];
+    const float* env;   // device, env_w*env_h*3
+    int env_w, env_h;
+};
+
+struct DevScene {
+    const float4* nodes;
+    const uint32_t* items;
+    const float4* sph;
+    const int2* sph_aux;
+    const float4* tri;
+    const float4* tri_n;
+    const float4* tri_vn;
+    const float4* quad;
+    const float4* light;
+    const int4* mat_i;
+    const float4* mat_f;
+    const int4* tex_i;
+    const float4* tex_f;
+    const int4* images;
+    const uint8_t* image_bytes;
+    uint32_t num_nodes;
+    uint32_t num_items;
+    uint32_t num_lights;
+    uint32_t num_materials;
+    uint32_t num_textures;
+    uint32_t num_images;
+    uint32_t num_sph, num_tri, num_quad;
+    DevCamera cam;
+    DevBackground bg;
+};
+
+// Per-launch parameters.
+struct DevParams {
+    int width, height;
+    int spp;           // as given (compat divides by it)
+    int sqrt_spp;      // compat: int(sqrt(spp))
+    int max_depth;
+    uint32_t seed;
+    int draw_order;    // 0 device (left to right), 1 host (right to left)
+    int64_t num_pixels;
+};
+
+// Counters (unsigned long long on device).
+enum CounterIdx { CNT_RAYS = 0, CNT_PATHS = 1, CNT_NODES = 2, CNT_PRIMS = 3, CNT_N = 4 };
+
+}  // namespace rtc

@@ -1,0 +1,265 @@
+// rtc_path.cuh - camera rays and the per-sample path loop.
+//
+// Compat mode restates camera::ray_color (core/src/cameras/camera.cuh:149-264) with the reference's
+// materials and PDFs, consuming one thrust::minstd_rand stream per pixel in the reference's order.
+// Clean mode keeps the same materials but draws from a counter-based stream per (pixel, sample),
+// samples the light list only when it is non-empty, and traces spp samples.
+#pragma once
+
+#include "rtc_trace.cuh"
+
+namespace rtc {
+
+// Multi-draw expressions: the reference builds vectors from several get_real() calls inside one
+// constructor call or overloaded-operator expression, whose evaluation order C++ leaves open.
+// ORDER 0 consumes them left to right (nvcc device build), ORDER 1 right to left (g++ build).
+template <int ORDER, class R>
+__device__ __forceinline__ void draw2(R& rng, float& first_arg, float& second_arg) {
+    if (ORDER == 0) { first_arg = rng.uniform(); second_arg = rng.uniform(); }
+    else { second_arg = rng.uniform(); first_arg = rng.uniform(); }
+}
+template <int ORDER, class R>
+__device__ __forceinline__ void draw3(R& rng, float& a, float& b, float& c) {
+    if (ORDER == 0) { a = rng.uniform(); b = rng.uniform(); c = rng.uniform(); }
+    else { c = rng.uniform(); b = rng.uniform(); a = rng.uniform(); }
+}
+
+// random_in_unit_disk (gpu_randomizer.cuh:61-67)
+template <int ORDER, class R>
+__device__ __forceinline__ V3 random_in_unit_disk(R& rng) {
+    V3 p;
+    do {
+        float a, b;
+        draw2<ORDER>(rng, a, b);
+        p = v3(2.0f * a - 1.0f, 2.0f * b - 1.0f, 2.0f * 0.0f - 0.0f);
+    } while (dot(p, p) >= 1.0f);
+    return p;
+}
+
+// random_in_unit_sphere (gpu_randomizer.cuh:70-76); l1() is the squared length (vector3.cuh:86-88)
+template <int ORDER, class R>
+__device__ __forceinline__ V3 random_in_unit_sphere(R& rng) {
+    V3 p;
+    do {
+        float a, b, c;
+        draw3<ORDER>(rng, a, b, c);
+        p = v3(2.0f * a - 1.0f, 2.0f * b - 1.0f, 2.0f * c - 1.0f);
+    } while (p.x * p.x + p.y * p.y + p.z * p.z >= 1.0f);
+    return p;
+}
+
+// cos/sin of random_cosine_direction: compat evaluates in double and rounds, which agrees with
+// glibc's cosf/sinf on ~98.7% of inputs and is within 1 ulp otherwise; clean uses sincosf.
+template <bool CLEAN>
+__device__ __forceinline__ void cos_sin(float phi, float& c, float& s) {
+    if (CLEAN) {
+        sincosf(phi, &s, &c);
+    } else {
+        double sd, cd;
+        sincos((double)phi, &sd, &cd);
+        c = (float)cd;
+        s = (float)sd;
+    }
+}
+
+// random_cosine_direction (gpu_randomizer.cuh:121-133)
+template <bool CLEAN, class R>
+__device__ __forceinline__ V3 random_cosine_direction(R& rng) {
+    const float r1 = rng.uniform();
+    const float r2 = rng.uniform();
+    const float phi = 6.28318530718f * r1;
+    const float z = sqrtf(1.0f - r2);
+    const float r2s = sqrtf(r2);
+    float c, s;
+    cos_sin<CLEAN>(phi, c, s);
+    return v3(c * r2s, s * r2s, z);
+}
+
+// onb::build_from_w (onb.cuh:122-128)
+struct Onb {
+    V3 u, v, w;
+};
+__device__ __forceinline__ Onb build_from_w(V3 n) {
+    Onb b;
+    b.w = unit(n);
+    V3 a = (fabsf(b.w.x) > 0.9f) ? v3(0.f, 1.f, 0.f) : v3(1.f, 0.f, 0.f);
+    b.v = unit(cross(b.w, a));
+    b.u = cross(b.w, b.v);
+    return b;
+}
+// onb::local (onb.cuh:117-120): a.x*u + a.y*v + a.z*w
+__device__ __forceinline__ V3 onb_local(const Onb& b, V3 a) {
+    return add(add(mul(a.x, b.u), mul(a.y, b.v)), mul(a.z, b.w));
+}
+
+// directional_light::random (directional_light.cuh:165-171): P + (U-0.5)*u + (U-0.5)*v - o
+template <int ORDER, class R>
+__device__ __forceinline__ V3 light_random(const DevScene& S, uint32_t li, V3 o, R& rng) {
+    const float4* q = S.light + 6 * (size_t)li;
+    float4 P = __ldg(q + 1), U = __ldg(q + 2), Vv = __ldg(q + 3);
+    float ru, rv;
+    draw2<ORDER>(rng, ru, rv);
+    V3 p = add(add(v3(P.x, P.y, P.z), mul(ru - 0.5f, v3(U.x, U.y, U.z))), mul(rv - 0.5f, v3(Vv.x, Vv.y, Vv.z)));
+    return sub(p, o);
+}
+
+struct Ray {
+    V3 o, d;
+    float time;
+};
+
+// perspective_camera::get_ray (perspective_camera.cuh:112-117): the disk sample and the time sample
+// are drawn even when the aperture is zero.
+template <int ORDER, class R>
+__device__ __forceinline__ Ray camera_ray(const DevCamera& c, float s, float t, R& rng) {
+    V3 rd = mul(c.lens_radius, random_in_unit_disk<ORDER>(rng));
+    V3 offset = add(mul(v3(c.u), rd.x), mul(v3(c.v), rd.y));
+    float time = c.time0 + rng.uniform() * (c.time1 - c.time0);
+    Ray r;
+    r.o = add(v3(c.origin), offset);
+    r.d = sub(sub(add(add(v3(c.llc), mul(s, v3(c.horizontal))), mul(t, v3(c.vertical))), v3(c.origin)), offset);
+    r.time = time;
+    return r;
+}
+
+struct PathCounters {
+    uint32_t rays, nodes, prims;
+};
+
+// One camera sample: camera::ray_color (camera.cuh:149-264).  Returns the radiance of the sample.
+// All additions of the reference are kept, including the zero emission of non-emitting materials,
+// so NaN/Inf propagate exactly as in the reference.
+template <bool CLEAN, int ORDER, class R>
+__device__ __forceinline__ RGB trace_sample(const DevScene& S, Ray r, int max_depth, R& rng, PathCounters& pc,
+                                            uint32_t& status) {
+    RGB result = rgb(0.f, 0.f, 0.f);
+    RGB att = rgb(1.f, 1.f, 1.f);
+    TraceStats st{0, 0};
+    for (int depth = max_depth; depth > 0; --depth) {
+        const bool hide = depth == max_depth;
+        float t;
+        uint32_t item;
+        pc.rays++;
+        if (!closest_hit(S, r.o, r.d, 0.00001f, 3.402823466e+38f, hide, t, item, st, status)) {
+            RGB bg = background(S, r.d);
+            result.r += att.r * bg.r;
+            result.g += att.g * bg.g;
+            result.b += att.b * bg.b;
+            break;
+        }
+        Hit h;
+        finalize_hit(S, item, t, r.o, r.d, h);
+        if ((uint32_t)h.mat >= S.num_materials) { status |= STATUS_BAD_MATERIAL; break; }
+        int4 mi = __ldg(S.mat_i + h.mat);
+        float4 mf = __ldg(S.mat_f + h.mat);
+        // emitted (diffuse_light.cuh:45-67; material::emitted returns (0,0,0) otherwise)
+        RGB em = rgb(0.f, 0.f, 0.f);
+        bool em_alpha0 = false;
+        if (mi.x == 3) {
+            if (mf.w != 0.0f && !h.front) {
+                em_alpha0 = true;   // RGBA(0,0,0,0): back face of a one-sided light
+            } else {
+                RGB tv = texture_value(S, mi.y, h.u, h.v, h.p, status);
+                em = rgb(tv.r * mf.z, tv.g * mf.z, tv.b * mf.z);
+            }
+        }
+        if (em_alpha0) {
+            // "invisible" re-hit from just behind the light (camera.cuh:177-183); rec is replaced only
+            // when the re-hit finds something, and `emitted` is not recomputed.
+            float t2;
+            uint32_t item2;
+            pc.rays++;
+            if (closest_hit(S, r.o, r.d, h.t + 0.001f, 3.402823466e+38f, hide, t2, item2, st, status)) {
+                finalize_hit(S, item2, t2, r.o, r.d, h);
+                if ((uint32_t)h.mat >= S.num_materials) { status |= STATUS_BAD_MATERIAL; break; }
+                mi = __ldg(S.mat_i + h.mat);
+                mf = __ldg(S.mat_f + h.mat);
+            }
+        }
+        if (mi.x == 3) {   // diffuse_light::scatter -> material::scatter returns false
+            result.r += att.r * em.r;
+            result.g += att.g * em.g;
+            result.b += att.b * em.b;
+            break;
+        }
+        result.r += att.r * em.r;
+        result.g += att.g * em.g;
+        result.b += att.b * em.b;
+
+        if (mi.x == 1) {
+            // metal::scatter (metal.cuh:57-64)
+            RGB a = texture_value(S, mi.y, h.u, h.v, h.p, status);
+            V3 refl = reflect(unit(r.d), h.n);
+            V3 rs = random_in_unit_sphere<ORDER>(rng);
+            r.o = h.p;
+            r.d = add(refl, mul(mf.x, rs));
+            att.r *= a.r;
+            att.g *= a.g;
+            att.b *= a.b;
+            continue;
+        }
+        if (mi.x == 2) {
+            // dielectric::scatter (dielectric.cuh:32-52) with Schlick (dielectric.cuh:57-63)
+            float ratio = h.front ? (1.0f / mf.y) : mf.y;
+            V3 ud = unit(r.d);
+            float ct = dot(neg(ud), h.n);
+            float cos_theta = ct < 1.0f ? ct : 1.0f;
+            float sin_theta = sqrtf(1.0f - cos_theta * cos_theta);
+            bool cannot_refract = ratio * sin_theta > 1.0f;
+            bool do_reflect = cannot_refract;
+            if (!cannot_refract) {
+                float r0 = (1.0f - ratio) / (1.0f + ratio);
+                r0 = r0 * r0;
+                // (float)pow(1 - cosine, 5): the x^5 product in double agrees with glibc's double pow
+                double x = (double)(1.0f - cos_theta);
+                double x2 = x * x;
+                float p5 = (float)(x2 * x2 * x);
+                float refl = r0 + (1.0f - r0) * p5;
+                do_reflect = refl > rng.uniform();
+            }
+            r.o = h.p;
+            r.d = do_reflect ? reflect(ud, h.n) : refract(ud, h.n, ratio);
+            continue;   // attenuation (1,1,1)
+        }
+        // lambertian::scatter (lambertian.cuh:63-131): attenuation from the texture, cosine_pdf(normal)
+        RGB a = texture_value(S, mi.y, h.u, h.v, h.p, status);
+        Onb b = build_from_w(h.n);
+        V3 dir;
+        float pdf_val, spdf;
+        if (!CLEAN || S.num_lights > 0) {
+            // mixture_pdf(hittable_pdf(lights, p), cosine_pdf), proportion 0.5 (mixture_pdf.cuh:28-47)
+            if (rng.uniform() < 0.5f) {
+                if (S.num_lights == 0) {
+                    dir = v3(0.f, 0.f, 0.f);   // hittable_list::random on an empty list
+                } else {
+                    if (S.num_lights > 1) (void)rng.uniform();   // get_int(rng, 0, n-1) == 0, one draw
+                    dir = light_random<ORDER>(S, 0, h.p, rng);
+                }
+            } else {
+                dir = onb_local(b, random_cosine_direction<CLEAN>(rng));
+            }
+            float cosv = dot(unit(dir), b.w) / 3.14159265358979323846f;
+            float cpdf = 0.0f > cosv ? 0.0f : cosv;   // ffmax(0, x) keeps NaN
+            pdf_val = 0.5f * lights_pdf_value(S, h.p, dir) + (1.0f - 0.5f) * cpdf;
+        } else {
+            dir = onb_local(b, random_cosine_direction<CLEAN>(rng));
+            float cosv = dot(unit(dir), b.w) / 3.14159265358979323846f;
+            pdf_val = 0.0f > cosv ? 0.0f : cosv;
+        }
+        // lambertian::scattering_pdf (lambertian.cuh:139-143)
+        float cos_theta = dot(h.n, unit(dir));
+        spdf = cos_theta < 0.0f ? 0.0f : cos_theta / 3.14159265358979323846f;
+        // current_attenuation *= srec.attenuation * scattering_pdf / pdf_val, where color / t = (1/t) * color
+        float rcp = 1.0f / pdf_val;
+        att.r *= rcp * (a.r * spdf);
+        att.g *= rcp * (a.g * spdf);
+        att.b *= rcp * (a.b * spdf);
+        r.o = h.p;
+        r.d = dir;
+    }
+    pc.nodes += st.nodes;
+    pc.prims += st.prims;
+    return result;
+}
+
+}  // namespace rtc

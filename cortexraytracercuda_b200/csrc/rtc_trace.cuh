@@ -1,0 +1,435 @@
+// rtc_trace.cuh - BVH traversal, primitive tests, materials, textures and the path loop.
+//
+// Every function states the reference function (flarive/CortexRaytracerCuda, core/src/...) whose
+// arithmetic it reproduces.  The reference evaluates one virtual hit() per BVH node and primitive
+// (bvh_node.cuh:110-118, hittable.cuh:47) with a ~120-byte hit_record copied per candidate; here the
+// traversal is an iterative short-stack walk over a flattened SAH BVH2 whose inner loop computes only
+// t, and the full hit record is computed once, for the winning primitive.
+#pragma once
+
+#include "rtc_dev.h"
+#include "rtc_math.cuh"
+
+namespace rtc {
+
+// ------------------------------------------------------------------------------------------------
+// random numbers
+// ------------------------------------------------------------------------------------------------
+
+// thrust::minstd_rand = linear_congruential_engine<uint32, 48271, 0, 2^31-1>
+// (thrust/random/linear_congruential_engine.h) with uniform_real_distribution<float>(0, 1):
+// U = float(x - 1) / (1.0f + float(2^31 - 3)) = float(x - 1) * 2^-31 (uniform_real_distribution.inl:61-74),
+// which rounds to exactly 1.0f for the largest states.  The modular product uses 2^31 = 1 (mod m).
+struct Minstd {
+    uint32_t x;
+    __device__ __forceinline__ void seed(uint32_t s) {
+        uint32_t r = s % 2147483647u;
+        x = r == 0u ? 1u : r;
+    }
+    __device__ __forceinline__ uint32_t next() {
+        uint64_t p = (uint64_t)x * 48271ull;
+        uint32_t r = (uint32_t)(p & 0x7fffffffull) + (uint32_t)(p >> 31);
+        if (r >= 2147483647u) r -= 2147483647u;
+        x = r;
+        return r;
+    }
+    __device__ __forceinline__ float uniform() {
+        return __uint2float_rn(next() - 1u) * 4.656612873077392578125e-10f;  // * 2^-31, exact
+    }
+};
+
+// PCG32 (O'Neill 2014, "PCG: A Family of Simple Fast Space-Efficient Statistically Good Algorithms
+// for Random Number Generation"): 64-bit LCG state, XSH-RR output.  Clean mode seeds one stream per
+// (pixel, sample) from a hash of (seed, pixel, sample), so samples of a pixel are independent.
+struct Pcg32 {
+    uint64_t state, inc;
+    __device__ __forceinline__ uint32_t next() {
+        uint64_t old = state;
+        state = old * 6364136223846793005ull + inc;
+        uint32_t xs = (uint32_t)(((old >> 18u) ^ old) >> 27u);
+        uint32_t rot = (uint32_t)(old >> 59u);
+        return (xs >> rot) | (xs << ((32u - rot) & 31u));
+    }
+    __device__ __forceinline__ float uniform() { return (float)(next() >> 8) * (1.0f / 16777216.0f); }
+    __device__ __forceinline__ void seed(uint64_t initstate, uint64_t seq) {
+        state = 0u;
+        inc = (seq << 1u) | 1u;
+        next();
+        state += initstate;
+        next();
+    }
+};
+
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {   // splitmix64 finaliser (Steele et al. 2014)
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+
+// ------------------------------------------------------------------------------------------------
+// hit record (the fields of hit_record the render path reads, misc/hit_record.cuh:8-38)
+// ------------------------------------------------------------------------------------------------
+struct Hit {
+    float t;
+    uint32_t item;     // leaf item (kind << 30 | index); 0xffffffff = none
+    V3 p;              // hit_point
+    V3 n;              // normal, facing the ray
+    float u, v;
+    bool front;
+    int mat;
+};
+
+// hit_record::set_face_normal (hit_record.cuh:34-38)
+__device__ __forceinline__ void set_face_normal(Hit& h, V3 dir, V3 outward) {
+    h.front = dot(dir, outward) < 0.0f;
+    h.n = h.front ? outward : neg(outward);
+}
+
+// ------------------------------------------------------------------------------------------------
+// primitive t tests: same arithmetic and interval rule as the reference's hit()
+// ------------------------------------------------------------------------------------------------
+
+// sphere::hit (sphere.cuh:111-135): half-b quadratic, strict interval (interval::surrounds).
+__device__ __forceinline__ bool sphere_t(float4 s, V3 o, V3 d, float tmin, float tmax, float& t) {
+    V3 c = v3(s.x, s.y, s.z);
+    V3 oc = sub(o, c);
+    float a = lensq(d);
+    float half_b = oc.x * d.x + oc.y * d.y + oc.z * d.z;   // dot_vector (vector3.cuh:92-94)
+    float cc = lensq(oc) - s.w * s.w;
+    float disc = half_b * half_b - a * cc;
+    if (disc < 0.0f) return false;
+    float sq = sqrtf(disc);
+    float root = (-half_b - sq) / a;
+    if (!(tmin < root && root < tmax)) {
+        root = (-half_b + sq) / a;
+        if (!(tmin < root && root < tmax)) return false;
+    }
+    t = root;
+    return true;
+}
+
+// quad::hit (quad.cuh:100-133) and directional_light::hit (directional_light.cuh:76-120).
+// q0 = (n, D), q1 = (Q or P), q2 = u, q3 = v, q4 = w.  centred: light interior test on [-0.5, 0.5].
+__device__ __forceinline__ bool planar_t(float4 q0, float4 q1, float4 q2, float4 q3, float4 q4, V3 o, V3 d,
+                                         float tmin, float tmax, bool centred, float& t, float& alpha,
+                                         float& beta) {
+    V3 n = v3(q0.x, q0.y, q0.z);
+    float denom = dot(n, d);
+    if ((double)fabsf(denom) < 1e-8) return false;          // fabs(denom) < 1e-8 (double literal)
+    float tt = (q0.w - dot(n, o)) / denom;
+    if (!(tmin <= tt && tt <= tmax)) return false;          // interval::contains
+    V3 ip = at(o, d, tt);
+    V3 pl = sub(ip, v3(q1.x, q1.y, q1.z));
+    V3 w = v3(q4.x, q4.y, q4.z);
+    float a = dot(w, cross(pl, v3(q3.x, q3.y, q3.z)));
+    float b = dot(w, cross(v3(q2.x, q2.y, q2.z), pl));
+    if (centred) {
+        if ((a < -0.5f) || (0.5f < a) || (b < -0.5f) || (0.5f < b)) return false;
+    } else {
+        if ((a < 0.0f) || (1.0f < a) || (b < 0.0f) || (1.0f < b)) return false;
+    }
+    t = tt;
+    alpha = a;
+    beta = b;
+    return true;
+}
+
+// triangle::hit (triangle.cuh:130-160): Moller-Trumbore, |det| < 1e-6 rejected, inclusive bounds.
+__device__ __forceinline__ bool tri_t(float4 a0, float4 a1, float4 a2, V3 o, V3 d, float tmin, float tmax,
+                                      float& t, float& bu, float& bv) {
+    V3 v0 = v3(a0.x, a0.y, a0.z), e1 = v3(a1.x, a1.y, a1.z), e2 = v3(a2.x, a2.y, a2.z);
+    V3 pv = cross(d, e2);
+    float det = dot(e1, pv);
+    if (fabsf(det) < 0.000001f) return false;
+    float inv_det = 1.0f / det;
+    V3 tv = sub(o, v0);
+    float u = dot(tv, pv) * inv_det;
+    if (u < 0.0f || u > 1.0f) return false;
+    V3 qv = cross(tv, e1);
+    float v = dot(d, qv) * inv_det;
+    if (v < 0.0f || u + v > 1.0f) return false;
+    float tt = dot(e2, qv) * inv_det;
+    if (tt < tmin || tt > tmax) return false;
+    t = tt;
+    bu = u;
+    bv = v;
+    return true;
+}
+
+// ------------------------------------------------------------------------------------------------
+// BVH traversal (closest hit)
+// ------------------------------------------------------------------------------------------------
+struct TraceStats {
+    uint32_t nodes, prims;
+};
+
+__device__ __forceinline__ bool slab2(const float4 n0, const float4 n1, const float4 n2, V3 inv, V3 oi,
+                                      float tmin, float tmax, float& tl, float& tr, bool& hr) {
+    // t = lo*inv - o*inv, one FMA per bound; boxes are padded on the host so rounding never culls.
+    float l0x = __fmaf_rn(n0.x, inv.x, -oi.x), l1x = __fmaf_rn(n0.y, inv.x, -oi.x);
+    float l0y = __fmaf_rn(n0.z, inv.y, -oi.y), l1y = __fmaf_rn(n0.w, inv.y, -oi.y);
+    float l0z = __fmaf_rn(n2.x, inv.z, -oi.z), l1z = __fmaf_rn(n2.y, inv.z, -oi.z);
+    float r0x = __fmaf_rn(n1.x, inv.x, -oi.x), r1x = __fmaf_rn(n1.y, inv.x, -oi.x);
+    float r0y = __fmaf_rn(n1.z, inv.y, -oi.y), r1y = __fmaf_rn(n1.w, inv.y, -oi.y);
+    float r0z = __fmaf_rn(n2.z, inv.z, -oi.z), r1z = __fmaf_rn(n2.w, inv.z, -oi.z);
+    float lin = fmaxf(fmaxf(fminf(l0x, l1x), fminf(l0y, l1y)), fmaxf(fminf(l0z, l1z), tmin));
+    float lout = fminf(fminf(fmaxf(l0x, l1x), fmaxf(l0y, l1y)), fminf(fmaxf(l0z, l1z), tmax));
+    float rin = fmaxf(fmaxf(fminf(r0x, r1x), fminf(r0y, r1y)), fmaxf(fminf(r0z, r1z), tmin));
+    float rout = fminf(fminf(fmaxf(r0x, r1x), fmaxf(r0y, r1y)), fminf(fmaxf(r0z, r1z), tmax));
+    tl = lin;
+    tr = rin;
+    hr = rin <= rout;
+    return lin <= lout;
+}
+
+// Tests every item of one leaf against [tmin, best_t]; returns true when the status word must be set.
+__device__ __forceinline__ void test_leaf(const DevScene& S, int32_t child, V3 o, V3 d, float tmin, float& best_t,
+                                          uint32_t& best_item, bool hide_invisible, TraceStats& st,
+                                          uint32_t& status) {
+    uint32_t enc = (uint32_t)(~child);
+    uint32_t first = enc >> LEAF_COUNT_BITS, cnt = enc & MAX_LEAF;
+    if (first + cnt > S.num_items) { status |= STATUS_BAD_ITEM; return; }
+    for (uint32_t k = 0; k < cnt; ++k) {
+        uint32_t it = __ldg(S.items + first + k);
+        uint32_t kind = it >> 30, idx = it & 0x3fffffffu;
+        float t;
+        st.prims++;
+        switch (kind) {
+        case ITEM_TRI: {
+            if (idx >= S.num_tri) { status |= STATUS_BAD_ITEM; break; }
+            const float4* p = S.tri + 3 * (size_t)idx;
+            float bu, bv;
+            if (tri_t(__ldg(p), __ldg(p + 1), __ldg(p + 2), o, d, tmin, best_t, t, bu, bv)) { best_t = t; best_item = it; }
+        } break;
+        case ITEM_SPHERE: {
+            if (idx >= S.num_sph) { status |= STATUS_BAD_ITEM; break; }
+            if (sphere_t(__ldg(S.sph + idx), o, d, tmin, best_t, t)) { best_t = t; best_item = it; }
+        } break;
+        case ITEM_QUAD: {
+            if (idx >= S.num_quad) { status |= STATUS_BAD_ITEM; break; }
+            const float4* q = S.quad + 5 * (size_t)idx;
+            float a, b;
+            if (planar_t(__ldg(q), __ldg(q + 1), __ldg(q + 2), __ldg(q + 3), __ldg(q + 4), o, d, tmin, best_t, false, t, a, b)) {
+                best_t = t;
+                best_item = it;
+            }
+        } break;
+        case ITEM_LIGHT: {
+            if (idx >= S.num_lights) { status |= STATUS_BAD_ITEM; break; }
+            const float4* q = S.light + 6 * (size_t)idx;
+            float a, b;
+            float4 q3 = __ldg(q + 3);
+            if (planar_t(__ldg(q), __ldg(q + 1), __ldg(q + 2), q3, __ldg(q + 4), o, d, tmin, best_t, true, t, a, b)) {
+                // "Hide light source": invisible lights are skipped when depth == max_depth
+                // (directional_light.cuh:106)
+                if (!(q3.w != 0.0f && hide_invisible)) { best_t = t; best_item = it; }
+            }
+        } break;
+        }
+    }
+}
+
+// Closest hit in [tmin, tmax] over the whole scene (the reference's world.hit through the BVH).
+__device__ __forceinline__ bool closest_hit(const DevScene& S, V3 o, V3 d, float tmin, float tmax,
+                                            bool hide_invisible, float& t_out, uint32_t& item_out,
+                                            TraceStats& st, uint32_t& status) {
+    V3 inv = v3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
+    V3 oi = v3(o.x * inv.x, o.y * inv.y, o.z * inv.z);
+    float best_t = tmax;
+    uint32_t best_item = 0xffffffffu;
+    int32_t stack[TRAVERSAL_STACK];
+    int sp = 0;
+    int32_t node = 0;
+    for (;;) {
+        const float4* np = S.nodes + 4 * (size_t)node;
+        float4 n0 = __ldg(np), n1 = __ldg(np + 1), n2 = __ldg(np + 2), n3 = __ldg(np + 3);
+        st.nodes++;
+        int32_t cl = __float_as_int(n3.x), cr = __float_as_int(n3.y);
+        float tl, tr;
+        bool hr;
+        bool hl = slab2(n0, n1, n2, inv, oi, tmin, best_t, tl, tr, hr);
+        if (hl && cl < 0) { test_leaf(S, cl, o, d, tmin, best_t, best_item, hide_invisible, st, status); hl = false; }
+        if (hr && cr < 0) { test_leaf(S, cr, o, d, tmin, best_t, best_item, hide_invisible, st, status); hr = false; }
+        if (hl && hr) {
+            int32_t nearc = tl <= tr ? cl : cr;
+            int32_t farc = tl <= tr ? cr : cl;
+            if (sp >= TRAVERSAL_STACK) { status |= STATUS_STACK_OVERFLOW; break; }
+            stack[sp++] = farc;
+            node = nearc;
+        } else if (hl) {
+            node = cl;
+        } else if (hr) {
+            node = cr;
+        } else {
+            if (sp == 0) break;
+            node = stack[--sp];
+        }
+        if ((uint32_t)node >= S.num_nodes) { status |= STATUS_BAD_ITEM; break; }
+    }
+    t_out = best_t;
+    item_out = best_item;
+    return best_item != 0xffffffffu;
+}
+
+// Full hit record of the winning item: the part of each reference hit() that runs after the
+// interval test (sphere.cuh:137-165, quad.cuh:122-132, directional_light.cuh:113-120,
+// triangle.cuh:160-184).
+__device__ __forceinline__ void finalize_hit(const DevScene& S, uint32_t it, float t, V3 o, V3 d, Hit& h) {
+    uint32_t kind = it >> 30, idx = it & 0x3fffffffu;
+    h.t = t;
+    h.item = it;
+    switch (kind) {
+    case ITEM_SPHERE: {
+        float4 s = __ldg(S.sph + idx);
+        h.p = at(o, d, t);
+        h.mat = __ldg(S.sph_aux + idx).x;
+        V3 c = v3(s.x, s.y, s.z);
+        V3 outward = divs(sub(h.p, c), s.w);
+        set_face_normal(h, d, outward);
+        // get_sphere_uv (uvmapping.cuh:204-228) with the default mapping (repeat 1, scale 1, offset 0);
+        // acos/atan2 evaluated in double and rounded, as close to glibc's float results as CUDA allows.
+        float theta = (float)acos((double)(-outward.y));
+        float phi = (float)atan2((double)(-outward.z), (double)outward.x) + 3.14159265358979323846f;
+        float sc = phi / (2.0f * 3.14159265358979323846f);
+        float tc = theta / 3.14159265358979323846f;
+        sc = fmodf(sc * 1.0f, 1.0f);
+        tc = fmodf(tc * 1.0f, 1.0f);
+        h.u = 1.0f * sc + 0.0f;
+        h.v = 1.0f * tc + 0.0f;
+    } break;
+    case ITEM_QUAD:
+    case ITEM_LIGHT: {
+        const float4* q = kind == ITEM_QUAD ? S.quad + 5 * (size_t)idx : S.light + 6 * (size_t)idx;
+        float4 q0 = __ldg(q), q1 = __ldg(q + 1), q2 = __ldg(q + 2), q3 = __ldg(q + 3), q4 = __ldg(q + 4);
+        V3 n = v3(q0.x, q0.y, q0.z);
+        V3 ip = at(o, d, t);
+        V3 pl = sub(ip, v3(q1.x, q1.y, q1.z));
+        V3 w = v3(q4.x, q4.y, q4.z);
+        float a = dot(w, cross(pl, v3(q3.x, q3.y, q3.z)));
+        float b = dot(w, cross(v3(q2.x, q2.y, q2.z), pl));
+        h.p = ip;
+        h.mat = __float_as_int(q1.w);
+        set_face_normal(h, d, n);
+        if (kind == ITEM_QUAD) { h.u = a; h.v = b; }
+        else { h.u = a + 0.5f; h.v = b + 0.5f; }
+    } break;
+    default: {  // triangle
+        const float4* p = S.tri + 3 * (size_t)idx;
+        float4 a0 = __ldg(p), a1 = __ldg(p + 1), a2 = __ldg(p + 2);
+        h.p = at(o, d, t);
+        h.mat = __float_as_int(a0.w);
+        float4 nn = __ldg(S.tri_n + idx);
+        V3 normal = v3(nn.x, nn.y, nn.z);
+        int sm = __float_as_int(a2.w);
+        if (sm >= 0) {
+            // smooth: a*vn1 + b*vn2 + c*vn0 with the barycentrics of triangle::hit (triangle.cuh:171-175)
+            V3 v0 = v3(a0.x, a0.y, a0.z), e1 = v3(a1.x, a1.y, a1.z), e2 = v3(a2.x, a2.y, a2.z);
+            V3 pv = cross(d, e2);
+            float det = dot(e1, pv);
+            float inv_det = 1.0f / det;
+            V3 tv = sub(o, v0);
+            float bu = dot(tv, pv) * inv_det;
+            V3 qv = cross(tv, e1);
+            float bv = dot(d, qv) * inv_det;
+            float bc = 1.0f - bu - bv;
+            const float4* vn = S.tri_vn + 3 * (size_t)sm;
+            normal = add(add(mul(bu, v3(__ldg(vn + 1))), mul(bv, v3(__ldg(vn + 2)))), mul(bc, v3(__ldg(vn))));
+        }
+        set_face_normal(h, d, normal);
+        // triangles carry no texture coordinates here: get_triangle_uv over all-zero vertex uvs gives
+        // (0, 0) (uvmapping.cuh:415-447)
+        h.u = 0.0f;
+        h.v = 0.0f;
+    } break;
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// textures and materials
+// ------------------------------------------------------------------------------------------------
+struct RGB {
+    float r, g, b;
+};
+__device__ __forceinline__ RGB rgb(float r, float g, float b) { RGB c; c.r = r; c.g = g; c.b = b; return c; }
+
+// texture::value dispatch: solid (solid_color_texture.cuh:34), checker (checker_texture.cuh:33-41),
+// image (image_texture.cuh:54-70 + bitmap_image::pixel_data, bitmap_image.cuh:74-91).
+__device__ __forceinline__ RGB texture_value(const DevScene& S, int tex, float u, float v, V3 p, uint32_t& status) {
+    for (int guard = 0; guard < 8; ++guard) {
+        if ((uint32_t)tex >= S.num_textures) { status |= STATUS_BAD_TEXTURE; return rgb(0.f, 0.f, 0.f); }
+        int4 ti = __ldg(S.tex_i + tex);
+        float4 tf = __ldg(S.tex_f + tex);
+        if (ti.x == 0) return rgb(tf.x, tf.y, tf.z);
+        if (ti.x == 1) {
+            int xi = (int)floorf(tf.w * p.x);
+            int yi = (int)floorf(tf.w * p.y);
+            int zi = (int)floorf(tf.w * p.z);
+            bool even = (xi + yi + zi) % 2 == 0;   // C++ remainder: odd negative sums give -1
+            tex = even ? ti.y : ti.z;
+            continue;
+        }
+        // image
+        if ((uint32_t)ti.w >= S.num_images) { status |= STATUS_BAD_TEXTURE; return rgb(0.f, 0.f, 0.f); }
+        int4 im = __ldg(S.images + ti.w);
+        int W = im.y, H = im.z;
+        if (H <= 0) return rgb(0.f, 1.f, 1.f);
+        float uu = u < 0.0f ? 0.0f : (u > 1.0f ? 1.0f : u);
+        float vc = v < 0.0f ? 0.0f : (v > 1.0f ? 1.0f : v);
+        float vv = 1.0f - vc;
+        int i = (int)(uu * (float)W);
+        int j = (int)(vv * (float)H);
+        i = i < 0 ? 0 : (i < W ? i : W - 1);
+        j = j < 0 ? 0 : (j < H ? j : H - 1);
+        const uint8_t* px = S.image_bytes + (size_t)im.x + (size_t)j * (size_t)(W * 3) + (size_t)i * 3;
+        const float cs = 1.0f / 255.0f;
+        return rgb(cs * (float)px[0], cs * (float)px[1], cs * (float)px[2]);
+    }
+    status |= STATUS_BAD_TEXTURE;
+    return rgb(0.f, 0.f, 0.f);
+}
+
+// background colour of a missed ray (camera.cuh:161-174)
+__device__ __forceinline__ RGB background(const DevScene& S, V3 dir) {
+    const DevBackground& B = S.bg;
+    if (B.kind == 0) return rgb(B.color[0], B.color[1], B.color[2]);
+    V3 ud = unit(dir);
+    if (B.kind == 1) {
+        float a = 0.5f * (ud.y + 1.0f);
+        float b = 1.0f - a;
+        return rgb(b * B.color[0] + a * B.top[0], b * B.color[1] + a * B.top[1], b * B.color[2] + a * B.top[2]);
+    }
+    double theta = acos((double)-ud.y);
+    double phi = atan2((double)-ud.z, (double)ud.x) + 3.14159265358979323846;
+    double uu = phi / (2.0 * 3.14159265358979323846);
+    double vv = theta / 3.14159265358979323846;
+    int W = B.env_w, H = B.env_h;
+    int x = (int)(uu * W);
+    x = x < 0 ? 0 : (x >= W ? W - 1 : x);
+    int y = (int)((1.0 - vv) * H);
+    y = y < 0 ? 0 : (y >= H ? H - 1 : y);
+    const float* px = B.env + 3 * ((size_t)y * W + x);
+    return rgb(__ldg(px), __ldg(px + 1), __ldg(px + 2));
+}
+
+// directional_light::pdf_value (directional_light.cuh:147-158) for light `li` seen from o along v.
+__device__ __forceinline__ float light_pdf_value(const DevScene& S, uint32_t li, V3 o, V3 v) {
+    const float4* q = S.light + 6 * (size_t)li;
+    float4 q0 = __ldg(q), q4 = __ldg(q + 4);
+    float t, a, b;
+    if (!planar_t(q0, __ldg(q + 1), __ldg(q + 2), __ldg(q + 3), q4, o, v, 0.00001f, INFINITY, true, t, a, b)) return 0.0f;
+    V3 n = v3(q0.x, q0.y, q0.z);
+    V3 nrm = dot(v, n) < 0.0f ? n : neg(n);
+    float distance_squared = t * t * lensq(v);
+    float cosine = fabsf(dot(v, nrm) / len(v));
+    return distance_squared / (cosine * q4.w);
+}
+
+// hittable_list::pdf_value over the light list (hittable_list.cuh:173-184)
+__device__ __forceinline__ float lights_pdf_value(const DevScene& S, V3 o, V3 v) {
+    float weight = 1.0f / (float)S.num_lights;
+    float sum = 0.0f;
+    for (uint32_t i = 0; i < S.num_lights; ++i) sum += weight * light_pdf_value(S, i, o, v);
+    return sum;
+}
+
+}  // namespace rtc

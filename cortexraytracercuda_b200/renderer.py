@@ -1,0 +1,162 @@
+"""Python host API over the C ABI, mirroring the reference's renderer interface.
+
+Reference interface (flarive/CortexRaytracerCuda):
+  * ``class renderer { virtual void render(const sceneConfig&, const render_parameters&) const = 0; }``
+    (core/src/renderers/renderer.h:16), implemented for CUDA by ``gpu_cuda_renderer``
+    (core/src/renderers/gpu_cuda_renderer.h:23-27), which calls
+  * ``launchGPU(sceneCfg, width, height, spp, max_depth, tx=16, ty=16, filepath, quiet=true)``
+    (core/src/gpu.cu:2127).
+
+Here ``GpuB200Renderer.render(scene, params)`` renders a :class:`~.scene.Scene` with
+:class:`RenderParameters` (the CLI-level ``render_parameters`` of misc/render_parameters.h:13-103:
+width, height, spp, max depth, save path, quiet) and ``launch_gpu`` has launchGPU's arguments.
+Errors raise :class:`RtcError` (the reference prints and exits(99), gpu.cu:119-129).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import weakref
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from ._lib import RtcError, check
+from .scene import MODE_COMPAT, DRAW_ORDER_DEVICE, RenderParams, Scene, SceneDesc, rtc_scene_info
+
+
+class Context:
+    """One CUDA device + stream (rtc_context)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = _lib.load()
+        h = C.c_void_p()
+        check(self.lib.rtc_context_create(device, C.byref(h)))
+        self.handle = h
+        self._scenes = weakref.WeakSet()
+
+    def close(self):
+        if self.handle:
+            for s in list(self._scenes):
+                s.close()
+            self.lib.rtc_context_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def upload(self, scene: Scene) -> "DeviceScene":
+        return DeviceScene(self, scene)
+
+
+class DeviceScene:
+    """A flattened scene resident on the device (rtc_scene): SAH BVH, primitives, textures."""
+
+    def __init__(self, ctx: Context, scene: Scene):
+        self.ctx = ctx
+        self.desc = SceneDesc(scene)
+        h = C.c_void_p()
+        if not ctx.handle:
+            raise RtcError(1, "context is closed")
+        check(ctx.lib.rtc_scene_create(ctx.handle, self.desc.ptr(), C.byref(h)))
+        self.handle = h
+        ctx._scenes.add(self)
+
+    def info(self) -> dict:
+        i = rtc_scene_info()
+        check(self.ctx.lib.rtc_scene_get_info(self.handle, C.byref(i)))
+        return {k: getattr(i, k) for k, _ in rtc_scene_info._fields_}
+
+    def close(self):
+        if self.handle:
+            self.ctx.lib.rtc_scene_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def render(self, params: RenderParams, want_rgb8: bool = False):
+        """Renders into host buffers.  Returns (radiance_sum (H, W, 4) float32 in frame-buffer order,
+        rgb8 (H, W, 3) uint8 in PNG order or None)."""
+        n = params.width * params.height
+        rad = np.empty((params.height, params.width, 4), np.float32)
+        rgb = np.empty((params.height, params.width, 3), np.uint8) if want_rgb8 else None
+        p = params.to_c()
+        check(self.ctx.lib.rtc_render(self.ctx.handle, self.handle, C.byref(p), rad.ctypes.data,
+                                      rgb.ctypes.data if rgb is not None else None))
+        assert rad.size == 4 * n
+        return rad, rgb
+
+    def render_device(self, params: RenderParams, d_radiance: int, d_rgb8: int | None = None,
+                      d_counters: int | None = None, stream: int | None = None):
+        """Asynchronous render into device buffers (raw device pointers, e.g. torch tensor .data_ptr())."""
+        p = params.to_c()
+        check(self.ctx.lib.rtc_render_device(self.ctx.handle, self.handle, C.byref(p), C.c_void_p(d_radiance),
+                                             C.c_void_p(d_rgb8) if d_rgb8 else None,
+                                             C.c_void_p(d_counters) if d_counters else None,
+                                             C.c_void_p(stream) if stream else None))
+
+    def trace_closest(self, rays: np.ndarray, depth: int = 0, max_depth: int = 1):
+        """Closest-hit primitive id (-1 = miss) and t for rays (n, 8) = (ox,oy,oz,tmin,dx,dy,dz,tmax)."""
+        rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+        n = rays.shape[0]
+        prim = np.empty(n, np.int32)
+        t = np.empty(n, np.float32)
+        check(self.ctx.lib.rtc_trace_closest(self.ctx.handle, self.handle, rays.ctypes.data, n, depth, max_depth,
+                                             prim.ctypes.data, t.ctypes.data))
+        return prim, t
+
+
+@dataclass
+class RenderParameters:
+    """The reference's render_parameters subset that reaches launchGPU (misc/render_parameters.h)."""
+    width: int = 256
+    height: int = 144          # 256 / (16/9), render_parameters.h:13-15
+    spp: int = 100
+    max_depth: int = 100
+    save_filepath: str = "image.png"
+    quiet: bool = True
+    mode: int = MODE_COMPAT
+    draw_order: int = DRAW_ORDER_DEVICE
+
+
+class GpuB200Renderer:
+    """Drop-in for gpu_cuda_renderer: render(scene, params) writes the PNG like launchGPU does."""
+
+    def __init__(self, device: int = 0):
+        self.ctx = Context(device)
+
+    def render(self, scene: Scene, params: RenderParameters):
+        ds = DeviceScene(self.ctx, scene)
+        try:
+            rp = RenderParams(params.width, params.height, params.spp, params.max_depth, 2580, params.mode,
+                              params.draw_order)
+            rad, rgb = ds.render(rp, want_rgb8=True)
+            check(self.ctx.lib.rtc_write_png(params.save_filepath.encode(), rgb.ctypes.data, params.width,
+                                             params.height))
+            return rad, rgb
+        finally:
+            ds.close()
+
+
+def launch_gpu(scene: Scene, width: int, height: int, spp: int, max_depth: int, tx: int = 16, ty: int = 16,
+               filepath: str = "image.png", quiet: bool = True) -> None:
+    """launchGPU (core/src/gpu.cu:2127) through the C ABI's rtc_launchGPU."""
+    lib = _lib.load()
+    d = SceneDesc(scene)
+    check(lib.rtc_launchGPU(d.ptr(), width, height, spp, max_depth, tx, ty, filepath.encode(), int(bool(quiet))))
+
+
+__all__ = ["Context", "DeviceScene", "GpuB200Renderer", "RenderParameters", "launch_gpu", "RtcError"]

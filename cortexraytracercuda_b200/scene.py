@@ -1,0 +1,308 @@
+"""Host-side scene description: a Python mirror of the C structs in include/rtc.h.
+
+The reference describes a scene as a ``sceneConfig`` POD tree with uint8_t per-type counts, built by
+``scene_builder`` from a libconfig ``.scene`` file (core/src/scenes/scene_config.h:452-459,
+core/src/scenes/scene_builder.cpp).  Here a scene is built programmatically with the same object
+vocabulary - textures, materials, directional lights, spheres, quads, triangle meshes, a perspective
+camera and a background - and handed to the C ABI as one ``rtc_scene_desc``.
+
+Objects keep the reference's load order (core/src/gpu.cu:504-635): directional lights, spheres, quads,
+meshes.  The global primitive id of an object is its position in that order.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+# --- enums (rtc.h) -------------------------------------------------------------------------------
+TEX_SOLID, TEX_CHECKER, TEX_IMAGE = 0, 1, 2
+MAT_LAMBERTIAN, MAT_METAL, MAT_DIELECTRIC, MAT_DIFFUSE_LIGHT = 0, 1, 2, 3
+BG_CONSTANT, BG_SKY_GRADIENT, BG_ENV_MAP = 0, 1, 2
+MODE_COMPAT, MODE_CLEAN = 0, 1
+DRAW_ORDER_DEVICE, DRAW_ORDER_HOST = 0, 1
+
+F3 = C.c_float * 3
+
+
+class rtc_texture(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("color", F3), ("scale", C.c_float), ("even", C.c_int32),
+                ("odd", C.c_int32), ("image", C.c_int32)]
+
+
+class rtc_image(C.Structure):
+    _fields_ = [("rgb", C.POINTER(C.c_uint8)), ("width", C.c_int32), ("height", C.c_int32)]
+
+
+class rtc_material(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("texture", C.c_int32), ("fuzz", C.c_float), ("ior", C.c_float),
+                ("intensity", C.c_float), ("directional", C.c_int32)]
+
+
+class rtc_sphere(C.Structure):
+    _fields_ = [("center", F3), ("radius", C.c_float), ("material", C.c_int32)]
+
+
+class rtc_quad(C.Structure):
+    _fields_ = [("q", F3), ("u", F3), ("v", F3), ("material", C.c_int32)]
+
+
+class rtc_dir_light(C.Structure):
+    _fields_ = [("position", F3), ("u", F3), ("v", F3), ("color", F3), ("intensity", C.c_float),
+                ("invisible", C.c_int32)]
+
+
+class rtc_mesh(C.Structure):
+    _fields_ = [("vertices", C.POINTER(C.c_float)), ("indices", C.POINTER(C.c_uint32)),
+                ("normals", C.POINTER(C.c_float)), ("uvs", C.POINTER(C.c_float)),
+                ("num_vertices", C.c_uint32), ("num_triangles", C.c_uint32), ("material", C.c_int32),
+                ("smooth", C.c_int32)]
+
+
+class rtc_camera(C.Structure):
+    _fields_ = [("look_from", F3), ("look_at", F3), ("up", F3), ("vfov", C.c_float), ("aspect", C.c_float),
+                ("aperture", C.c_float), ("focus", C.c_float)]
+
+
+class rtc_background(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("color", F3), ("top", F3), ("env_rgb", C.POINTER(C.c_float)),
+                ("env_width", C.c_int32), ("env_height", C.c_int32)]
+
+
+class rtc_scene_desc(C.Structure):
+    _fields_ = [("textures", C.POINTER(rtc_texture)), ("num_textures", C.c_uint32),
+                ("images", C.POINTER(rtc_image)), ("num_images", C.c_uint32),
+                ("materials", C.POINTER(rtc_material)), ("num_materials", C.c_uint32),
+                ("dir_lights", C.POINTER(rtc_dir_light)), ("num_dir_lights", C.c_uint32),
+                ("spheres", C.POINTER(rtc_sphere)), ("num_spheres", C.c_uint32),
+                ("quads", C.POINTER(rtc_quad)), ("num_quads", C.c_uint32),
+                ("meshes", C.POINTER(rtc_mesh)), ("num_meshes", C.c_uint32),
+                ("camera", rtc_camera), ("background", rtc_background)]
+
+
+class rtc_render_params(C.Structure):
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("spp", C.c_int32), ("max_depth", C.c_int32),
+                ("seed", C.c_uint32), ("mode", C.c_int32), ("draw_order", C.c_int32),
+                ("block_size", C.c_int32)]
+
+
+class rtc_scene_info(C.Structure):
+    _fields_ = [("num_primitives", C.c_uint32), ("num_lights", C.c_uint32), ("num_nodes", C.c_uint32),
+                ("max_leaf_size", C.c_uint32), ("device_bytes", C.c_uint64), ("build_ms", C.c_double)]
+
+
+def _f3(v) -> F3:
+    v = [float(x) for x in v]
+    if len(v) != 3:
+        raise ValueError("expected 3 components")
+    return F3(*v)
+
+
+def _carray(ctype, items):
+    arr = (ctype * max(1, len(items)))()
+    for k, it in enumerate(items):
+        arr[k] = it
+    return arr
+
+
+@dataclass
+class Camera:
+    look_from: tuple = (0.0, 0.0, 10.0)
+    look_at: tuple = (0.0, 0.0, 0.0)
+    up: tuple = (0.0, 1.0, 0.0)
+    vfov: float = 70.0
+    aspect: float = 16.0 / 9.0      # scene_builder's default camera (scene_builder.cpp:49)
+    aperture: float = 0.0
+    focus: float = 100.0
+
+
+@dataclass
+class RenderParams:
+    width: int
+    height: int
+    spp: int
+    max_depth: int
+    seed: int = 2580               # core/src/gpu.cu:2080
+    mode: int = MODE_COMPAT
+    draw_order: int = DRAW_ORDER_DEVICE
+    block_size: int = 0
+
+    def to_c(self) -> rtc_render_params:
+        return rtc_render_params(self.width, self.height, self.spp, self.max_depth, self.seed & 0xFFFFFFFF,
+                                 self.mode, self.draw_order, self.block_size)
+
+    @property
+    def traced_spp(self) -> int:
+        """Samples actually traced per pixel: int(sqrt(spp))^2 in compat mode (gpu.cu:1989)."""
+        if self.mode == MODE_COMPAT:
+            q = int(np.sqrt(np.float32(self.spp)))
+            return q * q
+        return self.spp
+
+
+@dataclass
+class Scene:
+    """A scene under construction.  ``add_*`` return the index of what they add."""
+    textures: list = field(default_factory=list)
+    images: list = field(default_factory=list)        # (H, W, 3) uint8 arrays, top row first
+    materials: list = field(default_factory=list)
+    dir_lights: list = field(default_factory=list)
+    spheres: list = field(default_factory=list)
+    quads: list = field(default_factory=list)
+    meshes: list = field(default_factory=list)        # dicts with numpy arrays
+    camera: Camera = field(default_factory=Camera)
+    background: dict = field(default_factory=lambda: {"kind": BG_CONSTANT, "color": (0.0, 0.0, 0.0)})
+    name: str = "scene"
+
+    # textures -------------------------------------------------------------------------------------
+    def solid(self, rgb) -> int:
+        self.textures.append(("solid", tuple(float(x) for x in rgb)))
+        return len(self.textures) - 1
+
+    def checker(self, scale, even_tex: int, odd_tex: int) -> int:
+        self.textures.append(("checker", float(scale), int(even_tex), int(odd_tex)))
+        return len(self.textures) - 1
+
+    def checker_colors(self, scale, odd_rgb, even_rgb) -> int:
+        """scene_factory::createCheckerTexture(name, oddColor, evenColor, ..., scale) followed by
+        checker_texture(scale, c1, c2): the odd colour lands in m_even and the even colour in m_odd
+        (core/src/scene_factory.cuh:619-629 with checker_texture.cuh:28-31)."""
+        return self.checker(scale, self.solid(odd_rgb), self.solid(even_rgb))
+
+    def image(self, rgb: np.ndarray) -> int:
+        rgb = np.ascontiguousarray(rgb, dtype=np.uint8)
+        if rgb.ndim != 3 or rgb.shape[2] != 3:
+            raise ValueError("image must be (H, W, 3) uint8")
+        self.images.append(rgb)
+        img = len(self.images) - 1
+        self.textures.append(("image", img))
+        return len(self.textures) - 1
+
+    # materials ------------------------------------------------------------------------------------
+    def lambertian(self, tex_or_rgb) -> int:
+        tex = tex_or_rgb if isinstance(tex_or_rgb, int) else self.solid(tex_or_rgb)
+        self.materials.append((MAT_LAMBERTIAN, tex, 0.0, 0.0, 0.0, 0))
+        return len(self.materials) - 1
+
+    def metal(self, rgb, fuzz) -> int:
+        tex = self.solid(rgb)
+        f = float(fuzz)
+        self.materials.append((MAT_METAL, tex, f if f < 1.0 else 1.0, 0.0, 0.0, 0))   # metal.cuh:52
+        return len(self.materials) - 1
+
+    def dielectric(self, ior) -> int:
+        self.materials.append((MAT_DIELECTRIC, -1, 0.0, float(ior), 0.0, 0))
+        return len(self.materials) - 1
+
+    def diffuse_light(self, rgb, intensity=1.0, directional=True) -> int:
+        tex = self.solid(rgb)
+        self.materials.append((MAT_DIFFUSE_LIGHT, tex, 0.0, 0.0, float(intensity), int(bool(directional))))
+        return len(self.materials) - 1
+
+    # objects --------------------------------------------------------------------------------------
+    def dir_light(self, position, u, v, rgb, intensity=1.0, invisible=True) -> int:
+        self.dir_lights.append((tuple(position), tuple(u), tuple(v), tuple(rgb), float(intensity), int(bool(invisible))))
+        return len(self.dir_lights) - 1
+
+    def sphere(self, center, radius, mat) -> int:
+        self.spheres.append((tuple(center), float(radius), int(mat)))
+        return len(self.spheres) - 1
+
+    def quad(self, q, u, v, mat) -> int:
+        self.quads.append((tuple(q), tuple(u), tuple(v), int(mat)))
+        return len(self.quads) - 1
+
+    def mesh(self, vertices, indices, mat, normals=None, uvs=None, smooth=False) -> int:
+        m = {"vertices": np.ascontiguousarray(vertices, dtype=np.float32).reshape(-1, 3),
+             "indices": np.ascontiguousarray(indices, dtype=np.uint32).reshape(-1, 3),
+             "normals": None if normals is None else np.ascontiguousarray(normals, dtype=np.float32).reshape(-1, 3),
+             "uvs": None if uvs is None else np.ascontiguousarray(uvs, dtype=np.float32).reshape(-1, 2),
+             "material": int(mat), "smooth": int(bool(smooth))}
+        self.meshes.append(m)
+        return len(self.meshes) - 1
+
+    # background -----------------------------------------------------------------------------------
+    def set_background_constant(self, rgb):
+        self.background = {"kind": BG_CONSTANT, "color": tuple(rgb)}
+
+    def set_background_sky(self, bottom=(1.0, 1.0, 1.0), top=(0.5, 0.7, 1.0)):
+        self.background = {"kind": BG_SKY_GRADIENT, "color": tuple(bottom), "top": tuple(top)}
+
+    def set_background_env(self, env_rgb: np.ndarray):
+        env = np.ascontiguousarray(env_rgb, dtype=np.float32)
+        if env.ndim != 3 or env.shape[2] != 3:
+            raise ValueError("env map must be (H, W, 3) float32")
+        self.background = {"kind": BG_ENV_MAP, "env": env}
+
+    # counts ---------------------------------------------------------------------------------------
+    @property
+    def num_triangles(self) -> int:
+        return int(sum(m["indices"].shape[0] for m in self.meshes))
+
+    @property
+    def num_primitives(self) -> int:
+        return len(self.dir_lights) + len(self.spheres) + len(self.quads) + self.num_triangles
+
+    # C description --------------------------------------------------------------------------------
+    def to_desc(self) -> "SceneDesc":
+        return SceneDesc(self)
+
+
+class SceneDesc:
+    """Owns the ctypes arrays behind one rtc_scene_desc; keep it alive while the desc is in use."""
+
+    def __init__(self, s: Scene):
+        keep = []
+        texs = []
+        for t in s.textures:
+            if t[0] == "solid":
+                texs.append(rtc_texture(TEX_SOLID, _f3(t[1]), 0.0, -1, -1, -1))
+            elif t[0] == "checker":
+                texs.append(rtc_texture(TEX_CHECKER, _f3((0, 0, 0)), t[1], t[2], t[3], -1))
+            else:
+                texs.append(rtc_texture(TEX_IMAGE, _f3((0, 0, 0)), 0.0, -1, -1, t[1]))
+        imgs = []
+        for im in s.images:
+            keep.append(im)
+            imgs.append(rtc_image(im.ctypes.data_as(C.POINTER(C.c_uint8)), im.shape[1], im.shape[0]))
+        mats = [rtc_material(*m) for m in s.materials]
+        lights = [rtc_dir_light(_f3(p), _f3(u), _f3(v), _f3(c), i, inv) for (p, u, v, c, i, inv) in s.dir_lights]
+        spheres = [rtc_sphere(_f3(c), r, m) for (c, r, m) in s.spheres]
+        quads = [rtc_quad(_f3(q), _f3(u), _f3(v), m) for (q, u, v, m) in s.quads]
+        meshes = []
+        for m in s.meshes:
+            keep.extend([m["vertices"], m["indices"]])
+            nrm = None
+            uv = None
+            if m["normals"] is not None:
+                keep.append(m["normals"])
+                nrm = m["normals"].ctypes.data_as(C.POINTER(C.c_float))
+            if m["uvs"] is not None:
+                keep.append(m["uvs"])
+                uv = m["uvs"].ctypes.data_as(C.POINTER(C.c_float))
+            meshes.append(rtc_mesh(m["vertices"].ctypes.data_as(C.POINTER(C.c_float)),
+                                   m["indices"].ctypes.data_as(C.POINTER(C.c_uint32)),
+                                   nrm, uv, m["vertices"].shape[0], m["indices"].shape[0], m["material"], m["smooth"]))
+        cam = s.camera
+        bg = s.background
+        env_ptr = None
+        ew = eh = 0
+        if bg["kind"] == BG_ENV_MAP:
+            keep.append(bg["env"])
+            env_ptr = bg["env"].ctypes.data_as(C.POINTER(C.c_float))
+            eh, ew = bg["env"].shape[:2]
+        cbg = rtc_background(bg["kind"], _f3(bg.get("color", (0, 0, 0))), _f3(bg.get("top", (0, 0, 0))), env_ptr, ew, eh)
+        self.arrays = [_carray(rtc_texture, texs), _carray(rtc_image, imgs), _carray(rtc_material, mats),
+                       _carray(rtc_dir_light, lights), _carray(rtc_sphere, spheres), _carray(rtc_quad, quads),
+                       _carray(rtc_mesh, meshes)]
+        a = self.arrays
+        self.desc = rtc_scene_desc(a[0], len(texs), a[1], len(imgs), a[2], len(mats), a[3], len(lights),
+                                   a[4], len(spheres), a[5], len(quads), a[6], len(meshes),
+                                   rtc_camera(_f3(cam.look_from), _f3(cam.look_at), _f3(cam.up), cam.vfov, cam.aspect,
+                                              cam.aperture, cam.focus), cbg)
+        self._keep = keep
+        self.scene = s
+
+    def ptr(self):
+        return C.byref(self.desc)

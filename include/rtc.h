@@ -1,0 +1,290 @@
+/*
+ * rtc.h - C ABI of the B200-native path-tracing hot path.
+ *
+ * This is the drop-in boundary for the render call of flarive/CortexRaytracerCuda:
+ *
+ *   void launchGPU(const sceneConfig& cfg, int width, int height, int spp, int max_depth,
+ *                  int tx, int ty, const char* filepath, bool quietMode)
+ *     (core/src/gpu.cu:2127, declared core/src/renderers/gpu_cuda_renderer.h:17)
+ *
+ * reached through the virtual renderer::render(const sceneConfig&, const render_parameters&)
+ * (core/src/renderers/renderer.h:16).  Every entry point takes plain pointers and sizes, returns
+ * an rtc_status and never exits the process (the reference prints and calls exit(99),
+ * core/src/gpu.cu:119-129).
+ *
+ * Scene model.  A scene is a flat POD description (rtc_scene_desc) with 32-bit counts, replacing the
+ * reference's sceneConfig tree with uint8_t counts (core/src/scenes/scene_config.h:394-459).  Objects
+ * get a global primitive id in the order the reference's load_scene adds them to its world list
+ * (core/src/gpu.cu:504-635): directional lights, then spheres, then quads, then mesh triangles (mesh
+ * by mesh, triangle by triangle).  Materials and textures are referenced by index instead of by name
+ * (the reference matches names with strcmp_device, core/src/gpu.cu:132).
+ *
+ * Pixel layout.  Radiance buffers use the reference's frame-buffer order: pixel (i, j) with j counted
+ * from the BOTTOM row is element j*width + i (core/src/gpu.cu:769).  The 8-bit RGB output is in PNG
+ * order (top row first), i.e. the rows are flipped as the reference's host loop does
+ * (core/src/gpu.cu:2098-2107).
+ */
+#ifndef RTC_H
+#define RTC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------------------------------ */
+/* status                                                                                            */
+/* ------------------------------------------------------------------------------------------------ */
+
+typedef enum rtc_status {
+    RTC_OK = 0,
+    RTC_ERR_INVALID_ARGUMENT = 1, /* null pointer, bad size, bad enum value                       */
+    RTC_ERR_BAD_SCENE = 2,        /* scene references a missing material/texture/image, NaN coords */
+    RTC_ERR_CUDA = 3,             /* a CUDA runtime call failed; see rtc_last_error_string()       */
+    RTC_ERR_OOM = 4,              /* device allocation failed or the HBM budget would be exceeded  */
+    RTC_ERR_TIMEOUT = 5,          /* a bounded device-side wait ran out                            */
+    RTC_ERR_NO_DEVICE = 6,        /* no CUDA device, or the device is not sm_100                   */
+    RTC_ERR_IO = 7,               /* file could not be written / read                               */
+    RTC_ERR_DEVICE_CHECK = 8,     /* a kernel's own bounds check fired (status word non-zero)      */
+    RTC_ERR_NOT_FOUND = 9,        /* unknown handle / request id                                    */
+    RTC_ERR_BUSY = 10             /* request still in flight                                        */
+} rtc_status;
+
+/* Text of the last error raised on the calling thread ("" when none). */
+const char* rtc_last_error_string(void);
+
+/* ------------------------------------------------------------------------------------------------ */
+/* scene description                                                                                 */
+/* ------------------------------------------------------------------------------------------------ */
+
+/* Textures (core/src/textures/). */
+typedef enum rtc_texture_kind {
+    RTC_TEX_SOLID = 0,   /* solid_color_texture::value (solid_color_texture.cuh:34)                  */
+    RTC_TEX_CHECKER = 1, /* checker_texture::value, spatial floor(p/scale) parity (checker_texture.cuh:33-41) */
+    RTC_TEX_IMAGE = 2    /* image_texture::value, nearest RGB8 with V flip (image_texture.cuh:54-70)  */
+} rtc_texture_kind;
+
+typedef struct rtc_texture {
+    int32_t kind;     /* rtc_texture_kind                                                            */
+    float color[3];   /* SOLID: the colour                                                           */
+    float scale;      /* CHECKER: cell size; the reference stores inv_scale = 1/scale               */
+    int32_t even;     /* CHECKER: texture used where the cell parity is even (checker m_even)       */
+    int32_t odd;      /* CHECKER: texture used where the parity is odd (checker m_odd)              */
+    int32_t image;    /* IMAGE: index into rtc_scene_desc.images                                    */
+} rtc_texture;
+
+/* 8-bit RGB image, row-major, top row first (stbi_load order, core/src/gpu.cu:1743). */
+typedef struct rtc_image {
+    const uint8_t* rgb;
+    int32_t width;
+    int32_t height;
+} rtc_image;
+
+/* Materials (core/src/materials/). */
+typedef enum rtc_material_kind {
+    RTC_MAT_LAMBERTIAN = 0,    /* lambertian.cuh:63-143, mixture-PDF importance sampling         */
+    RTC_MAT_METAL = 1,         /* metal.cuh:52-64                                                */
+    RTC_MAT_DIELECTRIC = 2,    /* dielectric.cuh:32-63                                           */
+    RTC_MAT_DIFFUSE_LIGHT = 3  /* diffuse_light.cuh:45-67, emits, never scatters                 */
+} rtc_material_kind;
+
+typedef struct rtc_material {
+    int32_t kind;        /* rtc_material_kind                                                      */
+    int32_t texture;     /* albedo (lambertian, metal) or emission (diffuse light) texture index   */
+    float fuzz;          /* METAL: fuzz; values >= 1 are clamped to 1 as metal::metal does         */
+    float ior;           /* DIELECTRIC: index of refraction                                        */
+    float intensity;     /* DIFFUSE_LIGHT: emission scale                                          */
+    int32_t directional; /* DIFFUSE_LIGHT: one-sided; back face emits RGBA(0,0,0,0)                */
+} rtc_material;
+
+/* Sphere (core/src/primitives/sphere.cuh). */
+typedef struct rtc_sphere {
+    float center[3];
+    float radius;
+    int32_t material;
+} rtc_sphere;
+
+/* Quad, lower-left corner q and edges u, v (core/src/primitives/quad.cuh). */
+typedef struct rtc_quad {
+    float q[3];
+    float u[3];
+    float v[3];
+    int32_t material;
+} rtc_quad;
+
+/* Directional (quad) light centred on position (core/src/lights/directional_light.cuh).  It gets
+ * its own diffuse_light(color, intensity, directional=true, invisible) material, and it is the only
+ * kind of object that enters the light list sampled by the lambertian mixture PDF
+ * (core/src/gpu.cu:681-694). */
+typedef struct rtc_dir_light {
+    float position[3];
+    float u[3];
+    float v[3];
+    float color[3];
+    float intensity;
+    int32_t invisible;   /* hidden to primary rays: directional_light.cuh:106 */
+} rtc_dir_light;
+
+/* Indexed triangle mesh; each triangle becomes one reference `triangle` (triangle.cuh:87-185). */
+typedef struct rtc_mesh {
+    const float* vertices;      /* 3 floats per vertex                                             */
+    const uint32_t* indices;    /* 3 per triangle                                                  */
+    const float* normals;       /* optional, 3 floats per vertex; used when smooth != 0            */
+    const float* uvs;           /* optional, 2 floats per vertex                                   */
+    uint32_t num_vertices;
+    uint32_t num_triangles;
+    int32_t material;
+    int32_t smooth;             /* barycentric normal interpolation (triangle.cuh:171-175)         */
+} rtc_mesh;
+
+/* Perspective camera (core/src/cameras/perspective_camera.cuh:41-117). */
+typedef struct rtc_camera {
+    float look_from[3];
+    float look_at[3];
+    float up[3];
+    float vfov;        /* degrees                                                                  */
+    float aspect;      /* the reference takes it from the CLI -ratio (scenes/scene_manager.cpp:83)  */
+    float aperture;    /* lens_radius = aperture / 2                                               */
+    float focus;       /* focus distance                                                           */
+} rtc_camera;
+
+typedef enum rtc_background_kind {
+    RTC_BG_CONSTANT = 0,     /* camera::background_color (core/src/gpu.cu:741)                       */
+    RTC_BG_SKY_GRADIENT = 1, /* lerp(bottom, top, 0.5*(unit.y+1)) of the ray direction               */
+    RTC_BG_ENV_MAP = 2       /* equirectangular FP32 RGB map, lookup convention of get_spherical_uv
+                                (core/src/utilities/uvmapping.cuh:144-158)                           */
+} rtc_background_kind;
+
+typedef struct rtc_background {
+    int32_t kind;
+    float color[3];          /* CONSTANT: the colour; SKY_GRADIENT: the colour at unit.y = -1      */
+    float top[3];            /* SKY_GRADIENT: the colour at unit.y = +1                             */
+    const float* env_rgb;    /* ENV_MAP: env_width*env_height*3 floats, top row first               */
+    int32_t env_width;
+    int32_t env_height;
+} rtc_background;
+
+typedef struct rtc_scene_desc {
+    const rtc_texture* textures;      uint32_t num_textures;
+    const rtc_image* images;          uint32_t num_images;
+    const rtc_material* materials;    uint32_t num_materials;
+    const rtc_dir_light* dir_lights;  uint32_t num_dir_lights;
+    const rtc_sphere* spheres;        uint32_t num_spheres;
+    const rtc_quad* quads;            uint32_t num_quads;
+    const rtc_mesh* meshes;           uint32_t num_meshes;
+    rtc_camera camera;
+    rtc_background background;
+} rtc_scene_desc;
+
+/* ------------------------------------------------------------------------------------------------ */
+/* render parameters                                                                                 */
+/* ------------------------------------------------------------------------------------------------ */
+
+typedef enum rtc_mode {
+    /* Reference semantics: one thrust::minstd_rand stream per pixel seeded seed + j*width + i and
+     * consumed by all samples in order (core/src/gpu.cu:761-790), the 50/50 light/cosine mixture
+     * for lambertian (camera.cuh:204-213), floor(sqrt(spp))^2 traced samples divided by spp
+     * (gpu.cu:1989, color.cuh:289-300), and the other quirks of the reference's render path. */
+    RTC_MODE_COMPAT = 0,
+    /* Counter-based stream per (pixel, sample); samples of one pixel are independent, light-list
+     * sampling only when the list is non-empty, cosine sampling otherwise, spp samples traced. */
+    RTC_MODE_CLEAN = 1
+} rtc_mode;
+
+/* Order in which the reference's multi-draw expressions consume the stream.  The reference calls
+ * get_real() several times inside one constructor call or one overloaded-operator expression
+ * (random_in_unit_disk, random_in_unit_sphere: gpu_randomizer.cuh:61-76; directional_light::random:
+ * directional_light.cuh:165-171), whose operand order C++ leaves unspecified.  g++ evaluates them
+ * right to left; the CUDA front end left to right. */
+typedef enum rtc_draw_order {
+    RTC_DRAW_ORDER_DEVICE = 0,  /* as the reference's nvcc build consumes it (left to right)      */
+    RTC_DRAW_ORDER_HOST = 1     /* as a g++ build of the reference's headers consumes it          */
+} rtc_draw_order;
+
+typedef struct rtc_render_params {
+    int32_t width;
+    int32_t height;
+    int32_t spp;
+    int32_t max_depth;
+    uint32_t seed;         /* reference: 2580 (core/src/gpu.cu:2080)                                 */
+    int32_t mode;          /* rtc_mode                                                               */
+    int32_t draw_order;    /* rtc_draw_order (COMPAT only)                                           */
+    int32_t block_size;    /* 0 = library default                                                    */
+} rtc_render_params;
+
+/* ------------------------------------------------------------------------------------------------ */
+/* context and scenes                                                                                */
+/* ------------------------------------------------------------------------------------------------ */
+
+typedef struct rtc_context rtc_context;
+typedef struct rtc_scene rtc_scene;
+
+/* Creates a context on CUDA device `device` (the reference picks the first device, gpu.cu:92-116). */
+rtc_status rtc_context_create(int device, rtc_context** out);
+rtc_status rtc_context_destroy(rtc_context* ctx);
+
+/* Flattens the description, builds the SAH BVH on the host and uploads everything to the device.
+ * Replaces the reference's prepare* deep copies and its single-thread load_scene<<<1,1>>> build
+ * (core/src/gpu.cu:862-1725, 481-751).  The description may be freed after the call. */
+rtc_status rtc_scene_create(rtc_context* ctx, const rtc_scene_desc* desc, rtc_scene** out);
+rtc_status rtc_scene_destroy(rtc_scene* scene);
+
+typedef struct rtc_scene_info {
+    uint32_t num_primitives;   /* lights + spheres + quads + triangles                             */
+    uint32_t num_lights;
+    uint32_t num_nodes;        /* BVH2 nodes                                                        */
+    uint32_t max_leaf_size;
+    uint64_t device_bytes;     /* bytes resident on the device for this scene                      */
+    double build_ms;           /* host BVH build time                                               */
+} rtc_scene_info;
+rtc_status rtc_scene_get_info(const rtc_scene* scene, rtc_scene_info* info);
+
+/* ------------------------------------------------------------------------------------------------ */
+/* render                                                                                            */
+/* ------------------------------------------------------------------------------------------------ */
+
+/* Renders one image end to end with HOST output buffers (either may be NULL):
+ *   radiance_sum: width*height*4 floats, the reference's per-pixel `pixel_color` sum over the traced
+ *                 samples before prepare_pixel_color (RGB + alpha), frame-buffer order;
+ *   rgb8:         width*height*3 bytes, int(255.99*clamp(sqrt(nan0(sum)/spp), 0, 0.999)) per channel,
+ *                 PNG order (gpu.cu:792-799, 2098-2107).
+ * Synchronous on the context's stream. */
+rtc_status rtc_render(rtc_context* ctx, const rtc_scene* scene, const rtc_render_params* params,
+                      float* radiance_sum, uint8_t* rgb8);
+
+/* Same render with DEVICE output buffers (inputs already resident); asynchronous on `stream`
+ * (a cudaStream_t, or NULL for the context's stream).  d_radiance_sum must hold width*height
+ * float4; d_rgb8 may be NULL.  d_counters, when not NULL, receives 4 uint64 counters: rays traced
+ * (closest-hit traversals), paths traced, BVH nodes visited, primitive tests. */
+rtc_status rtc_render_device(rtc_context* ctx, const rtc_scene* scene, const rtc_render_params* params,
+                             float* d_radiance_sum, uint8_t* d_rgb8, unsigned long long* d_counters,
+                             void* stream);
+
+/* Closest-hit queries on arbitrary rays (hit-identity tests).  rays: n x 8 floats
+ * (ox, oy, oz, tmin, dx, dy, dz, tmax) in host memory; `depth`/`max_depth` decide light visibility as
+ * in the reference's world.hit (directional_light.cuh:106).  Outputs (host, n each, may be NULL):
+ * prim_id (-1 on a miss) and t. */
+rtc_status rtc_trace_closest(rtc_context* ctx, const rtc_scene* scene, const float* rays, uint32_t n,
+                             int32_t depth, int32_t max_depth, int32_t* prim_id, float* t);
+
+/* ------------------------------------------------------------------------------------------------ */
+/* drop-in form of the reference call                                                                */
+/* ------------------------------------------------------------------------------------------------ */
+
+/* launchGPU (core/src/gpu.cu:2127) with the reference's semantics: compat mode, seed 2580, one image,
+ * 8-bit PNG written to `filepath` (rows flipped).  tx/ty are accepted for signature compatibility
+ * (the reference's block shape, gpu.cu:2072-2080) and otherwise ignored.  Unlike the reference it
+ * returns a status instead of exiting, and prints nothing unless quiet_mode is 0. */
+rtc_status rtc_launchGPU(const rtc_scene_desc* scene, int width, int height, int spp, int max_depth,
+                         int tx, int ty, const char* filepath, int quiet_mode);
+
+/* Writes an 8-bit RGB PNG (top row first). */
+rtc_status rtc_write_png(const char* filepath, const uint8_t* rgb8, int width, int height);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RTC_H */

@@ -1,0 +1,752 @@
+/*
+ * rt_port.c - TEST INFRASTRUCTURE ONLY (the oracle).  Never part of the product path.
+ *
+ * A plain-C restatement of the reference's per-sample path-tracing path (flarive/CortexRaytracerCuda,
+ * core/src/...), driven by the same rtc_scene_desc as the product.  Each function cites the reference
+ * code it restates.  Float expressions keep the reference's operation order; build with
+ * -ffp-contract=off (oracle/Makefile) so roundings match a plain g++ build of the reference.
+ * Transcendentals call glibc's float functions, as the reference's host build does.
+ *
+ * Pinned against the reference itself: tests/golden/ holds outputs of the reference's own classes
+ * (oracle/_ref/libref_cpu.so, generated by tests/golden/make_golden.py) and tests/test_oracle_port.py
+ * checks this port against them.
+ *
+ * Differences from the reference that do not change results: the BVH is a median-split tree of this
+ * file's own (the reference's is random-axis with an exchange sort, bvh_node.cuh:63-108); only the
+ * order of exactly-equal-t candidates can differ.
+ *
+ * Exported: port_scene_create / port_scene_destroy / port_render_pixels / port_trace_closest /
+ * port_rng_draws / port_set_trig / port_last_error.
+ */
+#include <math.h>
+#include <pthread.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#include <float.h>
+#include <stdio.h>
+
+#include "rtc.h"
+
+#define PI_F 3.14159265358979323846f   /* the reference's float M_PI (misc/constants.cuh:35) */
+
+static __thread char g_err[256];
+
+/* Transcendental evaluation: 0 = glibc's float functions (cosf, sinf, acosf, atan2f), as a g++ build
+ * of the reference calls them; 1 = evaluated in double and rounded to float, as the product's
+ * compat kernels do on the device.  The two differ only in the last ulp of these four functions. */
+static int g_trig = 0;
+void port_set_trig(int mode) { g_trig = mode; }
+static inline float f_cos(float x) { return g_trig ? (float)cos((double)x) : cosf(x); }
+static inline float f_sin(float x) { return g_trig ? (float)sin((double)x) : sinf(x); }
+static inline float f_acos(float x) { return g_trig ? (float)acos((double)x) : acosf(x); }
+static inline float f_atan2(float y, float x) { return g_trig ? (float)atan2((double)y, (double)x) : atan2f(y, x); }
+
+/* ---------------------------------------------------------------------------------------------- */
+/* vectors: glm semantics (func_geometric.inl), misc/vector3.cuh                                  */
+/* ---------------------------------------------------------------------------------------------- */
+typedef struct { float x, y, z; } v3;
+static inline v3 V(float x, float y, float z) { v3 r = {x, y, z}; return r; }
+static inline v3 Vp(const float* p) { return V(p[0], p[1], p[2]); }
+static inline v3 vadd(v3 a, v3 b) { return V(a.x + b.x, a.y + b.y, a.z + b.z); }
+static inline v3 vsub(v3 a, v3 b) { return V(a.x - b.x, a.y - b.y, a.z - b.z); }
+static inline v3 vneg(v3 a) { return V(-a.x, -a.y, -a.z); }
+static inline v3 vscale(float s, v3 a) { return V(s * a.x, s * a.y, s * a.z); }
+static inline v3 vdivs(v3 a, float s) { return V(a.x / s, a.y / s, a.z / s); }
+static inline float vdot(v3 a, v3 b) { float tx = a.x * b.x, ty = a.y * b.y, tz = a.z * b.z; return tx + ty + tz; }
+static inline v3 vcross(v3 x, v3 y) {
+    return V(x.y * y.z - y.y * x.z, x.z * y.x - y.z * x.x, x.x * y.y - y.x * x.y);
+}
+static inline float vlensq(v3 v) { return v.x * v.x + v.y * v.y + v.z * v.z; }   /* vector_length_squared */
+static inline float vlen(v3 v) { return sqrtf(vlensq(v)); }
+static inline v3 vunit(v3 v) { float l = sqrtf(vlensq(v)); return V(v.x / l, v.y / l, v.z / l); }   /* unit_vector */
+static inline v3 vreflect(v3 I, v3 N) { float d = vdot(N, I); v3 nd = V(N.x * d, N.y * d, N.z * d); return vsub(I, V(nd.x * 2.0f, nd.y * 2.0f, nd.z * 2.0f)); }
+static inline v3 vrefract(v3 I, v3 N, float eta) {
+    float dv = vdot(N, I);
+    float k = 1.0f - eta * eta * (1.0f - dv * dv);
+    if (k >= 0.0f) { float s = eta * dv + sqrtf(k); return vsub(vscale(eta, I), vscale(s, N)); }
+    return V(0.0f, 0.0f, 0.0f);
+}
+static inline v3 vat(v3 o, v3 d, float t) { return vadd(o, vscale(t, d)); }   /* ray::at */
+
+/* ---------------------------------------------------------------------------------------------- */
+/* random numbers: thrust minstd_rand + uniform_real_distribution<float>(0,1)                      */
+/* ---------------------------------------------------------------------------------------------- */
+typedef struct { int clean; uint32_t x; uint64_t st, inc; } rng_t;
+static inline void minstd_seed(rng_t* r, uint32_t s) { uint32_t m = s % 2147483647u; r->clean = 0; r->x = m ? m : 1u; }
+static inline float minstd_uniform(rng_t* r) {
+    r->x = (uint32_t)(((uint64_t)r->x * 48271ull) % 2147483647ull);
+    return (float)(r->x - 1u) / (1.0f + (float)(2147483646u - 1u));
+}
+/* PCG32 XSH-RR (O'Neill 2014) for clean mode, seeded like the product's clean kernel */
+static inline uint32_t pcg_next(rng_t* r) {
+    uint64_t old = r->st;
+    r->st = old * 6364136223846793005ull + r->inc;
+    uint32_t xs = (uint32_t)(((old >> 18u) ^ old) >> 27u), rot = (uint32_t)(old >> 59u);
+    return (xs >> rot) | (xs << ((32u - rot) & 31u));
+}
+static inline void pcg_seed(rng_t* r, uint64_t init, uint64_t seq) {
+    r->clean = 1; r->st = 0; r->inc = (seq << 1u) | 1u; pcg_next(r); r->st += init; pcg_next(r);
+}
+static inline float U(rng_t* r) {
+    if (r->clean) return (float)(pcg_next(r) >> 8) * (1.0f / 16777216.0f);
+    return minstd_uniform(r);
+}
+static inline uint64_t mix64(uint64_t z) {
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+
+/* multi-draw expression order: 0 = left to right (nvcc build), 1 = right to left (g++ build) */
+static inline void draw2(rng_t* r, int order, float* a, float* b) {
+    if (order == 0) { *a = U(r); *b = U(r); } else { *b = U(r); *a = U(r); }
+}
+static inline void draw3(rng_t* r, int order, float* a, float* b, float* c) {
+    if (order == 0) { *a = U(r); *b = U(r); *c = U(r); } else { *c = U(r); *b = U(r); *a = U(r); }
+}
+
+/* ---------------------------------------------------------------------------------------------- */
+/* scene                                                                                          */
+/* ---------------------------------------------------------------------------------------------- */
+enum { K_LIGHT = 0, K_SPHERE = 1, K_QUAD = 2, K_TRI = 3 };
+
+typedef struct {
+    int kind;
+    int mat;          /* material index (lights: index into the appended light materials) */
+    int light;        /* light index for K_LIGHT */
+    int invisible;
+    v3 a, b, c;       /* sphere: a=center, r in rad;  quad/light: a=Q|P, b=u, c=v;  tri: a=v0, b=v0v1, c=v0v2 */
+    float rad;
+    v3 normal, w;     /* planar */
+    float D, area;
+    v3 mid;           /* triangle middle_normal */
+    int smooth; v3 vn[3];
+    float lo[3], hi[3];
+} prim_t;
+
+typedef struct { int kind; float col[3]; float inv_scale; int even, odd, image; } tex_t;
+typedef struct { int kind; int tex; float fuzz, ior, intensity; int directional; } mat_t;
+typedef struct { float lo[3], hi[3]; int left, right, first, count; } node_t;
+
+typedef struct {
+    prim_t* prims; int nprims;
+    int* order;           /* BVH leaf order */
+    node_t* nodes; int nnodes;
+    tex_t* tex; int ntex;
+    mat_t* mat; int nmat;
+    rtc_image* img; int nimg;
+    unsigned char** img_bytes;
+    int* lights; int nlights;   /* prim index of each light, in light-list order */
+    rtc_camera cam;
+    rtc_background bg;
+    float* env;
+} scene_t;
+
+static void box_grow(float* lo, float* hi, v3 p) {
+    float c[3] = {p.x, p.y, p.z};
+    for (int k = 0; k < 3; ++k) { if (c[k] < lo[k]) lo[k] = c[k]; if (c[k] > hi[k]) hi[k] = c[k]; }
+}
+
+/* quad::quad (quad.cuh:55-67) / directional_light ctor (directional_light.cuh:45-58) */
+static void planar_init(prim_t* p) {
+    v3 n = vcross(p->b, p->c);
+    p->normal = vunit(n);
+    p->D = vdot(p->normal, p->a);
+    p->w = vdivs(n, vdot(n, n));
+    p->area = vlen(n);
+}
+
+static int cmp_axis;
+static const prim_t* cmp_prims;
+static int cmp_cent(const void* x, const void* y) {
+    const prim_t* a = &cmp_prims[*(const int*)x];
+    const prim_t* b = &cmp_prims[*(const int*)y];
+    float ca = a->lo[cmp_axis] + a->hi[cmp_axis], cb = b->lo[cmp_axis] + b->hi[cmp_axis];
+    return (ca > cb) - (ca < cb);
+}
+
+static int build_node(scene_t* s, int first, int count) {
+    int id = s->nnodes++;
+    node_t* nd = &s->nodes[id];
+    for (int k = 0; k < 3; ++k) { nd->lo[k] = FLT_MAX; nd->hi[k] = -FLT_MAX; }
+    for (int i = first; i < first + count; ++i) {
+        const prim_t* p = &s->prims[s->order[i]];
+        for (int k = 0; k < 3; ++k) {
+            if (p->lo[k] < nd->lo[k]) nd->lo[k] = p->lo[k];
+            if (p->hi[k] > nd->hi[k]) nd->hi[k] = p->hi[k];
+        }
+    }
+    if (count <= 2) { nd->left = nd->right = -1; nd->first = first; nd->count = count; return id; }
+    int ax = 0;
+    for (int k = 1; k < 3; ++k) if (nd->hi[k] - nd->lo[k] > nd->hi[ax] - nd->lo[ax]) ax = k;
+    cmp_axis = ax; cmp_prims = s->prims;
+    qsort(s->order + first, count, sizeof(int), cmp_cent);
+    int half = count / 2;
+    int l = build_node(s, first, half);
+    int r = build_node(s, first + half, count - half);
+    s->nodes[id].left = l; s->nodes[id].right = r; s->nodes[id].count = 0;
+    return id;
+}
+
+void* port_scene_create(const rtc_scene_desc* d) {
+    scene_t* s = (scene_t*)calloc(1, sizeof(scene_t));
+    if (!s || !d) { snprintf(g_err, sizeof g_err, "bad argument"); free(s); return NULL; }
+    int ntri = 0;
+    for (uint32_t m = 0; m < d->num_meshes; ++m) ntri += (int)d->meshes[m].num_triangles;
+    s->nprims = (int)(d->num_dir_lights + d->num_spheres + d->num_quads) + ntri;
+    s->prims = (prim_t*)calloc((size_t)s->nprims + 1, sizeof(prim_t));
+    s->ntex = (int)d->num_textures + (int)d->num_dir_lights;
+    s->tex = (tex_t*)calloc((size_t)s->ntex + 1, sizeof(tex_t));
+    s->nmat = (int)d->num_materials + (int)d->num_dir_lights;
+    s->mat = (mat_t*)calloc((size_t)s->nmat + 1, sizeof(mat_t));
+    s->nlights = (int)d->num_dir_lights;
+    s->lights = (int*)calloc((size_t)s->nlights + 1, sizeof(int));
+    for (uint32_t i = 0; i < d->num_textures; ++i) {
+        const rtc_texture* t = &d->textures[i];
+        tex_t* o = &s->tex[i];
+        o->kind = t->kind; memcpy(o->col, t->color, 12);
+        o->inv_scale = t->kind == RTC_TEX_CHECKER ? 1.0f / t->scale : 0.0f;   /* checker_texture.cuh:23 */
+        o->even = t->even; o->odd = t->odd; o->image = t->image;
+    }
+    for (uint32_t i = 0; i < d->num_materials; ++i) {
+        const rtc_material* m = &d->materials[i];
+        mat_t* o = &s->mat[i];
+        o->kind = m->kind; o->tex = m->texture; o->fuzz = m->fuzz < 1.0f ? m->fuzz : 1.0f;   /* metal.cuh:52 */
+        o->ior = m->ior; o->intensity = m->intensity; o->directional = m->directional;
+    }
+    s->nimg = (int)d->num_images;
+    s->img = (rtc_image*)calloc((size_t)s->nimg + 1, sizeof(rtc_image));
+    for (int i = 0; i < s->nimg; ++i) s->img[i] = d->images[i];
+    s->cam = d->camera;
+    s->bg = d->background;
+    int k = 0;
+    for (uint32_t i = 0; i < d->num_dir_lights; ++i, ++k) {
+        const rtc_dir_light* L = &d->dir_lights[i];
+        prim_t* p = &s->prims[k];
+        p->kind = K_LIGHT; p->light = (int)i; p->invisible = L->invisible;
+        p->a = Vp(L->position); p->b = Vp(L->u); p->c = Vp(L->v);
+        planar_init(p);
+        int ti = (int)d->num_textures + (int)i, mi = (int)d->num_materials + (int)i;
+        s->tex[ti].kind = RTC_TEX_SOLID; memcpy(s->tex[ti].col, L->color, 12);
+        /* m_mat = new diffuse_light(m_color, intensity, true, invisible) (directional_light.cuh:48) */
+        s->mat[mi].kind = RTC_MAT_DIFFUSE_LIGHT; s->mat[mi].tex = ti; s->mat[mi].intensity = L->intensity;
+        s->mat[mi].directional = 1;
+        p->mat = mi;
+        s->lights[i] = k;
+        v3 hu = vscale(0.5f, p->b), hv = vscale(0.5f, p->c);
+        for (int q = 0; q < 3; ++q) { p->lo[q] = FLT_MAX; p->hi[q] = -FLT_MAX; }
+        box_grow(p->lo, p->hi, vsub(vsub(p->a, hu), hv)); box_grow(p->lo, p->hi, vadd(vsub(p->a, hu), hv));
+        box_grow(p->lo, p->hi, vsub(vadd(p->a, hu), hv)); box_grow(p->lo, p->hi, vadd(vadd(p->a, hu), hv));
+    }
+    for (uint32_t i = 0; i < d->num_spheres; ++i, ++k) {
+        const rtc_sphere* S = &d->spheres[i];
+        prim_t* p = &s->prims[k];
+        p->kind = K_SPHERE; p->mat = S->material; p->a = Vp(S->center); p->rad = S->radius;
+        float r = fabsf(S->radius);
+        for (int q = 0; q < 3; ++q) { p->lo[q] = S->center[q] - r; p->hi[q] = S->center[q] + r; }
+    }
+    for (uint32_t i = 0; i < d->num_quads; ++i, ++k) {
+        const rtc_quad* Q = &d->quads[i];
+        prim_t* p = &s->prims[k];
+        p->kind = K_QUAD; p->mat = Q->material; p->a = Vp(Q->q); p->b = Vp(Q->u); p->c = Vp(Q->v);
+        planar_init(p);
+        for (int q = 0; q < 3; ++q) { p->lo[q] = FLT_MAX; p->hi[q] = -FLT_MAX; }
+        box_grow(p->lo, p->hi, p->a); box_grow(p->lo, p->hi, vadd(p->a, p->b));
+        box_grow(p->lo, p->hi, vadd(p->a, p->c)); box_grow(p->lo, p->hi, vadd(vadd(p->a, p->b), p->c));
+    }
+    for (uint32_t m = 0; m < d->num_meshes; ++m) {
+        const rtc_mesh* M = &d->meshes[m];
+        for (uint32_t f = 0; f < M->num_triangles; ++f, ++k) {
+            prim_t* p = &s->prims[k];
+            uint32_t ia = M->indices[3 * f], ib = M->indices[3 * f + 1], ic = M->indices[3 * f + 2];
+            v3 v0 = Vp(M->vertices + 3 * ia), v1 = Vp(M->vertices + 3 * ib), v2 = Vp(M->vertices + 3 * ic);
+            p->kind = K_TRI; p->mat = M->material;
+            /* triangle::triangle (triangle.cuh:87-123) */
+            p->a = v0; p->b = vsub(v1, v0); p->c = vsub(v2, v0);
+            p->mid = vunit(vcross(vsub(v0, v1), vsub(v0, v2)));
+            p->smooth = M->smooth && M->normals;
+            if (p->smooth) {
+                p->vn[0] = vunit(Vp(M->normals + 3 * ia)); p->vn[1] = vunit(Vp(M->normals + 3 * ib));
+                p->vn[2] = vunit(Vp(M->normals + 3 * ic));
+            }
+            for (int q = 0; q < 3; ++q) { p->lo[q] = FLT_MAX; p->hi[q] = -FLT_MAX; }
+            box_grow(p->lo, p->hi, v0); box_grow(p->lo, p->hi, v1); box_grow(p->lo, p->hi, v2);
+        }
+    }
+    for (int i = 0; i < s->nprims; ++i)   /* conservative padding */
+        for (int q = 0; q < 3; ++q) {
+            float e = 1e-4f * (fabsf(s->prims[i].lo[q]) + fabsf(s->prims[i].hi[q])) + 1e-5f;
+            s->prims[i].lo[q] -= e; s->prims[i].hi[q] += e;
+        }
+    s->order = (int*)malloc(sizeof(int) * ((size_t)s->nprims + 1));
+    for (int i = 0; i < s->nprims; ++i) s->order[i] = i;
+    s->nodes = (node_t*)calloc(2 * (size_t)s->nprims + 2, sizeof(node_t));
+    if (s->nprims > 0) build_node(s, 0, s->nprims);
+    if (d->background.kind == RTC_BG_ENV_MAP) s->env = (float*)d->background.env_rgb;   /* caller keeps it alive */
+    return s;
+}
+
+void port_scene_destroy(void* p) {
+    scene_t* s = (scene_t*)p;
+    if (!s) return;
+    free(s->prims); free(s->order); free(s->nodes); free(s->tex); free(s->mat); free(s->img); free(s->lights);
+    free(s);
+}
+
+/* ---------------------------------------------------------------------------------------------- */
+/* intersection                                                                                   */
+/* ---------------------------------------------------------------------------------------------- */
+typedef struct { float t; int prim; v3 p, n; float u, v; int front, mat; } hit_t;
+
+/* hit_record::set_face_normal (hit_record.cuh:34-38) */
+static inline void face(hit_t* h, v3 dir, v3 outward) {
+    h->front = vdot(dir, outward) < 0.0f;
+    h->n = h->front ? outward : vneg(outward);
+}
+
+/* sphere::hit (sphere.cuh:111-135) */
+static int sphere_t(const prim_t* p, v3 o, v3 d, float tmin, float tmax, float* t) {
+    v3 oc = vsub(o, p->a);
+    float a = vlensq(d);
+    float half_b = oc.x * d.x + oc.y * d.y + oc.z * d.z;
+    float c = vlensq(oc) - p->rad * p->rad;
+    float disc = half_b * half_b - a * c;
+    if (disc < 0) return 0;
+    float sq = sqrtf(disc);
+    float root = (-half_b - sq) / a;
+    if (!(tmin < root && root < tmax)) {
+        root = (-half_b + sq) / a;
+        if (!(tmin < root && root < tmax)) return 0;
+    }
+    *t = root;
+    return 1;
+}
+
+/* quad::hit (quad.cuh:100-133) and directional_light::hit (directional_light.cuh:76-120) */
+static int planar_t(const prim_t* p, v3 o, v3 d, float tmin, float tmax, int centred, float* t, float* al, float* be) {
+    float denom = vdot(p->normal, d);
+    if (fabs(denom) < 1e-8) return 0;
+    float tt = (p->D - vdot(p->normal, o)) / denom;
+    if (!(tmin <= tt && tt <= tmax)) return 0;
+    v3 ip = vat(o, d, tt);
+    v3 pl = vsub(ip, p->a);
+    float a = vdot(p->w, vcross(pl, p->c));
+    float b = vdot(p->w, vcross(p->b, pl));
+    if (centred) { if ((a < -0.5) || (0.5 < a) || (b < -0.5) || (0.5 < b)) return 0; }
+    else { if ((a < 0) || (1 < a) || (b < 0) || (1 < b)) return 0; }
+    *t = tt; *al = a; *be = b;
+    return 1;
+}
+
+/* triangle::hit (triangle.cuh:130-160) */
+static int tri_t(const prim_t* p, v3 o, v3 d, float tmin, float tmax, float* t, float* bu, float* bv) {
+    v3 pv = vcross(d, p->c);
+    float det = vdot(p->b, pv);
+    if (fabsf(det) < 0.000001f) return 0;
+    float inv_det = 1.0f / det;
+    v3 tv = vsub(o, p->a);
+    float u = vdot(tv, pv) * inv_det;
+    if (u < 0 || u > 1) return 0;
+    v3 qv = vcross(tv, p->b);
+    float v = vdot(d, qv) * inv_det;
+    if (v < 0 || u + v > 1) return 0;
+    float tt = vdot(p->c, qv) * inv_det;
+    if (tt < tmin || tt > tmax) return 0;
+    *t = tt; *bu = u; *bv = v;
+    return 1;
+}
+
+static int prim_t_test(const prim_t* p, v3 o, v3 d, float tmin, float tmax, int hide, float* t) {
+    float a, b;
+    switch (p->kind) {
+    case K_SPHERE: return sphere_t(p, o, d, tmin, tmax, t);
+    case K_QUAD: return planar_t(p, o, d, tmin, tmax, 0, t, &a, &b);
+    case K_LIGHT:
+        if (!planar_t(p, o, d, tmin, tmax, 1, t, &a, &b)) return 0;
+        return !(p->invisible && hide);   /* directional_light.cuh:106 */
+    default: return tri_t(p, o, d, tmin, tmax, t, &a, &b);
+    }
+}
+
+/* aabb::hit semantics (aabb.cuh:141-166) on the port's own (padded) boxes */
+static int box_hit(const node_t* n, v3 o, v3 d, float tmin, float tmax) {
+    const float oo[3] = {o.x, o.y, o.z}, dd[3] = {d.x, d.y, d.z};
+    for (int a = 0; a < 3; ++a) {
+        float invD = 1 / dd[a];
+        float t0 = (n->lo[a] - oo[a]) * invD, t1 = (n->hi[a] - oo[a]) * invD;
+        if (invD < 0) { float tmp = t0; t0 = t1; t1 = tmp; }
+        if (t0 > tmin) tmin = t0;
+        if (t1 < tmax) tmax = t1;
+        if (tmax < tmin) return 0;
+    }
+    return 1;
+}
+
+static int closest(const scene_t* s, v3 o, v3 d, float tmin, float tmax, int hide, float* tout, int* pout) {
+    int stack[128], sp = 0, best = -1;
+    float best_t = tmax;
+    if (s->nprims == 0) return 0;
+    stack[sp++] = 0;
+    while (sp) {
+        const node_t* n = &s->nodes[stack[--sp]];
+        if (!box_hit(n, o, d, tmin, best_t)) continue;
+        if (n->left < 0) {
+            for (int i = n->first; i < n->first + n->count; ++i) {
+                float t;
+                if (prim_t_test(&s->prims[s->order[i]], o, d, tmin, best_t, hide, &t)) { best_t = t; best = s->order[i]; }
+            }
+        } else {
+            if (sp + 2 > 128) return 0;
+            stack[sp++] = n->right;
+            stack[sp++] = n->left;
+        }
+    }
+    *tout = best_t; *pout = best;
+    return best >= 0;
+}
+
+/* the rest of each hit() for the winner */
+static void finalize(const scene_t* s, int pi, float t, v3 o, v3 d, hit_t* h) {
+    const prim_t* p = &s->prims[pi];
+    h->t = t; h->prim = pi; h->mat = p->mat;
+    if (p->kind == K_SPHERE) {
+        h->p = vat(o, d, t);
+        v3 outward = vdivs(vsub(h->p, p->a), p->rad);
+        face(h, d, outward);
+        /* get_sphere_uv (uvmapping.cuh:204-228), default mapping */
+        float theta = f_acos(-outward.y);
+        float phi = f_atan2(-outward.z, outward.x) + PI_F;
+        float sc = phi / (2 * PI_F), tc = theta / PI_F;
+        sc = fmodf(sc * 1.0f, 1.0f); tc = fmodf(tc * 1.0f, 1.0f);
+        h->u = 1.0f * sc + 0.0f; h->v = 1.0f * tc + 0.0f;
+    } else if (p->kind == K_QUAD || p->kind == K_LIGHT) {
+        v3 ip = vat(o, d, t), pl = vsub(ip, p->a);
+        float a = vdot(p->w, vcross(pl, p->c)), b = vdot(p->w, vcross(p->b, pl));
+        h->p = ip;
+        face(h, d, p->normal);
+        if (p->kind == K_QUAD) { h->u = a; h->v = b; } else { h->u = a + 0.5f; h->v = b + 0.5f; }
+    } else {
+        h->p = vat(o, d, t);
+        v3 normal = p->mid;
+        if (p->smooth) {
+            v3 pv = vcross(d, p->c);
+            float inv_det = 1.0f / vdot(p->b, pv);
+            v3 tv = vsub(o, p->a);
+            float bu = vdot(tv, pv) * inv_det;
+            float bv = vdot(d, vcross(tv, p->b)) * inv_det;
+            float bc = 1 - bu - bv;
+            normal = vadd(vadd(vscale(bu, p->vn[1]), vscale(bv, p->vn[2])), vscale(bc, p->vn[0]));
+        }
+        face(h, d, normal);
+        h->u = 0.0f; h->v = 0.0f;   /* get_triangle_uv over all-zero vertex uvs */
+    }
+}
+
+/* ---------------------------------------------------------------------------------------------- */
+/* shading                                                                                        */
+/* ---------------------------------------------------------------------------------------------- */
+typedef struct { float r, g, b; } rgb_t;
+
+/* texture::value: solid / checker / image (solid_color_texture.cuh:34, checker_texture.cuh:33-41,
+   image_texture.cuh:54-70, bitmap_image.cuh:74-91) */
+static rgb_t tex_value(const scene_t* s, int ti, float u, float v, v3 p) {
+    for (int guard = 0; guard < 8 && ti >= 0 && ti < s->ntex; ++guard) {
+        const tex_t* t = &s->tex[ti];
+        if (t->kind == RTC_TEX_SOLID) { rgb_t c = {t->col[0], t->col[1], t->col[2]}; return c; }
+        if (t->kind == RTC_TEX_CHECKER) {
+            int xi = (int)floorf(t->inv_scale * p.x), yi = (int)floorf(t->inv_scale * p.y), zi = (int)floorf(t->inv_scale * p.z);
+            ti = ((xi + yi + zi) % 2 == 0) ? t->even : t->odd;
+            continue;
+        }
+        const rtc_image* im = &s->img[t->image];
+        if (im->height <= 0) { rgb_t c = {0, 1, 1}; return c; }
+        float uu = u < 0 ? 0 : (u > 1 ? 1 : u);
+        float vc = v < 0 ? 0 : (v > 1 ? 1 : v);
+        float vv = 1.0f - vc;
+        int i = (int)(uu * im->width), j = (int)(vv * im->height);
+        i = i < 0 ? 0 : (i < im->width ? i : im->width - 1);
+        j = j < 0 ? 0 : (j < im->height ? j : im->height - 1);
+        const unsigned char* px = im->rgb + (size_t)j * im->width * 3 + (size_t)i * 3;
+        float cs = 1.0f / 255.0f;
+        rgb_t c = {cs * px[0], cs * px[1], cs * px[2]};
+        return c;
+    }
+    rgb_t z = {0, 0, 0};
+    return z;
+}
+
+static rgb_t background(const scene_t* s, v3 dir) {
+    const rtc_background* B = &s->bg;
+    rgb_t c;
+    if (B->kind == RTC_BG_CONSTANT) { c.r = B->color[0]; c.g = B->color[1]; c.b = B->color[2]; return c; }
+    v3 ud = vunit(dir);
+    if (B->kind == RTC_BG_SKY_GRADIENT) {
+        float a = 0.5f * (ud.y + 1.0f), b = 1.0f - a;
+        c.r = b * B->color[0] + a * B->top[0]; c.g = b * B->color[1] + a * B->top[1]; c.b = b * B->color[2] + a * B->top[2];
+        return c;
+    }
+    double theta = acos((double)-ud.y), phi = atan2((double)-ud.z, (double)ud.x) + 3.14159265358979323846;
+    double uu = phi / (2.0 * 3.14159265358979323846), vv = theta / 3.14159265358979323846;
+    int W = B->env_width, H = B->env_height;
+    int x = (int)(uu * W); x = x < 0 ? 0 : (x >= W ? W - 1 : x);
+    int y = (int)((1.0 - vv) * H); y = y < 0 ? 0 : (y >= H ? H - 1 : y);
+    const float* px = s->env + 3 * ((size_t)y * W + x);
+    c.r = px[0]; c.g = px[1]; c.b = px[2];
+    return c;
+}
+
+/* directional_light::pdf_value (directional_light.cuh:147-158) */
+static float light_pdf(const scene_t* s, int li, v3 o, v3 v) {
+    const prim_t* p = &s->prims[s->lights[li]];
+    float t, a, b;
+    if (!planar_t(p, o, v, 0.00001f, INFINITY, 1, &t, &a, &b)) return 0;
+    v3 nrm = vdot(v, p->normal) < 0.0f ? p->normal : vneg(p->normal);
+    float distance_squared = t * t * vlensq(v);
+    float cosine = fabsf(vdot(v, nrm) / vlen(v));
+    return distance_squared / (cosine * p->area);
+}
+
+typedef struct { v3 u, v, w; } onb_t;
+static onb_t build_from_w(v3 n) {   /* onb::build_from_w (onb.cuh:122-128) */
+    onb_t b;
+    b.w = vunit(n);
+    v3 a = (fabsf(b.w.x) > 0.9f) ? V(0, 1, 0) : V(1, 0, 0);
+    b.v = vunit(vcross(b.w, a));
+    b.u = vcross(b.w, b.v);
+    return b;
+}
+static v3 onb_local(const onb_t* b, v3 a) { return vadd(vadd(vscale(a.x, b->u), vscale(a.y, b->v)), vscale(a.z, b->w)); }
+
+/* camera::ray_color (camera.cuh:149-264) for one sample; returns radiance, counts closest-hit calls */
+static rgb_t ray_color(const scene_t* s, v3 o, v3 d, int max_depth, rng_t* rng, int order, int clean, uint64_t* rays) {
+    rgb_t res = {0, 0, 0}, att = {1, 1, 1};
+    for (int depth = max_depth; depth > 0; --depth) {
+        int hide = depth == max_depth;
+        float t; int pi;
+        (*rays)++;
+        if (!closest(s, o, d, 0.00001f, FLT_MAX, hide, &t, &pi)) {
+            rgb_t bg = background(s, d);
+            res.r += att.r * bg.r; res.g += att.g * bg.g; res.b += att.b * bg.b;
+            break;
+        }
+        hit_t h;
+        finalize(s, pi, t, o, d, &h);
+        const mat_t* m = &s->mat[h.mat];
+        rgb_t em = {0, 0, 0};
+        int alpha0 = 0;
+        if (m->kind == RTC_MAT_DIFFUSE_LIGHT) {   /* diffuse_light::emitted (diffuse_light.cuh:45-67) */
+            if (m->directional && !h.front) alpha0 = 1;
+            else { rgb_t tv = tex_value(s, m->tex, h.u, h.v, h.p); em.r = tv.r * m->intensity; em.g = tv.g * m->intensity; em.b = tv.b * m->intensity; }
+        }
+        if (alpha0) {   /* invisible re-hit (camera.cuh:177-183) */
+            float t2; int p2;
+            (*rays)++;
+            if (closest(s, o, d, h.t + 0.001f, FLT_MAX, hide, &t2, &p2)) { finalize(s, p2, t2, o, d, &h); m = &s->mat[h.mat]; }
+        }
+        if (m->kind == RTC_MAT_DIFFUSE_LIGHT) {
+            res.r += att.r * em.r; res.g += att.g * em.g; res.b += att.b * em.b;
+            break;
+        }
+        res.r += att.r * em.r; res.g += att.g * em.g; res.b += att.b * em.b;
+        if (m->kind == RTC_MAT_METAL) {   /* metal::scatter (metal.cuh:57-64) */
+            rgb_t a = tex_value(s, m->tex, h.u, h.v, h.p);
+            v3 refl = vreflect(vunit(d), h.n);
+            v3 p;
+            do {   /* random_in_unit_sphere (gpu_randomizer.cuh:70-76) */
+                float x, y, z;
+                draw3(rng, order, &x, &y, &z);
+                p = V(2.0f * x - 1.0f, 2.0f * y - 1.0f, 2.0f * z - 1.0f);
+            } while (p.x * p.x + p.y * p.y + p.z * p.z >= 1.0f);
+            o = h.p;
+            d = vadd(refl, vscale(m->fuzz, p));
+            att.r *= a.r; att.g *= a.g; att.b *= a.b;
+            continue;
+        }
+        if (m->kind == RTC_MAT_DIELECTRIC) {   /* dielectric::scatter (dielectric.cuh:32-63) */
+            float ratio = h.front ? (1.0f / m->ior) : m->ior;
+            v3 ud = vunit(d);
+            float ct = vdot(vneg(ud), h.n);
+            float cos_theta = ct < 1.0f ? ct : 1.0f;
+            float sin_theta = sqrtf(1.0f - cos_theta * cos_theta);
+            int reflect = ratio * sin_theta > 1.0;
+            if (!reflect) {
+                float r0 = (1 - ratio) / (1 + ratio);
+                r0 = r0 * r0;
+                float refl = r0 + (1 - r0) * (float)(pow((1 - cos_theta), 5));
+                reflect = refl > U(rng);
+            }
+            o = h.p;
+            d = reflect ? vreflect(ud, h.n) : vrefract(ud, h.n, ratio);
+            continue;
+        }
+        /* lambertian (lambertian.cuh:63-143) + mixture_pdf(hittable_pdf(lights), cosine_pdf) */
+        rgb_t a = tex_value(s, m->tex, h.u, h.v, h.p);
+        onb_t b = build_from_w(h.n);
+        v3 dir;
+        float pdf_val;
+        int mixture = !clean || s->nlights > 0;
+        if (mixture && U(rng) < 0.5f) {
+            if (s->nlights == 0) dir = V(0, 0, 0);
+            else {
+                if (s->nlights > 1) (void)U(rng);   /* get_int(rng, 0, n-1) == 0 */
+                const prim_t* L = &s->prims[s->lights[0]];
+                float ru, rv;
+                draw2(rng, order, &ru, &rv);
+                v3 pp = vadd(vadd(L->a, vscale(ru - 0.5f, L->b)), vscale(rv - 0.5f, L->c));
+                dir = vsub(pp, h.p);
+            }
+        } else {
+            float r1 = U(rng), r2 = U(rng);   /* random_cosine_direction (gpu_randomizer.cuh:121-133) */
+            float phi = 6.28318530718f * r1;
+            float z = sqrtf(1 - r2), r2s = sqrtf(r2);
+            dir = onb_local(&b, V(f_cos(phi) * r2s, f_sin(phi) * r2s, z));
+        }
+        float cosv = vdot(vunit(dir), b.w) / PI_F;
+        float cpdf = 0.0f > cosv ? 0.0f : cosv;
+        if (mixture) {
+            float weight = 1.0f / (float)s->nlights, sum = 0.0f;
+            for (int li = 0; li < s->nlights; ++li) sum += weight * light_pdf(s, li, h.p, dir);
+            pdf_val = 0.5f * sum + (1.0f - 0.5f) * cpdf;
+        } else {
+            pdf_val = cpdf;
+        }
+        float cth = vdot(h.n, vunit(dir));
+        float spdf = cth < 0 ? 0.0f : cth / PI_F;
+        float rcp = 1 / pdf_val;
+        att.r *= rcp * (a.r * spdf); att.g *= rcp * (a.g * spdf); att.b *= rcp * (a.b * spdf);
+        o = h.p;
+        d = dir;
+    }
+    return res;
+}
+
+/* ---------------------------------------------------------------------------------------------- */
+/* render loop (render kernel, gpu.cu:761-790)                                                    */
+/* ---------------------------------------------------------------------------------------------- */
+typedef struct {
+    v3 origin, llc, horizontal, vertical, u, v;
+    float lens_radius;
+} cam_t;
+
+/* perspective_camera::initialize (perspective_camera.cuh:41-108) */
+static cam_t make_cam(const rtc_camera* C) {
+    cam_t c;
+    float theta = C->vfov * PI_F / 180.0f;
+    float half_height = tanf(theta / 2);
+    v3 w = vunit(vsub(Vp(C->look_from), Vp(C->look_at)));
+    v3 u = vunit(vcross(Vp(C->up), w));
+    v3 v = vcross(w, u);
+    float half_width = C->aspect * half_height, f = C->focus;
+    c.origin = Vp(C->look_from);
+    c.llc = vsub(vsub(vsub(c.origin, vscale(half_width * f, u)), vscale(half_height * f, v)), vscale(f, w));
+    c.horizontal = vscale(2 * half_width * f, u);
+    c.vertical = vscale(2 * half_height * f, v);
+    c.u = u; c.v = v;
+    c.lens_radius = C->aperture / 2;
+    return c;
+}
+
+typedef struct {
+    const scene_t* s; const rtc_render_params* p; const int64_t* pix; int64_t n; float* out;
+    cam_t cam; int sq; volatile int64_t next; uint64_t rays; pthread_mutex_t mu;
+} job_t;
+
+static void render_one(job_t* J, int64_t q, uint64_t* rays) {
+    const rtc_render_params* P = J->p;
+    int64_t pixel_index = J->pix[q];
+    int i = (int)(pixel_index % P->width), j = (int)(pixel_index / P->width);
+    float pr = 0, pg = 0, pb = 0;
+    const cam_t* c = &J->cam;
+    int clean = P->mode == RTC_MODE_CLEAN, order = clean ? 0 : P->draw_order;
+    rng_t rng;
+    memset(&rng, 0, sizeof rng);
+    int nsamp = clean ? P->spp : J->sq * J->sq;
+    if (!clean) minstd_seed(&rng, P->seed + (uint32_t)pixel_index);
+    for (int sidx = 0; sidx < nsamp; ++sidx) {
+        float u, v;
+        if (clean) {
+            pcg_seed(&rng, mix64(((uint64_t)P->seed << 32) ^ (uint64_t)pixel_index), (uint64_t)sidx);
+            float ju = U(&rng), jv = U(&rng);
+            u = ((float)i + ju) / (float)P->width;
+            v = ((float)j + jv) / (float)P->height;
+        } else {
+            int s_j = sidx / J->sq, s_i = sidx % J->sq;
+            float ur = U(&rng);
+            u = (i + (s_i + ur) / J->sq) / (float)P->width;
+            v = (j + (s_j + ur) / J->sq) / (float)P->height;
+        }
+        /* perspective_camera::get_ray (perspective_camera.cuh:112-117) */
+        v3 p;
+        do {
+            float a, b;
+            draw2(&rng, order, &a, &b);
+            p = V(2.0f * a - 1.0f, 2.0f * b - 1.0f, 2.0f * 0.0f - 0.0f);
+        } while (vdot(p, p) >= 1.0f);
+        v3 rd = vscale(c->lens_radius, p);
+        v3 offset = vadd(V(c->u.x * rd.x, c->u.y * rd.x, c->u.z * rd.x), V(c->v.x * rd.y, c->v.y * rd.y, c->v.z * rd.y));
+        (void)(0.0f + U(&rng) * (1.0f - 0.0f));   /* time sample */
+        v3 o = vadd(c->origin, offset);
+        v3 d = vsub(vsub(vadd(vadd(c->llc, vscale(u, c->horizontal)), vscale(v, c->vertical)), c->origin), offset);
+        rgb_t col = ray_color(J->s, o, d, P->max_depth, &rng, order, clean, rays);
+        if (clean && !(isfinite(col.r) && isfinite(col.g) && isfinite(col.b))) continue;
+        pr += col.r; pg += col.g; pb += col.b;
+    }
+    J->out[4 * q] = pr; J->out[4 * q + 1] = pg; J->out[4 * q + 2] = pb; J->out[4 * q + 3] = 1.0f;
+}
+
+static void* worker(void* arg) {
+    job_t* J = (job_t*)arg;
+    uint64_t rays = 0;
+    for (;;) {
+        int64_t b = __atomic_fetch_add(&J->next, 16, __ATOMIC_RELAXED);
+        if (b >= J->n) break;
+        int64_t e = b + 16 < J->n ? b + 16 : J->n;
+        for (int64_t q = b; q < e; ++q) render_one(J, q, &rays);
+    }
+    __atomic_fetch_add(&J->rays, rays, __ATOMIC_RELAXED);
+    return NULL;
+}
+
+int port_render_pixels(void* sp, const rtc_render_params* p, const int64_t* pix, int64_t n, float* out,
+                       uint64_t* rays_out, int threads) {
+    scene_t* s = (scene_t*)sp;
+    if (!s || !p || !out || (n > 0 && !pix)) { snprintf(g_err, sizeof g_err, "bad argument"); return 1; }
+    job_t J;
+    memset(&J, 0, sizeof J);
+    J.s = s; J.p = p; J.pix = pix; J.n = n; J.out = out;
+    J.cam = make_cam(&s->cam);
+    J.sq = (int)sqrt((double)p->spp);
+    if (threads <= 0) threads = 1;
+    if (threads == 1) worker(&J);
+    else {
+        pthread_t* th = (pthread_t*)malloc(sizeof(pthread_t) * (size_t)threads);
+        for (int t = 0; t < threads; ++t) pthread_create(&th[t], NULL, worker, &J);
+        for (int t = 0; t < threads; ++t) pthread_join(th[t], NULL);
+        free(th);
+    }
+    if (rays_out) *rays_out = J.rays;
+    return 0;
+}
+
+int port_trace_closest(void* sp, const float* rays, int64_t n, int depth, int max_depth, int32_t* prim, float* tout) {
+    scene_t* s = (scene_t*)sp;
+    if (!s || !rays) return 1;
+    for (int64_t k = 0; k < n; ++k) {
+        const float* R = rays + 8 * k;
+        float t; int pi;
+        int h = closest(s, V(R[0], R[1], R[2]), V(R[4], R[5], R[6]), R[3], R[7], depth == max_depth, &t, &pi);
+        if (prim) prim[k] = h ? pi : -1;
+        if (tout) tout[k] = h ? t : INFINITY;
+    }
+    return 0;
+}
+
+int port_rng_draws(uint32_t seed, int64_t n, float* out) {
+    rng_t r;
+    minstd_seed(&r, seed);
+    for (int64_t k = 0; k < n; ++k) out[k] = U(&r);
+    return 0;
+}
+
+const char* port_last_error(void) { return g_err; }
