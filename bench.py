@@ -241,7 +241,9 @@ def main():
     out = torch.empty((H, W, 4), dtype=torch.float32, device="cuda")
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     counters = torch.zeros(4, dtype=torch.int64, device="cuda")
-    stream = torch.cuda.current_stream()
+    # a dedicated stream: the kernels and the CUDA events that time them are on the same stream
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     sp = stream.cuda_stream
 
     def launch(cnt=None):

@@ -1,0 +1,202 @@
+// rtc_sceneconfig.hpp - C++ adapter from the reference's sceneConfig to rtc_scene_desc.
+//
+// Header-only and templated on the config type, so it compiles wherever the reference's
+// scenes/scene_config.h (flarive/CortexRaytracerCuda core/src/scenes/scene_config.h:452-459) is
+// included, without this repository depending on glm.  It reproduces how the reference's load_scene
+// turns a sceneConfig into objects (core/src/gpu.cu:481-751):
+//   * object order: directional lights, spheres, quads (gpu.cu:504-547);
+//   * materials and textures resolved by name, first match wins, in the order fetchMaterial /
+//     fetchTexture search them (gpu.cu:193-470): lambertian (texture if named, else rgb), metal (rgb,
+//     fuzziness), dielectric (refraction); solid colour, checker (textures if both resolve, else
+//     colours; odd lands in m_even as scene_factory does, scene_factory.cuh:619-629), image;
+//   * an object whose material does not resolve is skipped, as `if (mat)` skips it (gpu.cu:531).
+// Primitives the B200 path does not cover (planes, boxes, cones, cylinders, disks, tori, volumes,
+// omni/spot lights, OBJ meshes) and transforms are reported in `skipped`.
+// Image textures need decoded RGB8 pixels: pass `load_image(filepath, &w, &h)` returning a pointer
+// that stays valid while the description is used (the reference decodes with stbi_load, gpu.cu:1743).
+#pragma once
+
+#include <cstring>
+#include <functional>
+#include <string>
+#include <vector>
+
+#include "rtc.h"
+
+namespace rtc_adapter {
+
+struct SceneHolder {
+    std::vector<rtc_texture> textures;
+    std::vector<rtc_image> images;
+    std::vector<rtc_material> materials;
+    std::vector<rtc_dir_light> dir_lights;
+    std::vector<rtc_sphere> spheres;
+    std::vector<rtc_quad> quads;
+    std::vector<std::string> skipped;
+    rtc_scene_desc desc{};
+
+    const rtc_scene_desc* finish() {
+        desc.textures = textures.data();
+        desc.num_textures = (uint32_t)textures.size();
+        desc.images = images.data();
+        desc.num_images = (uint32_t)images.size();
+        desc.materials = materials.data();
+        desc.num_materials = (uint32_t)materials.size();
+        desc.dir_lights = dir_lights.data();
+        desc.num_dir_lights = (uint32_t)dir_lights.size();
+        desc.spheres = spheres.data();
+        desc.num_spheres = (uint32_t)spheres.size();
+        desc.quads = quads.data();
+        desc.num_quads = (uint32_t)quads.size();
+        desc.meshes = nullptr;
+        desc.num_meshes = 0;
+        return &desc;
+    }
+};
+
+using ImageLoader = std::function<const uint8_t*(const char* filepath, int* width, int* height)>;
+
+namespace detail {
+inline bool same(const char* a, const char* b) { return a && b && std::strcmp(a, b) == 0; }
+inline bool named(const char* a) { return a && a[0] != '\0'; }
+template <class V> void put3(float* dst, const V& v) { dst[0] = v.x; dst[1] = v.y; dst[2] = v.z; }
+template <class C> void putc3(float* dst, const C& c) { dst[0] = c.r(); dst[1] = c.g(); dst[2] = c.b(); }
+}  // namespace detail
+
+// Converts `cfg` (a reference sceneConfig) into `out`; returns out.finish().
+template <class SceneConfig>
+const rtc_scene_desc* from_sceneconfig(const SceneConfig& cfg, SceneHolder& out, const ImageLoader& load_image = nullptr) {
+    using namespace detail;
+    const auto& T = cfg.texturesCfg;
+    const auto& M = cfg.materialsCfg;
+
+    auto solid = [&](const auto& c) {
+        rtc_texture t{};
+        t.kind = RTC_TEX_SOLID;
+        putc3(t.color, c);
+        t.even = t.odd = t.image = -1;
+        out.textures.push_back(t);
+        return (int)out.textures.size() - 1;
+    };
+
+    std::function<int(const char*, int)> fetch_texture = [&](const char* name, int depth) -> int {
+        if (!named(name) || depth > 4) return -1;
+        for (int i = 0; i < T.solidColorTextureCount; ++i)
+            if (same(T.solidColorTextures[i].name, name)) return solid(T.solidColorTextures[i].rgb);
+        for (int i = 0; i < T.imageTextureCount; ++i) {
+            if (!same(T.imageTextures[i].name, name)) continue;
+            if (!load_image) { out.skipped.push_back(std::string("image texture without loader: ") + name); return -1; }
+            int w = 0, h = 0;
+            const uint8_t* px = load_image(T.imageTextures[i].filepath, &w, &h);
+            if (!px || w <= 0 || h <= 0) { out.skipped.push_back(std::string("image not loaded: ") + name); return -1; }
+            out.images.push_back(rtc_image{px, w, h});
+            rtc_texture t{};
+            t.kind = RTC_TEX_IMAGE;
+            t.even = t.odd = -1;
+            t.image = (int)out.images.size() - 1;
+            out.textures.push_back(t);
+            return (int)out.textures.size() - 1;
+        }
+        for (int i = 0; i < T.checkerTextureCount; ++i) {
+            const auto& c = T.checkerTextures[i];
+            if (!same(c.name, name)) continue;
+            int odd = fetch_texture(c.oddTextureName, depth + 1);
+            int even = fetch_texture(c.evenTextureName, depth + 1);
+            if (odd < 0 || even < 0) { odd = solid(c.oddColor); even = solid(c.evenColor); }
+            rtc_texture t{};
+            t.kind = RTC_TEX_CHECKER;
+            t.scale = c.scale;
+            t.even = odd;    // checker_texture(scale, odd, even): m_even <- odd (checker_texture.cuh:28-31)
+            t.odd = even;
+            t.image = -1;
+            out.textures.push_back(t);
+            return (int)out.textures.size() - 1;
+        }
+        out.skipped.push_back(std::string("texture kind not covered: ") + name);
+        return -1;
+    };
+
+    auto fetch_material = [&](const char* name) -> int {
+        if (!named(name)) return -1;
+        for (int i = 0; i < M.lambertianMaterialCount; ++i) {
+            const auto& m = M.lambertianMaterials[i];
+            if (!same(m.name, name)) continue;
+            int tex = named(m.textureName) ? fetch_texture(m.textureName, 0) : solid(m.rgb);
+            if (tex < 0) return -1;
+            out.materials.push_back(rtc_material{RTC_MAT_LAMBERTIAN, tex, 0.f, 0.f, 0.f, 0});
+            return (int)out.materials.size() - 1;
+        }
+        for (int i = 0; i < M.metalMaterialCount; ++i) {
+            const auto& m = M.metalMaterials[i];
+            if (!same(m.name, name)) continue;
+            out.materials.push_back(rtc_material{RTC_MAT_METAL, solid(m.rgb), m.fuzziness < 1 ? m.fuzziness : 1.f, 0.f, 0.f, 0});
+            return (int)out.materials.size() - 1;
+        }
+        for (int i = 0; i < M.dielectricMaterialCount; ++i) {
+            const auto& m = M.dielectricMaterials[i];
+            if (!same(m.name, name)) continue;
+            out.materials.push_back(rtc_material{RTC_MAT_DIELECTRIC, -1, 0.f, m.refraction, 0.f, 0});
+            return (int)out.materials.size() - 1;
+        }
+        out.skipped.push_back(std::string("material not covered or missing: ") + name);
+        return -1;
+    };
+
+    const auto& L = cfg.lightsCfg;
+    if (L.omniLightCount) out.skipped.push_back("omni lights");
+    for (int i = 0; i < L.dirLightCount; ++i) {
+        const auto& d = L.dirLights[i];
+        rtc_dir_light l{};
+        put3(l.position, d.position);
+        put3(l.u, d.u);
+        put3(l.v, d.v);
+        putc3(l.color, d.rgb);
+        l.intensity = d.intensity;
+        l.invisible = d.invisible ? 1 : 0;
+        out.dir_lights.push_back(l);
+    }
+    if (L.spotLightCount) out.skipped.push_back("spot lights");
+
+    const auto& P = cfg.primitivesCfg;
+    for (int i = 0; i < P.spherePrimitiveCount; ++i) {
+        const auto& s = P.spherePrimitives[i];
+        int m = fetch_material(s.materialName);
+        if (m < 0) continue;
+        rtc_sphere o{};
+        put3(o.center, s.position);
+        o.radius = s.radius;
+        o.material = m;
+        out.spheres.push_back(o);
+    }
+    if (P.planePrimitiveCount) out.skipped.push_back("planes");
+    for (int i = 0; i < P.quadPrimitiveCount; ++i) {
+        const auto& q = P.quadPrimitives[i];
+        int m = fetch_material(q.materialName);
+        if (m < 0) continue;
+        rtc_quad o{};
+        put3(o.q, q.position);
+        put3(o.u, q.u);
+        put3(o.v, q.v);
+        o.material = m;
+        out.quads.push_back(o);
+    }
+    if (P.boxPrimitiveCount) out.skipped.push_back("boxes");
+    if (P.conePrimitiveCount || P.cylinderPrimitiveCount || P.diskPrimitiveCount || P.torusPrimitiveCount ||
+        P.volumePrimitiveCount)
+        out.skipped.push_back("cones/cylinders/disks/tori/volumes");
+    if (cfg.meshesCfg.objMeshCount) out.skipped.push_back("OBJ meshes (pass triangles as rtc_mesh)");
+
+    const auto& C = cfg.cameraCfg;
+    put3(out.desc.camera.look_from, C.lookFrom);
+    put3(out.desc.camera.look_at, C.lookAt);
+    put3(out.desc.camera.up, C.upAxis);
+    out.desc.camera.vfov = C.fov;
+    out.desc.camera.aspect = C.aspectRatio;
+    out.desc.camera.aperture = C.aperture;
+    out.desc.camera.focus = C.focus;
+    out.desc.background.kind = RTC_BG_CONSTANT;   // the GPU path uses background.rgb only (gpu.cu:729-742)
+    putc3(out.desc.background.color, cfg.imageCfg.background.rgb);
+    return out.finish();
+}
+
+}  // namespace rtc_adapter

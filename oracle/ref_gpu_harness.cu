@@ -185,6 +185,27 @@ __global__ void refg_trace(DWorld* w, const float* rays, int64_t n, int depth, i
     tout[k] = h ? rec.t : INFINITY;
 }
 
+__global__ void refg_camera(rtc_camera cd, rtc_render_params p, int sqrt_spp, int i, int j, float* out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    perspective_camera cam;
+    cam.initialize(dv3(cd.look_from), dv3(cd.look_at), dv3(cd.up), p.width, cd.aspect, cd.vfov, cd.aperture, cd.focus,
+                   0.0f, 0.0f, 1.0f, sqrt_spp);
+    thrust::minstd_rand rng(p.seed + (uint32_t)(j * p.width + i));
+    thrust::uniform_real_distribution<float> uniform_dist(0.0f, 1.0f);
+    int q = 0;
+    for (int s_j = 0; s_j < sqrt_spp; ++s_j)
+        for (int s_i = 0; s_i < sqrt_spp; ++s_i, ++q) {
+            float uniform_random = uniform_dist(rng);
+            float u = (i + (s_i + uniform_random) / sqrt_spp) / float(p.width);
+            float v = (j + (s_j + uniform_random) / sqrt_spp) / float(p.height);
+            ray r = cam.get_ray(u, v, s_i, s_j, nullptr, rng);
+            float* o = out + 7 * q;
+            o[0] = r.origin().x; o[1] = r.origin().y; o[2] = r.origin().z;
+            o[3] = r.direction().x; o[4] = r.direction().y; o[5] = r.direction().z;
+            o[6] = r.time();
+        }
+}
+
 __global__ void refg_samplers(int which, uint32_t seed, int64_t n, float* out) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     thrust::minstd_rand rng(seed);
@@ -327,6 +348,18 @@ int refg_trace_closest(void* p, const float* rays, int64_t n, int depth, int max
     if (ok) ok = check(cudaMemcpy(prim, dp, n * 4, cudaMemcpyDeviceToHost), "copy") &&
                  check(cudaMemcpy(tout, dt, n * 4, cudaMemcpyDeviceToHost), "copy");
     cudaFree(dr); cudaFree(dp); cudaFree(dt);
+    return ok ? 0 : 1;
+}
+
+int refg_camera_rays(void* p, const rtc_render_params* prm, int i, int j, float* out) {
+    GpuScene* s = static_cast<GpuScene*>(p);
+    if (!s || !prm || !out) return 1;
+    int sq = (int)std::sqrt((double)prm->spp);
+    float* d = nullptr;
+    if (!check(cudaMalloc(&d, (size_t)sq * sq * 28), "malloc")) return 1;
+    refg_camera<<<1, 1>>>(s->cam, *prm, sq, i, j, d);
+    bool ok = check(cudaDeviceSynchronize(), "refg_camera") && check(cudaMemcpy(out, d, (size_t)sq * sq * 28, cudaMemcpyDeviceToHost), "copy");
+    cudaFree(d);
     return ok ? 0 : 1;
 }
 
