@@ -40,7 +40,8 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 from cortexraytracercuda_b200 import configs  # noqa: E402
-from cortexraytracercuda_b200.scene import DRAW_ORDER_DEVICE, DRAW_ORDER_HOST, MODE_CLEAN, MODE_COMPAT  # noqa: E402
+from cortexraytracercuda_b200.scene import (DRAW_ORDER_DEVICE, DRAW_ORDER_HOST, ENGINE_MEGAKERNEL,  # noqa: E402
+                                            ENGINE_WAVEFRONT, MODE_CLEAN, MODE_COMPAT)
 
 METRIC = "Mpaths/s"
 PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
@@ -200,10 +201,12 @@ def main():
     ap.add_argument("--config", default="spheres", choices=["spheres", "cornell", "meshes"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--mode", default="compat", choices=["compat", "clean"])
+    ap.add_argument("--engine", default="wavefront", choices=["wavefront", "megakernel"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-baseline-s", type=float, default=12.0)
     ap.add_argument("--ref-step-s", type=float, default=8.0)
     ap.add_argument("--small", action="store_true", help="quarter-size frame, 16 spp (profiling captures)")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling captures)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -235,6 +238,7 @@ def main():
         params.mode = MODE_CLEAN
     if args.small:
         params.width, params.height, params.spp = params.width // 4, params.height // 4, 16
+    params.engine = ENGINE_WAVEFRONT if args.engine == "wavefront" else ENGINE_MEGAKERNEL
     ds = DeviceScene(ctx, scene)
     info = ds.info()
     W, H = params.width, params.height
@@ -291,7 +295,7 @@ def main():
     import ctypes as C
     host_out = torch.empty((H, W, 4), dtype=torch.float32, pin_memory=True).numpy()
     e2e_ms = []
-    for k in range(args.warmup + args.steps):
+    for k in range(0 if args.no_e2e else args.warmup + args.steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         ds2 = DeviceScene(ctx, scene)
@@ -302,7 +306,7 @@ def main():
         dt = (time.perf_counter() - t0) * 1e3
         if k >= args.warmup:
             e2e_ms.append(dt)
-    e2e_total = float(np.sum(e2e_ms))
+    e2e_total = float(np.sum(e2e_ms)) if e2e_ms else float("nan")
     if world > 1:
         tt = torch.tensor([e2e_total], device="cuda")
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)

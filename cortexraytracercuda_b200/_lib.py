@@ -9,7 +9,7 @@ import ctypes as C
 import os
 from pathlib import Path
 
-from .scene import rtc_render_params, rtc_scene_desc, rtc_scene_info
+from .scene import rtc_render_params, rtc_render_stats, rtc_scene_desc, rtc_scene_info
 
 LIB_PATH = Path(__file__).resolve().parent / "librtc_b200.so"
 
@@ -28,6 +28,7 @@ PROTOTYPES = {
     "rtc_scene_get_info": (C.c_int, [_P, C.POINTER(rtc_scene_info)]),
     "rtc_render": (C.c_int, [_P, _P, C.POINTER(rtc_render_params), _P, _P]),
     "rtc_render_device": (C.c_int, [_P, _P, C.POINTER(rtc_render_params), _P, _P, _P, _P]),
+    "rtc_get_render_stats": (C.c_int, [_P, C.POINTER(rtc_render_stats)]),
     "rtc_trace_closest": (C.c_int, [_P, _P, _P, C.c_uint32, C.c_int32, C.c_int32, _P, _P]),
     "rtc_launchGPU": (C.c_int, [C.POINTER(rtc_scene_desc), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                 C.c_char_p, C.c_int]),

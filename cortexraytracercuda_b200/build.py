@@ -33,10 +33,13 @@ CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-Wall", "-Wno-u
 SOURCES = [
     ("render_compat.cu", "nvcc", ["--fmad=false"]),
     ("render_clean.cu", "nvcc", ["--fmad=true"]),
+    ("wavefront_compat.cu", "nvcc", ["--fmad=false"]),
+    ("wavefront_clean.cu", "nvcc", ["--fmad=true"]),
     ("rtc_api.cpp", "cxx", []),
     ("bvh_build.cpp", "cxx", []),
 ]
-HEADERS = ["rtc_dev.h", "rtc_math.cuh", "rtc_trace.cuh", "rtc_path.cuh", "rtc_kernels.h", "bvh_build.h"]
+HEADERS = ["rtc_dev.h", "rtc_math.cuh", "rtc_trace.cuh", "rtc_path.cuh", "rtc_wavefront.cuh", "rtc_kernels.h",
+           "bvh_build.h"]
 
 
 def _newer(target: Path, deps) -> bool:

@@ -12,6 +12,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <new>
@@ -55,6 +56,15 @@ struct rtc_context {
     size_t out_cap = 0;         // float4 elements
     uint8_t* d_rgb8 = nullptr;
     size_t rgb8_cap = 0;
+    int num_sms = 148;
+    // wavefront scratch: path slots (SoA) and the two slot queues
+    void* d_wf = nullptr;
+    uint32_t wf_cap = 0;
+    uint32_t* h_poll = nullptr;       // pinned: queue sizes read back between batches
+    cudaEvent_t poll_ev[2] = {nullptr, nullptr};
+    cudaEvent_t phase_ev[3] = {nullptr, nullptr, nullptr};   // render start, drain start, render end
+    rtc_render_stats last{};
+    bool last_timed = false;
     std::mutex mu;
 };
 
@@ -84,6 +94,7 @@ extern "C" rtc_status rtc_context_create(int device, rtc_context** out) {
     rtc_context* c = new (std::nothrow) rtc_context();
     if (!c) return fail(RTC_ERR_OOM, "host allocation failed");
     c->device = device;
+    c->num_sms = prop.multiProcessorCount;
     cudaError_t e1 = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     cudaError_t e2 = cudaMalloc(&c->d_status, sizeof(uint32_t));
     cudaError_t e3 = cudaMalloc(&c->d_counters, CNT_N * sizeof(unsigned long long));
@@ -104,6 +115,12 @@ extern "C" rtc_status rtc_context_destroy(rtc_context* c) {
     cudaFree(c->d_counters);
     cudaFree(c->d_out);
     cudaFree(c->d_rgb8);
+    cudaFree(c->d_wf);
+    if (c->h_poll) cudaFreeHost(c->h_poll);
+    for (cudaEvent_t& e : c->poll_ev)
+        if (e) cudaEventDestroy(e);
+    for (cudaEvent_t& e : c->phase_ev)
+        if (e) cudaEventDestroy(e);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return RTC_OK;
@@ -513,6 +530,8 @@ rtc_status check_params(const rtc_render_params* p) {
     if (p->mode != RTC_MODE_COMPAT && p->mode != RTC_MODE_CLEAN) return fail(RTC_ERR_INVALID_ARGUMENT, "unknown mode");
     if (p->draw_order != RTC_DRAW_ORDER_DEVICE && p->draw_order != RTC_DRAW_ORDER_HOST)
         return fail(RTC_ERR_INVALID_ARGUMENT, "unknown draw order");
+    if (p->engine < RTC_ENGINE_AUTO || p->engine > RTC_ENGINE_WAVEFRONT)
+        return fail(RTC_ERR_INVALID_ARGUMENT, "unknown engine");
     return RTC_OK;
 }
 
@@ -529,8 +548,133 @@ DevParams dev_params(const rtc_render_params* p) {
     return P;
 }
 
+// Bytes of wavefront scratch per path slot.
+constexpr size_t WF_SLOT_BYTES = 5 * sizeof(float4) + 2 * sizeof(uint4) + sizeof(float2) + 2 * sizeof(uint32_t);
+constexpr uint32_t WF_MAX_SLOTS = 1u << 22;   // 4,194,304 slots = 432 MiB of path state
+
+rtc_status ensure_wavefront(rtc_context* c, uint32_t slots, WfBuffers& B) {
+    if (c->wf_cap < slots) {
+        cudaFree(c->d_wf);
+        c->d_wf = nullptr;
+        c->wf_cap = 0;
+        size_t bytes = (size_t)slots * WF_SLOT_BYTES + 16 * 256;
+        RTC_CUDA(cudaMalloc(&c->d_wf, bytes));
+        c->wf_cap = slots;
+    }
+    if (!c->h_poll) {
+        RTC_CUDA(cudaMallocHost(&c->h_poll, 2 * sizeof(uint32_t)));
+        RTC_CUDA(cudaEventCreateWithFlags(&c->poll_ev[0], cudaEventDisableTiming));
+        RTC_CUDA(cudaEventCreateWithFlags(&c->poll_ev[1], cudaEventDisableTiming));
+        for (cudaEvent_t& e : c->phase_ev) RTC_CUDA(cudaEventCreate(&e));
+    }
+    const size_t n = c->wf_cap;
+    uint8_t* p = (uint8_t*)c->d_wf;
+    auto take = [&](size_t bytes) {
+        uint8_t* r = p;
+        p += (bytes + 255) & ~(size_t)255;
+        return (void*)r;
+    };
+    B.ray_o = (float4*)take(n * 16);
+    B.ray_d = (float4*)take(n * 16);
+    B.att = (float4*)take(n * 16);
+    B.acc = (float4*)take(n * 16);
+    B.psum = (float4*)take(n * 16);
+    B.meta = (uint4*)take(n * 16);
+    B.pcg = (uint4*)take(n * 16);
+    B.hit = (float2*)take(n * 8);
+    B.queue[0] = (uint32_t*)take(n * 4);
+    B.queue[1] = (uint32_t*)take(n * 4);
+    B.ctr = (uint32_t*)take(WF_CTR_N * 4);
+    B.slots = slots;
+    return RTC_OK;
+}
+
+// Wavefront engine: init, then batches of (extend, shade) iterations until the slot queue drains.
+// The queue size after each batch is copied to pinned memory; the batch after it is already queued
+// when the host looks, so the GPU never waits for the host.
+rtc_status launch_wavefront(rtc_context* c, const rtc_scene* s, const rtc_render_params* p, float4* d_out,
+                            unsigned long long* d_counters, cudaStream_t st) {
+    DevParams P = dev_params(p);
+    const bool clean = p->mode == RTC_MODE_CLEAN;
+    const uint32_t slots = (uint32_t)std::min<int64_t>(P.num_pixels, WF_MAX_SLOTS);
+    WfBuffers B;
+    rtc_status r = ensure_wavefront(c, slots, B);
+    if (r != RTC_OK) return r;
+    RTC_CUDA(cudaEventRecord(c->phase_ev[0], st));
+    RTC_CUDA(cudaMemsetAsync(B.ctr, 0, WF_CTR_N * sizeof(uint32_t), st));
+    const int grid = c->num_sms * 8;
+    const int init_grid = (int)std::min<int64_t>((slots + 127) / 128, (int64_t)c->num_sms * 16);
+    cudaError_t e = clean ? rtc_wf_launch_init_clean(s->dev, P, B, d_out, init_grid, st)
+                          : rtc_wf_launch_init_compat(p->draw_order, s->dev, P, B, d_out, init_grid, st);
+    if (e != cudaSuccess) return cuda_fail(e, "wavefront init");
+    const uint64_t nsamp = clean ? (uint64_t)P.spp : (uint64_t)P.sqrt_spp * P.sqrt_spp;
+    const uint64_t rounds = (uint64_t)((P.num_pixels + slots - 1) / slots);
+    const uint64_t max_iters = rounds * nsamp * (uint64_t)(P.max_depth + 1) + 64;
+    const int BATCH = 8;
+    // drain threshold: below this many queued slots the finish kernel takes over
+    uint32_t drain = (uint32_t)c->num_sms * 512u;
+    if (const char* ev = std::getenv("RTC_WF_DRAIN")) drain = (uint32_t)std::strtoul(ev, nullptr, 10);
+    // fused iteration (trace + shade in one launch) or split extend / shade kernels
+    bool fused = true;
+    if (const char* ev = std::getenv("RTC_WF_SPLIT")) fused = std::atoi(ev) == 0;
+    uint64_t it = 0;
+    int pending = -1;   // poll slot of the previous batch
+    bool finish = false;
+    for (int b = 0;; ++b) {
+        for (int k = 0; k < BATCH; ++k, ++it) {
+            const WfIter w = wf_iter(it);
+            if (fused) {
+                e = clean ? rtc_wf_launch_bounce_clean(s->dev, P, B, w, d_out, d_counters, c->d_status, grid, st)
+                          : rtc_wf_launch_bounce_compat(p->draw_order, s->dev, P, B, w, d_out, d_counters, c->d_status,
+                                                        grid, st);
+            } else {
+                e = rtc_wf_launch_extend(s->dev, P, B, w, d_counters, c->d_status, grid, st);
+                if (e == cudaSuccess)
+                    e = clean ? rtc_wf_launch_shade_clean(s->dev, P, B, w, d_out, d_counters, c->d_status, grid, st)
+                              : rtc_wf_launch_shade_compat(p->draw_order, s->dev, P, B, w, d_out, d_counters,
+                                                           c->d_status, grid, st);
+            }
+            if (e != cudaSuccess) return cuda_fail(e, "wavefront iteration");
+        }
+        const int slot = b & 1;
+        RTC_CUDA(cudaMemcpyAsync(c->h_poll + slot, B.ctr + wf_iter(it).cin, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                 st));
+        RTC_CUDA(cudaEventRecord(c->poll_ev[slot], st));
+        if (pending >= 0) {
+            RTC_CUDA(cudaEventSynchronize(c->poll_ev[pending]));
+            const uint32_t left = c->h_poll[pending];
+            if (left == 0) break;
+            if (left < drain) { finish = true; break; }
+        }
+        pending = slot;
+        if (it > max_iters) return fail(RTC_ERR_TIMEOUT, "wavefront did not drain within its iteration bound");
+    }
+    c->last = rtc_render_stats{};
+    c->last.engine = RTC_ENGINE_WAVEFRONT;
+    c->last.iterations = (uint32_t)it;
+    c->last.launches = (uint32_t)(1 + (fused ? 1 : 2) * it + (finish ? 1 : 0));
+    c->last.drained_slots = finish ? c->h_poll[pending] : 0u;
+    RTC_CUDA(cudaEventRecord(c->phase_ev[1], st));
+    if (finish) {
+        const WfIter w = wf_iter(it);
+        const int fgrid = (int)std::max<uint32_t>(1u, (drain + 127u) / 128u);
+        e = clean ? rtc_wf_launch_finish_clean(s->dev, P, B, w, d_out, d_counters, c->d_status, fgrid, st)
+                  : rtc_wf_launch_finish_compat(p->draw_order, s->dev, P, B, w, d_out, d_counters, c->d_status, fgrid,
+                                                st);
+        if (e != cudaSuccess) return cuda_fail(e, "wavefront finish");
+    }
+    RTC_CUDA(cudaEventRecord(c->phase_ev[2], st));
+    c->last_timed = true;
+    return RTC_OK;
+}
+
 rtc_status launch(rtc_context* c, const rtc_scene* s, const rtc_render_params* p, float4* d_out,
                   unsigned long long* d_counters, cudaStream_t st) {
+    if (p->engine != RTC_ENGINE_MEGAKERNEL) return launch_wavefront(c, s, p, d_out, d_counters, st);
+    c->last = rtc_render_stats{};
+    c->last.engine = RTC_ENGINE_MEGAKERNEL;
+    c->last.launches = 1;
+    c->last_timed = false;
     DevParams P = dev_params(p);
     cudaError_t e = p->mode == RTC_MODE_COMPAT
                         ? rtc_launch_render_compat(s->dev, P, d_out, d_counters, c->d_status, p->block_size, st)
@@ -600,6 +744,17 @@ extern "C" rtc_status rtc_render_device(rtc_context* c, const rtc_scene* s, cons
     r = launch(c, s, p, (float4*)d_radiance_sum, d_counters, st);
     if (r != RTC_OK) return r;
     if (d_rgb8) RTC_CUDA(rtc_launch_quantize((const float4*)d_radiance_sum, d_rgb8, p->width, p->height, p->spp, st));
+    return RTC_OK;
+}
+
+extern "C" rtc_status rtc_get_render_stats(rtc_context* c, rtc_render_stats* out) {
+    if (!c || !out) return fail(RTC_ERR_INVALID_ARGUMENT, "null argument");
+    *out = c->last;
+    if (c->last_timed) {
+        RTC_CUDA(cudaEventSynchronize(c->phase_ev[2]));
+        RTC_CUDA(cudaEventElapsedTime(&out->bulk_ms, c->phase_ev[0], c->phase_ev[1]));
+        RTC_CUDA(cudaEventElapsedTime(&out->drain_ms, c->phase_ev[1], c->phase_ev[2]));
+    }
     return RTC_OK;
 }
 
@@ -715,7 +870,8 @@ extern "C" rtc_status rtc_launchGPU(const rtc_scene_desc* scene, int width, int 
     rtc_scene* s = nullptr;
     r = rtc_scene_create(c, scene, &s);
     if (r == RTC_OK) {
-        rtc_render_params p{width, height, spp, max_depth, 2580u, RTC_MODE_COMPAT, RTC_DRAW_ORDER_DEVICE, 0};
+        rtc_render_params p{width, height, spp, max_depth, 2580u, RTC_MODE_COMPAT, RTC_DRAW_ORDER_DEVICE, 0,
+                            RTC_ENGINE_AUTO};
         std::vector<uint8_t> img((size_t)std::max(0, width) * std::max(0, height) * 3);
         if (!quiet_mode) std::printf("[INFO] Rendering %dx%d %d samples > %s\n", width, height, spp, filepath);
         r = rtc_render(c, s, &p, nullptr, img.data());

@@ -97,6 +97,36 @@ struct DevParams {
     int64_t num_pixels;
 };
 
+// Wavefront path slots (SoA, one slot = one pixel in flight) and the two slot queues.
+struct WfBuffers {
+    float4* ray_o;     // origin.xyz, time
+    float4* ray_d;     // direction.xyz
+    float4* att;       // path attenuation rgb
+    float4* acc;       // radiance of the current sample rgb
+    float4* psum;      // pixel sum rgb (pixel_color)
+    uint4* meta;       // x pixel (0xffffffff idle), y sample index, z minstd state, w depth left
+    uint4* pcg;        // clean mode: PCG32 state (lo, hi) and increment (lo, hi)
+    float2* hit;       // t, item bits (0xffffffff = miss)
+    uint32_t* queue[2];
+    uint32_t* ctr;     // [0..2] queue sizes (rotating), [3] next pixel to fetch
+    uint32_t slots;
+};
+
+// Iteration k reads queue (k & 1) with size ctr[k % 3], appends to queue ((k+1) & 1) counted in
+// ctr[(k+1) % 3] and clears ctr[(k+2) % 3], which iteration k+1 appends to.
+enum WfCtr { WF_NEXT_PIXEL = 3, WF_CTR_N = 4 };
+struct WfIter {
+    int qin, cin, cout, czero;
+};
+inline __host__ __device__ WfIter wf_iter(uint64_t k) {
+    WfIter w;
+    w.qin = (int)(k & 1u);
+    w.cin = (int)(k % 3u);
+    w.cout = (int)((k + 1u) % 3u);
+    w.czero = (int)((k + 2u) % 3u);
+    return w;
+}
+
 // Counters (unsigned long long on device).
 enum CounterIdx { CNT_RAYS = 0, CNT_PATHS = 1, CNT_NODES = 2, CNT_PRIMS = 3, CNT_N = 4 };
 

@@ -126,9 +126,131 @@ struct PathCounters {
     uint32_t rays, nodes, prims;
 };
 
-// One camera sample: camera::ray_color (camera.cuh:149-264).  Returns the radiance of the sample.
+// One bounce of camera::ray_color (camera.cuh:153-227) AFTER the closest-hit query of the current ray:
+// `hit` tells whether world.hit found something at (t, item).  Updates the path's running radiance
+// `result`, its attenuation `att` and its ray; returns false when the path ends at this bounce.
 // All additions of the reference are kept, including the zero emission of non-emitting materials,
-// so NaN/Inf propagate exactly as in the reference.
+// so NaN/Inf propagate exactly as in the reference.  The megakernel and the wavefront shade kernel
+// both call this, so the two engines are the same arithmetic.
+template <bool CLEAN, int ORDER, class R>
+__device__ __forceinline__ bool shade_bounce(const DevScene& S, Ray& r, bool hit, float t, uint32_t item, bool hide,
+                                             RGB& result, RGB& att, R& rng, PathCounters& pc, TraceStats& st,
+                                             uint32_t& status) {
+    if (!hit) {
+        RGB bg = background(S, r.d);
+        result.r += att.r * bg.r;
+        result.g += att.g * bg.g;
+        result.b += att.b * bg.b;
+        return false;
+    }
+    Hit h;
+    finalize_hit(S, item, t, r.o, r.d, h);
+    if ((uint32_t)h.mat >= S.num_materials) { status |= STATUS_BAD_MATERIAL; return false; }
+    int4 mi = __ldg(S.mat_i + h.mat);
+    float4 mf = __ldg(S.mat_f + h.mat);
+    // emitted (diffuse_light.cuh:45-67; material::emitted returns (0,0,0) otherwise)
+    RGB em = rgb(0.f, 0.f, 0.f);
+    bool em_alpha0 = false;
+    if (mi.x == 3) {
+        if (mf.w != 0.0f && !h.front) {
+            em_alpha0 = true;   // RGBA(0,0,0,0): back face of a one-sided light
+        } else {
+            RGB tv = texture_value(S, mi.y, h.u, h.v, h.p, status);
+            em = rgb(tv.r * mf.z, tv.g * mf.z, tv.b * mf.z);
+        }
+    }
+    if (em_alpha0) {
+        // "invisible" re-hit from just behind the light (camera.cuh:177-183); rec is replaced only
+        // when the re-hit finds something, and `emitted` is not recomputed.
+        float t2;
+        uint32_t item2;
+        pc.rays++;
+        if (closest_hit(S, r.o, r.d, h.t + 0.001f, 3.402823466e+38f, hide, t2, item2, st, status)) {
+            finalize_hit(S, item2, t2, r.o, r.d, h);
+            if ((uint32_t)h.mat >= S.num_materials) { status |= STATUS_BAD_MATERIAL; return false; }
+            mi = __ldg(S.mat_i + h.mat);
+            mf = __ldg(S.mat_f + h.mat);
+        }
+    }
+    result.r += att.r * em.r;
+    result.g += att.g * em.g;
+    result.b += att.b * em.b;
+    if (mi.x == 3) return false;   // diffuse_light::scatter -> material::scatter returns false
+
+    if (mi.x == 1) {
+        // metal::scatter (metal.cuh:57-64)
+        RGB a = texture_value(S, mi.y, h.u, h.v, h.p, status);
+        V3 refl = reflect(unit(r.d), h.n);
+        V3 rs = random_in_unit_sphere<ORDER>(rng);
+        r.o = h.p;
+        r.d = add(refl, mul(mf.x, rs));
+        att.r *= a.r;
+        att.g *= a.g;
+        att.b *= a.b;
+        return true;
+    }
+    if (mi.x == 2) {
+        // dielectric::scatter (dielectric.cuh:32-52) with Schlick (dielectric.cuh:57-63)
+        float ratio = h.front ? (1.0f / mf.y) : mf.y;
+        V3 ud = unit(r.d);
+        float ct = dot(neg(ud), h.n);
+        float cos_theta = ct < 1.0f ? ct : 1.0f;
+        float sin_theta = sqrtf(1.0f - cos_theta * cos_theta);
+        bool cannot_refract = ratio * sin_theta > 1.0f;
+        bool do_reflect = cannot_refract;
+        if (!cannot_refract) {
+            float r0 = (1.0f - ratio) / (1.0f + ratio);
+            r0 = r0 * r0;
+            // (float)pow(1 - cosine, 5): the x^5 product in double agrees with glibc's double pow
+            double x = (double)(1.0f - cos_theta);
+            double x2 = x * x;
+            float p5 = (float)(x2 * x2 * x);
+            float refl = r0 + (1.0f - r0) * p5;
+            do_reflect = refl > rng.uniform();
+        }
+        r.o = h.p;
+        r.d = do_reflect ? reflect(ud, h.n) : refract(ud, h.n, ratio);
+        return true;   // attenuation (1,1,1)
+    }
+    // lambertian::scatter (lambertian.cuh:63-131): attenuation from the texture, cosine_pdf(normal)
+    RGB a = texture_value(S, mi.y, h.u, h.v, h.p, status);
+    Onb b = build_from_w(h.n);
+    V3 dir;
+    float pdf_val, spdf;
+    if (!CLEAN || S.num_lights > 0) {
+        // mixture_pdf(hittable_pdf(lights, p), cosine_pdf), proportion 0.5 (mixture_pdf.cuh:28-47)
+        if (rng.uniform() < 0.5f) {
+            if (S.num_lights == 0) {
+                dir = v3(0.f, 0.f, 0.f);   // hittable_list::random on an empty list
+            } else {
+                if (S.num_lights > 1) (void)rng.uniform();   // get_int(rng, 0, n-1) == 0, one draw
+                dir = light_random<ORDER>(S, 0, h.p, rng);
+            }
+        } else {
+            dir = onb_local(b, random_cosine_direction<CLEAN>(rng));
+        }
+        float cosv = dot(unit(dir), b.w) / 3.14159265358979323846f;
+        float cpdf = 0.0f > cosv ? 0.0f : cosv;   // ffmax(0, x) keeps NaN
+        pdf_val = 0.5f * lights_pdf_value(S, h.p, dir) + (1.0f - 0.5f) * cpdf;
+    } else {
+        dir = onb_local(b, random_cosine_direction<CLEAN>(rng));
+        float cosv = dot(unit(dir), b.w) / 3.14159265358979323846f;
+        pdf_val = 0.0f > cosv ? 0.0f : cosv;
+    }
+    // lambertian::scattering_pdf (lambertian.cuh:139-143)
+    float cos_theta = dot(h.n, unit(dir));
+    spdf = cos_theta < 0.0f ? 0.0f : cos_theta / 3.14159265358979323846f;
+    // current_attenuation *= srec.attenuation * scattering_pdf / pdf_val, where color / t = (1/t) * color
+    float rcp = 1.0f / pdf_val;
+    att.r *= rcp * (a.r * spdf);
+    att.g *= rcp * (a.g * spdf);
+    att.b *= rcp * (a.b * spdf);
+    r.o = h.p;
+    r.d = dir;
+    return true;
+}
+
+// One camera sample: camera::ray_color (camera.cuh:149-264).  Returns the radiance of the sample.
 template <bool CLEAN, int ORDER, class R>
 __device__ __forceinline__ RGB trace_sample(const DevScene& S, Ray r, int max_depth, R& rng, PathCounters& pc,
                                             uint32_t& status) {
@@ -140,122 +262,8 @@ __device__ __forceinline__ RGB trace_sample(const DevScene& S, Ray r, int max_de
         float t;
         uint32_t item;
         pc.rays++;
-        if (!closest_hit(S, r.o, r.d, 0.00001f, 3.402823466e+38f, hide, t, item, st, status)) {
-            RGB bg = background(S, r.d);
-            result.r += att.r * bg.r;
-            result.g += att.g * bg.g;
-            result.b += att.b * bg.b;
-            break;
-        }
-        Hit h;
-        finalize_hit(S, item, t, r.o, r.d, h);
-        if ((uint32_t)h.mat >= S.num_materials) { status |= STATUS_BAD_MATERIAL; break; }
-        int4 mi = __ldg(S.mat_i + h.mat);
-        float4 mf = __ldg(S.mat_f + h.mat);
-        // emitted (diffuse_light.cuh:45-67; material::emitted returns (0,0,0) otherwise)
-        RGB em = rgb(0.f, 0.f, 0.f);
-        bool em_alpha0 = false;
-        if (mi.x == 3) {
-            if (mf.w != 0.0f && !h.front) {
-                em_alpha0 = true;   // RGBA(0,0,0,0): back face of a one-sided light
-            } else {
-                RGB tv = texture_value(S, mi.y, h.u, h.v, h.p, status);
-                em = rgb(tv.r * mf.z, tv.g * mf.z, tv.b * mf.z);
-            }
-        }
-        if (em_alpha0) {
-            // "invisible" re-hit from just behind the light (camera.cuh:177-183); rec is replaced only
-            // when the re-hit finds something, and `emitted` is not recomputed.
-            float t2;
-            uint32_t item2;
-            pc.rays++;
-            if (closest_hit(S, r.o, r.d, h.t + 0.001f, 3.402823466e+38f, hide, t2, item2, st, status)) {
-                finalize_hit(S, item2, t2, r.o, r.d, h);
-                if ((uint32_t)h.mat >= S.num_materials) { status |= STATUS_BAD_MATERIAL; break; }
-                mi = __ldg(S.mat_i + h.mat);
-                mf = __ldg(S.mat_f + h.mat);
-            }
-        }
-        if (mi.x == 3) {   // diffuse_light::scatter -> material::scatter returns false
-            result.r += att.r * em.r;
-            result.g += att.g * em.g;
-            result.b += att.b * em.b;
-            break;
-        }
-        result.r += att.r * em.r;
-        result.g += att.g * em.g;
-        result.b += att.b * em.b;
-
-        if (mi.x == 1) {
-            // metal::scatter (metal.cuh:57-64)
-            RGB a = texture_value(S, mi.y, h.u, h.v, h.p, status);
-            V3 refl = reflect(unit(r.d), h.n);
-            V3 rs = random_in_unit_sphere<ORDER>(rng);
-            r.o = h.p;
-            r.d = add(refl, mul(mf.x, rs));
-            att.r *= a.r;
-            att.g *= a.g;
-            att.b *= a.b;
-            continue;
-        }
-        if (mi.x == 2) {
-            // dielectric::scatter (dielectric.cuh:32-52) with Schlick (dielectric.cuh:57-63)
-            float ratio = h.front ? (1.0f / mf.y) : mf.y;
-            V3 ud = unit(r.d);
-            float ct = dot(neg(ud), h.n);
-            float cos_theta = ct < 1.0f ? ct : 1.0f;
-            float sin_theta = sqrtf(1.0f - cos_theta * cos_theta);
-            bool cannot_refract = ratio * sin_theta > 1.0f;
-            bool do_reflect = cannot_refract;
-            if (!cannot_refract) {
-                float r0 = (1.0f - ratio) / (1.0f + ratio);
-                r0 = r0 * r0;
-                // (float)pow(1 - cosine, 5): the x^5 product in double agrees with glibc's double pow
-                double x = (double)(1.0f - cos_theta);
-                double x2 = x * x;
-                float p5 = (float)(x2 * x2 * x);
-                float refl = r0 + (1.0f - r0) * p5;
-                do_reflect = refl > rng.uniform();
-            }
-            r.o = h.p;
-            r.d = do_reflect ? reflect(ud, h.n) : refract(ud, h.n, ratio);
-            continue;   // attenuation (1,1,1)
-        }
-        // lambertian::scatter (lambertian.cuh:63-131): attenuation from the texture, cosine_pdf(normal)
-        RGB a = texture_value(S, mi.y, h.u, h.v, h.p, status);
-        Onb b = build_from_w(h.n);
-        V3 dir;
-        float pdf_val, spdf;
-        if (!CLEAN || S.num_lights > 0) {
-            // mixture_pdf(hittable_pdf(lights, p), cosine_pdf), proportion 0.5 (mixture_pdf.cuh:28-47)
-            if (rng.uniform() < 0.5f) {
-                if (S.num_lights == 0) {
-                    dir = v3(0.f, 0.f, 0.f);   // hittable_list::random on an empty list
-                } else {
-                    if (S.num_lights > 1) (void)rng.uniform();   // get_int(rng, 0, n-1) == 0, one draw
-                    dir = light_random<ORDER>(S, 0, h.p, rng);
-                }
-            } else {
-                dir = onb_local(b, random_cosine_direction<CLEAN>(rng));
-            }
-            float cosv = dot(unit(dir), b.w) / 3.14159265358979323846f;
-            float cpdf = 0.0f > cosv ? 0.0f : cosv;   // ffmax(0, x) keeps NaN
-            pdf_val = 0.5f * lights_pdf_value(S, h.p, dir) + (1.0f - 0.5f) * cpdf;
-        } else {
-            dir = onb_local(b, random_cosine_direction<CLEAN>(rng));
-            float cosv = dot(unit(dir), b.w) / 3.14159265358979323846f;
-            pdf_val = 0.0f > cosv ? 0.0f : cosv;
-        }
-        // lambertian::scattering_pdf (lambertian.cuh:139-143)
-        float cos_theta = dot(h.n, unit(dir));
-        spdf = cos_theta < 0.0f ? 0.0f : cos_theta / 3.14159265358979323846f;
-        // current_attenuation *= srec.attenuation * scattering_pdf / pdf_val, where color / t = (1/t) * color
-        float rcp = 1.0f / pdf_val;
-        att.r *= rcp * (a.r * spdf);
-        att.g *= rcp * (a.g * spdf);
-        att.b *= rcp * (a.b * spdf);
-        r.o = h.p;
-        r.d = dir;
+        bool hit = closest_hit(S, r.o, r.d, 0.00001f, 3.402823466e+38f, hide, t, item, st, status);
+        if (!shade_bounce<CLEAN, ORDER>(S, r, hit, t, item, hide, result, att, rng, pc, st, status)) break;
     }
     pc.nodes += st.nodes;
     pc.prims += st.prims;

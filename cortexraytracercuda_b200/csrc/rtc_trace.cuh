@@ -67,6 +67,23 @@ __device__ __forceinline__ uint64_t mix64(uint64_t z) {   // splitmix64 finalise
 }
 
 // ------------------------------------------------------------------------------------------------
+// scene loads: read-only, kept in L1 with the evict_last priority so that streaming path state
+// (loaded with evict-first __ldcs in the wavefront kernels) does not push the BVH out of L1
+// ------------------------------------------------------------------------------------------------
+__device__ __forceinline__ float4 ld_scene(const float4* p) {
+    float4 r;
+    asm("ld.global.nc.L1::evict_last.v4.f32 {%0, %1, %2, %3}, [%4];"
+        : "=f"(r.x), "=f"(r.y), "=f"(r.z), "=f"(r.w)
+        : "l"(p));
+    return r;
+}
+__device__ __forceinline__ uint32_t ld_scene(const uint32_t* p) {
+    uint32_t r;
+    asm("ld.global.nc.L1::evict_last.u32 %0, [%1];" : "=r"(r) : "l"(p));
+    return r;
+}
+
+// ------------------------------------------------------------------------------------------------
 // hit record (the fields of hit_record the render path reads, misc/hit_record.cuh:8-38)
 // ------------------------------------------------------------------------------------------------
 struct Hit {
@@ -190,7 +207,7 @@ __device__ __forceinline__ void test_leaf(const DevScene& S, int32_t child, V3 o
     uint32_t first = enc >> LEAF_COUNT_BITS, cnt = enc & MAX_LEAF;
     if (first + cnt > S.num_items) { status |= STATUS_BAD_ITEM; return; }
     for (uint32_t k = 0; k < cnt; ++k) {
-        uint32_t it = __ldg(S.items + first + k);
+        uint32_t it = ld_scene(S.items + first + k);
         uint32_t kind = it >> 30, idx = it & 0x3fffffffu;
         float t;
         st.prims++;
@@ -199,11 +216,11 @@ __device__ __forceinline__ void test_leaf(const DevScene& S, int32_t child, V3 o
             if (idx >= S.num_tri) { status |= STATUS_BAD_ITEM; break; }
             const float4* p = S.tri + 3 * (size_t)idx;
             float bu, bv;
-            if (tri_t(__ldg(p), __ldg(p + 1), __ldg(p + 2), o, d, tmin, best_t, t, bu, bv)) { best_t = t; best_item = it; }
+            if (tri_t(ld_scene(p), ld_scene(p + 1), ld_scene(p + 2), o, d, tmin, best_t, t, bu, bv)) { best_t = t; best_item = it; }
         } break;
         case ITEM_SPHERE: {
             if (idx >= S.num_sph) { status |= STATUS_BAD_ITEM; break; }
-            if (sphere_t(__ldg(S.sph + idx), o, d, tmin, best_t, t)) { best_t = t; best_item = it; }
+            if (sphere_t(ld_scene(S.sph + idx), o, d, tmin, best_t, t)) { best_t = t; best_item = it; }
         } break;
         case ITEM_QUAD: {
             if (idx >= S.num_quad) { status |= STATUS_BAD_ITEM; break; }
@@ -242,7 +259,7 @@ __device__ __forceinline__ bool closest_hit(const DevScene& S, V3 o, V3 d, float
     int32_t node = 0;
     for (;;) {
         const float4* np = S.nodes + 4 * (size_t)node;
-        float4 n0 = __ldg(np), n1 = __ldg(np + 1), n2 = __ldg(np + 2), n3 = __ldg(np + 3);
+        float4 n0 = ld_scene(np), n1 = ld_scene(np + 1), n2 = ld_scene(np + 2), n3 = ld_scene(np + 3);
         st.nodes++;
         int32_t cl = __float_as_int(n3.x), cr = __float_as_int(n3.y);
         float tl, tr;

@@ -1,0 +1,375 @@
+// rtc_wavefront.cuh - wavefront form of the path loop: init / extend / shade kernels over compacted
+// slot queues.
+//
+// A slot holds one pixel in flight.  Its samples run in order on the slot (the compat stream is one
+// thrust::minstd_rand per pixel, consumed by all samples, core/src/gpu.cu:770-790), so the radiance
+// is bit-identical to the megakernel's.  What changes is the shape of the work:
+//   extend  every queued slot runs only the closest-hit traversal of its current ray;
+//   shade   every queued slot runs one bounce of camera::ray_color (shade_bounce); a finished sample
+//           adds into the pixel sum and the slot regenerates the next camera sample, a finished pixel
+//           is written out and the slot fetches the next pixel from a global counter;
+// and survivors are compacted into the next queue with one atomic per warp (ballot + popc + shfl).
+// Queue counters live on the device; the host launches batches of iterations and polls the count.
+#pragma once
+
+#include "rtc_path.cuh"
+
+namespace rtc {
+
+// Appends `slot` to queue `q` when `pred`; every active lane of the warp must call it together.
+__device__ __forceinline__ void wf_push(uint32_t* q, uint32_t* cnt, uint32_t slot, bool pred) {
+    const unsigned act = __activemask();
+    const unsigned m = __ballot_sync(act, pred);
+    if (m == 0u) return;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(m) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(cnt, (uint32_t)__popc(m));
+    base = __shfl_sync(act, base, leader);
+    if (pred) q[base + (uint32_t)__popc(m & ((1u << lane) - 1u))] = slot;
+}
+
+template <bool CLEAN>
+struct WfRngT {
+    using type = Minstd;
+};
+template <>
+struct WfRngT<true> {
+    using type = Pcg32;
+};
+template <bool CLEAN>
+using WfRng = typename WfRngT<CLEAN>::type;
+
+__device__ __forceinline__ void pcg_load(Pcg32& r, uint4 v) {
+    r.state = ((uint64_t)v.y << 32) | v.x;
+    r.inc = ((uint64_t)v.w << 32) | v.z;
+}
+__device__ __forceinline__ uint4 pcg_store(const Pcg32& r) {
+    return make_uint4((uint32_t)r.state, (uint32_t)(r.state >> 32), (uint32_t)r.inc, (uint32_t)(r.inc >> 32));
+}
+
+// Starts sample `s` of pixel `pixel`: jitter and camera ray (perspective_camera::get_ray).
+// Compat: one shared stream per pixel, samples in stratum order (gpu.cu:776-786).
+// Clean: a PCG32 stream per (pixel, sample).
+template <bool CLEAN, int ORDER>
+__device__ __forceinline__ void wf_start_sample(const DevScene& S, const DevParams& P, WfRng<CLEAN>& rng,
+                                                uint32_t pixel, uint32_t s, Ray& r) {
+    const int i = (int)(pixel % (uint32_t)P.width);
+    const int j = (int)(pixel / (uint32_t)P.width);
+    if constexpr (CLEAN) {
+        rng.seed(mix64(((uint64_t)P.seed << 32) ^ (uint64_t)pixel), (uint64_t)s);
+        float ju = rng.uniform(), jv = rng.uniform();
+        float u = ((float)i + ju) / (float)P.width;
+        float v = ((float)j + jv) / (float)P.height;
+        r = camera_ray<0>(S.cam, u, v, rng);
+    } else {
+        const int sq = P.sqrt_spp;
+        const int s_j = (int)s / sq, s_i = (int)s % sq;
+        float ur = rng.uniform();
+        float u = ((float)i + ((float)s_i + ur) / (float)sq) / (float)P.width;
+        float v = ((float)j + ((float)s_j + ur) / (float)sq) / (float)P.height;
+        r = camera_ray<ORDER>(S.cam, u, v, rng);
+    }
+}
+
+template <bool CLEAN>
+__device__ __forceinline__ void rng_save(const WfBuffers& B, uint32_t slot, const WfRng<CLEAN>& rng, uint4& m) {
+    if constexpr (CLEAN) B.pcg[slot] = pcg_store(rng);
+    else m.z = rng.x;
+}
+
+__device__ __forceinline__ uint32_t wf_samples(const DevParams& P, bool clean) {
+    return clean ? (uint32_t)P.spp : (uint32_t)(P.sqrt_spp * P.sqrt_spp);
+}
+
+// Fetches the next pixel for a slot and starts its first sample; returns false when none is left.
+template <bool CLEAN, int ORDER>
+__device__ __forceinline__ bool wf_fetch_pixel(const DevScene& S, const DevParams& P, const WfBuffers& B,
+                                               uint32_t slot, float4* out, uint32_t& status) {
+    uint32_t pixel = atomicAdd(B.ctr + WF_NEXT_PIXEL, 1u);
+    if ((int64_t)pixel >= P.num_pixels) {
+        B.meta[slot] = make_uint4(0xffffffffu, 0u, 0u, 0u);
+        return false;
+    }
+    WfRng<CLEAN> rng;
+    if constexpr (!CLEAN) rng.seed(P.seed + pixel);
+    Ray r;
+    wf_start_sample<CLEAN, ORDER>(S, P, rng, pixel, 0u, r);
+    B.ray_o[slot] = make_float4(r.o.x, r.o.y, r.o.z, r.time);
+    B.ray_d[slot] = make_float4(r.d.x, r.d.y, r.d.z, 0.f);
+    B.att[slot] = make_float4(1.f, 1.f, 1.f, 0.f);
+    B.acc[slot] = make_float4(0.f, 0.f, 0.f, 0.f);
+    B.psum[slot] = make_float4(0.f, 0.f, 0.f, 0.f);
+    uint4 m = make_uint4(pixel, 0u, 0u, (uint32_t)P.max_depth);
+    rng_save<CLEAN>(B, slot, rng, m);
+    B.meta[slot] = m;
+    (void)out;
+    (void)status;
+    return true;
+}
+
+template <bool CLEAN, int ORDER>
+__global__ void __launch_bounds__(128) wf_init(DevScene S, DevParams P, WfBuffers B, float4* out) {
+    uint32_t status = 0;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < B.slots; base += stride) {
+        const uint32_t slot = base + threadIdx.x;
+        bool live = false;
+        if (slot < B.slots) live = wf_fetch_pixel<CLEAN, ORDER>(S, P, B, slot, out, status);
+        wf_push(B.queue[0], B.ctr + 0, slot, live);
+    }
+}
+
+template <bool COUNT>
+__global__ void __launch_bounds__(128) wf_extend(DevScene S, DevParams P, WfBuffers B, WfIter w,
+                                                 unsigned long long* counters, uint32_t* status_word) {
+    const uint32_t n = B.ctr[w.cin];
+    if (blockIdx.x == 0 && threadIdx.x == 0) B.ctr[w.czero] = 0u;
+    const uint32_t* q = B.queue[w.qin];
+    TraceStats st{0, 0};
+    uint32_t status = 0, rays = 0;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
+        const uint32_t slot = __ldcs(q + k);
+        const float4 o = __ldcs(B.ray_o + slot), d = __ldcs(B.ray_d + slot);
+        const uint32_t depth = __ldcs(&B.meta[slot].w);
+        float t;
+        uint32_t item;
+        bool h = closest_hit(S, v3(o), v3(d), 0.00001f, 3.402823466e+38f, depth == (uint32_t)P.max_depth, t, item,
+                             st, status);
+        B.hit[slot] = make_float2(t, __uint_as_float(h ? item : 0xffffffffu));
+        ++rays;
+    }
+    if (COUNT && counters) {
+        unsigned long long r = rays, nn = st.nodes, pp = st.prims;
+        for (int off = 16; off > 0; off >>= 1) {
+            r += __shfl_down_sync(0xffffffffu, r, off);
+            nn += __shfl_down_sync(0xffffffffu, nn, off);
+            pp += __shfl_down_sync(0xffffffffu, pp, off);
+        }
+        if ((threadIdx.x & 31) == 0) {
+            atomicAdd(counters + CNT_RAYS, r);
+            atomicAdd(counters + CNT_NODES, nn);
+            atomicAdd(counters + CNT_PRIMS, pp);
+        }
+    }
+    if (status) atomicOr(status_word, status);
+}
+
+// One shade step of a slot whose current ray has been traced: shade_bounce, then the slot's
+// bookkeeping (next bounce / next sample / next pixel).  Returns true while the slot has a ray to trace.
+template <bool CLEAN, int ORDER>
+__device__ __forceinline__ bool wf_step(const DevScene& S, const DevParams& P, const WfBuffers& B, uint32_t slot,
+                                        float t, uint32_t item, float4* __restrict__ out, PathCounters& pc,
+                                        TraceStats& st, uint32_t& paths, uint32_t& status) {
+    uint4 m = __ldcs(B.meta + slot);
+    const float4 o = __ldcs(B.ray_o + slot), d = __ldcs(B.ray_d + slot), a4 = __ldcs(B.att + slot),
+                 c4 = __ldcs(B.acc + slot);
+    Ray r;
+    r.o = v3(o);
+    r.d = v3(d);
+    r.time = o.w;
+    RGB att = rgb(a4.x, a4.y, a4.z), acc = rgb(c4.x, c4.y, c4.z);
+    WfRng<CLEAN> rng;
+    if constexpr (CLEAN) pcg_load(rng, __ldcs(B.pcg + slot));
+    else rng.x = m.z;
+    const bool hide = m.w == (uint32_t)P.max_depth;
+    const bool cont = shade_bounce<CLEAN, ORDER>(S, r, item != 0xffffffffu, t, item, hide, acc, att, rng, pc, st, status);
+    uint32_t depth = m.w;
+    if (cont) --depth;
+    if (cont && depth > 0u) {
+        // the path continues: next bounce
+        B.ray_o[slot] = make_float4(r.o.x, r.o.y, r.o.z, r.time);
+        B.ray_d[slot] = make_float4(r.d.x, r.d.y, r.d.z, 0.f);
+        B.att[slot] = make_float4(att.r, att.g, att.b, 0.f);
+        B.acc[slot] = make_float4(acc.r, acc.g, acc.b, 0.f);
+        m.w = depth;
+        rng_save<CLEAN>(B, slot, rng, m);
+        B.meta[slot] = m;
+        return true;
+    }
+    // the sample is done: pixel_color += ray_color(...) (gpu.cu:787)
+    ++paths;
+    float4 ps = __ldcs(B.psum + slot);
+    if (!CLEAN || (isfinite(acc.r) && isfinite(acc.g) && isfinite(acc.b))) {
+        ps.x += acc.r;
+        ps.y += acc.g;
+        ps.z += acc.b;
+    }
+    const uint32_t s = m.y + 1u;
+    if (s < wf_samples(P, CLEAN)) {
+        // regenerate: the pixel's next sample on the same slot
+        Ray nr;
+        wf_start_sample<CLEAN, ORDER>(S, P, rng, m.x, s, nr);
+        B.ray_o[slot] = make_float4(nr.o.x, nr.o.y, nr.o.z, nr.time);
+        B.ray_d[slot] = make_float4(nr.d.x, nr.d.y, nr.d.z, 0.f);
+        B.att[slot] = make_float4(1.f, 1.f, 1.f, 0.f);
+        B.acc[slot] = make_float4(0.f, 0.f, 0.f, 0.f);
+        B.psum[slot] = ps;
+        m.y = s;
+        m.w = (uint32_t)P.max_depth;
+        rng_save<CLEAN>(B, slot, rng, m);
+        B.meta[slot] = m;
+        return true;
+    }
+    // the pixel is done: write it and take the next pixel
+    out[m.x] = make_float4(ps.x, ps.y, ps.z, 1.0f);
+    return wf_fetch_pixel<CLEAN, ORDER>(S, P, B, slot, out, status);
+}
+
+template <bool COUNT>
+__device__ __forceinline__ void wf_flush(unsigned long long* counters, uint32_t rays, uint32_t paths, const TraceStats& st) {
+    if (!COUNT || !counters) return;
+    unsigned long long r = rays, p = paths, nn = st.nodes, pp = st.prims;
+    for (int off = 16; off > 0; off >>= 1) {
+        r += __shfl_down_sync(0xffffffffu, r, off);
+        p += __shfl_down_sync(0xffffffffu, p, off);
+        nn += __shfl_down_sync(0xffffffffu, nn, off);
+        pp += __shfl_down_sync(0xffffffffu, pp, off);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(counters + CNT_RAYS, r);
+        atomicAdd(counters + CNT_PATHS, p);
+        atomicAdd(counters + CNT_NODES, nn);
+        atomicAdd(counters + CNT_PRIMS, pp);
+    }
+}
+
+template <bool CLEAN, int ORDER, bool COUNT>
+__global__ void __launch_bounds__(128) wf_shade(DevScene S, DevParams P, WfBuffers B, WfIter w, float4* __restrict__ out,
+                                                unsigned long long* counters, uint32_t* status_word) {
+    const uint32_t n = B.ctr[w.cin];
+    const uint32_t* q = B.queue[w.qin];
+    uint32_t* qn = B.queue[w.qin ^ 1];
+    uint32_t* cn = B.ctr + w.cout;
+    uint32_t status = 0, paths = 0;
+    PathCounters pc{0, 0, 0};
+    TraceStats st{0, 0};
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t limit = (n + 31u) & ~31u;   // whole warps iterate together so wf_push sees full warps
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < limit; k += stride) {
+        bool live = false;
+        uint32_t slot = 0;
+        if (k < n) {
+            slot = __ldcs(q + k);
+            const float2 hv = __ldcs(B.hit + slot);
+            live = wf_step<CLEAN, ORDER>(S, P, B, slot, hv.x, __float_as_uint(hv.y), out, pc, st, paths, status);
+        }
+        wf_push(qn, cn, slot, live);
+    }
+    wf_flush<COUNT>(counters, pc.rays, paths, st);
+    if (status) atomicOr(status_word, status);
+}
+
+// Fused form of one iteration: trace + shade of every queued slot in one launch (each lane still does
+// exactly one bounce, so the warp stays in the same phase), then compaction into the next queue.
+template <bool CLEAN, int ORDER, bool COUNT>
+__global__ void __launch_bounds__(128) wf_bounce(DevScene S, DevParams P, WfBuffers B, WfIter w, float4* __restrict__ out,
+                                                 unsigned long long* counters, uint32_t* status_word) {
+    const uint32_t n = B.ctr[w.cin];
+    if (blockIdx.x == 0 && threadIdx.x == 0) B.ctr[w.czero] = 0u;   // appended to by the next iteration
+    const uint32_t* q = B.queue[w.qin];
+    uint32_t* qn = B.queue[w.qin ^ 1];
+    uint32_t* cn = B.ctr + w.cout;
+    uint32_t status = 0, paths = 0, rays = 0;
+    PathCounters pc{0, 0, 0};
+    TraceStats st{0, 0};
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t limit = (n + 31u) & ~31u;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < limit; k += stride) {
+        bool live = false;
+        uint32_t slot = 0;
+        if (k < n) {
+            slot = q[k];
+            const float4 o = B.ray_o[slot], d = B.ray_d[slot];
+            const uint4 m = B.meta[slot];
+            float t;
+            uint32_t item;
+            ++rays;
+            bool h = closest_hit(S, v3(o), v3(d), 0.00001f, 3.402823466e+38f, m.w == (uint32_t)P.max_depth, t, item,
+                                 st, status);
+            live = wf_step<CLEAN, ORDER>(S, P, B, slot, t, h ? item : 0xffffffffu, out, pc, st, paths, status);
+        }
+        wf_push(qn, cn, slot, live);
+    }
+    wf_flush<COUNT>(counters, rays + pc.rays, paths, st);
+    if (status) atomicOr(status_word, status);
+}
+
+// Drain phase: once the queue is small, each remaining slot is finished in place by one thread
+// instead of paying two kernel launches per bounce for a nearly empty queue.  Pixels whose samples
+// have long paths (glass) make this tail thousands of bounces long in compat mode, where a pixel's
+// samples cannot run in parallel, so the loop keeps the whole path state in registers (the
+// megakernel's loop, resumed from the slot) and touches memory only to write the finished pixel.
+template <bool CLEAN, int ORDER, bool COUNT>
+__global__ void __launch_bounds__(128) wf_finish(DevScene S, DevParams P, WfBuffers B, WfIter w, float4* __restrict__ out,
+                                                 unsigned long long* counters, uint32_t* status_word) {
+    const uint32_t n = B.ctr[w.cin];
+    const uint32_t* q = B.queue[w.qin];
+    uint32_t status = 0, paths = 0;
+    PathCounters pc{0, 0, 0};
+    TraceStats st{0, 0};
+    const uint32_t nsamp = wf_samples(P, CLEAN);
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
+        const uint32_t slot = q[k];
+        uint4 m = B.meta[slot];
+        const float4 o = B.ray_o[slot], d = B.ray_d[slot], a4 = B.att[slot], c4 = B.acc[slot], p4 = B.psum[slot];
+        Ray r;
+        r.o = v3(o);
+        r.d = v3(d);
+        r.time = o.w;
+        RGB att = rgb(a4.x, a4.y, a4.z), acc = rgb(c4.x, c4.y, c4.z);
+        float pr = p4.x, pg = p4.y, pb = p4.z;
+        WfRng<CLEAN> rng;
+        if constexpr (CLEAN) pcg_load(rng, B.pcg[slot]);
+        else rng.x = m.z;
+        uint32_t pixel = m.x, sample = m.y;
+        int depth = (int)m.w;
+        for (;;) {
+            // the rest of the current sample: camera::ray_color's loop from `depth` down
+            for (; depth > 0; --depth) {
+                const bool hide = depth == P.max_depth;
+                float t;
+                uint32_t item;
+                pc.rays++;
+                bool h = closest_hit(S, r.o, r.d, 0.00001f, 3.402823466e+38f, hide, t, item, st, status);
+                if (!shade_bounce<CLEAN, ORDER>(S, r, h, t, item, hide, acc, att, rng, pc, st, status)) break;
+            }
+            ++paths;
+            if (!CLEAN || (isfinite(acc.r) && isfinite(acc.g) && isfinite(acc.b))) {
+                pr += acc.r;
+                pg += acc.g;
+                pb += acc.b;
+            }
+            if (++sample < nsamp) {
+                wf_start_sample<CLEAN, ORDER>(S, P, rng, pixel, sample, r);
+                att = rgb(1.f, 1.f, 1.f);
+                acc = rgb(0.f, 0.f, 0.f);
+                depth = P.max_depth;
+                continue;
+            }
+            out[pixel] = make_float4(pr, pg, pb, 1.0f);
+            // a slot that still has pixels to take (fewer slots than pixels) continues through memory
+            if (!wf_fetch_pixel<CLEAN, ORDER>(S, P, B, slot, out, status)) break;
+            m = B.meta[slot];
+            const float4 o2 = B.ray_o[slot], d2 = B.ray_d[slot];
+            r.o = v3(o2);
+            r.d = v3(d2);
+            r.time = o2.w;
+            att = rgb(1.f, 1.f, 1.f);
+            acc = rgb(0.f, 0.f, 0.f);
+            pr = pg = pb = 0.f;
+            if constexpr (CLEAN) pcg_load(rng, B.pcg[slot]);
+            else rng.x = m.z;
+            pixel = m.x;
+            sample = 0;
+            depth = P.max_depth;
+            if (status) break;
+        }
+    }
+    wf_flush<COUNT>(counters, pc.rays, paths, st);
+    if (status) atomicOr(status_word, status);
+}
+
+}  // namespace rtc

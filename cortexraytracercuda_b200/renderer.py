@@ -22,7 +22,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import RtcError, check
-from .scene import MODE_COMPAT, DRAW_ORDER_DEVICE, RenderParams, Scene, SceneDesc, rtc_scene_info
+from .scene import MODE_COMPAT, DRAW_ORDER_DEVICE, RenderParams, Scene, SceneDesc, rtc_render_stats, rtc_scene_info
 
 
 class Context:
@@ -56,6 +56,12 @@ class Context:
 
     def upload(self, scene: Scene) -> "DeviceScene":
         return DeviceScene(self, scene)
+
+    def last_stats(self) -> dict:
+        """Statistics of the last render (iterations, launches, drained slots, bulk/drain device ms)."""
+        st = rtc_render_stats()
+        check(self.lib.rtc_get_render_stats(self.handle, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in rtc_render_stats._fields_}
 
 
 class DeviceScene:

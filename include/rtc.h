@@ -203,6 +203,13 @@ typedef enum rtc_draw_order {
     RTC_DRAW_ORDER_HOST = 1     /* as a g++ build of the reference's headers consumes it          */
 } rtc_draw_order;
 
+/* Execution engine.  Both compute bit-identical radiance for the same mode and draw order. */
+typedef enum rtc_engine {
+    RTC_ENGINE_AUTO = 0,        /* the library's choice (wavefront)                                       */
+    RTC_ENGINE_MEGAKERNEL = 1,  /* one thread per pixel runs whole paths (the reference's kernel shape)   */
+    RTC_ENGINE_WAVEFRONT = 2    /* extend / shade kernels over compacted path queues                      */
+} rtc_engine;
+
 typedef struct rtc_render_params {
     int32_t width;
     int32_t height;
@@ -212,6 +219,7 @@ typedef struct rtc_render_params {
     int32_t mode;          /* rtc_mode                                                               */
     int32_t draw_order;    /* rtc_draw_order (COMPAT only)                                           */
     int32_t block_size;    /* 0 = library default                                                    */
+    int32_t engine;        /* rtc_engine                                                             */
 } rtc_render_params;
 
 /* ------------------------------------------------------------------------------------------------ */
@@ -254,13 +262,28 @@ rtc_status rtc_scene_get_info(const rtc_scene* scene, rtc_scene_info* info);
 rtc_status rtc_render(rtc_context* ctx, const rtc_scene* scene, const rtc_render_params* params,
                       float* radiance_sum, uint8_t* rgb8);
 
-/* Same render with DEVICE output buffers (inputs already resident); asynchronous on `stream`
+/* Same render with DEVICE output buffers (inputs already resident), on `stream`
  * (a cudaStream_t, or NULL for the context's stream).  d_radiance_sum must hold width*height
  * float4; d_rgb8 may be NULL.  d_counters, when not NULL, receives 4 uint64 counters: rays traced
- * (closest-hit traversals), paths traced, BVH nodes visited, primitive tests. */
+ * (closest-hit traversals), paths traced, BVH nodes visited, primitive tests.  The megakernel engine
+ * returns without waiting for the GPU; the wavefront engine polls its queue counter between batches
+ * of iterations and returns once the frame is complete. */
 rtc_status rtc_render_device(rtc_context* ctx, const rtc_scene* scene, const rtc_render_params* params,
                              float* d_radiance_sum, uint8_t* d_rgb8, unsigned long long* d_counters,
                              void* stream);
+
+/* Statistics of the last render on this context (wavefront engine): iterations of (extend, shade),
+ * kernel launches, whether the drain kernel ran and for how many slots, and the device time of the
+ * bulk iterations and of the drain kernel (ms, from CUDA events; the call waits for the render). */
+typedef struct rtc_render_stats {
+    uint32_t iterations;
+    uint32_t launches;
+    uint32_t drained_slots;
+    uint32_t engine;
+    float bulk_ms;
+    float drain_ms;
+} rtc_render_stats;
+rtc_status rtc_get_render_stats(rtc_context* ctx, rtc_render_stats* stats);
 
 /* Closest-hit queries on arbitrary rays (hit-identity tests).  rays: n x 8 floats
  * (ox, oy, oz, tmin, dx, dy, dz, tmax) in host memory; `depth`/`max_depth` decide light visibility as

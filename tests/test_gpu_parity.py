@@ -22,7 +22,8 @@ import pytest
 
 from cortexraytracercuda_b200 import configs
 from cortexraytracercuda_b200.renderer import DeviceScene
-from cortexraytracercuda_b200.scene import DRAW_ORDER_DEVICE, DRAW_ORDER_HOST, MODE_COMPAT
+from cortexraytracercuda_b200.scene import (DRAW_ORDER_DEVICE, DRAW_ORDER_HOST, ENGINE_MEGAKERNEL, ENGINE_WAVEFRONT,
+                                            MODE_CLEAN, MODE_COMPAT)
 
 import oracles
 
@@ -36,11 +37,12 @@ SCENES = [
 ]
 
 
-def _params(name, kw, order):
+def _params(name, kw, order, engine=ENGINE_WAVEFRONT):
     mk, mp = configs.SCENES[name]
     p = mp(**kw)
     p.mode = MODE_COMPAT
     p.draw_order = order
+    p.engine = engine
     return mk(), p
 
 
@@ -63,15 +65,16 @@ def port():
     return o
 
 
+@pytest.mark.parametrize("engine", [ENGINE_MEGAKERNEL, ENGINE_WAVEFRONT])
 @pytest.mark.parametrize("order", [DRAW_ORDER_HOST, DRAW_ORDER_DEVICE])
 @pytest.mark.parametrize("name,kw", SCENES)
-def test_kernel_bitexact_vs_port(ctx, port, name, kw, order):
-    scene, params = _params(name, kw, order)
+def test_kernel_bitexact_vs_port(ctx, port, name, kw, order, engine):
+    scene, params = _params(name, kw, order, engine)
     ours, _ = DeviceScene(ctx, scene).render(params)
     pix = np.arange(params.width * params.height, dtype=np.int64)
     ref, _ = port.scene(scene).render_pixels(params, pix, trig=1)
     st = oracles.parity_stats(ours.reshape(-1, 4), ref)
-    print(name, order, st)
+    print(name, order, engine, st)
     # exact-t ties between primitives may resolve differently in two different BVHs
     assert st["frac_exact"] >= 0.999, st
 
@@ -158,3 +161,47 @@ def test_closest_hit_identity(ctx, refcpu, name):
         assert int(hard.sum()) == 0
         both = (ours >= 0) & (ours == ref)
         assert np.array_equal(t_ours[both], t_ref[both])
+
+
+@pytest.mark.parametrize("name,kw", SCENES)
+def test_wavefront_equals_megakernel(ctx, name, kw):
+    """The two engines run the same shade_bounce arithmetic: identical sums, not just close ones."""
+    scene, params = _params(name, kw, DRAW_ORDER_DEVICE, ENGINE_MEGAKERNEL)
+    ds = DeviceScene(ctx, scene)
+    a, _ = ds.render(params)
+    params.engine = ENGINE_WAVEFRONT
+    b, _ = ds.render(params)
+    assert np.array_equal(np.nan_to_num(a, nan=-7.0), np.nan_to_num(b, nan=-7.0))
+
+
+def test_wavefront_fewer_slots_than_pixels_and_reuse(ctx):
+    """A frame larger than one render before it reuses the context's scratch; repeated renders are
+    identical (no state leaks between frames)."""
+    scene, params = _params("cornell", dict(width=40, height=40, spp=4, max_depth=6), DRAW_ORDER_DEVICE)
+    ds = DeviceScene(ctx, scene)
+    a, _ = ds.render(params)
+    big = params.__class__(**{**params.__dict__, "width": 96, "height": 96})
+    ds.render(big)
+    b, _ = ds.render(params)
+    assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("name", ["cornell", "spheres"])
+def test_clean_mode_statistics(ctx, port, name):
+    """Clean mode (PCG stream per pixel and sample, FMA allowed) against the C restatement's clean mode:
+    same estimator, so the images agree statistically (quartiles within 5% at 64 spp)."""
+    mk, mp = configs.SCENES[name]
+    scene = mk()
+    params = mp(width=48, height=32, spp=64, max_depth=12)
+    params.mode = MODE_CLEAN
+    ds = DeviceScene(ctx, scene)
+    outs = []
+    for eng in (ENGINE_MEGAKERNEL, ENGINE_WAVEFRONT):
+        params.engine = eng
+        outs.append(ds.render(params)[0])
+    pix = np.arange(params.width * params.height, dtype=np.int64)
+    ref, _ = port.scene(scene).render_pixels(params, pix, trig=1)
+    (q0, _), (q1, _), (qr, mr) = _quantiles(outs[0]), _quantiles(outs[1]), _quantiles(ref)
+    print(name, q0, q1, qr)
+    for q in (q0, q1):
+        assert np.all(np.abs(q - qr) <= 0.05 * np.maximum(np.abs(qr), 1e-3 * mr)), (q, qr)
