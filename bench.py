@@ -41,7 +41,7 @@ sys.path.insert(0, str(ROOT))
 
 from cortexraytracercuda_b200 import configs  # noqa: E402
 from cortexraytracercuda_b200.scene import (DRAW_ORDER_DEVICE, DRAW_ORDER_HOST, ENGINE_MEGAKERNEL,  # noqa: E402
-                                            ENGINE_WAVEFRONT, MODE_CLEAN, MODE_COMPAT)
+                                            ENGINE_WAVEFRONT, FLAG_KERNEL_TIMING, MODE_CLEAN, MODE_COMPAT)
 
 METRIC = "Mpaths/s"
 PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
@@ -51,6 +51,7 @@ FALLBACK_HBM_GBS = 6650.0
 NODE_BYTES = 64          # BVH2 node: two child boxes + two child links (4 x float4)
 PRIM_BYTES = {"spheres": 16, "cornell": 48, "meshes": 48}   # dominant primitive record of each workload
 STATE_BYTES = 32 + 16 + 2 * 48   # ray read + hit write + path state read/write per traversal
+EXTEND_STATE_BYTES = 4 + 32 + 4 + 8   # queue entry + ray (origin, direction) + depth word read, hit record write
 
 
 def workload(name):
@@ -244,7 +245,7 @@ def main():
     W, H = params.width, params.height
     out = torch.empty((H, W, 4), dtype=torch.float32, device="cuda")
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-    counters = torch.zeros(4, dtype=torch.int64, device="cuda")
+    counters = torch.zeros(8, dtype=torch.int64, device="cuda")
     # a dedicated stream: the kernels and the CUDA events that time them are on the same stream
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
@@ -257,7 +258,10 @@ def main():
     counters.zero_()
     launch(counters)
     torch.cuda.synchronize()
-    rays, paths, nodes, prims = [int(x) for x in counters.tolist()]
+    rays, paths, nodes, prims, ext_rays, ext_nodes, ext_prims, _ = [int(x) for x in counters.tolist()]
+    wavefront = params.engine == ENGINE_WAVEFRONT
+    if wavefront:
+        params.flags |= FLAG_KERNEL_TIMING      # CUDA events around every extend / shade launch
 
     for _ in range(args.warmup):
         flush.fill_(1.0)
@@ -271,11 +275,13 @@ def main():
     barrier()
     torch.cuda.synchronize()
     t_wall = time.perf_counter()
+    kstats = []
     for k in range(args.steps):
         flush.fill_(float(k))          # L2 flush between steps (outside the kernel's events)
         ev[k][0].record(stream)
         launch()
         ev[k][1].record(stream)
+        kstats.append(ctx.last_stats())
     torch.cuda.synchronize()
     barrier()
     t_wall = time.perf_counter() - t_wall
@@ -316,15 +322,37 @@ def main():
     # ---- roofline -------------------------------------------------------------------------------
     peak, peak_kind = hbm_peak()
     prim_b = PRIM_BYTES[args.config]
-    alg_bytes = nodes * NODE_BYTES + prims * prim_b + rays * STATE_BYTES
-    achieved = alg_bytes / (kernel_ms / 1e3) / 1e9
-    roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-            "frac": round(achieved / peak, 4), "traffic": None, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
-            "kernel": "rtc::rtc_render_compat<0>" if params.mode == MODE_COMPAT else "rtc::rtc_render_clean",
-            "alg_bytes_per_launch": int(alg_bytes), "kernel_ms": round(kernel_ms, 3),
-            "per_launch": {"rays": rays, "paths": paths, "node_visits": nodes, "prim_tests": prims},
-            "bytes_per_ray": round(alg_bytes / max(rays, 1), 1)}
-    prof = ROOT / "profiles" / f"traffic_{args.config}.json"
+    if wavefront:
+        # dominant kernel: wf_extend (closest-hit traversal of every queued ray).  Algorithmic bytes of
+        # its launches in one frame, from its own counters, over its summed CUDA-event time.
+        ext_ms = float(np.mean([st["extend_ms"] for st in kstats]))
+        ext_launches = int(np.mean([st["extend_launches"] for st in kstats]))
+        ext_bytes = ext_nodes * NODE_BYTES + ext_prims * prim_b + ext_rays * EXTEND_STATE_BYTES
+        achieved = ext_bytes / (ext_ms / 1e3) / 1e9
+        roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": None,
+                "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                "kernel": "rtc::wf_extend", "launches_per_frame": ext_launches,
+                "alg_bytes_per_launch": int(ext_bytes / max(ext_launches, 1)),
+                "avg_launch_ms": round(ext_ms / max(ext_launches, 1), 4), "kernel_ms_per_frame": round(ext_ms, 3),
+                "share_of_frame": round(ext_ms / kernel_ms, 3),
+                "per_frame": {"rays": ext_rays, "node_visits": ext_nodes, "prim_tests": ext_prims},
+                "bytes_per_ray": round(ext_bytes / max(ext_rays, 1), 1),
+                "frame": {"shade_ms": round(float(np.mean([st["shade_ms"] for st in kstats])), 3),
+                          "drain_ms": round(float(np.mean([st["drain_ms"] for st in kstats])), 3),
+                          "iterations": int(np.mean([st["iterations"] for st in kstats])),
+                          "rays": rays, "paths": paths, "node_visits": nodes, "prim_tests": prims}}
+    else:
+        alg_bytes = nodes * NODE_BYTES + prims * prim_b + rays * STATE_BYTES
+        achieved = alg_bytes / (kernel_ms / 1e3) / 1e9
+        roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": None,
+                "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                "kernel": "rtc::rtc_render_compat" if params.mode == MODE_COMPAT else "rtc::rtc_render_clean",
+                "alg_bytes_per_launch": int(alg_bytes), "kernel_ms": round(kernel_ms, 3),
+                "per_launch": {"rays": rays, "paths": paths, "node_visits": nodes, "prim_tests": prims},
+                "bytes_per_ray": round(alg_bytes / max(rays, 1), 1)}
+    prof = ROOT / "profiles" / f"traffic_{'wf_extend' if wavefront else 'megakernel'}_{args.config}.json"
     if prof.exists():
         try:
             roof["traffic"] = json.loads(prof.read_text()).get("dram_bytes_per_launch")
@@ -336,7 +364,8 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {**describe(args.config, params, scene), "parallelism": f"replicas x{world}",
                        "bvh_nodes": info["num_nodes"]},
-            "mrays_per_s": round(mrays, 3), "gpu_launches": args.steps,
+            "mrays_per_s": round(mrays, 3),
+            "gpu_launches": int(sum(st["launches"] for st in kstats)) if wavefront else args.steps,
             "e2e": {"value": round(e2e_value, 3), "unit": METRIC, "h2d_bytes_per_step": int(info["device_bytes"]),
                     "d2h_bytes_per_step": int(W * H * 16), "ms_per_step": round(e2e_total / args.steps, 3)},
             "roofline": roof, "clocks": clk, "wall_s": round(t_wall, 3)}

@@ -13,6 +13,7 @@ from .scene import rtc_render_params, rtc_render_stats, rtc_scene_desc, rtc_scen
 
 LIB_PATH = Path(__file__).resolve().parent / "librtc_b200.so"
 
+
 STATUS_NAMES = {0: "RTC_OK", 1: "RTC_ERR_INVALID_ARGUMENT", 2: "RTC_ERR_BAD_SCENE", 3: "RTC_ERR_CUDA",
                 4: "RTC_ERR_OOM", 5: "RTC_ERR_TIMEOUT", 6: "RTC_ERR_NO_DEVICE", 7: "RTC_ERR_IO",
                 8: "RTC_ERR_DEVICE_CHECK", 9: "RTC_ERR_NOT_FOUND", 10: "RTC_ERR_BUSY"}

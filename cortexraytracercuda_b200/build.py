@@ -29,17 +29,21 @@ CXX = os.environ.get("CXX", "g++")
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-Wall", "-Wno-unused-function",
              "-I", str(CSRC), "-I", str(INCLUDE), "-I", os.path.join(CUDA_HOME, "include")]
 
-# (source, compiler, extra flags)
+# (source, object name, compiler, extra flags).  The compat sources are built once per reference
+# build flavour: RTC_FLAVOR=1 reproduces a g++ build of the reference (no FMA contraction),
+# RTC_FLAVOR=0 its nvcc build (FMA contraction on, nvcc's default).
 SOURCES = [
-    ("render_compat.cu", "nvcc", ["--fmad=false"]),
-    ("render_clean.cu", "nvcc", ["--fmad=true"]),
-    ("wavefront_compat.cu", "nvcc", ["--fmad=false"]),
-    ("wavefront_clean.cu", "nvcc", ["--fmad=true"]),
-    ("rtc_api.cpp", "cxx", []),
-    ("bvh_build.cpp", "cxx", []),
+    ("render_compat.cu", "render_compat_host", "nvcc", ["--fmad=false", "-DRTC_FLAVOR=1"]),
+    ("render_compat.cu", "render_compat_dev", "nvcc", ["--fmad=true", "-DRTC_FLAVOR=0"]),
+    ("wavefront_compat.cu", "wavefront_compat_host", "nvcc", ["--fmad=false", "-DRTC_FLAVOR=1"]),
+    ("wavefront_compat.cu", "wavefront_compat_dev", "nvcc", ["--fmad=true", "-DRTC_FLAVOR=0"]),
+    ("render_clean.cu", "render_clean", "nvcc", ["--fmad=true"]),
+    ("wavefront_clean.cu", "wavefront_clean", "nvcc", ["--fmad=true"]),
+    ("rtc_api.cpp", "rtc_api", "cxx", []),
+    ("bvh_build.cpp", "bvh_build", "cxx", []),
 ]
 HEADERS = ["rtc_dev.h", "rtc_math.cuh", "rtc_trace.cuh", "rtc_path.cuh", "rtc_wavefront.cuh", "rtc_kernels.h",
-           "bvh_build.h"]
+           "bvh_build.h", "rtc_internal.h"]
 
 
 def _newer(target: Path, deps) -> bool:
@@ -66,9 +70,9 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
     BUILD.mkdir(exist_ok=True)
     headers = [CSRC / h for h in HEADERS] + [INCLUDE / "rtc.h"]
     objs = []
-    for src, comp, extra in SOURCES:
+    for src, obj, comp, extra in SOURCES:
         s = CSRC / src
-        o = BUILD / (src + ".o")
+        o = BUILD / (obj + ".o")
         objs.append(o)
         if not force and not _newer(o, [s] + headers + [Path(__file__)]):
             continue

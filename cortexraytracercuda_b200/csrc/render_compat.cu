@@ -1,9 +1,15 @@
 // render_compat.cu - compat-mode kernels (reference semantics, per-pixel minstd stream).
 //
-// Built with --fmad=false: every float expression restated from the reference is evaluated with
-// the reference's roundings (no FMA contraction), so the only differences left against a g++ build of
-// the reference are the last-ulp results of cos/sin/acos/atan2.  The BVH slab test uses explicit
-// __fmaf_rn, which is unaffected by the flag.
+// Compiled twice, once per reference build flavour (RTC_FLAVOR):
+//   RTC_FLAVOR=1 (g++ flavour, --fmad=false): every float expression restated from the reference is
+//     evaluated with the roundings of a g++ build of the reference (no FMA contraction, right-to-left
+//     multi-draw order), so the only differences left against it are the last-ulp results of
+//     cos/sin/acos/atan2;
+//   RTC_FLAVOR=0 (nvcc flavour, --fmad=true): left-to-right draws, FMA contraction and CUDA's float
+//     trig, like the reference's own device build.  The reference's image depends on contraction (its
+//     shadow-acne epsilon, constants.cuh:27, sits at rounding level for scenes of size ~10^2-10^3), so
+//     this flavour reproduces the device build's statistics.
+// The BVH slab test uses explicit __fmaf_rn in both.
 //
 // Kernels:
 //   rtc_render_compat<ORDER>  one thread per pixel, all samples of the pixel in sequence
@@ -13,6 +19,10 @@
 //                             (color.cuh:289-309, gpu.cu:792-799, 2098-2107).
 #include "rtc_kernels.h"
 #include "rtc_path.cuh"
+
+#ifndef RTC_FLAVOR
+#error "compile with -DRTC_FLAVOR=0 (nvcc flavour) or -DRTC_FLAVOR=1 (g++ flavour)"
+#endif
 
 namespace rtc {
 
@@ -67,6 +77,7 @@ __global__ void __launch_bounds__(128) rtc_render_compat(DevScene S, DevParams P
     if (status) atomicOr(status_word, status);
 }
 
+#if RTC_FLAVOR == 1
 __device__ __forceinline__ int32_t item_gid(const DevScene& S, uint32_t it) {
     uint32_t kind = it >> 30, idx = it & 0x3fffffffu;
     switch (kind) {
@@ -112,22 +123,23 @@ __global__ void rtc_quantize(const float4* __restrict__ sum, uint8_t* __restrict
         o[k] = (uint8_t)q;
     }
 }
+#endif  // RTC_FLAVOR == 1
 
 }  // namespace rtc
 
 using namespace rtc;
 
-cudaError_t rtc_launch_render_compat(const DevScene& S, const DevParams& P, float4* out,
-                                     unsigned long long* counters, uint32_t* status, int block, cudaStream_t st) {
+cudaError_t RTC_FLAVOR_FN(rtc_launch_render_compat)(const DevScene& S, const DevParams& P, float4* out,
+                                                   unsigned long long* counters, uint32_t* status, int block,
+                                                   cudaStream_t st) {
     (void)block;
     const int threads = 128;
     const unsigned grid = (unsigned)((P.num_pixels + threads - 1) / threads);
-    if (P.draw_order == 1)
-        rtc_render_compat<1><<<grid, threads, 0, st>>>(S, P, out, counters, status);
-    else
-        rtc_render_compat<0><<<grid, threads, 0, st>>>(S, P, out, counters, status);
+    rtc_render_compat<RTC_FLAVOR><<<grid, threads, 0, st>>>(S, P, out, counters, status);
     return cudaGetLastError();
 }
+
+#if RTC_FLAVOR == 1
 
 cudaError_t rtc_launch_trace_closest(const DevScene& S, const float* rays, uint32_t n, int depth, int max_depth,
                                      int32_t* prim, float* t, uint32_t* status, cudaStream_t st) {
@@ -144,3 +156,4 @@ cudaError_t rtc_launch_quantize(const float4* sum, uint8_t* rgb8, int width, int
     rtc_quantize<<<(unsigned)((n + threads - 1) / threads), threads, 0, st>>>(sum, rgb8, width, height, spp);
     return cudaGetLastError();
 }
+#endif  // RTC_FLAVOR == 1

@@ -22,6 +22,7 @@
 #include "bvh_build.h"
 #include "rtc_dev.h"
 #include "rtc_kernels.h"
+#include "rtc_internal.h"
 #include "rtc_math.cuh"
 
 using namespace rtc;
@@ -65,6 +66,9 @@ struct rtc_context {
     cudaEvent_t phase_ev[3] = {nullptr, nullptr, nullptr};   // render start, drain start, render end
     rtc_render_stats last{};
     bool last_timed = false;
+    std::vector<cudaEvent_t> kev;      // per-launch timing events (RTC_FLAG_KERNEL_TIMING)
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> kev_pairs;   // extend pairs, then shade pairs
+    uint32_t kev_ext = 0, kev_shade = 0;   // pairs used by the last render
     std::mutex mu;
 };
 
@@ -121,6 +125,7 @@ extern "C" rtc_status rtc_context_destroy(rtc_context* c) {
         if (e) cudaEventDestroy(e);
     for (cudaEvent_t& e : c->phase_ev)
         if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : c->kev) cudaEventDestroy(e);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return RTC_OK;
@@ -552,6 +557,31 @@ DevParams dev_params(const rtc_render_params* p) {
 constexpr size_t WF_SLOT_BYTES = 5 * sizeof(float4) + 2 * sizeof(uint4) + sizeof(float2) + 2 * sizeof(uint32_t);
 constexpr uint32_t WF_MAX_SLOTS = 1u << 22;   // 4,194,304 slots = 432 MiB of path state
 
+// Lays out the wavefront buffers for `slots` path slots in one block of device memory at `base`
+// (the context's scratch, or the allocation-free entry point's static array).
+size_t carve_wavefront(void* base, uint32_t slots, WfBuffers& B) {
+    uint8_t* p = (uint8_t*)base;
+    auto take = [&](size_t bytes) {
+        uint8_t* r = p;
+        p += (bytes + 255) & ~(size_t)255;
+        return (void*)r;
+    };
+    const size_t n = slots;
+    B.ray_o = (float4*)take(n * 16);
+    B.ray_d = (float4*)take(n * 16);
+    B.att = (float4*)take(n * 16);
+    B.acc = (float4*)take(n * 16);
+    B.psum = (float4*)take(n * 16);
+    B.meta = (uint4*)take(n * 16);
+    B.pcg = (uint4*)take(n * 16);
+    B.hit = (float2*)take(n * 8);
+    B.queue[0] = (uint32_t*)take(n * 4);
+    B.queue[1] = (uint32_t*)take(n * 4);
+    B.ctr = (uint32_t*)take(WF_CTR_N * 4);
+    B.slots = slots;
+    return (size_t)(p - (uint8_t*)base);
+}
+
 rtc_status ensure_wavefront(rtc_context* c, uint32_t slots, WfBuffers& B) {
     if (c->wf_cap < slots) {
         cudaFree(c->d_wf);
@@ -567,106 +597,208 @@ rtc_status ensure_wavefront(rtc_context* c, uint32_t slots, WfBuffers& B) {
         RTC_CUDA(cudaEventCreateWithFlags(&c->poll_ev[1], cudaEventDisableTiming));
         for (cudaEvent_t& e : c->phase_ev) RTC_CUDA(cudaEventCreate(&e));
     }
-    const size_t n = c->wf_cap;
-    uint8_t* p = (uint8_t*)c->d_wf;
-    auto take = [&](size_t bytes) {
-        uint8_t* r = p;
-        p += (bytes + 255) & ~(size_t)255;
-        return (void*)r;
-    };
-    B.ray_o = (float4*)take(n * 16);
-    B.ray_d = (float4*)take(n * 16);
-    B.att = (float4*)take(n * 16);
-    B.acc = (float4*)take(n * 16);
-    B.psum = (float4*)take(n * 16);
-    B.meta = (uint4*)take(n * 16);
-    B.pcg = (uint4*)take(n * 16);
-    B.hit = (float2*)take(n * 8);
-    B.queue[0] = (uint32_t*)take(n * 4);
-    B.queue[1] = (uint32_t*)take(n * 4);
-    B.ctr = (uint32_t*)take(WF_CTR_N * 4);
-    B.slots = slots;
+    carve_wavefront(c->d_wf, slots, B);
     return RTC_OK;
 }
 
-// Wavefront engine: init, then batches of (extend, shade) iterations until the slot queue drains.
-// The queue size after each batch is copied to pinned memory; the batch after it is already queued
-// when the host looks, so the GPU never waits for the host.
-rtc_status launch_wavefront(rtc_context* c, const rtc_scene* s, const rtc_render_params* p, float4* d_out,
-                            unsigned long long* d_counters, cudaStream_t st) {
+// How the host learns the queue size after a batch of iterations.
+struct WfPoller {
+    uint32_t* h = nullptr;           // pinned slots: the next batch is queued before the host looks
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    bool sync = false;               // synchronous copy into a host variable (no pinned memory, no events)
+};
+
+struct WfRun {
+    uint64_t iterations = 0;
+    bool drained = false;
+    uint32_t drained_slots = 0;
+};
+
+// Wavefront engine: init, then batches of (extend, shade) iterations until the slot queue drains or
+// falls under the drain threshold, where one finish launch completes the remaining slots.
+// Optional per-launch timing: event pairs around extend launches (first half of the pool order) and
+// shade launches, created on demand.
+struct WfTimer {
+    std::vector<cudaEvent_t>* pool = nullptr;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ext, shade;
+    size_t used = 0;
+    cudaError_t pair(cudaEvent_t& a, cudaEvent_t& b) {
+        while (pool->size() < used + 2) {
+            cudaEvent_t e;
+            cudaError_t r = cudaEventCreate(&e);
+            if (r != cudaSuccess) return r;
+            pool->push_back(e);
+        }
+        a = (*pool)[used];
+        b = (*pool)[used + 1];
+        used += 2;
+        return cudaSuccess;
+    }
+};
+
+rtc_status run_wavefront(const DevScene& S, const rtc_render_params* p, const WfBuffers& B, uint32_t* d_status,
+                         float4* d_out, unsigned long long* d_counters, cudaStream_t st, int num_sms,
+                         const WfPoller& poll, cudaEvent_t* phase, WfRun& run, WfTimer* timer = nullptr) {
     DevParams P = dev_params(p);
     const bool clean = p->mode == RTC_MODE_CLEAN;
-    const uint32_t slots = (uint32_t)std::min<int64_t>(P.num_pixels, WF_MAX_SLOTS);
-    WfBuffers B;
-    rtc_status r = ensure_wavefront(c, slots, B);
-    if (r != RTC_OK) return r;
-    RTC_CUDA(cudaEventRecord(c->phase_ev[0], st));
+    if (phase) RTC_CUDA(cudaEventRecord(phase[0], st));
     RTC_CUDA(cudaMemsetAsync(B.ctr, 0, WF_CTR_N * sizeof(uint32_t), st));
-    const int grid = c->num_sms * 8;
-    const int init_grid = (int)std::min<int64_t>((slots + 127) / 128, (int64_t)c->num_sms * 16);
-    cudaError_t e = clean ? rtc_wf_launch_init_clean(s->dev, P, B, d_out, init_grid, st)
-                          : rtc_wf_launch_init_compat(p->draw_order, s->dev, P, B, d_out, init_grid, st);
+    const int grid = num_sms * 8;
+    const int init_grid = (int)std::min<int64_t>((B.slots + 127) / 128, (int64_t)num_sms * 16);
+    const bool host = !clean && p->draw_order == RTC_DRAW_ORDER_HOST;   // g++ flavour of the compat kernels
+    cudaError_t e = clean ? rtc_wf_launch_init_clean(S, P, B, d_out, init_grid, st)
+                    : host ? rtc_wf_launch_init_compat_host(S, P, B, d_out, init_grid, st)
+                           : rtc_wf_launch_init_compat_dev(S, P, B, d_out, init_grid, st);
     if (e != cudaSuccess) return cuda_fail(e, "wavefront init");
     const uint64_t nsamp = clean ? (uint64_t)P.spp : (uint64_t)P.sqrt_spp * P.sqrt_spp;
-    const uint64_t rounds = (uint64_t)((P.num_pixels + slots - 1) / slots);
+    const uint64_t rounds = (uint64_t)((P.num_pixels + B.slots - 1) / B.slots);
     const uint64_t max_iters = rounds * nsamp * (uint64_t)(P.max_depth + 1) + 64;
     const int BATCH = 8;
     // drain threshold: below this many queued slots the finish kernel takes over
-    uint32_t drain = (uint32_t)c->num_sms * 512u;
+    uint32_t drain = (uint32_t)num_sms * 512u;
     if (const char* ev = std::getenv("RTC_WF_DRAIN")) drain = (uint32_t)std::strtoul(ev, nullptr, 10);
-    // fused iteration (trace + shade in one launch) or split extend / shade kernels
-    bool fused = true;
-    if (const char* ev = std::getenv("RTC_WF_SPLIT")) fused = std::atoi(ev) == 0;
+    // split extend / shade kernels (default) or one fused launch per iteration
+    bool fused = false;
+    if (const char* ev = std::getenv("RTC_WF_FUSED")) fused = std::atoi(ev) != 0;
     uint64_t it = 0;
     int pending = -1;   // poll slot of the previous batch
-    bool finish = false;
+    uint32_t left = 0;
+    uint32_t sync_counts[2] = {0, 0};
     for (int b = 0;; ++b) {
         for (int k = 0; k < BATCH; ++k, ++it) {
             const WfIter w = wf_iter(it);
             if (fused) {
-                e = clean ? rtc_wf_launch_bounce_clean(s->dev, P, B, w, d_out, d_counters, c->d_status, grid, st)
-                          : rtc_wf_launch_bounce_compat(p->draw_order, s->dev, P, B, w, d_out, d_counters, c->d_status,
-                                                        grid, st);
+                e = clean  ? rtc_wf_launch_bounce_clean(S, P, B, w, d_out, d_counters, d_status, grid, st)
+                    : host ? rtc_wf_launch_bounce_compat_host(S, P, B, w, d_out, d_counters, d_status, grid, st)
+                           : rtc_wf_launch_bounce_compat_dev(S, P, B, w, d_out, d_counters, d_status, grid, st);
             } else {
-                e = rtc_wf_launch_extend(s->dev, P, B, w, d_counters, c->d_status, grid, st);
+                cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr, e3 = nullptr;
+                if (timer) {
+                    RTC_CUDA(timer->pair(e0, e1));
+                    RTC_CUDA(timer->pair(e2, e3));
+                    RTC_CUDA(cudaEventRecord(e0, st));
+                }
+                e = host ? rtc_wf_launch_extend_host(S, P, B, w, d_counters, d_status, grid, st)
+                         : rtc_wf_launch_extend_dev(S, P, B, w, d_counters, d_status, grid, st);
+                if (timer) {
+                    RTC_CUDA(cudaEventRecord(e1, st));
+                    RTC_CUDA(cudaEventRecord(e2, st));
+                    timer->ext.push_back({e0, e1});
+                }
                 if (e == cudaSuccess)
-                    e = clean ? rtc_wf_launch_shade_clean(s->dev, P, B, w, d_out, d_counters, c->d_status, grid, st)
-                              : rtc_wf_launch_shade_compat(p->draw_order, s->dev, P, B, w, d_out, d_counters,
-                                                           c->d_status, grid, st);
+                    e = clean  ? rtc_wf_launch_shade_clean(S, P, B, w, d_out, d_counters, d_status, grid, st)
+                        : host ? rtc_wf_launch_shade_compat_host(S, P, B, w, d_out, d_counters, d_status, grid, st)
+                               : rtc_wf_launch_shade_compat_dev(S, P, B, w, d_out, d_counters, d_status, grid, st);
+                if (timer) {
+                    RTC_CUDA(cudaEventRecord(e3, st));
+                    timer->shade.push_back({e2, e3});
+                }
             }
             if (e != cudaSuccess) return cuda_fail(e, "wavefront iteration");
         }
+        // Both polling modes act on the count of the PREVIOUS batch (the next batch is already
+        // queued when the host looks), so the drain point - and with it the result - does not depend
+        // on the polling mode.
+        bool have = false;
         const int slot = b & 1;
-        RTC_CUDA(cudaMemcpyAsync(c->h_poll + slot, B.ctr + wf_iter(it).cin, sizeof(uint32_t), cudaMemcpyDeviceToHost,
-                                 st));
-        RTC_CUDA(cudaEventRecord(c->poll_ev[slot], st));
-        if (pending >= 0) {
-            RTC_CUDA(cudaEventSynchronize(c->poll_ev[pending]));
-            const uint32_t left = c->h_poll[pending];
-            if (left == 0) break;
-            if (left < drain) { finish = true; break; }
+        if (poll.sync) {
+            uint32_t h = 0;
+            RTC_CUDA(cudaMemcpyAsync(&h, B.ctr + wf_iter(it).cin, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+            RTC_CUDA(cudaStreamSynchronize(st));
+            sync_counts[slot] = h;
+            if (pending >= 0) {
+                left = sync_counts[pending];
+                have = true;
+            }
+        } else {
+            RTC_CUDA(cudaMemcpyAsync(poll.h + slot, B.ctr + wf_iter(it).cin, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                     st));
+            RTC_CUDA(cudaEventRecord(poll.ev[slot], st));
+            if (pending >= 0) {
+                RTC_CUDA(cudaEventSynchronize(poll.ev[pending]));
+                left = poll.h[pending];
+                have = true;
+            }
         }
         pending = slot;
+        if (have && left == 0) break;
+        if (have && left < drain) {
+            run.drained = true;
+            break;
+        }
         if (it > max_iters) return fail(RTC_ERR_TIMEOUT, "wavefront did not drain within its iteration bound");
     }
-    c->last = rtc_render_stats{};
-    c->last.engine = RTC_ENGINE_WAVEFRONT;
-    c->last.iterations = (uint32_t)it;
-    c->last.launches = (uint32_t)(1 + (fused ? 1 : 2) * it + (finish ? 1 : 0));
-    c->last.drained_slots = finish ? c->h_poll[pending] : 0u;
-    RTC_CUDA(cudaEventRecord(c->phase_ev[1], st));
-    if (finish) {
+    run.iterations = it;
+    run.drained_slots = run.drained ? left : 0u;
+    if (phase) RTC_CUDA(cudaEventRecord(phase[1], st));
+    if (run.drained) {
         const WfIter w = wf_iter(it);
         const int fgrid = (int)std::max<uint32_t>(1u, (drain + 127u) / 128u);
-        e = clean ? rtc_wf_launch_finish_clean(s->dev, P, B, w, d_out, d_counters, c->d_status, fgrid, st)
-                  : rtc_wf_launch_finish_compat(p->draw_order, s->dev, P, B, w, d_out, d_counters, c->d_status, fgrid,
-                                                st);
+        e = clean  ? rtc_wf_launch_finish_clean(S, P, B, w, d_out, d_counters, d_status, fgrid, st)
+            : host ? rtc_wf_launch_finish_compat_host(S, P, B, w, d_out, d_counters, d_status, fgrid, st)
+                   : rtc_wf_launch_finish_compat_dev(S, P, B, w, d_out, d_counters, d_status, fgrid, st);
         if (e != cudaSuccess) return cuda_fail(e, "wavefront finish");
     }
-    RTC_CUDA(cudaEventRecord(c->phase_ev[2], st));
+    if (phase) RTC_CUDA(cudaEventRecord(phase[2], st));
+    return RTC_OK;
+}
+
+rtc_status launch_wavefront(rtc_context* c, const rtc_scene* s, const rtc_render_params* p, float4* d_out,
+                            unsigned long long* d_counters, cudaStream_t st) {
+    const int64_t npix = (int64_t)p->width * p->height;
+    const uint32_t slots = (uint32_t)std::min<int64_t>(npix, WF_MAX_SLOTS);
+    WfBuffers B;
+    rtc_status r = ensure_wavefront(c, slots, B);
+    if (r != RTC_OK) return r;
+    WfPoller poll;
+    poll.h = c->h_poll;
+    poll.ev[0] = c->poll_ev[0];
+    poll.ev[1] = c->poll_ev[1];
+    WfRun run;
+    WfTimer timer;
+    timer.pool = &c->kev;
+    const bool timed = (p->flags & RTC_FLAG_KERNEL_TIMING) != 0;
+    r = run_wavefront(s->dev, p, B, c->d_status, d_out, d_counters, st, c->num_sms, poll, c->phase_ev, run,
+                      timed ? &timer : nullptr);
+    if (r != RTC_OK) return r;
+    c->kev_ext = c->kev_shade = 0;
+    c->kev_pairs.clear();
+    if (timed) {
+        c->kev_ext = (uint32_t)timer.ext.size();
+        c->kev_shade = (uint32_t)timer.shade.size();
+        for (auto& pr : timer.ext) c->kev_pairs.push_back(pr);
+        for (auto& pr : timer.shade) c->kev_pairs.push_back(pr);
+    }
+    const bool fused = std::getenv("RTC_WF_FUSED") && std::atoi(std::getenv("RTC_WF_FUSED")) != 0;
+    c->last = rtc_render_stats{};
+    c->last.engine = RTC_ENGINE_WAVEFRONT;
+    c->last.iterations = (uint32_t)run.iterations;
+    c->last.launches = (uint32_t)(1 + (fused ? 1 : 2) * run.iterations + (run.drained ? 1 : 0));
+    c->last.drained_slots = run.drained_slots;
     c->last_timed = true;
     return RTC_OK;
 }
+
+}  // namespace
+
+// ---- internal helpers shared with render_noalloc.cu (rtc_internal.h) ----
+size_t rtc_wf_slot_bytes() { return WF_SLOT_BYTES; }
+size_t rtc_carve_wavefront(void* base, uint32_t slots, WfBuffers& B) { return carve_wavefront(base, slots, B); }
+rtc_status rtc_set_error(rtc_status s, const char* msg) { return fail(s, msg); }
+rtc_status rtc_check_render_params(const rtc_render_params* p) { return check_params(p); }
+int rtc_scene_device(const rtc_scene* s) { return s->device; }
+rtc_status rtc_run_wavefront_sync(const rtc_scene* s, const rtc_render_params* p, const WfBuffers& B,
+                                  uint32_t* d_status, float4* d_out, cudaStream_t st) {
+    int dev = 0, sms = 148;
+    RTC_CUDA(cudaGetDevice(&dev));
+    RTC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    WfPoller poll;
+    poll.sync = true;
+    WfRun run;
+    return run_wavefront(s->dev, p, B, d_status, d_out, nullptr, st, sms, poll, nullptr, run);
+}
+
+namespace {
 
 rtc_status launch(rtc_context* c, const rtc_scene* s, const rtc_render_params* p, float4* d_out,
                   unsigned long long* d_counters, cudaStream_t st) {
@@ -676,9 +808,11 @@ rtc_status launch(rtc_context* c, const rtc_scene* s, const rtc_render_params* p
     c->last.launches = 1;
     c->last_timed = false;
     DevParams P = dev_params(p);
-    cudaError_t e = p->mode == RTC_MODE_COMPAT
-                        ? rtc_launch_render_compat(s->dev, P, d_out, d_counters, c->d_status, p->block_size, st)
-                        : rtc_launch_render_clean(s->dev, P, d_out, d_counters, c->d_status, p->block_size, st);
+    cudaError_t e =
+        p->mode == RTC_MODE_CLEAN ? rtc_launch_render_clean(s->dev, P, d_out, d_counters, c->d_status, p->block_size, st)
+        : p->draw_order == RTC_DRAW_ORDER_HOST
+            ? rtc_launch_render_compat_host(s->dev, P, d_out, d_counters, c->d_status, p->block_size, st)
+            : rtc_launch_render_compat_dev(s->dev, P, d_out, d_counters, c->d_status, p->block_size, st);
     if (e != cudaSuccess) return cuda_fail(e, "render launch");
     return RTC_OK;
 }
@@ -754,6 +888,14 @@ extern "C" rtc_status rtc_get_render_stats(rtc_context* c, rtc_render_stats* out
         RTC_CUDA(cudaEventSynchronize(c->phase_ev[2]));
         RTC_CUDA(cudaEventElapsedTime(&out->bulk_ms, c->phase_ev[0], c->phase_ev[1]));
         RTC_CUDA(cudaEventElapsedTime(&out->drain_ms, c->phase_ev[1], c->phase_ev[2]));
+        out->extend_launches = c->kev_ext;
+        out->shade_launches = c->kev_shade;
+        for (uint32_t i = 0; i < c->kev_ext + c->kev_shade; ++i) {
+            float ms = 0.f;
+            RTC_CUDA(cudaEventElapsedTime(&ms, c->kev_pairs[i].first, c->kev_pairs[i].second));
+            if (i < c->kev_ext) out->extend_ms += ms;
+            else out->shade_ms += ms;
+        }
     }
     return RTC_OK;
 }
@@ -871,7 +1013,7 @@ extern "C" rtc_status rtc_launchGPU(const rtc_scene_desc* scene, int width, int 
     r = rtc_scene_create(c, scene, &s);
     if (r == RTC_OK) {
         rtc_render_params p{width, height, spp, max_depth, 2580u, RTC_MODE_COMPAT, RTC_DRAW_ORDER_DEVICE, 0,
-                            RTC_ENGINE_AUTO};
+                            RTC_ENGINE_AUTO, 0};
         std::vector<uint8_t> img((size_t)std::max(0, width) * std::max(0, height) * 3);
         if (!quiet_mode) std::printf("[INFO] Rendering %dx%d %d samples > %s\n", width, height, spp, filepath);
         r = rtc_render(c, s, &p, nullptr, img.data());

@@ -128,6 +128,10 @@ inline __host__ __device__ WfIter wf_iter(uint64_t k) {
 }
 
 // Counters (unsigned long long on device).
-enum CounterIdx { CNT_RAYS = 0, CNT_PATHS = 1, CNT_NODES = 2, CNT_PRIMS = 3, CNT_N = 4 };
+// Totals of the render, then the wavefront extend kernel's own share.
+enum CounterIdx {
+    CNT_RAYS = 0, CNT_PATHS = 1, CNT_NODES = 2, CNT_PRIMS = 3,
+    CNT_EXT_RAYS = 4, CNT_EXT_NODES = 5, CNT_EXT_PRIMS = 6, CNT_N = 8
+};
 
 }  // namespace rtc

@@ -1,0 +1,21 @@
+// rtc_internal.h - helpers shared by the C ABI translation units (not part of the public ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include "../../include/rtc.h"
+#include "rtc_dev.h"
+
+// bytes of wavefront scratch per path slot, and the layout of `slots` slots starting at `base`
+size_t rtc_wf_slot_bytes();
+size_t rtc_carve_wavefront(void* base, uint32_t slots, rtc::WfBuffers& B);
+// records an error message for rtc_last_error_string() and returns `s`
+rtc_status rtc_set_error(rtc_status s, const char* msg);
+rtc_status rtc_check_render_params(const rtc_render_params* p);
+int rtc_scene_device(const rtc_scene* s);
+// runs the wavefront engine on caller-provided buffers with synchronous queue polling: no device or
+// pinned allocations, no events
+rtc_status rtc_run_wavefront_sync(const rtc_scene* s, const rtc_render_params* p, const rtc::WfBuffers& B,
+                                  uint32_t* d_status, float4* d_out, cudaStream_t st);

@@ -48,11 +48,13 @@ __device__ __forceinline__ V3 random_in_unit_sphere(R& rng) {
     return p;
 }
 
-// cos/sin of random_cosine_direction: compat evaluates in double and rounds, which agrees with
-// glibc's cosf/sinf on ~98.7% of inputs and is within 1 ulp otherwise; clean uses sincosf.
-template <bool CLEAN>
+// Transcendentals follow the reference build being reproduced.  FLOAT_TRIG (the nvcc flavour and
+// clean mode): CUDA's float functions, as the reference's device build calls them.  Otherwise (the g++
+// flavour): evaluated in double and rounded, which agrees with glibc's cosf/sinf on ~98.7% of inputs
+// and is within 1 ulp otherwise.
+template <bool FLOAT_TRIG>
 __device__ __forceinline__ void cos_sin(float phi, float& c, float& s) {
-    if (CLEAN) {
+    if (FLOAT_TRIG) {
         sincosf(phi, &s, &c);
     } else {
         double sd, cd;
@@ -63,7 +65,7 @@ __device__ __forceinline__ void cos_sin(float phi, float& c, float& s) {
 }
 
 // random_cosine_direction (gpu_randomizer.cuh:121-133)
-template <bool CLEAN, class R>
+template <bool FLOAT_TRIG, class R>
 __device__ __forceinline__ V3 random_cosine_direction(R& rng) {
     const float r1 = rng.uniform();
     const float r2 = rng.uniform();
@@ -71,7 +73,7 @@ __device__ __forceinline__ V3 random_cosine_direction(R& rng) {
     const float z = sqrtf(1.0f - r2);
     const float r2s = sqrtf(r2);
     float c, s;
-    cos_sin<CLEAN>(phi, c, s);
+    cos_sin<FLOAT_TRIG>(phi, c, s);
     return v3(c * r2s, s * r2s, z);
 }
 
@@ -122,6 +124,24 @@ __device__ __forceinline__ Ray camera_ray(const DevCamera& c, float s, float t, 
     return r;
 }
 
+// Clean mode starts scattered rays from a point pushed off the surface along the normal of the side
+// the new ray leaves from: Waechter & Binder, "A Fast and Robust Method for Avoiding Self-Intersection",
+// Ray Tracing Gems (2019), ch. 6.  The offset is a fixed number of ulps of each coordinate (a fixed
+// distance near the origin), so whether the next ray re-hits its own surface no longer depends on
+// last-bit rounding.  Compat mode keeps the reference's start point and tmin = 1e-5 (constants.cuh:27).
+__device__ __forceinline__ float offset_coord(float p, float n) {
+    const float kOrigin = 1.0f / 32.0f, kFloatScale = 1.0f / 65536.0f, kIntScale = 256.0f;
+    const int of = (int)(kIntScale * n);
+    const float pi = __int_as_float(__float_as_int(p) + (p < 0.0f ? -of : of));
+    return fabsf(p) < kOrigin ? p + kFloatScale * n : pi;
+}
+template <bool CLEAN>
+__device__ __forceinline__ V3 scatter_origin(V3 p, V3 n, V3 dir) {
+    if (!CLEAN) return p;
+    const V3 side = dot(dir, n) < 0.0f ? neg(n) : n;
+    return v3(offset_coord(p.x, side.x), offset_coord(p.y, side.y), offset_coord(p.z, side.z));
+}
+
 struct PathCounters {
     uint32_t rays, nodes, prims;
 };
@@ -143,8 +163,9 @@ __device__ __forceinline__ bool shade_bounce(const DevScene& S, Ray& r, bool hit
         result.b += att.b * bg.b;
         return false;
     }
+    constexpr bool FT = CLEAN || ORDER == 0;   // float trig in the nvcc flavour and in clean mode
     Hit h;
-    finalize_hit(S, item, t, r.o, r.d, h);
+    finalize_hit<FT>(S, item, t, r.o, r.d, h);
     if ((uint32_t)h.mat >= S.num_materials) { status |= STATUS_BAD_MATERIAL; return false; }
     int4 mi = __ldg(S.mat_i + h.mat);
     float4 mf = __ldg(S.mat_f + h.mat);
@@ -166,7 +187,7 @@ __device__ __forceinline__ bool shade_bounce(const DevScene& S, Ray& r, bool hit
         uint32_t item2;
         pc.rays++;
         if (closest_hit(S, r.o, r.d, h.t + 0.001f, 3.402823466e+38f, hide, t2, item2, st, status)) {
-            finalize_hit(S, item2, t2, r.o, r.d, h);
+            finalize_hit<FT>(S, item2, t2, r.o, r.d, h);
             if ((uint32_t)h.mat >= S.num_materials) { status |= STATUS_BAD_MATERIAL; return false; }
             mi = __ldg(S.mat_i + h.mat);
             mf = __ldg(S.mat_f + h.mat);
@@ -182,8 +203,8 @@ __device__ __forceinline__ bool shade_bounce(const DevScene& S, Ray& r, bool hit
         RGB a = texture_value(S, mi.y, h.u, h.v, h.p, status);
         V3 refl = reflect(unit(r.d), h.n);
         V3 rs = random_in_unit_sphere<ORDER>(rng);
-        r.o = h.p;
         r.d = add(refl, mul(mf.x, rs));
+        r.o = scatter_origin<CLEAN>(h.p, h.n, r.d);
         att.r *= a.r;
         att.g *= a.g;
         att.b *= a.b;
@@ -208,8 +229,8 @@ __device__ __forceinline__ bool shade_bounce(const DevScene& S, Ray& r, bool hit
             float refl = r0 + (1.0f - r0) * p5;
             do_reflect = refl > rng.uniform();
         }
-        r.o = h.p;
         r.d = do_reflect ? reflect(ud, h.n) : refract(ud, h.n, ratio);
+        r.o = scatter_origin<CLEAN>(h.p, h.n, r.d);
         return true;   // attenuation (1,1,1)
     }
     // lambertian::scatter (lambertian.cuh:63-131): attenuation from the texture, cosine_pdf(normal)
@@ -227,13 +248,13 @@ __device__ __forceinline__ bool shade_bounce(const DevScene& S, Ray& r, bool hit
                 dir = light_random<ORDER>(S, 0, h.p, rng);
             }
         } else {
-            dir = onb_local(b, random_cosine_direction<CLEAN>(rng));
+            dir = onb_local(b, random_cosine_direction<FT>(rng));
         }
         float cosv = dot(unit(dir), b.w) / 3.14159265358979323846f;
         float cpdf = 0.0f > cosv ? 0.0f : cosv;   // ffmax(0, x) keeps NaN
         pdf_val = 0.5f * lights_pdf_value(S, h.p, dir) + (1.0f - 0.5f) * cpdf;
     } else {
-        dir = onb_local(b, random_cosine_direction<CLEAN>(rng));
+        dir = onb_local(b, random_cosine_direction<FT>(rng));
         float cosv = dot(unit(dir), b.w) / 3.14159265358979323846f;
         pdf_val = 0.0f > cosv ? 0.0f : cosv;
     }
@@ -245,7 +266,7 @@ __device__ __forceinline__ bool shade_bounce(const DevScene& S, Ray& r, bool hit
     att.r *= rcp * (a.r * spdf);
     att.g *= rcp * (a.g * spdf);
     att.b *= rcp * (a.b * spdf);
-    r.o = h.p;
+    r.o = scatter_origin<CLEAN>(h.p, h.n, dir);
     r.d = dir;
     return true;
 }

@@ -291,6 +291,7 @@ __device__ __forceinline__ bool closest_hit(const DevScene& S, V3 o, V3 d, float
 // Full hit record of the winning item: the part of each reference hit() that runs after the
 // interval test (sphere.cuh:137-165, quad.cuh:122-132, directional_light.cuh:113-120,
 // triangle.cuh:160-184).
+template <bool FLOAT_TRIG>
 __device__ __forceinline__ void finalize_hit(const DevScene& S, uint32_t it, float t, V3 o, V3 d, Hit& h) {
     uint32_t kind = it >> 30, idx = it & 0x3fffffffu;
     h.t = t;
@@ -304,9 +305,15 @@ __device__ __forceinline__ void finalize_hit(const DevScene& S, uint32_t it, flo
         V3 outward = divs(sub(h.p, c), s.w);
         set_face_normal(h, d, outward);
         // get_sphere_uv (uvmapping.cuh:204-228) with the default mapping (repeat 1, scale 1, offset 0);
-        // acos/atan2 evaluated in double and rounded, as close to glibc's float results as CUDA allows.
-        float theta = (float)acos((double)(-outward.y));
-        float phi = (float)atan2((double)(-outward.z), (double)outward.x) + 3.14159265358979323846f;
+        // float acos/atan2 for the nvcc flavour, double-evaluated for the g++ flavour (closest to glibc)
+        float theta, phi;
+        if (FLOAT_TRIG) {
+            theta = acosf(-outward.y);
+            phi = atan2f(-outward.z, outward.x) + 3.14159265358979323846f;
+        } else {
+            theta = (float)acos((double)(-outward.y));
+            phi = (float)atan2((double)(-outward.z), (double)outward.x) + 3.14159265358979323846f;
+        }
         float sc = phi / (2.0f * 3.14159265358979323846f);
         float tc = theta / 3.14159265358979323846f;
         sc = fmodf(sc * 1.0f, 1.0f);

@@ -120,7 +120,7 @@ __global__ void __launch_bounds__(128) wf_init(DevScene S, DevParams P, WfBuffer
     }
 }
 
-template <bool COUNT>
+template <bool COUNT, int FLAVOR>
 __global__ void __launch_bounds__(128) wf_extend(DevScene S, DevParams P, WfBuffers B, WfIter w,
                                                  unsigned long long* counters, uint32_t* status_word) {
     const uint32_t n = B.ctr[w.cin];
@@ -151,6 +151,9 @@ __global__ void __launch_bounds__(128) wf_extend(DevScene S, DevParams P, WfBuff
             atomicAdd(counters + CNT_RAYS, r);
             atomicAdd(counters + CNT_NODES, nn);
             atomicAdd(counters + CNT_PRIMS, pp);
+            atomicAdd(counters + CNT_EXT_RAYS, r);
+            atomicAdd(counters + CNT_EXT_NODES, nn);
+            atomicAdd(counters + CNT_EXT_PRIMS, pp);
         }
     }
     if (status) atomicOr(status_word, status);

@@ -1,4 +1,5 @@
-// wavefront_clean.cu - wavefront init/shade kernels in clean mode (FMA contraction allowed).
+// wavefront_clean.cu - wavefront init/shade/finish kernels in clean mode (FMA contraction on); the
+// extend pass is the nvcc-flavour one of wavefront_compat.cu.
 #include "rtc_kernels.h"
 #include "rtc_wavefront.cuh"
 

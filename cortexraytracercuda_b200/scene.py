@@ -22,6 +22,7 @@ MAT_LAMBERTIAN, MAT_METAL, MAT_DIELECTRIC, MAT_DIFFUSE_LIGHT = 0, 1, 2, 3
 BG_CONSTANT, BG_SKY_GRADIENT, BG_ENV_MAP = 0, 1, 2
 MODE_COMPAT, MODE_CLEAN = 0, 1
 ENGINE_AUTO, ENGINE_MEGAKERNEL, ENGINE_WAVEFRONT = 0, 1, 2
+FLAG_KERNEL_TIMING = 1
 DRAW_ORDER_DEVICE, DRAW_ORDER_HOST = 0, 1
 
 F3 = C.c_float * 3
@@ -85,12 +86,13 @@ class rtc_scene_desc(C.Structure):
 class rtc_render_params(C.Structure):
     _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("spp", C.c_int32), ("max_depth", C.c_int32),
                 ("seed", C.c_uint32), ("mode", C.c_int32), ("draw_order", C.c_int32),
-                ("block_size", C.c_int32), ("engine", C.c_int32)]
+                ("block_size", C.c_int32), ("engine", C.c_int32), ("flags", C.c_int32)]
 
 
 class rtc_render_stats(C.Structure):
     _fields_ = [("iterations", C.c_uint32), ("launches", C.c_uint32), ("drained_slots", C.c_uint32),
-                ("engine", C.c_uint32), ("bulk_ms", C.c_float), ("drain_ms", C.c_float)]
+                ("engine", C.c_uint32), ("bulk_ms", C.c_float), ("drain_ms", C.c_float), ("extend_ms", C.c_float),
+                ("shade_ms", C.c_float), ("extend_launches", C.c_uint32), ("shade_launches", C.c_uint32)]
 
 
 class rtc_scene_info(C.Structure):
@@ -134,10 +136,11 @@ class RenderParams:
     draw_order: int = DRAW_ORDER_DEVICE
     block_size: int = 0
     engine: int = ENGINE_AUTO
+    flags: int = 0
 
     def to_c(self) -> rtc_render_params:
         return rtc_render_params(self.width, self.height, self.spp, self.max_depth, self.seed & 0xFFFFFFFF,
-                                 self.mode, self.draw_order, self.block_size, self.engine)
+                                 self.mode, self.draw_order, self.block_size, self.engine, self.flags)
 
     @property
     def traced_spp(self) -> int:

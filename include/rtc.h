@@ -220,7 +220,12 @@ typedef struct rtc_render_params {
     int32_t draw_order;    /* rtc_draw_order (COMPAT only)                                           */
     int32_t block_size;    /* 0 = library default                                                    */
     int32_t engine;        /* rtc_engine                                                             */
+    int32_t flags;         /* RTC_FLAG_* bits                                                        */
 } rtc_render_params;
+
+/* Record CUDA events around every extend and shade launch of the wavefront engine; the per-kernel
+ * device times are then reported by rtc_get_render_stats (extend_ms / shade_ms / *_launches). */
+#define RTC_FLAG_KERNEL_TIMING 1
 
 /* ------------------------------------------------------------------------------------------------ */
 /* context and scenes                                                                                */
@@ -264,8 +269,9 @@ rtc_status rtc_render(rtc_context* ctx, const rtc_scene* scene, const rtc_render
 
 /* Same render with DEVICE output buffers (inputs already resident), on `stream`
  * (a cudaStream_t, or NULL for the context's stream).  d_radiance_sum must hold width*height
- * float4; d_rgb8 may be NULL.  d_counters, when not NULL, receives 4 uint64 counters: rays traced
- * (closest-hit traversals), paths traced, BVH nodes visited, primitive tests.  The megakernel engine
+ * float4; d_rgb8 may be NULL.  d_counters, when not NULL, must hold 8 uint64 (zeroed by the caller)
+ * and receives: rays traced (closest-hit traversals), paths traced, BVH nodes visited, primitive
+ * tests, then the wavefront extend kernel's own rays, node visits and primitive tests, one unused.  The megakernel engine
  * returns without waiting for the GPU; the wavefront engine polls its queue counter between batches
  * of iterations and returns once the frame is complete. */
 rtc_status rtc_render_device(rtc_context* ctx, const rtc_scene* scene, const rtc_render_params* params,
@@ -282,6 +288,10 @@ typedef struct rtc_render_stats {
     uint32_t engine;
     float bulk_ms;
     float drain_ms;
+    float extend_ms;           /* with RTC_FLAG_KERNEL_TIMING: summed device time of the extend launches */
+    float shade_ms;            /* ... of the shade launches                                              */
+    uint32_t extend_launches;
+    uint32_t shade_launches;
 } rtc_render_stats;
 rtc_status rtc_get_render_stats(rtc_context* ctx, rtc_render_stats* stats);
 

@@ -518,6 +518,25 @@ static onb_t build_from_w(v3 n) {   /* onb::build_from_w (onb.cuh:122-128) */
 }
 static v3 onb_local(const onb_t* b, v3 a) { return vadd(vadd(vscale(a.x, b->u), vscale(a.y, b->v)), vscale(a.z, b->w)); }
 
+/* Clean mode: scattered rays start from a point offset along the normal of the side they leave from,
+   Waechter & Binder, "A Fast and Robust Method for Avoiding Self-Intersection", Ray Tracing Gems
+   (2019), ch. 6.  Compat mode starts them at the hit point (the reference's behaviour). */
+static inline float offset_coord(float p, float n) {
+    const float kOrigin = 1.0f / 32.0f, kFloatScale = 1.0f / 65536.0f, kIntScale = 256.0f;
+    int of = (int)(kIntScale * n);
+    int32_t bits;
+    memcpy(&bits, &p, 4);
+    bits += (p < 0.0f ? -of : of);
+    float pi;
+    memcpy(&pi, &bits, 4);
+    return fabsf(p) < kOrigin ? p + kFloatScale * n : pi;
+}
+static inline v3 scatter_origin(int clean, v3 p, v3 n, v3 dir) {
+    if (!clean) return p;
+    v3 side = vdot(dir, n) < 0.0f ? vneg(n) : n;
+    return V(offset_coord(p.x, side.x), offset_coord(p.y, side.y), offset_coord(p.z, side.z));
+}
+
 /* camera::ray_color (camera.cuh:149-264) for one sample; returns radiance, counts closest-hit calls */
 static rgb_t ray_color(const scene_t* s, v3 o, v3 d, int max_depth, rng_t* rng, int order, int clean, uint64_t* rays) {
     rgb_t res = {0, 0, 0}, att = {1, 1, 1};
@@ -558,8 +577,8 @@ static rgb_t ray_color(const scene_t* s, v3 o, v3 d, int max_depth, rng_t* rng, 
                 draw3(rng, order, &x, &y, &z);
                 p = V(2.0f * x - 1.0f, 2.0f * y - 1.0f, 2.0f * z - 1.0f);
             } while (p.x * p.x + p.y * p.y + p.z * p.z >= 1.0f);
-            o = h.p;
             d = vadd(refl, vscale(m->fuzz, p));
+            o = scatter_origin(clean, h.p, h.n, d);
             att.r *= a.r; att.g *= a.g; att.b *= a.b;
             continue;
         }
@@ -576,8 +595,8 @@ static rgb_t ray_color(const scene_t* s, v3 o, v3 d, int max_depth, rng_t* rng, 
                 float refl = r0 + (1 - r0) * (float)(pow((1 - cos_theta), 5));
                 reflect = refl > U(rng);
             }
-            o = h.p;
             d = reflect ? vreflect(ud, h.n) : vrefract(ud, h.n, ratio);
+            o = scatter_origin(clean, h.p, h.n, d);
             continue;
         }
         /* lambertian (lambertian.cuh:63-143) + mixture_pdf(hittable_pdf(lights), cosine_pdf) */
@@ -615,7 +634,7 @@ static rgb_t ray_color(const scene_t* s, v3 o, v3 d, int max_depth, rng_t* rng, 
         float spdf = cth < 0 ? 0.0f : cth / PI_F;
         float rcp = 1 / pdf_val;
         att.r *= rcp * (a.r * spdf); att.g *= rcp * (a.g * spdf); att.b *= rcp * (a.b * spdf);
-        o = h.p;
+        o = scatter_origin(clean, h.p, h.n, dir);
         d = dir;
     }
     return res;

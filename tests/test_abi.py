@@ -44,7 +44,7 @@ def test_every_declared_symbol_is_exported(lib):
 
 def test_struct_sizes_match_header(lib):
     # the ctypes mirror and the C layout agree on the sizes the ABI depends on
-    assert C.sizeof(rtc_render_params) == 9 * 4
+    assert C.sizeof(rtc_render_params) == 10 * 4
 
 
 def test_null_arguments_are_rejected(lib):
