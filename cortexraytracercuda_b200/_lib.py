@@ -13,6 +13,8 @@ from .scene import rtc_render_params, rtc_render_stats, rtc_scene_desc, rtc_scen
 
 LIB_PATH = Path(__file__).resolve().parent / "librtc_b200.so"
 
+# include/rtc.h: RTC_NOALLOC_MAX_PIXELS
+NOALLOC_MAX_PIXELS = 524264
 
 STATUS_NAMES = {0: "RTC_OK", 1: "RTC_ERR_INVALID_ARGUMENT", 2: "RTC_ERR_BAD_SCENE", 3: "RTC_ERR_CUDA",
                 4: "RTC_ERR_OOM", 5: "RTC_ERR_TIMEOUT", 6: "RTC_ERR_NO_DEVICE", 7: "RTC_ERR_IO",
@@ -29,6 +31,7 @@ PROTOTYPES = {
     "rtc_scene_get_info": (C.c_int, [_P, C.POINTER(rtc_scene_info)]),
     "rtc_render": (C.c_int, [_P, _P, C.POINTER(rtc_render_params), _P, _P]),
     "rtc_render_device": (C.c_int, [_P, _P, C.POINTER(rtc_render_params), _P, _P, _P, _P]),
+    "rtc_render_noalloc": (C.c_int, [_P, C.POINTER(rtc_render_params), _P, _P]),
     "rtc_get_render_stats": (C.c_int, [_P, C.POINTER(rtc_render_stats)]),
     "rtc_trace_closest": (C.c_int, [_P, _P, _P, C.c_uint32, C.c_int32, C.c_int32, _P, _P]),
     "rtc_launchGPU": (C.c_int, [C.POINTER(rtc_scene_desc), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,

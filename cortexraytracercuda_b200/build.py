@@ -39,6 +39,7 @@ SOURCES = [
     ("wavefront_compat.cu", "wavefront_compat_dev", "nvcc", ["--fmad=true", "-DRTC_FLAVOR=0"]),
     ("render_clean.cu", "render_clean", "nvcc", ["--fmad=true"]),
     ("wavefront_clean.cu", "wavefront_clean", "nvcc", ["--fmad=true"]),
+    ("render_noalloc.cu", "render_noalloc", "nvcc", []),
     ("rtc_api.cpp", "rtc_api", "cxx", []),
     ("bvh_build.cpp", "bvh_build", "cxx", []),
 ]

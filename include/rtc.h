@@ -295,6 +295,22 @@ typedef struct rtc_render_stats {
 } rtc_render_stats;
 rtc_status rtc_get_render_stats(rtc_context* ctx, rtc_render_stats* stats);
 
+/* Allocation-free render.  No counterpart in the reference: an addition for callers that cannot
+ * allocate device memory when they render - code living under a memory budget fixed at start-up, a
+ * process whose device allocator belongs to another framework, or a render issued where a cudaMalloc
+ * would synchronise the device.  It runs the same wavefront kernels as rtc_render_device (same
+ * results), with their path state in a 64 MiB static device array that every GPU loading this
+ * library holds until exit, so it renders at most RTC_NOALLOC_MAX_PIXELS pixels per call (one path
+ * slot per pixel) and rejects larger images with RTC_ERR_INVALID_ARGUMENT.  It allocates nothing
+ * and needs no context: the scene (already on its device) and the 16-byte aligned device output
+ * (width*height float4, frame-buffer order) come from the caller; `stream` may be NULL (legacy
+ * stream).  The first call on a device looks up the array's address; make it before any stream
+ * capture.  All calls share the array, so calls that overlap on the GPU race.  Returns when the frame
+ * is complete. */
+#define RTC_NOALLOC_MAX_PIXELS 524264u
+rtc_status rtc_render_noalloc(const rtc_scene* scene, const rtc_render_params* params, float* d_radiance_sum,
+                              void* stream);
+
 /* Closest-hit queries on arbitrary rays (hit-identity tests).  rays: n x 8 floats
  * (ox, oy, oz, tmin, dx, dy, dz, tmax) in host memory; `depth`/`max_depth` decide light visibility as
  * in the reference's world.hit (directional_light.cuh:106).  Outputs (host, n each, may be NULL):
