@@ -20,7 +20,16 @@ roofline: algorithmic bytes of the render kernel per launch (BVH node visits x 6
 cpu_baseline: the reference's own CPU code (oracle/_ref/libref_cpu.so: the reference's classes built
          with g++) on all host cores, on a deterministic pixel subsample of the same frame.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--config spheres|cornell|meshes] [--impl ours|reference]
+  batched            64 heterogeneous scenes (1K-500K triangles, 256^2..1024^2, spp 4/16/64, depth
+                     8-32, seed 20261203) rendered as one batch per step through rtc_render_batch, against
+                     the plain form: the same 64 images one rtc_render_device call each.
+  served             Poisson request streams (rate --lambdas, --requests each) over the batched scenes
+                     (Zipf s=1.1 popularity, orbiting cameras, each scene's resolution/spp/depth) through
+                     the render server; p50/p95/p99 latency and Mpaths/s, against a plain server that
+                     renders one request per launch in arrival order.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--config spheres|cornell|meshes|batched|served]
+                  [--impl ours|reference]
 """
 from __future__ import annotations
 
@@ -194,12 +203,288 @@ def run_reference_arm(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def _mode_order(args):
+    return (MODE_CLEAN, DRAW_ORDER_DEVICE) if args.mode == "clean" else (MODE_COMPAT, DRAW_ORDER_DEVICE)
+
+
+def _init_dist(world, local):
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    return dist
+
+
+def _max_over_ranks(x, world):
+    import torch
+    import torch.distributed as dist
+    if world == 1:
+        return x
+    t = torch.tensor([x], device="cuda", dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def run_batched(args, rank, world, local):
+    """64 heterogeneous images per step: one rtc_render_batch call vs one plain launch per image."""
+    import torch
+    from cortexraytracercuda_b200.renderer import Context, DeviceScene, Job
+    dist = _init_dist(world, local)
+    mode, order = _mode_order(args)
+    ctx = Context(local)
+    work = configs.batch_workload(args.scenes)
+    t0 = time.perf_counter()
+    dss = [DeviceScene(ctx, sc) for sc, _ in work]
+    setup_s = time.perf_counter() - t0
+    params = []
+    for _, p in work:
+        p.mode, p.draw_order, p.engine = mode, order, ENGINE_WAVEFRONT
+        params.append(p)
+    outs = [torch.empty((p.height, p.width, 4), dtype=torch.float32, device="cuda") for p in params]
+    plain_outs = [torch.empty_like(o) for o in outs]
+    jobs = [Job(ds, p, o.data_ptr()) for ds, p, o in zip(dss, params, outs)]
+    paths = sum(p.width * p.height * p.traced_spp for p in params)
+    pixels = sum(p.width * p.height for p in params)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    sp = stream.cuda_stream
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def batched():
+        ctx.render_batch(jobs, slots=args.slots, drain=args.drain, stream=sp)
+
+    def plain():
+        for ds, p, o in zip(dss, params, plain_outs):
+            ds.render_device(p, o.data_ptr(), stream=sp)
+
+    def timed(fn, steps):
+        evs = []
+        for k in range(steps):
+            flush.fill_(float(k))
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            evs.append((a, b))
+        torch.cuda.synchronize()
+        return [a.elapsed_time(b) for a, b in evs]
+
+    for _ in range(args.warmup):
+        batched()
+    plain()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    if world > 1:
+        dist.barrier()
+    stats = []
+    b_ms = timed(lambda: (batched(), stats.append(ctx.last_stats())), args.steps)
+    p_steps = max(1, min(args.steps, 2))
+    p_ms = timed(plain, p_steps)
+    clk = clocks.stop()
+    b_tot = _max_over_ranks(float(np.sum(b_ms)), world)
+    p_tot = _max_over_ranks(float(np.sum(p_ms)), world)
+    value = paths * world * args.steps / (b_tot / 1e3) / 1e6
+    plain_value = paths * world * p_steps / (p_tot / 1e3) / 1e6
+    # same images: bit-identical pixels and image-mean agreement of batched vs plain
+    same, mean_dev = [], []
+    for o, q in zip(outs, plain_outs):
+        a, b = o[..., :3].double().nan_to_num(), q[..., :3].double().nan_to_num()
+        same.append(float((a == b).all(-1).float().mean()))
+        mean_dev.append(float((a.mean() - b.mean()).abs() / b.mean().clamp_min(1e-9)))
+    # end to end: the batch with every image copied to pinned host memory
+    host = [torch.empty(o.shape, dtype=torch.float32, pin_memory=True) for o in outs]
+    e2e = []
+    for k in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        batched()
+        for h, o in zip(host, outs):
+            h.copy_(o, non_blocking=True)
+        torch.cuda.synchronize()
+        if k >= args.warmup:
+            e2e.append(time.perf_counter() - t)
+    e2e_tot = _max_over_ranks(float(np.sum(e2e)), world)
+    import ctypes as C
+    from cortexraytracercuda_b200.scene import rtc_job
+    line = {"metric": METRIC, "value": round(value, 3), "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(b_tot / args.steps, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"batched: {len(work)} scenes, {pixels} pixels, {paths} paths per step",
+                       "triangles": int(sum(sc.num_triangles for sc, _ in work)),
+                       "mode": "compat" if mode == MODE_COMPAT else "clean",
+                       "slots": args.slots or "default", "drain": args.drain or "default",
+                       "l2": "flushed between steps (256 MiB write)", "seed": configs.DEFAULT_SEED,
+                       "parallelism": f"replicas x{world}"},
+            "plain": {"value": round(plain_value, 3), "unit": METRIC, "ms_per_step": round(p_tot / p_steps, 3),
+                      "form": "one rtc_render_device per image"},
+            "batched_over_plain": round(value / plain_value, 3),
+            "equal_to_plain": {"bit_identical_pixels_min": round(min(same), 4),
+                               "image_mean_rel_dev_max": round(max(mean_dev), 6)},
+            "gpu_launches": int(sum(st["launches"] for st in stats)),
+            "iterations": int(np.mean([st["iterations"] for st in stats])),
+            "e2e": {"value": round(paths * world * args.steps / e2e_tot / 1e6, 3), "unit": METRIC,
+                    "h2d_bytes_per_step": len(jobs) * C.sizeof(rtc_job), "d2h_bytes_per_step": pixels * 16},
+            "setup_s": round(setup_s, 2), "clocks": clk, "roofline": None, "cpu_baseline": None}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    for ds in dss:
+        ds.close()
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def _zipf_weights(n, s=1.1):
+    w = 1.0 / np.arange(1, n + 1) ** s
+    return w / w.sum()
+
+
+def _percentiles(lat):
+    lat = np.asarray(lat, np.float64)
+    return {"p50_ms": round(float(np.percentile(lat, 50)), 2), "p95_ms": round(float(np.percentile(lat, 95)), 2),
+            "p99_ms": round(float(np.percentile(lat, 99)), 2), "mean_ms": round(float(lat.mean()), 2)}
+
+
+def run_served(args, rank, world, local):
+    """Poisson request streams through the render server vs a plain one-request-per-launch server."""
+    import torch
+    from cortexraytracercuda_b200.renderer import Context, DeviceScene, Job, RenderServer
+    dist = _init_dist(world, local)
+    mode, order = _mode_order(args)
+    work = configs.batch_workload(args.scenes)
+    srv = RenderServer(local, mode=mode, draw_order=order, slots=args.slots)
+    t0 = time.perf_counter()
+    ids = [srv.add_scene(sc) for sc, _ in work]
+    setup_s = time.perf_counter() - t0
+    ctx = Context(local)
+    dss = [DeviceScene(ctx, sc) for sc, _ in work]   # the plain server's resident scenes
+    weights = _zipf_weights(len(work))
+    rng = np.random.default_rng(configs.DEFAULT_SEED + rank)
+    pools = {}
+
+    def take(shape):
+        lst = pools.setdefault(shape, [])
+        return lst.pop() if lst else torch.empty(shape, dtype=torch.float32, pin_memory=True)
+
+    def stream_of(lam, n):
+        arr = np.cumsum(rng.exponential(1.0 / lam, n))
+        sc = rng.choice(len(work), n, p=weights)
+        ang = rng.uniform(0.0, 2.0 * np.pi, n)
+        return arr, sc, ang
+
+    def request(k, sc, ang):
+        cam = configs.orbit_camera(work[sc][0].camera, float(ang))
+        p = work[sc][1]
+        rp = p.__class__(**{**p.__dict__, "mode": mode, "draw_order": order, "engine": ENGINE_WAVEFRONT})
+        return rp, cam
+
+    # warm-up: every scene once (uploads), not timed
+    for k in range(len(work)):
+        rp, cam = request(k, k, 0.0)
+        out = take((rp.height, rp.width, 4))
+        srv.wait(srv.submit(ids[k], rp, cam, out)[0])
+        pools[(rp.height, rp.width, 4)].append(out)
+    per_rate = {}
+    clocks = ClockSampler(local)
+    clocks.start()
+    for lam in [float(x) for x in args.lambdas.split(",")]:
+        arr, scs, angs = stream_of(lam, args.requests)
+        tickets = []
+        lock = threading.Lock()
+
+        def submitter():
+            start = time.perf_counter()
+            for k in range(len(arr)):
+                dt = arr[k] - (time.perf_counter() - start)
+                if dt > 0:
+                    time.sleep(dt)
+                rp, cam = request(k, scs[k], angs[k])
+                with lock:
+                    out = take((rp.height, rp.width, 4))
+                t, _ = srv.submit(ids[scs[k]], rp, cam, out)
+                with lock:
+                    tickets.append((t, out, rp.width * rp.height * rp.traced_spp))
+
+        th = threading.Thread(target=submitter)
+        th.start()
+        lat, first, last, total, k = [], None, 0.0, 0, 0
+        while k < len(arr):
+            with lock:
+                have = len(tickets)
+            if k >= have:
+                time.sleep(0.0005)
+                continue
+            t, out, npaths = tickets[k]
+            _, info = srv.wait(t)
+            with lock:
+                pools[tuple(out.shape)].append(out)
+            lat.append(info["done_ms"] - info["submit_ms"])
+            first = info["submit_ms"] if first is None else min(first, info["submit_ms"])
+            last = max(last, info["done_ms"])
+            total += npaths
+            k += 1
+        th.join()
+        served = {"requests": len(arr), **_percentiles(lat), "mpaths_per_s": round(total / ((last - first) / 1e3) / 1e6, 3),
+                  "offered_mpaths_per_s": round(total / arr[-1] / 1e6, 3)}
+        # plain comparison: one launch per request, in arrival order, same stream prefix
+        n_plain = min(args.plain_requests, len(arr))
+        plat, ptotal = [], 0
+        start = time.perf_counter()
+        busy_until = 0.0
+        for q in range(n_plain):
+            now = time.perf_counter() - start
+            if arr[q] > now:
+                time.sleep(arr[q] - now)
+            rp, cam = request(q, scs[q], angs[q])
+            out = torch.empty((rp.height, rp.width, 4), dtype=torch.float32, device="cuda")
+            host = take((rp.height, rp.width, 4))
+            ds = dss[int(scs[q])]
+            ctx.render_batch([Job(ds, rp, out.data_ptr(), cam)], slots=1 << 20)   # one image per launch
+            host.copy_(out)
+            pools[tuple(host.shape)].append(host)
+            done = time.perf_counter() - start
+            plat.append((done - arr[q]) * 1e3)
+            ptotal += rp.width * rp.height * rp.traced_spp
+            busy_until = done
+        plain = {"requests": n_plain, **_percentiles(plat),
+                 "mpaths_per_s": round(ptotal / (busy_until - arr[0]) / 1e6, 3)}
+        per_rate[str(int(lam))] = {"served": served, "plain": plain,
+                                   "served_over_plain": round(served["mpaths_per_s"] / plain["mpaths_per_s"], 3)}
+    clk = clocks.stop()
+    st = srv.stats()
+    top = per_rate[max(per_rate, key=lambda x: float(x))]
+    line = {"metric": METRIC, "value": top["served"]["mpaths_per_s"], "unit": METRIC, "n_gpus": world,
+            "steps": len(per_rate), "warmup": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"served: Poisson streams over {len(work)} batched scenes, Zipf s=1.1, "
+                                   f"orbit cameras, {args.requests} requests per rate",
+                       "mode": "compat" if mode == MODE_COMPAT else "clean", "slots": args.slots or "default",
+                       "hbm_budget": "120 GB", "parallelism": f"replicas x{world}", "seed": configs.DEFAULT_SEED},
+            "rates": per_rate, "server": {k: st[k] for k in ("completed", "failed", "scene_uploads", "scene_evictions",
+                                                             "peak_resident_bytes", "iterations", "launches")},
+            "gpu_launches": int(st["launches"]),
+            "e2e": {"value": top["served"]["mpaths_per_s"], "unit": METRIC, "h2d_bytes_per_step": None,
+                    "d2h_bytes_per_step": None, "note": "requests in, radiance in pinned host buffers out"},
+            "setup_s": round(setup_s, 2), "clocks": clk, "roofline": None, "cpu_baseline": None}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    srv.close()
+    for ds in dss:
+        ds.close()
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--config", default="spheres", choices=["spheres", "cornell", "meshes"])
+    ap.add_argument("--config", default="spheres", choices=["spheres", "cornell", "meshes", "batched", "served"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--mode", default="compat", choices=["compat", "clean"])
     ap.add_argument("--engine", default="wavefront", choices=["wavefront", "megakernel"])
@@ -208,6 +493,12 @@ def main():
     ap.add_argument("--ref-step-s", type=float, default=8.0)
     ap.add_argument("--small", action="store_true", help="quarter-size frame, 16 spp (profiling captures)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling captures)")
+    ap.add_argument("--scenes", type=int, default=64, help="batched/served: number of scenes")
+    ap.add_argument("--slots", type=int, default=0, help="batched/served: path slots (0: library default)")
+    ap.add_argument("--drain", type=int, default=0, help="batched: drain threshold (0: default, 1: no drain)")
+    ap.add_argument("--lambdas", default="50,200,800", help="served: request rates (1/s)")
+    ap.add_argument("--requests", type=int, default=300, help="served: requests per rate")
+    ap.add_argument("--plain-requests", type=int, default=120, help="served: requests of the plain comparison")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -218,6 +509,12 @@ def main():
 
     if args.impl == "reference":
         run_reference_arm(args, rank, world)
+        return
+    if args.config == "batched":
+        run_batched(args, rank, world, local)
+        return
+    if args.config == "served":
+        run_served(args, rank, world, local)
         return
 
     import torch

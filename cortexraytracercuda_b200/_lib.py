@@ -9,7 +9,8 @@ import ctypes as C
 import os
 from pathlib import Path
 
-from .scene import rtc_render_params, rtc_render_stats, rtc_scene_desc, rtc_scene_info
+from .scene import (rtc_batch_params, rtc_job, rtc_render_params, rtc_render_stats, rtc_request, rtc_request_info,
+                    rtc_scene_desc, rtc_scene_info, rtc_server_config, rtc_server_stats)
 
 LIB_PATH = Path(__file__).resolve().parent / "librtc_b200.so"
 
@@ -33,6 +34,14 @@ PROTOTYPES = {
     "rtc_render_device": (C.c_int, [_P, _P, C.POINTER(rtc_render_params), _P, _P, _P, _P]),
     "rtc_render_noalloc": (C.c_int, [_P, C.POINTER(rtc_render_params), _P, _P]),
     "rtc_get_render_stats": (C.c_int, [_P, C.POINTER(rtc_render_stats)]),
+    "rtc_render_batch": (C.c_int, [_P, C.POINTER(rtc_job), C.c_uint32, C.POINTER(rtc_batch_params), _P]),
+    "rtc_server_create": (C.c_int, [C.POINTER(rtc_server_config), C.POINTER(C.c_void_p)]),
+    "rtc_server_destroy": (C.c_int, [_P]),
+    "rtc_server_add_scene": (C.c_int, [_P, C.POINTER(rtc_scene_desc), C.POINTER(C.c_uint32)]),
+    "rtc_server_submit": (C.c_int, [_P, C.POINTER(rtc_request), _P, C.POINTER(C.c_uint64)]),
+    "rtc_server_poll": (C.c_int, [_P, C.c_uint64, C.POINTER(rtc_request_info)]),
+    "rtc_server_wait": (C.c_int, [_P, C.c_uint64, C.c_int32, C.POINTER(rtc_request_info)]),
+    "rtc_server_get_stats": (C.c_int, [_P, C.POINTER(rtc_server_stats)]),
     "rtc_trace_closest": (C.c_int, [_P, _P, _P, C.c_uint32, C.c_int32, C.c_int32, _P, _P]),
     "rtc_launchGPU": (C.c_int, [C.POINTER(rtc_scene_desc), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                 C.c_char_p, C.c_int]),

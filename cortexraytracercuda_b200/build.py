@@ -13,6 +13,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
@@ -41,10 +42,13 @@ SOURCES = [
     ("wavefront_clean.cu", "wavefront_clean", "nvcc", ["--fmad=true"]),
     ("render_noalloc.cu", "render_noalloc", "nvcc", []),
     ("rtc_api.cpp", "rtc_api", "cxx", []),
+    ("rtc_engine.cpp", "rtc_engine", "cxx", []),
+    ("rtc_batch.cpp", "rtc_batch", "cxx", []),
+    ("rtc_server.cpp", "rtc_server", "cxx", []),
     ("bvh_build.cpp", "bvh_build", "cxx", []),
 ]
 HEADERS = ["rtc_dev.h", "rtc_math.cuh", "rtc_trace.cuh", "rtc_path.cuh", "rtc_wavefront.cuh", "rtc_kernels.h",
-           "bvh_build.h", "rtc_internal.h"]
+           "bvh_build.h", "rtc_internal.h", "rtc_objects.h", "rtc_engine.h"]
 
 
 def _newer(target: Path, deps) -> bool:
@@ -71,6 +75,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
     BUILD.mkdir(exist_ok=True)
     headers = [CSRC / h for h in HEADERS] + [INCLUDE / "rtc.h"]
     objs = []
+    cmds = []
     for src, obj, comp, extra in SOURCES:
         s = CSRC / src
         o = BUILD / (obj + ".o")
@@ -81,7 +86,12 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
             cmd = [NVCC] + NVCC_COMMON + extra + (["-Xptxas", "-v"] if ptxas_verbose else []) + ["-c", str(s), "-o", str(o)]
         else:
             cmd = [CXX] + CXX_FLAGS + extra + ["-c", str(s), "-o", str(o)]
-        _run(cmd, verbose or ptxas_verbose)
+        cmds.append(cmd)
+    # independent translation units compile in parallel
+    workers = max(1, min(len(cmds), os.cpu_count() or 1))
+    with ThreadPoolExecutor(max_workers=workers) as ex:
+        for f in [ex.submit(_run, cmd, verbose or ptxas_verbose) for cmd in cmds]:
+            f.result()
     if force or _newer(LIB, objs):
         tmp = LIB.with_suffix(".so.tmp")
         cmd = [NVCC, "-shared"] + ARCH + ["-o", str(tmp)] + [str(o) for o in objs] + ["-cudart", "static", "-lpthread"]

@@ -20,6 +20,12 @@ sizes and value distributions follow the workloads the library is measured on:
                      2048x1024 FP32 equirectangular environment map (sky gradient + Gaussian sun lobe);
                      1920x1080, 128 spp, depth 16.
 * ``textured``     - spheres and quads with checker and image textures (parity of the texture paths).
+* batched workload (:func:`batch_workload`) - 64 heterogeneous scenes drawn from the seed: triangle
+                     counts log-uniform in [1K, 500K] (instances of one displaced icosphere level) plus
+                     20-120 random r=0.2 spheres, the ``spheres`` material mix (80/15/5 %), a ground
+                     sphere, a quad light and a sky; resolutions uniform over {256^2, 512^2, 768x432,
+                     1024^2}, spp uniform over {4, 16, 64}, depth uniform in 8..32.  The served workload
+                     draws requests over these scenes (Zipf popularity, orbiting cameras).
 * ``icosphere``    - a 1,280-triangle icosphere with lambertian, metal and dielectric instances.
 """
 from __future__ import annotations
@@ -276,6 +282,75 @@ def icosphere_scene(level=3, seed=DEFAULT_SEED) -> Scene:
                       aperture=0.05, focus=7.0)
     s.set_background_constant((0.3, 0.35, 0.45))
     return s
+
+
+# -------------------------------------------------------------------------------------------------
+# batched / served workload
+# -------------------------------------------------------------------------------------------------
+BATCH_RESOLUTIONS = [(256, 256), (512, 512), (768, 432), (1024, 1024)]
+BATCH_SPP = [4, 16, 64]
+_ICO_CACHE: dict = {}
+
+
+def _mix_material(s: Scene, rng) -> int:
+    """The ``spheres`` material mix: 80% lambertian (albedo U^3*U^3), 15% metal, 5% dielectric."""
+    choose = rng.random()
+    if choose < 0.8:
+        return s.lambertian(tuple(rng.random(3) * rng.random(3)))
+    if choose < 0.95:
+        return s.metal(tuple(0.5 + 0.5 * rng.random(3)), 0.5 * rng.random())
+    return s.dielectric(1.5)
+
+
+def _cached_icosphere(level: int, seed: int):
+    key = (level, seed)
+    if key not in _ICO_CACHE:
+        _ICO_CACHE[key] = displaced_icosphere(level, 0.15, seed)
+    return _ICO_CACHE[key]
+
+
+def batch_scene(k: int, seed=DEFAULT_SEED):
+    """Scene `k` of the batched workload and its render parameters (see the module docstring)."""
+    rng = np.random.default_rng([seed, k])
+    target = math.exp(rng.uniform(math.log(1e3), math.log(5e5)))
+    level, count = min(((lv, n) for lv in range(3, 8) for n in range(1, 5) if n * 20 * 4 ** lv <= 5e5),
+                       key=lambda ln: abs(math.log(ln[1] * 20 * 4 ** ln[0] / target)))
+    v, f = _cached_icosphere(level, seed)
+    s = Scene(name=f"batch{k}")
+    s.dir_light((0.0, 12.0, 0.0), (8.0, 0.0, 0.0), (0.0, 0.0, 8.0), (5.0, 5.0, 5.0), intensity=1.5, invisible=True)
+    s.sphere((0.0, -1000.0, 0.0), 1000.0, s.lambertian((0.5, 0.5, 0.5)))
+    for i in range(count):
+        x = (i - (count - 1) / 2.0) * 2.4
+        scale = 0.8 + 0.4 * rng.random()
+        s.mesh((v * scale + np.array([x, scale * 1.15, 0.0])).astype(np.float32), f, _mix_material(s, rng))
+    for _ in range(int(rng.integers(20, 121))):
+        c = (rng.uniform(-7.0, 7.0), 0.2, rng.uniform(-7.0, 7.0))
+        if abs(c[2]) < 1.6 and abs(c[0]) < 1.3 * count + 0.3:
+            continue   # keep the instances' footprint clear
+        s.sphere(c, 0.2, _mix_material(s, rng))
+    w, h = BATCH_RESOLUTIONS[int(rng.integers(len(BATCH_RESOLUTIONS)))]
+    angle = rng.uniform(0.0, 2.0 * math.pi)
+    dist = 10.0 + 2.0 * count
+    s.camera = Camera(look_from=(dist * math.sin(angle), 3.0, dist * math.cos(angle)), look_at=(0.0, 1.0, 0.0),
+                      up=(0, 1, 0), vfov=30.0, aspect=w / h, aperture=0.05, focus=dist)
+    s.set_background_sky()
+    params = RenderParams(width=w, height=h, spp=int(BATCH_SPP[int(rng.integers(len(BATCH_SPP)))]),
+                          max_depth=int(rng.integers(8, 33)))
+    return s, params
+
+
+def batch_workload(n=64, seed=DEFAULT_SEED):
+    """The batched workload: a list of (scene, params) for n scenes."""
+    return [batch_scene(k, seed) for k in range(n)]
+
+
+def orbit_camera(cam: Camera, angle: float, center=(0.0, 1.0, 0.0)) -> Camera:
+    """`cam` rotated by `angle` radians about the vertical axis through `center` (served requests)."""
+    f = np.asarray(cam.look_from, np.float64) - np.asarray(center, np.float64)
+    ca, sa = math.cos(angle), math.sin(angle)
+    r = np.array([ca * f[0] + sa * f[2], f[1], -sa * f[0] + ca * f[2]]) + np.asarray(center, np.float64)
+    return Camera(look_from=tuple(r), look_at=tuple(center), up=cam.up, vfov=cam.vfov, aspect=cam.aspect,
+                  aperture=cam.aperture, focus=cam.focus)
 
 
 SCENES = {

@@ -17,12 +17,14 @@
 #include <mutex>
 #include <new>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "bvh_build.h"
 #include "rtc_dev.h"
 #include "rtc_kernels.h"
 #include "rtc_internal.h"
+#include "rtc_objects.h"
 #include "rtc_math.cuh"
 
 using namespace rtc;
@@ -47,40 +49,6 @@ rtc_status cuda_fail(cudaError_t e, const char* what) {
 bool finite3(const float* p) { return std::isfinite(p[0]) && std::isfinite(p[1]) && std::isfinite(p[2]); }
 
 }  // namespace
-
-struct rtc_context {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    uint32_t* d_status = nullptr;
-    unsigned long long* d_counters = nullptr;
-    float4* d_out = nullptr;
-    size_t out_cap = 0;         // float4 elements
-    uint8_t* d_rgb8 = nullptr;
-    size_t rgb8_cap = 0;
-    int num_sms = 148;
-    // wavefront scratch: path slots (SoA) and the two slot queues
-    void* d_wf = nullptr;
-    uint32_t wf_cap = 0;
-    uint32_t* h_poll = nullptr;       // pinned: queue sizes read back between batches
-    cudaEvent_t poll_ev[2] = {nullptr, nullptr};
-    cudaEvent_t phase_ev[3] = {nullptr, nullptr, nullptr};   // render start, drain start, render end
-    rtc_render_stats last{};
-    bool last_timed = false;
-    std::vector<cudaEvent_t> kev;      // per-launch timing events (RTC_FLAG_KERNEL_TIMING)
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> kev_pairs;   // extend pairs, then shade pairs
-    uint32_t kev_ext = 0, kev_shade = 0;   // pairs used by the last render
-    std::mutex mu;
-};
-
-struct rtc_scene {
-    rtc_context* ctx = nullptr;   // creating context; not dereferenced after creation
-    int device = 0;
-    void* d_slab = nullptr;
-    size_t slab_bytes = 0;
-    DevScene dev{};
-    rtc_camera cam{};
-    rtc_scene_info info{};
-};
 
 extern "C" const char* rtc_last_error_string(void) { return g_err.c_str(); }
 
@@ -115,6 +83,7 @@ extern "C" rtc_status rtc_context_destroy(rtc_context* c) {
     if (!c) return RTC_OK;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    c->engine.reset();
     cudaFree(c->d_status);
     cudaFree(c->d_counters);
     cudaFree(c->d_out);
@@ -174,9 +143,36 @@ size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 }  // namespace
 
-extern "C" rtc_status rtc_scene_create(rtc_context* ctx, const rtc_scene_desc* d, rtc_scene** out) {
-    if (!ctx || !d || !out) return fail(RTC_ERR_INVALID_ARGUMENT, "null argument");
-    *out = nullptr;
+// perspective_camera::initialize (perspective_camera.cuh:41-108), operation by operation.
+bool rtc_make_camera(const rtc_camera& C, DevCamera& cam) {
+    cam = DevCamera{};
+    float theta = C.vfov * 3.14159265358979323846f / 180.0f;   // degrees_to_radians (math_utils.cuh)
+    float half_height = std::tan(theta / 2.0f);
+    float ratio = C.aspect;
+    float focus = C.focus;
+    V3 lookfrom = v3(C.look_from), lookat = v3(C.look_at), vup = v3(C.up);
+    V3 w = unit(sub(lookfrom, lookat));
+    V3 u = unit(cross(vup, w));
+    V3 v = cross(w, u);
+    float half_width = ratio * half_height;
+    V3 origin = lookfrom;
+    V3 llc = sub(sub(sub(origin, mul(half_width * focus, u)), mul(half_height * focus, v)), mul(focus, w));
+    V3 horizontal = mul(2.0f * half_width * focus, u);
+    V3 vertical = mul(2.0f * half_height * focus, v);
+    const V3 vals[6] = {origin, llc, horizontal, vertical, u, v};
+    float* dst[6] = {cam.origin, cam.llc, cam.horizontal, cam.vertical, cam.u, cam.v};
+    for (int k = 0; k < 6; ++k) { dst[k][0] = vals[k].x; dst[k][1] = vals[k].y; dst[k][2] = vals[k].z; }
+    cam.lens_radius = C.aperture / 2.0f;
+    cam.time0 = 0.0f;
+    cam.time1 = 1.0f;
+    return std::isfinite(cam.llc[0] + cam.llc[1] + cam.llc[2] + horizontal.x + vertical.y);
+}
+
+const DevScene& rtc_scene_dev(const rtc_scene* s) { return s->dev; }
+DevParams rtc_dev_params(const rtc_render_params* p);
+
+rtc_status rtc_build_host_scene(const rtc_scene_desc* d, HostScene& H) {
+    if (!d) return fail(RTC_ERR_INVALID_ARGUMENT, "null argument");
     auto t0 = std::chrono::steady_clock::now();
     // ---- validation --------------------------------------------------------------------------
     auto bad = [&](const std::string& m) { return fail(RTC_ERR_BAD_SCENE, m); };
@@ -392,30 +388,7 @@ extern "C" rtc_status rtc_scene_create(rtc_context* ctx, const rtc_scene_desc* d
 
     // ---- camera: perspective_camera::initialize (perspective_camera.cuh:41-108) -----------------
     DevCamera cam{};
-    {
-        const rtc_camera& C = d->camera;
-        float theta = C.vfov * 3.14159265358979323846f / 180.0f;   // degrees_to_radians (math_utils.cuh)
-        float half_height = std::tan(theta / 2.0f);
-        float ratio = C.aspect;
-        float focus = C.focus;
-        V3 lookfrom = v3(C.look_from), lookat = v3(C.look_at), vup = v3(C.up);
-        V3 w = unit(sub(lookfrom, lookat));
-        V3 u = unit(cross(vup, w));
-        V3 v = cross(w, u);
-        float half_width = ratio * half_height;
-        V3 origin = lookfrom;
-        V3 llc = sub(sub(sub(origin, mul(half_width * focus, u)), mul(half_height * focus, v)), mul(focus, w));
-        V3 horizontal = mul(2.0f * half_width * focus, u);
-        V3 vertical = mul(2.0f * half_height * focus, v);
-        const V3 vals[6] = {origin, llc, horizontal, vertical, u, v};
-        float* dst[6] = {cam.origin, cam.llc, cam.horizontal, cam.vertical, cam.u, cam.v};
-        for (int k = 0; k < 6; ++k) { dst[k][0] = vals[k].x; dst[k][1] = vals[k].y; dst[k][2] = vals[k].z; }
-        cam.lens_radius = C.aperture / 2.0f;
-        cam.time0 = 0.0f;
-        cam.time1 = 1.0f;
-        if (!std::isfinite(cam.llc[0] + cam.llc[1] + cam.llc[2] + horizontal.x + vertical.y))
-            return bad("degenerate camera");
-    }
+    if (!rtc_make_camera(d->camera, cam)) return bad("degenerate camera");
 
     // ---- one device slab ----------------------------------------------------------------------
     struct Chunk { const void* src; size_t bytes; size_t off; };
@@ -446,39 +419,28 @@ extern "C" rtc_status rtc_scene_create(rtc_context* ctx, const rtc_scene_desc* d
                            ? (size_t)d->background.env_width * d->background.env_height * 3 * sizeof(float) : 0;
     size_t o_env = add_chunk(env_bytes ? d->background.env_rgb : nullptr, env_bytes);
 
-    rtc_scene* s = new (std::nothrow) rtc_scene();
-    if (!s) return fail(RTC_ERR_OOM, "host allocation failed");
-    s->ctx = ctx;
-    s->device = ctx->device;
-    cudaSetDevice(ctx->device);
-    cudaError_t e = cudaMalloc(&s->d_slab, total);
-    if (e != cudaSuccess) { delete s; return cuda_fail(e, "cudaMalloc(scene)"); }
-    s->slab_bytes = total;
-    uint8_t* base = (uint8_t*)s->d_slab;
-    for (const Chunk& c : chunks) {
-        if (!c.src || !c.bytes) continue;
-        e = cudaMemcpyAsync(base + c.off, c.src, c.bytes, cudaMemcpyHostToDevice, ctx->stream);
-        if (e != cudaSuccess) { cudaFree(s->d_slab); delete s; return cuda_fail(e, "scene upload"); }
-    }
-    e = cudaStreamSynchronize(ctx->stream);
-    if (e != cudaSuccess) { cudaFree(s->d_slab); delete s; return cuda_fail(e, "scene upload"); }
-
-    DevScene& D = s->dev;
-    D.nodes = (const float4*)(base + o_nodes);
-    D.items = (const uint32_t*)(base + o_items);
-    D.sph = (const float4*)(base + o_sph);
-    D.sph_aux = (const int2*)(base + o_sphx);
-    D.tri = (const float4*)(base + o_tri);
-    D.tri_n = (const float4*)(base + o_trin);
-    D.tri_vn = (const float4*)(base + o_trivn);
-    D.quad = (const float4*)(base + o_quad);
-    D.light = (const float4*)(base + o_light);
-    D.mat_i = (const int4*)(base + o_mi);
-    D.mat_f = (const float4*)(base + o_mf);
-    D.tex_i = (const int4*)(base + o_ti);
-    D.tex_f = (const float4*)(base + o_tf);
-    D.images = (const int4*)(base + o_img);
-    D.image_bytes = (const uint8_t*)(base + o_imgb);
+    // host image of the device slab; the DevScene's pointer fields hold byte offsets into it
+    H.slab.assign(total, 0);
+    for (const Chunk& c : chunks)
+        if (c.src && c.bytes) std::memcpy(H.slab.data() + c.off, c.src, c.bytes);
+    auto off = [](size_t o) { return reinterpret_cast<uint8_t*>(static_cast<uintptr_t>(o)); };
+    DevScene& D = H.dev;
+    D = DevScene{};
+    D.nodes = (const float4*)off(o_nodes);
+    D.items = (const uint32_t*)off(o_items);
+    D.sph = (const float4*)off(o_sph);
+    D.sph_aux = (const int2*)off(o_sphx);
+    D.tri = (const float4*)off(o_tri);
+    D.tri_n = (const float4*)off(o_trin);
+    D.tri_vn = (const float4*)off(o_trivn);
+    D.quad = (const float4*)off(o_quad);
+    D.light = (const float4*)off(o_light);
+    D.mat_i = (const int4*)off(o_mi);
+    D.mat_f = (const float4*)off(o_mf);
+    D.tex_i = (const int4*)off(o_ti);
+    D.tex_f = (const float4*)off(o_tf);
+    D.images = (const int4*)off(o_img);
+    D.image_bytes = (const uint8_t*)off(o_imgb);
     D.num_nodes = bvh.num_nodes;
     D.num_items = (uint32_t)items.size();
     D.num_lights = d->num_dir_lights;
@@ -491,16 +453,52 @@ extern "C" rtc_status rtc_scene_create(rtc_context* ctx, const rtc_scene_desc* d
     D.cam = cam;
     D.bg.kind = d->background.kind;
     for (int k = 0; k < 3; ++k) { D.bg.color[k] = d->background.color[k]; D.bg.top[k] = d->background.top[k]; }
-    D.bg.env = env_bytes ? (const float*)(base + o_env) : nullptr;
+    D.bg.env = env_bytes ? (const float*)off(o_env) : nullptr;
     D.bg.env_w = d->background.env_width;
     D.bg.env_h = d->background.env_height;
-    s->cam = d->camera;
-    s->info.num_primitives = (uint32_t)nprims;
-    s->info.num_lights = d->num_dir_lights;
-    s->info.num_nodes = bvh.num_nodes;
-    s->info.max_leaf_size = bvh.max_leaf_seen;
-    s->info.device_bytes = total;
-    s->info.build_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    H.cam = d->camera;
+    H.info = rtc_scene_info{};
+    H.info.num_primitives = (uint32_t)nprims;
+    H.info.num_lights = d->num_dir_lights;
+    H.info.num_nodes = bvh.num_nodes;
+    H.info.max_leaf_size = bvh.max_leaf_seen;
+    H.info.device_bytes = total;
+    H.info.build_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    return RTC_OK;
+}
+
+DevScene rtc_rebase_scene(const HostScene& H, uint8_t* base) {
+    DevScene D = H.dev;
+    auto rb = [base](auto& p) {
+        p = reinterpret_cast<std::remove_reference_t<decltype(p)>>(base + reinterpret_cast<uintptr_t>(p));
+    };
+    rb(D.nodes); rb(D.items); rb(D.sph); rb(D.sph_aux); rb(D.tri); rb(D.tri_n); rb(D.tri_vn); rb(D.quad);
+    rb(D.light); rb(D.mat_i); rb(D.mat_f); rb(D.tex_i); rb(D.tex_f); rb(D.images); rb(D.image_bytes);
+    if (D.bg.env) rb(D.bg.env);
+    return D;
+}
+
+extern "C" rtc_status rtc_scene_create(rtc_context* ctx, const rtc_scene_desc* d, rtc_scene** out) {
+    if (!ctx || !d || !out) return fail(RTC_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    HostScene H;
+    rtc_status r = rtc_build_host_scene(d, H);
+    if (r != RTC_OK) return r;
+    rtc_scene* s = new (std::nothrow) rtc_scene();
+    if (!s) return fail(RTC_ERR_OOM, "host allocation failed");
+    s->ctx = ctx;
+    s->device = ctx->device;
+    cudaSetDevice(ctx->device);
+    const size_t total = H.slab.size();
+    cudaError_t e = cudaMalloc(&s->d_slab, total);
+    if (e != cudaSuccess) { delete s; return cuda_fail(e, "cudaMalloc(scene)"); }
+    s->slab_bytes = total;
+    e = cudaMemcpyAsync(s->d_slab, H.slab.data(), total, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) { cudaFree(s->d_slab); delete s; return cuda_fail(e, "scene upload"); }
+    s->dev = rtc_rebase_scene(H, (uint8_t*)s->d_slab);
+    s->cam = H.cam;
+    s->info = H.info;
     *out = s;
     return RTC_OK;
 }
@@ -531,7 +529,7 @@ rtc_status check_params(const rtc_render_params* p) {
     if (p->width <= 0 || p->height <= 0) return fail(RTC_ERR_INVALID_ARGUMENT, "width/height must be positive");
     if ((int64_t)p->width * p->height > (1ll << 31)) return fail(RTC_ERR_INVALID_ARGUMENT, "image too large");
     if (p->spp <= 0) return fail(RTC_ERR_INVALID_ARGUMENT, "spp must be positive");
-    if (p->max_depth <= 0 || p->max_depth > 100000) return fail(RTC_ERR_INVALID_ARGUMENT, "max_depth out of range");
+    if (p->max_depth <= 0 || p->max_depth > WF_MAX_DEPTH) return fail(RTC_ERR_INVALID_ARGUMENT, "max_depth out of range (1..65535)");
     if (p->mode != RTC_MODE_COMPAT && p->mode != RTC_MODE_CLEAN) return fail(RTC_ERR_INVALID_ARGUMENT, "unknown mode");
     if (p->draw_order != RTC_DRAW_ORDER_DEVICE && p->draw_order != RTC_DRAW_ORDER_HOST)
         return fail(RTC_ERR_INVALID_ARGUMENT, "unknown draw order");
@@ -540,7 +538,11 @@ rtc_status check_params(const rtc_render_params* p) {
     return RTC_OK;
 }
 
-DevParams dev_params(const rtc_render_params* p) {
+DevParams dev_params(const rtc_render_params* p) { return rtc_dev_params(p); }
+
+}  // namespace
+
+DevParams rtc_dev_params(const rtc_render_params* p) {
     DevParams P;
     P.width = p->width;
     P.height = p->height;
@@ -552,6 +554,8 @@ DevParams dev_params(const rtc_render_params* p) {
     P.num_pixels = (int64_t)p->width * p->height;
     return P;
 }
+
+namespace {
 
 // Bytes of wavefront scratch per path slot.
 constexpr size_t WF_SLOT_BYTES = 5 * sizeof(float4) + 2 * sizeof(uint4) + sizeof(float2) + 2 * sizeof(uint32_t);
@@ -636,20 +640,32 @@ struct WfTimer {
     }
 };
 
+rtc::WfOneFn wf_one_fn(const rtc_render_params* p) {
+    if (p->mode == RTC_MODE_CLEAN) return rtc_wf_one_clean;
+    return p->draw_order == RTC_DRAW_ORDER_HOST ? rtc_wf_one_compat_host : rtc_wf_one_compat_dev;
+}
+
 rtc_status run_wavefront(const DevScene& S, const rtc_render_params* p, const WfBuffers& B, uint32_t* d_status,
                          float4* d_out, unsigned long long* d_counters, cudaStream_t st, int num_sms,
                          const WfPoller& poll, cudaEvent_t* phase, WfRun& run, WfTimer* timer = nullptr) {
-    DevParams P = dev_params(p);
+    const DevParams P = dev_params(p);
     const bool clean = p->mode == RTC_MODE_CLEAN;
+    const WfOneFn fn = wf_one_fn(p);
+    WfOneArgs J;
+    J.S = S;
+    J.P = P;
+    J.out = d_out;
+    WfLaunch L{};
+    L.counters = d_counters;
+    L.status = d_status;
+    L.st = st;
     if (phase) RTC_CUDA(cudaEventRecord(phase[0], st));
     RTC_CUDA(cudaMemsetAsync(B.ctr, 0, WF_CTR_N * sizeof(uint32_t), st));
     const int grid = num_sms * 8;
-    const int init_grid = (int)std::min<int64_t>((B.slots + 127) / 128, (int64_t)num_sms * 16);
-    const bool host = !clean && p->draw_order == RTC_DRAW_ORDER_HOST;   // g++ flavour of the compat kernels
-    cudaError_t e = clean ? rtc_wf_launch_init_clean(S, P, B, d_out, init_grid, st)
-                    : host ? rtc_wf_launch_init_compat_host(S, P, B, d_out, init_grid, st)
-                           : rtc_wf_launch_init_compat_dev(S, P, B, d_out, init_grid, st);
+    L.grid = (int)std::min<int64_t>((B.slots + 127) / 128, (int64_t)num_sms * 16);
+    cudaError_t e = fn(WF_OP_INIT, J, B, L);
     if (e != cudaSuccess) return cuda_fail(e, "wavefront init");
+    L.grid = grid;
     const uint64_t nsamp = clean ? (uint64_t)P.spp : (uint64_t)P.sqrt_spp * P.sqrt_spp;
     const uint64_t rounds = (uint64_t)((P.num_pixels + B.slots - 1) / B.slots);
     const uint64_t max_iters = rounds * nsamp * (uint64_t)(P.max_depth + 1) + 64;
@@ -666,11 +682,9 @@ rtc_status run_wavefront(const DevScene& S, const rtc_render_params* p, const Wf
     uint32_t sync_counts[2] = {0, 0};
     for (int b = 0;; ++b) {
         for (int k = 0; k < BATCH; ++k, ++it) {
-            const WfIter w = wf_iter(it);
+            L.w = wf_iter(it);
             if (fused) {
-                e = clean  ? rtc_wf_launch_bounce_clean(S, P, B, w, d_out, d_counters, d_status, grid, st)
-                    : host ? rtc_wf_launch_bounce_compat_host(S, P, B, w, d_out, d_counters, d_status, grid, st)
-                           : rtc_wf_launch_bounce_compat_dev(S, P, B, w, d_out, d_counters, d_status, grid, st);
+                e = fn(WF_OP_BOUNCE, J, B, L);
             } else {
                 cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr, e3 = nullptr;
                 if (timer) {
@@ -678,17 +692,13 @@ rtc_status run_wavefront(const DevScene& S, const rtc_render_params* p, const Wf
                     RTC_CUDA(timer->pair(e2, e3));
                     RTC_CUDA(cudaEventRecord(e0, st));
                 }
-                e = host ? rtc_wf_launch_extend_host(S, P, B, w, d_counters, d_status, grid, st)
-                         : rtc_wf_launch_extend_dev(S, P, B, w, d_counters, d_status, grid, st);
+                e = fn(WF_OP_EXTEND, J, B, L);
                 if (timer) {
                     RTC_CUDA(cudaEventRecord(e1, st));
                     RTC_CUDA(cudaEventRecord(e2, st));
                     timer->ext.push_back({e0, e1});
                 }
-                if (e == cudaSuccess)
-                    e = clean  ? rtc_wf_launch_shade_clean(S, P, B, w, d_out, d_counters, d_status, grid, st)
-                        : host ? rtc_wf_launch_shade_compat_host(S, P, B, w, d_out, d_counters, d_status, grid, st)
-                               : rtc_wf_launch_shade_compat_dev(S, P, B, w, d_out, d_counters, d_status, grid, st);
+                if (e == cudaSuccess) e = fn(WF_OP_SHADE, J, B, L);
                 if (timer) {
                     RTC_CUDA(cudaEventRecord(e3, st));
                     timer->shade.push_back({e2, e3});
@@ -732,11 +742,9 @@ rtc_status run_wavefront(const DevScene& S, const rtc_render_params* p, const Wf
     run.drained_slots = run.drained ? left : 0u;
     if (phase) RTC_CUDA(cudaEventRecord(phase[1], st));
     if (run.drained) {
-        const WfIter w = wf_iter(it);
-        const int fgrid = (int)std::max<uint32_t>(1u, (drain + 127u) / 128u);
-        e = clean  ? rtc_wf_launch_finish_clean(S, P, B, w, d_out, d_counters, d_status, fgrid, st)
-            : host ? rtc_wf_launch_finish_compat_host(S, P, B, w, d_out, d_counters, d_status, fgrid, st)
-                   : rtc_wf_launch_finish_compat_dev(S, P, B, w, d_out, d_counters, d_status, fgrid, st);
+        L.w = wf_iter(it);
+        L.grid = (int)std::max<uint32_t>(1u, (drain + 127u) / 128u);
+        e = fn(WF_OP_FINISH, J, B, L);
         if (e != cudaSuccess) return cuda_fail(e, "wavefront finish");
     }
     if (phase) RTC_CUDA(cudaEventRecord(phase[2], st));

@@ -104,12 +104,54 @@ struct WfBuffers {
     float4* att;       // path attenuation rgb
     float4* acc;       // radiance of the current sample rgb
     float4* psum;      // pixel sum rgb (pixel_color)
-    uint4* meta;       // x pixel (0xffffffff idle), y sample index, z minstd state, w depth left
+    uint4* meta;       // x pixel (0xffffffff idle), y sample index, z minstd state,
+                       // w depth left (low 16 bits) | job slot (high 16 bits, 0 for a single image)
     uint4* pcg;        // clean mode: PCG32 state (lo, hi) and increment (lo, hi)
     float2* hit;       // t, item bits (0xffffffff = miss)
     uint32_t* queue[2];
     uint32_t* ctr;     // [0..2] queue sizes (rotating), [3] next pixel to fetch
     uint32_t slots;
+};
+
+constexpr uint32_t WF_IDLE = 0xffffffffu;
+constexpr int WF_MAX_DEPTH = 0xffff;
+constexpr uint32_t WF_MAX_JOBS = 1u << 16;   // job ring capacity limit (job slot in 16 bits)
+__host__ __device__ __forceinline__ uint32_t wf_depth(uint32_t w) { return w & 0xffffu; }
+__host__ __device__ __forceinline__ uint32_t wf_job(uint32_t w) { return w >> 16; }
+__host__ __device__ __forceinline__ uint32_t wf_pack(uint32_t depth, uint32_t job) { return (job << 16) | depth; }
+
+// One image of a batched or served render: a record in the device job ring.
+struct DevJob {
+    DevScene S;                  // the scene's arrays, with this job's camera
+    DevParams P;
+    float4* out;                 // width*height radiance sums, frame-buffer order
+    unsigned long long begin;    // first index of the job's pixels in the engine's global pixel sequence
+};
+
+// Hand-out state of the global pixel sequence (device).  Pixels [next, limit) are admitted and not yet
+// claimed; jobs with sequence numbers in [lo, hi) may own them (ring slot = sequence & mask).
+struct WfWindow {
+    unsigned long long limit;
+    uint32_t lo, hi;
+};
+struct WfFeed {
+    unsigned long long next;
+    WfWindow win;
+    uint32_t pad[2];
+};
+
+// Kernel arguments of the two job sources (the device-side policy types in rtc_wavefront.cuh add
+// their methods to these).
+struct WfOneArgs {             // one image
+    DevScene S;
+    DevParams P;
+    float4* out;
+};
+struct WfTableArgs {           // a ring of jobs
+    const DevJob* jobs;
+    WfFeed* feed;
+    uint32_t* done;            // per ring slot: pixels written
+    uint32_t mask;             // ring capacity - 1 (a power of two)
 };
 
 // Iteration k reads queue (k & 1) with size ctr[k % 3], appends to queue ((k+1) & 1) counted in

@@ -14,6 +14,11 @@ size_t rtc_carve_wavefront(void* base, uint32_t slots, rtc::WfBuffers& B);
 // records an error message for rtc_last_error_string() and returns `s`
 rtc_status rtc_set_error(rtc_status s, const char* msg);
 rtc_status rtc_check_render_params(const rtc_render_params* p);
+// device-side view of a scene, and the per-launch parameters of a render
+const rtc::DevScene& rtc_scene_dev(const rtc_scene* s);
+rtc::DevParams rtc_dev_params(const rtc_render_params* p);
+// perspective_camera::initialize; false for a degenerate camera
+bool rtc_make_camera(const rtc_camera& c, rtc::DevCamera& out);
 int rtc_scene_device(const rtc_scene* s);
 // runs the wavefront engine on caller-provided buffers with synchronous queue polling: no device or
 // pinned allocations, no events

@@ -18,27 +18,29 @@
 #define RTC_FLAVOR_FN(name) RTC_FLAVOR_CAT(name, _host)
 #endif
 
+namespace rtc {
+// Wavefront kernel launches.  One dispatcher per (mode, flavour) and job source; `op` picks the kernel.
+enum WfOp { WF_OP_INIT = 0, WF_OP_ADMIT = 1, WF_OP_EXTEND = 2, WF_OP_SHADE = 3, WF_OP_FINISH = 4, WF_OP_BOUNCE = 5 };
+struct WfLaunch {
+    WfIter w;
+    WfWindow win;                    // ADMIT: the window to publish
+    unsigned long long* counters;    // NULL: no instrumentation
+    uint32_t* status;
+    int grid;
+    cudaStream_t st;
+};
+using WfOneFn = cudaError_t (*)(WfOp, const WfOneArgs&, const WfBuffers&, const WfLaunch&);
+using WfTableFn = cudaError_t (*)(WfOp, const WfTableArgs&, const WfBuffers&, const WfLaunch&);
+}  // namespace rtc
+
 #define RTC_DECLARE_COMPAT(sfx)                                                                                     \
     cudaError_t rtc_launch_render_compat##sfx(const rtc::DevScene& S, const rtc::DevParams& P, float4* out,        \
                                               unsigned long long* counters, uint32_t* status, int block,            \
                                               cudaStream_t st);                                                     \
-    cudaError_t rtc_wf_launch_init_compat##sfx(const rtc::DevScene& S, const rtc::DevParams& P,                   \
-                                               const rtc::WfBuffers& B, float4* out, int grid, cudaStream_t st);    \
-    cudaError_t rtc_wf_launch_extend##sfx(const rtc::DevScene& S, const rtc::DevParams& P, const rtc::WfBuffers& B, \
-                                          rtc::WfIter w, unsigned long long* counters, uint32_t* status, int grid,  \
-                                          cudaStream_t st);                                                         \
-    cudaError_t rtc_wf_launch_shade_compat##sfx(const rtc::DevScene& S, const rtc::DevParams& P,                  \
-                                                const rtc::WfBuffers& B, rtc::WfIter w, float4* out,              \
-                                                unsigned long long* counters, uint32_t* status, int grid,         \
-                                                cudaStream_t st);                                                   \
-    cudaError_t rtc_wf_launch_finish_compat##sfx(const rtc::DevScene& S, const rtc::DevParams& P,                 \
-                                                 const rtc::WfBuffers& B, rtc::WfIter w, float4* out,             \
-                                                 unsigned long long* counters, uint32_t* status, int grid,        \
-                                                 cudaStream_t st);                                                  \
-    cudaError_t rtc_wf_launch_bounce_compat##sfx(const rtc::DevScene& S, const rtc::DevParams& P,                 \
-                                                 const rtc::WfBuffers& B, rtc::WfIter w, float4* out,             \
-                                                 unsigned long long* counters, uint32_t* status, int grid,        \
-                                                 cudaStream_t st);
+    cudaError_t rtc_wf_one_compat##sfx(rtc::WfOp op, const rtc::WfOneArgs& a, const rtc::WfBuffers& B,            \
+                                       const rtc::WfLaunch& L);                                                     \
+    cudaError_t rtc_wf_table_compat##sfx(rtc::WfOp op, const rtc::WfTableArgs& a, const rtc::WfBuffers& B,        \
+                                         const rtc::WfLaunch& L);
 
 RTC_DECLARE_COMPAT(_dev)
 RTC_DECLARE_COMPAT(_host)
@@ -50,15 +52,6 @@ cudaError_t rtc_launch_trace_closest(const rtc::DevScene& S, const float* rays, 
 cudaError_t rtc_launch_quantize(const float4* sum, uint8_t* rgb8, int width, int height, int spp,
                                 cudaStream_t st);
 
-// clean-mode wavefront (wavefront_clean.cu); its extend pass is rtc_wf_launch_extend_dev
-cudaError_t rtc_wf_launch_init_clean(const rtc::DevScene& S, const rtc::DevParams& P, const rtc::WfBuffers& B,
-                                     float4* out, int grid, cudaStream_t st);
-cudaError_t rtc_wf_launch_shade_clean(const rtc::DevScene& S, const rtc::DevParams& P, const rtc::WfBuffers& B,
-                                      rtc::WfIter w, float4* out, unsigned long long* counters, uint32_t* status,
-                                      int grid, cudaStream_t st);
-cudaError_t rtc_wf_launch_finish_clean(const rtc::DevScene& S, const rtc::DevParams& P, const rtc::WfBuffers& B,
-                                       rtc::WfIter w, float4* out, unsigned long long* counters, uint32_t* status,
-                                       int grid, cudaStream_t st);
-cudaError_t rtc_wf_launch_bounce_clean(const rtc::DevScene& S, const rtc::DevParams& P, const rtc::WfBuffers& B,
-                                       rtc::WfIter w, float4* out, unsigned long long* counters, uint32_t* status,
-                                       int grid, cudaStream_t st);
+// clean-mode wavefront (wavefront_clean.cu)
+cudaError_t rtc_wf_one_clean(rtc::WfOp op, const rtc::WfOneArgs& a, const rtc::WfBuffers& B, const rtc::WfLaunch& L);
+cudaError_t rtc_wf_table_clean(rtc::WfOp op, const rtc::WfTableArgs& a, const rtc::WfBuffers& B, const rtc::WfLaunch& L);

@@ -25,14 +25,19 @@ __device__ __forceinline__ void draw3(R& rng, float& a, float& b, float& c) {
 }
 
 // random_in_unit_disk (gpu_randomizer.cuh:61-67)
+//
+// ORDER 0 (the builds with FMA contraction: the nvcc flavour and clean mode) writes the camera
+// sample's multiply-adds as explicit fused operations, so its rounding is fixed by the source and not
+// by how the compiler contracts the kernel that inlines it: a pixel's camera rays are the same bits
+// whichever kernel (admission, shade, drain) starts its sample.
 template <int ORDER, class R>
 __device__ __forceinline__ V3 random_in_unit_disk(R& rng) {
     V3 p;
     do {
         float a, b;
         draw2<ORDER>(rng, a, b);
-        p = v3(2.0f * a - 1.0f, 2.0f * b - 1.0f, 2.0f * 0.0f - 0.0f);
-    } while (dot(p, p) >= 1.0f);
+        p = v3(2.0f * a - 1.0f, 2.0f * b - 1.0f, 2.0f * 0.0f - 0.0f);   // 2*a is exact: fused or not
+    } while ((ORDER == 0 ? __fmaf_rn(p.x, p.x, __fmaf_rn(p.y, p.y, __fmul_rn(p.z, p.z))) : dot(p, p)) >= 1.0f);
     return p;
 }
 
@@ -115,12 +120,27 @@ struct Ray {
 template <int ORDER, class R>
 __device__ __forceinline__ Ray camera_ray(const DevCamera& c, float s, float t, R& rng) {
     V3 rd = mul(c.lens_radius, random_in_unit_disk<ORDER>(rng));
-    V3 offset = add(mul(v3(c.u), rd.x), mul(v3(c.v), rd.y));
-    float time = c.time0 + rng.uniform() * (c.time1 - c.time0);
     Ray r;
-    r.o = add(v3(c.origin), offset);
-    r.d = sub(sub(add(add(v3(c.llc), mul(s, v3(c.horizontal))), mul(t, v3(c.vertical))), v3(c.origin)), offset);
-    r.time = time;
+    if constexpr (ORDER == 0) {
+        // fused multiply-adds spelled out (see random_in_unit_disk)
+        float off[3], o[3], d[3];
+        for (int k = 0; k < 3; ++k) off[k] = __fmaf_rn(c.v[k], rd.y, __fmul_rn(c.u[k], rd.x));
+        float time = __fmaf_rn(rng.uniform(), __fsub_rn(c.time1, c.time0), c.time0);
+        for (int k = 0; k < 3; ++k) {
+            o[k] = __fadd_rn(c.origin[k], off[k]);
+            d[k] = __fsub_rn(__fsub_rn(__fmaf_rn(t, c.vertical[k], __fmaf_rn(s, c.horizontal[k], c.llc[k])), c.origin[k]),
+                             off[k]);
+        }
+        r.o = v3(o[0], o[1], o[2]);
+        r.d = v3(d[0], d[1], d[2]);
+        r.time = time;
+    } else {
+        V3 offset = add(mul(v3(c.u), rd.x), mul(v3(c.v), rd.y));
+        float time = c.time0 + rng.uniform() * (c.time1 - c.time0);
+        r.o = add(v3(c.origin), offset);
+        r.d = sub(sub(add(add(v3(c.llc), mul(s, v3(c.horizontal))), mul(t, v3(c.vertical))), v3(c.origin)), offset);
+        r.time = time;
+    }
     return r;
 }
 

@@ -10,8 +10,18 @@
 //           is written out and the slot fetches the next pixel from a global counter;
 // and survivors are compacted into the next queue with one atomic per warp (ballot + popc + shfl).
 // Queue counters live on the device; the host launches batches of iterations and polls the count.
+//
+// Where a slot's pixels come from is a policy type J:
+//   WfOne    one image; scene, parameters and output in kernel parameter space (the plain render);
+//   WfTable  a ring of job records (DevJob) in device memory and one global pixel sequence over all
+//            admitted jobs (batched and served renders): images of different scenes, cameras,
+//            resolutions, spp and depths share the slots, each pixel still computed exactly as the
+//            plain render computes it.
 #pragma once
 
+#include <type_traits>
+
+#include "rtc_kernels.h"
 #include "rtc_path.cuh"
 
 namespace rtc {
@@ -82,15 +92,77 @@ __device__ __forceinline__ uint32_t wf_samples(const DevParams& P, bool clean) {
     return clean ? (uint32_t)P.spp : (uint32_t)(P.sqrt_spp * P.sqrt_spp);
 }
 
+// ---- job sources ---------------------------------------------------------------------------------
+
+// One image.  Pixels are handed out by a plain atomicAdd on ctr[WF_NEXT_PIXEL] (overshoot is harmless:
+// nothing is admitted later).
+struct WfOne : WfOneArgs {
+    __device__ __forceinline__ WfWindow window() const { return WfWindow{0ull, 0u, 0u}; }
+    __device__ __forceinline__ const DevScene& scene(uint32_t) const { return S; }
+    __device__ __forceinline__ const DevParams& params(uint32_t) const { return P; }
+    __device__ __forceinline__ float4* output(uint32_t) const { return out; }
+    __device__ __forceinline__ void pixel_done(uint32_t) const {}
+    __device__ __forceinline__ bool claim(const WfBuffers& B, const WfWindow&, uint32_t& job, uint32_t& pixel,
+                                          uint32_t&) const {
+        const uint32_t p = atomicAdd(B.ctr + WF_NEXT_PIXEL, 1u);
+        if ((int64_t)p >= P.num_pixels) return false;
+        job = 0u;
+        pixel = p;
+        return true;
+    }
+};
+
+// A ring of jobs.  The lanes of a warp that need a pixel claim consecutive indices of the global pixel
+// sequence with one atomicAdd by the warp's leader; indices at or past the admitted limit are refused
+// (the cursor may run past the limit, and the next admission moves it back to the old limit before it
+// extends the sequence, so no pixel is skipped).  The owning job is found by binary search over the
+// ring's first-pixel indices.
+struct WfTable : WfTableArgs {
+    __device__ __forceinline__ WfWindow window() const {
+        const volatile WfFeed* f = feed;
+        WfWindow w;
+        w.limit = f->win.limit;
+        w.lo = f->win.lo;
+        w.hi = f->win.hi;
+        return w;
+    }
+    __device__ __forceinline__ const DevScene& scene(uint32_t j) const { return jobs[j].S; }
+    __device__ __forceinline__ const DevParams& params(uint32_t j) const { return jobs[j].P; }
+    __device__ __forceinline__ float4* output(uint32_t j) const { return jobs[j].out; }
+    __device__ __forceinline__ void pixel_done(uint32_t j) const { atomicAdd(done + j, 1u); }
+    __device__ __forceinline__ bool claim(const WfBuffers&, const WfWindow& win, uint32_t& job, uint32_t& pixel,
+                                          uint32_t&) const {
+        const unsigned act = __activemask();
+        const int lane = threadIdx.x & 31;
+        const int leader = __ffs(act) - 1;
+        unsigned long long base = 0ull;
+        if (lane == leader) base = atomicAdd(&feed->next, (unsigned long long)__popc(act));
+        base = __shfl_sync(act, base, leader);
+        const unsigned long long g = base + (unsigned long long)__popc(act & ((1u << lane) - 1u));
+        if (g >= win.limit) return false;
+        uint32_t lo = win.lo, hi = win.hi;   // jobs[lo].begin <= g < jobs[hi].begin (hi exclusive)
+        while (hi - lo > 1u) {
+            const uint32_t mid = lo + (hi - lo) / 2u;
+            if (jobs[mid & mask].begin <= g) lo = mid;
+            else hi = mid;
+        }
+        job = lo & mask;
+        pixel = (uint32_t)(g - jobs[job].begin);
+        return true;
+    }
+};
+
 // Fetches the next pixel for a slot and starts its first sample; returns false when none is left.
-template <bool CLEAN, int ORDER>
-__device__ __forceinline__ bool wf_fetch_pixel(const DevScene& S, const DevParams& P, const WfBuffers& B,
-                                               uint32_t slot, float4* out, uint32_t& status) {
-    uint32_t pixel = atomicAdd(B.ctr + WF_NEXT_PIXEL, 1u);
-    if ((int64_t)pixel >= P.num_pixels) {
-        B.meta[slot] = make_uint4(0xffffffffu, 0u, 0u, 0u);
+template <bool CLEAN, int ORDER, class J>
+__device__ __forceinline__ bool wf_fetch_pixel(const J& jobs, const WfWindow& win, const WfBuffers& B, uint32_t slot,
+                                               uint32_t& status) {
+    uint32_t job = 0, pixel = 0;
+    if (!jobs.claim(B, win, job, pixel, status)) {
+        B.meta[slot] = make_uint4(WF_IDLE, 0u, 0u, 0u);
         return false;
     }
+    const DevScene& S = jobs.scene(job);
+    const DevParams& P = jobs.params(job);
     WfRng<CLEAN> rng;
     if constexpr (!CLEAN) rng.seed(P.seed + pixel);
     Ray r;
@@ -100,29 +172,52 @@ __device__ __forceinline__ bool wf_fetch_pixel(const DevScene& S, const DevParam
     B.att[slot] = make_float4(1.f, 1.f, 1.f, 0.f);
     B.acc[slot] = make_float4(0.f, 0.f, 0.f, 0.f);
     B.psum[slot] = make_float4(0.f, 0.f, 0.f, 0.f);
-    uint4 m = make_uint4(pixel, 0u, 0u, (uint32_t)P.max_depth);
+    uint4 m = make_uint4(pixel, 0u, 0u, wf_pack((uint32_t)P.max_depth, job));
     rng_save<CLEAN>(B, slot, rng, m);
     B.meta[slot] = m;
-    (void)out;
-    (void)status;
     return true;
 }
 
+// First fill of a single-image render: slot k takes a pixel, joins queue 0.
 template <bool CLEAN, int ORDER>
-__global__ void __launch_bounds__(128) wf_init(DevScene S, DevParams P, WfBuffers B, float4* out) {
+__global__ void __launch_bounds__(128) wf_init(WfOne J, WfBuffers B) {
+    uint32_t status = 0;
+    const WfWindow win = J.window();
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < B.slots; base += stride) {
+        const uint32_t slot = base + threadIdx.x;
+        bool live = false;
+        if (slot < B.slots) live = wf_fetch_pixel<CLEAN, ORDER>(J, win, B, slot, status);
+        wf_push(B.queue[0], B.ctr + 0, slot, live);
+    }
+}
+
+// Publishes a new window of the job ring (one thread, in stream order between iterations): the claim
+// cursor moves back to the previous limit if refused claims ran past it, then the window widens.
+static __global__ void wf_feed_set(WfFeed* f, WfWindow win) {
+    const unsigned long long old = f->win.limit;
+    if (f->next > old) f->next = old;
+    f->win = win;
+}
+
+// Admission: every idle slot claims a pixel of the admitted jobs and joins the queue iteration `w`
+// reads.  Runs in stream order between iterations, after wf_feed_set.
+template <bool CLEAN, int ORDER>
+__global__ void __launch_bounds__(128) wf_admit(WfTable J, WfBuffers B, WfIter w, WfWindow win, uint32_t* status_word) {
     uint32_t status = 0;
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t base = blockIdx.x * blockDim.x; base < B.slots; base += stride) {
         const uint32_t slot = base + threadIdx.x;
         bool live = false;
-        if (slot < B.slots) live = wf_fetch_pixel<CLEAN, ORDER>(S, P, B, slot, out, status);
-        wf_push(B.queue[0], B.ctr + 0, slot, live);
+        if (slot < B.slots && B.meta[slot].x == WF_IDLE) live = wf_fetch_pixel<CLEAN, ORDER>(J, win, B, slot, status);
+        wf_push(B.queue[w.qin], B.ctr + w.cin, slot, live);
     }
+    if (status) atomicOr(status_word, status);
 }
 
-template <bool COUNT, int FLAVOR>
-__global__ void __launch_bounds__(128) wf_extend(DevScene S, DevParams P, WfBuffers B, WfIter w,
-                                                 unsigned long long* counters, uint32_t* status_word) {
+template <bool COUNT, int FLAVOR, class J>
+__global__ void __launch_bounds__(128) wf_extend(J jobs, WfBuffers B, WfIter w, unsigned long long* counters,
+                                                 uint32_t* status_word) {
     const uint32_t n = B.ctr[w.cin];
     if (blockIdx.x == 0 && threadIdx.x == 0) B.ctr[w.czero] = 0u;
     const uint32_t* q = B.queue[w.qin];
@@ -132,11 +227,12 @@ __global__ void __launch_bounds__(128) wf_extend(DevScene S, DevParams P, WfBuff
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
         const uint32_t slot = __ldcs(q + k);
         const float4 o = __ldcs(B.ray_o + slot), d = __ldcs(B.ray_d + slot);
-        const uint32_t depth = __ldcs(&B.meta[slot].w);
+        const uint32_t mw = __ldcs(&B.meta[slot].w);
+        const uint32_t job = wf_job(mw);
         float t;
         uint32_t item;
-        bool h = closest_hit(S, v3(o), v3(d), 0.00001f, 3.402823466e+38f, depth == (uint32_t)P.max_depth, t, item,
-                             st, status);
+        bool h = closest_hit(jobs.scene(job), v3(o), v3(d), 0.00001f, 3.402823466e+38f,
+                             wf_depth(mw) == (uint32_t)jobs.params(job).max_depth, t, item, st, status);
         B.hit[slot] = make_float2(t, __uint_as_float(h ? item : 0xffffffffu));
         ++rays;
     }
@@ -161,11 +257,14 @@ __global__ void __launch_bounds__(128) wf_extend(DevScene S, DevParams P, WfBuff
 
 // One shade step of a slot whose current ray has been traced: shade_bounce, then the slot's
 // bookkeeping (next bounce / next sample / next pixel).  Returns true while the slot has a ray to trace.
-template <bool CLEAN, int ORDER>
-__device__ __forceinline__ bool wf_step(const DevScene& S, const DevParams& P, const WfBuffers& B, uint32_t slot,
-                                        float t, uint32_t item, float4* __restrict__ out, PathCounters& pc,
-                                        TraceStats& st, uint32_t& paths, uint32_t& status) {
+template <bool CLEAN, int ORDER, class J>
+__device__ __forceinline__ bool wf_step(const J& jobs, const WfWindow& win, const WfBuffers& B, uint32_t slot,
+                                        float t, uint32_t item, PathCounters& pc, TraceStats& st, uint32_t& paths,
+                                        uint32_t& status) {
     uint4 m = __ldcs(B.meta + slot);
+    const uint32_t job = wf_job(m.w);
+    const DevScene& S = jobs.scene(job);
+    const DevParams& P = jobs.params(job);
     const float4 o = __ldcs(B.ray_o + slot), d = __ldcs(B.ray_d + slot), a4 = __ldcs(B.att + slot),
                  c4 = __ldcs(B.acc + slot);
     Ray r;
@@ -176,9 +275,9 @@ __device__ __forceinline__ bool wf_step(const DevScene& S, const DevParams& P, c
     WfRng<CLEAN> rng;
     if constexpr (CLEAN) pcg_load(rng, __ldcs(B.pcg + slot));
     else rng.x = m.z;
-    const bool hide = m.w == (uint32_t)P.max_depth;
+    uint32_t depth = wf_depth(m.w);
+    const bool hide = depth == (uint32_t)P.max_depth;
     const bool cont = shade_bounce<CLEAN, ORDER>(S, r, item != 0xffffffffu, t, item, hide, acc, att, rng, pc, st, status);
-    uint32_t depth = m.w;
     if (cont) --depth;
     if (cont && depth > 0u) {
         // the path continues: next bounce
@@ -186,7 +285,7 @@ __device__ __forceinline__ bool wf_step(const DevScene& S, const DevParams& P, c
         B.ray_d[slot] = make_float4(r.d.x, r.d.y, r.d.z, 0.f);
         B.att[slot] = make_float4(att.r, att.g, att.b, 0.f);
         B.acc[slot] = make_float4(acc.r, acc.g, acc.b, 0.f);
-        m.w = depth;
+        m.w = wf_pack(depth, job);
         rng_save<CLEAN>(B, slot, rng, m);
         B.meta[slot] = m;
         return true;
@@ -210,14 +309,15 @@ __device__ __forceinline__ bool wf_step(const DevScene& S, const DevParams& P, c
         B.acc[slot] = make_float4(0.f, 0.f, 0.f, 0.f);
         B.psum[slot] = ps;
         m.y = s;
-        m.w = (uint32_t)P.max_depth;
+        m.w = wf_pack((uint32_t)P.max_depth, job);
         rng_save<CLEAN>(B, slot, rng, m);
         B.meta[slot] = m;
         return true;
     }
     // the pixel is done: write it and take the next pixel
-    out[m.x] = make_float4(ps.x, ps.y, ps.z, 1.0f);
-    return wf_fetch_pixel<CLEAN, ORDER>(S, P, B, slot, out, status);
+    jobs.output(job)[m.x] = make_float4(ps.x, ps.y, ps.z, 1.0f);
+    jobs.pixel_done(job);
+    return wf_fetch_pixel<CLEAN, ORDER>(jobs, win, B, slot, status);
 }
 
 template <bool COUNT>
@@ -238,10 +338,11 @@ __device__ __forceinline__ void wf_flush(unsigned long long* counters, uint32_t 
     }
 }
 
-template <bool CLEAN, int ORDER, bool COUNT>
-__global__ void __launch_bounds__(128) wf_shade(DevScene S, DevParams P, WfBuffers B, WfIter w, float4* __restrict__ out,
-                                                unsigned long long* counters, uint32_t* status_word) {
+template <bool CLEAN, int ORDER, bool COUNT, class J>
+__global__ void __launch_bounds__(128) wf_shade(J jobs, WfBuffers B, WfIter w, unsigned long long* counters,
+                                                uint32_t* status_word) {
     const uint32_t n = B.ctr[w.cin];
+    const WfWindow win = jobs.window();
     const uint32_t* q = B.queue[w.qin];
     uint32_t* qn = B.queue[w.qin ^ 1];
     uint32_t* cn = B.ctr + w.cout;
@@ -256,7 +357,7 @@ __global__ void __launch_bounds__(128) wf_shade(DevScene S, DevParams P, WfBuffe
         if (k < n) {
             slot = __ldcs(q + k);
             const float2 hv = __ldcs(B.hit + slot);
-            live = wf_step<CLEAN, ORDER>(S, P, B, slot, hv.x, __float_as_uint(hv.y), out, pc, st, paths, status);
+            live = wf_step<CLEAN, ORDER>(jobs, win, B, slot, hv.x, __float_as_uint(hv.y), pc, st, paths, status);
         }
         wf_push(qn, cn, slot, live);
     }
@@ -266,11 +367,12 @@ __global__ void __launch_bounds__(128) wf_shade(DevScene S, DevParams P, WfBuffe
 
 // Fused form of one iteration: trace + shade of every queued slot in one launch (each lane still does
 // exactly one bounce, so the warp stays in the same phase), then compaction into the next queue.
-template <bool CLEAN, int ORDER, bool COUNT>
-__global__ void __launch_bounds__(128) wf_bounce(DevScene S, DevParams P, WfBuffers B, WfIter w, float4* __restrict__ out,
-                                                 unsigned long long* counters, uint32_t* status_word) {
+template <bool CLEAN, int ORDER, bool COUNT, class J>
+__global__ void __launch_bounds__(128) wf_bounce(J jobs, WfBuffers B, WfIter w, unsigned long long* counters,
+                                                 uint32_t* status_word) {
     const uint32_t n = B.ctr[w.cin];
     if (blockIdx.x == 0 && threadIdx.x == 0) B.ctr[w.czero] = 0u;   // appended to by the next iteration
+    const WfWindow win = jobs.window();
     const uint32_t* q = B.queue[w.qin];
     uint32_t* qn = B.queue[w.qin ^ 1];
     uint32_t* cn = B.ctr + w.cout;
@@ -285,13 +387,14 @@ __global__ void __launch_bounds__(128) wf_bounce(DevScene S, DevParams P, WfBuff
         if (k < n) {
             slot = q[k];
             const float4 o = B.ray_o[slot], d = B.ray_d[slot];
-            const uint4 m = B.meta[slot];
+            const uint32_t mw = B.meta[slot].w;
+            const uint32_t job = wf_job(mw);
             float t;
             uint32_t item;
             ++rays;
-            bool h = closest_hit(S, v3(o), v3(d), 0.00001f, 3.402823466e+38f, m.w == (uint32_t)P.max_depth, t, item,
-                                 st, status);
-            live = wf_step<CLEAN, ORDER>(S, P, B, slot, t, h ? item : 0xffffffffu, out, pc, st, paths, status);
+            bool h = closest_hit(jobs.scene(job), v3(o), v3(d), 0.00001f, 3.402823466e+38f,
+                                 wf_depth(mw) == (uint32_t)jobs.params(job).max_depth, t, item, st, status);
+            live = wf_step<CLEAN, ORDER>(jobs, win, B, slot, t, h ? item : 0xffffffffu, pc, st, paths, status);
         }
         wf_push(qn, cn, slot, live);
     }
@@ -304,15 +407,15 @@ __global__ void __launch_bounds__(128) wf_bounce(DevScene S, DevParams P, WfBuff
 // have long paths (glass) make this tail thousands of bounces long in compat mode, where a pixel's
 // samples cannot run in parallel, so the loop keeps the whole path state in registers (the
 // megakernel's loop, resumed from the slot) and touches memory only to write the finished pixel.
-template <bool CLEAN, int ORDER, bool COUNT>
-__global__ void __launch_bounds__(128) wf_finish(DevScene S, DevParams P, WfBuffers B, WfIter w, float4* __restrict__ out,
-                                                 unsigned long long* counters, uint32_t* status_word) {
+template <bool CLEAN, int ORDER, bool COUNT, class J>
+__global__ void __launch_bounds__(128) wf_finish(J jobs, WfBuffers B, WfIter w, unsigned long long* counters,
+                                                 uint32_t* status_word) {
     const uint32_t n = B.ctr[w.cin];
+    const WfWindow win = jobs.window();
     const uint32_t* q = B.queue[w.qin];
     uint32_t status = 0, paths = 0;
     PathCounters pc{0, 0, 0};
     TraceStats st{0, 0};
-    const uint32_t nsamp = wf_samples(P, CLEAN);
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
         const uint32_t slot = q[k];
@@ -327,9 +430,12 @@ __global__ void __launch_bounds__(128) wf_finish(DevScene S, DevParams P, WfBuff
         WfRng<CLEAN> rng;
         if constexpr (CLEAN) pcg_load(rng, B.pcg[slot]);
         else rng.x = m.z;
-        uint32_t pixel = m.x, sample = m.y;
-        int depth = (int)m.w;
+        uint32_t pixel = m.x, sample = m.y, job = wf_job(m.w);
+        int depth = (int)wf_depth(m.w);
+        // one pass of the loop finishes the current sample of the current pixel
         for (;;) {
+            const DevScene& S = jobs.scene(job);
+            const DevParams& P = jobs.params(job);
             // the rest of the current sample: camera::ray_color's loop from `depth` down
             for (; depth > 0; --depth) {
                 const bool hide = depth == P.max_depth;
@@ -345,16 +451,17 @@ __global__ void __launch_bounds__(128) wf_finish(DevScene S, DevParams P, WfBuff
                 pg += acc.g;
                 pb += acc.b;
             }
-            if (++sample < nsamp) {
+            if (++sample < wf_samples(P, CLEAN)) {
                 wf_start_sample<CLEAN, ORDER>(S, P, rng, pixel, sample, r);
                 att = rgb(1.f, 1.f, 1.f);
                 acc = rgb(0.f, 0.f, 0.f);
                 depth = P.max_depth;
                 continue;
             }
-            out[pixel] = make_float4(pr, pg, pb, 1.0f);
+            jobs.output(job)[pixel] = make_float4(pr, pg, pb, 1.0f);
+            jobs.pixel_done(job);
             // a slot that still has pixels to take (fewer slots than pixels) continues through memory
-            if (!wf_fetch_pixel<CLEAN, ORDER>(S, P, B, slot, out, status)) break;
+            if (!wf_fetch_pixel<CLEAN, ORDER>(jobs, win, B, slot, status)) break;
             m = B.meta[slot];
             const float4 o2 = B.ray_o[slot], d2 = B.ray_d[slot];
             r.o = v3(o2);
@@ -367,12 +474,55 @@ __global__ void __launch_bounds__(128) wf_finish(DevScene S, DevParams P, WfBuff
             else rng.x = m.z;
             pixel = m.x;
             sample = 0;
-            depth = P.max_depth;
+            job = wf_job(m.w);
+            depth = (int)wf_depth(m.w);
             if (status) break;
         }
     }
     wf_flush<COUNT>(counters, pc.rays, paths, st);
     if (status) atomicOr(status_word, status);
+}
+
+// ---- launch dispatch (instantiated once per translation unit / flavour) ---------------------------
+
+template <bool CLEAN, int ORDER, int FLAVOR, class J, class A>
+cudaError_t wf_dispatch(WfOp op, const A& args, const WfBuffers& B, const WfLaunch& L) {
+    J jobs;
+    static_cast<A&>(jobs) = args;
+    const bool c = L.counters != nullptr;
+    switch (op) {
+    case WF_OP_INIT:
+        if constexpr (std::is_same<J, WfOne>::value) wf_init<CLEAN, ORDER><<<L.grid, 128, 0, L.st>>>(jobs, B);
+        else return cudaErrorInvalidValue;
+        break;
+    case WF_OP_ADMIT:
+        if constexpr (std::is_same<J, WfTable>::value) {
+            wf_feed_set<<<1, 1, 0, L.st>>>(jobs.feed, L.win);
+            wf_admit<CLEAN, ORDER><<<L.grid, 128, 0, L.st>>>(jobs, B, L.w, L.win, L.status);
+        } else {
+            return cudaErrorInvalidValue;
+        }
+        break;
+    case WF_OP_EXTEND:
+        if (c) wf_extend<true, FLAVOR><<<L.grid, 128, 0, L.st>>>(jobs, B, L.w, L.counters, L.status);
+        else wf_extend<false, FLAVOR><<<L.grid, 128, 0, L.st>>>(jobs, B, L.w, nullptr, L.status);
+        break;
+    case WF_OP_SHADE:
+        if (c) wf_shade<CLEAN, ORDER, true><<<L.grid, 128, 0, L.st>>>(jobs, B, L.w, L.counters, L.status);
+        else wf_shade<CLEAN, ORDER, false><<<L.grid, 128, 0, L.st>>>(jobs, B, L.w, nullptr, L.status);
+        break;
+    case WF_OP_FINISH:
+        if (c) wf_finish<CLEAN, ORDER, true><<<L.grid, 128, 0, L.st>>>(jobs, B, L.w, L.counters, L.status);
+        else wf_finish<CLEAN, ORDER, false><<<L.grid, 128, 0, L.st>>>(jobs, B, L.w, nullptr, L.status);
+        break;
+    case WF_OP_BOUNCE:
+        if (c) wf_bounce<CLEAN, ORDER, true><<<L.grid, 128, 0, L.st>>>(jobs, B, L.w, L.counters, L.status);
+        else wf_bounce<CLEAN, ORDER, false><<<L.grid, 128, 0, L.st>>>(jobs, B, L.w, nullptr, L.status);
+        break;
+    default:
+        return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
 }
 
 }  // namespace rtc

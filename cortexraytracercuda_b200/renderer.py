@@ -22,7 +22,9 @@ import numpy as np
 
 from . import _lib
 from ._lib import RtcError, check
-from .scene import MODE_COMPAT, DRAW_ORDER_DEVICE, RenderParams, Scene, SceneDesc, rtc_render_stats, rtc_scene_info
+from .scene import (MODE_COMPAT, DRAW_ORDER_DEVICE, REQ_DONE, REQ_FAILED, Camera, RenderParams, Scene, SceneDesc,
+                    rtc_batch_params, rtc_job, rtc_render_stats, rtc_request, rtc_request_info, rtc_scene_info,
+                    rtc_server_config, rtc_server_stats)
 
 
 class Context:
@@ -56,6 +58,23 @@ class Context:
 
     def upload(self, scene: Scene) -> "DeviceScene":
         return DeviceScene(self, scene)
+
+    def render_batch(self, jobs, slots: int = 0, ring: int = 0, batch: int = 0, drain: int = 0,
+                     stream: int | None = None) -> None:
+        """Renders many images through one wavefront (rtc_render_batch).  ``jobs`` are :class:`Job`s whose
+        ``d_radiance`` device buffers receive each image's radiance sums; returns when all are complete."""
+        arr = (rtc_job * max(1, len(jobs)))()
+        cams = []
+        for k, j in enumerate(jobs):
+            cam = None
+            if j.camera is not None:
+                c = j.camera.to_c()
+                cams.append(c)
+                cam = C.pointer(c)
+            arr[k] = rtc_job(j.scene.handle.value, cam, j.params.to_c(), j.d_radiance)
+        bp = rtc_batch_params(slots, ring, batch, drain)
+        check(self.lib.rtc_render_batch(self.handle, arr, len(jobs), C.byref(bp),
+                                        C.c_void_p(stream) if stream else None))
 
     def last_stats(self) -> dict:
         """Statistics of the last render (iterations, launches, drained slots, bulk/drain device ms)."""
@@ -123,6 +142,101 @@ class DeviceScene:
         check(self.ctx.lib.rtc_trace_closest(self.ctx.handle, self.handle, rays.ctypes.data, n, depth, max_depth,
                                              prim.ctypes.data, t.ctypes.data))
         return prim, t
+
+
+@dataclass
+class Job:
+    """One image of a batched render: a resident scene, its parameters, a device output buffer
+    (width*height float4, e.g. a torch tensor's data_ptr()) and optionally its own camera."""
+    scene: DeviceScene
+    params: RenderParams
+    d_radiance: int
+    camera: Camera | None = None
+
+
+def _host_ptr(buf) -> int:
+    if hasattr(buf, "data_ptr"):
+        return buf.data_ptr()
+    return buf.ctypes.data
+
+
+class RenderServer:
+    """A render server on one device (rtc_server): requests are submitted while others render, admitted
+    into the running wavefront as memory and ring entries free up, and copied to the caller's buffer
+    when complete.  Scenes are registered once and kept resident under an HBM budget (LRU eviction)."""
+
+    def __init__(self, device: int = 0, mode: int = MODE_COMPAT, draw_order: int = DRAW_ORDER_DEVICE,
+                 slots: int = 0, ring: int = 0, batch: int = 0, hbm_budget_bytes: int = 0):
+        self.lib = _lib.load()
+        cfg = rtc_server_config(device, mode, draw_order, batch, slots, ring, hbm_budget_bytes)
+        h = C.c_void_p()
+        check(self.lib.rtc_server_create(C.byref(cfg), C.byref(h)))
+        self.handle = h
+        self._outs = {}
+
+    def close(self):
+        if self.handle:
+            self.lib.rtc_server_destroy(self.handle)
+            self.handle = None
+            self._outs.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_scene(self, scene: Scene) -> int:
+        desc = SceneDesc(scene)
+        sid = C.c_uint32()
+        check(self.lib.rtc_server_add_scene(self.handle, desc.ptr(), C.byref(sid)))
+        return sid.value
+
+    def submit(self, scene_id: int, params: RenderParams, camera: Camera | None = None, out=None):
+        """Queues a request; ``out`` (default: a new numpy array) is an (H, W, 4) float32 host buffer that
+        receives the radiance sums (page-locked memory, e.g. a pinned torch tensor, lets the copy
+        overlap).  Returns (ticket, out)."""
+        if out is None:
+            out = np.empty((params.height, params.width, 4), np.float32)
+        req = rtc_request(scene_id, 1 if camera is None else 0, (camera or Camera()).to_c(), params.width,
+                          params.height, params.spp, params.max_depth, params.seed & 0xFFFFFFFF)
+        t = C.c_uint64()
+        check(self.lib.rtc_server_submit(self.handle, C.byref(req), C.c_void_p(_host_ptr(out)), C.byref(t)))
+        self._outs[t.value] = out
+        return t.value, out
+
+    @staticmethod
+    def _info(i: rtc_request_info) -> dict:
+        return {k: getattr(i, k) for k, _ in rtc_request_info._fields_}
+
+    def poll(self, ticket: int):
+        """(done, info): done once the result is in the buffer (the request is then released)."""
+        i = rtc_request_info()
+        r = self.lib.rtc_server_poll(self.handle, ticket, C.byref(i))
+        if r == 10:   # RTC_ERR_BUSY
+            return False, self._info(i)
+        self._outs.pop(ticket, None)
+        check(r)
+        return True, self._info(i)
+
+    def wait(self, ticket: int, timeout_ms: int = -1):
+        """Blocks until the request is done; returns (out, info)."""
+        i = rtc_request_info()
+        r = self.lib.rtc_server_wait(self.handle, ticket, timeout_ms, C.byref(i))
+        out = self._outs.pop(ticket, None) if r != 5 else self._outs.get(ticket)
+        check(r)
+        return out, self._info(i)
+
+    def stats(self) -> dict:
+        st = rtc_server_stats()
+        check(self.lib.rtc_server_get_stats(self.handle, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in rtc_server_stats._fields_}
 
 
 @dataclass

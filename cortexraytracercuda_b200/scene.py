@@ -100,6 +100,41 @@ class rtc_scene_info(C.Structure):
                 ("max_leaf_size", C.c_uint32), ("device_bytes", C.c_uint64), ("build_ms", C.c_double)]
 
 
+class rtc_job(C.Structure):
+    _fields_ = [("scene", C.c_void_p), ("camera", C.POINTER(rtc_camera)), ("params", rtc_render_params),
+                ("d_radiance_sum", C.c_void_p)]
+
+
+class rtc_batch_params(C.Structure):
+    _fields_ = [("slots", C.c_uint32), ("ring", C.c_uint32), ("batch", C.c_int32), ("drain", C.c_uint32)]
+
+
+class rtc_server_config(C.Structure):
+    _fields_ = [("device", C.c_int32), ("mode", C.c_int32), ("draw_order", C.c_int32), ("batch", C.c_int32),
+                ("slots", C.c_uint32), ("ring", C.c_uint32), ("hbm_budget_bytes", C.c_uint64)]
+
+
+class rtc_request(C.Structure):
+    _fields_ = [("scene_id", C.c_uint32), ("use_scene_camera", C.c_int32), ("camera", rtc_camera),
+                ("width", C.c_int32), ("height", C.c_int32), ("spp", C.c_int32), ("max_depth", C.c_int32),
+                ("seed", C.c_uint32)]
+
+
+class rtc_request_info(C.Structure):
+    _fields_ = [("state", C.c_int32), ("scene_uploaded", C.c_int32), ("submit_ms", C.c_double),
+                ("admit_ms", C.c_double), ("done_ms", C.c_double), ("paths", C.c_uint64)]
+
+
+class rtc_server_stats(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("failed", C.c_uint64), ("paths", C.c_uint64),
+                ("scene_uploads", C.c_uint64), ("scene_evictions", C.c_uint64), ("resident_bytes", C.c_uint64),
+                ("peak_resident_bytes", C.c_uint64), ("iterations", C.c_uint64), ("launches", C.c_uint64),
+                ("queued", C.c_uint32), ("in_flight", C.c_uint32)]
+
+
+REQ_QUEUED, REQ_RUNNING, REQ_COPYING, REQ_DONE, REQ_FAILED = range(5)
+
+
 def _f3(v) -> F3:
     v = [float(x) for x in v]
     if len(v) != 3:
@@ -123,6 +158,10 @@ class Camera:
     aspect: float = 16.0 / 9.0      # scene_builder's default camera (scene_builder.cpp:49)
     aperture: float = 0.0
     focus: float = 100.0
+
+    def to_c(self) -> rtc_camera:
+        return rtc_camera(_f3(self.look_from), _f3(self.look_at), _f3(self.up), self.vfov, self.aspect,
+                          self.aperture, self.focus)
 
 
 @dataclass

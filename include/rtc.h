@@ -311,6 +311,115 @@ rtc_status rtc_get_render_stats(rtc_context* ctx, rtc_render_stats* stats);
 rtc_status rtc_render_noalloc(const rtc_scene* scene, const rtc_render_params* params, float* d_radiance_sum,
                               void* stream);
 
+/* ------------------------------------------------------------------------------------------------ */
+/* batched render                                                                                    */
+/* ------------------------------------------------------------------------------------------------ */
+
+/* One image of a batch.  The reference renders one image per launchGPU call (core/src/gpu.cu:2127);
+ * a batch renders many images - different scenes, cameras, resolutions, spp and depths - through one
+ * set of wavefront path slots and one extend/shade launch per iteration for all of them.  Each image
+ * is computed exactly as rtc_render_device computes it alone (same per-pixel stream and sample order),
+ * so its result does not depend on the rest of the batch. */
+typedef struct rtc_job {
+    const rtc_scene* scene;       /* resident scene (same device as the context)                         */
+    const rtc_camera* camera;     /* NULL: the scene's own camera; else this job's camera                */
+    rtc_render_params params;     /* width, height, spp, max_depth, seed of this image; mode and
+                                     draw_order must be equal across the batch; engine, block_size and
+                                     flags are ignored                                                   */
+    float* d_radiance_sum;        /* device, width*height float4, 16-byte aligned, frame-buffer order    */
+} rtc_job;
+
+typedef struct rtc_batch_params {
+    uint32_t slots;    /* path slots (pixels in flight); 0: min(total pixels, 2^20)                      */
+    uint32_t ring;     /* job ring capacity, a power of two <= 65536; 0: 1024.  Larger batches are
+                          admitted as earlier images complete.                                            */
+    int32_t batch;     /* (extend, shade) iterations between two host polls; 0: 8                        */
+    uint32_t drain;    /* queued slots below which the drain kernel finishes the batch; 0: 512 per SM   */
+} rtc_batch_params;
+
+/* Renders `num_jobs` images on `stream` (a cudaStream_t, or NULL for the context's stream) and returns
+ * once all of them are complete.  `bp` may be NULL (defaults).  rtc_get_render_stats then reports the
+ * batch's iterations, launches and drained slots. */
+rtc_status rtc_render_batch(rtc_context* ctx, const rtc_job* jobs, uint32_t num_jobs, const rtc_batch_params* bp,
+                            void* stream);
+
+/* ------------------------------------------------------------------------------------------------ */
+/* served render                                                                                     */
+/* ------------------------------------------------------------------------------------------------ */
+
+/* A render server on one device.  No counterpart in the reference, which renders one image per process
+ * call (core/src/gpu.cu:2127).  Requests (scene, camera, resolution, spp, depth) are submitted from any
+ * thread while others are on the GPU; a server thread admits them into the running job-ring wavefront
+ * as ring entries and device memory free up (continuous batching), and copies each result to the
+ * caller's host buffer when its last pixel is written.  Scenes are registered once (host BVH build) and
+ * kept resident on the device under an HBM budget: a request whose scene is not resident uploads it,
+ * evicting the least recently used scenes that no request in flight uses.  Each request is computed
+ * exactly as rtc_render_device computes that image alone. */
+typedef struct rtc_server rtc_server;
+
+typedef struct rtc_server_config {
+    int32_t device;
+    int32_t mode;                /* rtc_mode, shared by every request                                  */
+    int32_t draw_order;          /* rtc_draw_order (COMPAT), shared by every request                   */
+    int32_t batch;               /* (extend, shade) iterations between two host polls; 0: 8            */
+    uint32_t slots;              /* path slots; 0: 2^20                                                 */
+    uint32_t ring;               /* requests in flight at most (power of two <= 65536); 0: 1024        */
+    uint64_t hbm_budget_bytes;   /* device bytes for slots, resident scenes and request outputs;
+                                    0: 120 GB                                                           */
+} rtc_server_config;
+
+typedef struct rtc_request {
+    uint32_t scene_id;           /* from rtc_server_add_scene                                          */
+    int32_t use_scene_camera;    /* nonzero: the scene's own camera; zero: `camera`                     */
+    rtc_camera camera;
+    int32_t width, height, spp, max_depth;
+    uint32_t seed;
+} rtc_request;
+
+typedef enum rtc_request_state {
+    RTC_REQ_QUEUED = 0,          /* waiting for a ring entry or device memory                           */
+    RTC_REQ_RUNNING = 1,         /* admitted, pixels in flight                                          */
+    RTC_REQ_COPYING = 2,         /* complete on the device, result on its way to the host buffer        */
+    RTC_REQ_DONE = 3,
+    RTC_REQ_FAILED = 4
+} rtc_request_state;
+
+typedef struct rtc_request_info {
+    int32_t state;               /* rtc_request_state                                                   */
+    int32_t scene_uploaded;      /* 1 when admitting this request uploaded its scene (cache miss)       */
+    double submit_ms;            /* server clock: ms since rtc_server_create                            */
+    double admit_ms;
+    double done_ms;              /* result in the caller's buffer                                       */
+    uint64_t paths;              /* traced camera samples of the image                                  */
+} rtc_request_info;
+
+typedef struct rtc_server_stats {
+    uint64_t submitted, completed, failed;
+    uint64_t paths;                       /* traced camera samples of completed requests                */
+    uint64_t scene_uploads, scene_evictions;
+    uint64_t resident_bytes, peak_resident_bytes;   /* slots + resident scenes + request outputs       */
+    uint64_t iterations, launches;
+    uint32_t queued, in_flight;
+} rtc_server_stats;
+
+rtc_status rtc_server_create(const rtc_server_config* cfg, rtc_server** out);
+/* Stops the server: queued requests fail, requests in flight complete first. */
+rtc_status rtc_server_destroy(rtc_server* server);
+/* Registers a scene: validation, flattening and BVH build on the host (rtc_scene_create's work).  The
+ * description may be freed after the call; the scene uploads on its first request. */
+rtc_status rtc_server_add_scene(rtc_server* server, const rtc_scene_desc* desc, uint32_t* scene_id);
+/* Queues a request.  `radiance_sum` (host, width*height*4 floats, frame-buffer order, as rtc_render
+ * writes it) receives the result and must stay valid until the request is done; page-locked memory
+ * lets the copy overlap the rendering of other requests. */
+rtc_status rtc_server_submit(rtc_server* server, const rtc_request* req, float* radiance_sum, uint64_t* ticket);
+/* RTC_OK once the request is done (its record is released), RTC_ERR_BUSY while queued, running or
+ * copying, RTC_ERR_NOT_FOUND for an unknown ticket; `info` (may be NULL) is filled in every case. */
+rtc_status rtc_server_poll(rtc_server* server, uint64_t ticket, rtc_request_info* info);
+/* Blocks until the request is done (RTC_OK, record released) or `timeout_ms` passes (RTC_ERR_TIMEOUT;
+ * a negative timeout waits without limit).  A failed request returns its error. */
+rtc_status rtc_server_wait(rtc_server* server, uint64_t ticket, int32_t timeout_ms, rtc_request_info* info);
+rtc_status rtc_server_get_stats(rtc_server* server, rtc_server_stats* stats);
+
 /* Closest-hit queries on arbitrary rays (hit-identity tests).  rays: n x 8 floats
  * (ox, oy, oz, tmin, dx, dy, dz, tmax) in host memory; `depth`/`max_depth` decide light visibility as
  * in the reference's world.hit (directional_light.cuh:106).  Outputs (host, n each, may be NULL):
