@@ -259,6 +259,12 @@ def run_batched(args, rank, world, local):
         for ds, p, o in zip(dss, params, plain_outs):
             ds.render_device(p, o.data_ptr(), stream=sp)
 
+    mk_params = [p.__class__(**{**p.__dict__, "engine": ENGINE_MEGAKERNEL}) for p in params]
+
+    def plain_megakernel():
+        for ds, p, o in zip(dss, mk_params, plain_outs):
+            ds.render_device(p, o.data_ptr(), stream=sp)
+
     def timed(fn, steps):
         evs = []
         for k in range(steps):
@@ -283,12 +289,28 @@ def run_batched(args, rank, world, local):
     b_ms = timed(lambda: (batched(), stats.append(ctx.last_stats())), args.steps)
     p_steps = max(1, min(args.steps, 2))
     p_ms = timed(plain, p_steps)
+    plain_megakernel()
+    m_ms = timed(plain_megakernel, 1)
     clk = clocks.stop()
+    # the reference's per-call pattern (launchGPU builds and uploads its world for every image):
+    # rtc_scene_create + rtc_render with a host buffer + destroy, per image, one pass
+    t = time.perf_counter()
+    for (sc, _), p in zip(work, params):
+        host_img = np.empty((p.height, p.width, 4), np.float32)
+        d2 = DeviceScene(ctx, sc)
+        import ctypes as C
+        from cortexraytracercuda_b200._lib import check
+        pc = p.to_c()
+        check(ctx.lib.rtc_render(ctx.handle, d2.handle, C.byref(pc), host_img.ctypes.data, None))
+        d2.close()
+    l_s = time.perf_counter() - t
     b_tot = _max_over_ranks(float(np.sum(b_ms)), world)
     p_tot = _max_over_ranks(float(np.sum(p_ms)), world)
     value = paths * world * args.steps / (b_tot / 1e3) / 1e6
     plain_value = paths * world * p_steps / (p_tot / 1e3) / 1e6
     # same images: bit-identical pixels and image-mean agreement of batched vs plain
+    plain()
+    torch.cuda.synchronize()
     same, mean_dev = [], []
     for o, q in zip(outs, plain_outs):
         a, b = o[..., :3].double().nan_to_num(), q[..., :3].double().nan_to_num()
@@ -319,8 +341,17 @@ def run_batched(args, rank, world, local):
                        "l2": "flushed between steps (256 MiB write)", "seed": configs.DEFAULT_SEED,
                        "parallelism": f"replicas x{world}"},
             "plain": {"value": round(plain_value, 3), "unit": METRIC, "ms_per_step": round(p_tot / p_steps, 3),
-                      "form": "one rtc_render_device per image"},
+                      "form": "one rtc_render_device per image, wavefront engine, scene resident"},
+            "plain_megakernel": {"value": round(paths / (m_ms[0] / 1e3) / 1e6, 3), "unit": METRIC,
+                                 "ms_per_step": round(m_ms[0], 3),
+                                 "form": "one rtc_render_device per image, megakernel (one thread per pixel, "
+                                         "the reference's kernel shape), scene resident"},
+            "plain_launchgpu": {"value": round(paths / l_s / 1e6, 3), "unit": METRIC, "ms_per_step": round(l_s * 1e3, 1),
+                                "form": "per image: rtc_scene_create (host BVH + upload) + rtc_render to a host "
+                                        "buffer + destroy, as launchGPU rebuilds its world per call"},
             "batched_over_plain": round(value / plain_value, 3),
+            "batched_over_plain_megakernel": round(value / (paths / (m_ms[0] / 1e3) / 1e6), 3),
+            "batched_over_plain_launchgpu": round(value / (paths / l_s / 1e6), 3),
             "equal_to_plain": {"bit_identical_pixels_min": round(min(same), 4),
                                "image_mean_rel_dev_max": round(max(mean_dev), 6)},
             "gpu_launches": int(sum(st["launches"] for st in stats)),

@@ -66,9 +66,9 @@ extern "C" rtc_status rtc_render_batch(rtc_context* c, const rtc_job* jobs, uint
     cfg.num_sms = c->num_sms;
     cfg.mode = jobs[0].params.mode;
     cfg.draw_order = cfg.mode == RTC_MODE_CLEAN ? RTC_DRAW_ORDER_DEVICE : jobs[0].params.draw_order;
-    cfg.slots = bp && bp->slots ? bp->slots : (uint32_t)std::min<uint64_t>(total_pix, 1u << 20);
+    cfg.slots = bp && bp->slots ? bp->slots : (uint32_t)std::min<uint64_t>(total_pix, 1u << 22);
     cfg.ring = bp && bp->ring ? bp->ring : 1024u;
-    cfg.batch = bp && bp->batch > 0 ? bp->batch : 8;
+    cfg.batch = bp && bp->batch > 0 ? bp->batch : 12;
     cfg.drain = bp ? bp->drain : 0u;
     if (cfg.ring != next_pow2(cfg.ring)) return rtc_set_error(RTC_ERR_INVALID_ARGUMENT, "ring must be a power of two");
 
@@ -87,6 +87,7 @@ extern "C" rtc_status rtc_render_batch(rtc_context* c, const rtc_job* jobs, uint
     }
     Engine& E = *c->engine;
     E.set_stream(st);
+    E.set_counters(bp ? bp->d_counters : nullptr);
     rtc_status r = E.reset();
     if (r != RTC_OK) return r;
 

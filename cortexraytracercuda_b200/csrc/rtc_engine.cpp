@@ -31,6 +31,7 @@ rtc_status cuda_err(cudaError_t e, const char* what) {
 
 Engine::~Engine() {
     if (st_) cudaStreamSynchronize(st_);
+    drop_graph();
     cudaFree(d_wf_);
     cudaFree(d_jobs_);
     cudaFree(d_prog_);
@@ -170,16 +171,48 @@ rtc_status Engine::observe(int slot) {
     return RTC_OK;
 }
 
-rtc_status Engine::step() {
-    if (staged_from_ < hi_ || refill_) {
-        rtc_status r = enqueue_admit();
-        if (r != RTC_OK) return r;
-    }
+void Engine::drop_graph() {
+    if (graph_) cudaGraphExecDestroy(graph_);
+    graph_ = nullptr;
+}
+
+rtc_status Engine::enqueue_iterations() {
     WfTableArgs A{d_jobs_, (WfFeed*)d_prog_, (uint32_t*)(d_prog_ + sizeof(WfFeed)), cfg_.ring - 1};
     WfLaunch L{};
     L.status = d_status_;
-    L.st = st_;
+    L.counters = counters_;
     L.grid = cfg_.num_sms * 8;
+    const bool use_graph = cfg_.graphs && st_ != nullptr && cfg_.batch % 6 == 0 && it_ % 6 == 0;
+    if (use_graph && (!graph_ || graph_counters_ != counters_)) {
+        drop_graph();
+        cudaGraph_t g = nullptr;
+        ENG_CUDA(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
+        L.st = st_;
+        cudaError_t e = cudaSuccess;
+        for (int k = 0; k < 6 && e == cudaSuccess; ++k) {
+            L.w = wf_iter((uint64_t)k);
+            e = fn_(WF_OP_EXTEND, A, B_, L);
+            if (e == cudaSuccess) e = fn_(WF_OP_SHADE, A, B_, L);
+        }
+        cudaError_t e2 = cudaStreamEndCapture(st_, &g);
+        if (e == cudaSuccess) e = e2;
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&graph_, g, 0);
+        if (g) cudaGraphDestroy(g);
+        if (e != cudaSuccess) {   // capture unavailable here: launch directly from now on
+            graph_ = nullptr;
+            cfg_.graphs = false;
+            cudaGetLastError();
+        } else {
+            graph_counters_ = counters_;
+        }
+    }
+    if (use_graph && graph_) {
+        for (int k = 0; k < cfg_.batch; k += 6) ENG_CUDA(cudaGraphLaunch(graph_, st_));
+        it_ += (uint64_t)cfg_.batch;
+        launches_ += 2u * (uint64_t)cfg_.batch;
+        return RTC_OK;
+    }
+    L.st = st_;
     for (int k = 0; k < cfg_.batch; ++k, ++it_) {
         L.w = wf_iter(it_);
         cudaError_t e = fn_(WF_OP_EXTEND, A, B_, L);
@@ -187,7 +220,17 @@ rtc_status Engine::step() {
         if (e != cudaSuccess) return cuda_err(e, "wavefront iteration");
         launches_ += 2;
     }
-    rtc_status r = enqueue_poll();
+    return RTC_OK;
+}
+
+rtc_status Engine::step() {
+    if (staged_from_ < hi_ || refill_) {
+        rtc_status r = enqueue_admit();
+        if (r != RTC_OK) return r;
+    }
+    rtc_status r = enqueue_iterations();
+    if (r != RTC_OK) return r;
+    r = enqueue_poll();
     if (r != RTC_OK) return r;
     const int slot = batch_no_ & 1;
     ++batch_no_;
@@ -205,6 +248,7 @@ rtc_status Engine::finish() {
     WfLaunch L{};
     L.w = wf_iter(it_);
     L.status = d_status_;
+    L.counters = counters_;
     L.st = st_;
     L.grid = (int)std::max<uint32_t>(1u, (drain_ + 127u) / 128u);
     cudaError_t e = fn_(WF_OP_FINISH, A, B_, L);

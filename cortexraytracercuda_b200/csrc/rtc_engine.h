@@ -26,12 +26,13 @@ namespace rtc {
 struct EngineConfig {
     int device = 0;
     int num_sms = 148;
-    uint32_t slots = 1u << 20;     // path slots (pixels in flight)
+    uint32_t slots = 1u << 22;     // path slots (pixels in flight)
     uint32_t ring = 1024;          // job ring capacity (power of two, <= 65536)
     int mode = RTC_MODE_COMPAT;    // every job of an engine shares mode and draw order
     int draw_order = RTC_DRAW_ORDER_DEVICE;
-    int batch = 8;                 // iterations per batch
+    int batch = 12;                // iterations per batch
     uint32_t drain = 0;            // drain threshold in slots (0: 512 per SM)
+    bool graphs = true;            // replay batches as a captured CUDA graph (batch a multiple of 6)
 };
 
 // Host view of one admitted job.
@@ -88,11 +89,15 @@ public:
     cudaStream_t stream() const { return st_; }
     // Changes the stream of the next run (call between runs only).
     void set_stream(cudaStream_t st) { st_ = st; }
+    // Instrumentation counters (8 device uint64) for the next run, or null.
+    void set_counters(unsigned long long* c) { counters_ = c; }
 
 private:
     rtc_status enqueue_admit();
     rtc_status enqueue_poll();
     rtc_status observe(int slot);
+    rtc_status enqueue_iterations();
+    void drop_graph();
 
     EngineConfig cfg_;
     cudaStream_t st_ = nullptr;
@@ -102,6 +107,7 @@ private:
     DevJob* d_jobs_ = nullptr;
     uint8_t* d_prog_ = nullptr;     // WfFeed, then done[ring]
     uint32_t* d_status_ = nullptr;
+    unsigned long long* counters_ = nullptr;
     DevJob* h_jobs_ = nullptr;      // pinned staging of job records
     uint8_t* h_poll_ = nullptr;     // pinned: 2 x (live count, pad, WfFeed, done[ring])
     size_t poll_bytes_ = 0;
@@ -124,6 +130,10 @@ private:
     uint64_t jobs_total_ = 0, jobs_done_ = 0;
     std::vector<uint64_t> completed_;
     uint64_t it_ = 0, launches_ = 0;
+    // six (extend, shade) iterations captured once: the queue rotation repeats every six iterations,
+    // so the same graph serves every batch that starts at a multiple of six
+    cudaGraphExec_t graph_ = nullptr;
+    unsigned long long* graph_counters_ = nullptr;
 };
 
 }  // namespace rtc

@@ -206,7 +206,7 @@ __device__ __forceinline__ bool shade_bounce(const DevScene& S, Ray& r, bool hit
         float t2;
         uint32_t item2;
         pc.rays++;
-        if (closest_hit(S, r.o, r.d, h.t + 0.001f, 3.402823466e+38f, hide, t2, item2, st, status)) {
+        if (closest_hit<CLEAN>(S, r.o, r.d, h.t + 0.001f, 3.402823466e+38f, hide, t2, item2, st, status)) {
             finalize_hit<FT>(S, item2, t2, r.o, r.d, h);
             if ((uint32_t)h.mat >= S.num_materials) { status |= STATUS_BAD_MATERIAL; return false; }
             mi = __ldg(S.mat_i + h.mat);
@@ -303,7 +303,7 @@ __device__ __forceinline__ RGB trace_sample(const DevScene& S, Ray r, int max_de
         float t;
         uint32_t item;
         pc.rays++;
-        bool hit = closest_hit(S, r.o, r.d, 0.00001f, 3.402823466e+38f, hide, t, item, st, status);
+        bool hit = closest_hit<CLEAN>(S, r.o, r.d, 0.00001f, 3.402823466e+38f, hide, t, item, st, status);
         if (!shade_bounce<CLEAN, ORDER>(S, r, hit, t, item, hide, result, att, rng, pc, st, status)) break;
     }
     pc.nodes += st.nodes;

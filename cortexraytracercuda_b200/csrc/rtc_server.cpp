@@ -340,11 +340,11 @@ extern "C" rtc_status rtc_server_create(const rtc_server_config* cfg, rtc_server
     EngineConfig ec;
     ec.device = cfg->device;
     ec.num_sms = s->num_sms;
-    ec.slots = cfg->slots ? cfg->slots : (1u << 20);
+    ec.slots = cfg->slots ? cfg->slots : (1u << 22);
     ec.ring = cfg->ring ? cfg->ring : 1024u;
     ec.mode = s->cfg.mode;
     ec.draw_order = s->cfg.draw_order;
-    ec.batch = cfg->batch > 0 ? cfg->batch : 8;
+    ec.batch = cfg->batch > 0 ? cfg->batch : 12;
     s->eng.reset(new (std::nothrow) Engine());
     if (!s->eng) return rtc_set_error(RTC_ERR_OOM, "host allocation failed");
     rtc_status r = s->eng->init(ec, s->st);

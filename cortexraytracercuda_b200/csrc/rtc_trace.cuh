@@ -125,6 +125,29 @@ __device__ __forceinline__ bool sphere_t(float4 s, V3 o, V3 d, float tmin, float
     return true;
 }
 
+// Clean mode's sphere test: the same quadratic in double.  In float, |o-c|^2 - r^2 cancels
+// catastrophically for large spheres (a ground sphere of radius 1000: ulp(1e6) = 0.06), so hit
+// distances are off by ~3e-5, more than tmin and the robust offset, and bounce rays re-hit their own
+// surface: the float image is ~5% darker than the double-precision estimate on such scenes.  The
+// reference has the same defect, which compat mode keeps.
+__device__ __forceinline__ bool sphere_t_exact(float4 s, V3 o, V3 d, float tmin, float tmax, float& t) {
+    const double ox = (double)o.x - (double)s.x, oy = (double)o.y - (double)s.y, oz = (double)o.z - (double)s.z;
+    const double dx = d.x, dy = d.y, dz = d.z;
+    const double a = dx * dx + dy * dy + dz * dz;
+    const double hb = ox * dx + oy * dy + oz * dz;
+    const double cc = ox * ox + oy * oy + oz * oz - (double)s.w * (double)s.w;
+    const double disc = hb * hb - a * cc;
+    if (disc < 0.0) return false;
+    const double sq = sqrt(disc);
+    double root = (-hb - sq) / a;
+    if (!((double)tmin < root && root < (double)tmax)) {
+        root = (-hb + sq) / a;
+        if (!((double)tmin < root && root < (double)tmax)) return false;
+    }
+    t = (float)root;
+    return true;
+}
+
 // quad::hit (quad.cuh:100-133) and directional_light::hit (directional_light.cuh:76-120).
 // q0 = (n, D), q1 = (Q or P), q2 = u, q3 = v, q4 = w.  centred: light interior test on [-0.5, 0.5].
 __device__ __forceinline__ bool planar_t(float4 q0, float4 q1, float4 q2, float4 q3, float4 q4, V3 o, V3 d,
@@ -199,7 +222,8 @@ __device__ __forceinline__ bool slab2(const float4 n0, const float4 n1, const fl
     return lin <= lout;
 }
 
-// Tests every item of one leaf against [tmin, best_t]; returns true when the status word must be set.
+// Tests every item of one leaf against [tmin, best_t].  EXACT: clean mode's double-precision sphere test.
+template <bool EXACT>
 __device__ __forceinline__ void test_leaf(const DevScene& S, int32_t child, V3 o, V3 d, float tmin, float& best_t,
                                           uint32_t& best_item, bool hide_invisible, TraceStats& st,
                                           uint32_t& status) {
@@ -220,7 +244,11 @@ __device__ __forceinline__ void test_leaf(const DevScene& S, int32_t child, V3 o
         } break;
         case ITEM_SPHERE: {
             if (idx >= S.num_sph) { status |= STATUS_BAD_ITEM; break; }
-            if (sphere_t(ld_scene(S.sph + idx), o, d, tmin, best_t, t)) { best_t = t; best_item = it; }
+            const float4 sp = ld_scene(S.sph + idx);
+            if (EXACT ? sphere_t_exact(sp, o, d, tmin, best_t, t) : sphere_t(sp, o, d, tmin, best_t, t)) {
+                best_t = t;
+                best_item = it;
+            }
         } break;
         case ITEM_QUAD: {
             if (idx >= S.num_quad) { status |= STATUS_BAD_ITEM; break; }
@@ -247,6 +275,8 @@ __device__ __forceinline__ void test_leaf(const DevScene& S, int32_t child, V3 o
 }
 
 // Closest hit in [tmin, tmax] over the whole scene (the reference's world.hit through the BVH).
+// EXACT: clean mode (double-precision sphere test).
+template <bool EXACT = false>
 __device__ __forceinline__ bool closest_hit(const DevScene& S, V3 o, V3 d, float tmin, float tmax,
                                             bool hide_invisible, float& t_out, uint32_t& item_out,
                                             TraceStats& st, uint32_t& status) {
@@ -265,8 +295,8 @@ __device__ __forceinline__ bool closest_hit(const DevScene& S, V3 o, V3 d, float
         float tl, tr;
         bool hr;
         bool hl = slab2(n0, n1, n2, inv, oi, tmin, best_t, tl, tr, hr);
-        if (hl && cl < 0) { test_leaf(S, cl, o, d, tmin, best_t, best_item, hide_invisible, st, status); hl = false; }
-        if (hr && cr < 0) { test_leaf(S, cr, o, d, tmin, best_t, best_item, hide_invisible, st, status); hr = false; }
+        if (hl && cl < 0) { test_leaf<EXACT>(S, cl, o, d, tmin, best_t, best_item, hide_invisible, st, status); hl = false; }
+        if (hr && cr < 0) { test_leaf<EXACT>(S, cr, o, d, tmin, best_t, best_item, hide_invisible, st, status); hr = false; }
         if (hl && hr) {
             int32_t nearc = tl <= tr ? cl : cr;
             int32_t farc = tl <= tr ? cr : cl;

@@ -215,6 +215,7 @@ __global__ void __launch_bounds__(128) wf_admit(WfTable J, WfBuffers B, WfIter w
     if (status) atomicOr(status_word, status);
 }
 
+// FLAVOR: 0 nvcc flavour, 1 g++ flavour, 2 clean mode (double-precision sphere test).
 template <bool COUNT, int FLAVOR, class J>
 __global__ void __launch_bounds__(128) wf_extend(J jobs, WfBuffers B, WfIter w, unsigned long long* counters,
                                                  uint32_t* status_word) {
@@ -231,8 +232,8 @@ __global__ void __launch_bounds__(128) wf_extend(J jobs, WfBuffers B, WfIter w, 
         const uint32_t job = wf_job(mw);
         float t;
         uint32_t item;
-        bool h = closest_hit(jobs.scene(job), v3(o), v3(d), 0.00001f, 3.402823466e+38f,
-                             wf_depth(mw) == (uint32_t)jobs.params(job).max_depth, t, item, st, status);
+        bool h = closest_hit<FLAVOR == 2>(jobs.scene(job), v3(o), v3(d), 0.00001f, 3.402823466e+38f,
+                                          wf_depth(mw) == (uint32_t)jobs.params(job).max_depth, t, item, st, status);
         B.hit[slot] = make_float2(t, __uint_as_float(h ? item : 0xffffffffu));
         ++rays;
     }
@@ -392,7 +393,7 @@ __global__ void __launch_bounds__(128) wf_bounce(J jobs, WfBuffers B, WfIter w, 
             float t;
             uint32_t item;
             ++rays;
-            bool h = closest_hit(jobs.scene(job), v3(o), v3(d), 0.00001f, 3.402823466e+38f,
+            bool h = closest_hit<CLEAN>(jobs.scene(job), v3(o), v3(d), 0.00001f, 3.402823466e+38f,
                                  wf_depth(mw) == (uint32_t)jobs.params(job).max_depth, t, item, st, status);
             live = wf_step<CLEAN, ORDER>(jobs, win, B, slot, t, h ? item : 0xffffffffu, pc, st, paths, status);
         }
@@ -442,7 +443,7 @@ __global__ void __launch_bounds__(128) wf_finish(J jobs, WfBuffers B, WfIter w, 
                 float t;
                 uint32_t item;
                 pc.rays++;
-                bool h = closest_hit(S, r.o, r.d, 0.00001f, 3.402823466e+38f, hide, t, item, st, status);
+                bool h = closest_hit<CLEAN>(S, r.o, r.d, 0.00001f, 3.402823466e+38f, hide, t, item, st, status);
                 if (!shade_bounce<CLEAN, ORDER>(S, r, h, t, item, hide, acc, att, rng, pc, st, status)) break;
             }
             ++paths;

@@ -106,7 +106,8 @@ class rtc_job(C.Structure):
 
 
 class rtc_batch_params(C.Structure):
-    _fields_ = [("slots", C.c_uint32), ("ring", C.c_uint32), ("batch", C.c_int32), ("drain", C.c_uint32)]
+    _fields_ = [("slots", C.c_uint32), ("ring", C.c_uint32), ("batch", C.c_int32), ("drain", C.c_uint32),
+                ("d_counters", C.c_void_p)]
 
 
 class rtc_server_config(C.Structure):

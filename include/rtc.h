@@ -330,11 +330,16 @@ typedef struct rtc_job {
 } rtc_job;
 
 typedef struct rtc_batch_params {
-    uint32_t slots;    /* path slots (pixels in flight); 0: min(total pixels, 2^20)                      */
+    uint32_t slots;    /* path slots (pixels in flight); 0: min(total pixels, 2^22)                      */
     uint32_t ring;     /* job ring capacity, a power of two <= 65536; 0: 1024.  Larger batches are
                           admitted as earlier images complete.                                            */
-    int32_t batch;     /* (extend, shade) iterations between two host polls; 0: 8                        */
-    uint32_t drain;    /* queued slots below which the drain kernel finishes the batch; 0: 512 per SM   */
+    int32_t batch;     /* (extend, shade) iterations between two host polls; 0: 12.  A multiple of 6 is
+                          replayed as a captured CUDA graph of six iterations                             */
+    uint32_t drain;    /* queued slots below which the drain kernel finishes the batch; 0: 512 per SM;
+                          1: no drain (every bounce runs in the extend/shade kernels)                     */
+    unsigned long long* d_counters;   /* NULL, or 8 device uint64 (zeroed by the caller) that receive the
+                          counts of rtc_render_device: rays, paths, node visits, primitive tests, then the
+                          extend kernel's own rays, node visits and primitive tests                      */
 } rtc_batch_params;
 
 /* Renders `num_jobs` images on `stream` (a cudaStream_t, or NULL for the context's stream) and returns
@@ -361,8 +366,8 @@ typedef struct rtc_server_config {
     int32_t device;
     int32_t mode;                /* rtc_mode, shared by every request                                  */
     int32_t draw_order;          /* rtc_draw_order (COMPAT), shared by every request                   */
-    int32_t batch;               /* (extend, shade) iterations between two host polls; 0: 8            */
-    uint32_t slots;              /* path slots; 0: 2^20                                                 */
+    int32_t batch;               /* (extend, shade) iterations between two host polls; 0: 12           */
+    uint32_t slots;              /* path slots; 0: 2^22                                                 */
     uint32_t ring;               /* requests in flight at most (power of two <= 65536); 0: 1024        */
     uint64_t hbm_budget_bytes;   /* device bytes for slots, resident scenes and request outputs;
                                     0: 120 GB                                                           */

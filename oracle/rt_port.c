@@ -323,6 +323,26 @@ static int sphere_t(const prim_t* p, v3 o, v3 d, float tmin, float tmax, float* 
     return 1;
 }
 
+/* Clean mode: the same quadratic in double (the float form cancels catastrophically for large
+ * spheres; the clean kernels do the same). */
+static int sphere_t_exact(const prim_t* p, v3 o, v3 d, float tmin, float tmax, float* t) {
+    double ox = (double)o.x - (double)p->a.x, oy = (double)o.y - (double)p->a.y, oz = (double)o.z - (double)p->a.z;
+    double dx = d.x, dy = d.y, dz = d.z;
+    double a = dx * dx + dy * dy + dz * dz;
+    double hb = ox * dx + oy * dy + oz * dz;
+    double c = ox * ox + oy * oy + oz * oz - (double)p->rad * (double)p->rad;
+    double disc = hb * hb - a * c;
+    if (disc < 0.0) return 0;
+    double sq = sqrt(disc);
+    double root = (-hb - sq) / a;
+    if (!((double)tmin < root && root < (double)tmax)) {
+        root = (-hb + sq) / a;
+        if (!((double)tmin < root && root < (double)tmax)) return 0;
+    }
+    *t = (float)root;
+    return 1;
+}
+
 /* quad::hit (quad.cuh:100-133) and directional_light::hit (directional_light.cuh:76-120) */
 static int planar_t(const prim_t* p, v3 o, v3 d, float tmin, float tmax, int centred, float* t, float* al, float* be) {
     float denom = vdot(p->normal, d);
@@ -357,10 +377,10 @@ static int tri_t(const prim_t* p, v3 o, v3 d, float tmin, float tmax, float* t, 
     return 1;
 }
 
-static int prim_t_test(const prim_t* p, v3 o, v3 d, float tmin, float tmax, int hide, float* t) {
+static int prim_t_test(const prim_t* p, v3 o, v3 d, float tmin, float tmax, int hide, int exact, float* t) {
     float a, b;
     switch (p->kind) {
-    case K_SPHERE: return sphere_t(p, o, d, tmin, tmax, t);
+    case K_SPHERE: return exact ? sphere_t_exact(p, o, d, tmin, tmax, t) : sphere_t(p, o, d, tmin, tmax, t);
     case K_QUAD: return planar_t(p, o, d, tmin, tmax, 0, t, &a, &b);
     case K_LIGHT:
         if (!planar_t(p, o, d, tmin, tmax, 1, t, &a, &b)) return 0;
@@ -383,7 +403,8 @@ static int box_hit(const node_t* n, v3 o, v3 d, float tmin, float tmax) {
     return 1;
 }
 
-static int closest(const scene_t* s, v3 o, v3 d, float tmin, float tmax, int hide, float* tout, int* pout) {
+/* exact: clean mode's double-precision sphere test */
+static int closest(const scene_t* s, v3 o, v3 d, float tmin, float tmax, int hide, int exact, float* tout, int* pout) {
     int stack[128], sp = 0, best = -1;
     float best_t = tmax;
     if (s->nprims == 0) return 0;
@@ -394,7 +415,7 @@ static int closest(const scene_t* s, v3 o, v3 d, float tmin, float tmax, int hid
         if (n->left < 0) {
             for (int i = n->first; i < n->first + n->count; ++i) {
                 float t;
-                if (prim_t_test(&s->prims[s->order[i]], o, d, tmin, best_t, hide, &t)) { best_t = t; best = s->order[i]; }
+                if (prim_t_test(&s->prims[s->order[i]], o, d, tmin, best_t, hide, exact, &t)) { best_t = t; best = s->order[i]; }
             }
         } else {
             if (sp + 2 > 128) return 0;
@@ -544,7 +565,7 @@ static rgb_t ray_color(const scene_t* s, v3 o, v3 d, int max_depth, rng_t* rng, 
         int hide = depth == max_depth;
         float t; int pi;
         (*rays)++;
-        if (!closest(s, o, d, 0.00001f, FLT_MAX, hide, &t, &pi)) {
+        if (!closest(s, o, d, 0.00001f, FLT_MAX, hide, clean, &t, &pi)) {
             rgb_t bg = background(s, d);
             res.r += att.r * bg.r; res.g += att.g * bg.g; res.b += att.b * bg.b;
             break;
@@ -561,7 +582,7 @@ static rgb_t ray_color(const scene_t* s, v3 o, v3 d, int max_depth, rng_t* rng, 
         if (alpha0) {   /* invisible re-hit (camera.cuh:177-183) */
             float t2; int p2;
             (*rays)++;
-            if (closest(s, o, d, h.t + 0.001f, FLT_MAX, hide, &t2, &p2)) { finalize(s, p2, t2, o, d, &h); m = &s->mat[h.mat]; }
+            if (closest(s, o, d, h.t + 0.001f, FLT_MAX, hide, clean, &t2, &p2)) { finalize(s, p2, t2, o, d, &h); m = &s->mat[h.mat]; }
         }
         if (m->kind == RTC_MAT_DIFFUSE_LIGHT) {
             res.r += att.r * em.r; res.g += att.g * em.g; res.b += att.b * em.b;
@@ -754,7 +775,7 @@ int port_trace_closest(void* sp, const float* rays, int64_t n, int depth, int ma
     for (int64_t k = 0; k < n; ++k) {
         const float* R = rays + 8 * k;
         float t; int pi;
-        int h = closest(s, V(R[0], R[1], R[2]), V(R[4], R[5], R[6]), R[3], R[7], depth == max_depth, &t, &pi);
+        int h = closest(s, V(R[0], R[1], R[2]), V(R[4], R[5], R[6]), R[3], R[7], depth == max_depth, 0, &t, &pi);
         if (prim) prim[k] = h ? pi : -1;
         if (tout) tout[k] = h ? t : INFINITY;
     }

@@ -231,6 +231,39 @@ def port():
     return Port(lib) if lib else None
 
 
+class Fp64:
+    """The double-precision clean-mode estimator (oracle/fp64_clean.c): converged-image reference."""
+
+    def __init__(self, lib):
+        self.lib = lib
+        lib.f64_scene_create.restype = C.c_void_p
+        lib.f64_scene_destroy.argtypes = [C.c_void_p]
+        lib.f64_render.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint32, C.c_void_p,
+                                   C.c_int64, C.c_void_p, C.c_int]
+
+    def render(self, scene: Scene, width: int, height: int, spp: int, max_depth: int, seed: int,
+               pix: np.ndarray | None = None, threads: int = 0) -> np.ndarray:
+        """Radiance sums (n, 3) float64 of the given frame-buffer pixels (all pixels by default)."""
+        import os
+        d = SceneDesc(scene)
+        h = self.lib.f64_scene_create(d.ptr())
+        try:
+            if pix is None:
+                pix = np.arange(width * height, dtype=np.int64)
+            pix = np.ascontiguousarray(pix, dtype=np.int64)
+            out = np.empty((pix.size, 3), np.float64)
+            self.lib.f64_render(h, width, height, spp, max_depth, seed & 0xFFFFFFFF, pix.ctypes.data, pix.size,
+                                out.ctypes.data, threads or (os.cpu_count() or 1))
+        finally:
+            self.lib.f64_scene_destroy(h)
+        return out
+
+
+def fp64():
+    lib = _load(ORACLE / "librt_fp64.so")
+    return Fp64(lib) if lib else None
+
+
 def ref_cpu():
     lib = _load(ORACLE / "_ref" / "libref_cpu.so")
     return RefCpu(lib) if lib else None
