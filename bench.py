@@ -50,7 +50,8 @@ sys.path.insert(0, str(ROOT))
 
 from cortexraytracercuda_b200 import configs  # noqa: E402
 from cortexraytracercuda_b200.scene import (DRAW_ORDER_DEVICE, DRAW_ORDER_HOST, ENGINE_MEGAKERNEL,  # noqa: E402
-                                            ENGINE_WAVEFRONT, FLAG_KERNEL_TIMING, MODE_CLEAN, MODE_COMPAT)
+                                            ENGINE_WAVEFRONT, FLAG_KERNEL_TIMING, FLAG_WIDE_BVH, MODE_CLEAN,
+                                            MODE_COMPAT)
 
 METRIC = "Mpaths/s"
 PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
@@ -58,6 +59,7 @@ FALLBACK_HBM_GBS = 6650.0
 
 # bytes fetched per visit (ignoring caches) for the roofline's algorithmic traffic
 NODE_BYTES = 64          # BVH2 node: two child boxes + two child links (4 x float4)
+NODE4_BYTES = 128        # 4-wide node: four child boxes + four child links (8 x float4, one cache line)
 PRIM_BYTES = {"spheres": 16, "cornell": 48, "meshes": 48}   # dominant primitive record of each workload
 STATE_BYTES = 32 + 16 + 2 * 48   # ray read + hit write + path state read/write per traversal
 EXTEND_STATE_BYTES = 4 + 32 + 4 + 8   # queue entry + ray (origin, direction) + depth word read, hit record write
@@ -241,6 +243,8 @@ def run_batched(args, rank, world, local):
     params = []
     for _, p in work:
         p.mode, p.draw_order, p.engine = mode, order, ENGINE_WAVEFRONT
+        if args.bvh == "4":
+            p.flags |= FLAG_WIDE_BVH
         params.append(p)
     outs = [torch.empty((p.height, p.width, 4), dtype=torch.float32, device="cuda") for p in params]
     plain_outs = [torch.empty_like(o) for o in outs]
@@ -519,6 +523,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--mode", default="compat", choices=["compat", "clean"])
     ap.add_argument("--engine", default="wavefront", choices=["wavefront", "megakernel"])
+    ap.add_argument("--bvh", default="2", choices=["2", "4"], help="BVH node layout (binary or 4-wide)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-baseline-s", type=float, default=12.0)
     ap.add_argument("--ref-step-s", type=float, default=8.0)
@@ -568,6 +573,8 @@ def main():
     if args.small:
         params.width, params.height, params.spp = params.width // 4, params.height // 4, 16
     params.engine = ENGINE_WAVEFRONT if args.engine == "wavefront" else ENGINE_MEGAKERNEL
+    if args.bvh == "4":
+        params.flags |= FLAG_WIDE_BVH
     ds = DeviceScene(ctx, scene)
     info = ds.info()
     W, H = params.width, params.height
@@ -650,12 +657,13 @@ def main():
     # ---- roofline -------------------------------------------------------------------------------
     peak, peak_kind = hbm_peak()
     prim_b = PRIM_BYTES[args.config]
+    node_b = NODE_BYTES if args.bvh == "2" else NODE4_BYTES
     if wavefront:
         # dominant kernel: wf_extend (closest-hit traversal of every queued ray).  Algorithmic bytes of
         # its launches in one frame, from its own counters, over its summed CUDA-event time.
         ext_ms = float(np.mean([st["extend_ms"] for st in kstats]))
         ext_launches = int(np.mean([st["extend_launches"] for st in kstats]))
-        ext_bytes = ext_nodes * NODE_BYTES + ext_prims * prim_b + ext_rays * EXTEND_STATE_BYTES
+        ext_bytes = ext_nodes * node_b + ext_prims * prim_b + ext_rays * EXTEND_STATE_BYTES
         achieved = ext_bytes / (ext_ms / 1e3) / 1e9
         roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": None,
@@ -671,7 +679,7 @@ def main():
                           "iterations": int(np.mean([st["iterations"] for st in kstats])),
                           "rays": rays, "paths": paths, "node_visits": nodes, "prim_tests": prims}}
     else:
-        alg_bytes = nodes * NODE_BYTES + prims * prim_b + rays * STATE_BYTES
+        alg_bytes = nodes * node_b + prims * prim_b + rays * STATE_BYTES
         achieved = alg_bytes / (kernel_ms / 1e3) / 1e9
         roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": None,
@@ -691,7 +699,7 @@ def main():
             "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {**describe(args.config, params, scene), "parallelism": f"replicas x{world}",
-                       "bvh_nodes": info["num_nodes"]},
+                       "bvh_nodes": info["num_nodes"], "bvh_layout": "binary" if args.bvh == "2" else "4-wide"},
             "mrays_per_s": round(mrays, 3),
             "gpu_launches": int(sum(st["launches"] for st in kstats)) if wavefront else args.steps,
             "e2e": {"value": round(e2e_value, 3), "unit": METRIC, "h2d_bytes_per_step": int(info["device_bytes"]),

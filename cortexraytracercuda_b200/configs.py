@@ -253,13 +253,18 @@ def meshes_params(**kw) -> RenderParams:
     return RenderParams(**p)
 
 
-def textured(seed=DEFAULT_SEED) -> Scene:
-    """Checker and image textures on spheres and quads, lit by a quad light and a sky."""
+def textured(seed=DEFAULT_SEED, floor_y=0.0) -> Scene:
+    """Checker and image textures on spheres and quads, lit by a quad light and a sky.
+
+    With the default floor_y = 0 the floor lies on a checker cell boundary (cells of 0.5 on every
+    axis), so the floor's cell parity, floor(2 * hit_y), is decided by the sign of the hit point's
+    rounding error - a rounding-level test of the texture path (bit-exact parity).  Convergence
+    comparisons lift the floor off the boundary."""
     s = Scene(name="textured")
     s.dir_light((0.0, 8.0, 0.0), (4.0, 0.0, 0.0), (0.0, 0.0, 4.0), (6.0, 6.0, 6.0), intensity=1.0, invisible=True)
     img = s.image(procedural_image(64, 48, seed))
     chk = s.checker_colors(0.5, (0.2, 0.3, 0.1), (0.9, 0.9, 0.9))   # all_textures_spheres.scene scale style
-    s.quad((-6.0, 0.0, -6.0), (12.0, 0.0, 0.0), (0.0, 0.0, 12.0), s.lambertian(chk))
+    s.quad((-6.0, floor_y, -6.0), (12.0, 0.0, 0.0), (0.0, 0.0, 12.0), s.lambertian(chk))
     s.sphere((-1.6, 1.0, 0.0), 1.0, s.lambertian(img))
     s.sphere((1.6, 1.0, 0.0), 1.0, s.lambertian(s.checker_colors(0.3, (0.8, 0.1, 0.1), (0.9, 0.9, 0.2))))
     s.sphere((0.0, 0.6, 1.8), 0.6, s.metal((0.9, 0.9, 0.9), 0.2))

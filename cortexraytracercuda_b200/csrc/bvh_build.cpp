@@ -41,14 +41,38 @@ inline double area(const Aabb& a) {
     return 2.0 * (dx * dy + dy * dz + dz * dx);
 }
 
-struct Builder {
+constexpr int PAR_DEPTH = 4;            // subtrees below the first four levels are built concurrently
+constexpr uint32_t PAR_MIN = 32768;     // ... when they hold at least this many primitives
+
+struct Shared {
     const std::vector<Aabb>& boxes;
     std::vector<float> cen;          // 3 per primitive
-    std::vector<uint32_t> idx;
+    std::vector<uint32_t> idx;       // subtrees partition disjoint ranges of it
+    int max_leaf;
+};
+
+struct Builder {
+    Shared& sh;
+    const std::vector<Aabb>& boxes;
+    std::vector<float>& cen;
+    std::vector<uint32_t>& idx;
     int max_leaf;
     std::vector<BNode> nodes;        // per-builder (one per subtree task)
 
-    Builder(const std::vector<Aabb>& b, int ml) : boxes(b), max_leaf(ml) {}
+    explicit Builder(Shared& s) : sh(s), boxes(s.boxes), cen(s.cen), idx(s.idx), max_leaf(s.max_leaf) {}
+
+    // Appends another builder's tree (its node 0 is its root); returns the root's id here.
+    int32_t splice(const Builder& o) {
+        const int32_t off = (int32_t)nodes.size();
+        for (BNode b : o.nodes) {
+            if (!b.leaf) {
+                b.left += off;
+                b.right += off;
+            }
+            nodes.push_back(b);
+        }
+        return off;
+    }
 
     int32_t build(uint32_t start, uint32_t end, int depth, uint32_t& max_depth) {
         int32_t id = (int32_t)nodes.size();
@@ -135,6 +159,20 @@ struct Builder {
             std::nth_element(idx.begin() + start, idx.begin() + mid, idx.begin() + end,
                              [&](uint32_t a, uint32_t b) { return cen[3 * a + ax] < cen[3 * b + ax]; });
         }
+        if (depth <= PAR_DEPTH && n >= PAR_MIN) {
+            // the two halves on two threads, each into its own node array, then spliced in
+            Builder L(sh), R(sh);
+            uint32_t dl = 0, dr = 0;
+            std::thread t([&] { L.build(start, mid, depth + 1, dl); });
+            R.build(mid, end, depth + 1, dr);
+            t.join();
+            max_depth = std::max(max_depth, std::max(dl, dr));
+            const int32_t l = splice(L);
+            const int32_t r = splice(R);
+            nodes[id].left = l;
+            nodes[id].right = r;
+            return id;
+        }
         int32_t l = build(start, mid, depth + 1, max_depth);
         int32_t r = build(mid, end, depth + 1, max_depth);
         nodes[id].left = l;
@@ -151,13 +189,14 @@ bool build_bvh(const BvhInput& in, int max_leaf, int threads, BvhOutput& out, co
     if (max_leaf < 1) max_leaf = 1;
     if (max_leaf > MAX_LEAF) max_leaf = MAX_LEAF;
     if (n >= (1u << 26)) { if (err) *err = "too many primitives for the leaf encoding (max 2^26)"; return false; }
-    Builder B(in.boxes, max_leaf);
-    B.cen.resize(3 * n);
-    B.idx.resize(n);
+    Shared SH{in.boxes, {}, {}, max_leaf};
+    SH.cen.resize(3 * n);
+    SH.idx.resize(n);
     for (size_t p = 0; p < n; ++p) {
-        B.idx[p] = (uint32_t)p;
-        for (int k = 0; k < 3; ++k) B.cen[3 * p + k] = 0.5f * (in.boxes[p].lo[k] + in.boxes[p].hi[k]);
+        SH.idx[p] = (uint32_t)p;
+        for (int k = 0; k < 3; ++k) SH.cen[3 * p + k] = 0.5f * (in.boxes[p].lo[k] + in.boxes[p].hi[k]);
     }
+    Builder B(SH);
     B.nodes.reserve(2 * n + 2);
     uint32_t max_depth = 0;
     int32_t root = n ? B.build(0, (uint32_t)n, 1, max_depth) : -1;
@@ -219,6 +258,118 @@ bool build_bvh(const BvhInput& in, int max_leaf, int threads, BvhOutput& out, co
     }
     out.num_nodes = (uint32_t)(out.nodes.size() / 16);
     out.max_depth = max_depth;
+
+    // 4-wide collapse of the same tree.  A wide node starts with its binary node's two children and
+    // repeatedly opens the inner child of largest surface area in place (left child where it was,
+    // right child just after it), so children stay in left-to-right order and the leaves are met in
+    // exactly the binary flattening's order: both layouts share one leaf order (items array).
+    out.nodes4.clear();
+    auto alloc4 = [&]() {
+        out.nodes4.resize(out.nodes4.size() + 32, 0.0f);
+        return (int32_t)(out.nodes4.size() / 32 - 1);
+    };
+    std::vector<int32_t> leaf_enc;
+    {
+        // the binary flattening assigned leaf encodings in DFS left-first order: replay it
+        std::vector<int32_t> st;
+        if (root >= 0) st.push_back(root);
+        uint32_t first = 0;
+        while (!st.empty()) {
+            int32_t b = st.back();
+            st.pop_back();
+            const BNode& bn = B.nodes[b];
+            if (bn.leaf) {
+                leaf_enc.push_back((int32_t)~((first << LEAF_COUNT_BITS) | bn.count));
+                first += bn.count;
+            } else {
+                st.push_back(bn.right);
+                st.push_back(bn.left);
+            }
+        }
+    }
+    std::vector<int32_t> leaf_of(B.nodes.size(), 0);
+    {
+        std::vector<int32_t> st;
+        if (root >= 0) st.push_back(root);
+        size_t k = 0;
+        while (!st.empty()) {
+            int32_t b = st.back();
+            st.pop_back();
+            const BNode& bn = B.nodes[b];
+            if (bn.leaf) {
+                leaf_of[b] = leaf_enc[k++];
+            } else {
+                st.push_back(bn.right);
+                st.push_back(bn.left);
+            }
+        }
+    }
+    auto put4 = [&](int32_t slot, int c, const Aabb& bx, int32_t enc) {
+        float* f = &out.nodes4[32 * (size_t)slot];
+        f[0 + c] = bx.lo[0];
+        f[4 + c] = bx.hi[0];
+        f[8 + c] = bx.lo[1];
+        f[12 + c] = bx.hi[1];
+        f[16 + c] = bx.lo[2];
+        f[20 + c] = bx.hi[2];
+        std::memcpy(&f[24 + c], &enc, 4);
+    };
+    const Aabb nobox = [] {
+        Aabb a;
+        for (int k = 0; k < 3; ++k) { a.lo[k] = INFINITY; a.hi[k] = -INFINITY; }
+        return a;
+    }();
+    struct Work4 { int32_t bnode; int32_t slot; uint32_t depth; };
+    std::vector<Work4> w4;
+    uint32_t depth4 = 1;
+    int32_t r4 = alloc4();
+    for (int c = 0; c < 4; ++c) put4(r4, c, nobox, (int32_t)~0u);
+    if (root >= 0) {
+        if (B.nodes[root].leaf) put4(r4, 0, B.nodes[root].box, leaf_of[root]);
+        else w4.push_back({root, r4, 1});
+    }
+    while (!w4.empty()) {
+        Work4 w = w4.back();
+        w4.pop_back();
+        depth4 = std::max(depth4, w.depth);
+        const BNode& bn = B.nodes[w.bnode];
+        int32_t ch[4] = {bn.left, bn.right, -1, -1};
+        int n = 2;
+        while (n < 4) {
+            int best = -1;
+            double ba = -1.0;
+            for (int i = 0; i < n; ++i) {
+                const BNode& c = B.nodes[ch[i]];
+                if (!c.leaf && area(c.box) > ba) { ba = area(c.box); best = i; }
+            }
+            if (best < 0) break;
+            const BNode& o = B.nodes[ch[best]];
+            for (int i = n; i > best + 1; --i) ch[i] = ch[i - 1];
+            ch[best] = o.left;
+            ch[best + 1] = o.right;
+            ++n;
+        }
+        // children are filled in order; inner children get their node index now and are expanded later
+        std::vector<Work4> kids;
+        for (int i = 0; i < 4; ++i) {
+            if (i >= n) { put4(w.slot, i, nobox, (int32_t)~0u); continue; }
+            const BNode& c = B.nodes[ch[i]];
+            if (c.leaf) {
+                put4(w.slot, i, c.box, leaf_of[ch[i]]);
+            } else {
+                int32_t s = alloc4();
+                put4(w.slot, i, c.box, s);
+                kids.push_back({ch[i], s, w.depth + 1});
+            }
+        }
+        for (auto it = kids.rbegin(); it != kids.rend(); ++it) w4.push_back(*it);
+    }
+    out.num_nodes4 = (uint32_t)(out.nodes4.size() / 32);
+    // the 4-wide walk holds at most 3 entries per level plus the leaves of the deepest node
+    if (3 * depth4 + 4 > (uint32_t)TRAVERSAL_STACK4) {
+        out.nodes4.clear();   // too deep for its stack: renders use the binary nodes
+        out.num_nodes4 = 0;
+    }
     if (max_depth + 2 > (uint32_t)TRAVERSAL_STACK) { if (err) *err = "BVH too deep for the traversal stack"; return false; }
     return true;
 }

@@ -23,8 +23,11 @@ struct BvhInput {
 
 struct BvhOutput {
     std::vector<float> nodes;      // 16 floats per node (4 x float4), see rtc_dev.h
+    std::vector<float> nodes4;     // the same tree collapsed to 4-wide nodes: 32 floats (8 x float4) per
+                                   // node, see rtc_dev.h; same leaves, same leaf order
     std::vector<uint32_t> order;   // primitive index per leaf slot, leaf order
     uint32_t num_nodes = 0;
+    uint32_t num_nodes4 = 0;
     uint32_t max_depth = 0;
     uint32_t max_leaf_seen = 0;
 };

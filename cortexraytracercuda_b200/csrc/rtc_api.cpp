@@ -169,6 +169,12 @@ bool rtc_make_camera(const rtc_camera& C, DevCamera& cam) {
 }
 
 const DevScene& rtc_scene_dev(const rtc_scene* s) { return s->dev; }
+
+DevScene rtc_scene_view(const rtc_scene* s, const rtc_render_params* p) {
+    DevScene S = s->dev;
+    if (!p || !(p->flags & RTC_FLAG_WIDE_BVH)) S.nodes4 = nullptr;
+    return S;
+}
 DevParams rtc_dev_params(const rtc_render_params* p);
 
 rtc_status rtc_build_host_scene(const rtc_scene_desc* d, HostScene& H) {
@@ -401,6 +407,7 @@ rtc_status rtc_build_host_scene(const rtc_scene_desc* d, HostScene& H) {
         return off;
     };
     size_t o_nodes = add_chunk(bvh.nodes.data(), bvh.nodes.size() * sizeof(float));
+    size_t o_nodes4 = add_chunk(bvh.nodes4.data(), bvh.nodes4.size() * sizeof(float));
     size_t o_items = add_chunk(items.data(), items.size() * 4);
     size_t o_sph = add_chunk(sph.data(), sph.size() * 16);
     size_t o_sphx = add_chunk(sph_aux.data(), sph_aux.size() * 8);
@@ -427,6 +434,7 @@ rtc_status rtc_build_host_scene(const rtc_scene_desc* d, HostScene& H) {
     DevScene& D = H.dev;
     D = DevScene{};
     D.nodes = (const float4*)off(o_nodes);
+    D.nodes4 = bvh.num_nodes4 ? (const float4*)off(o_nodes4) : nullptr;
     D.items = (const uint32_t*)off(o_items);
     D.sph = (const float4*)off(o_sph);
     D.sph_aux = (const int2*)off(o_sphx);
@@ -442,6 +450,7 @@ rtc_status rtc_build_host_scene(const rtc_scene_desc* d, HostScene& H) {
     D.images = (const int4*)off(o_img);
     D.image_bytes = (const uint8_t*)off(o_imgb);
     D.num_nodes = bvh.num_nodes;
+    D.num_nodes4 = bvh.num_nodes4;
     D.num_items = (uint32_t)items.size();
     D.num_lights = d->num_dir_lights;
     D.num_materials = (uint32_t)mat_i.size();
@@ -472,7 +481,10 @@ DevScene rtc_rebase_scene(const HostScene& H, uint8_t* base) {
     auto rb = [base](auto& p) {
         p = reinterpret_cast<std::remove_reference_t<decltype(p)>>(base + reinterpret_cast<uintptr_t>(p));
     };
-    rb(D.nodes); rb(D.items); rb(D.sph); rb(D.sph_aux); rb(D.tri); rb(D.tri_n); rb(D.tri_vn); rb(D.quad);
+    rb(D.nodes);
+    rb(D.items);
+    if (D.nodes4) rb(D.nodes4);
+    rb(D.sph); rb(D.sph_aux); rb(D.tri); rb(D.tri_n); rb(D.tri_vn); rb(D.quad);
     rb(D.light); rb(D.mat_i); rb(D.mat_f); rb(D.tex_i); rb(D.tex_f); rb(D.images); rb(D.image_bytes);
     if (D.bg.env) rb(D.bg.env);
     return D;
@@ -766,8 +778,8 @@ rtc_status launch_wavefront(rtc_context* c, const rtc_scene* s, const rtc_render
     WfTimer timer;
     timer.pool = &c->kev;
     const bool timed = (p->flags & RTC_FLAG_KERNEL_TIMING) != 0;
-    r = run_wavefront(s->dev, p, B, c->d_status, d_out, d_counters, st, c->num_sms, poll, c->phase_ev, run,
-                      timed ? &timer : nullptr);
+    r = run_wavefront(rtc_scene_view(s, p), p, B, c->d_status, d_out, d_counters, st, c->num_sms, poll,
+                      c->phase_ev, run, timed ? &timer : nullptr);
     if (r != RTC_OK) return r;
     c->kev_ext = c->kev_shade = 0;
     c->kev_pairs.clear();
@@ -803,7 +815,7 @@ rtc_status rtc_run_wavefront_sync(const rtc_scene* s, const rtc_render_params* p
     WfPoller poll;
     poll.sync = true;
     WfRun run;
-    return run_wavefront(s->dev, p, B, d_status, d_out, nullptr, st, sms, poll, nullptr, run);
+    return run_wavefront(rtc_scene_view(s, p), p, B, d_status, d_out, nullptr, st, sms, poll, nullptr, run);
 }
 
 namespace {
@@ -816,11 +828,12 @@ rtc_status launch(rtc_context* c, const rtc_scene* s, const rtc_render_params* p
     c->last.launches = 1;
     c->last_timed = false;
     DevParams P = dev_params(p);
+    const DevScene S = rtc_scene_view(s, p);
     cudaError_t e =
-        p->mode == RTC_MODE_CLEAN ? rtc_launch_render_clean(s->dev, P, d_out, d_counters, c->d_status, p->block_size, st)
+        p->mode == RTC_MODE_CLEAN ? rtc_launch_render_clean(S, P, d_out, d_counters, c->d_status, p->block_size, st)
         : p->draw_order == RTC_DRAW_ORDER_HOST
-            ? rtc_launch_render_compat_host(s->dev, P, d_out, d_counters, c->d_status, p->block_size, st)
-            : rtc_launch_render_compat_dev(s->dev, P, d_out, d_counters, c->d_status, p->block_size, st);
+            ? rtc_launch_render_compat_host(S, P, d_out, d_counters, c->d_status, p->block_size, st)
+            : rtc_launch_render_compat_dev(S, P, d_out, d_counters, c->d_status, p->block_size, st);
     if (e != cudaSuccess) return cuda_fail(e, "render launch");
     return RTC_OK;
 }
@@ -925,7 +938,7 @@ extern "C" rtc_status rtc_trace_closest(rtc_context* c, const rtc_scene* s, cons
     if (r == RTC_OK) {
         e = cudaMemcpyAsync(d_rays, rays, (size_t)n * 8 * sizeof(float), cudaMemcpyHostToDevice, c->stream);
         if (e == cudaSuccess) e = cudaMemsetAsync(c->d_status, 0, 4, c->stream);
-        if (e == cudaSuccess) e = rtc_launch_trace_closest(s->dev, d_rays, n, depth, max_depth, d_prim, d_t, c->d_status, c->stream);
+        if (e == cudaSuccess) e = rtc_launch_trace_closest(rtc_scene_view(s, nullptr), d_rays, n, depth, max_depth, d_prim, d_t, c->d_status, c->stream);
         if (e == cudaSuccess && prim) e = cudaMemcpyAsync(prim, d_prim, (size_t)n * 4, cudaMemcpyDeviceToHost, c->stream);
         if (e == cudaSuccess && t) e = cudaMemcpyAsync(t, d_t, (size_t)n * 4, cudaMemcpyDeviceToHost, c->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);

@@ -31,7 +31,7 @@ uint32_t next_pow2(uint32_t x) {
 rtc_status rtc_make_job(const rtc_scene* scene, const rtc_camera* camera, const rtc_render_params* params,
                         float* d_out, DevJob& J) {
     J = DevJob{};
-    J.S = rtc_scene_dev(scene);
+    J.S = rtc_scene_view(scene, params);
     if (camera && !rtc_make_camera(*camera, J.S.cam)) return rtc_set_error(RTC_ERR_INVALID_ARGUMENT, "degenerate camera");
     J.P = rtc_dev_params(params);
     J.out = (float4*)d_out;

@@ -340,7 +340,7 @@ extern "C" rtc_status rtc_server_create(const rtc_server_config* cfg, rtc_server
     EngineConfig ec;
     ec.device = cfg->device;
     ec.num_sms = s->num_sms;
-    ec.slots = cfg->slots ? cfg->slots : (1u << 22);
+    ec.slots = cfg->slots ? cfg->slots : (1u << 20);
     ec.ring = cfg->ring ? cfg->ring : 1024u;
     ec.mode = s->cfg.mode;
     ec.draw_order = s->cfg.draw_order;

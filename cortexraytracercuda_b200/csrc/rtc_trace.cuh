@@ -274,13 +274,105 @@ __device__ __forceinline__ void test_leaf(const DevScene& S, int32_t child, V3 o
     }
 }
 
-// Closest hit in [tmin, tmax] over the whole scene (the reference's world.hit through the BVH).
+// Near/far distances of one child box of a 4-wide node (the slab2 arithmetic, one child).
+__device__ __forceinline__ float slab1(float lx, float hx, float ly, float hy, float lz, float hz, V3 inv, V3 oi,
+                                       float tmin, float tmax, float& tf) {
+    float ax = __fmaf_rn(lx, inv.x, -oi.x), bx = __fmaf_rn(hx, inv.x, -oi.x);
+    float ay = __fmaf_rn(ly, inv.y, -oi.y), by = __fmaf_rn(hy, inv.y, -oi.y);
+    float az = __fmaf_rn(lz, inv.z, -oi.z), bz = __fmaf_rn(hz, inv.z, -oi.z);
+    tf = fminf(fminf(fmaxf(ax, bx), fmaxf(ay, by)), fminf(fmaxf(az, bz), tmax));
+    return fmaxf(fmaxf(fminf(ax, bx), fminf(ay, by)), fmaxf(fminf(az, bz), tmin));
+}
+
+__device__ __forceinline__ void cswap(uint32_t& a, uint32_t& b) {
+    const uint32_t lo = min(a, b), hi = max(a, b);
+    a = lo;
+    b = hi;
+}
+
+// Closest hit through the 4-wide nodes.  Each visit loads one 128-byte node, tests its four child boxes,
+// sorts the hit children by entry distance (key = distance bits with the child index in the two low
+// bits; distances are >= tmin > 0, so the bits order like the floats and clearing two low bits rounds
+// down, which keeps the culling conservative), and pushes them far to near.  Leaves travel through the
+// stack too, so the leaf test is inlined once; an entry farther than the current best hit is dropped
+// when popped.
+template <bool EXACT>
+__device__ __forceinline__ bool closest_hit4(const DevScene& S, V3 o, V3 d, V3 inv, V3 oi, float tmin, float tmax,
+                                             bool hide_invisible, float& t_out, uint32_t& item_out,
+                                             TraceStats& st, uint32_t& status) {
+    float best_t = tmax;
+    uint32_t best_item = 0xffffffffu;
+    int2 stk[TRAVERSAL_STACK4];   // (child reference, entry distance bits)
+    int sp = 0;
+    int32_t ref = 0;   // the root node
+    for (;;) {
+        if (ref >= 0) {
+            if ((uint32_t)ref >= S.num_nodes4) { status |= STATUS_BAD_ITEM; break; }
+            const float4* np = S.nodes4 + 8 * (size_t)ref;
+            const float4 lx = ld_scene(np), hx = ld_scene(np + 1), ly = ld_scene(np + 2), hy = ld_scene(np + 3);
+            const float4 lz = ld_scene(np + 4), hz = ld_scene(np + 5), ch = ld_scene(np + 6);
+            st.nodes++;
+            float f0, f1, f2, f3;
+            const float n0 = slab1(lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, inv, oi, tmin, best_t, f0);
+            const float n1 = slab1(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, inv, oi, tmin, best_t, f1);
+            const float n2 = slab1(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, inv, oi, tmin, best_t, f2);
+            const float n3 = slab1(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, inv, oi, tmin, best_t, f3);
+            const int32_t c0 = __float_as_int(ch.x), c1 = __float_as_int(ch.y), c2 = __float_as_int(ch.z),
+                          c3 = __float_as_int(ch.w);
+            uint32_t k0 = (n0 <= f0 && c0 != -1) ? ((__float_as_uint(n0) & ~3u) | 0u) : 0xffffffffu;
+            uint32_t k1 = (n1 <= f1 && c1 != -1) ? ((__float_as_uint(n1) & ~3u) | 1u) : 0xffffffffu;
+            uint32_t k2 = (n2 <= f2 && c2 != -1) ? ((__float_as_uint(n2) & ~3u) | 2u) : 0xffffffffu;
+            uint32_t k3 = (n3 <= f3 && c3 != -1) ? ((__float_as_uint(n3) & ~3u) | 3u) : 0xffffffffu;
+            cswap(k0, k1);
+            cswap(k2, k3);
+            cswap(k0, k2);
+            cswap(k1, k3);
+            cswap(k1, k2);
+            // push far to near: the nearest child ends on top
+            const uint32_t ks[4] = {k3, k2, k1, k0};
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const uint32_t k = ks[q];
+                if (k == 0xffffffffu) continue;
+                const uint32_t c = k & 3u;
+                const int32_t r = c == 0u ? c0 : (c == 1u ? c1 : (c == 2u ? c2 : c3));
+                if (sp >= TRAVERSAL_STACK4) { status |= STATUS_STACK_OVERFLOW; break; }
+                stk[sp] = make_int2(r, (int)(k & ~3u));
+                ++sp;
+            }
+            if (status & STATUS_STACK_OVERFLOW) break;
+        } else {
+            test_leaf<EXACT>(S, ref, o, d, tmin, best_t, best_item, hide_invisible, st, status);
+        }
+        // next entry that is still nearer than the best hit
+        bool found = false;
+        while (sp > 0) {
+            const int2 e = stk[--sp];
+            if (__int_as_float(e.y) <= best_t) {
+                ref = e.x;
+                found = true;
+                break;
+            }
+        }
+        if (!found) break;
+    }
+    t_out = best_t;
+    item_out = best_item;
+    return best_item != 0xffffffffu;
+}
+
+// Closest hit in [tmin, tmax] over the whole scene (the reference's world.hit through the BVH):
+// through the 4-wide nodes when the scene carries them, else the binary nodes.
 // EXACT: clean mode (double-precision sphere test).
 template <bool EXACT = false>
 __device__ __forceinline__ bool closest_hit(const DevScene& S, V3 o, V3 d, float tmin, float tmax,
                                             bool hide_invisible, float& t_out, uint32_t& item_out,
                                             TraceStats& st, uint32_t& status) {
     V3 inv = v3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
+    if (S.nodes4) {
+        V3 oi4 = v3(o.x * inv.x, o.y * inv.y, o.z * inv.z);
+        return closest_hit4<EXACT>(S, o, d, inv, oi4, tmin, tmax, hide_invisible, t_out, item_out, st, status);
+    }
     V3 oi = v3(o.x * inv.x, o.y * inv.y, o.z * inv.z);
     float best_t = tmax;
     uint32_t best_item = 0xffffffffu;

@@ -23,6 +23,7 @@ BG_CONSTANT, BG_SKY_GRADIENT, BG_ENV_MAP = 0, 1, 2
 MODE_COMPAT, MODE_CLEAN = 0, 1
 ENGINE_AUTO, ENGINE_MEGAKERNEL, ENGINE_WAVEFRONT = 0, 1, 2
 FLAG_KERNEL_TIMING = 1
+FLAG_WIDE_BVH = 2
 DRAW_ORDER_DEVICE, DRAW_ORDER_HOST = 0, 1
 
 F3 = C.c_float * 3

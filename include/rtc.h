@@ -226,6 +226,11 @@ typedef struct rtc_render_params {
 /* Record CUDA events around every extend and shade launch of the wavefront engine; the per-kernel
  * device times are then reported by rtc_get_render_stats (extend_ms / shade_ms / *_launches). */
 #define RTC_FLAG_KERNEL_TIMING 1
+/* Traverse the 4-wide BVH (128-byte nodes) instead of the binary one (64-byte nodes, the default).  Both
+ * hold the same leaves in the same order; the closest hit is the same except for which of several
+ * primitives at exactly the same distance is reported.  Measured slower on B200 (its traversal stack
+ * does not stay in L1), kept as a node-layout option. */
+#define RTC_FLAG_WIDE_BVH 2
 
 /* ------------------------------------------------------------------------------------------------ */
 /* context and scenes                                                                                */
@@ -367,7 +372,8 @@ typedef struct rtc_server_config {
     int32_t mode;                /* rtc_mode, shared by every request                                  */
     int32_t draw_order;          /* rtc_draw_order (COMPAT), shared by every request                   */
     int32_t batch;               /* (extend, shade) iterations between two host polls; 0: 12           */
-    uint32_t slots;              /* path slots; 0: 2^22                                                 */
+    uint32_t slots;              /* path slots; 0: 2^20 (fewer slots in flight: shorter iterations,     
+                                    lower latency)                                                      */
     uint32_t ring;               /* requests in flight at most (power of two <= 65536); 0: 1024        */
     uint64_t hbm_budget_bytes;   /* device bytes for slots, resident scenes and request outputs;
                                     0: 120 GB                                                           */

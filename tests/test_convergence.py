@@ -1,9 +1,8 @@
 """Converged-image checks against the double-precision clean-mode estimator (oracle/fp64_clean.c).
 
 * CPU (pinning the oracle): on the same PCG draws, fp64 and the float C restatement in clean mode
-  follow the same paths except where rounding flips a branch, so most pixels agree within 1e-3
-  relative (>= 90%; >= 60% on the textured scene, where float and double hit points fall in different
-  texels and checker cells along their boundaries) and the image means within 0.5%.
+  follow the same paths except where rounding flips a branch, so >= 90% of pixels agree within 1e-3
+  relative and the image means within 0.5%.
 * GPU (T4): the clean kernels' image at N spp converges to the fp64 estimate: with independent seeds,
   RMSE(kernel, fp64) must not exceed 1.2x the seed-to-seed noise floor RMSE(kernel seed A, kernel seed
   B), and the image means must agree within 4 standard errors (a bias would add to both)."""
@@ -23,13 +22,18 @@ def _ico_scene():
     return configs.icosphere_scene(level=1)
 
 
+def _textured():
+    # floor off the checker cell boundary: on the boundary the cell parity is rounding noise, whose
+    # statistics differ between FMA-contracted float, plain float and double arithmetic
+    return configs.textured(floor_y=0.013)
+
+
 CASES = [
     ("cornell", configs.cornell, 32, 32, 8),
-    ("textured", configs.textured, 32, 24, 10),
+    ("textured", _textured, 32, 24, 10),
     ("spheres", _small_spheres, 40, 24, 16),
     ("icosphere", _ico_scene, 36, 24, 12),
 ]
-SAME_PATH_SHARE = {"cornell": 0.9, "textured": 0.6, "spheres": 0.9, "icosphere": 0.9}
 
 
 @pytest.fixture(scope="module")
@@ -53,7 +57,7 @@ def test_fp64_oracle_matches_float_restatement(f64, name, mk, w, h, depth):
     b = b[:, :3].astype(np.float64)
     close = np.mean(np.all(np.isclose(a, b, rtol=1e-3, atol=1e-6), axis=1))
     print(name, "pixels within 1e-3:", close, "mean", a.mean(), b.mean())
-    assert close >= SAME_PATH_SHARE[name]
+    assert close >= 0.9
     assert abs(a.mean() - b.mean()) <= 0.005 * b.mean()
 
 

@@ -220,3 +220,19 @@ def test_clean_mode_statistics(ctx, port, name):
     print(name, q0, q1, qr)
     for q in (q0, q1):
         assert np.all(np.abs(q - qr) <= 0.05 * np.maximum(np.abs(qr), 1e-3 * mr)), (q, qr)
+
+
+@pytest.mark.parametrize("name,kw", SCENES)
+def test_wide_bvh_matches_binary(ctx, name, kw):
+    """The 4-wide nodes hold the same leaves as the binary ones, so the closest hit is the same except
+    for exact-distance ties; the g++ flavour's images agree pixel for pixel (ties shade alike here)."""
+    from cortexraytracercuda_b200.scene import FLAG_WIDE_BVH
+    scene, params = _params(name, kw, DRAW_ORDER_HOST)
+    ds = DeviceScene(ctx, scene)
+    binary, _ = ds.render(params)
+    params.flags |= FLAG_WIDE_BVH
+    wide, _ = ds.render(params)
+    ds.close()
+    same = np.mean(np.all(wide == binary, axis=-1) | np.all(np.isnan(wide) & np.isnan(binary), axis=-1))
+    print(name, "identical pixels", same)
+    assert same >= 0.999
