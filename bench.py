@@ -219,14 +219,21 @@ def _init_dist(world, local):
     return dist
 
 
-def _max_over_ranks(x, world):
+def _max_over_ranks(x, world, device="cuda"):
+    """The largest value of `x` over all ranks (the whole job's time is its slowest rank's)."""
     import torch
     import torch.distributed as dist
     if world == 1:
         return x
-    t = torch.tensor([x], device="cuda", dtype=torch.float64)
+    t = torch.tensor([x], device=device, dtype=torch.float64)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def replica_rate(units_per_rank, world, steps, total_ms):
+    """Whole-job rate of `world` replicas, each processing `units_per_rank` per step for `steps` steps,
+    timed by the slowest rank's total (ms): millions of units per second."""
+    return units_per_rank * world * steps / (total_ms / 1e3) / 1e6
 
 
 def run_batched(args, rank, world, local):
@@ -623,14 +630,10 @@ def main():
     step_ms = [a.elapsed_time(b) for a, b in ev]
     clk = clocks.stop()
     kernel_ms = float(np.mean(step_ms))
-    total_ms = float(np.sum(step_ms))
-    if world > 1:
-        tt = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        total_ms = float(tt.item())
+    total_ms = _max_over_ranks(float(np.sum(step_ms)), world)
     traced = W * H * params.traced_spp
-    value = traced * world * args.steps / (total_ms / 1e3) / 1e6
-    mrays = rays * world * args.steps / (total_ms / 1e3) / 1e6
+    value = replica_rate(traced, world, args.steps, total_ms)
+    mrays = replica_rate(rays, world, args.steps, total_ms)
 
     # ---- end to end through the C ABI with host buffers ----------------------------------------
     import ctypes as C
@@ -647,12 +650,8 @@ def main():
         dt = (time.perf_counter() - t0) * 1e3
         if k >= args.warmup:
             e2e_ms.append(dt)
-    e2e_total = float(np.sum(e2e_ms)) if e2e_ms else float("nan")
-    if world > 1:
-        tt = torch.tensor([e2e_total], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_total = float(tt.item())
-    e2e_value = traced * world * args.steps / (e2e_total / 1e3) / 1e6
+    e2e_total = _max_over_ranks(float(np.sum(e2e_ms)) if e2e_ms else float("nan"), world)
+    e2e_value = replica_rate(traced, world, args.steps, e2e_total)
 
     # ---- roofline -------------------------------------------------------------------------------
     peak, peak_kind = hbm_peak()
