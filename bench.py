@@ -263,8 +263,18 @@ def run_batched(args, rank, world, local):
     sp = stream.cuda_stream
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
+    tuned = None
+    if args.autotune:
+        from cortexraytracercuda_b200 import autotune
+        tuned = autotune.autotune_batch(ctx, jobs, space={"slots": [1 << 20, 1 << 21, 1 << 22], "batch": [12]},
+                                        repeats=1, stream=sp)
+        jobs = autotune.with_layout(jobs, tuned.layout)
+        args.slots, args.drain = tuned.slots, tuned.drain
+        torch.cuda.synchronize()
+
     def batched():
-        ctx.render_batch(jobs, slots=args.slots, drain=args.drain, stream=sp)
+        ctx.render_batch(jobs, slots=args.slots, drain=args.drain, stream=sp,
+                         batch=tuned.batch if tuned else 0)
 
     def plain():
         for ds, p, o in zip(dss, params, plain_outs):
@@ -370,6 +380,10 @@ def run_batched(args, rank, world, local):
             "e2e": {"value": round(paths * world * args.steps / e2e_tot / 1e6, 3), "unit": METRIC,
                     "h2d_bytes_per_step": len(jobs) * C.sizeof(rtc_job), "d2h_bytes_per_step": pixels * 16},
             "setup_s": round(setup_s, 2), "clocks": clk, "roofline": None, "cpu_baseline": None}
+    if tuned:
+        line["autotune"] = {"chosen": {"slots": tuned.slots, "batch": tuned.batch, "drain": tuned.drain,
+                                       "layout": tuned.layout},
+                            "candidates_ms": [[c, round(ms, 1)] for c, ms in tuned.table]}
     if rank == 0:
         print(json.dumps(line), flush=True)
     for ds in dss:
@@ -539,6 +553,8 @@ def main():
     ap.add_argument("--scenes", type=int, default=64, help="batched/served: number of scenes")
     ap.add_argument("--slots", type=int, default=0, help="batched/served: path slots (0: library default)")
     ap.add_argument("--drain", type=int, default=0, help="batched: drain threshold (0: default, 1: no drain)")
+    ap.add_argument("--autotune", action="store_true",
+                    help="batched: pick slots / batch / drain / BVH layout with the autotuner before timing")
     ap.add_argument("--lambdas", default="50,200,800", help="served: request rates (1/s)")
     ap.add_argument("--requests", type=int, default=300, help="served: requests per rate")
     ap.add_argument("--plain-requests", type=int, default=120, help="served: requests of the plain comparison")

@@ -15,7 +15,7 @@ from .scene import (rtc_batch_params, rtc_job, rtc_render_params, rtc_render_sta
 LIB_PATH = Path(__file__).resolve().parent / "librtc_b200.so"
 
 # include/rtc.h: RTC_NOALLOC_MAX_PIXELS
-NOALLOC_MAX_PIXELS = 524264
+NOALLOC_MAX_PIXELS = 508376
 
 STATUS_NAMES = {0: "RTC_OK", 1: "RTC_ERR_INVALID_ARGUMENT", 2: "RTC_ERR_BAD_SCENE", 3: "RTC_ERR_CUDA",
                 4: "RTC_ERR_OOM", 5: "RTC_ERR_TIMEOUT", 6: "RTC_ERR_NO_DEVICE", 7: "RTC_ERR_IO",

@@ -11,7 +11,7 @@
 // Limits and behaviour:
 //   * the array is NOALLOC_SCRATCH_BYTES = 64 MiB; every GPU that loads this library holds it until
 //     the process exits;
-//   * one path slot per pixel, so one call renders at most RTC_NOALLOC_MAX_PIXELS (524,264) pixels
+//   * one path slot per pixel, so one call renders at most RTC_NOALLOC_MAX_PIXELS (508,376) pixels
 //     and rejects larger images with RTC_ERR_INVALID_ARGUMENT before touching the GPU;
 //   * the first call on a device looks up the array's device address (cudaGetSymbolAddress, once per
 //     device, with that device current); make that first call before any stream capture;

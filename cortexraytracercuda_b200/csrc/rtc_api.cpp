@@ -94,6 +94,9 @@ extern "C" rtc_status rtc_context_destroy(rtc_context* c) {
         if (e) cudaEventDestroy(e);
     for (cudaEvent_t& e : c->phase_ev)
         if (e) cudaEventDestroy(e);
+    for (cudaEvent_t& e : c->split_ev)
+        if (e) cudaEventDestroy(e);
+    if (c->stream_long) cudaStreamDestroy(c->stream_long);
     for (cudaEvent_t e : c->kev) cudaEventDestroy(e);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -570,7 +573,7 @@ DevParams rtc_dev_params(const rtc_render_params* p) {
 namespace {
 
 // Bytes of wavefront scratch per path slot.
-constexpr size_t WF_SLOT_BYTES = 5 * sizeof(float4) + 2 * sizeof(uint4) + sizeof(float2) + 2 * sizeof(uint32_t);
+constexpr size_t WF_SLOT_BYTES = 5 * sizeof(float4) + 2 * sizeof(uint4) + sizeof(float2) + 3 * sizeof(uint32_t);
 constexpr uint32_t WF_MAX_SLOTS = 1u << 22;   // 4,194,304 slots = 432 MiB of path state
 
 // Lays out the wavefront buffers for `slots` path slots in one block of device memory at `base`
@@ -593,6 +596,7 @@ size_t carve_wavefront(void* base, uint32_t slots, WfBuffers& B) {
     B.hit = (float2*)take(n * 8);
     B.queue[0] = (uint32_t*)take(n * 4);
     B.queue[1] = (uint32_t*)take(n * 4);
+    B.queue[2] = (uint32_t*)take(n * 4);
     B.ctr = (uint32_t*)take(WF_CTR_N * 4);
     B.slots = slots;
     return (size_t)(p - (uint8_t*)base);
@@ -612,6 +616,8 @@ rtc_status ensure_wavefront(rtc_context* c, uint32_t slots, WfBuffers& B) {
         RTC_CUDA(cudaEventCreateWithFlags(&c->poll_ev[0], cudaEventDisableTiming));
         RTC_CUDA(cudaEventCreateWithFlags(&c->poll_ev[1], cudaEventDisableTiming));
         for (cudaEvent_t& e : c->phase_ev) RTC_CUDA(cudaEventCreate(&e));
+        for (cudaEvent_t& e : c->split_ev) RTC_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        RTC_CUDA(cudaStreamCreateWithFlags(&c->stream_long, cudaStreamNonBlocking));
     }
     carve_wavefront(c->d_wf, slots, B);
     return RTC_OK;
@@ -622,12 +628,17 @@ struct WfPoller {
     uint32_t* h = nullptr;           // pinned slots: the next batch is queued before the host looks
     cudaEvent_t ev[2] = {nullptr, nullptr};
     bool sync = false;               // synchronous copy into a host variable (no pinned memory, no events)
+    // long-chain split: the stream its drain kernel runs on (null: the render's own stream, in order)
+    // and the two events that order it (split done -> long chains start; long chains done -> render end)
+    cudaStream_t st_long = nullptr;
+    cudaEvent_t split_ev[2] = {nullptr, nullptr};
 };
 
 struct WfRun {
     uint64_t iterations = 0;
     bool drained = false;
     uint32_t drained_slots = 0;
+    bool split = false;
 };
 
 // Wavefront engine: init, then batches of (extend, shade) iterations until the slot queue drains or
@@ -685,6 +696,15 @@ rtc_status run_wavefront(const DevScene& S, const rtc_render_params* p, const Wf
     // drain threshold: below this many queued slots the finish kernel takes over
     uint32_t drain = (uint32_t)num_sms * 512u;
     if (const char* ev = std::getenv("RTC_WF_DRAIN")) drain = (uint32_t)std::strtoul(ev, nullptr, 10);
+    // long-chain split: at iteration `split_at` (0: never), slots predicted to need more than
+    // `split_thr` further iterations move to the drain kernel, running beside the bulk iterations
+    uint64_t split_at = 0;
+    float split_thr = 1024.0f;
+    if (const char* ev = std::getenv("RTC_WF_SPLIT")) split_at = std::strtoull(ev, nullptr, 10);
+    if (const char* ev = std::getenv("RTC_WF_SPLIT_THRESH")) split_thr = std::strtof(ev, nullptr);
+    int split_blocks = 1;   // blocks per SM of the long-chain kernel (its registers stay taken while it runs)
+    if (const char* ev = std::getenv("RTC_WF_SPLIT_BLOCKS")) split_blocks = std::max(1, std::atoi(ev));
+    int64_t last_left = -1;   // queue size last observed (one batch late in both polling modes)
     // split extend / shade kernels (default) or one fused launch per iteration
     bool fused = false;
     if (const char* ev = std::getenv("RTC_WF_FUSED")) fused = std::atoi(ev) != 0;
@@ -693,6 +713,27 @@ rtc_status run_wavefront(const DevScene& S, const rtc_render_params* p, const Wf
     uint32_t left = 0;
     uint32_t sync_counts[2] = {0, 0};
     for (int b = 0;; ++b) {
+        if (!run.split && split_at > 0 && it >= split_at && last_left >= (int64_t)drain) {
+            // the split takes the place of one iteration (same queue rotation)
+            L.w = wf_iter(it);
+            L.k0 = (float)it;
+            L.threshold = split_thr;
+            e = fn(WF_OP_SPLIT, J, B, L);
+            if (e != cudaSuccess) return cuda_fail(e, "wavefront split");
+            ++it;
+            run.split = true;
+            WfLaunch LL = L;
+            LL.w = WfIter{2, WF_LONG, 0, 0};
+            LL.grid = num_sms * split_blocks;
+            LL.st = poll.st_long ? poll.st_long : st;
+            if (poll.st_long) {
+                RTC_CUDA(cudaEventRecord(poll.split_ev[0], st));
+                RTC_CUDA(cudaStreamWaitEvent(poll.st_long, poll.split_ev[0], 0));
+            }
+            e = fn(WF_OP_FINISH, J, B, LL);
+            if (e != cudaSuccess) return cuda_fail(e, "wavefront long chains");
+            if (poll.st_long) RTC_CUDA(cudaEventRecord(poll.split_ev[1], poll.st_long));
+        }
         for (int k = 0; k < BATCH; ++k, ++it) {
             L.w = wf_iter(it);
             if (fused) {
@@ -743,6 +784,7 @@ rtc_status run_wavefront(const DevScene& S, const rtc_render_params* p, const Wf
             }
         }
         pending = slot;
+        if (have) last_left = (int64_t)left;
         if (have && left == 0) break;
         if (have && left < drain) {
             run.drained = true;
@@ -759,6 +801,7 @@ rtc_status run_wavefront(const DevScene& S, const rtc_render_params* p, const Wf
         e = fn(WF_OP_FINISH, J, B, L);
         if (e != cudaSuccess) return cuda_fail(e, "wavefront finish");
     }
+    if (run.split && poll.st_long) RTC_CUDA(cudaStreamWaitEvent(st, poll.split_ev[1], 0));   // long chains done
     if (phase) RTC_CUDA(cudaEventRecord(phase[2], st));
     return RTC_OK;
 }
@@ -774,6 +817,9 @@ rtc_status launch_wavefront(rtc_context* c, const rtc_scene* s, const rtc_render
     poll.h = c->h_poll;
     poll.ev[0] = c->poll_ev[0];
     poll.ev[1] = c->poll_ev[1];
+    poll.st_long = c->stream_long;
+    poll.split_ev[0] = c->split_ev[0];
+    poll.split_ev[1] = c->split_ev[1];
     WfRun run;
     WfTimer timer;
     timer.pool = &c->kev;
@@ -793,6 +839,7 @@ rtc_status launch_wavefront(rtc_context* c, const rtc_scene* s, const rtc_render
     c->last = rtc_render_stats{};
     c->last.engine = RTC_ENGINE_WAVEFRONT;
     c->last.iterations = (uint32_t)run.iterations;
+    // (the split pass counts as one iteration: the split launch and the long-chain drain launch)
     c->last.launches = (uint32_t)(1 + (fused ? 1 : 2) * run.iterations + (run.drained ? 1 : 0));
     c->last.drained_slots = run.drained_slots;
     c->last_timed = true;

@@ -115,8 +115,8 @@ struct WfBuffers {
                        // w depth left (low 16 bits) | job slot (high 16 bits, 0 for a single image)
     uint4* pcg;        // clean mode: PCG32 state (lo, hi) and increment (lo, hi)
     float2* hit;       // t, item bits (0xffffffff = miss)
-    uint32_t* queue[2];
-    uint32_t* ctr;     // [0..2] queue sizes (rotating), [3] next pixel to fetch
+    uint32_t* queue[3];   // [0], [1]: the alternating slot queues; [2]: slots split off as long chains
+    uint32_t* ctr;     // [0..2] queue sizes (rotating), [3] next pixel to fetch, [4] long-chain queue size
     uint32_t slots;
 };
 
@@ -163,7 +163,7 @@ struct WfTableArgs {           // a ring of jobs
 
 // Iteration k reads queue (k & 1) with size ctr[k % 3], appends to queue ((k+1) & 1) counted in
 // ctr[(k+1) % 3] and clears ctr[(k+2) % 3], which iteration k+1 appends to.
-enum WfCtr { WF_NEXT_PIXEL = 3, WF_CTR_N = 4 };
+enum WfCtr { WF_NEXT_PIXEL = 3, WF_LONG = 4, WF_CTR_N = 5 };
 struct WfIter {
     int qin, cin, cout, czero;
 };

@@ -20,10 +20,14 @@
 
 namespace rtc {
 // Wavefront kernel launches.  One dispatcher per (mode, flavour) and job source; `op` picks the kernel.
-enum WfOp { WF_OP_INIT = 0, WF_OP_ADMIT = 1, WF_OP_EXTEND = 2, WF_OP_SHADE = 3, WF_OP_FINISH = 4, WF_OP_BOUNCE = 5 };
+enum WfOp {
+    WF_OP_INIT = 0, WF_OP_ADMIT = 1, WF_OP_EXTEND = 2, WF_OP_SHADE = 3, WF_OP_FINISH = 4, WF_OP_BOUNCE = 5,
+    WF_OP_SPLIT = 6
+};
 struct WfLaunch {
     WfIter w;
     WfWindow win;                    // ADMIT: the window to publish
+    float k0, threshold;             // SPLIT: iterations so far, long-chain threshold (iterations)
     unsigned long long* counters;    // NULL: no instrumentation
     uint32_t* status;
     int grid;

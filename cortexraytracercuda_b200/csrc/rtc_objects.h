@@ -28,6 +28,8 @@ struct rtc_context {
     uint32_t* h_poll = nullptr;       // pinned: queue sizes read back between batches
     cudaEvent_t poll_ev[2] = {nullptr, nullptr};
     cudaEvent_t phase_ev[3] = {nullptr, nullptr, nullptr};   // render start, drain start, render end
+    cudaStream_t stream_long = nullptr;    // the long-chain drain kernel, beside the bulk iterations
+    cudaEvent_t split_ev[2] = {nullptr, nullptr};
     rtc_render_stats last{};
     bool last_timed = false;
     std::vector<cudaEvent_t> kev;      // per-launch timing events (RTC_FLAG_KERNEL_TIMING)

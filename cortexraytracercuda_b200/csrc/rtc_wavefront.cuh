@@ -403,6 +403,38 @@ __global__ void __launch_bounds__(128) wf_bounce(J jobs, WfBuffers B, WfIter w, 
     if (status) atomicOr(status_word, status);
 }
 
+// Long-chain split (one pass in place of an iteration): a slot whose predicted remaining work - samples
+// left times the iterations each of its samples has taken so far (`k0` iterations since the start) -
+// exceeds `threshold` iterations moves to the long-chain queue, which the drain kernel finishes in
+// registers on a second stream while the bulk iterations go on with the other slots.  In compat mode
+// a pixel's samples share one stream and cannot run in parallel, so the few pixels whose samples keep
+// bouncing (glass) are the frame's critical path; the split starts their register-resident loop ~k0
+// iterations into the frame instead of at its end.
+template <bool CLEAN, class J>
+__global__ void __launch_bounds__(128) wf_split(J jobs, WfBuffers B, WfIter w, float k0, float threshold) {
+    const uint32_t n = B.ctr[w.cin];
+    if (blockIdx.x == 0 && threadIdx.x == 0) B.ctr[w.czero] = 0u;   // appended to by the next iteration
+    const uint32_t* q = B.queue[w.qin];
+    uint32_t* qn = B.queue[w.qin ^ 1];
+    uint32_t* cn = B.ctr + w.cout;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t limit = (n + 31u) & ~31u;   // whole warps, for the warp-aggregated appends
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < limit; k += stride) {
+        bool keep = false, longc = false;
+        uint32_t slot = 0;
+        if (k < n) {
+            slot = q[k];
+            const uint4 m = B.meta[slot];
+            const uint32_t nsamp = wf_samples(jobs.params(wf_job(m.w)), CLEAN);
+            const float rem = (float)(nsamp - m.y - 1u) * (k0 / ((float)m.y + 1.0f));
+            longc = rem > threshold;
+            keep = !longc;
+        }
+        wf_push(qn, cn, slot, keep);
+        wf_push(B.queue[2], B.ctr + WF_LONG, slot, longc);
+    }
+}
+
 // Drain phase: once the queue is small, each remaining slot is finished in place by one thread
 // instead of paying two kernel launches per bounce for a nearly empty queue.  Pixels whose samples
 // have long paths (glass) make this tail thousands of bounces long in compat mode, where a pixel's
@@ -515,6 +547,9 @@ cudaError_t wf_dispatch(WfOp op, const A& args, const WfBuffers& B, const WfLaun
     case WF_OP_FINISH:
         if (c) wf_finish<CLEAN, ORDER, true><<<L.grid, 128, 0, L.st>>>(jobs, B, L.w, L.counters, L.status);
         else wf_finish<CLEAN, ORDER, false><<<L.grid, 128, 0, L.st>>>(jobs, B, L.w, nullptr, L.status);
+        break;
+    case WF_OP_SPLIT:
+        wf_split<CLEAN><<<L.grid, 128, 0, L.st>>>(jobs, B, L.w, L.k0, L.threshold);
         break;
     case WF_OP_BOUNCE:
         if (c) wf_bounce<CLEAN, ORDER, true><<<L.grid, 128, 0, L.st>>>(jobs, B, L.w, L.counters, L.status);

@@ -312,7 +312,7 @@ rtc_status rtc_get_render_stats(rtc_context* ctx, rtc_render_stats* stats);
  * stream).  The first call on a device looks up the array's address; make it before any stream
  * capture.  All calls share the array, so calls that overlap on the GPU race.  Returns when the frame
  * is complete. */
-#define RTC_NOALLOC_MAX_PIXELS 524264u
+#define RTC_NOALLOC_MAX_PIXELS 508376u
 rtc_status rtc_render_noalloc(const rtc_scene* scene, const rtc_render_params* params, float* d_radiance_sum,
                               void* stream);
 
