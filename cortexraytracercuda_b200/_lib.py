@@ -63,7 +63,8 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
     global _lib
     if _lib is not None and path is None:
         return _lib
-    p = Path(path) if path else LIB_PATH
+    # RTC_LIBRARY: load another build of the same ABI (variant builds of `build.py --out`)
+    p = Path(path) if path else Path(os.environ.get("RTC_LIBRARY", LIB_PATH))
     if not p.exists():
         raise RtcError(-1, f"{p} is missing; build it with `python -m cortexraytracercuda_b200.build`")
     lib = C.CDLL(str(p))

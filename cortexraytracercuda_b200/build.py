@@ -69,21 +69,27 @@ def _run(cmd, verbose):
         sys.stderr.write(r.stdout + r.stderr)
 
 
-def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = False) -> Path:
+def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = False, defines=(), out: Path | None = None,
+          objdir: Path | None = None) -> Path:
+    """Compiles every translation unit (in parallel) and links the library.  `defines` (NAME=VALUE)
+    are passed to the CUDA compiles; with `out`/`objdir` a variant library is built elsewhere."""
     if not os.path.exists(NVCC):
         raise RuntimeError(f"nvcc not found at {NVCC}")
-    BUILD.mkdir(exist_ok=True)
+    build_dir = Path(objdir) if objdir else BUILD
+    lib = Path(out) if out else LIB
+    build_dir.mkdir(parents=True, exist_ok=True)
+    dflags = [f"-D{d}" for d in defines]
     headers = [CSRC / h for h in HEADERS] + [INCLUDE / "rtc.h"]
     objs = []
     cmds = []
     for src, obj, comp, extra in SOURCES:
         s = CSRC / src
-        o = BUILD / (obj + ".o")
+        o = build_dir / (obj + ".o")
         objs.append(o)
         if not force and not _newer(o, [s] + headers + [Path(__file__)]):
             continue
         if comp == "nvcc":
-            cmd = [NVCC] + NVCC_COMMON + extra + (["-Xptxas", "-v"] if ptxas_verbose else []) + ["-c", str(s), "-o", str(o)]
+            cmd = [NVCC] + NVCC_COMMON + extra + dflags + (["-Xptxas", "-v"] if ptxas_verbose else []) + ["-c", str(s), "-o", str(o)]
         else:
             cmd = [CXX] + CXX_FLAGS + extra + ["-c", str(s), "-o", str(o)]
         cmds.append(cmd)
@@ -92,12 +98,12 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
     with ThreadPoolExecutor(max_workers=workers) as ex:
         for f in [ex.submit(_run, cmd, verbose or ptxas_verbose) for cmd in cmds]:
             f.result()
-    if force or _newer(LIB, objs):
-        tmp = LIB.with_suffix(".so.tmp")
+    if force or _newer(lib, objs):
+        tmp = lib.with_suffix(".so.tmp")
         cmd = [NVCC, "-shared"] + ARCH + ["-o", str(tmp)] + [str(o) for o in objs] + ["-cudart", "static", "-lpthread"]
         _run(cmd, verbose)
-        os.replace(tmp, LIB)
-    return LIB
+        os.replace(tmp, lib)
+    return lib
 
 
 def main():
@@ -105,8 +111,12 @@ def main():
     ap.add_argument("--force", action="store_true")
     ap.add_argument("--verbose", action="store_true")
     ap.add_argument("--ptxas", action="store_true", help="print -Xptxas -v register/spill report")
+    ap.add_argument("--define", action="append", default=[], help="NAME=VALUE for the CUDA compiles")
+    ap.add_argument("--out", default=None, help="library path (a variant build)")
+    ap.add_argument("--objdir", default=None, help="object directory (a variant build)")
     a = ap.parse_args()
-    p = build(force=a.force, verbose=a.verbose, ptxas_verbose=a.ptxas)
+    p = build(force=a.force, verbose=a.verbose, ptxas_verbose=a.ptxas, defines=a.define,
+              out=Path(a.out) if a.out else None, objdir=Path(a.objdir) if a.objdir else None)
     print(p)
 
 

@@ -712,6 +712,31 @@ rtc_status run_wavefront(const DevScene& S, const rtc_render_params* p, const Wf
     int pending = -1;   // poll slot of the previous batch
     uint32_t left = 0;
     uint32_t sync_counts[2] = {0, 0};
+    // Copies the queue size after the batch just enqueued and reads the previous batch's (lagged).
+    auto poll_batch = [&](int b, bool& have) -> rtc_status {
+        const int slot = b & 1;
+        if (poll.sync) {
+            uint32_t h = 0;
+            RTC_CUDA(cudaMemcpyAsync(&h, B.ctr + wf_iter(it).cin, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+            RTC_CUDA(cudaStreamSynchronize(st));
+            sync_counts[slot] = h;
+            if (pending >= 0) {
+                left = sync_counts[pending];
+                have = true;
+            }
+        } else {
+            RTC_CUDA(cudaMemcpyAsync(poll.h + slot, B.ctr + wf_iter(it).cin, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                     st));
+            RTC_CUDA(cudaEventRecord(poll.ev[slot], st));
+            if (pending >= 0) {
+                RTC_CUDA(cudaEventSynchronize(poll.ev[pending]));
+                left = poll.h[pending];
+                have = true;
+            }
+        }
+        pending = slot;
+        return RTC_OK;
+    };
     for (int b = 0;; ++b) {
         if (!run.split && split_at > 0 && it >= split_at && last_left >= (int64_t)drain) {
             // the split takes the place of one iteration (same queue rotation)
@@ -763,27 +788,8 @@ rtc_status run_wavefront(const DevScene& S, const rtc_render_params* p, const Wf
         // queued when the host looks), so the drain point - and with it the result - does not depend
         // on the polling mode.
         bool have = false;
-        const int slot = b & 1;
-        if (poll.sync) {
-            uint32_t h = 0;
-            RTC_CUDA(cudaMemcpyAsync(&h, B.ctr + wf_iter(it).cin, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-            RTC_CUDA(cudaStreamSynchronize(st));
-            sync_counts[slot] = h;
-            if (pending >= 0) {
-                left = sync_counts[pending];
-                have = true;
-            }
-        } else {
-            RTC_CUDA(cudaMemcpyAsync(poll.h + slot, B.ctr + wf_iter(it).cin, sizeof(uint32_t), cudaMemcpyDeviceToHost,
-                                     st));
-            RTC_CUDA(cudaEventRecord(poll.ev[slot], st));
-            if (pending >= 0) {
-                RTC_CUDA(cudaEventSynchronize(poll.ev[pending]));
-                left = poll.h[pending];
-                have = true;
-            }
-        }
-        pending = slot;
+        rtc_status pr = poll_batch(b, have);
+        if (pr != RTC_OK) return pr;
         if (have) last_left = (int64_t)left;
         if (have && left == 0) break;
         if (have && left < drain) {

@@ -21,6 +21,26 @@
 
 #include <type_traits>
 
+// Launch bounds of the two iteration kernels.  Build-time knobs for occupancy sweeps: RTC_EXTEND_MINB /
+// RTC_SHADE_MINB ask for that many resident blocks per SM (a register cap of 65536 / (128 x blocks)).
+// Without them the compiler's own choice stands, which measured best (extend 63 registers, shade 108);
+// note that an explicit minimum of 1 is not the same: it lets extend grow to 80 registers.
+#ifdef RTC_EXTEND_MINB
+#define RTC_EXTEND_BOUNDS __launch_bounds__(128, RTC_EXTEND_MINB)
+#else
+#define RTC_EXTEND_BOUNDS __launch_bounds__(128)
+#endif
+#ifdef RTC_SHADE_MINB
+#define RTC_SHADE_BOUNDS __launch_bounds__(128, RTC_SHADE_MINB)
+#else
+#define RTC_SHADE_BOUNDS __launch_bounds__(128)
+#endif
+#ifdef RTC_FINISH_MINB
+#define RTC_FINISH_BOUNDS __launch_bounds__(128, RTC_FINISH_MINB)
+#else
+#define RTC_FINISH_BOUNDS __launch_bounds__(128)
+#endif
+
 #include "rtc_kernels.h"
 #include "rtc_path.cuh"
 
@@ -217,7 +237,7 @@ __global__ void __launch_bounds__(128) wf_admit(WfTable J, WfBuffers B, WfIter w
 
 // FLAVOR: 0 nvcc flavour, 1 g++ flavour, 2 clean mode (double-precision sphere test).
 template <bool COUNT, int FLAVOR, class J>
-__global__ void __launch_bounds__(128) wf_extend(J jobs, WfBuffers B, WfIter w, unsigned long long* counters,
+__global__ void RTC_EXTEND_BOUNDS wf_extend(J jobs, WfBuffers B, WfIter w, unsigned long long* counters,
                                                  uint32_t* status_word) {
     const uint32_t n = B.ctr[w.cin];
     if (blockIdx.x == 0 && threadIdx.x == 0) B.ctr[w.czero] = 0u;
@@ -340,7 +360,7 @@ __device__ __forceinline__ void wf_flush(unsigned long long* counters, uint32_t 
 }
 
 template <bool CLEAN, int ORDER, bool COUNT, class J>
-__global__ void __launch_bounds__(128) wf_shade(J jobs, WfBuffers B, WfIter w, unsigned long long* counters,
+__global__ void RTC_SHADE_BOUNDS wf_shade(J jobs, WfBuffers B, WfIter w, unsigned long long* counters,
                                                 uint32_t* status_word) {
     const uint32_t n = B.ctr[w.cin];
     const WfWindow win = jobs.window();
@@ -441,7 +461,7 @@ __global__ void __launch_bounds__(128) wf_split(J jobs, WfBuffers B, WfIter w, f
 // samples cannot run in parallel, so the loop keeps the whole path state in registers (the
 // megakernel's loop, resumed from the slot) and touches memory only to write the finished pixel.
 template <bool CLEAN, int ORDER, bool COUNT, class J>
-__global__ void __launch_bounds__(128) wf_finish(J jobs, WfBuffers B, WfIter w, unsigned long long* counters,
+__global__ void RTC_FINISH_BOUNDS wf_finish(J jobs, WfBuffers B, WfIter w, unsigned long long* counters,
                                                  uint32_t* status_word) {
     const uint32_t n = B.ctr[w.cin];
     const WfWindow win = jobs.window();

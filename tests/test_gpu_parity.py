@@ -259,3 +259,4 @@ def test_long_chain_split(ctx, monkeypatch, order):
     else:
         st = oracles.parity_stats(wf.reshape(-1, 4), mk.reshape(-1, 4))
         assert abs(st["mean_rel"]) <= 0.02, st
+
