@@ -682,6 +682,7 @@ rtc_status run_wavefront(const DevScene& S, const rtc_render_params* p, const Wf
     L.counters = d_counters;
     L.status = d_status;
     L.st = st;
+    L.wide = S.nodes4 != nullptr;
     if (phase) RTC_CUDA(cudaEventRecord(phase[0], st));
     RTC_CUDA(cudaMemsetAsync(B.ctr, 0, WF_CTR_N * sizeof(uint32_t), st));
     const int grid = num_sms * 8;

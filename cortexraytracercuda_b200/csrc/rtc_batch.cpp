@@ -70,6 +70,7 @@ extern "C" rtc_status rtc_render_batch(rtc_context* c, const rtc_job* jobs, uint
     cfg.ring = bp && bp->ring ? bp->ring : 1024u;
     cfg.batch = bp && bp->batch > 0 ? bp->batch : 12;
     cfg.drain = bp ? bp->drain : 0u;
+    cfg.wide = (jobs[0].params.flags & RTC_FLAG_WIDE_BVH) != 0;
     if (cfg.ring != next_pow2(cfg.ring)) return rtc_set_error(RTC_ERR_INVALID_ARGUMENT, "ring must be a power of two");
 
     std::lock_guard<std::mutex> lk(c->mu);
@@ -78,7 +79,8 @@ extern "C" rtc_status rtc_render_batch(rtc_context* c, const rtc_job* jobs, uint
     cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
     const EngineConfig* have = c->engine ? &c->engine->config() : nullptr;
     if (!have || have->slots != cfg.slots || have->ring != cfg.ring || have->mode != cfg.mode ||
-        have->draw_order != cfg.draw_order || have->batch != cfg.batch || have->drain != cfg.drain) {
+        have->draw_order != cfg.draw_order || have->batch != cfg.batch || have->drain != cfg.drain ||
+        have->wide != cfg.wide) {
         c->engine.reset();
         std::unique_ptr<Engine> eng(new Engine());
         rtc_status r = eng->init(cfg, st);

@@ -181,6 +181,7 @@ rtc_status Engine::enqueue_iterations() {
     WfLaunch L{};
     L.status = d_status_;
     L.counters = counters_;
+    L.wide = cfg_.wide;
     L.grid = cfg_.num_sms * 8;
     const bool use_graph = cfg_.graphs && st_ != nullptr && cfg_.batch % 6 == 0 && it_ % 6 == 0;
     if (use_graph && (!graph_ || graph_counters_ != counters_)) {
@@ -249,6 +250,7 @@ rtc_status Engine::finish() {
     L.w = wf_iter(it_);
     L.status = d_status_;
     L.counters = counters_;
+    L.wide = cfg_.wide;
     L.st = st_;
     L.grid = (int)std::max<uint32_t>(1u, (drain_ + 127u) / 128u);
     cudaError_t e = fn_(WF_OP_FINISH, A, B_, L);

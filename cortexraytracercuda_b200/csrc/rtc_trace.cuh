@@ -361,17 +361,19 @@ __device__ __forceinline__ bool closest_hit4(const DevScene& S, V3 o, V3 d, V3 i
     return best_item != 0xffffffffu;
 }
 
-// Closest hit in [tmin, tmax] over the whole scene (the reference's world.hit through the BVH):
-// through the 4-wide nodes when the scene carries them, else the binary nodes.
-// EXACT: clean mode (double-precision sphere test).
-template <bool EXACT = false>
+// Closest hit in [tmin, tmax] over the whole scene (the reference's world.hit through the BVH).
+// EXACT: clean mode (double-precision sphere test).  WIDE: walk the 4-wide nodes when the scene
+// carries them (only the extend kernel is built with it, so the other kernels carry no code for it).
+template <bool EXACT = false, bool WIDE = false>
 __device__ __forceinline__ bool closest_hit(const DevScene& S, V3 o, V3 d, float tmin, float tmax,
                                             bool hide_invisible, float& t_out, uint32_t& item_out,
                                             TraceStats& st, uint32_t& status) {
     V3 inv = v3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
-    if (S.nodes4) {
-        V3 oi4 = v3(o.x * inv.x, o.y * inv.y, o.z * inv.z);
-        return closest_hit4<EXACT>(S, o, d, inv, oi4, tmin, tmax, hide_invisible, t_out, item_out, st, status);
+    if constexpr (WIDE) {
+        if (S.nodes4) {
+            V3 oi4 = v3(o.x * inv.x, o.y * inv.y, o.z * inv.z);
+            return closest_hit4<EXACT>(S, o, d, inv, oi4, tmin, tmax, hide_invisible, t_out, item_out, st, status);
+        }
     }
     V3 oi = v3(o.x * inv.x, o.y * inv.y, o.z * inv.z);
     float best_t = tmax;

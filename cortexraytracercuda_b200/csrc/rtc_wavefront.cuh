@@ -236,7 +236,8 @@ __global__ void __launch_bounds__(128) wf_admit(WfTable J, WfBuffers B, WfIter w
 }
 
 // FLAVOR: 0 nvcc flavour, 1 g++ flavour, 2 clean mode (double-precision sphere test).
-template <bool COUNT, int FLAVOR, class J>
+// WIDE: the 4-wide node layout (RTC_FLAG_WIDE_BVH; the other kernels always walk the binary nodes).
+template <bool COUNT, int FLAVOR, class J, bool WIDE>
 __global__ void RTC_EXTEND_BOUNDS wf_extend(J jobs, WfBuffers B, WfIter w, unsigned long long* counters,
                                                  uint32_t* status_word) {
     const uint32_t n = B.ctr[w.cin];
@@ -252,7 +253,7 @@ __global__ void RTC_EXTEND_BOUNDS wf_extend(J jobs, WfBuffers B, WfIter w, unsig
         const uint32_t job = wf_job(mw);
         float t;
         uint32_t item;
-        bool h = closest_hit<FLAVOR == 2>(jobs.scene(job), v3(o), v3(d), 0.00001f, 3.402823466e+38f,
+        bool h = closest_hit<FLAVOR == 2, WIDE>(jobs.scene(job), v3(o), v3(d), 0.00001f, 3.402823466e+38f,
                                           wf_depth(mw) == (uint32_t)jobs.params(job).max_depth, t, item, st, status);
         B.hit[slot] = make_float2(t, __uint_as_float(h ? item : 0xffffffffu));
         ++rays;
@@ -557,8 +558,13 @@ cudaError_t wf_dispatch(WfOp op, const A& args, const WfBuffers& B, const WfLaun
         }
         break;
     case WF_OP_EXTEND:
-        if (c) wf_extend<true, FLAVOR><<<L.grid, 128, 0, L.st>>>(jobs, B, L.w, L.counters, L.status);
-        else wf_extend<false, FLAVOR><<<L.grid, 128, 0, L.st>>>(jobs, B, L.w, nullptr, L.status);
+        if (L.wide) {
+            if (c) wf_extend<true, FLAVOR, J, true><<<L.grid, 128, 0, L.st>>>(jobs, B, L.w, L.counters, L.status);
+            else wf_extend<false, FLAVOR, J, true><<<L.grid, 128, 0, L.st>>>(jobs, B, L.w, nullptr, L.status);
+        } else {
+            if (c) wf_extend<true, FLAVOR, J, false><<<L.grid, 128, 0, L.st>>>(jobs, B, L.w, L.counters, L.status);
+            else wf_extend<false, FLAVOR, J, false><<<L.grid, 128, 0, L.st>>>(jobs, B, L.w, nullptr, L.status);
+        }
         break;
     case WF_OP_SHADE:
         if (c) wf_shade<CLEAN, ORDER, true><<<L.grid, 128, 0, L.st>>>(jobs, B, L.w, L.counters, L.status);
