@@ -50,8 +50,8 @@ sys.path.insert(0, str(ROOT))
 
 from cortexraytracercuda_b200 import configs  # noqa: E402
 from cortexraytracercuda_b200.scene import (DRAW_ORDER_DEVICE, DRAW_ORDER_HOST, ENGINE_MEGAKERNEL,  # noqa: E402
-                                            ENGINE_WAVEFRONT, FLAG_KERNEL_TIMING, FLAG_WIDE_BVH, MODE_CLEAN,
-                                            MODE_COMPAT)
+                                            ENGINE_WAVEFRONT, FLAG_KERNEL_TIMING, FLAG_SAMPLE_GROUPS,
+                                            FLAG_WIDE_BVH, MODE_CLEAN, MODE_COMPAT)
 
 METRIC = "Mpaths/s"
 PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
@@ -250,6 +250,8 @@ def run_batched(args, rank, world, local):
     params = []
     for _, p in work:
         p.mode, p.draw_order, p.engine = mode, order, ENGINE_WAVEFRONT
+        if args.groups:
+            p.flags |= FLAG_SAMPLE_GROUPS
         if args.bvh == "4":
             p.flags |= FLAG_WIDE_BVH
         params.append(p)
@@ -411,7 +413,8 @@ def run_served(args, rank, world, local):
     dist = _init_dist(world, local)
     mode, order = _mode_order(args)
     work = configs.batch_workload(args.scenes)
-    srv = RenderServer(local, mode=mode, draw_order=order, slots=args.slots)
+    gflags = FLAG_SAMPLE_GROUPS if args.groups else 0
+    srv = RenderServer(local, mode=mode, draw_order=order, slots=args.slots, flags=gflags)
     t0 = time.perf_counter()
     ids = [srv.add_scene(sc) for sc, _ in work]
     setup_s = time.perf_counter() - t0
@@ -434,7 +437,8 @@ def run_served(args, rank, world, local):
     def request(k, sc, ang):
         cam = configs.orbit_camera(work[sc][0].camera, float(ang))
         p = work[sc][1]
-        rp = p.__class__(**{**p.__dict__, "mode": mode, "draw_order": order, "engine": ENGINE_WAVEFRONT})
+        rp = p.__class__(**{**p.__dict__, "mode": mode, "draw_order": order, "engine": ENGINE_WAVEFRONT,
+                            "flags": gflags})
         return rp, cam
 
     # warm-up: every scene once (uploads), not timed
@@ -518,7 +522,7 @@ def run_served(args, rank, world, local):
             "config": {"workload": f"served: Poisson streams over {len(work)} batched scenes, Zipf s=1.1, "
                                    f"orbit cameras, {args.requests} requests per rate",
                        "mode": "compat" if mode == MODE_COMPAT else "clean", "slots": args.slots or "default",
-                       "hbm_budget": "120 GB", "parallelism": f"replicas x{world}", "seed": configs.DEFAULT_SEED},
+                       "sample_groups": bool(args.groups), "hbm_budget": "120 GB", "parallelism": f"replicas x{world}", "seed": configs.DEFAULT_SEED},
             "rates": per_rate, "server": {k: st[k] for k in ("completed", "failed", "scene_uploads", "scene_evictions",
                                                              "peak_resident_bytes", "iterations", "launches")},
             "gpu_launches": int(st["launches"]),
@@ -555,6 +559,8 @@ def main():
     ap.add_argument("--drain", type=int, default=0, help="batched: drain threshold (0: default, 1: no drain)")
     ap.add_argument("--autotune", action="store_true",
                     help="batched: pick slots / batch / drain / BVH layout with the autotuner before timing")
+    ap.add_argument("--groups", action="store_true",
+                    help="batched/served, clean mode: split pixels into sample groups (RTC_FLAG_SAMPLE_GROUPS)")
     ap.add_argument("--lambdas", default="50,200,800", help="served: request rates (1/s)")
     ap.add_argument("--requests", type=int, default=300, help="served: requests per rate")
     ap.add_argument("--plain-requests", type=int, default=120, help="served: requests of the plain comparison")
@@ -593,6 +599,8 @@ def main():
     scene, params = workload(args.config)
     if args.mode == "clean":
         params.mode = MODE_CLEAN
+        if args.groups:
+            params.flags |= FLAG_SAMPLE_GROUPS
     if args.small:
         params.width, params.height, params.spp = params.width // 4, params.height // 4, 16
     params.engine = ENGINE_WAVEFRONT if args.engine == "wavefront" else ENGINE_MEGAKERNEL

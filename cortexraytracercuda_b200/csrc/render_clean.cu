@@ -18,8 +18,15 @@ __global__ void __launch_bounds__(128) rtc_render_clean(DevScene S, DevParams P,
     if (active) {
         const int i = (int)(pixel_index % P.width);
         const int j = (int)(pixel_index / P.width);
+        // sample groups (RTC_FLAG_SAMPLE_GROUPS): each group summed on its own, then the group sums in
+        // group order - the wavefront's arithmetic, where the groups run on separate slots
+        const int G = P.groups > 1 ? P.groups : 1;
+        float tr = 0.f, tg = 0.f, tb = 0.f;
+        for (int g = 0; g < G; ++g) {
+        const int s0 = (int)(((int64_t)g * P.spp) / G);
+        const int s1 = g + 1 == G ? P.spp : (int)(((int64_t)(g + 1) * P.spp) / G);
         float pr = 0.f, pg = 0.f, pb = 0.f;
-        for (int s = 0; s < P.spp; ++s) {
+        for (int s = s0; s < s1; ++s) {
             Pcg32 rng;
             rng.seed(mix64(((uint64_t)P.seed << 32) ^ (uint64_t)pixel_index), (uint64_t)s);
             float ju = rng.uniform(), jv = rng.uniform();
@@ -31,7 +38,17 @@ __global__ void __launch_bounds__(128) rtc_render_clean(DevScene S, DevParams P,
             if (isfinite(c.r) && isfinite(c.g) && isfinite(c.b)) { pr += c.r; pg += c.g; pb += c.b; }
             ++paths;
         }
-        out[pixel_index] = make_float4(pr, pg, pb, 1.0f);
+        if (g == 0) {
+            tr = pr;
+            tg = pg;
+            tb = pb;
+        } else {
+            tr += pr;
+            tg += pg;
+            tb += pb;
+        }
+        }
+        out[pixel_index] = make_float4(tr, tg, tb, 1.0f);
     }
     if (counters) {
         unsigned long long r = pc.rays, p = paths, n = pc.nodes, q = pc.prims;

@@ -62,6 +62,8 @@ extern "C" rtc_status rtc_render_noalloc(const rtc_scene* scene, const rtc_rende
         return rtc_set_error(RTC_ERR_INVALID_ARGUMENT, "radiance buffer must be 16-byte aligned");
     rtc_status r = rtc_check_render_params(params);
     if (r != RTC_OK) return r;
+    if (rtc_group_bytes(params) != 0)
+        return rtc_set_error(RTC_ERR_INVALID_ARGUMENT, "RTC_FLAG_SAMPLE_GROUPS needs scratch memory; use rtc_render_device");
     const uint64_t npix = (uint64_t)params->width * (uint64_t)params->height;
     const uint64_t cap = RTC_NOALLOC_MAX_PIXELS;
     if (npix > cap) {

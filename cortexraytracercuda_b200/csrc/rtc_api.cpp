@@ -89,6 +89,8 @@ extern "C" rtc_status rtc_context_destroy(rtc_context* c) {
     cudaFree(c->d_out);
     cudaFree(c->d_rgb8);
     cudaFree(c->d_wf);
+    cudaFree(c->d_groups);
+    cudaFree(c->d_batch_groups);
     if (c->h_poll) cudaFreeHost(c->h_poll);
     for (cudaEvent_t& e : c->poll_ev)
         if (e) cudaEventDestroy(e);
@@ -567,7 +569,22 @@ DevParams rtc_dev_params(const rtc_render_params* p) {
     P.seed = p->seed;
     P.draw_order = p->draw_order;
     P.num_pixels = (int64_t)p->width * p->height;
+    P.groups = (p->mode == RTC_MODE_CLEAN && (p->flags & RTC_FLAG_SAMPLE_GROUPS)) ? std::min(8, p->spp) : 1;
     return P;
+}
+
+size_t rtc_group_bytes(const rtc_render_params* p) {
+    const DevParams P = rtc_dev_params(p);
+    if (P.groups <= 1) return 0;
+    const size_t npix = (size_t)P.num_pixels;
+    return ((npix * (size_t)P.groups * sizeof(float4) + 255) & ~(size_t)255) + npix * sizeof(uint32_t);
+}
+
+void rtc_carve_groups(void* base, const rtc_render_params* p, float4** part, uint32_t** gcnt) {
+    const DevParams P = rtc_dev_params(p);
+    const size_t npix = (size_t)P.num_pixels;
+    *part = (float4*)base;
+    *gcnt = (uint32_t*)((uint8_t*)base + ((npix * (size_t)P.groups * sizeof(float4) + 255) & ~(size_t)255));
 }
 
 namespace {
@@ -670,7 +687,8 @@ rtc::WfOneFn wf_one_fn(const rtc_render_params* p) {
 
 rtc_status run_wavefront(const DevScene& S, const rtc_render_params* p, const WfBuffers& B, uint32_t* d_status,
                          float4* d_out, unsigned long long* d_counters, cudaStream_t st, int num_sms,
-                         const WfPoller& poll, cudaEvent_t* phase, WfRun& run, WfTimer* timer = nullptr) {
+                         const WfPoller& poll, cudaEvent_t* phase, WfRun& run, WfTimer* timer = nullptr,
+                         void* groups = nullptr) {
     const DevParams P = dev_params(p);
     const bool clean = p->mode == RTC_MODE_CLEAN;
     const WfOneFn fn = wf_one_fn(p);
@@ -678,6 +696,13 @@ rtc_status run_wavefront(const DevScene& S, const rtc_render_params* p, const Wf
     J.S = S;
     J.P = P;
     J.out = d_out;
+    J.part = nullptr;
+    J.gcnt = nullptr;
+    if (P.groups > 1) {
+        if (!groups) return fail(RTC_ERR_INVALID_ARGUMENT, "sample groups need scratch memory");
+        rtc_carve_groups(groups, p, &J.part, &J.gcnt);
+        RTC_CUDA(cudaMemsetAsync(J.gcnt, 0, (size_t)P.num_pixels * sizeof(uint32_t), st));
+    }
     WfLaunch L{};
     L.counters = d_counters;
     L.status = d_status;
@@ -691,7 +716,7 @@ rtc_status run_wavefront(const DevScene& S, const rtc_render_params* p, const Wf
     if (e != cudaSuccess) return cuda_fail(e, "wavefront init");
     L.grid = grid;
     const uint64_t nsamp = clean ? (uint64_t)P.spp : (uint64_t)P.sqrt_spp * P.sqrt_spp;
-    const uint64_t rounds = (uint64_t)((P.num_pixels + B.slots - 1) / B.slots);
+    const uint64_t rounds = (uint64_t)((P.num_pixels * P.groups + B.slots - 1) / B.slots);
     const uint64_t max_iters = rounds * nsamp * (uint64_t)(P.max_depth + 1) + 64;
     const int BATCH = 8;
     // drain threshold: below this many queued slots the finish kernel takes over
@@ -815,11 +840,19 @@ rtc_status run_wavefront(const DevScene& S, const rtc_render_params* p, const Wf
 
 rtc_status launch_wavefront(rtc_context* c, const rtc_scene* s, const rtc_render_params* p, float4* d_out,
                             unsigned long long* d_counters, cudaStream_t st) {
-    const int64_t npix = (int64_t)p->width * p->height;
-    const uint32_t slots = (uint32_t)std::min<int64_t>(npix, WF_MAX_SLOTS);
+    const int64_t units = (int64_t)p->width * p->height * dev_params(p).groups;
+    const uint32_t slots = (uint32_t)std::min<int64_t>(units, WF_MAX_SLOTS);
     WfBuffers B;
     rtc_status r = ensure_wavefront(c, slots, B);
     if (r != RTC_OK) return r;
+    const size_t gbytes = rtc_group_bytes(p);
+    if (gbytes > c->groups_cap) {
+        cudaFree(c->d_groups);
+        c->d_groups = nullptr;
+        c->groups_cap = 0;
+        RTC_CUDA(cudaMalloc(&c->d_groups, gbytes));
+        c->groups_cap = gbytes;
+    }
     WfPoller poll;
     poll.h = c->h_poll;
     poll.ev[0] = c->poll_ev[0];
@@ -832,7 +865,7 @@ rtc_status launch_wavefront(rtc_context* c, const rtc_scene* s, const rtc_render
     timer.pool = &c->kev;
     const bool timed = (p->flags & RTC_FLAG_KERNEL_TIMING) != 0;
     r = run_wavefront(rtc_scene_view(s, p), p, B, c->d_status, d_out, d_counters, st, c->num_sms, poll,
-                      c->phase_ev, run, timed ? &timer : nullptr);
+                      c->phase_ev, run, timed ? &timer : nullptr, c->d_groups);
     if (r != RTC_OK) return r;
     c->kev_ext = c->kev_shade = 0;
     c->kev_pairs.clear();

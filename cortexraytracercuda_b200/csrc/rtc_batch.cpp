@@ -29,8 +29,9 @@ uint32_t next_pow2(uint32_t x) {
 
 // Builds the device record of one job: the scene's arrays with the job's camera and parameters.
 rtc_status rtc_make_job(const rtc_scene* scene, const rtc_camera* camera, const rtc_render_params* params,
-                        float* d_out, DevJob& J) {
+                        float* d_out, DevJob& J, void* groups) {
     J = DevJob{};
+    if (groups) rtc_carve_groups(groups, params, &J.part, &J.gcnt);
     J.S = rtc_scene_view(scene, params);
     if (camera && !rtc_make_camera(*camera, J.S.cam)) return rtc_set_error(RTC_ERR_INVALID_ARGUMENT, "degenerate camera");
     J.P = rtc_dev_params(params);
@@ -58,8 +59,15 @@ extern "C" rtc_status rtc_render_batch(rtc_context* c, const rtc_job* jobs, uint
         const uint64_t npix = (uint64_t)j.params.width * j.params.height;
         const uint64_t sq = (uint64_t)std::max(1, (int)std::sqrt((double)j.params.spp));
         const uint64_t nsamp = j.params.mode == RTC_MODE_CLEAN ? (uint64_t)j.params.spp : sq * sq;
-        total_pix += npix;
+        total_pix += npix * (uint64_t)rtc_dev_params(&j.params).groups;
         bound += npix * nsamp * (uint64_t)(j.params.max_depth + 1);
+    }
+    // sample-group scratch of every image that uses it, zeroed counters (one buffer for the batch)
+    std::vector<size_t> goff(n, 0);
+    size_t gtotal = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        goff[i] = gtotal;
+        gtotal += (rtc_group_bytes(&jobs[i].params) + 255) & ~(size_t)255;
     }
     EngineConfig cfg;
     cfg.device = c->device;
@@ -87,6 +95,18 @@ extern "C" rtc_status rtc_render_batch(rtc_context* c, const rtc_job* jobs, uint
         if (r != RTC_OK) return r;
         c->engine = std::move(eng);
     }
+    if (gtotal > c->batch_groups_cap) {
+        cudaFree(c->d_batch_groups);
+        c->d_batch_groups = nullptr;
+        c->batch_groups_cap = 0;
+        e = cudaMalloc(&c->d_batch_groups, gtotal);
+        if (e != cudaSuccess) return cuda_err(e, "cudaMalloc(sample groups)");
+        c->batch_groups_cap = gtotal;
+    }
+    if (gtotal) {
+        e = cudaMemsetAsync(c->d_batch_groups, 0, gtotal, st);
+        if (e != cudaSuccess) return cuda_err(e, "cudaMemsetAsync(sample groups)");
+    }
     Engine& E = *c->engine;
     E.set_stream(st);
     E.set_counters(bp ? bp->d_counters : nullptr);
@@ -100,7 +120,8 @@ extern "C" rtc_status rtc_render_batch(rtc_context* c, const rtc_job* jobs, uint
         while (next_job < n && E.ring_free() > 0) {
             DevJob J;
             const rtc_job& j = jobs[next_job];
-            r = rtc_make_job(j.scene, j.camera, &j.params, j.d_radiance_sum, J);
+            void* g = rtc_group_bytes(&j.params) ? (uint8_t*)c->d_batch_groups + goff[next_job] : nullptr;
+            r = rtc_make_job(j.scene, j.camera, &j.params, j.d_radiance_sum, J, g);
             if (r == RTC_OK) r = E.admit(J, next_job, nullptr);
             if (r != RTC_OK) return r;
             ++next_job;

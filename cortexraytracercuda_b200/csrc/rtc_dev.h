@@ -102,6 +102,7 @@ struct DevParams {
     uint32_t seed;
     int draw_order;    // 0 device (left to right), 1 host (right to left)
     int64_t num_pixels;
+    int groups;        // sample groups per pixel (clean mode, RTC_FLAG_SAMPLE_GROUPS), else 1
 };
 
 // Wavefront path slots (SoA, one slot = one pixel in flight) and the two slot queues.
@@ -132,7 +133,10 @@ struct DevJob {
     DevScene S;                  // the scene's arrays, with this job's camera
     DevParams P;
     float4* out;                 // width*height radiance sums, frame-buffer order
-    unsigned long long begin;    // first index of the job's pixels in the engine's global pixel sequence
+    unsigned long long begin;    // first index of the job's work units (pixel x sample group) in the
+                                 // engine's global sequence
+    float4* part;                // P.groups > 1: width*height*groups partial sums
+    uint32_t* gcnt;              // P.groups > 1: per pixel, groups finished (zero at admission)
 };
 
 // Hand-out state of the global pixel sequence (device).  Pixels [next, limit) are admitted and not yet
@@ -153,6 +157,8 @@ struct WfOneArgs {             // one image
     DevScene S;
     DevParams P;
     float4* out;
+    float4* part;              // P.groups > 1: partial sums (width*height*groups)
+    uint32_t* gcnt;            // P.groups > 1: per-pixel count of finished groups (zeroed per render)
 };
 struct WfTableArgs {           // a ring of jobs
     const DevJob* jobs;

@@ -94,7 +94,7 @@ rtc_status Engine::admit(DevJob job, uint64_t tag, uint64_t* seq) {
     const uint32_t slot = (uint32_t)(s & (cfg_.ring - 1));
     const uint64_t npix = (uint64_t)job.P.num_pixels;
     job.begin = limit_;
-    limit_ += npix;
+    limit_ += npix * (uint64_t)std::max(1, job.P.groups);   // work units: pixel x sample group
     h_jobs_[slot] = job;
     ENG_CUDA(cudaMemcpyAsync(d_jobs_ + slot, h_jobs_ + slot, sizeof(DevJob), cudaMemcpyHostToDevice, st_));
     uint32_t* d_done = (uint32_t*)(d_prog_ + sizeof(WfFeed));

@@ -19,6 +19,9 @@ const rtc::DevScene& rtc_scene_dev(const rtc_scene* s);
 // the device view a render uses: the 4-wide nodes only when the params ask for RTC_FLAG_WIDE_BVH
 rtc::DevScene rtc_scene_view(const rtc_scene* s, const rtc_render_params* p);
 rtc::DevParams rtc_dev_params(const rtc_render_params* p);
+// scratch of an image rendered with sample groups (0 without), and its layout at `base`
+size_t rtc_group_bytes(const rtc_render_params* p);
+void rtc_carve_groups(void* base, const rtc_render_params* p, float4** part, uint32_t** gcnt);
 // perspective_camera::initialize; false for a degenerate camera
 bool rtc_make_camera(const rtc_camera& c, rtc::DevCamera& out);
 int rtc_scene_device(const rtc_scene* s);

@@ -25,6 +25,10 @@ struct rtc_context {
     // wavefront scratch: path slots (SoA) and the two slot queues
     void* d_wf = nullptr;
     uint32_t wf_cap = 0;
+    void* d_groups = nullptr;          // sample-group partial sums and counters (RTC_FLAG_SAMPLE_GROUPS)
+    size_t groups_cap = 0;
+    void* d_batch_groups = nullptr;    // the same for the images of a batch
+    size_t batch_groups_cap = 0;
     uint32_t* h_poll = nullptr;       // pinned: queue sizes read back between batches
     cudaEvent_t poll_ev[2] = {nullptr, nullptr};
     cudaEvent_t phase_ev[3] = {nullptr, nullptr, nullptr};   // render start, drain start, render end

@@ -31,8 +31,7 @@
 
 using namespace rtc;
 
-rtc_status rtc_make_job(const rtc_scene* scene, const rtc_camera* camera, const rtc_render_params* params,
-                        float* d_out, DevJob& J);
+
 
 namespace {
 
@@ -50,6 +49,8 @@ struct Request {
     float* host_out = nullptr;
     size_t out_bytes = 0;
     float4* d_out = nullptr;
+    void* d_groups = nullptr;         // sample-group scratch (RTC_FLAG_SAMPLE_GROUPS)
+    size_t group_bytes = 0;
     cudaEvent_t copy_ev = nullptr;
     rtc_request_info info{};
     rtc_status err = RTC_OK;
@@ -109,6 +110,7 @@ rtc_render_params request_params(const rtc_server* s, const rtc_request& r) {
     p.mode = s->cfg.mode;
     p.draw_order = s->cfg.draw_order;
     p.engine = RTC_ENGINE_WAVEFRONT;
+    p.flags = s->cfg.flags & ~RTC_FLAG_KERNEL_TIMING;
     return p;
 }
 
@@ -162,7 +164,9 @@ rtc_status admit_queued(rtc_server* s) {
         Request& R = *s->reqs.at(s->queue.front());
         SceneEntry& E = *s->scenes[R.req.scene_id];
         const bool upload = E.d_slab == nullptr;
-        const uint64_t need = R.out_bytes + (upload ? E.host.slab.size() : 0);
+        const rtc_render_params rp = request_params(s, R.req);
+        R.group_bytes = rtc_group_bytes(&rp);
+        const uint64_t need = R.out_bytes + R.group_bytes + (upload ? E.host.slab.size() : 0);
         if (need + s->eng->device_bytes() > s->budget) {   // can never fit
             fail_request(s, R, RTC_ERR_OOM, "request needs more device memory than the server's HBM budget");
             s->queue.pop_front();
@@ -185,20 +189,31 @@ rtc_status admit_queued(rtc_server* s) {
         if (e != cudaSuccess) return rtc_set_error(RTC_ERR_CUDA, (std::string("request output: ") + cudaGetErrorString(e)).c_str());
         R.d_out = (float4*)out;
         s->resident += R.out_bytes;
-        note_resident(s);
         DevJob J{};
+        if (R.group_bytes) {
+            e = cudaMallocFromPoolAsync(&R.d_groups, R.group_bytes, s->pool, s->st);
+            if (e == cudaSuccess) e = cudaMemsetAsync(R.d_groups, 0, R.group_bytes, s->st);
+            if (e != cudaSuccess) return rtc_set_error(RTC_ERR_CUDA, (std::string("sample groups: ") + cudaGetErrorString(e)).c_str());
+            rtc_carve_groups(R.d_groups, &rp, &J.part, &J.gcnt);
+            s->resident += R.group_bytes;
+        }
+        note_resident(s);
         J.S = E.dev;
         if (!R.req.use_scene_camera && !rtc_make_camera(R.req.camera, J.S.cam)) {
             cudaFreeAsync(out, s->st);
             R.d_out = nullptr;
             s->resident -= R.out_bytes;
+            if (R.d_groups) {
+                cudaFreeAsync(R.d_groups, s->st);
+                R.d_groups = nullptr;
+                s->resident -= R.group_bytes;
+            }
             fail_request(s, R, RTC_ERR_INVALID_ARGUMENT, "degenerate camera");
             s->queue.pop_front();
             s->cv_done.notify_all();
             continue;
         }
-        const rtc_render_params p = request_params(s, R.req);
-        J.P = rtc_dev_params(&p);
+        J.P = rtc_dev_params(&rp);
         J.out = R.d_out;
         rtc_status r = s->eng->admit(J, R.ticket, nullptr);
         if (r != RTC_OK) return r;
@@ -232,6 +247,11 @@ rtc_status start_copies(rtc_server* s) {
         cudaError_t e = cudaMemcpyAsync(R.host_out, R.d_out, R.out_bytes, cudaMemcpyDeviceToHost, s->st_copy);
         if (e == cudaSuccess) e = cudaEventRecord(ev, s->st_copy);
         if (e == cudaSuccess) e = cudaFreeAsync(R.d_out, s->st_copy);
+        if (e == cudaSuccess && R.d_groups) {   // every pixel is final: the group scratch is free
+            e = cudaFreeAsync(R.d_groups, s->st_copy);
+            R.d_groups = nullptr;
+            s->resident -= R.group_bytes;
+        }
         if (e != cudaSuccess) return rtc_set_error(RTC_ERR_CUDA, (std::string("result copy: ") + cudaGetErrorString(e)).c_str());
         R.d_out = nullptr;
         R.copy_ev = ev;
@@ -374,6 +394,7 @@ extern "C" rtc_status rtc_server_destroy(rtc_server* s) {
         if (e->d_slab) cudaFreeAsync(e->d_slab, s->st);
     for (auto& kv : s->reqs) {
         if (kv.second->d_out) cudaFreeAsync(kv.second->d_out, s->st);
+        if (kv.second->d_groups) cudaFreeAsync(kv.second->d_groups, s->st);
         if (kv.second->copy_ev) cudaEventDestroy(kv.second->copy_ev);
     }
     cudaStreamSynchronize(s->st);

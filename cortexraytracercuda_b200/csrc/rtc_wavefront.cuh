@@ -112,6 +112,16 @@ __device__ __forceinline__ uint32_t wf_samples(const DevParams& P, bool clean) {
     return clean ? (uint32_t)P.spp : (uint32_t)(P.sqrt_spp * P.sqrt_spp);
 }
 
+// Sample groups (clean mode with RTC_FLAG_SAMPLE_GROUPS): a pixel's samples are split into P.groups
+// consecutive ranges, each its own work unit on its own slot; group g covers samples
+// [g*spp/G, (g+1)*spp/G).  Compat mode always has one group (its samples share one stream).
+__device__ __forceinline__ uint32_t wf_group_begin(const DevParams& P, uint32_t g) {
+    return (uint32_t)(((uint64_t)g * (uint64_t)P.spp) / (uint64_t)P.groups);
+}
+__device__ __forceinline__ uint32_t wf_group_end(const DevParams& P, uint32_t g, bool clean) {
+    return g + 1u >= (uint32_t)P.groups ? wf_samples(P, clean) : wf_group_begin(P, g + 1u);
+}
+
 // ---- job sources ---------------------------------------------------------------------------------
 
 // One image.  Pixels are handed out by a plain atomicAdd on ctr[WF_NEXT_PIXEL] (overshoot is harmless:
@@ -121,13 +131,16 @@ struct WfOne : WfOneArgs {
     __device__ __forceinline__ const DevScene& scene(uint32_t) const { return S; }
     __device__ __forceinline__ const DevParams& params(uint32_t) const { return P; }
     __device__ __forceinline__ float4* output(uint32_t) const { return out; }
+    __device__ __forceinline__ float4* partials(uint32_t) const { return part; }
+    __device__ __forceinline__ uint32_t* group_counts(uint32_t) const { return gcnt; }
     __device__ __forceinline__ void pixel_done(uint32_t) const {}
-    __device__ __forceinline__ bool claim(const WfBuffers& B, const WfWindow&, uint32_t& job, uint32_t& pixel,
+    // claims the next work unit (pixel x sample group)
+    __device__ __forceinline__ bool claim(const WfBuffers& B, const WfWindow&, uint32_t& job, uint32_t& unit,
                                           uint32_t&) const {
         const uint32_t p = atomicAdd(B.ctr + WF_NEXT_PIXEL, 1u);
-        if ((int64_t)p >= P.num_pixels) return false;
+        if ((int64_t)p >= P.num_pixels * (int64_t)P.groups) return false;
         job = 0u;
-        pixel = p;
+        unit = p;
         return true;
     }
 };
@@ -149,8 +162,11 @@ struct WfTable : WfTableArgs {
     __device__ __forceinline__ const DevScene& scene(uint32_t j) const { return jobs[j].S; }
     __device__ __forceinline__ const DevParams& params(uint32_t j) const { return jobs[j].P; }
     __device__ __forceinline__ float4* output(uint32_t j) const { return jobs[j].out; }
+    __device__ __forceinline__ float4* partials(uint32_t j) const { return jobs[j].part; }
+    __device__ __forceinline__ uint32_t* group_counts(uint32_t j) const { return jobs[j].gcnt; }
     __device__ __forceinline__ void pixel_done(uint32_t j) const { atomicAdd(done + j, 1u); }
-    __device__ __forceinline__ bool claim(const WfBuffers&, const WfWindow& win, uint32_t& job, uint32_t& pixel,
+    // claims the next work unit (pixel x sample group) of the global sequence
+    __device__ __forceinline__ bool claim(const WfBuffers&, const WfWindow& win, uint32_t& job, uint32_t& unit,
                                           uint32_t&) const {
         const unsigned act = __activemask();
         const int lane = threadIdx.x & 31;
@@ -167,7 +183,7 @@ struct WfTable : WfTableArgs {
             else hi = mid;
         }
         job = lo & mask;
-        pixel = (uint32_t)(g - jobs[job].begin);
+        unit = (uint32_t)(g - jobs[job].begin);
         return true;
     }
 };
@@ -176,26 +192,56 @@ struct WfTable : WfTableArgs {
 template <bool CLEAN, int ORDER, class J>
 __device__ __forceinline__ bool wf_fetch_pixel(const J& jobs, const WfWindow& win, const WfBuffers& B, uint32_t slot,
                                                uint32_t& status) {
-    uint32_t job = 0, pixel = 0;
-    if (!jobs.claim(B, win, job, pixel, status)) {
+    uint32_t job = 0, unit = 0;
+    if (!jobs.claim(B, win, job, unit, status)) {
         B.meta[slot] = make_uint4(WF_IDLE, 0u, 0u, 0u);
         return false;
     }
     const DevScene& S = jobs.scene(job);
     const DevParams& P = jobs.params(job);
+    const uint32_t G = (uint32_t)P.groups;
+    const uint32_t pixel = G > 1u ? unit / G : unit, grp = G > 1u ? unit % G : 0u;
+    const uint32_t s0 = G > 1u ? wf_group_begin(P, grp) : 0u;
     WfRng<CLEAN> rng;
     if constexpr (!CLEAN) rng.seed(P.seed + pixel);
     Ray r;
-    wf_start_sample<CLEAN, ORDER>(S, P, rng, pixel, 0u, r);
+    wf_start_sample<CLEAN, ORDER>(S, P, rng, pixel, s0, r);
     B.ray_o[slot] = make_float4(r.o.x, r.o.y, r.o.z, r.time);
     B.ray_d[slot] = make_float4(r.d.x, r.d.y, r.d.z, 0.f);
     B.att[slot] = make_float4(1.f, 1.f, 1.f, 0.f);
     B.acc[slot] = make_float4(0.f, 0.f, 0.f, 0.f);
     B.psum[slot] = make_float4(0.f, 0.f, 0.f, 0.f);
-    uint4 m = make_uint4(pixel, 0u, 0u, wf_pack((uint32_t)P.max_depth, job));
+    uint4 m = make_uint4(pixel, s0, grp, wf_pack((uint32_t)P.max_depth, job));   // clean: z = group
     rng_save<CLEAN>(B, slot, rng, m);
     B.meta[slot] = m;
     return true;
+}
+
+// A finished sample group: with one group the pixel's sum is final; otherwise the group's sum is
+// stored, and the last group of the pixel to finish adds the partial sums in group order (so the
+// result does not depend on which group finished last).
+template <class J>
+__device__ __forceinline__ void wf_group_done(const J& jobs, uint32_t job, uint32_t pixel, uint32_t grp, float4 ps) {
+    const DevParams& P = jobs.params(job);
+    if (P.groups <= 1) {
+        jobs.output(job)[pixel] = make_float4(ps.x, ps.y, ps.z, 1.0f);
+        jobs.pixel_done(job);
+        return;
+    }
+    float4* part = jobs.partials(job) + (size_t)pixel * (size_t)P.groups;
+    part[grp] = ps;
+    __threadfence();
+    if (atomicAdd(jobs.group_counts(job) + pixel, 1u) != (uint32_t)P.groups - 1u) return;
+    __threadfence();
+    float4 t = __ldcg(part);
+    for (int g = 1; g < P.groups; ++g) {
+        const float4 v = __ldcg(part + g);
+        t.x += v.x;
+        t.y += v.y;
+        t.z += v.z;
+    }
+    jobs.output(job)[pixel] = make_float4(t.x, t.y, t.z, 1.0f);
+    jobs.pixel_done(job);
 }
 
 // First fill of a single-image render: slot k takes a pixel, joins queue 0.
@@ -321,7 +367,8 @@ __device__ __forceinline__ bool wf_step(const J& jobs, const WfWindow& win, cons
         ps.z += acc.b;
     }
     const uint32_t s = m.y + 1u;
-    if (s < wf_samples(P, CLEAN)) {
+    const uint32_t grp = CLEAN ? m.z : 0u;
+    if (s < (P.groups > 1 ? wf_group_end(P, grp, CLEAN) : wf_samples(P, CLEAN))) {
         // regenerate: the pixel's next sample on the same slot
         Ray nr;
         wf_start_sample<CLEAN, ORDER>(S, P, rng, m.x, s, nr);
@@ -336,9 +383,8 @@ __device__ __forceinline__ bool wf_step(const J& jobs, const WfWindow& win, cons
         B.meta[slot] = m;
         return true;
     }
-    // the pixel is done: write it and take the next pixel
-    jobs.output(job)[m.x] = make_float4(ps.x, ps.y, ps.z, 1.0f);
-    jobs.pixel_done(job);
+    // the pixel (or its sample group) is done: write it and take the next work unit
+    wf_group_done(jobs, job, m.x, grp, ps);
     return wf_fetch_pixel<CLEAN, ORDER>(jobs, win, B, slot, status);
 }
 
@@ -484,7 +530,7 @@ __global__ void RTC_FINISH_BOUNDS wf_finish(J jobs, WfBuffers B, WfIter w, unsig
         WfRng<CLEAN> rng;
         if constexpr (CLEAN) pcg_load(rng, B.pcg[slot]);
         else rng.x = m.z;
-        uint32_t pixel = m.x, sample = m.y, job = wf_job(m.w);
+        uint32_t pixel = m.x, sample = m.y, job = wf_job(m.w), grp = CLEAN ? m.z : 0u;
         int depth = (int)wf_depth(m.w);
         // one pass of the loop finishes the current sample of the current pixel
         for (;;) {
@@ -505,15 +551,14 @@ __global__ void RTC_FINISH_BOUNDS wf_finish(J jobs, WfBuffers B, WfIter w, unsig
                 pg += acc.g;
                 pb += acc.b;
             }
-            if (++sample < wf_samples(P, CLEAN)) {
+            if (++sample < (P.groups > 1 ? wf_group_end(P, grp, CLEAN) : wf_samples(P, CLEAN))) {
                 wf_start_sample<CLEAN, ORDER>(S, P, rng, pixel, sample, r);
                 att = rgb(1.f, 1.f, 1.f);
                 acc = rgb(0.f, 0.f, 0.f);
                 depth = P.max_depth;
                 continue;
             }
-            jobs.output(job)[pixel] = make_float4(pr, pg, pb, 1.0f);
-            jobs.pixel_done(job);
+            wf_group_done(jobs, job, pixel, grp, make_float4(pr, pg, pb, 0.0f));
             // a slot that still has pixels to take (fewer slots than pixels) continues through memory
             if (!wf_fetch_pixel<CLEAN, ORDER>(jobs, win, B, slot, status)) break;
             m = B.meta[slot];
@@ -527,7 +572,8 @@ __global__ void RTC_FINISH_BOUNDS wf_finish(J jobs, WfBuffers B, WfIter w, unsig
             if constexpr (CLEAN) pcg_load(rng, B.pcg[slot]);
             else rng.x = m.z;
             pixel = m.x;
-            sample = 0;
+            sample = m.y;
+            grp = CLEAN ? m.z : 0u;
             job = wf_job(m.w);
             depth = (int)wf_depth(m.w);
             if (status) break;

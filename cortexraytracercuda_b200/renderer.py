@@ -166,9 +166,9 @@ class RenderServer:
     when complete.  Scenes are registered once and kept resident under an HBM budget (LRU eviction)."""
 
     def __init__(self, device: int = 0, mode: int = MODE_COMPAT, draw_order: int = DRAW_ORDER_DEVICE,
-                 slots: int = 0, ring: int = 0, batch: int = 0, hbm_budget_bytes: int = 0):
+                 slots: int = 0, ring: int = 0, batch: int = 0, hbm_budget_bytes: int = 0, flags: int = 0):
         self.lib = _lib.load()
-        cfg = rtc_server_config(device, mode, draw_order, batch, slots, ring, hbm_budget_bytes)
+        cfg = rtc_server_config(device, mode, draw_order, batch, slots, ring, hbm_budget_bytes, flags)
         h = C.c_void_p()
         check(self.lib.rtc_server_create(C.byref(cfg), C.byref(h)))
         self.handle = h

@@ -24,6 +24,7 @@ MODE_COMPAT, MODE_CLEAN = 0, 1
 ENGINE_AUTO, ENGINE_MEGAKERNEL, ENGINE_WAVEFRONT = 0, 1, 2
 FLAG_KERNEL_TIMING = 1
 FLAG_WIDE_BVH = 2
+FLAG_SAMPLE_GROUPS = 4
 DRAW_ORDER_DEVICE, DRAW_ORDER_HOST = 0, 1
 
 F3 = C.c_float * 3
@@ -113,7 +114,8 @@ class rtc_batch_params(C.Structure):
 
 class rtc_server_config(C.Structure):
     _fields_ = [("device", C.c_int32), ("mode", C.c_int32), ("draw_order", C.c_int32), ("batch", C.c_int32),
-                ("slots", C.c_uint32), ("ring", C.c_uint32), ("hbm_budget_bytes", C.c_uint64)]
+                ("slots", C.c_uint32), ("ring", C.c_uint32), ("hbm_budget_bytes", C.c_uint64),
+                ("flags", C.c_int32)]
 
 
 class rtc_request(C.Structure):

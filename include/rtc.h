@@ -231,6 +231,13 @@ typedef struct rtc_render_params {
  * primitives at exactly the same distance is reported.  Measured slower on B200 (its traversal stack
  * does not stay in L1), kept as a node-layout option. */
 #define RTC_FLAG_WIDE_BVH 2
+/* Clean mode: split each pixel's samples into min(8, spp) consecutive groups that run on separate path
+ * slots, so a pixel's samples trace in parallel instead of one after another (shorter critical path,
+ * lower latency for an image).  Each group sums its samples in order, then the group sums are added in
+ * group order: results are deterministic and the same in both engines, but differ from the one-group
+ * sum in the last bits (float addition is not associative).  Needs per-image scratch: not available to
+ * rtc_render_noalloc.  Compat mode ignores it (a pixel's samples share one stream there). */
+#define RTC_FLAG_SAMPLE_GROUPS 4
 
 /* ------------------------------------------------------------------------------------------------ */
 /* context and scenes                                                                                */
@@ -377,6 +384,7 @@ typedef struct rtc_server_config {
     uint32_t ring;               /* requests in flight at most (power of two <= 65536); 0: 1024        */
     uint64_t hbm_budget_bytes;   /* device bytes for slots, resident scenes and request outputs;
                                     0: 120 GB                                                           */
+    int32_t flags;               /* RTC_FLAG_* applied to every request (e.g. RTC_FLAG_SAMPLE_GROUPS)    */
 } rtc_server_config;
 
 typedef struct rtc_request {
