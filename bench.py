@@ -426,7 +426,7 @@ def run_served(args, rank, world, local):
 
     def take(shape):
         lst = pools.setdefault(shape, [])
-        return lst.pop() if lst else torch.empty(shape, dtype=torch.float32, pin_memory=True)
+        return lst.pop() if lst else np.empty(shape, np.float32)   # the server stages through pinned memory
 
     def stream_of(lam, n):
         arr = np.cumsum(rng.exponential(1.0 / lam, n))
@@ -503,7 +503,7 @@ def run_served(args, rank, world, local):
             host = take((rp.height, rp.width, 4))
             ds = dss[int(scs[q])]
             ctx.render_batch([Job(ds, rp, out.data_ptr(), cam)], slots=1 << 20)   # one image per launch
-            host.copy_(out)
+            np.copyto(host, out.cpu().numpy())
             pools[tuple(host.shape)].append(host)
             done = time.perf_counter() - start
             plat.append((done - arr[q]) * 1e3)
@@ -561,7 +561,7 @@ def main():
                     help="batched: pick slots / batch / drain / BVH layout with the autotuner before timing")
     ap.add_argument("--groups", action="store_true",
                     help="batched/served, clean mode: split pixels into sample groups (RTC_FLAG_SAMPLE_GROUPS)")
-    ap.add_argument("--lambdas", default="50,200,800", help="served: request rates (1/s)")
+    ap.add_argument("--lambdas", default="20,50,200,800", help="served: request rates (1/s)")
     ap.add_argument("--requests", type=int, default=300, help="served: requests per rate")
     ap.add_argument("--plain-requests", type=int, default=120, help="served: requests of the plain comparison")
     args = ap.parse_args()

@@ -9,7 +9,7 @@ import ctypes as C
 import os
 from pathlib import Path
 
-from .scene import (rtc_batch_params, rtc_job, rtc_render_params, rtc_render_stats, rtc_request, rtc_request_info,
+from .scene import (rtc_batch_params, rtc_job, rtc_obj_mesh, rtc_render_params, rtc_render_stats, rtc_request, rtc_request_info,
                     rtc_scene_desc, rtc_scene_info, rtc_server_config, rtc_server_stats)
 
 LIB_PATH = Path(__file__).resolve().parent / "librtc_b200.so"
@@ -45,6 +45,8 @@ PROTOTYPES = {
     "rtc_trace_closest": (C.c_int, [_P, _P, _P, C.c_uint32, C.c_int32, C.c_int32, _P, _P]),
     "rtc_launchGPU": (C.c_int, [C.POINTER(rtc_scene_desc), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                 C.c_char_p, C.c_int]),
+    "rtc_load_obj": (C.c_int, [C.c_char_p, C.POINTER(rtc_obj_mesh)]),
+    "rtc_free_obj": (None, [C.POINTER(rtc_obj_mesh)]),
     "rtc_write_png": (C.c_int, [C.c_char_p, _P, C.c_int, C.c_int]),
 }
 

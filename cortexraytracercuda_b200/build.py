@@ -45,6 +45,7 @@ SOURCES = [
     ("rtc_engine.cpp", "rtc_engine", "cxx", []),
     ("rtc_batch.cpp", "rtc_batch", "cxx", []),
     ("rtc_server.cpp", "rtc_server", "cxx", []),
+    ("rtc_obj.cpp", "rtc_obj", "cxx", []),
     ("bvh_build.cpp", "bvh_build", "cxx", []),
 ]
 HEADERS = ["rtc_dev.h", "rtc_math.cuh", "rtc_trace.cuh", "rtc_path.cuh", "rtc_wavefront.cuh", "rtc_kernels.h",

@@ -3,8 +3,9 @@
 // Threads.  Client threads submit, poll and wait; one server thread owns the device work: it admits
 // queued requests (FIFO) whenever the job ring has a free entry and the HBM budget has room for the
 // request's output and, on a cache miss, its scene; it runs batches of wavefront iterations while
-// anything is in flight; and when a request's last pixel is written it copies the image to the
-// caller's buffer on a second stream, so the copy overlaps the next batches.
+// anything is in flight; and when a request's last pixel is written it copies the image on a second
+// stream into a reusable page-locked staging buffer (so the copy overlaps the next batches, whatever
+// memory the caller's buffer is), then into the caller's buffer.
 //
 // Memory.  Scene slabs and request outputs come from a stream-ordered memory pool of this server
 // (cudaMallocAsync / cudaFreeAsync on the server's streams), so neither admission nor eviction waits
@@ -16,6 +17,7 @@
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
+#include <cstring>
 #include <deque>
 #include <memory>
 #include <mutex>
@@ -50,6 +52,7 @@ struct Request {
     size_t out_bytes = 0;
     float4* d_out = nullptr;
     void* d_groups = nullptr;         // sample-group scratch (RTC_FLAG_SAMPLE_GROUPS)
+    void* h_stage = nullptr;          // page-locked staging of the result (server-owned)
     size_t group_bytes = 0;
     cudaEvent_t copy_ev = nullptr;
     rtc_request_info info{};
@@ -76,6 +79,11 @@ struct rtc_server {
     std::deque<uint64_t> queue;       // tickets waiting for admission
     std::vector<uint64_t> copying;    // server thread only
     std::vector<cudaEvent_t> free_events;
+    // page-locked staging buffers for result copies, reused by size: the device-to-host copy is
+    // asynchronous whatever memory the caller's buffer is, and no page-locked allocation (a blocking
+    // driver call) happens once the sizes in use have been seen
+    std::unordered_map<size_t, std::vector<void*>> stage_free;
+    std::vector<void*> stage_all;
     uint64_t next_ticket = 1;
     uint64_t lru_clock = 0;
     uint64_t in_flight = 0;           // engine jobs in flight as of the last batch (read by clients)
@@ -243,8 +251,16 @@ rtc_status start_copies(rtc_server* s) {
         } else if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
             return rtc_set_error(RTC_ERR_CUDA, "cudaEventCreate");
         }
+        std::vector<void*>& fl = s->stage_free[R.out_bytes];
+        if (!fl.empty()) {
+            R.h_stage = fl.back();
+            fl.pop_back();
+        } else {
+            if (cudaMallocHost(&R.h_stage, R.out_bytes) != cudaSuccess) return rtc_set_error(RTC_ERR_OOM, "cudaMallocHost(result staging)");
+            s->stage_all.push_back(R.h_stage);
+        }
         // the poll that reported the job complete has been waited for, so its pixels are final
-        cudaError_t e = cudaMemcpyAsync(R.host_out, R.d_out, R.out_bytes, cudaMemcpyDeviceToHost, s->st_copy);
+        cudaError_t e = cudaMemcpyAsync(R.h_stage, R.d_out, R.out_bytes, cudaMemcpyDeviceToHost, s->st_copy);
         if (e == cudaSuccess) e = cudaEventRecord(ev, s->st_copy);
         if (e == cudaSuccess) e = cudaFreeAsync(R.d_out, s->st_copy);
         if (e == cudaSuccess && R.d_groups) {   // every pixel is final: the group scratch is free
@@ -273,6 +289,9 @@ void finish_copies(rtc_server* s) {
         }
         s->free_events.push_back(R.copy_ev);
         R.copy_ev = nullptr;
+        std::memcpy(R.host_out, R.h_stage, R.out_bytes);   // into the caller's buffer
+        s->stage_free[R.out_bytes].push_back(R.h_stage);
+        R.h_stage = nullptr;
         R.info.state = RTC_REQ_DONE;
         R.info.done_ms = s->now_ms();
         s->resident -= R.out_bytes;
@@ -399,6 +418,7 @@ extern "C" rtc_status rtc_server_destroy(rtc_server* s) {
     }
     cudaStreamSynchronize(s->st);
     for (cudaEvent_t e : s->free_events) cudaEventDestroy(e);
+    for (void* h : s->stage_all) cudaFreeHost(h);
     s->eng.reset();   // the engine's buffers are released before the streams go
     if (s->pool) cudaMemPoolDestroy(s->pool);
     if (s->st_copy) cudaStreamDestroy(s->st_copy);

@@ -200,8 +200,7 @@ class RenderServer:
 
     def submit(self, scene_id: int, params: RenderParams, camera: Camera | None = None, out=None):
         """Queues a request; ``out`` (default: a new numpy array) is an (H, W, 4) float32 host buffer that
-        receives the radiance sums (page-locked memory, e.g. a pinned torch tensor, lets the copy
-        overlap).  Returns (ticket, out)."""
+        receives the radiance sums.  Returns (ticket, out)."""
         if out is None:
             out = np.empty((params.height, params.width, 4), np.float32)
         req = rtc_request(scene_id, 1 if camera is None else 0, (camera or Camera()).to_c(), params.width,

@@ -102,6 +102,11 @@ class rtc_scene_info(C.Structure):
                 ("max_leaf_size", C.c_uint32), ("device_bytes", C.c_uint64), ("build_ms", C.c_double)]
 
 
+class rtc_obj_mesh(C.Structure):
+    _fields_ = [("vertices", C.POINTER(C.c_float)), ("normals", C.POINTER(C.c_float)), ("uvs", C.POINTER(C.c_float)),
+                ("indices", C.POINTER(C.c_uint32)), ("num_vertices", C.c_uint32), ("num_triangles", C.c_uint32)]
+
+
 class rtc_job(C.Structure):
     _fields_ = [("scene", C.c_void_p), ("camera", C.POINTER(rtc_camera)), ("params", rtc_render_params),
                 ("d_radiance_sum", C.c_void_p)]
@@ -359,3 +364,22 @@ class SceneDesc:
 
     def ptr(self):
         return C.byref(self.desc)
+
+
+def load_obj(path):
+    """Reads a Wavefront OBJ file through the library's reader (rtc_load_obj): returns (vertices (n, 3),
+    indices (m, 3) uint32, normals (n, 3) or None, uvs (n, 2) or None) as numpy arrays, ready for
+    Scene.mesh()."""
+    from . import _lib
+    lib = _lib.load()
+    m = rtc_obj_mesh()
+    _lib.check(lib.rtc_load_obj(str(path).encode(), C.byref(m)))
+    try:
+        nv, nt = m.num_vertices, m.num_triangles
+        v = np.ctypeslib.as_array(m.vertices, shape=(nv, 3)).copy()
+        f = np.ctypeslib.as_array(m.indices, shape=(nt, 3)).copy()
+        n = np.ctypeslib.as_array(m.normals, shape=(nv, 3)).copy() if m.normals else None
+        t = np.ctypeslib.as_array(m.uvs, shape=(nv, 2)).copy() if m.uvs else None
+    finally:
+        lib.rtc_free_obj(C.byref(m))
+    return v, f, n, t

@@ -178,6 +178,22 @@ typedef struct rtc_scene_desc {
     rtc_background background;
 } rtc_scene_desc;
 
+/* Triangle geometry read from a Wavefront OBJ file, laid out for rtc_mesh: per-vertex positions (and
+ * normals / texture coordinates when the file has them, else NULL), 32-bit triangle indices.  Replaces
+ * the reference's tinyobjloader path (core/src/utilities/mesh_loader.cuh), which keeps shape 0 only
+ * (core/src/gpu.cu:628): here every object and group is merged, polygons are fan-triangulated and
+ * negative (relative) indices are resolved.  Free with rtc_free_obj. */
+typedef struct rtc_obj_mesh {
+    float* vertices;          /* num_vertices*3                                                    */
+    float* normals;           /* num_vertices*3 or NULL                                            */
+    float* uvs;               /* num_vertices*2 or NULL                                            */
+    uint32_t* indices;        /* num_triangles*3                                                   */
+    uint32_t num_vertices;
+    uint32_t num_triangles;
+} rtc_obj_mesh;
+rtc_status rtc_load_obj(const char* path, rtc_obj_mesh* mesh);
+void rtc_free_obj(rtc_obj_mesh* mesh);
+
 /* ------------------------------------------------------------------------------------------------ */
 /* render parameters                                                                                 */
 /* ------------------------------------------------------------------------------------------------ */
@@ -428,8 +444,8 @@ rtc_status rtc_server_destroy(rtc_server* server);
  * description may be freed after the call; the scene uploads on its first request. */
 rtc_status rtc_server_add_scene(rtc_server* server, const rtc_scene_desc* desc, uint32_t* scene_id);
 /* Queues a request.  `radiance_sum` (host, width*height*4 floats, frame-buffer order, as rtc_render
- * writes it) receives the result and must stay valid until the request is done; page-locked memory
- * lets the copy overlap the rendering of other requests. */
+ * writes it; any host memory) receives the result and must stay valid until the request is done.  The
+ * device-to-host copy goes through page-locked staging buffers the server keeps for reuse. */
 rtc_status rtc_server_submit(rtc_server* server, const rtc_request* req, float* radiance_sum, uint64_t* ticket);
 /* RTC_OK once the request is done (its record is released), RTC_ERR_BUSY while queued, running or
  * copying, RTC_ERR_NOT_FOUND for an unknown ticket; `info` (may be NULL) is filled in every case. */

@@ -10,8 +10,9 @@
 //     fuzziness), dielectric (refraction); solid colour, checker (textures if both resolve, else
 //     colours; odd lands in m_even as scene_factory does, scene_factory.cuh:619-629), image;
 //   * an object whose material does not resolve is skipped, as `if (mat)` skips it (gpu.cu:531).
+// OBJ meshes are read through an optional loader callback (with this library: rtc_load_obj).
 // Primitives the B200 path does not cover (planes, boxes, cones, cylinders, disks, tori, volumes,
-// omni/spot lights, OBJ meshes) and transforms are reported in `skipped`.
+// omni/spot lights) and transforms are reported in `skipped`.
 // Image textures need decoded RGB8 pixels: pass `load_image(filepath, &w, &h)` returning a pointer
 // that stays valid while the description is used (the reference decodes with stbi_load, gpu.cu:1743).
 #pragma once
@@ -32,6 +33,10 @@ struct SceneHolder {
     std::vector<rtc_dir_light> dir_lights;
     std::vector<rtc_sphere> spheres;
     std::vector<rtc_quad> quads;
+    std::vector<rtc_mesh> meshes;
+    // geometry of the OBJ meshes (owned here; rtc_mesh points into it)
+    std::vector<std::vector<float>> mesh_vertices, mesh_normals;
+    std::vector<std::vector<uint32_t>> mesh_indices;
     std::vector<std::string> skipped;
     rtc_scene_desc desc{};
 
@@ -48,13 +53,23 @@ struct SceneHolder {
         desc.num_spheres = (uint32_t)spheres.size();
         desc.quads = quads.data();
         desc.num_quads = (uint32_t)quads.size();
-        desc.meshes = nullptr;
-        desc.num_meshes = 0;
+        for (size_t i = 0; i < meshes.size(); ++i) {   // vectors may have moved since push_back
+            meshes[i].vertices = mesh_vertices[i].data();
+            meshes[i].indices = mesh_indices[i].data();
+            meshes[i].normals = mesh_normals[i].empty() ? nullptr : mesh_normals[i].data();
+        }
+        desc.meshes = meshes.data();
+        desc.num_meshes = (uint32_t)meshes.size();
         return &desc;
     }
 };
 
 using ImageLoader = std::function<const uint8_t*(const char* filepath, int* width, int* height)>;
+// Reads an OBJ file's triangles: positions (3 per vertex), indices (3 per triangle) and per-vertex
+// normals (3 per vertex, or left empty); returns false when the file cannot be read.  With this
+// library, a wrapper around rtc_load_obj / rtc_free_obj.
+using ObjLoader = std::function<bool(const char* filepath, std::vector<float>& vertices, std::vector<uint32_t>& indices,
+                                     std::vector<float>& normals)>;
 
 namespace detail {
 inline bool same(const char* a, const char* b) { return a && b && std::strcmp(a, b) == 0; }
@@ -65,7 +80,8 @@ template <class C> void putc3(float* dst, const C& c) { dst[0] = c.r(); dst[1] =
 
 // Converts `cfg` (a reference sceneConfig) into `out`; returns out.finish().
 template <class SceneConfig>
-const rtc_scene_desc* from_sceneconfig(const SceneConfig& cfg, SceneHolder& out, const ImageLoader& load_image = nullptr) {
+const rtc_scene_desc* from_sceneconfig(const SceneConfig& cfg, SceneHolder& out, const ImageLoader& load_image = nullptr,
+                                       const ObjLoader& load_obj = nullptr) {
     using namespace detail;
     const auto& T = cfg.texturesCfg;
     const auto& M = cfg.materialsCfg;
@@ -184,7 +200,38 @@ const rtc_scene_desc* from_sceneconfig(const SceneConfig& cfg, SceneHolder& out,
     if (P.conePrimitiveCount || P.cylinderPrimitiveCount || P.diskPrimitiveCount || P.torusPrimitiveCount ||
         P.volumePrimitiveCount)
         out.skipped.push_back("cones/cylinders/disks/tori/volumes");
-    if (cfg.meshesCfg.objMeshCount) out.skipped.push_back("OBJ meshes (pass triangles as rtc_mesh)");
+    // OBJ meshes (load_scene adds them after the quads, gpu.cu:612-635): geometry offset by `position`,
+    // one material for the whole mesh (use_mtl materials and transforms beyond the offset are reported)
+    const auto& MS = cfg.meshesCfg;
+    for (int i = 0; i < MS.objMeshCount; ++i) {
+        const auto& m = MS.objMeshes[i];
+        if (!load_obj) { out.skipped.push_back(std::string("OBJ mesh without loader: ") + (m.filepath ? m.filepath : "")); continue; }
+        const int mat = fetch_material(m.materialName);
+        if (mat < 0) continue;
+        std::vector<float> v, n;
+        std::vector<uint32_t> idx;
+        if (!m.filepath || !load_obj(m.filepath, v, idx, n) || idx.empty()) {
+            out.skipped.push_back(std::string("OBJ mesh not loaded: ") + (m.filepath ? m.filepath : ""));
+            continue;
+        }
+        float off[3];
+        put3(off, m.position);
+        for (size_t k = 0; k < v.size(); k += 3) {
+            v[k] += off[0];
+            v[k + 1] += off[1];
+            v[k + 2] += off[2];
+        }
+        if (m.use_mtl) out.skipped.push_back(std::string("OBJ materials (use_mtl) of ") + m.filepath);
+        rtc_mesh r{};
+        r.num_vertices = (uint32_t)(v.size() / 3);
+        r.num_triangles = (uint32_t)(idx.size() / 3);
+        r.material = mat;
+        r.smooth = (m.use_smoothing && n.size() == v.size()) ? 1 : 0;
+        out.mesh_vertices.push_back(std::move(v));
+        out.mesh_indices.push_back(std::move(idx));
+        out.mesh_normals.push_back(r.smooth ? std::move(n) : std::vector<float>());
+        out.meshes.push_back(r);
+    }
 
     const auto& C = cfg.cameraCfg;
     put3(out.desc.camera.look_from, C.lookFrom);

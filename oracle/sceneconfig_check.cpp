@@ -112,8 +112,29 @@ int main() {
     cfg.primitivesCfg.boxPrimitives = boxes;
     cfg.primitivesCfg.boxPrimitiveCount = 1;
 
+    static objMeshConfig objs[2];
+    objs[0].name = "tetra";
+    objs[0].position = point3(10.0f, 20.0f, 30.0f);
+    objs[0].filepath = "tetra.obj";
+    objs[0].materialName = "mirror";
+    objs[0].use_mtl = false;
+    objs[0].use_smoothing = true;
+    objs[1].name = "unreadable";
+    objs[1].filepath = "missing.obj";
+    objs[1].materialName = "white";
+    cfg.meshesCfg.objMeshes = objs;
+    cfg.meshesCfg.objMeshCount = 2;
+    // a stand-in for rtc_load_obj: one tetrahedron with normals for "tetra.obj", nothing else
+    auto load_obj = [](const char* path, std::vector<float>& v, std::vector<uint32_t>& idx, std::vector<float>& n) {
+        if (std::strcmp(path, "tetra.obj") != 0) return false;
+        v = {0, 0, 0, 1, 0, 0, 0, 1, 0, 0, 0, 1};
+        idx = {0, 2, 1, 0, 1, 3, 0, 3, 2, 1, 2, 3};
+        n = {-1, -1, -1, 1, 0, 0, 0, 1, 0, 0, 0, 1};
+        return true;
+    };
+
     rtc_adapter::SceneHolder h;
-    const rtc_scene_desc* d = rtc_adapter::from_sceneconfig(cfg, h);
+    const rtc_scene_desc* d = rtc_adapter::from_sceneconfig(cfg, h, nullptr, load_obj);
 
     std::printf("{\"textures\": [");
     for (uint32_t i = 0; i < d->num_textures; ++i) {
@@ -153,6 +174,15 @@ int main() {
         arr3("u", q.u);
         arr3("v", q.v);
         std::printf("\"material\": %d}", q.material);
+    }
+    std::printf("], \"meshes\": [");
+    for (uint32_t i = 0; i < d->num_meshes; ++i) {
+        const rtc_mesh& m = d->meshes[i];
+        std::printf("%s{\"num_vertices\": %u, \"num_triangles\": %u, \"material\": %d, \"smooth\": %d, ", i ? ", " : "",
+                    m.num_vertices, m.num_triangles, m.material, m.smooth);
+        arr3("v0", m.vertices);
+        arr3("v3", m.vertices + 9);
+        std::printf("\"has_normals\": %d, \"i1\": %u}", m.normals ? 1 : 0, m.indices[1]);
     }
     std::printf("], \"camera\": {");
     arr3("look_from", d->camera.look_from);

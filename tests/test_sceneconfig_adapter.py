@@ -76,3 +76,14 @@ def test_quads_and_checker_from_colours(desc):
     # colours: odd colour -> m_even, even colour -> m_odd (scene_factory.cuh:619-629)
     assert _tex(d, floor["even"])["color"] == [1.0, 0.0, 0.0]
     assert _tex(d, floor["odd"])["color"] == [0.0, 1.0, 0.0]
+
+
+def test_obj_meshes_through_the_loader(desc):
+    d = desc
+    assert len(d["meshes"]) == 1                        # the unreadable file is reported, not added
+    m = d["meshes"][0]
+    assert m["num_vertices"] == 4 and m["num_triangles"] == 4 and m["smooth"] == 1 and m["has_normals"] == 1
+    assert m["v0"] == [10.0, 20.0, 30.0] and m["v3"] == [10.0, 20.0, 31.0]   # offset by the mesh position
+    assert m["i1"] == 2
+    assert d["materials"][m["material"]]["kind"] == 1   # "mirror" is a metal
+    assert any("missing.obj" in s for s in d["skipped"])
