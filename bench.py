@@ -13,7 +13,8 @@ semantics: per-pixel thrust::minstd_rand stream, mixture-PDF lambertian, floor(s
 value  = Mpaths/s of the whole job (all ranks; weak scaling, one replica frame per rank), device time
          from CUDA events on the launching stream, L2 flushed (256 MiB write) between steps.
 e2e    = the same metric through the public C ABI with host buffers: per step rtc_scene_create
-         (flatten + SAH BVH + H2D upload) + rtc_render (kernel + D2H of the FP32 radiance) + destroy.
+         (flatten + BVH build + H2D upload) + rtc_render (kernel + D2H of the FP32 radiance) + destroy.
+         The BVH is the host SAH build unless --builder device (linear BVH built on the GPU).
 roofline: algorithmic bytes of the render kernel per launch (BVH node visits x 64 B + primitive tests x
          their record size + per-ray state), counted by an instrumented launch of the same frame, divided
          by the mean event time of the timed launches, against the measured HBM copy bandwidth.
@@ -51,7 +52,7 @@ sys.path.insert(0, str(ROOT))
 from cortexraytracercuda_b200 import configs  # noqa: E402
 from cortexraytracercuda_b200.scene import (DRAW_ORDER_DEVICE, DRAW_ORDER_HOST, ENGINE_MEGAKERNEL,  # noqa: E402
                                             ENGINE_WAVEFRONT, FLAG_KERNEL_TIMING, FLAG_SAMPLE_GROUPS,
-                                            FLAG_WIDE_BVH, MODE_CLEAN, MODE_COMPAT)
+                                            FLAG_WIDE_BVH, MODE_CLEAN, MODE_COMPAT, BVH_DEVICE, BVH_SAH)
 
 METRIC = "Mpaths/s"
 PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
@@ -549,6 +550,8 @@ def main():
     ap.add_argument("--mode", default="compat", choices=["compat", "clean"])
     ap.add_argument("--engine", default="wavefront", choices=["wavefront", "megakernel"])
     ap.add_argument("--bvh", default="2", choices=["2", "4"], help="BVH node layout (binary or 4-wide)")
+    ap.add_argument("--builder", default="sah", choices=["sah", "device"],
+                    help="BVH builder: host binned SAH or the device linear BVH (Morton codes)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-baseline-s", type=float, default=12.0)
     ap.add_argument("--ref-step-s", type=float, default=8.0)
@@ -606,7 +609,8 @@ def main():
     params.engine = ENGINE_WAVEFRONT if args.engine == "wavefront" else ENGINE_MEGAKERNEL
     if args.bvh == "4":
         params.flags |= FLAG_WIDE_BVH
-    ds = DeviceScene(ctx, scene)
+    builder = BVH_DEVICE if args.builder == "device" else BVH_SAH
+    ds = DeviceScene(ctx, scene, builder)
     info = ds.info()
     W, H = params.width, params.height
     out = torch.empty((H, W, 4), dtype=torch.float32, device="cuda")
@@ -666,7 +670,7 @@ def main():
     for k in range(0 if args.no_e2e else args.warmup + args.steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        ds2 = DeviceScene(ctx, scene)
+        ds2 = DeviceScene(ctx, scene, builder)
         p = params.to_c()
         from cortexraytracercuda_b200._lib import check
         check(ctx.lib.rtc_render(ctx.handle, ds2.handle, C.byref(p), host_out.ctypes.data, None))
@@ -722,7 +726,9 @@ def main():
             "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {**describe(args.config, params, scene), "parallelism": f"replicas x{world}",
-                       "bvh_nodes": info["num_nodes"], "bvh_layout": "binary" if args.bvh == "2" else "4-wide"},
+                       "bvh_nodes": info["num_nodes"], "bvh_layout": "binary" if args.bvh == "2" else "4-wide",
+                       "bvh_builder": "device LBVH" if info["bvh_builder"] == BVH_DEVICE else "host SAH",
+                       "scene_build_ms": round(info["build_ms"], 1)},
             "mrays_per_s": round(mrays, 3),
             "gpu_launches": int(sum(st["launches"] for st in kstats)) if wavefront else args.steps,
             "e2e": {"value": round(e2e_value, 3), "unit": METRIC, "h2d_bytes_per_step": int(info["device_bytes"]),

@@ -10,7 +10,7 @@ import os
 from pathlib import Path
 
 from .scene import (rtc_batch_params, rtc_job, rtc_obj_mesh, rtc_render_params, rtc_render_stats, rtc_request, rtc_request_info,
-                    rtc_scene_desc, rtc_scene_info, rtc_server_config, rtc_server_stats)
+                    rtc_scene_desc, rtc_scene_info, rtc_scene_options, rtc_server_config, rtc_server_stats)
 
 LIB_PATH = Path(__file__).resolve().parent / "librtc_b200.so"
 
@@ -28,6 +28,8 @@ PROTOTYPES = {
     "rtc_context_create": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
     "rtc_context_destroy": (C.c_int, [_P]),
     "rtc_scene_create": (C.c_int, [_P, C.POINTER(rtc_scene_desc), C.POINTER(C.c_void_p)]),
+    "rtc_scene_create_ex": (C.c_int, [_P, C.POINTER(rtc_scene_desc), C.POINTER(rtc_scene_options),
+                                      C.POINTER(C.c_void_p)]),
     "rtc_scene_destroy": (C.c_int, [_P]),
     "rtc_scene_get_info": (C.c_int, [_P, C.POINTER(rtc_scene_info)]),
     "rtc_render": (C.c_int, [_P, _P, C.POINTER(rtc_render_params), _P, _P]),

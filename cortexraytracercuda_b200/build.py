@@ -46,6 +46,7 @@ SOURCES = [
     ("rtc_batch.cpp", "rtc_batch", "cxx", []),
     ("rtc_server.cpp", "rtc_server", "cxx", []),
     ("rtc_obj.cpp", "rtc_obj", "cxx", []),
+    ("bvh_device.cu", "bvh_device", "nvcc", []),
     ("bvh_build.cpp", "bvh_build", "cxx", []),
 ]
 HEADERS = ["rtc_dev.h", "rtc_math.cuh", "rtc_trace.cuh", "rtc_path.cuh", "rtc_wavefront.cuh", "rtc_kernels.h",

@@ -1,0 +1,283 @@
+// bvh_device.cu - device BVH build (linear BVH over Morton codes) for rtc_scene_create_ex.
+//
+// The reference builds its BVH on one device thread, choosing a random axis per node and
+// exchange-sorting the span (O(n^2), core/src/misc/bvh_node.cuh:63-108, called from gpu.cu:749).  The
+// library's default is a binned SAH build on host threads (bvh_build.cpp); this is the fast
+// alternative for large meshes and cache misses, in the layout the traversal already reads:
+//   1. 30-bit Morton code of each primitive's box centroid (10 bits per axis over the centroid bounds);
+//   2. radix sort of (code, primitive) pairs (CUB);
+//   3. one thread per internal node finds the node's key range and split from the longest common
+//      prefixes of neighbouring codes (Karras, "Maximizing Parallelism in the Construction of BVHs,
+//      Octrees, and k-d Trees", HPG 2012), ties between equal codes broken by sorted position;
+//   4. bottom-up boxes: every leaf walks towards the root; the first thread to reach a node stops, the
+//      second (both children now known) writes the node's 64-byte record and goes on - no thread ever
+//      waits for another.
+// Every leaf holds one primitive; the leaf order is the sorted order.  Quality is below the SAH
+// build's (more node visits per ray); the build is a few milliseconds where the host build of a
+// million triangles takes a second.
+#include <cub/device/device_radix_sort.cuh>
+
+#include <algorithm>
+#include <cfloat>
+#include <cstring>
+#include <vector>
+
+#include "bvh_build.h"
+#include "rtc_dev.h"
+
+namespace rtc {
+namespace {
+
+__device__ __forceinline__ uint32_t spread10(uint32_t v) {   // bit k of v -> bit 3k
+    v = (v * 0x00010001u) & 0xFF0000FFu;
+    v = (v * 0x00000101u) & 0x0F00F00Fu;
+    v = (v * 0x00000011u) & 0xC30C30C3u;
+    v = (v * 0x00000005u) & 0x49249249u;
+    return v;
+}
+
+__global__ void k_morton(const Aabb* __restrict__ boxes, uint32_t n, float3 lo, float3 scale, uint32_t* keys,
+                         uint32_t* vals) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const Aabb b = boxes[i];
+    uint32_t q[3];
+    const float c[3] = {0.5f * (b.lo[0] + b.hi[0]), 0.5f * (b.lo[1] + b.hi[1]), 0.5f * (b.lo[2] + b.hi[2])};
+    const float l[3] = {lo.x, lo.y, lo.z}, s[3] = {scale.x, scale.y, scale.z};
+    for (int k = 0; k < 3; ++k) {
+        float x = (c[k] - l[k]) * s[k];
+        x = x < 0.0f ? 0.0f : (x > 1023.0f ? 1023.0f : x);
+        q[k] = (uint32_t)x;
+    }
+    keys[i] = (spread10(q[0]) << 2) | (spread10(q[1]) << 1) | spread10(q[2]);
+    vals[i] = i;
+}
+
+// Length of the common prefix of sorted keys a and b (-1 outside [0, n)); equal keys compare their
+// positions, so every prefix is distinct.
+__device__ __forceinline__ int delta(const uint32_t* __restrict__ k, int64_t n, int64_t a, int64_t b) {
+    if (b < 0 || b >= n) return -1;
+    const uint32_t ka = k[a], kb = k[b];
+    if (ka == kb) return 32 + __clz((uint32_t)a ^ (uint32_t)b);
+    return __clz(ka ^ kb);
+}
+
+// Children of internal node i: >= 0 an internal node, < 0 a leaf in the node layout's encoding.
+__global__ void k_internal(const uint32_t* __restrict__ keys, uint32_t n, int32_t* __restrict__ child,
+                           int32_t* __restrict__ parent_int, int32_t* __restrict__ parent_leaf, uint32_t* error) {
+    const int64_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t N = n;
+    if (i >= N - 1) return;
+    const int d = delta(keys, N, i, i + 1) - delta(keys, N, i, i - 1) >= 0 ? 1 : -1;
+    const int dmin = delta(keys, N, i, i - d);
+    int64_t lmax = 2;
+    int guard = 0;
+    while (delta(keys, N, i, i + lmax * d) > dmin) {
+        lmax *= 2;
+        if (++guard > 40) { atomicOr(error, 1u); return; }
+    }
+    int64_t l = 0;
+    for (int64_t t = lmax / 2; t >= 1; t /= 2)
+        if (delta(keys, N, i, i + (l + t) * d) > dmin) l += t;
+    const int64_t j = i + l * d;
+    const int dnode = delta(keys, N, i, j);
+    int64_t s = 0, t = l;
+    do {
+        t = (t + 1) / 2;
+        if (delta(keys, N, i, i + (s + t) * d) > dnode) s += t;
+    } while (t > 1);
+    const int64_t g = i + s * d + (d < 0 ? -1 : 0);
+    const int64_t lo = i < j ? i : j, hi = i < j ? j : i;
+    int32_t cl, cr;
+    if (lo == g) {
+        cl = (int32_t)~(((uint32_t)g << LEAF_COUNT_BITS) | 1u);
+        parent_leaf[g] = (int32_t)i;
+    } else {
+        cl = (int32_t)g;
+        parent_int[g] = (int32_t)i;
+    }
+    if (hi == g + 1) {
+        cr = (int32_t)~(((uint32_t)(g + 1) << LEAF_COUNT_BITS) | 1u);
+        parent_leaf[g + 1] = (int32_t)i;
+    } else {
+        cr = (int32_t)(g + 1);
+        parent_int[g + 1] = (int32_t)i;
+    }
+    child[2 * i] = cl;
+    child[2 * i + 1] = cr;
+}
+
+// A child's box: an inner node's box was written by another thread (possibly on another SM), so it is
+// read from L2 (ld.global.cg), never from a possibly stale L1 line.
+__device__ __forceinline__ Aabb box_of(int32_t c, const Aabb* __restrict__ boxes, const uint32_t* __restrict__ vals,
+                                       const Aabb* node_box) {
+    Aabb b;
+    if (c >= 0) {
+        const float* f = node_box[c].lo;
+        for (int k = 0; k < 3; ++k) {
+            b.lo[k] = __ldcg(f + k);
+            b.hi[k] = __ldcg(f + 3 + k);
+        }
+        return b;
+    }
+    const uint32_t pos = ((uint32_t)~c) >> LEAF_COUNT_BITS;
+    return boxes[vals[pos]];
+}
+
+// Bottom-up pass: writes every internal node's record (both child boxes and child links) and box, and
+// the depth of the deepest leaf.
+__global__ void k_bottom_up(const Aabb* __restrict__ boxes, const uint32_t* __restrict__ vals, uint32_t n,
+                            const int32_t* __restrict__ child, const int32_t* __restrict__ parent_int,
+                            const int32_t* __restrict__ parent_leaf, uint32_t* flags, Aabb* node_box,
+                            float4* nodes, uint32_t* max_depth, uint32_t* error) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    // Every index read from the link arrays is range-checked (they start as -1): a malformed tree sets
+    // an error bit instead of reading out of bounds.
+    const int32_t inner = (int32_t)n - 1;
+    auto inner_ok = [inner](int32_t p) { return p >= 0 && p < inner; };
+    // depth of this leaf
+    uint32_t depth = 1;
+    int32_t p = parent_leaf[k];
+    if (!inner_ok(p)) { atomicOr(error, 2u); return; }
+    while (p != 0) {
+        p = parent_int[p];
+        if (++depth > 4096u || !inner_ok(p)) { atomicOr(error, 2u); return; }
+    }
+    atomicMax(max_depth, depth + 1u);
+    int32_t node = parent_leaf[k];
+    for (uint32_t steps = 0; steps < 4096u; ++steps) {
+        __threadfence();
+        if (atomicAdd(flags + node, 1u) == 0u) return;   // the other child is not done yet: it goes on
+        __threadfence();
+        const int32_t cl = child[2 * node], cr = child[2 * node + 1];
+        const bool okl = cl >= 0 ? cl < inner : (((uint32_t)~cl) >> LEAF_COUNT_BITS) < n;
+        const bool okr = cr >= 0 ? cr < inner : (((uint32_t)~cr) >> LEAF_COUNT_BITS) < n;
+        if (!okl || !okr) { atomicOr(error, 8u); return; }
+        const Aabb L = box_of(cl, boxes, vals, node_box), R = box_of(cr, boxes, vals, node_box);
+        Aabb U;
+        for (int a = 0; a < 3; ++a) {
+            U.lo[a] = fminf(L.lo[a], R.lo[a]);
+            U.hi[a] = fmaxf(L.hi[a], R.hi[a]);
+        }
+        node_box[node] = U;
+        float4* np = nodes + 4 * (size_t)node;
+        np[0] = make_float4(L.lo[0], L.hi[0], L.lo[1], L.hi[1]);
+        np[1] = make_float4(R.lo[0], R.hi[0], R.lo[1], R.hi[1]);
+        np[2] = make_float4(L.lo[2], L.hi[2], R.lo[2], R.hi[2]);
+        np[3] = make_float4(__int_as_float(cl), __int_as_float(cr), 0.0f, 0.0f);
+        if (node == 0) return;
+        node = parent_int[node];
+        if (!inner_ok(node)) { atomicOr(error, 8u); return; }
+    }
+    atomicOr(error, 4u);
+}
+
+template <class T>
+cudaError_t dalloc(T** p, size_t n, cudaStream_t st) {
+    return cudaMallocAsync((void**)p, std::max<size_t>(n, 1) * sizeof(T), st);
+}
+
+}  // namespace
+
+int build_bvh_device(const BvhInput& in, int device, BvhOutput& out, const char** err) {
+    const size_t n = in.boxes.size();
+    if (n < 2 || n >= (1u << 26)) {
+        if (err) *err = "device BVH build needs 2 .. 2^26-1 primitives";
+        return BVH_DEVICE_UNSUPPORTED;
+    }
+    // centroid bounds (one host pass over the boxes the caller already computed)
+    float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    for (const Aabb& b : in.boxes)
+        for (int k = 0; k < 3; ++k) {
+            const float c = 0.5f * (b.lo[k] + b.hi[k]);
+            lo[k] = std::min(lo[k], c);
+            hi[k] = std::max(hi[k], c);
+        }
+    float sc[3];
+    for (int k = 0; k < 3; ++k) sc[k] = hi[k] > lo[k] ? 1023.0f / (hi[k] - lo[k]) : 0.0f;
+
+    // Own non-blocking stream and stream-ordered allocations: a build never waits for (or stalls) work
+    // that other threads have in flight on the device.
+    cudaError_t e = cudaSetDevice(device);
+    cudaStream_t st = nullptr;
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        if (err) *err = cudaGetErrorString(e);
+        return BVH_DEVICE_ERROR;
+    }
+    Aabb* d_boxes = nullptr;
+    uint32_t *d_keys = nullptr, *d_keys2 = nullptr, *d_vals = nullptr, *d_vals2 = nullptr, *d_flags = nullptr,
+             *d_info = nullptr;
+    int32_t *d_child = nullptr, *d_pint = nullptr, *d_pleaf = nullptr;
+    Aabb* d_nbox = nullptr;
+    float4* d_nodes = nullptr;
+    void* d_temp = nullptr;
+    size_t temp_bytes = 0;
+    int rc = BVH_DEVICE_ERROR;
+    const char* what = nullptr;
+    uint32_t* h_info = nullptr;
+    do {
+        if ((e = dalloc(&d_boxes, n, st)) || (e = dalloc(&d_keys, n, st)) || (e = dalloc(&d_keys2, n, st)) ||
+            (e = dalloc(&d_vals, n, st)) || (e = dalloc(&d_vals2, n, st)) || (e = dalloc(&d_flags, n, st)) ||
+            (e = dalloc(&d_info, 4, st)) || (e = dalloc(&d_child, 2 * n, st)) || (e = dalloc(&d_pint, n, st)) ||
+            (e = dalloc(&d_pleaf, n, st)) || (e = dalloc(&d_nbox, n, st)) || (e = dalloc(&d_nodes, 4 * n, st)))
+            break;
+        if ((e = cudaMallocHost((void**)&h_info, 4 * sizeof(uint32_t)))) break;
+        if ((e = cudaMemcpyAsync(d_boxes, in.boxes.data(), n * sizeof(Aabb), cudaMemcpyHostToDevice, st))) break;
+        if ((e = cudaMemsetAsync(d_flags, 0, n * sizeof(uint32_t), st))) break;
+        if ((e = cudaMemsetAsync(d_child, 0xFF, 2 * n * sizeof(int32_t), st))) break;
+        if ((e = cudaMemsetAsync(d_pint, 0xFF, n * sizeof(int32_t), st))) break;
+        if ((e = cudaMemsetAsync(d_pleaf, 0xFF, n * sizeof(int32_t), st))) break;
+        if ((e = cudaMemsetAsync(d_info, 0, 4 * sizeof(uint32_t), st))) break;
+        const unsigned grid = (unsigned)((n + 255) / 256);
+        k_morton<<<grid, 256, 0, st>>>(d_boxes, (uint32_t)n, make_float3(lo[0], lo[1], lo[2]),
+                                       make_float3(sc[0], sc[1], sc[2]), d_keys, d_vals);
+        if ((e = cudaGetLastError())) break;
+        cub::DoubleBuffer<uint32_t> K(d_keys, d_keys2), V(d_vals, d_vals2);
+        if ((e = cub::DeviceRadixSort::SortPairs(nullptr, temp_bytes, K, V, (int)n, 0, 30, st))) break;
+        if ((e = cudaMallocAsync(&d_temp, std::max<size_t>(temp_bytes, 1), st))) break;
+        if ((e = cub::DeviceRadixSort::SortPairs(d_temp, temp_bytes, K, V, (int)n, 0, 30, st))) break;
+        const uint32_t* keys = K.Current();
+        const uint32_t* vals = V.Current();
+        k_internal<<<grid, 256, 0, st>>>(keys, (uint32_t)n, d_child, d_pint, d_pleaf, d_info);
+        if ((e = cudaGetLastError())) break;
+        k_bottom_up<<<grid, 256, 0, st>>>(d_boxes, vals, (uint32_t)n, d_child, d_pint, d_pleaf, d_flags, d_nbox,
+                                          d_nodes, d_info + 1, d_info);
+        if ((e = cudaGetLastError())) break;
+        out.nodes.resize((n - 1) * 16);
+        out.order.resize(n);
+        if ((e = cudaMemcpyAsync(h_info, d_info, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st))) break;
+        if ((e = cudaMemcpyAsync(out.nodes.data(), d_nodes, (n - 1) * 16 * sizeof(float), cudaMemcpyDeviceToHost, st)))
+            break;
+        if ((e = cudaMemcpyAsync(out.order.data(), vals, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, st))) break;
+        if ((e = cudaStreamSynchronize(st))) break;
+        if (h_info[0]) {
+            what = "device BVH build produced an inconsistent tree";
+            break;
+        }
+        out.num_nodes = (uint32_t)(n - 1);
+        out.max_depth = h_info[1];
+        out.max_leaf_seen = 1;
+        out.nodes4.clear();
+        out.num_nodes4 = 0;
+        if (out.max_depth + 2 > (uint32_t)TRAVERSAL_STACK) {
+            what = "device BVH too deep for the traversal stack";
+            rc = BVH_DEVICE_TOO_DEEP;
+        } else {
+            rc = BVH_DEVICE_OK;
+        }
+    } while (false);
+    for (void* p : {(void*)d_boxes, (void*)d_keys, (void*)d_keys2, (void*)d_vals, (void*)d_vals2, (void*)d_flags,
+                    (void*)d_info, (void*)d_child, (void*)d_pint, (void*)d_pleaf, (void*)d_nbox, (void*)d_nodes, d_temp})
+        if (p) cudaFreeAsync(p, st);
+    const cudaError_t e2 = cudaStreamSynchronize(st);
+    if (h_info) cudaFreeHost(h_info);
+    cudaStreamDestroy(st);
+    if (e == cudaSuccess) e = e2;
+    if (e != cudaSuccess) rc = BVH_DEVICE_ERROR;
+    if (rc != BVH_DEVICE_OK && err) *err = e != cudaSuccess ? cudaGetErrorString(e) : what;
+    return rc;
+}
+
+}  // namespace rtc

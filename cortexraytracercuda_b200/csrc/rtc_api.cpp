@@ -124,16 +124,23 @@ PlanarPre planar_pre(V3 pos, V3 u, V3 v) {
     return p;
 }
 
-Aabb pad_box(Aabb b) {
-    // conservative padding so the FMA slab test never culls a primitive its exact test accepts
+// Conservative padding so the FMA slab test never culls a primitive its exact test accepts.  The slab
+// distance fma(lo, 1/d, -o/d) carries an absolute error of about 2^-24 |o| / |d| from the rounded o/d,
+// so a flat box (an axis-aligned quad or triangle: zero extent on one axis) near the world origin seen
+// from a far ray origin needs padding in proportion to the ray origin's magnitude, not to its own
+// coordinates.  `scene_scale` bounds |o| for every secondary ray (the largest coordinate of any
+// primitive) and for primary rays from the scene's camera; 2^-21 of it covers origins up to about
+// four times farther out.
+Aabb pad_box(Aabb b, float scene_scale) {
     for (int k = 0; k < 3; ++k) {
         float m = std::max(std::fabs(b.lo[k]), std::fabs(b.hi[k]));
-        float e = 1e-5f * m + 1e-6f + 1e-5f * (b.hi[k] - b.lo[k]);
+        float e = 1e-5f * m + 1e-6f + 1e-5f * (b.hi[k] - b.lo[k]) + 0x1p-21f * scene_scale;
         b.lo[k] -= e;
         b.hi[k] += e;
     }
     return b;
 }
+// Unpadded bounds of n points (pad_box follows once the scene's scale is known).
 Aabb box_of(const V3* pts, int n) {
     Aabb b;
     for (int k = 0; k < 3; ++k) { b.lo[k] = INFINITY; b.hi[k] = -INFINITY; }
@@ -141,7 +148,7 @@ Aabb box_of(const V3* pts, int n) {
         const float c[3] = {pts[i].x, pts[i].y, pts[i].z};
         for (int k = 0; k < 3; ++k) { b.lo[k] = std::min(b.lo[k], c[k]); b.hi[k] = std::max(b.hi[k], c[k]); }
     }
-    return pad_box(b);
+    return b;
 }
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -182,8 +189,10 @@ DevScene rtc_scene_view(const rtc_scene* s, const rtc_render_params* p) {
 }
 DevParams rtc_dev_params(const rtc_render_params* p);
 
-rtc_status rtc_build_host_scene(const rtc_scene_desc* d, HostScene& H) {
+rtc_status rtc_build_host_scene(const rtc_scene_desc* d, HostScene& H, uint32_t bvh_builder, int device) {
     if (!d) return fail(RTC_ERR_INVALID_ARGUMENT, "null argument");
+    if (bvh_builder != RTC_BVH_SAH && bvh_builder != RTC_BVH_DEVICE)
+        return fail(RTC_ERR_INVALID_ARGUMENT, "unknown BVH builder");
     auto t0 = std::chrono::steady_clock::now();
     // ---- validation --------------------------------------------------------------------------
     auto bad = [&](const std::string& m) { return fail(RTC_ERR_BAD_SCENE, m); };
@@ -287,10 +296,25 @@ rtc_status rtc_build_host_scene(const rtc_scene_desc* d, HostScene& H) {
         }
     }
 
+    {
+        float scale = 0.0f;
+        for (int k = 0; k < 3; ++k) scale = std::max(scale, std::fabs(d->camera.look_from[k]));
+        for (const Aabb& b : bin.boxes)
+            for (int k = 0; k < 3; ++k) scale = std::max(scale, std::max(std::fabs(b.lo[k]), std::fabs(b.hi[k])));
+        for (Aabb& b : bin.boxes) b = pad_box(b, scale);
+    }
+
     // ---- BVH -----------------------------------------------------------------------------------
     BvhOutput bvh;
     const char* berr = nullptr;
-    if (!build_bvh(bin, 4, 0, bvh, &berr)) return bad(berr ? berr : "BVH build failed");
+    uint32_t builder = RTC_BVH_SAH;
+    if (bvh_builder == RTC_BVH_DEVICE) {
+        const int rc = build_bvh_device(bin, device, bvh, &berr);
+        if (rc == BVH_DEVICE_ERROR) return fail(RTC_ERR_CUDA, std::string("device BVH build: ") + (berr ? berr : "failed"));
+        if (rc == BVH_DEVICE_OK) builder = RTC_BVH_DEVICE;
+        berr = nullptr;
+    }
+    if (builder == RTC_BVH_SAH && !build_bvh(bin, 4, 0, bvh, &berr)) return bad(berr ? berr : "BVH build failed");
     auto t1 = std::chrono::steady_clock::now();
 
     // ---- materials / textures (directional lights get their own diffuse_light + solid texture) --
@@ -478,6 +502,7 @@ rtc_status rtc_build_host_scene(const rtc_scene_desc* d, HostScene& H) {
     H.info.max_leaf_size = bvh.max_leaf_seen;
     H.info.device_bytes = total;
     H.info.build_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    H.info.bvh_builder = builder;
     return RTC_OK;
 }
 
@@ -496,10 +521,17 @@ DevScene rtc_rebase_scene(const HostScene& H, uint8_t* base) {
 }
 
 extern "C" rtc_status rtc_scene_create(rtc_context* ctx, const rtc_scene_desc* d, rtc_scene** out) {
+    return rtc_scene_create_ex(ctx, d, nullptr, out);
+}
+
+extern "C" rtc_status rtc_scene_create_ex(rtc_context* ctx, const rtc_scene_desc* d, const rtc_scene_options* opt,
+                                          rtc_scene** out) {
     if (!ctx || !d || !out) return fail(RTC_ERR_INVALID_ARGUMENT, "null argument");
     *out = nullptr;
+    if (opt && (opt->reserved[0] || opt->reserved[1] || opt->reserved[2]))
+        return fail(RTC_ERR_INVALID_ARGUMENT, "reserved scene options must be zero");
     HostScene H;
-    rtc_status r = rtc_build_host_scene(d, H);
+    rtc_status r = rtc_build_host_scene(d, H, opt ? opt->bvh_builder : RTC_BVH_SAH, ctx->device);
     if (r != RTC_OK) return r;
     rtc_scene* s = new (std::nothrow) rtc_scene();
     if (!s) return fail(RTC_ERR_OOM, "host allocation failed");

@@ -65,6 +65,7 @@ struct HostScene {
 };
 // Validates and flattens a scene description, building its BVH (the work of rtc_scene_create before
 // the upload).
-rtc_status rtc_build_host_scene(const rtc_scene_desc* d, HostScene& out);
+// `bvh_builder` is an RTC_BVH_* value; RTC_BVH_DEVICE builds on CUDA device `device`.
+rtc_status rtc_build_host_scene(const rtc_scene_desc* d, HostScene& out, uint32_t bvh_builder = 0, int device = 0);
 // The DevScene of a host scene whose slab was copied to `base`.
 rtc::DevScene rtc_rebase_scene(const HostScene& h, uint8_t* base);

@@ -354,6 +354,8 @@ extern "C" rtc_status rtc_server_create(const rtc_server_config* cfg, rtc_server
     int n = 0;
     if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) return rtc_set_error(RTC_ERR_NO_DEVICE, "no CUDA device available");
     if (cfg->device < 0 || cfg->device >= n) return rtc_set_error(RTC_ERR_INVALID_ARGUMENT, "device index out of range");
+    if (cfg->bvh_builder != RTC_BVH_SAH && cfg->bvh_builder != RTC_BVH_DEVICE)
+        return rtc_set_error(RTC_ERR_INVALID_ARGUMENT, "unknown BVH builder");
     cudaDeviceProp prop;
     if (cudaGetDeviceProperties(&prop, cfg->device) != cudaSuccess) return rtc_set_error(RTC_ERR_CUDA, "cudaGetDeviceProperties");
     if (prop.major < 10) return rtc_set_error(RTC_ERR_NO_DEVICE, (std::string("device is not sm_100: ") + prop.name).c_str());
@@ -431,7 +433,7 @@ extern "C" rtc_status rtc_server_add_scene(rtc_server* s, const rtc_scene_desc* 
     if (!s || !desc || !scene_id) return rtc_set_error(RTC_ERR_INVALID_ARGUMENT, "null argument");
     std::unique_ptr<SceneEntry> e(new (std::nothrow) SceneEntry());
     if (!e) return rtc_set_error(RTC_ERR_OOM, "host allocation failed");
-    rtc_status r = rtc_build_host_scene(desc, e->host);   // outside the lock: host BVH build
+    rtc_status r = rtc_build_host_scene(desc, e->host, s->cfg.bvh_builder, s->cfg.device);   // outside the lock
     if (r != RTC_OK) return r;
     std::lock_guard<std::mutex> lk(s->mu);
     *scene_id = (uint32_t)s->scenes.size();

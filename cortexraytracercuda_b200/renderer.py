@@ -23,7 +23,7 @@ import numpy as np
 from . import _lib
 from ._lib import RtcError, check
 from .scene import (MODE_COMPAT, DRAW_ORDER_DEVICE, REQ_DONE, REQ_FAILED, Camera, RenderParams, Scene, SceneDesc,
-                    rtc_batch_params, rtc_job, rtc_render_stats, rtc_request, rtc_request_info, rtc_scene_info,
+                    rtc_batch_params, rtc_job, rtc_render_stats, rtc_request, rtc_request_info, rtc_scene_info, rtc_scene_options,
                     rtc_server_config, rtc_server_stats)
 
 
@@ -84,15 +84,17 @@ class Context:
 
 
 class DeviceScene:
-    """A flattened scene resident on the device (rtc_scene): SAH BVH, primitives, textures."""
+    """A flattened scene resident on the device (rtc_scene): BVH, primitives, textures.  `bvh_builder`:
+    BVH_SAH (host binned SAH, default) or BVH_DEVICE (linear BVH built on the device)."""
 
-    def __init__(self, ctx: Context, scene: Scene):
+    def __init__(self, ctx: Context, scene: Scene, bvh_builder: int = 0):
         self.ctx = ctx
         self.desc = SceneDesc(scene)
         h = C.c_void_p()
         if not ctx.handle:
             raise RtcError(1, "context is closed")
-        check(ctx.lib.rtc_scene_create(ctx.handle, self.desc.ptr(), C.byref(h)))
+        opt = rtc_scene_options(bvh_builder)
+        check(ctx.lib.rtc_scene_create_ex(ctx.handle, self.desc.ptr(), C.byref(opt), C.byref(h)))
         self.handle = h
         ctx._scenes.add(self)
 
@@ -166,9 +168,10 @@ class RenderServer:
     when complete.  Scenes are registered once and kept resident under an HBM budget (LRU eviction)."""
 
     def __init__(self, device: int = 0, mode: int = MODE_COMPAT, draw_order: int = DRAW_ORDER_DEVICE,
-                 slots: int = 0, ring: int = 0, batch: int = 0, hbm_budget_bytes: int = 0, flags: int = 0):
+                 slots: int = 0, ring: int = 0, batch: int = 0, hbm_budget_bytes: int = 0, flags: int = 0,
+                 bvh_builder: int = 0):
         self.lib = _lib.load()
-        cfg = rtc_server_config(device, mode, draw_order, batch, slots, ring, hbm_budget_bytes, flags)
+        cfg = rtc_server_config(device, mode, draw_order, batch, slots, ring, hbm_budget_bytes, flags, bvh_builder)
         h = C.c_void_p()
         check(self.lib.rtc_server_create(C.byref(cfg), C.byref(h)))
         self.handle = h

@@ -25,6 +25,8 @@ ENGINE_AUTO, ENGINE_MEGAKERNEL, ENGINE_WAVEFRONT = 0, 1, 2
 FLAG_KERNEL_TIMING = 1
 FLAG_WIDE_BVH = 2
 FLAG_SAMPLE_GROUPS = 4
+BVH_SAH = 0        # binned SAH on host threads (default)
+BVH_DEVICE = 1     # linear BVH (Morton codes + radix sort) built on the device
 DRAW_ORDER_DEVICE, DRAW_ORDER_HOST = 0, 1
 
 F3 = C.c_float * 3
@@ -99,7 +101,12 @@ class rtc_render_stats(C.Structure):
 
 class rtc_scene_info(C.Structure):
     _fields_ = [("num_primitives", C.c_uint32), ("num_lights", C.c_uint32), ("num_nodes", C.c_uint32),
-                ("max_leaf_size", C.c_uint32), ("device_bytes", C.c_uint64), ("build_ms", C.c_double)]
+                ("max_leaf_size", C.c_uint32), ("device_bytes", C.c_uint64), ("build_ms", C.c_double),
+                ("bvh_builder", C.c_uint32)]
+
+
+class rtc_scene_options(C.Structure):
+    _fields_ = [("bvh_builder", C.c_uint32), ("reserved", C.c_uint32 * 3)]
 
 
 class rtc_obj_mesh(C.Structure):
@@ -120,7 +127,7 @@ class rtc_batch_params(C.Structure):
 class rtc_server_config(C.Structure):
     _fields_ = [("device", C.c_int32), ("mode", C.c_int32), ("draw_order", C.c_int32), ("batch", C.c_int32),
                 ("slots", C.c_uint32), ("ring", C.c_uint32), ("hbm_budget_bytes", C.c_uint64),
-                ("flags", C.c_int32)]
+                ("flags", C.c_int32), ("bvh_builder", C.c_uint32)]
 
 
 class rtc_request(C.Structure):

@@ -272,13 +272,31 @@ rtc_status rtc_context_destroy(rtc_context* ctx);
 rtc_status rtc_scene_create(rtc_context* ctx, const rtc_scene_desc* desc, rtc_scene** out);
 rtc_status rtc_scene_destroy(rtc_scene* scene);
 
+/* BVH builders.  The reference builds its tree on one device thread (random axis, exchange sort of the
+ * span, bvh_node.cuh:63-108 via gpu.cu:749); it has no choice of builder, so rtc_scene_create_ex and
+ * the option below have no reference counterpart. */
+#define RTC_BVH_SAH 0      /* binned SAH on host threads, leaves of up to 4 items, 4-wide copy (default) */
+#define RTC_BVH_DEVICE 1   /* linear BVH on the device: 30-bit Morton codes of the primitive centroids,
+                              radix sort, one primitive per leaf; milliseconds for a million triangles,
+                              more node visits per ray than SAH.  No 4-wide copy (RTC_FLAG_WIDE_BVH
+                              renders use the binary nodes).  Falls back to RTC_BVH_SAH for a single
+                              primitive or a tree deeper than the traversal stack. */
+typedef struct rtc_scene_options {
+    uint32_t bvh_builder;      /* RTC_BVH_*                                                          */
+    uint32_t reserved[3];      /* zero                                                               */
+} rtc_scene_options;
+/* rtc_scene_create with options (NULL options: rtc_scene_create). */
+rtc_status rtc_scene_create_ex(rtc_context* ctx, const rtc_scene_desc* desc, const rtc_scene_options* options,
+                               rtc_scene** out);
+
 typedef struct rtc_scene_info {
     uint32_t num_primitives;   /* lights + spheres + quads + triangles                             */
     uint32_t num_lights;
     uint32_t num_nodes;        /* BVH2 nodes                                                        */
     uint32_t max_leaf_size;
     uint64_t device_bytes;     /* bytes resident on the device for this scene                      */
-    double build_ms;           /* host BVH build time                                               */
+    double build_ms;           /* validation, flattening and BVH build time (host wall clock)        */
+    uint32_t bvh_builder;      /* RTC_BVH_* that built the tree                                      */
 } rtc_scene_info;
 rtc_status rtc_scene_get_info(const rtc_scene* scene, rtc_scene_info* info);
 
@@ -401,6 +419,7 @@ typedef struct rtc_server_config {
     uint64_t hbm_budget_bytes;   /* device bytes for slots, resident scenes and request outputs;
                                     0: 120 GB                                                           */
     int32_t flags;               /* RTC_FLAG_* applied to every request (e.g. RTC_FLAG_SAMPLE_GROUPS)    */
+    uint32_t bvh_builder;        /* RTC_BVH_* for rtc_server_add_scene                                  */
 } rtc_server_config;
 
 typedef struct rtc_request {
