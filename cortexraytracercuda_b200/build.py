@@ -74,12 +74,13 @@ def _run(cmd, verbose):
 def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = False, defines=(), out: Path | None = None,
           objdir: Path | None = None) -> Path:
     """Compiles every translation unit (in parallel) and links the library.  `defines` (NAME=VALUE)
-    are passed to the CUDA compiles; with `out`/`objdir` a variant library is built elsewhere."""
+    are passed to every compile; with `out`/`objdir` a variant library is built elsewhere."""
     if not os.path.exists(NVCC):
         raise RuntimeError(f"nvcc not found at {NVCC}")
     build_dir = Path(objdir) if objdir else BUILD
     lib = Path(out) if out else LIB
     build_dir.mkdir(parents=True, exist_ok=True)
+    lib.parent.mkdir(parents=True, exist_ok=True)
     dflags = [f"-D{d}" for d in defines]
     headers = [CSRC / h for h in HEADERS] + [INCLUDE / "rtc.h"]
     objs = []
@@ -93,7 +94,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
         if comp == "nvcc":
             cmd = [NVCC] + NVCC_COMMON + extra + dflags + (["-Xptxas", "-v"] if ptxas_verbose else []) + ["-c", str(s), "-o", str(o)]
         else:
-            cmd = [CXX] + CXX_FLAGS + extra + ["-c", str(s), "-o", str(o)]
+            cmd = [CXX] + CXX_FLAGS + extra + dflags + ["-c", str(s), "-o", str(o)]
         cmds.append(cmd)
     # independent translation units compile in parallel
     workers = max(1, min(len(cmds), os.cpu_count() or 1))
@@ -113,7 +114,7 @@ def main():
     ap.add_argument("--force", action="store_true")
     ap.add_argument("--verbose", action="store_true")
     ap.add_argument("--ptxas", action="store_true", help="print -Xptxas -v register/spill report")
-    ap.add_argument("--define", action="append", default=[], help="NAME=VALUE for the CUDA compiles")
+    ap.add_argument("--define", action="append", default=[], help="NAME=VALUE for every compile (CUDA and host)")
     ap.add_argument("--out", default=None, help="library path (a variant build)")
     ap.add_argument("--objdir", default=None, help="object directory (a variant build)")
     a = ap.parse_args()
