@@ -14,7 +14,7 @@ value  = Mpaths/s of the whole job (all ranks; weak scaling, one replica frame p
          from CUDA events on the launching stream, L2 flushed (256 MiB write) between steps.
 e2e    = the same metric through the public C ABI with host buffers: per step rtc_scene_create
          (flatten + BVH build + H2D upload) + rtc_render (kernel + D2H of the FP32 radiance) + destroy.
-         The BVH is the host SAH build unless --builder device (linear BVH built on the GPU).
+         The BVH is the host SAH build unless --builder device|lbvh (PLOC or linear BVH built on the GPU).
 roofline: algorithmic bytes of the render kernel per launch (BVH node visits x 64 B + primitive tests x
          their record size + per-ray state), counted by an instrumented launch of the same frame, divided
          by the mean event time of the timed launches, against the measured HBM copy bandwidth.
@@ -52,7 +52,7 @@ sys.path.insert(0, str(ROOT))
 from cortexraytracercuda_b200 import configs  # noqa: E402
 from cortexraytracercuda_b200.scene import (DRAW_ORDER_DEVICE, DRAW_ORDER_HOST, ENGINE_MEGAKERNEL,  # noqa: E402
                                             ENGINE_WAVEFRONT, FLAG_KERNEL_TIMING, FLAG_SAMPLE_GROUPS,
-                                            FLAG_WIDE_BVH, MODE_CLEAN, MODE_COMPAT, BVH_DEVICE, BVH_SAH)
+                                            FLAG_WIDE_BVH, MODE_CLEAN, MODE_COMPAT, BVH_DEVICE, BVH_DEVICE_LBVH, BVH_SAH)
 
 METRIC = "Mpaths/s"
 PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
@@ -550,8 +550,8 @@ def main():
     ap.add_argument("--mode", default="compat", choices=["compat", "clean"])
     ap.add_argument("--engine", default="wavefront", choices=["wavefront", "megakernel"])
     ap.add_argument("--bvh", default="2", choices=["2", "4"], help="BVH node layout (binary or 4-wide)")
-    ap.add_argument("--builder", default="sah", choices=["sah", "device"],
-                    help="BVH builder: host binned SAH or the device linear BVH (Morton codes)")
+    ap.add_argument("--builder", default="sah", choices=["sah", "device", "lbvh"],
+                    help="BVH builder: host binned SAH, device PLOC, or device linear BVH")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-baseline-s", type=float, default=12.0)
     ap.add_argument("--ref-step-s", type=float, default=8.0)
@@ -609,7 +609,7 @@ def main():
     params.engine = ENGINE_WAVEFRONT if args.engine == "wavefront" else ENGINE_MEGAKERNEL
     if args.bvh == "4":
         params.flags |= FLAG_WIDE_BVH
-    builder = BVH_DEVICE if args.builder == "device" else BVH_SAH
+    builder = {"sah": BVH_SAH, "device": BVH_DEVICE, "lbvh": BVH_DEVICE_LBVH}[args.builder]
     ds = DeviceScene(ctx, scene, builder)
     info = ds.info()
     W, H = params.width, params.height
@@ -727,7 +727,8 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {**describe(args.config, params, scene), "parallelism": f"replicas x{world}",
                        "bvh_nodes": info["num_nodes"], "bvh_layout": "binary" if args.bvh == "2" else "4-wide",
-                       "bvh_builder": "device LBVH" if info["bvh_builder"] == BVH_DEVICE else "host SAH",
+                       "bvh_builder": {BVH_SAH: "host SAH", BVH_DEVICE: "device PLOC",
+                                       BVH_DEVICE_LBVH: "device LBVH"}[info["bvh_builder"]],
                        "scene_build_ms": round(info["build_ms"], 1)},
             "mrays_per_s": round(mrays, 3),
             "gpu_launches": int(sum(st["launches"] for st in kstats)) if wavefront else args.steps,

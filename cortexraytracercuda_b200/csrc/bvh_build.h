@@ -35,9 +35,11 @@ struct BvhOutput {
 // Returns false (with a message) if the tree would not fit the traversal stack or the item encoding.
 bool build_bvh(const BvhInput& in, int max_leaf, int threads, BvhOutput& out, const char** err);
 
-// Linear BVH built on CUDA device `device` (bvh_device.cu): Morton-ordered, one primitive per leaf, no
-// 4-wide nodes.  BVH_DEVICE_TOO_DEEP and BVH_DEVICE_UNSUPPORTED leave the SAH build as the way out.
+// BVH built on CUDA device `device` (bvh_device.cu) over Morton-sorted primitives, one primitive per
+// leaf, no 4-wide nodes: PLOC clustering (BVH_DEVICE_PLOC) or the linear BVH (BVH_DEVICE_LBVH).
+// BVH_DEVICE_TOO_DEEP and BVH_DEVICE_UNSUPPORTED leave the SAH build as the way out.
 enum BvhDeviceStatus { BVH_DEVICE_OK = 0, BVH_DEVICE_TOO_DEEP = 1, BVH_DEVICE_UNSUPPORTED = 2, BVH_DEVICE_ERROR = 3 };
-int build_bvh_device(const BvhInput& in, int device, BvhOutput& out, const char** err);
+enum BvhDeviceMethod { BVH_DEVICE_PLOC = 0, BVH_DEVICE_LBVH = 1 };
+int build_bvh_device(const BvhInput& in, int device, BvhDeviceMethod method, BvhOutput& out, const char** err);
 
 }  // namespace rtc

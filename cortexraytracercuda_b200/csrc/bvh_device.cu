@@ -15,7 +15,18 @@
 // Every leaf holds one primitive; the leaf order is the sorted order.  Quality is below the SAH
 // build's (more node visits per ray); the build is a few milliseconds where the host build of a
 // million triangles takes a second.
+//
+// The default device method replaces steps 3-4 with PLOC (Meister and Bittner, "Parallel Locally-Ordered
+// Clustering for Bounding Volume Hierarchy Construction", IEEE TVCG 2018): starting from the sorted
+// primitives as clusters, each round finds every cluster's nearest neighbour among the PLOC_RADIUS
+// clusters on either side (the one whose union box has the smallest surface area, the smaller position
+// on a tie), merges mutual nearest neighbours into a new node, and compacts the survivors in order.
+// Merging by the surface-area distance gives trees close to a SAH build's.  Node indices count down from
+// the round's cluster count, so the last merge - the root - is node 0, and the numbering is
+// deterministic (a prefix sum orders each round's merges).
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
+#include <cub/device/device_select.cuh>
 
 #include <algorithm>
 #include <cfloat>
@@ -173,14 +184,192 @@ __global__ void k_bottom_up(const Aabb* __restrict__ boxes, const uint32_t* __re
     atomicOr(error, 4u);
 }
 
+// ---- PLOC ---------------------------------------------------------------------------------------
+constexpr int PLOC_RADIUS = 16;
+constexpr int PLOC_BLOCK = 256;
+constexpr int PLOC_MAX_ROUNDS = 512;
+
+struct Cluster {
+    Aabb box;
+    int32_t id;   // >= 0 inner node, < 0 leaf in the node layout's encoding
+};
+
+__device__ __forceinline__ Aabb unite(const Aabb& a, const Aabb& b) {
+    Aabb u;
+    for (int k = 0; k < 3; ++k) {
+        u.lo[k] = fminf(a.lo[k], b.lo[k]);
+        u.hi[k] = fmaxf(a.hi[k], b.hi[k]);
+    }
+    return u;
+}
+__device__ __forceinline__ float half_area(const Aabb& b) {
+    const float x = b.hi[0] - b.lo[0], y = b.hi[1] - b.lo[1], z = b.hi[2] - b.lo[2];
+    return x * y + y * z + z * x;
+}
+
+__global__ void k_ploc_init(const Aabb* __restrict__ boxes, const uint32_t* __restrict__ vals, uint32_t n,
+                            Cluster* __restrict__ c) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    c[i].box = boxes[vals[i]];
+    c[i].id = (int32_t)~((i << LEAF_COUNT_BITS) | 1u);
+}
+
+// nn[i] = the position j != i, |i - j| <= PLOC_RADIUS, whose union with cluster i has the smallest area.
+// blockDim.x == PLOC_BLOCK; the block's clusters and their neighbours are staged in shared memory.
+__global__ void __launch_bounds__(PLOC_BLOCK) k_ploc_nn(const Cluster* __restrict__ c, uint32_t m,
+                                                        uint32_t* __restrict__ nn) {
+    __shared__ Aabb sb[PLOC_BLOCK + 2 * PLOC_RADIUS];
+    const int64_t start = (int64_t)blockIdx.x * PLOC_BLOCK - PLOC_RADIUS;
+    for (int t = threadIdx.x; t < PLOC_BLOCK + 2 * PLOC_RADIUS; t += blockDim.x) {
+        const int64_t g = start + t;
+        if (g >= 0 && g < (int64_t)m) sb[t] = c[g].box;
+    }
+    __syncthreads();
+    const int64_t i = (int64_t)blockIdx.x * PLOC_BLOCK + threadIdx.x;
+    if (i >= (int64_t)m) return;
+    const Aabb a = sb[threadIdx.x + PLOC_RADIUS];
+    // Candidates are ordered by (area, |i - j|, parity of min(i, j), min(i, j)).  The order is the same
+    // seen from either end of a pair, so the least pair of the round is always mutual (every round
+    // merges), and among equal areas adjacent pairs starting at even positions win: n identical boxes
+    // pair up as (0,1)(2,3)... and halve every round instead of merging one pair at a time.
+    float best = FLT_MAX;
+    int64_t bj = i;
+    int bdist = 1 << 30, bpar = 2;
+    for (int o = -PLOC_RADIUS; o <= PLOC_RADIUS; ++o) {
+        const int64_t j = i + o;
+        if (o == 0 || j < 0 || j >= (int64_t)m) continue;
+        const float d = half_area(unite(a, sb[threadIdx.x + PLOC_RADIUS + o]));
+        const int dist = o < 0 ? -o : o;
+        const int64_t lo = j < i ? j : i;
+        const int par = (int)(lo & 1);
+        const int64_t blo = bj < i ? bj : i;
+        if (d < best || (d == best && (dist < bdist || (dist == bdist && (par < bpar || (par == bpar && lo < blo)))))) {
+            best = d;
+            bj = j;
+            bdist = dist;
+            bpar = par;
+        }
+    }
+    nn[i] = (uint32_t)bj;
+}
+
+// keep[i]: the cluster survives the round (a merged pair survives at its lower position);
+// fresh[i]: position i creates a node this round.
+__global__ void k_ploc_flags(const uint32_t* __restrict__ nn, uint32_t m, uint32_t* __restrict__ keep,
+                             uint32_t* __restrict__ fresh) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    const uint32_t j = nn[i];
+    const bool mutual = j < m && j != i && nn[j] == i;
+    keep[i] = !(mutual && i > j);
+    fresh[i] = mutual && i < j;
+}
+
+// Writes the round's nodes (index m - 2 - rank) and the round's clusters before compaction.
+__global__ void k_ploc_merge(const Cluster* __restrict__ c, const uint32_t* __restrict__ nn,
+                             const uint32_t* __restrict__ fresh, const uint32_t* __restrict__ rank, uint32_t m,
+                             uint32_t n, Cluster* __restrict__ out, float4* __restrict__ nodes, uint32_t* error) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    if (!fresh[i]) {
+        out[i] = c[i];
+        return;
+    }
+    const uint32_t j = nn[i];
+    const int64_t idx = (int64_t)m - 2 - (int64_t)rank[i];
+    if (j >= m || idx < 0 || idx >= (int64_t)n - 1) {
+        atomicOr(error, 16u);
+        out[i] = c[i];
+        return;
+    }
+    const Cluster L = c[i], R = c[j];
+    float4* np = nodes + 4 * (size_t)idx;
+    np[0] = make_float4(L.box.lo[0], L.box.hi[0], L.box.lo[1], L.box.hi[1]);
+    np[1] = make_float4(R.box.lo[0], R.box.hi[0], R.box.lo[1], R.box.hi[1]);
+    np[2] = make_float4(L.box.lo[2], L.box.hi[2], R.box.lo[2], R.box.hi[2]);
+    np[3] = make_float4(__int_as_float(L.id), __int_as_float(R.id), 0.0f, 0.0f);
+    out[i].box = unite(L.box, R.box);
+    out[i].id = (int32_t)idx;
+}
+
+// Depth of the deepest leaf (root = 1, as the host build counts), walking the downloaded nodes; 0 if
+// the links do not form a tree over nodes [0, inner).
+uint32_t tree_depth(const std::vector<float>& nodes, uint32_t inner) {
+    std::vector<std::pair<int32_t, uint32_t>> stack{{0, 1u}};
+    uint32_t deepest = 0, visited = 0;
+    while (!stack.empty()) {
+        const auto [node, depth] = stack.back();
+        stack.pop_back();
+        if (node < 0 || (uint32_t)node >= inner || ++visited > inner) return 0;
+        for (int side = 0; side < 2; ++side) {
+            int32_t c;
+            std::memcpy(&c, &nodes[16 * (size_t)node + 12 + side], 4);
+            if (c < 0) deepest = std::max(deepest, depth + 1);
+            else stack.push_back({c, depth + 1});
+        }
+    }
+    return visited == inner ? deepest : 0;
+}
+
 template <class T>
 cudaError_t dalloc(T** p, size_t n, cudaStream_t st) {
     return cudaMallocAsync((void**)p, std::max<size_t>(n, 1) * sizeof(T), st);
 }
 
+// PLOC rounds on `st` until one cluster is left; the nodes go to `nodes` (n - 1 records, root 0).
+// `h_count` is page-locked host memory for the per-round cluster count.
+cudaError_t ploc(const Aabb* d_boxes, const uint32_t* vals, uint32_t n, float4* d_nodes, uint32_t* d_error,
+                 uint32_t* h_count, cudaStream_t st, const char** what) {
+    Cluster *cur = nullptr, *tmp = nullptr, *nxt = nullptr;
+    uint32_t *nn = nullptr, *keep = nullptr, *fresh = nullptr, *rank = nullptr, *nsel = nullptr;
+    void* temp = nullptr;
+    size_t scan_bytes = 0, sel_bytes = 0;
+    cudaError_t e = cudaSuccess;
+    do {
+        if ((e = dalloc(&cur, n, st)) || (e = dalloc(&tmp, n, st)) || (e = dalloc(&nxt, n, st)) ||
+            (e = dalloc(&nn, n, st)) || (e = dalloc(&keep, n, st)) || (e = dalloc(&fresh, n, st)) ||
+            (e = dalloc(&rank, n, st)) || (e = dalloc(&nsel, 1, st)))
+            break;
+        if ((e = cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, fresh, rank, (int)n, st))) break;
+        if ((e = cub::DeviceSelect::Flagged(nullptr, sel_bytes, tmp, keep, nxt, nsel, (int)n, st))) break;
+        if ((e = cudaMallocAsync(&temp, std::max<size_t>(std::max(scan_bytes, sel_bytes), 1), st))) break;
+        k_ploc_init<<<(n + 255) / 256, 256, 0, st>>>(d_boxes, vals, n, cur);
+        if ((e = cudaGetLastError())) break;
+        uint32_t m = n;
+        for (int round = 0; m > 1; ++round) {
+            if (round >= PLOC_MAX_ROUNDS) {
+                *what = "device BVH build did not converge";
+                break;
+            }
+            const unsigned g = (m + 255) / 256;
+            k_ploc_nn<<<(m + PLOC_BLOCK - 1) / PLOC_BLOCK, PLOC_BLOCK, 0, st>>>(cur, m, nn);
+            k_ploc_flags<<<g, 256, 0, st>>>(nn, m, keep, fresh);
+            size_t b = scan_bytes;
+            if ((e = cub::DeviceScan::ExclusiveSum(temp, b, fresh, rank, (int)m, st))) break;
+            k_ploc_merge<<<g, 256, 0, st>>>(cur, nn, fresh, rank, m, n, tmp, d_nodes, d_error);
+            if ((e = cudaGetLastError())) break;
+            b = sel_bytes;
+            if ((e = cub::DeviceSelect::Flagged(temp, b, tmp, keep, nxt, nsel, (int)m, st))) break;
+            if ((e = cudaMemcpyAsync(h_count, nsel, sizeof(uint32_t), cudaMemcpyDeviceToHost, st))) break;
+            if ((e = cudaStreamSynchronize(st))) break;
+            if (*h_count >= m || *h_count == 0) {   // every round merges at least the closest pair
+                *what = "device BVH build made no progress";
+                break;
+            }
+            m = *h_count;
+            std::swap(cur, nxt);
+        }
+    } while (false);
+    for (void* p : {(void*)cur, (void*)tmp, (void*)nxt, (void*)nn, (void*)keep, (void*)fresh, (void*)rank,
+                    (void*)nsel, temp})
+        if (p) cudaFreeAsync(p, st);
+    return e;
+}
+
 }  // namespace
 
-int build_bvh_device(const BvhInput& in, int device, BvhOutput& out, const char** err) {
+int build_bvh_device(const BvhInput& in, int device, BvhDeviceMethod method, BvhOutput& out, const char** err) {
     const size_t n = in.boxes.size();
     if (n < 2 || n >= (1u << 26)) {
         if (err) *err = "device BVH build needs 2 .. 2^26-1 primitives";
@@ -240,14 +429,20 @@ int build_bvh_device(const BvhInput& in, int device, BvhOutput& out, const char*
         if ((e = cub::DeviceRadixSort::SortPairs(d_temp, temp_bytes, K, V, (int)n, 0, 30, st))) break;
         const uint32_t* keys = K.Current();
         const uint32_t* vals = V.Current();
-        k_internal<<<grid, 256, 0, st>>>(keys, (uint32_t)n, d_child, d_pint, d_pleaf, d_info);
-        if ((e = cudaGetLastError())) break;
-        k_bottom_up<<<grid, 256, 0, st>>>(d_boxes, vals, (uint32_t)n, d_child, d_pint, d_pleaf, d_flags, d_nbox,
-                                          d_nodes, d_info + 1, d_info);
-        if ((e = cudaGetLastError())) break;
+        if (method == BVH_DEVICE_LBVH) {
+            k_internal<<<grid, 256, 0, st>>>(keys, (uint32_t)n, d_child, d_pint, d_pleaf, d_info);
+            if ((e = cudaGetLastError())) break;
+            k_bottom_up<<<grid, 256, 0, st>>>(d_boxes, vals, (uint32_t)n, d_child, d_pint, d_pleaf, d_flags, d_nbox,
+                                              d_nodes, d_info + 1, d_info);
+            if ((e = cudaGetLastError())) break;
+        } else {
+            e = ploc(d_boxes, vals, (uint32_t)n, d_nodes, d_info, h_info + 2, st, &what);
+            if (e == cudaSuccess && what) rc = BVH_DEVICE_TOO_DEEP;   // no tree: the SAH build takes over
+            if (e != cudaSuccess || what) break;
+        }
         out.nodes.resize((n - 1) * 16);
         out.order.resize(n);
-        if ((e = cudaMemcpyAsync(h_info, d_info, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st))) break;
+        if ((e = cudaMemcpyAsync(h_info, d_info, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st))) break;
         if ((e = cudaMemcpyAsync(out.nodes.data(), d_nodes, (n - 1) * 16 * sizeof(float), cudaMemcpyDeviceToHost, st)))
             break;
         if ((e = cudaMemcpyAsync(out.order.data(), vals, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, st))) break;
@@ -257,7 +452,11 @@ int build_bvh_device(const BvhInput& in, int device, BvhOutput& out, const char*
             break;
         }
         out.num_nodes = (uint32_t)(n - 1);
-        out.max_depth = h_info[1];
+        out.max_depth = method == BVH_DEVICE_LBVH ? h_info[1] : tree_depth(out.nodes, (uint32_t)(n - 1));
+        if (out.max_depth == 0) {
+            what = "device BVH build produced an inconsistent tree";
+            break;
+        }
         out.max_leaf_seen = 1;
         out.nodes4.clear();
         out.num_nodes4 = 0;

@@ -191,7 +191,7 @@ DevParams rtc_dev_params(const rtc_render_params* p);
 
 rtc_status rtc_build_host_scene(const rtc_scene_desc* d, HostScene& H, uint32_t bvh_builder, int device) {
     if (!d) return fail(RTC_ERR_INVALID_ARGUMENT, "null argument");
-    if (bvh_builder != RTC_BVH_SAH && bvh_builder != RTC_BVH_DEVICE)
+    if (bvh_builder != RTC_BVH_SAH && bvh_builder != RTC_BVH_DEVICE && bvh_builder != RTC_BVH_DEVICE_LBVH)
         return fail(RTC_ERR_INVALID_ARGUMENT, "unknown BVH builder");
     auto t0 = std::chrono::steady_clock::now();
     // ---- validation --------------------------------------------------------------------------
@@ -308,10 +308,11 @@ rtc_status rtc_build_host_scene(const rtc_scene_desc* d, HostScene& H, uint32_t 
     BvhOutput bvh;
     const char* berr = nullptr;
     uint32_t builder = RTC_BVH_SAH;
-    if (bvh_builder == RTC_BVH_DEVICE) {
-        const int rc = build_bvh_device(bin, device, bvh, &berr);
+    if (bvh_builder != RTC_BVH_SAH) {
+        const int rc = build_bvh_device(bin, device, bvh_builder == RTC_BVH_DEVICE_LBVH ? BVH_DEVICE_LBVH : BVH_DEVICE_PLOC,
+                                        bvh, &berr);
         if (rc == BVH_DEVICE_ERROR) return fail(RTC_ERR_CUDA, std::string("device BVH build: ") + (berr ? berr : "failed"));
-        if (rc == BVH_DEVICE_OK) builder = RTC_BVH_DEVICE;
+        if (rc == BVH_DEVICE_OK) builder = bvh_builder;
         berr = nullptr;
     }
     if (builder == RTC_BVH_SAH && !build_bvh(bin, 4, 0, bvh, &berr)) return bad(berr ? berr : "BVH build failed");

@@ -354,7 +354,7 @@ extern "C" rtc_status rtc_server_create(const rtc_server_config* cfg, rtc_server
     int n = 0;
     if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) return rtc_set_error(RTC_ERR_NO_DEVICE, "no CUDA device available");
     if (cfg->device < 0 || cfg->device >= n) return rtc_set_error(RTC_ERR_INVALID_ARGUMENT, "device index out of range");
-    if (cfg->bvh_builder != RTC_BVH_SAH && cfg->bvh_builder != RTC_BVH_DEVICE)
+    if (cfg->bvh_builder != RTC_BVH_SAH && cfg->bvh_builder != RTC_BVH_DEVICE && cfg->bvh_builder != RTC_BVH_DEVICE_LBVH)
         return rtc_set_error(RTC_ERR_INVALID_ARGUMENT, "unknown BVH builder");
     cudaDeviceProp prop;
     if (cudaGetDeviceProperties(&prop, cfg->device) != cudaSuccess) return rtc_set_error(RTC_ERR_CUDA, "cudaGetDeviceProperties");

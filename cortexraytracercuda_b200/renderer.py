@@ -85,7 +85,8 @@ class Context:
 
 class DeviceScene:
     """A flattened scene resident on the device (rtc_scene): BVH, primitives, textures.  `bvh_builder`:
-    BVH_SAH (host binned SAH, default) or BVH_DEVICE (linear BVH built on the device)."""
+    BVH_SAH (host binned SAH, default), BVH_DEVICE (PLOC built on the device) or BVH_DEVICE_LBVH (linear
+    BVH built on the device)."""
 
     def __init__(self, ctx: Context, scene: Scene, bvh_builder: int = 0):
         self.ctx = ctx

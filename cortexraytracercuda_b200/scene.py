@@ -26,7 +26,8 @@ FLAG_KERNEL_TIMING = 1
 FLAG_WIDE_BVH = 2
 FLAG_SAMPLE_GROUPS = 4
 BVH_SAH = 0        # binned SAH on host threads (default)
-BVH_DEVICE = 1     # linear BVH (Morton codes + radix sort) built on the device
+BVH_DEVICE = 1     # built on the device: Morton sort + PLOC clustering (near-SAH quality)
+BVH_DEVICE_LBVH = 2   # built on the device: Morton sort + linear BVH (fastest build)
 DRAW_ORDER_DEVICE, DRAW_ORDER_HOST = 0, 1
 
 F3 = C.c_float * 3

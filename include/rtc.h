@@ -276,11 +276,15 @@ rtc_status rtc_scene_destroy(rtc_scene* scene);
  * span, bvh_node.cuh:63-108 via gpu.cu:749); it has no choice of builder, so rtc_scene_create_ex and
  * the option below have no reference counterpart. */
 #define RTC_BVH_SAH 0      /* binned SAH on host threads, leaves of up to 4 items, 4-wide copy (default) */
-#define RTC_BVH_DEVICE 1   /* linear BVH on the device: 30-bit Morton codes of the primitive centroids,
-                              radix sort, one primitive per leaf; milliseconds for a million triangles,
-                              more node visits per ray than SAH.  No 4-wide copy (RTC_FLAG_WIDE_BVH
-                              renders use the binary nodes).  Falls back to RTC_BVH_SAH for a single
-                              primitive or a tree deeper than the traversal stack. */
+#define RTC_BVH_DEVICE 1   /* built on the device: primitives sorted by the 30-bit Morton code of their
+                              centroids, then clustered bottom-up (PLOC: mutual nearest neighbours by
+                              union surface area within 16 positions); one primitive per leaf, tree
+                              quality close to SAH.  No 4-wide copy (RTC_FLAG_WIDE_BVH renders use the
+                              binary nodes).  Falls back to RTC_BVH_SAH for a single primitive or a tree
+                              deeper than the traversal stack. */
+#define RTC_BVH_DEVICE_LBVH 2   /* built on the device as a linear BVH over the same sorted codes
+                                   (Karras 2012): the fastest build, more node visits per ray.  Same
+                                   limits and fallback as RTC_BVH_DEVICE. */
 typedef struct rtc_scene_options {
     uint32_t bvh_builder;      /* RTC_BVH_*                                                          */
     uint32_t reserved[3];      /* zero                                                               */
