@@ -269,15 +269,14 @@ def run_batched(args, rank, world, local):
     tuned = None
     if args.autotune:
         from cortexraytracercuda_b200 import autotune
-        tuned = autotune.autotune_batch(ctx, jobs, space={"slots": [1 << 20, 1 << 21, 1 << 22], "batch": [12]},
-                                        repeats=1, stream=sp)
+        tuned = autotune.autotune_batch(ctx, jobs, repeats=1, stream=sp)
         jobs = autotune.with_layout(jobs, tuned.layout)
         args.slots, args.drain = tuned.slots, tuned.drain
         torch.cuda.synchronize()
 
     def batched():
         ctx.render_batch(jobs, slots=args.slots, drain=args.drain, stream=sp,
-                         batch=tuned.batch if tuned else 0)
+                         batch=tuned.batch if tuned else 0, block=tuned.block if tuned else 0)
 
     def plain():
         for ds, p, o in zip(dss, params, plain_outs):
@@ -385,7 +384,8 @@ def run_batched(args, rank, world, local):
             "setup_s": round(setup_s, 2), "clocks": clk, "roofline": None, "cpu_baseline": None}
     if tuned:
         line["autotune"] = {"chosen": {"slots": tuned.slots, "batch": tuned.batch, "drain": tuned.drain,
-                                       "layout": tuned.layout},
+                                       "layout": tuned.layout, "block": tuned.block},
+                            "search": "coordinate descent",
                             "candidates_ms": [[c, round(ms, 1)] for c, ms in tuned.table]}
     if rank == 0:
         print(json.dumps(line), flush=True)

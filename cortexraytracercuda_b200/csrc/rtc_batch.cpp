@@ -79,6 +79,9 @@ extern "C" rtc_status rtc_render_batch(rtc_context* c, const rtc_job* jobs, uint
     cfg.batch = bp && bp->batch > 0 ? bp->batch : 12;
     cfg.drain = bp ? bp->drain : 0u;
     cfg.wide = (jobs[0].params.flags & RTC_FLAG_WIDE_BVH) != 0;
+    cfg.block = bp && bp->block ? (int)bp->block : 128;
+    if (cfg.block != 128 && cfg.block != 256 && cfg.block != 512)
+        return rtc_set_error(RTC_ERR_INVALID_ARGUMENT, "block must be 128, 256 or 512");
     if (cfg.ring != next_pow2(cfg.ring)) return rtc_set_error(RTC_ERR_INVALID_ARGUMENT, "ring must be a power of two");
 
     std::lock_guard<std::mutex> lk(c->mu);
@@ -88,7 +91,7 @@ extern "C" rtc_status rtc_render_batch(rtc_context* c, const rtc_job* jobs, uint
     const EngineConfig* have = c->engine ? &c->engine->config() : nullptr;
     if (!have || have->slots != cfg.slots || have->ring != cfg.ring || have->mode != cfg.mode ||
         have->draw_order != cfg.draw_order || have->batch != cfg.batch || have->drain != cfg.drain ||
-        have->wide != cfg.wide) {
+        have->wide != cfg.wide || have->block != cfg.block) {
         c->engine.reset();
         std::unique_ptr<Engine> eng(new Engine());
         rtc_status r = eng->init(cfg, st);

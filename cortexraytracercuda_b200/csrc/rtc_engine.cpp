@@ -182,7 +182,8 @@ rtc_status Engine::enqueue_iterations() {
     L.status = d_status_;
     L.counters = counters_;
     L.wide = cfg_.wide;
-    L.grid = cfg_.num_sms * 8;
+    L.block = cfg_.block;
+    L.grid = cfg_.num_sms * 8 * 128 / cfg_.block;   // 1,024 threads per SM
     const bool use_graph = cfg_.graphs && st_ != nullptr && cfg_.batch % 6 == 0 && it_ % 6 == 0;
     if (use_graph && (!graph_ || graph_counters_ != counters_)) {
         drop_graph();

@@ -34,6 +34,7 @@ struct EngineConfig {
     uint32_t drain = 0;            // drain threshold in slots (0: 512 per SM)
     bool graphs = true;            // replay batches as a captured CUDA graph (batch a multiple of 6)
     bool wide = false;             // extend walks the 4-wide nodes (jobs asked for RTC_FLAG_WIDE_BVH)
+    int block = 128;               // threads per block of the extend and shade kernels (128, 256, 512)
 };
 
 // Host view of one admitted job.

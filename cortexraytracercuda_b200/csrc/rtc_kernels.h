@@ -32,6 +32,7 @@ struct WfLaunch {
     unsigned long long* counters;    // NULL: no instrumentation
     uint32_t* status;
     int grid;
+    int block;                       // EXTEND / SHADE / BOUNCE: threads per block (0: 128; at most 512)
     cudaStream_t st;
 };
 using WfOneFn = cudaError_t (*)(WfOp, const WfOneArgs&, const WfBuffers&, const WfLaunch&);

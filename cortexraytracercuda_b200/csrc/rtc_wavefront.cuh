@@ -21,19 +21,21 @@
 
 #include <type_traits>
 
-// Launch bounds of the two iteration kernels.  Build-time knobs for occupancy sweeps: RTC_EXTEND_MINB /
-// RTC_SHADE_MINB ask for that many resident blocks per SM (a register cap of 65536 / (128 x blocks)).
-// Without them the compiler's own choice stands, which measured best (extend 63 registers, shade 108);
-// note that an explicit minimum of 1 is not the same: it lets extend grow to 80 registers.
+// Launch bounds of the iteration kernels (extend, shade, fused bounce), which run with 128, 256 or 512
+// threads per block (WfLaunch::block, a batch autotuner knob).  Build-time knobs for occupancy sweeps:
+// RTC_EXTEND_MINB / RTC_SHADE_MINB ask for that many resident 512-thread blocks per SM (a register cap of
+// 65536 / (512 x blocks)).  Without them the compiler's own choice stands, which measured best (extend
+// 64 registers, shade 114); note that an explicit minimum of 1 is not the same as none.
+#define RTC_ITER_BLOCK_MAX 512
 #ifdef RTC_EXTEND_MINB
-#define RTC_EXTEND_BOUNDS __launch_bounds__(128, RTC_EXTEND_MINB)
+#define RTC_EXTEND_BOUNDS __launch_bounds__(RTC_ITER_BLOCK_MAX, RTC_EXTEND_MINB)
 #else
-#define RTC_EXTEND_BOUNDS __launch_bounds__(128)
+#define RTC_EXTEND_BOUNDS __launch_bounds__(RTC_ITER_BLOCK_MAX)
 #endif
 #ifdef RTC_SHADE_MINB
-#define RTC_SHADE_BOUNDS __launch_bounds__(128, RTC_SHADE_MINB)
+#define RTC_SHADE_BOUNDS __launch_bounds__(RTC_ITER_BLOCK_MAX, RTC_SHADE_MINB)
 #else
-#define RTC_SHADE_BOUNDS __launch_bounds__(128)
+#define RTC_SHADE_BOUNDS __launch_bounds__(RTC_ITER_BLOCK_MAX)
 #endif
 #ifdef RTC_FINISH_MINB
 #define RTC_FINISH_BOUNDS __launch_bounds__(128, RTC_FINISH_MINB)
@@ -436,7 +438,7 @@ __global__ void RTC_SHADE_BOUNDS wf_shade(J jobs, WfBuffers B, WfIter w, unsigne
 // Fused form of one iteration: trace + shade of every queued slot in one launch (each lane still does
 // exactly one bounce, so the warp stays in the same phase), then compaction into the next queue.
 template <bool CLEAN, int ORDER, bool COUNT, class J>
-__global__ void __launch_bounds__(128) wf_bounce(J jobs, WfBuffers B, WfIter w, unsigned long long* counters,
+__global__ void __launch_bounds__(RTC_ITER_BLOCK_MAX) wf_bounce(J jobs, WfBuffers B, WfIter w, unsigned long long* counters,
                                                  uint32_t* status_word) {
     const uint32_t n = B.ctr[w.cin];
     if (blockIdx.x == 0 && threadIdx.x == 0) B.ctr[w.czero] = 0u;   // appended to by the next iteration
@@ -590,6 +592,8 @@ cudaError_t wf_dispatch(WfOp op, const A& args, const WfBuffers& B, const WfLaun
     J jobs;
     static_cast<A&>(jobs) = args;
     const bool c = L.counters != nullptr;
+    const int blk = L.block > 0 ? L.block : 128;
+    if (blk > RTC_ITER_BLOCK_MAX || blk % 32 != 0) return cudaErrorInvalidValue;
     switch (op) {
     case WF_OP_INIT:
         if constexpr (std::is_same<J, WfOne>::value) wf_init<CLEAN, ORDER><<<L.grid, 128, 0, L.st>>>(jobs, B);
@@ -605,16 +609,16 @@ cudaError_t wf_dispatch(WfOp op, const A& args, const WfBuffers& B, const WfLaun
         break;
     case WF_OP_EXTEND:
         if (L.wide) {
-            if (c) wf_extend<true, FLAVOR, J, true><<<L.grid, 128, 0, L.st>>>(jobs, B, L.w, L.counters, L.status);
-            else wf_extend<false, FLAVOR, J, true><<<L.grid, 128, 0, L.st>>>(jobs, B, L.w, nullptr, L.status);
+            if (c) wf_extend<true, FLAVOR, J, true><<<L.grid, blk, 0, L.st>>>(jobs, B, L.w, L.counters, L.status);
+            else wf_extend<false, FLAVOR, J, true><<<L.grid, blk, 0, L.st>>>(jobs, B, L.w, nullptr, L.status);
         } else {
-            if (c) wf_extend<true, FLAVOR, J, false><<<L.grid, 128, 0, L.st>>>(jobs, B, L.w, L.counters, L.status);
-            else wf_extend<false, FLAVOR, J, false><<<L.grid, 128, 0, L.st>>>(jobs, B, L.w, nullptr, L.status);
+            if (c) wf_extend<true, FLAVOR, J, false><<<L.grid, blk, 0, L.st>>>(jobs, B, L.w, L.counters, L.status);
+            else wf_extend<false, FLAVOR, J, false><<<L.grid, blk, 0, L.st>>>(jobs, B, L.w, nullptr, L.status);
         }
         break;
     case WF_OP_SHADE:
-        if (c) wf_shade<CLEAN, ORDER, true><<<L.grid, 128, 0, L.st>>>(jobs, B, L.w, L.counters, L.status);
-        else wf_shade<CLEAN, ORDER, false><<<L.grid, 128, 0, L.st>>>(jobs, B, L.w, nullptr, L.status);
+        if (c) wf_shade<CLEAN, ORDER, true><<<L.grid, blk, 0, L.st>>>(jobs, B, L.w, L.counters, L.status);
+        else wf_shade<CLEAN, ORDER, false><<<L.grid, blk, 0, L.st>>>(jobs, B, L.w, nullptr, L.status);
         break;
     case WF_OP_FINISH:
         if (c) wf_finish<CLEAN, ORDER, true><<<L.grid, 128, 0, L.st>>>(jobs, B, L.w, L.counters, L.status);
@@ -624,8 +628,8 @@ cudaError_t wf_dispatch(WfOp op, const A& args, const WfBuffers& B, const WfLaun
         wf_split<CLEAN><<<L.grid, 128, 0, L.st>>>(jobs, B, L.w, L.k0, L.threshold);
         break;
     case WF_OP_BOUNCE:
-        if (c) wf_bounce<CLEAN, ORDER, true><<<L.grid, 128, 0, L.st>>>(jobs, B, L.w, L.counters, L.status);
-        else wf_bounce<CLEAN, ORDER, false><<<L.grid, 128, 0, L.st>>>(jobs, B, L.w, nullptr, L.status);
+        if (c) wf_bounce<CLEAN, ORDER, true><<<L.grid, blk, 0, L.st>>>(jobs, B, L.w, L.counters, L.status);
+        else wf_bounce<CLEAN, ORDER, false><<<L.grid, blk, 0, L.st>>>(jobs, B, L.w, nullptr, L.status);
         break;
     default:
         return cudaErrorInvalidValue;

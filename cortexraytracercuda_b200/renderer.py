@@ -60,7 +60,7 @@ class Context:
         return DeviceScene(self, scene)
 
     def render_batch(self, jobs, slots: int = 0, ring: int = 0, batch: int = 0, drain: int = 0,
-                     stream: int | None = None, d_counters: int | None = None) -> None:
+                     stream: int | None = None, d_counters: int | None = None, block: int = 0) -> None:
         """Renders many images through one wavefront (rtc_render_batch).  ``jobs`` are :class:`Job`s whose
         ``d_radiance`` device buffers receive each image's radiance sums; returns when all are complete."""
         arr = (rtc_job * max(1, len(jobs)))()
@@ -72,7 +72,7 @@ class Context:
                 cams.append(c)
                 cam = C.pointer(c)
             arr[k] = rtc_job(j.scene.handle.value, cam, j.params.to_c(), j.d_radiance)
-        bp = rtc_batch_params(slots, ring, batch, drain, d_counters)
+        bp = rtc_batch_params(slots, ring, batch, drain, d_counters, block)
         check(self.lib.rtc_render_batch(self.handle, arr, len(jobs), C.byref(bp),
                                         C.c_void_p(stream) if stream else None))
 

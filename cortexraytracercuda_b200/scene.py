@@ -122,7 +122,7 @@ class rtc_job(C.Structure):
 
 class rtc_batch_params(C.Structure):
     _fields_ = [("slots", C.c_uint32), ("ring", C.c_uint32), ("batch", C.c_int32), ("drain", C.c_uint32),
-                ("d_counters", C.c_void_p)]
+                ("d_counters", C.c_void_p), ("block", C.c_uint32)]
 
 
 class rtc_server_config(C.Structure):

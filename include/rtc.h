@@ -390,6 +390,8 @@ typedef struct rtc_batch_params {
     unsigned long long* d_counters;   /* NULL, or 8 device uint64 (zeroed by the caller) that receive the
                           counts of rtc_render_device: rays, paths, node visits, primitive tests, then the
                           extend kernel's own rays, node visits and primitive tests                      */
+    uint32_t block;    /* threads per block of the extend and shade kernels: 128, 256 or 512; 0: 128.
+                          The grid keeps 1,024 threads per SM.                                            */
 } rtc_batch_params;
 
 /* Renders `num_jobs` images on `stream` (a cudaStream_t, or NULL for the context's stream) and returns
