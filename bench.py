@@ -60,7 +60,7 @@ FALLBACK_HBM_GBS = 6650.0
 
 # bytes fetched per visit (ignoring caches) for the roofline's algorithmic traffic
 NODE_BYTES = 64          # BVH2 node: two child boxes + two child links (4 x float4)
-NODE4_BYTES = 128        # 4-wide node: four child boxes + four child links (8 x float4, one cache line)
+NODE8_BYTES = 96         # 8-wide node: header, quantised child boxes (8-bit), eight child links (6 x float4)
 PRIM_BYTES = {"spheres": 16, "cornell": 48, "meshes": 48}   # dominant primitive record of each workload
 STATE_BYTES = 32 + 16 + 2 * 48   # ray read + hit write + path state read/write per traversal
 EXTEND_STATE_BYTES = 4 + 32 + 4 + 8   # queue entry + ray (origin, direction) + depth word read, hit record write
@@ -253,7 +253,7 @@ def run_batched(args, rank, world, local):
         p.mode, p.draw_order, p.engine = mode, order, ENGINE_WAVEFRONT
         if args.groups:
             p.flags |= FLAG_SAMPLE_GROUPS
-        if args.bvh == "4":
+        if args.bvh == "8":
             p.flags |= FLAG_WIDE_BVH
         params.append(p)
     outs = [torch.empty((p.height, p.width, 4), dtype=torch.float32, device="cuda") for p in params]
@@ -549,7 +549,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--mode", default="compat", choices=["compat", "clean"])
     ap.add_argument("--engine", default="wavefront", choices=["wavefront", "megakernel"])
-    ap.add_argument("--bvh", default="2", choices=["2", "4"], help="BVH node layout (binary or 4-wide)")
+    ap.add_argument("--bvh", default="2", choices=["2", "8"], help="BVH node layout (binary or 8-wide quantised)")
     ap.add_argument("--builder", default="sah", choices=["sah", "device", "lbvh"],
                     help="BVH builder: host binned SAH, device PLOC, or device linear BVH")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -607,7 +607,7 @@ def main():
     if args.small:
         params.width, params.height, params.spp = params.width // 4, params.height // 4, 16
     params.engine = ENGINE_WAVEFRONT if args.engine == "wavefront" else ENGINE_MEGAKERNEL
-    if args.bvh == "4":
+    if args.bvh == "8":
         params.flags |= FLAG_WIDE_BVH
     builder = {"sah": BVH_SAH, "device": BVH_DEVICE, "lbvh": BVH_DEVICE_LBVH}[args.builder]
     ds = DeviceScene(ctx, scene, builder)
@@ -684,7 +684,7 @@ def main():
     # ---- roofline -------------------------------------------------------------------------------
     peak, peak_kind = hbm_peak()
     prim_b = PRIM_BYTES[args.config]
-    node_b = NODE_BYTES if args.bvh == "2" else NODE4_BYTES
+    node_b = NODE_BYTES if args.bvh == "2" else NODE8_BYTES
     if wavefront:
         # dominant kernel: wf_extend (closest-hit traversal of every queued ray).  Algorithmic bytes of
         # its launches in one frame, from its own counters, over its summed CUDA-event time.
@@ -726,7 +726,7 @@ def main():
             "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {**describe(args.config, params, scene), "parallelism": f"replicas x{world}",
-                       "bvh_nodes": info["num_nodes"], "bvh_layout": "binary" if args.bvh == "2" else "4-wide",
+                       "bvh_nodes": info["num_nodes"], "bvh_layout": "binary" if args.bvh == "2" else "8-wide quantised",
                        "bvh_builder": {BVH_SAH: "host SAH", BVH_DEVICE: "device PLOC",
                                        BVH_DEVICE_LBVH: "device LBVH"}[info["bvh_builder"]],
                        "scene_build_ms": round(info["build_ms"], 1)},

@@ -28,6 +28,7 @@ PROTOTYPES = {
     "rtc_context_create": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
     "rtc_context_destroy": (C.c_int, [_P]),
     "rtc_scene_create": (C.c_int, [_P, C.POINTER(rtc_scene_desc), C.POINTER(C.c_void_p)]),
+    "rtc_trace_closest_ex": (C.c_int, [_P, _P, _P, C.c_uint32, C.c_int32, C.c_int32, C.c_int32, _P, _P]),
     "rtc_scene_create_ex": (C.c_int, [_P, C.POINTER(rtc_scene_desc), C.POINTER(rtc_scene_options),
                                       C.POINTER(C.c_void_p)]),
     "rtc_scene_destroy": (C.c_int, [_P]),

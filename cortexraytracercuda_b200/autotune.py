@@ -6,7 +6,8 @@ Knobs (all of them change how the work is scheduled, none changes what a pixel c
   * batch   - (extend, shade) iterations between two host polls (multiples of 6 replay a CUDA graph);
   * drain   - queued slots below which the register-resident drain kernel finishes the batch
               (1: never drain);
-  * layout  - BVH node layout: the binary nodes (64 B) or the 4-wide nodes (128 B);
+  * layout  - BVH node layout: the binary nodes (64 B) or the 8-wide nodes with quantised child
+              boxes (96 B);
   * block   - threads per block of the extend and shade kernels (128, 256 or 512).
 
 Search: coordinate descent by default - each knob in turn is swept with the others held at the best

@@ -259,14 +259,18 @@ bool build_bvh(const BvhInput& in, int max_leaf, int threads, BvhOutput& out, co
     out.num_nodes = (uint32_t)(out.nodes.size() / 16);
     out.max_depth = max_depth;
 
-    // 4-wide collapse of the same tree.  A wide node starts with its binary node's two children and
-    // repeatedly opens the inner child of largest surface area in place (left child where it was,
-    // right child just after it), so children stay in left-to-right order and the leaves are met in
-    // exactly the binary flattening's order: both layouts share one leaf order (items array).
-    out.nodes4.clear();
-    auto alloc4 = [&]() {
-        out.nodes4.resize(out.nodes4.size() + 32, 0.0f);
-        return (int32_t)(out.nodes4.size() / 32 - 1);
+    // 8-wide collapse of the same tree, with quantised child boxes.  A wide node starts with its binary
+    // node's two children and repeatedly opens the inner child of largest surface area in place (left
+    // child where it was, right child just after it), so children stay in left-to-right order and the
+    // leaves are met in exactly the binary flattening's order: both layouts share one leaf order (items
+    // array).  Each node stores its box's low corner p, one power-of-two step 2^e per axis with
+    // 255 * 2^e >= the box's extent, and per child and axis an 8-bit low bound floor((lo - p) / 2^e)
+    // and high bound ceil((hi - p) / 2^e): p + q * 2^e encloses the child's box exactly (checked in
+    // double below), so the quantised test never loses a hit the binary nodes find.
+    out.nodes8.clear();
+    auto alloc8 = [&]() {
+        out.nodes8.resize(out.nodes8.size() + NODE8_FLOATS, 0.0f);
+        return (int32_t)(out.nodes8.size() / NODE8_FLOATS - 1);
     };
     std::vector<int32_t> leaf_enc;
     {
@@ -304,38 +308,64 @@ bool build_bvh(const BvhInput& in, int max_leaf, int threads, BvhOutput& out, co
             }
         }
     }
-    auto put4 = [&](int32_t slot, int c, const Aabb& bx, int32_t enc) {
-        float* f = &out.nodes4[32 * (size_t)slot];
-        f[0 + c] = bx.lo[0];
-        f[4 + c] = bx.hi[0];
-        f[8 + c] = bx.lo[1];
-        f[12 + c] = bx.hi[1];
-        f[16 + c] = bx.lo[2];
-        f[20 + c] = bx.hi[2];
-        std::memcpy(&f[24 + c], &enc, 4);
+    bool quant_ok = true;
+    // writes node `slot` from `n` children (binary node ids) and their links
+    auto put8 = [&](int32_t slot, const int32_t* ch, int n, const int32_t* link) {
+        float* f = &out.nodes8[NODE8_FLOATS * (size_t)slot];
+        Aabb nb;
+        for (int k = 0; k < 3; ++k) { nb.lo[k] = INFINITY; nb.hi[k] = -INFINITY; }
+        for (int i = 0; i < n; ++i) grow(nb, B.nodes[ch[i]].box);
+        uint32_t hdr = (uint32_t)n << 24;
+        uint8_t q[3][2][8] = {};   // axis, (low, high), child
+        for (int k = 0; k < 3; ++k) {
+            const double ext = (double)nb.hi[k] - (double)nb.lo[k];
+            int e = -126;
+            while (e < 127 && std::ldexp(255.0, e) < ext) ++e;
+            const double step = std::ldexp(1.0, e);
+            hdr |= (uint32_t)(e + 127) << (8 * k);
+            for (int i = 0; i < n; ++i) {
+                const Aabb& c = B.nodes[ch[i]].box;
+                const double ql = std::floor(((double)c.lo[k] - (double)nb.lo[k]) / step);
+                const double qh = std::ceil(((double)c.hi[k] - (double)nb.lo[k]) / step);
+                const double l = std::min(std::max(ql, 0.0), 255.0), h = std::min(std::max(qh, 0.0), 255.0);
+                if ((double)nb.lo[k] + l * step > (double)c.lo[k] || (double)nb.lo[k] + h * step < (double)c.hi[k])
+                    quant_ok = false;
+                q[k][0][i] = (uint8_t)l;
+                q[k][1][i] = (uint8_t)h;
+            }
+        }
+        f[0] = nb.lo[0];
+        f[1] = nb.lo[1];
+        f[2] = nb.lo[2];
+        std::memcpy(&f[3], &hdr, 4);
+        for (int k = 0; k < 3; ++k) {   // float4 1 + k: low bytes of children 0-7, then high bytes
+            std::memcpy(&f[4 + 4 * k], q[k][0], 8);
+            std::memcpy(&f[6 + 4 * k], q[k][1], 8);
+        }
+        for (int i = 0; i < 8; ++i) {
+            const int32_t l = i < n ? link[i] : (int32_t)~0u;
+            std::memcpy(&f[16 + i], &l, 4);
+        }
     };
-    const Aabb nobox = [] {
-        Aabb a;
-        for (int k = 0; k < 3; ++k) { a.lo[k] = INFINITY; a.hi[k] = -INFINITY; }
-        return a;
-    }();
-    struct Work4 { int32_t bnode; int32_t slot; uint32_t depth; };
-    std::vector<Work4> w4;
-    uint32_t depth4 = 1;
-    int32_t r4 = alloc4();
-    for (int c = 0; c < 4; ++c) put4(r4, c, nobox, (int32_t)~0u);
+    struct Work8 { int32_t bnode; int32_t slot; uint32_t depth; };
+    std::vector<Work8> w8;
+    uint32_t depth8 = 1;
+    int32_t r8 = alloc8();
     if (root >= 0) {
-        if (B.nodes[root].leaf) put4(r4, 0, B.nodes[root].box, leaf_of[root]);
-        else w4.push_back({root, r4, 1});
+        if (B.nodes[root].leaf) {
+            put8(r8, &root, 1, &leaf_of[root]);
+        } else {
+            w8.push_back({root, r8, 1});
+        }
     }
-    while (!w4.empty()) {
-        Work4 w = w4.back();
-        w4.pop_back();
-        depth4 = std::max(depth4, w.depth);
+    while (!w8.empty()) {
+        Work8 w = w8.back();
+        w8.pop_back();
+        depth8 = std::max(depth8, w.depth);
         const BNode& bn = B.nodes[w.bnode];
-        int32_t ch[4] = {bn.left, bn.right, -1, -1};
+        int32_t ch[8] = {bn.left, bn.right, -1, -1, -1, -1, -1, -1};
         int n = 2;
-        while (n < 4) {
+        while (n < 8) {
             int best = -1;
             double ba = -1.0;
             for (int i = 0; i < n; ++i) {
@@ -349,26 +379,26 @@ bool build_bvh(const BvhInput& in, int max_leaf, int threads, BvhOutput& out, co
             ch[best + 1] = o.right;
             ++n;
         }
-        // children are filled in order; inner children get their node index now and are expanded later
-        std::vector<Work4> kids;
-        for (int i = 0; i < 4; ++i) {
-            if (i >= n) { put4(w.slot, i, nobox, (int32_t)~0u); continue; }
+        // inner children get their node index now and are expanded later, in order
+        int32_t link[8];
+        std::vector<Work8> kids;
+        for (int i = 0; i < n; ++i) {
             const BNode& c = B.nodes[ch[i]];
             if (c.leaf) {
-                put4(w.slot, i, c.box, leaf_of[ch[i]]);
+                link[i] = leaf_of[ch[i]];
             } else {
-                int32_t s = alloc4();
-                put4(w.slot, i, c.box, s);
-                kids.push_back({ch[i], s, w.depth + 1});
+                link[i] = alloc8();
+                kids.push_back({ch[i], link[i], w.depth + 1});
             }
         }
-        for (auto it = kids.rbegin(); it != kids.rend(); ++it) w4.push_back(*it);
+        put8(w.slot, ch, n, link);
+        for (auto it = kids.rbegin(); it != kids.rend(); ++it) w8.push_back(*it);
     }
-    out.num_nodes4 = (uint32_t)(out.nodes4.size() / 32);
-    // the 4-wide walk holds at most 3 entries per level plus the leaves of the deepest node
-    if (3 * depth4 + 4 > (uint32_t)TRAVERSAL_STACK4) {
-        out.nodes4.clear();   // too deep for its stack: renders use the binary nodes
-        out.num_nodes4 = 0;
+    out.num_nodes8 = (uint32_t)(out.nodes8.size() / NODE8_FLOATS);
+    // the 8-wide walk holds at most 7 entries per level plus the children of the deepest node
+    if (!quant_ok || 7 * depth8 + 8 > (uint32_t)TRAVERSAL_STACK8) {
+        out.nodes8.clear();   // renders use the binary nodes
+        out.num_nodes8 = 0;
     }
     if (max_depth + 2 > (uint32_t)TRAVERSAL_STACK) { if (err) *err = "BVH too deep for the traversal stack"; return false; }
     return true;

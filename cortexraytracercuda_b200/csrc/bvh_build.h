@@ -23,11 +23,12 @@ struct BvhInput {
 
 struct BvhOutput {
     std::vector<float> nodes;      // 16 floats per node (4 x float4), see rtc_dev.h
-    std::vector<float> nodes4;     // the same tree collapsed to 4-wide nodes: 32 floats (8 x float4) per
-                                   // node, see rtc_dev.h; same leaves, same leaf order
+    std::vector<float> nodes8;     // the same tree collapsed to 8-wide nodes with quantised child boxes:
+                                   // NODE8_FLOATS (6 x float4) per node, see rtc_dev.h; same leaves, same
+                                   // leaf order
     std::vector<uint32_t> order;   // primitive index per leaf slot, leaf order
     uint32_t num_nodes = 0;
-    uint32_t num_nodes4 = 0;
+    uint32_t num_nodes8 = 0;
     uint32_t max_depth = 0;
     uint32_t max_leaf_seen = 0;
 };
@@ -36,7 +37,7 @@ struct BvhOutput {
 bool build_bvh(const BvhInput& in, int max_leaf, int threads, BvhOutput& out, const char** err);
 
 // BVH built on CUDA device `device` (bvh_device.cu) over Morton-sorted primitives, one primitive per
-// leaf, no 4-wide nodes: PLOC clustering (BVH_DEVICE_PLOC) or the linear BVH (BVH_DEVICE_LBVH).
+// leaf, no 8-wide nodes: PLOC clustering (BVH_DEVICE_PLOC) or the linear BVH (BVH_DEVICE_LBVH).
 // BVH_DEVICE_TOO_DEEP and BVH_DEVICE_UNSUPPORTED leave the SAH build as the way out.
 enum BvhDeviceStatus { BVH_DEVICE_OK = 0, BVH_DEVICE_TOO_DEEP = 1, BVH_DEVICE_UNSUPPORTED = 2, BVH_DEVICE_ERROR = 3 };
 enum BvhDeviceMethod { BVH_DEVICE_PLOC = 0, BVH_DEVICE_LBVH = 1 };

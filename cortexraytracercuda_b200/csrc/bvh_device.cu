@@ -458,8 +458,8 @@ int build_bvh_device(const BvhInput& in, int device, BvhDeviceMethod method, Bvh
             break;
         }
         out.max_leaf_seen = 1;
-        out.nodes4.clear();
-        out.num_nodes4 = 0;
+        out.nodes8.clear();
+        out.num_nodes8 = 0;
         if (out.max_depth + 2 > (uint32_t)TRAVERSAL_STACK) {
             what = "device BVH too deep for the traversal stack";
             rc = BVH_DEVICE_TOO_DEEP;

@@ -88,6 +88,7 @@ __device__ __forceinline__ int32_t item_gid(const DevScene& S, uint32_t it) {
     }
 }
 
+template <bool WIDE>
 __global__ void __launch_bounds__(128) rtc_trace_closest(DevScene S, const float* __restrict__ rays, uint32_t n,
                                                          int depth, int max_depth, int32_t* prim, float* tout,
                                                          uint32_t* status_word) {
@@ -98,7 +99,7 @@ __global__ void __launch_bounds__(128) rtc_trace_closest(DevScene S, const float
     float t;
     uint32_t item, status = 0;
     TraceStats st{0, 0};
-    bool h = closest_hit(S, o, d, R[3], R[7], depth == max_depth, t, item, st, status);
+    bool h = closest_hit<false, WIDE>(S, o, d, R[3], R[7], depth == max_depth, t, item, st, status);
     if (prim) prim[k] = h ? item_gid(S, item) : -1;
     if (tout) tout[k] = h ? t : INFINITY;
     if (status) atomicOr(status_word, status);
@@ -145,7 +146,10 @@ cudaError_t rtc_launch_trace_closest(const DevScene& S, const float* rays, uint3
                                      int32_t* prim, float* t, uint32_t* status, cudaStream_t st) {
     if (n == 0) return cudaSuccess;
     const int threads = 128;
-    rtc_trace_closest<<<(n + threads - 1) / threads, threads, 0, st>>>(S, rays, n, depth, max_depth, prim, t, status);
+    if (S.nodes8)   // the scene view carries the 8-wide nodes only when they were asked for
+        rtc_trace_closest<true><<<(n + threads - 1) / threads, threads, 0, st>>>(S, rays, n, depth, max_depth, prim, t, status);
+    else
+        rtc_trace_closest<false><<<(n + threads - 1) / threads, threads, 0, st>>>(S, rays, n, depth, max_depth, prim, t, status);
     return cudaGetLastError();
 }
 

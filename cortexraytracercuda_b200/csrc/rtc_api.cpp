@@ -184,7 +184,7 @@ const DevScene& rtc_scene_dev(const rtc_scene* s) { return s->dev; }
 
 DevScene rtc_scene_view(const rtc_scene* s, const rtc_render_params* p) {
     DevScene S = s->dev;
-    if (!p || !(p->flags & RTC_FLAG_WIDE_BVH)) S.nodes4 = nullptr;
+    if (!p || !(p->flags & RTC_FLAG_WIDE_BVH)) S.nodes8 = nullptr;
     return S;
 }
 DevParams rtc_dev_params(const rtc_render_params* p);
@@ -437,7 +437,7 @@ rtc_status rtc_build_host_scene(const rtc_scene_desc* d, HostScene& H, uint32_t 
         return off;
     };
     size_t o_nodes = add_chunk(bvh.nodes.data(), bvh.nodes.size() * sizeof(float));
-    size_t o_nodes4 = add_chunk(bvh.nodes4.data(), bvh.nodes4.size() * sizeof(float));
+    size_t o_nodes8 = add_chunk(bvh.nodes8.data(), bvh.nodes8.size() * sizeof(float));
     size_t o_items = add_chunk(items.data(), items.size() * 4);
     size_t o_sph = add_chunk(sph.data(), sph.size() * 16);
     size_t o_sphx = add_chunk(sph_aux.data(), sph_aux.size() * 8);
@@ -464,7 +464,7 @@ rtc_status rtc_build_host_scene(const rtc_scene_desc* d, HostScene& H, uint32_t 
     DevScene& D = H.dev;
     D = DevScene{};
     D.nodes = (const float4*)off(o_nodes);
-    D.nodes4 = bvh.num_nodes4 ? (const float4*)off(o_nodes4) : nullptr;
+    D.nodes8 = bvh.num_nodes8 ? (const float4*)off(o_nodes8) : nullptr;
     D.items = (const uint32_t*)off(o_items);
     D.sph = (const float4*)off(o_sph);
     D.sph_aux = (const int2*)off(o_sphx);
@@ -480,7 +480,7 @@ rtc_status rtc_build_host_scene(const rtc_scene_desc* d, HostScene& H, uint32_t 
     D.images = (const int4*)off(o_img);
     D.image_bytes = (const uint8_t*)off(o_imgb);
     D.num_nodes = bvh.num_nodes;
-    D.num_nodes4 = bvh.num_nodes4;
+    D.num_nodes8 = bvh.num_nodes8;
     D.num_items = (uint32_t)items.size();
     D.num_lights = d->num_dir_lights;
     D.num_materials = (uint32_t)mat_i.size();
@@ -504,6 +504,7 @@ rtc_status rtc_build_host_scene(const rtc_scene_desc* d, HostScene& H, uint32_t 
     H.info.device_bytes = total;
     H.info.build_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
     H.info.bvh_builder = builder;
+    H.info.num_wide_nodes = bvh.num_nodes8;
     return RTC_OK;
 }
 
@@ -514,7 +515,7 @@ DevScene rtc_rebase_scene(const HostScene& H, uint8_t* base) {
     };
     rb(D.nodes);
     rb(D.items);
-    if (D.nodes4) rb(D.nodes4);
+    if (D.nodes8) rb(D.nodes8);
     rb(D.sph); rb(D.sph_aux); rb(D.tri); rb(D.tri_n); rb(D.tri_vn); rb(D.quad);
     rb(D.light); rb(D.mat_i); rb(D.mat_f); rb(D.tex_i); rb(D.tex_f); rb(D.images); rb(D.image_bytes);
     if (D.bg.env) rb(D.bg.env);
@@ -740,7 +741,7 @@ rtc_status run_wavefront(const DevScene& S, const rtc_render_params* p, const Wf
     L.counters = d_counters;
     L.status = d_status;
     L.st = st;
-    L.wide = S.nodes4 != nullptr;
+    L.wide = S.nodes8 != nullptr;
     if (phase) RTC_CUDA(cudaEventRecord(phase[0], st));
     RTC_CUDA(cudaMemsetAsync(B.ctr, 0, WF_CTR_N * sizeof(uint32_t), st));
     const int grid = num_sms * 8;
@@ -1043,6 +1044,11 @@ extern "C" rtc_status rtc_get_render_stats(rtc_context* c, rtc_render_stats* out
 
 extern "C" rtc_status rtc_trace_closest(rtc_context* c, const rtc_scene* s, const float* rays, uint32_t n,
                                         int32_t depth, int32_t max_depth, int32_t* prim, float* t) {
+    return rtc_trace_closest_ex(c, s, rays, n, depth, max_depth, 0, prim, t);
+}
+
+extern "C" rtc_status rtc_trace_closest_ex(rtc_context* c, const rtc_scene* s, const float* rays, uint32_t n,
+                                           int32_t depth, int32_t max_depth, int32_t flags, int32_t* prim, float* t) {
     if (!c || !s || (n && !rays)) return fail(RTC_ERR_INVALID_ARGUMENT, "null argument");
     if (n == 0) return RTC_OK;
     std::lock_guard<std::mutex> lk(c->mu);
@@ -1058,7 +1064,9 @@ extern "C" rtc_status rtc_trace_closest(rtc_context* c, const rtc_scene* s, cons
     if (r == RTC_OK) {
         e = cudaMemcpyAsync(d_rays, rays, (size_t)n * 8 * sizeof(float), cudaMemcpyHostToDevice, c->stream);
         if (e == cudaSuccess) e = cudaMemsetAsync(c->d_status, 0, 4, c->stream);
-        if (e == cudaSuccess) e = rtc_launch_trace_closest(rtc_scene_view(s, nullptr), d_rays, n, depth, max_depth, d_prim, d_t, c->d_status, c->stream);
+        rtc_render_params vp{};
+        vp.flags = flags;
+        if (e == cudaSuccess) e = rtc_launch_trace_closest(rtc_scene_view(s, &vp), d_rays, n, depth, max_depth, d_prim, d_t, c->d_status, c->stream);
         if (e == cudaSuccess && prim) e = cudaMemcpyAsync(prim, d_prim, (size_t)n * 4, cudaMemcpyDeviceToHost, c->stream);
         if (e == cudaSuccess && t) e = cudaMemcpyAsync(t, d_t, (size_t)n * 4, cudaMemcpyDeviceToHost, c->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);

@@ -6,10 +6,13 @@
 //                n0 = (L.lo.x, L.hi.x, L.lo.y, L.hi.y)   n1 = (R.lo.x, R.hi.x, R.lo.y, R.hi.y)
 //                n2 = (L.lo.z, L.hi.z, R.lo.z, R.hi.z)   n3 = (child L, child R, -, -) as int bits
 //              child >= 0: inner node index; child < 0: leaf, ~child = (first_item << 5) | count.
-//   nodes4     the same tree collapsed to 4-wide nodes, 8 x float4 = 128 B (one cache line) per node:
-//                (lo.x[0..3]) (hi.x[0..3]) (lo.y[0..3]) (hi.y[0..3]) (lo.z[0..3]) (hi.z[0..3])
-//                (child[0..3] as int bits) (unused); empty child slots hold -1 and an inverted box.
-//              Same leaves and leaf order as `nodes`; renders use it when RTC_FLAG_WIDE_BVH is set.
+//   nodes8     the same tree collapsed to 8-wide nodes with quantised child boxes, 6 x float4 = 96 B:
+//                (p.xyz, header)  header = (e.x+127) | (e.y+127) << 8 | (e.z+127) << 16 | children << 24
+//                (qlo.x[0..7] bytes, qhi.x[0..7] bytes) (same for y) (same for z)
+//                (child[0..3] as int bits) (child[4..7] as int bits)
+//              child c's box on axis a is [p.a + qlo.a[c] * 2^e.a, p.a + qhi.a[c] * 2^e.a] (rounded outwards
+//              when built, so it encloses the child's exact box); slots at or past `children` are
+//              unused.  Same leaves and leaf order as `nodes`; renders use it when RTC_FLAG_WIDE_BVH is set.
 //   items      uint32 per leaf entry, leaf order: (kind << 30) | index into that kind's array.
 //   sph        float4 (center.xyz, radius)                      16 B / sphere  (leaf order)
 //   sph_aux    int2   (material, global id)
@@ -34,7 +37,8 @@ enum ItemKind : uint32_t { ITEM_SPHERE = 0, ITEM_QUAD = 1, ITEM_TRI = 2, ITEM_LI
 constexpr int LEAF_COUNT_BITS = 5;
 constexpr int MAX_LEAF = 31;
 constexpr int TRAVERSAL_STACK = 64;
-constexpr int TRAVERSAL_STACK4 = 96;   // 4-wide: up to 3 entries per level, leaves included
+constexpr int TRAVERSAL_STACK8 = 128;  // 8-wide: up to 7 entries per level, leaves included
+constexpr int NODE8_FLOATS = 24;       // 6 x float4 per 8-wide node
 
 // kernel status word bits (device -> host)
 enum StatusBits : uint32_t {
@@ -66,7 +70,7 @@ struct DevBackground {
 
 struct DevScene {
     const float4* nodes;
-    const float4* nodes4;      // null: binary traversal
+    const float4* nodes8;      // null: binary traversal
     const uint32_t* items;
     const float4* sph;
     const int2* sph_aux;
@@ -82,7 +86,7 @@ struct DevScene {
     const int4* images;
     const uint8_t* image_bytes;
     uint32_t num_nodes;
-    uint32_t num_nodes4;
+    uint32_t num_nodes8;
     uint32_t num_items;
     uint32_t num_lights;
     uint32_t num_materials;

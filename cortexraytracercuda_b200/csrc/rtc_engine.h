@@ -33,7 +33,7 @@ struct EngineConfig {
     int batch = 12;                // iterations per batch
     uint32_t drain = 0;            // drain threshold in slots (0: 512 per SM)
     bool graphs = true;            // replay batches as a captured CUDA graph (batch a multiple of 6)
-    bool wide = false;             // extend walks the 4-wide nodes (jobs asked for RTC_FLAG_WIDE_BVH)
+    bool wide = false;             // extend walks the 8-wide nodes (jobs asked for RTC_FLAG_WIDE_BVH)
     int block = 128;               // threads per block of the extend and shade kernels (128, 256, 512)
 };
 

@@ -16,7 +16,7 @@ rtc_status rtc_set_error(rtc_status s, const char* msg);
 rtc_status rtc_check_render_params(const rtc_render_params* p);
 // device-side view of a scene, and the per-launch parameters of a render
 const rtc::DevScene& rtc_scene_dev(const rtc_scene* s);
-// the device view a render uses: the 4-wide nodes only when the params ask for RTC_FLAG_WIDE_BVH
+// the device view a render uses: the 8-wide nodes only when the params ask for RTC_FLAG_WIDE_BVH
 rtc::DevScene rtc_scene_view(const rtc_scene* s, const rtc_render_params* p);
 rtc::DevParams rtc_dev_params(const rtc_render_params* p);
 // scratch of an image rendered with sample groups (0 without), and its layout at `base`

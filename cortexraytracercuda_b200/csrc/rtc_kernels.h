@@ -28,7 +28,7 @@ struct WfLaunch {
     WfIter w;
     WfWindow win;                    // ADMIT: the window to publish
     float k0, threshold;             // SPLIT: iterations so far, long-chain threshold (iterations)
-    bool wide;                       // EXTEND: walk the 4-wide nodes (where the scene carries them)
+    bool wide;                       // EXTEND: walk the 8-wide nodes (where the scene carries them)
     unsigned long long* counters;    // NULL: no instrumentation
     uint32_t* status;
     int grid;

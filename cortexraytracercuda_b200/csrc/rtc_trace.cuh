@@ -274,15 +274,14 @@ __device__ __forceinline__ void test_leaf(const DevScene& S, int32_t child, V3 o
     }
 }
 
-// Near/far distances of one child box of a 4-wide node (the slab2 arithmetic, one child).
-__device__ __forceinline__ float slab1(float lx, float hx, float ly, float hy, float lz, float hz, V3 inv, V3 oi,
-                                       float tmin, float tmax, float& tf) {
-    float ax = __fmaf_rn(lx, inv.x, -oi.x), bx = __fmaf_rn(hx, inv.x, -oi.x);
-    float ay = __fmaf_rn(ly, inv.y, -oi.y), by = __fmaf_rn(hy, inv.y, -oi.y);
-    float az = __fmaf_rn(lz, inv.z, -oi.z), bz = __fmaf_rn(hz, inv.z, -oi.z);
-    tf = fminf(fminf(fmaxf(ax, bx), fmaxf(ay, by)), fminf(fmaxf(az, bz), tmax));
-    return fmaxf(fmaxf(fminf(ax, bx), fminf(ay, by)), fmaxf(fminf(az, bz), tmin));
-}
+// Direction component for the slab tests' reciprocal.  The slab distance is fma(lo, 1/d, -o/d); with a
+// zero component the two infinite products cancel to NaN or collapse to -inf by the SIGNS of lo and o,
+// not by whether o lies between the slab's planes, so a box whose slab holds the origin could be culled
+// (the reference subtracts first, (lo - o) / d, and keeps it).  Components below 1e-20 in magnitude are
+// traced as +-1e-20: the reciprocal stays finite, a slab that holds the origin spans about
+// [-1e20 |lo - o|, +1e20 |hi - o|], and one that does not lies beyond any finite hit.  Other components
+// are unchanged, so every other ray walks the tree exactly as before.
+__device__ __forceinline__ float slab_dir(float x) { return fabsf(x) < 1e-20f ? copysignf(1e-20f, x) : x; }
 
 __device__ __forceinline__ void cswap(uint32_t& a, uint32_t& b) {
     const uint32_t lo = min(a, b), hi = max(a, b);
@@ -290,54 +289,82 @@ __device__ __forceinline__ void cswap(uint32_t& a, uint32_t& b) {
     b = hi;
 }
 
-// Closest hit through the 4-wide nodes.  Each visit loads one 128-byte node, tests its four child boxes,
-// sorts the hit children by entry distance (key = distance bits with the child index in the two low
-// bits; distances are >= tmin > 0, so the bits order like the floats and clearing two low bits rounds
-// down, which keeps the culling conservative), and pushes them far to near.  Leaves travel through the
-// stack too, so the leaf test is inlined once; an entry farther than the current best hit is dropped
-// when popped.
+// Byte `c` (0-3) of `w` as a float: the byte becomes the low mantissa byte of 2^23, and subtracting
+// 2^23 leaves exactly its value (two full-rate instructions instead of an integer-to-float conversion).
+__device__ __forceinline__ float byte_f(uint32_t w, int c) {
+    return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7650u | (uint32_t)c)) - 8388608.0f;
+}
+
+// Link of child `c` (0-7) from the node's two link words, by selects (no indexed register array).
+__device__ __forceinline__ int32_t child8(const float4& a, const float4& b, uint32_t c) {
+    const float4& v = c < 4u ? a : b;
+    const uint32_t k = c & 3u;
+    return __float_as_int(k < 2u ? (k == 0u ? v.x : v.y) : (k == 2u ? v.z : v.w));
+}
+
+// Closest hit through the 8-wide nodes with quantised child boxes.  A visit loads one 96-byte node and
+// tests its children's boxes: on each axis the child bound p + q * 2^e gives the distance
+// fma(q, 2^e / d, (p - o) / d), the same rounding model as the binary slab (the step is a power of two,
+// so 2^e / d is exact).  Hit children are sorted by entry distance (key = distance bits with the child
+// slot in the three low bits; distances are >= tmin > 0, so the bits order like the floats, and clearing
+// the low bits rounds down, which keeps the culling conservative) with a 19-comparator network and
+// pushed far to near.  Leaves travel through the stack too, so the leaf test is inlined once; an entry
+// farther than the current best hit is dropped when popped.
 template <bool EXACT>
-__device__ __forceinline__ bool closest_hit4(const DevScene& S, V3 o, V3 d, V3 inv, V3 oi, float tmin, float tmax,
+__device__ __forceinline__ bool closest_hit8(const DevScene& S, V3 o, V3 d, V3 inv, V3 oi, float tmin, float tmax,
                                              bool hide_invisible, float& t_out, uint32_t& item_out,
                                              TraceStats& st, uint32_t& status) {
     float best_t = tmax;
     uint32_t best_item = 0xffffffffu;
-    int2 stk[TRAVERSAL_STACK4];   // (child reference, entry distance bits)
+    int2 stk[TRAVERSAL_STACK8];   // (child reference, entry distance bits)
     int sp = 0;
     int32_t ref = 0;   // the root node
+    // A walk visits each node and leaf at most once; more visits than that mean malformed links, and
+    // the walk stops with STATUS_TIMEOUT instead of running on.
+    const uint32_t visit_limit = 2u * (S.num_nodes8 + S.num_items) + 64u;
+    uint32_t visits = 0;
     for (;;) {
+        if (++visits > visit_limit) { status |= STATUS_TIMEOUT; break; }
         if (ref >= 0) {
-            if ((uint32_t)ref >= S.num_nodes4) { status |= STATUS_BAD_ITEM; break; }
-            const float4* np = S.nodes4 + 8 * (size_t)ref;
-            const float4 lx = ld_scene(np), hx = ld_scene(np + 1), ly = ld_scene(np + 2), hy = ld_scene(np + 3);
-            const float4 lz = ld_scene(np + 4), hz = ld_scene(np + 5), ch = ld_scene(np + 6);
+            if ((uint32_t)ref >= S.num_nodes8) { status |= STATUS_BAD_ITEM; break; }
+            const float4* np = S.nodes8 + 6 * (size_t)ref;
+            const float4 h = ld_scene(np), qx = ld_scene(np + 1), qy = ld_scene(np + 2), qz = ld_scene(np + 3);
+            const float4 la = ld_scene(np + 4), lb = ld_scene(np + 5);
             st.nodes++;
-            float f0, f1, f2, f3;
-            const float n0 = slab1(lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, inv, oi, tmin, best_t, f0);
-            const float n1 = slab1(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, inv, oi, tmin, best_t, f1);
-            const float n2 = slab1(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, inv, oi, tmin, best_t, f2);
-            const float n3 = slab1(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, inv, oi, tmin, best_t, f3);
-            const int32_t c0 = __float_as_int(ch.x), c1 = __float_as_int(ch.y), c2 = __float_as_int(ch.z),
-                          c3 = __float_as_int(ch.w);
-            uint32_t k0 = (n0 <= f0 && c0 != -1) ? ((__float_as_uint(n0) & ~3u) | 0u) : 0xffffffffu;
-            uint32_t k1 = (n1 <= f1 && c1 != -1) ? ((__float_as_uint(n1) & ~3u) | 1u) : 0xffffffffu;
-            uint32_t k2 = (n2 <= f2 && c2 != -1) ? ((__float_as_uint(n2) & ~3u) | 2u) : 0xffffffffu;
-            uint32_t k3 = (n3 <= f3 && c3 != -1) ? ((__float_as_uint(n3) & ~3u) | 3u) : 0xffffffffu;
-            cswap(k0, k1);
-            cswap(k2, k3);
-            cswap(k0, k2);
-            cswap(k1, k3);
-            cswap(k1, k2);
-            // push far to near: the nearest child ends on top
-            const uint32_t ks[4] = {k3, k2, k1, k0};
+            const uint32_t hdr = __float_as_uint(h.w);
+            const uint32_t n = hdr >> 24;
+            const float ax = __uint_as_float((hdr & 0xffu) << 23) * inv.x;
+            const float ay = __uint_as_float(((hdr >> 8) & 0xffu) << 23) * inv.y;
+            const float az = __uint_as_float(((hdr >> 16) & 0xffu) << 23) * inv.z;
+            const float bx = __fmaf_rn(h.x, inv.x, -oi.x), by = __fmaf_rn(h.y, inv.y, -oi.y),
+                        bz = __fmaf_rn(h.z, inv.z, -oi.z);
+            uint32_t key[8];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const uint32_t k = ks[q];
+            for (int c = 0; c < 8; ++c) {
+                const int b = c & 3;
+                const uint32_t wlx = __float_as_uint(c < 4 ? qx.x : qx.y), whx = __float_as_uint(c < 4 ? qx.z : qx.w);
+                const uint32_t wly = __float_as_uint(c < 4 ? qy.x : qy.y), why = __float_as_uint(c < 4 ? qy.z : qy.w);
+                const uint32_t wlz = __float_as_uint(c < 4 ? qz.x : qz.y), whz = __float_as_uint(c < 4 ? qz.z : qz.w);
+                const float x0 = __fmaf_rn(byte_f(wlx, b), ax, bx), x1 = __fmaf_rn(byte_f(whx, b), ax, bx);
+                const float y0 = __fmaf_rn(byte_f(wly, b), ay, by), y1 = __fmaf_rn(byte_f(why, b), ay, by);
+                const float z0 = __fmaf_rn(byte_f(wlz, b), az, bz), z1 = __fmaf_rn(byte_f(whz, b), az, bz);
+                const float tn = fmaxf(fmaxf(fminf(x0, x1), fminf(y0, y1)), fmaxf(fminf(z0, z1), tmin));
+                const float tf = fminf(fminf(fmaxf(x0, x1), fmaxf(y0, y1)), fminf(fmaxf(z0, z1), best_t));
+                key[c] = ((uint32_t)c < n && tn <= tf) ? ((__float_as_uint(tn) & ~7u) | (uint32_t)c) : 0xffffffffu;
+            }
+            cswap(key[0], key[1]); cswap(key[2], key[3]); cswap(key[4], key[5]); cswap(key[6], key[7]);
+            cswap(key[0], key[2]); cswap(key[1], key[3]); cswap(key[4], key[6]); cswap(key[5], key[7]);
+            cswap(key[1], key[2]); cswap(key[5], key[6]);
+            cswap(key[0], key[4]); cswap(key[1], key[5]); cswap(key[2], key[6]); cswap(key[3], key[7]);
+            cswap(key[2], key[4]); cswap(key[3], key[5]);
+            cswap(key[1], key[2]); cswap(key[3], key[4]); cswap(key[5], key[6]);
+            // push far to near: the nearest child ends on top
+#pragma unroll
+            for (int q = 7; q >= 0; --q) {
+                const uint32_t k = key[q];
                 if (k == 0xffffffffu) continue;
-                const uint32_t c = k & 3u;
-                const int32_t r = c == 0u ? c0 : (c == 1u ? c1 : (c == 2u ? c2 : c3));
-                if (sp >= TRAVERSAL_STACK4) { status |= STATUS_STACK_OVERFLOW; break; }
-                stk[sp] = make_int2(r, (int)(k & ~3u));
+                if (sp >= TRAVERSAL_STACK8) { status |= STATUS_STACK_OVERFLOW; break; }
+                stk[sp] = make_int2(child8(la, lb, k & 7u), (int)(k & ~7u));
                 ++sp;
             }
             if (status & STATUS_STACK_OVERFLOW) break;
@@ -362,17 +389,25 @@ __device__ __forceinline__ bool closest_hit4(const DevScene& S, V3 o, V3 d, V3 i
 }
 
 // Closest hit in [tmin, tmax] over the whole scene (the reference's world.hit through the BVH).
-// EXACT: clean mode (double-precision sphere test).  WIDE: walk the 4-wide nodes when the scene
+// EXACT: clean mode (double-precision sphere test).  WIDE: walk the 8-wide nodes when the scene
 // carries them (only the extend kernel is built with it, so the other kernels carry no code for it).
 template <bool EXACT = false, bool WIDE = false>
 __device__ __forceinline__ bool closest_hit(const DevScene& S, V3 o, V3 d, float tmin, float tmax,
                                             bool hide_invisible, float& t_out, uint32_t& item_out,
                                             TraceStats& st, uint32_t& status) {
-    V3 inv = v3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
+    // A zero direction meets no primitive: every test of the reference's hit() rejects it (0/0 roots,
+    // zero denominator, zero determinant), so it misses without a walk.  Such rays are common: a
+    // lambertian bounce with an empty light list scatters along a zero vector.
+    if (d.x == 0.0f && d.y == 0.0f && d.z == 0.0f) {
+        t_out = tmax;
+        item_out = 0xffffffffu;
+        return false;
+    }
+    V3 inv = v3(1.0f / slab_dir(d.x), 1.0f / slab_dir(d.y), 1.0f / slab_dir(d.z));
     if constexpr (WIDE) {
-        if (S.nodes4) {
-            V3 oi4 = v3(o.x * inv.x, o.y * inv.y, o.z * inv.z);
-            return closest_hit4<EXACT>(S, o, d, inv, oi4, tmin, tmax, hide_invisible, t_out, item_out, st, status);
+        if (S.nodes8) {
+            V3 oi8 = v3(o.x * inv.x, o.y * inv.y, o.z * inv.z);
+            return closest_hit8<EXACT>(S, o, d, inv, oi8, tmin, tmax, hide_invisible, t_out, item_out, st, status);
         }
     }
     V3 oi = v3(o.x * inv.x, o.y * inv.y, o.z * inv.z);

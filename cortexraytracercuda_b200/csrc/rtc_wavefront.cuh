@@ -284,7 +284,7 @@ __global__ void __launch_bounds__(128) wf_admit(WfTable J, WfBuffers B, WfIter w
 }
 
 // FLAVOR: 0 nvcc flavour, 1 g++ flavour, 2 clean mode (double-precision sphere test).
-// WIDE: the 4-wide node layout (RTC_FLAG_WIDE_BVH; the other kernels always walk the binary nodes).
+// WIDE: the 8-wide node layout (RTC_FLAG_WIDE_BVH; the other kernels always walk the binary nodes).
 template <bool COUNT, int FLAVOR, class J, bool WIDE>
 __global__ void RTC_EXTEND_BOUNDS wf_extend(J jobs, WfBuffers B, WfIter w, unsigned long long* counters,
                                                  uint32_t* status_word) {

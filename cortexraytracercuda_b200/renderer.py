@@ -136,14 +136,15 @@ class DeviceScene:
                                              C.c_void_p(d_counters) if d_counters else None,
                                              C.c_void_p(stream) if stream else None))
 
-    def trace_closest(self, rays: np.ndarray, depth: int = 0, max_depth: int = 1):
-        """Closest-hit primitive id (-1 = miss) and t for rays (n, 8) = (ox,oy,oz,tmin,dx,dy,dz,tmax)."""
+    def trace_closest(self, rays: np.ndarray, depth: int = 0, max_depth: int = 1, flags: int = 0):
+        """Closest-hit primitive id (-1 = miss) and t for rays (n, 8) = (ox,oy,oz,tmin,dx,dy,dz,tmax).
+        ``flags``: FLAG_WIDE_BVH walks the 8-wide nodes."""
         rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
         n = rays.shape[0]
         prim = np.empty(n, np.int32)
         t = np.empty(n, np.float32)
-        check(self.ctx.lib.rtc_trace_closest(self.ctx.handle, self.handle, rays.ctypes.data, n, depth, max_depth,
-                                             prim.ctypes.data, t.ctypes.data))
+        check(self.ctx.lib.rtc_trace_closest_ex(self.ctx.handle, self.handle, rays.ctypes.data, n, depth, max_depth,
+                                                flags, prim.ctypes.data, t.ctypes.data))
         return prim, t
 
 

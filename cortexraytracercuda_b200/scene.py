@@ -103,7 +103,7 @@ class rtc_render_stats(C.Structure):
 class rtc_scene_info(C.Structure):
     _fields_ = [("num_primitives", C.c_uint32), ("num_lights", C.c_uint32), ("num_nodes", C.c_uint32),
                 ("max_leaf_size", C.c_uint32), ("device_bytes", C.c_uint64), ("build_ms", C.c_double),
-                ("bvh_builder", C.c_uint32)]
+                ("bvh_builder", C.c_uint32), ("num_wide_nodes", C.c_uint32)]
 
 
 class rtc_scene_options(C.Structure):

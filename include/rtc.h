@@ -242,10 +242,12 @@ typedef struct rtc_render_params {
 /* Record CUDA events around every extend and shade launch of the wavefront engine; the per-kernel
  * device times are then reported by rtc_get_render_stats (extend_ms / shade_ms / *_launches). */
 #define RTC_FLAG_KERNEL_TIMING 1
-/* Traverse the 4-wide BVH (128-byte nodes) instead of the binary one (64-byte nodes, the default).  Both
+/* Traverse the 8-wide BVH with quantised child boxes (96-byte nodes: an 8-bit grid per axis, bounds
+ * rounded outwards so no hit is lost) instead of the binary one (64-byte nodes, the default).  Both
  * hold the same leaves in the same order; the closest hit is the same except for which of several
- * primitives at exactly the same distance is reported.  Measured slower on B200 (its traversal stack
- * does not stay in L1), kept as a node-layout option. */
+ * primitives at exactly the same distance is reported.  A node-layout option for the batch autotuner;
+ * scenes whose 8-wide tree would be too deep for its stack, and device-built trees, use the binary
+ * nodes. */
 #define RTC_FLAG_WIDE_BVH 2
 /* Clean mode: split each pixel's samples into min(8, spp) consecutive groups that run on separate path
  * slots, so a pixel's samples trace in parallel instead of one after another (shorter critical path,
@@ -275,11 +277,11 @@ rtc_status rtc_scene_destroy(rtc_scene* scene);
 /* BVH builders.  The reference builds its tree on one device thread (random axis, exchange sort of the
  * span, bvh_node.cuh:63-108 via gpu.cu:749); it has no choice of builder, so rtc_scene_create_ex and
  * the option below have no reference counterpart. */
-#define RTC_BVH_SAH 0      /* binned SAH on host threads, leaves of up to 4 items, 4-wide copy (default) */
+#define RTC_BVH_SAH 0      /* binned SAH on host threads, leaves of up to 4 items, 8-wide copy (default) */
 #define RTC_BVH_DEVICE 1   /* built on the device: primitives sorted by the 30-bit Morton code of their
                               centroids, then clustered bottom-up (PLOC: mutual nearest neighbours by
                               union surface area within 16 positions); one primitive per leaf, tree
-                              quality close to SAH.  No 4-wide copy (RTC_FLAG_WIDE_BVH renders use the
+                              quality close to SAH.  No 8-wide copy (RTC_FLAG_WIDE_BVH renders use the
                               binary nodes).  Falls back to RTC_BVH_SAH for a single primitive or a tree
                               deeper than the traversal stack. */
 #define RTC_BVH_DEVICE_LBVH 2   /* built on the device as a linear BVH over the same sorted codes
@@ -301,6 +303,7 @@ typedef struct rtc_scene_info {
     uint64_t device_bytes;     /* bytes resident on the device for this scene                      */
     double build_ms;           /* validation, flattening and BVH build time (host wall clock)        */
     uint32_t bvh_builder;      /* RTC_BVH_* that built the tree                                      */
+    uint32_t num_wide_nodes;   /* 8-wide nodes (RTC_FLAG_WIDE_BVH); 0: the scene has only binary nodes */
 } rtc_scene_info;
 rtc_status rtc_scene_get_info(const rtc_scene* scene, rtc_scene_info* info);
 
@@ -486,6 +489,10 @@ rtc_status rtc_server_get_stats(rtc_server* server, rtc_server_stats* stats);
  * prim_id (-1 on a miss) and t. */
 rtc_status rtc_trace_closest(rtc_context* ctx, const rtc_scene* scene, const float* rays, uint32_t n,
                              int32_t depth, int32_t max_depth, int32_t* prim_id, float* t);
+/* rtc_trace_closest with render flags: RTC_FLAG_WIDE_BVH walks the 8-wide nodes (where the scene has
+ * them), so both node layouts can be checked against each other.  No counterpart in the reference. */
+rtc_status rtc_trace_closest_ex(rtc_context* ctx, const rtc_scene* scene, const float* rays, uint32_t n,
+                                int32_t depth, int32_t max_depth, int32_t flags, int32_t* prim_id, float* t);
 
 /* ------------------------------------------------------------------------------------------------ */
 /* drop-in form of the reference call                                                                */

@@ -96,7 +96,7 @@ def test_device_bvh_images(ctx, name, kw, builder):
     print(name, "identical pixels", same, "means", ma, mb)
     assert same >= 0.995
     assert abs(ma - mb) <= 0.005 * ma
-    # no 4-wide copy: the wide flag falls back to the binary nodes and changes nothing
+    # no 8-wide copy: the wide flag falls back to the binary nodes and changes nothing
     pw = configs.SCENES[name][1](**kw)
     pw.mode, pw.draw_order, pw.engine, pw.flags = MODE_COMPAT, DRAW_ORDER_HOST, ENGINE_WAVEFRONT, FLAG_WIDE_BVH
     assert np.array_equal(_img(dev, pw), b, equal_nan=True)

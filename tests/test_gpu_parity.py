@@ -224,11 +224,14 @@ def test_clean_mode_statistics(ctx, port, name):
 
 @pytest.mark.parametrize("name,kw", SCENES)
 def test_wide_bvh_matches_binary(ctx, name, kw):
-    """The 4-wide nodes hold the same leaves as the binary ones, so the closest hit is the same except
-    for exact-distance ties; the g++ flavour's images agree pixel for pixel (ties shade alike here)."""
+    """The 8-wide nodes hold the same leaves as the binary ones and their quantised boxes enclose the
+    exact ones, so the closest hit is the same except for exact-distance ties; the g++ flavour's images
+    agree pixel for pixel (ties shade alike here)."""
     from cortexraytracercuda_b200.scene import FLAG_WIDE_BVH
     scene, params = _params(name, kw, DRAW_ORDER_HOST)
     ds = DeviceScene(ctx, scene)
+    info = ds.info()
+    assert 0 < info["num_wide_nodes"] <= max(1, info["num_nodes"])   # the 8-wide copy exists
     binary, _ = ds.render(params)
     params.flags |= FLAG_WIDE_BVH
     wide, _ = ds.render(params)
