@@ -263,3 +263,23 @@ def test_long_chain_split(ctx, monkeypatch, order):
         st = oracles.parity_stats(wf.reshape(-1, 4), mk.reshape(-1, 4))
         assert abs(st["mean_rel"]) <= 0.02, st
 
+
+
+@pytest.mark.parametrize("name", ["cornell", "spheres", "icosphere", "textured", "meshes6"])
+def test_wide_bvh_hit_identity(ctx, name):
+    """Closest hits through the 8-wide quantised nodes equal the binary walk's on random rays, including
+    rays with a zero direction component and all-zero directions (which miss in both walks)."""
+    from cortexraytracercuda_b200.scene import FLAG_WIDE_BVH
+    from golden.make_golden import golden_rays
+    scene = configs.meshes(level=6, env_size=(64, 32)) if name == "meshes6" else configs.SCENES[name][0]()
+    ds = DeviceScene(ctx, scene)
+    assert ds.info()["num_wide_nodes"] > 0
+    rays = golden_rays("spheres" if name == "meshes6" else name, 20000, seed=23)
+    rays[::7, 4] = 0.0          # one zero component
+    rays[::11, 4:7] = 0.0       # zero direction
+    a, ta = ds.trace_closest(rays, 0, 8)
+    b, tb = ds.trace_closest(rays, 0, 8, FLAG_WIDE_BVH)
+    assert np.all(a[::11] == -1) and np.all(b[::11] == -1)
+    assert np.array_equal(ta.view(np.uint32), tb.view(np.uint32))
+    assert int((a != b).sum()) <= max(3, int(0.001 * len(rays)))   # exact-t ties only
+    ds.close()
