@@ -289,6 +289,29 @@ def icosphere_scene(level=3, seed=DEFAULT_SEED) -> Scene:
     return s
 
 
+def lights_scene(seed=DEFAULT_SEED) -> Scene:
+    """Every light type: two omni lights (one hidden to primary rays), a directional quad light and a
+    spot light cone, over lambertian, metal and dielectric spheres, a small displaced icosphere and a
+    floor.  The light list is omni, omni, directional, spot, so light 0 (always the sampled one) is an
+    omni light."""
+    s = Scene(name="lights")
+    s.omni_light((-2.5, 3.0, 1.0), 0.4, (6.0, 5.0, 4.0), intensity=1.5, invisible=True)
+    s.omni_light((2.8, 2.2, -1.5), 0.3, (3.0, 4.0, 6.0), intensity=2.0, invisible=False)
+    s.dir_light((0.0, 5.0, 0.0), (2.0, 0.0, 0.0), (0.0, 0.0, 2.0), (4.0, 4.0, 4.0), intensity=1.0, invisible=True)
+    s.spot_light((0.0, 3.5, 2.5), (0.0, -1.0, -0.6), 35.0, 4.0, (8.0, 8.0, 7.0), intensity=2.0, radius=0.25,
+                 invisible=False)
+    s.quad((-8.0, 0.0, -8.0), (16.0, 0.0, 0.0), (0.0, 0.0, 16.0), s.lambertian((0.6, 0.6, 0.6)))
+    s.sphere((-1.5, 0.8, 0.0), 0.8, s.lambertian((0.8, 0.3, 0.2)))
+    s.sphere((0.3, 0.6, 0.6), 0.6, s.metal((0.9, 0.9, 0.8), 0.15))
+    s.sphere((1.6, 0.7, -0.4), 0.7, s.dielectric(1.5))
+    v, f = displaced_icosphere(2, 0.1, seed)
+    s.mesh((0.5 * v + np.array([0.0, 0.5, -2.0])).astype(np.float32), f, s.lambertian((0.2, 0.5, 0.8)))
+    s.camera = Camera(look_from=(0.0, 2.2, 6.5), look_at=(0.0, 0.8, 0.0), up=(0, 1, 0), vfov=45.0, aspect=4.0 / 3.0,
+                      aperture=0.0, focus=6.5)
+    s.set_background_constant((0.02, 0.02, 0.03))
+    return s
+
+
 # -------------------------------------------------------------------------------------------------
 # batched / served workload
 # -------------------------------------------------------------------------------------------------
@@ -364,4 +387,5 @@ SCENES = {
     "meshes": (meshes, meshes_params),
     "textured": (textured, lambda **kw: RenderParams(**{**dict(width=160, height=120, spp=16, max_depth=10), **kw})),
     "icosphere": (icosphere_scene, lambda **kw: RenderParams(**{**dict(width=150, height=100, spp=16, max_depth=12), **kw})),
+    "lights": (lights_scene, lambda **kw: RenderParams(**{**dict(width=120, height=90, spp=16, max_depth=10), **kw})),
 }

@@ -198,6 +198,7 @@ rtc_status rtc_build_host_scene(const rtc_scene_desc* d, HostScene& H, uint32_t 
     auto bad = [&](const std::string& m) { return fail(RTC_ERR_BAD_SCENE, m); };
     if ((d->num_textures && !d->textures) || (d->num_images && !d->images) || (d->num_materials && !d->materials) ||
         (d->num_dir_lights && !d->dir_lights) || (d->num_spheres && !d->spheres) || (d->num_quads && !d->quads) ||
+        (d->num_omni_lights && !d->omni_lights) || (d->num_spot_lights && !d->spot_lights) ||
         (d->num_meshes && !d->meshes))
         return bad("count > 0 with a null array");
     for (uint32_t i = 0; i < d->num_images; ++i)
@@ -237,7 +238,21 @@ rtc_status rtc_build_host_scene(const rtc_scene_desc* d, HostScene& H, uint32_t 
     for (uint32_t i = 0; i < d->num_quads; ++i)
         if (!mat_ok(d->quads[i].material) || !finite3(d->quads[i].q) || !finite3(d->quads[i].u) || !finite3(d->quads[i].v))
             return bad("quad " + std::to_string(i) + " is invalid");
-    const uint64_t nprims = (uint64_t)d->num_dir_lights + d->num_spheres + d->num_quads + ntri;
+    for (uint32_t i = 0; i < d->num_omni_lights; ++i) {
+        const rtc_omni_light& L = d->omni_lights[i];
+        if (!finite3(L.position) || !std::isfinite(L.radius) || !finite3(L.color) || !std::isfinite(L.intensity))
+            return bad("omni light " + std::to_string(i) + " is invalid");
+    }
+    for (uint32_t i = 0; i < d->num_spot_lights; ++i) {
+        const rtc_spot_light& L = d->spot_lights[i];
+        if (!finite3(L.position) || !finite3(L.direction) || !std::isfinite(L.radius) || !finite3(L.color) ||
+            !std::isfinite(L.intensity) || !std::isfinite(L.cutoff) || !std::isfinite(L.falloff))
+            return bad("spot light " + std::to_string(i) + " is invalid");
+    }
+    // the light list: omni lights, directional lights, spot lights (load_scene, gpu.cu:504-523)
+    const uint32_t n_omni = d->num_omni_lights, n_dir = d->num_dir_lights, n_spot = d->num_spot_lights;
+    const uint32_t nlights = n_omni + n_dir + n_spot;
+    const uint64_t nprims = (uint64_t)nlights + d->num_spheres + d->num_quads + ntri;
     if (nprims == 0) return bad("scene has no primitives");
     if (nprims >= (1ull << 26)) return bad("scene has too many primitives (max 2^26)");
     if (d->background.kind < 0 || d->background.kind > 2) return bad("unknown background kind");
@@ -251,13 +266,26 @@ rtc_status rtc_build_host_scene(const rtc_scene_desc* d, HostScene& H, uint32_t 
     prims.reserve(nprims);
     BvhInput bin;
     bin.boxes.reserve(nprims);
+    auto sphere_light_box = [&](const float* c, float radius) {
+        const float r = std::fabs(radius);
+        V3 cc[2] = {v3(c[0] - r, c[1] - r, c[2] - r), v3(c[0] + r, c[1] + r, c[2] + r)};
+        return box_of(cc, 2);
+    };
+    for (uint32_t i = 0; i < n_omni; ++i) {
+        bin.boxes.push_back(sphere_light_box(d->omni_lights[i].position, d->omni_lights[i].radius));
+        prims.push_back({ITEM_LIGHT, i});
+    }
     for (uint32_t i = 0; i < d->num_dir_lights; ++i) {
         const rtc_dir_light& L = d->dir_lights[i];
         V3 P = v3(L.position), U = v3(L.u), Vv = v3(L.v);
         V3 hu = mul(0.5f, U), hv = mul(0.5f, Vv);
         V3 c[4] = {sub(sub(P, hu), hv), add(sub(P, hu), hv), sub(add(P, hu), hv), add(add(P, hu), hv)};
         bin.boxes.push_back(box_of(c, 4));
-        prims.push_back({ITEM_LIGHT, i});
+        prims.push_back({ITEM_LIGHT, n_omni + i});
+    }
+    for (uint32_t i = 0; i < n_spot; ++i) {
+        bin.boxes.push_back(sphere_light_box(d->spot_lights[i].position, d->spot_lights[i].radius));
+        prims.push_back({ITEM_LIGHT, n_omni + n_dir + i});
     }
     for (uint32_t i = 0; i < d->num_spheres; ++i) {
         const rtc_sphere& S = d->spheres[i];
@@ -335,17 +363,26 @@ rtc_status rtc_build_host_scene(const rtc_scene_desc* d, HostScene& H, uint32_t 
         mat_i.push_back(make_int4(m.kind, m.texture, 0, 0));
         mat_f.push_back(make_float4(fuzz, m.ior, m.intensity, m.directional ? 1.0f : 0.0f));
     }
-    std::vector<int32_t> light_mat(d->num_dir_lights);
-    for (uint32_t i = 0; i < d->num_dir_lights; ++i) {
-        const rtc_dir_light& L = d->dir_lights[i];
+    // Each light gets a solid texture of its colour and its own material, in light-list order:
+    //   omni:        diffuse_light(color, intensity, directional = false)   (omni_light.cuh:13-16)
+    //   directional: diffuse_light(color, intensity, directional = true)    (directional_light.cuh)
+    //   spot:        diffuse_spot_light(solid(color), ...) (spot_light.cuh:47-53), kind MAT_SPOT_LIGHT,
+    //                its cone read from the light record (mat_i.z = light index)
+    std::vector<int32_t> light_mat(nlights);
+    auto add_light_mat = [&](uint32_t li, int kind, const float* col, float intensity, float directional) {
         int32_t tex = (int32_t)tex_i.size();
         tex_i.push_back(make_int4(RTC_TEX_SOLID, 0, 0, 0));
-        tex_f.push_back(make_float4(L.color[0], L.color[1], L.color[2], 0.0f));
-        light_mat[i] = (int32_t)mat_i.size();
-        // directional_light: m_mat = new diffuse_light(m_color, intensity, true, invisible)
-        mat_i.push_back(make_int4(RTC_MAT_DIFFUSE_LIGHT, tex, 0, 0));
-        mat_f.push_back(make_float4(0.0f, 0.0f, L.intensity, 1.0f));
-    }
+        tex_f.push_back(make_float4(col[0], col[1], col[2], 0.0f));
+        light_mat[li] = (int32_t)mat_i.size();
+        mat_i.push_back(make_int4(kind, tex, (int)li, 0));
+        mat_f.push_back(make_float4(0.0f, 0.0f, intensity, directional));
+    };
+    for (uint32_t i = 0; i < n_omni; ++i)
+        add_light_mat(i, RTC_MAT_DIFFUSE_LIGHT, d->omni_lights[i].color, d->omni_lights[i].intensity, 0.0f);
+    for (uint32_t i = 0; i < n_dir; ++i)
+        add_light_mat(n_omni + i, RTC_MAT_DIFFUSE_LIGHT, d->dir_lights[i].color, d->dir_lights[i].intensity, 1.0f);
+    for (uint32_t i = 0; i < n_spot; ++i)
+        add_light_mat(n_omni + n_dir + i, MAT_SPOT_LIGHT, d->spot_lights[i].color, d->spot_lights[i].intensity, 1.0f);
     std::vector<int4> img_i;
     std::vector<uint8_t> img_bytes;
     for (uint32_t i = 0; i < d->num_images; ++i) {
@@ -358,21 +395,45 @@ rtc_status rtc_build_host_scene(const rtc_scene_desc* d, HostScene& H, uint32_t 
 
     // ---- per-kind arrays in leaf order ---------------------------------------------------------
     std::vector<uint32_t> items(bvh.order.size());
-    std::vector<float4> sph, tri, tri_n, tri_vn, quad, light(6 * (size_t)d->num_dir_lights);
+    std::vector<float4> sph, tri, tri_n, tri_vn, quad, light(6 * (size_t)nlights);
     std::vector<int2> sph_aux;
-    // global id bases
-    const uint32_t base_sph = d->num_dir_lights, base_quad = base_sph + d->num_spheres, base_tri = base_quad + d->num_quads;
-    for (uint32_t i = 0; i < d->num_dir_lights; ++i) {   // lights keep light-list order (index = light id)
+    // global id bases: the lights come first, in light-list order (index = light id = global id)
+    const uint32_t base_sph = nlights, base_quad = base_sph + d->num_spheres, base_tri = base_quad + d->num_quads;
+    for (uint32_t i = 0; i < n_dir; ++i) {
         const rtc_dir_light& L = d->dir_lights[i];
+        const uint32_t li = n_omni + i;
         V3 P = v3(L.position), U = v3(L.u), Vv = v3(L.v);
         PlanarPre pp = planar_pre(P, U, Vv);
-        float4* q = &light[6 * (size_t)i];
+        float4* q = &light[6 * (size_t)li];
         q[0] = make_float4(pp.normal.x, pp.normal.y, pp.normal.z, pp.D);
-        q[1] = make_float4(P.x, P.y, P.z, ibits(light_mat[i]));
-        q[2] = make_float4(U.x, U.y, U.z, ibits((int32_t)i));
+        q[1] = make_float4(P.x, P.y, P.z, ibits(light_mat[li]));
+        q[2] = make_float4(U.x, U.y, U.z, ibits((int32_t)li));
         q[3] = make_float4(Vv.x, Vv.y, Vv.z, L.invisible ? 1.0f : 0.0f);
         q[4] = make_float4(pp.w.x, pp.w.y, pp.w.z, pp.area);
         q[5] = make_float4(L.color[0], L.color[1], L.color[2], L.intensity);
+    }
+    // sphere lights (see rtc_dev.h): q4.w < 0 marks them
+    auto put_sphere_light = [&](uint32_t li, const float* pos, float radius, const float* dir, float cos_cutoff,
+                                float falloff, int32_t invisible, const float* col, float intensity) {
+        float4* q = &light[6 * (size_t)li];
+        q[0] = make_float4(pos[0], pos[1], pos[2], radius);
+        q[1] = make_float4(0.0f, 0.0f, 0.0f, ibits(light_mat[li]));
+        q[2] = make_float4(dir ? dir[0] : 0.0f, dir ? dir[1] : 0.0f, dir ? dir[2] : 0.0f, ibits((int32_t)li));
+        q[3] = make_float4(cos_cutoff, falloff, 0.0f, invisible ? 1.0f : 0.0f);
+        q[4] = make_float4(0.0f, 0.0f, 0.0f, -1.0f);
+        q[5] = make_float4(col[0], col[1], col[2], intensity);
+    };
+    for (uint32_t i = 0; i < n_omni; ++i) {
+        const rtc_omni_light& L = d->omni_lights[i];
+        put_sphere_light(i, L.position, L.radius, nullptr, 0.0f, 0.0f, L.invisible, L.color, L.intensity);
+    }
+    for (uint32_t i = 0; i < n_spot; ++i) {
+        const rtc_spot_light& L = d->spot_lights[i];
+        // m_cutoff = cos(degrees_to_radians(cutoff)) (spot_light.cuh:51): degrees * M_PI / 180.0f, all float
+        // (the reference's M_PI is a float literal, misc/constants.cuh:35), then the float cosine
+        const float rad = L.cutoff * 3.14159265358979323846f / 180.0f;
+        put_sphere_light(n_omni + n_dir + i, L.position, L.radius, L.direction, std::cos(rad), L.falloff, L.invisible,
+                         L.color, L.intensity);
     }
     for (size_t k = 0; k < bvh.order.size(); ++k) {
         const PrimRef& pr = prims[bvh.order[k]];
@@ -482,7 +543,7 @@ rtc_status rtc_build_host_scene(const rtc_scene_desc* d, HostScene& H, uint32_t 
     D.num_nodes = bvh.num_nodes;
     D.num_nodes8 = bvh.num_nodes8;
     D.num_items = (uint32_t)items.size();
-    D.num_lights = d->num_dir_lights;
+    D.num_lights = nlights;
     D.num_materials = (uint32_t)mat_i.size();
     D.num_textures = (uint32_t)tex_i.size();
     D.num_images = (uint32_t)img_i.size();
@@ -498,7 +559,7 @@ rtc_status rtc_build_host_scene(const rtc_scene_desc* d, HostScene& H, uint32_t 
     H.cam = d->camera;
     H.info = rtc_scene_info{};
     H.info.num_primitives = (uint32_t)nprims;
-    H.info.num_lights = d->num_dir_lights;
+    H.info.num_lights = nlights;
     H.info.num_nodes = bvh.num_nodes;
     H.info.max_leaf_size = bvh.max_leaf_seen;
     H.info.device_bytes = total;

@@ -21,8 +21,12 @@
 //   tri_n      float4 (middle_normal.xyz, -)                    fetched once per final hit only
 //   tri_vn     3 x float4 vertex normals (unit_vector'd) for smooth triangles
 //   quad       5 x float4: (n.xyz, D) (Q.xyz, mat) (u.xyz, gid) (v.xyz, -) (w.xyz, -)
-//   light      6 x float4: (n.xyz, D) (P.xyz, mat) (u.xyz, gid) (v.xyz, invisible) (w.xyz, area)
-//                          (emit.rgb * 1, intensity)       - directional lights in light-list order
+//   light      6 x float4 per light, in light-list order (omni, directional, spot lights):
+//              directional (quad): (n.xyz, D) (P.xyz, mat) (u.xyz, gid) (v.xyz, invisible) (w.xyz, area)
+//                                  (emit.rgb, intensity)
+//              omni / spot (sphere): (center.xyz, radius) (-, -, -, mat) (spot direction.xyz, gid)
+//                                  (cos cutoff, falloff, -, invisible) (-, -, -, -1: the sphere marker)
+//                                  (emit.rgb, intensity)
 //   materials  int4 (kind, texture, -, -) + float4 (fuzz, ior, intensity, directional)
 //   textures   int4 (kind, even, odd, image) + float4 (color.rgb, inv_scale)
 //   images     int4 (byte offset, width, height, -) into image_bytes
@@ -34,6 +38,8 @@
 namespace rtc {
 
 enum ItemKind : uint32_t { ITEM_SPHERE = 0, ITEM_QUAD = 1, ITEM_TRI = 2, ITEM_LIGHT = 3 };
+// Material kinds past the public rtc_material_kind values: a spot light's diffuse_spot_light.
+constexpr int MAT_SPOT_LIGHT = 4;
 constexpr int LEAF_COUNT_BITS = 5;
 constexpr int MAX_LEAF = 31;
 constexpr int TRAVERSAL_STACK = 64;

@@ -99,10 +99,31 @@ __device__ __forceinline__ V3 onb_local(const Onb& b, V3 a) {
     return add(add(mul(a.x, b.u), mul(a.y, b.v)), mul(a.z, b.w));
 }
 
-// directional_light::random (directional_light.cuh:165-171): P + (U-0.5)*u + (U-0.5)*v - o
+// random_to_sphere (gpu_randomizer.cuh:82-93): z = 1 + r2 (sqrt(1 - R^2/d^2) - 1), phi = 2 M_PI r1 in float
+// (the reference's M_PI is a float literal, misc/constants.cuh:35), x = cos(phi) sqrt(1 - z^2),
+// y = sin(phi) sqrt(1 - z^2).
+template <bool FLOAT_TRIG, class R>
+__device__ __forceinline__ V3 random_to_sphere(R& rng, float radius, float distance_squared) {
+    const float r1 = rng.uniform();
+    const float r2 = rng.uniform();
+    const float z = 1.0f + r2 * (sqrtf(1.0f - radius * radius / distance_squared) - 1.0f);
+    const float phi = 2.0f * 3.14159265358979323846f * r1;
+    float c, s;
+    cos_sin<FLOAT_TRIG>(phi, c, s);
+    return v3(c * sqrtf(1.0f - z * z), s * sqrtf(1.0f - z * z), z);
+}
+
+// directional_light::random (directional_light.cuh:165-171): P + (U-0.5)*u + (U-0.5)*v - o; for omni
+// and spot lights omni_light::random (omni_light.cuh:117-124): onb(center - o).local(random_to_sphere).
 template <int ORDER, class R>
 __device__ __forceinline__ V3 light_random(const DevScene& S, uint32_t li, V3 o, R& rng) {
     const float4* q = S.light + 6 * (size_t)li;
+    if (__ldg(q + 4).w < 0.0f) {
+        const float4 c = __ldg(q);
+        const V3 dir = sub(v3(c.x, c.y, c.z), o);
+        const Onb b = build_from_w(dir);
+        return onb_local(b, random_to_sphere<ORDER == 0>(rng, c.w, lensq(dir)));
+    }
     float4 P = __ldg(q + 1), U = __ldg(q + 2), Vv = __ldg(q + 3);
     float ru, rv;
     draw2<ORDER>(rng, ru, rv);
@@ -199,6 +220,26 @@ __device__ __forceinline__ bool shade_bounce(const DevScene& S, Ray& r, bool hit
             RGB tv = texture_value(S, mi.y, h.u, h.v, h.p, status);
             em = rgb(tv.r * mf.z, tv.g * mf.z, tv.b * mf.z);
         }
+    } else if (mi.x == MAT_SPOT_LIGHT) {
+        // diffuse_spot_light::emitted (diffuse_spot_light.cuh:33-49).  Back face: RGBA(0,0,0,0) when
+        // invisible, else RGBA(1,1,1,0) (both re-hit; the product with the attenuation adds 0 or 1);
+        // outside the cone RGBA(1,1,1,1); inside texture * (intensity * pow(cos, falloff)).
+        const float4* q = S.light + 6 * (size_t)mi.z;
+        const float4 sd = __ldg(q + 2), cone = __ldg(q + 3);
+        if (!h.front) {
+            em_alpha0 = true;
+            if (cone.w == 0.0f) em = rgb(1.f, 1.f, 1.f);
+        } else {
+            const float cos_theta = dot(unit(r.d), unit(v3(sd.x, sd.y, sd.z)));
+            if (cos_theta < cone.x) {
+                em = rgb(1.f, 1.f, 1.f);
+            } else {
+                const float attn = FT ? powf(cos_theta, cone.y) : (float)pow((double)cos_theta, (double)cone.y);
+                const float k = mf.z * attn;
+                RGB tv = texture_value(S, mi.y, h.u, h.v, h.p, status);
+                em = rgb(tv.r * k, tv.g * k, tv.b * k);
+            }
+        }
     }
     if (em_alpha0) {
         // "invisible" re-hit from just behind the light (camera.cuh:177-183); rec is replaced only
@@ -216,7 +257,7 @@ __device__ __forceinline__ bool shade_bounce(const DevScene& S, Ray& r, bool hit
     result.r += att.r * em.r;
     result.g += att.g * em.g;
     result.b += att.b * em.b;
-    if (mi.x == 3) return false;   // diffuse_light::scatter -> material::scatter returns false
+    if (mi.x == 3 || mi.x == MAT_SPOT_LIGHT) return false;   // lights: material::scatter returns false
 
     if (mi.x == 1) {
         // metal::scatter (metal.cuh:57-64)

@@ -263,12 +263,18 @@ __device__ __forceinline__ void test_leaf(const DevScene& S, int32_t child, V3 o
             if (idx >= S.num_lights) { status |= STATUS_BAD_ITEM; break; }
             const float4* q = S.light + 6 * (size_t)idx;
             float a, b;
-            float4 q3 = __ldg(q + 3);
-            if (planar_t(__ldg(q), __ldg(q + 1), __ldg(q + 2), q3, __ldg(q + 4), o, d, tmin, best_t, true, t, a, b)) {
-                // "Hide light source": invisible lights are skipped when depth == max_depth
-                // (directional_light.cuh:106)
-                if (!(q3.w != 0.0f && hide_invisible)) { best_t = t; best_item = it; }
+            const float4 q3 = __ldg(q + 3), q4 = __ldg(q + 4);
+            bool hitl;
+            if (q4.w < 0.0f) {
+                // omni_light::hit / spot_light::hit (omni_light.cuh:55-83): the sphere quadratic, strict
+                const float4 sp = __ldg(q);
+                hitl = EXACT ? sphere_t_exact(sp, o, d, tmin, best_t, t) : sphere_t(sp, o, d, tmin, best_t, t);
+            } else {
+                hitl = planar_t(__ldg(q), __ldg(q + 1), __ldg(q + 2), q3, q4, o, d, tmin, best_t, true, t, a, b);
             }
+            // "Hide light source": invisible lights are skipped when depth == max_depth
+            // (directional_light.cuh:106, omni_light.cuh:76-80)
+            if (hitl && !(q3.w != 0.0f && hide_invisible)) { best_t = t; best_item = it; }
         } break;
         }
     }
@@ -484,6 +490,16 @@ __device__ __forceinline__ void finalize_hit(const DevScene& S, uint32_t it, flo
     case ITEM_LIGHT: {
         const float4* q = kind == ITEM_QUAD ? S.quad + 5 * (size_t)idx : S.light + 6 * (size_t)idx;
         float4 q0 = __ldg(q), q1 = __ldg(q + 1), q2 = __ldg(q + 2), q3 = __ldg(q + 3), q4 = __ldg(q + 4);
+        if (kind == ITEM_LIGHT && q4.w < 0.0f) {
+            // omni / spot light (omni_light.cuh:85-102): outward normal (p - c) / radius; its texture is
+            // a solid colour, so the sphere uv the reference also computes is not needed
+            h.p = at(o, d, t);
+            h.mat = __float_as_int(q1.w);
+            set_face_normal(h, d, divs(sub(h.p, v3(q0.x, q0.y, q0.z)), q0.w));
+            h.u = 0.0f;
+            h.v = 0.0f;
+            break;
+        }
         V3 n = v3(q0.x, q0.y, q0.z);
         V3 ip = at(o, d, t);
         V3 pl = sub(ip, v3(q1.x, q1.y, q1.z));
@@ -594,11 +610,20 @@ __device__ __forceinline__ RGB background(const DevScene& S, V3 dir) {
     return rgb(__ldg(px), __ldg(px + 1), __ldg(px + 2));
 }
 
-// directional_light::pdf_value (directional_light.cuh:147-158) for light `li` seen from o along v.
+// directional_light::pdf_value (directional_light.cuh:147-158) for light `li` seen from o along v;
+// omni_light::pdf_value / spot_light::pdf_value (omni_light.cuh:104-115): 1 / the solid angle of the
+// sphere, 2 * M_PI * (1 - cos_theta_max), all in float: the reference's M_PI is a float literal
+// (misc/constants.cuh:35).
 __device__ __forceinline__ float light_pdf_value(const DevScene& S, uint32_t li, V3 o, V3 v) {
     const float4* q = S.light + 6 * (size_t)li;
     float4 q0 = __ldg(q), q4 = __ldg(q + 4);
     float t, a, b;
+    if (q4.w < 0.0f) {
+        if (!sphere_t(q0, o, v, 0.00001f, INFINITY, t)) return 0.0f;
+        const float ctm = sqrtf(1.0f - q0.w * q0.w / lensq(sub(v3(q0.x, q0.y, q0.z), o)));
+        const float solid_angle = 2.0f * 3.14159265358979323846f * (1.0f - ctm);
+        return 1.0f / solid_angle;
+    }
     if (!planar_t(q0, __ldg(q + 1), __ldg(q + 2), __ldg(q + 3), q4, o, v, 0.00001f, INFINITY, true, t, a, b)) return 0.0f;
     V3 n = v3(q0.x, q0.y, q0.z);
     V3 nrm = dot(v, n) < 0.0f ? n : neg(n);

@@ -60,6 +60,16 @@ class rtc_dir_light(C.Structure):
                 ("invisible", C.c_int32)]
 
 
+class rtc_omni_light(C.Structure):
+    _fields_ = [("position", F3), ("radius", C.c_float), ("color", F3), ("intensity", C.c_float),
+                ("invisible", C.c_int32)]
+
+
+class rtc_spot_light(C.Structure):
+    _fields_ = [("position", F3), ("direction", F3), ("cutoff", C.c_float), ("falloff", C.c_float),
+                ("intensity", C.c_float), ("radius", C.c_float), ("color", F3), ("invisible", C.c_int32)]
+
+
 class rtc_mesh(C.Structure):
     _fields_ = [("vertices", C.POINTER(C.c_float)), ("indices", C.POINTER(C.c_uint32)),
                 ("normals", C.POINTER(C.c_float)), ("uvs", C.POINTER(C.c_float)),
@@ -85,7 +95,9 @@ class rtc_scene_desc(C.Structure):
                 ("spheres", C.POINTER(rtc_sphere)), ("num_spheres", C.c_uint32),
                 ("quads", C.POINTER(rtc_quad)), ("num_quads", C.c_uint32),
                 ("meshes", C.POINTER(rtc_mesh)), ("num_meshes", C.c_uint32),
-                ("camera", rtc_camera), ("background", rtc_background)]
+                ("camera", rtc_camera), ("background", rtc_background),
+                ("omni_lights", C.POINTER(rtc_omni_light)), ("num_omni_lights", C.c_uint32),
+                ("spot_lights", C.POINTER(rtc_spot_light)), ("num_spot_lights", C.c_uint32)]
 
 
 class rtc_render_params(C.Structure):
@@ -214,6 +226,8 @@ class Scene:
     images: list = field(default_factory=list)        # (H, W, 3) uint8 arrays, top row first
     materials: list = field(default_factory=list)
     dir_lights: list = field(default_factory=list)
+    omni_lights: list = field(default_factory=list)
+    spot_lights: list = field(default_factory=list)
     spheres: list = field(default_factory=list)
     quads: list = field(default_factory=list)
     meshes: list = field(default_factory=list)        # dicts with numpy arrays
@@ -270,6 +284,19 @@ class Scene:
     def dir_light(self, position, u, v, rgb, intensity=1.0, invisible=True) -> int:
         self.dir_lights.append((tuple(position), tuple(u), tuple(v), tuple(rgb), float(intensity), int(bool(invisible))))
         return len(self.dir_lights) - 1
+
+    def omni_light(self, position, radius, rgb, intensity=1.0, invisible=True) -> int:
+        """An emitting sphere (omni_light); the light list puts omni lights first."""
+        self.omni_lights.append((tuple(position), float(radius), tuple(rgb), float(intensity), int(bool(invisible))))
+        return len(self.omni_lights) - 1
+
+    def spot_light(self, position, direction, cutoff_deg, falloff, rgb, intensity=1.0, radius=0.1,
+                   invisible=True) -> int:
+        """An emitting sphere lit within `cutoff_deg` of `direction` (spot_light); listed after the
+        directional lights."""
+        self.spot_lights.append((tuple(position), tuple(direction), float(cutoff_deg), float(falloff), float(intensity),
+                                 float(radius), tuple(rgb), int(bool(invisible))))
+        return len(self.spot_lights) - 1
 
     def sphere(self, center, radius, mat) -> int:
         self.spheres.append((tuple(center), float(radius), int(mat)))
@@ -334,6 +361,9 @@ class SceneDesc:
             imgs.append(rtc_image(im.ctypes.data_as(C.POINTER(C.c_uint8)), im.shape[1], im.shape[0]))
         mats = [rtc_material(*m) for m in s.materials]
         lights = [rtc_dir_light(_f3(p), _f3(u), _f3(v), _f3(c), i, inv) for (p, u, v, c, i, inv) in s.dir_lights]
+        omnis = [rtc_omni_light(_f3(p), r, _f3(c), i, inv) for (p, r, c, i, inv) in s.omni_lights]
+        spots = [rtc_spot_light(_f3(p), _f3(d), cu, fo, i, r, _f3(c), inv)
+                 for (p, d, cu, fo, i, r, c, inv) in s.spot_lights]
         spheres = [rtc_sphere(_f3(c), r, m) for (c, r, m) in s.spheres]
         quads = [rtc_quad(_f3(q), _f3(u), _f3(v), m) for (q, u, v, m) in s.quads]
         meshes = []
@@ -361,12 +391,12 @@ class SceneDesc:
         cbg = rtc_background(bg["kind"], _f3(bg.get("color", (0, 0, 0))), _f3(bg.get("top", (0, 0, 0))), env_ptr, ew, eh)
         self.arrays = [_carray(rtc_texture, texs), _carray(rtc_image, imgs), _carray(rtc_material, mats),
                        _carray(rtc_dir_light, lights), _carray(rtc_sphere, spheres), _carray(rtc_quad, quads),
-                       _carray(rtc_mesh, meshes)]
+                       _carray(rtc_mesh, meshes), _carray(rtc_omni_light, omnis), _carray(rtc_spot_light, spots)]
         a = self.arrays
         self.desc = rtc_scene_desc(a[0], len(texs), a[1], len(imgs), a[2], len(mats), a[3], len(lights),
                                    a[4], len(spheres), a[5], len(quads), a[6], len(meshes),
                                    rtc_camera(_f3(cam.look_from), _f3(cam.look_at), _f3(cam.up), cam.vfov, cam.aspect,
-                                              cam.aperture, cam.focus), cbg)
+                                              cam.aperture, cam.focus), cbg, a[7], len(omnis), a[8], len(spots))
         self._keep = keep
         self.scene = s
 

@@ -127,6 +127,32 @@ typedef struct rtc_dir_light {
     int32_t invisible;   /* hidden to primary rays: directional_light.cuh:106 */
 } rtc_dir_light;
 
+/* Omni light (omni_light, lights/omni_light.cuh): an emitting sphere; diffuse_light material that
+ * emits color * intensity from both faces; sampled by solid angle (random_to_sphere); hidden to primary
+ * rays when invisible. */
+typedef struct rtc_omni_light {
+    float position[3];
+    float radius;
+    float color[3];
+    float intensity;
+    int32_t invisible;
+} rtc_omni_light;
+
+/* Spot light (spot_light, lights/spot_light.cuh, with diffuse_spot_light, materials/
+ * diffuse_spot_light.cuh): an emitting sphere whose front faces emit color * intensity *
+ * cos^falloff toward rays within `cutoff` degrees of `direction` (and white outside it, as the
+ * reference does); sampled like an omni light. */
+typedef struct rtc_spot_light {
+    float position[3];
+    float direction[3];
+    float cutoff;        /* degrees */
+    float falloff;       /* exponent */
+    float intensity;
+    float radius;
+    float color[3];
+    int32_t invisible;
+} rtc_spot_light;
+
 /* Indexed triangle mesh; each triangle becomes one reference `triangle` (triangle.cuh:87-185). */
 typedef struct rtc_mesh {
     const float* vertices;      /* 3 floats per vertex                                             */
@@ -176,6 +202,10 @@ typedef struct rtc_scene_desc {
     const rtc_mesh* meshes;           uint32_t num_meshes;
     rtc_camera camera;
     rtc_background background;
+    /* Further lights.  The light list holds omni lights, then directional lights, then spot lights, as
+     * load_scene adds them (gpu.cu:504-523); that order also numbers them before the spheres. */
+    const rtc_omni_light* omni_lights;  uint32_t num_omni_lights;
+    const rtc_spot_light* spot_lights;  uint32_t num_spot_lights;
 } rtc_scene_desc;
 
 /* Triangle geometry read from a Wavefront OBJ file, laid out for rtc_mesh: per-vertex positions (and

@@ -11,8 +11,9 @@
 //     colours; odd lands in m_even as scene_factory does, scene_factory.cuh:619-629), image;
 //   * an object whose material does not resolve is skipped, as `if (mat)` skips it (gpu.cu:531).
 // OBJ meshes are read through an optional loader callback (with this library: rtc_load_obj).
-// Primitives the B200 path does not cover (planes, boxes, cones, cylinders, disks, tori, volumes,
-// omni/spot lights) and transforms are reported in `skipped`.
+// Lights map to omni, directional and spot lights in the light list's order.  Primitives the B200 path
+// does not cover (planes, boxes, cones, cylinders, disks, tori, volumes) and transforms are reported in
+// `skipped`.
 // Image textures need decoded RGB8 pixels: pass `load_image(filepath, &w, &h)` returning a pointer
 // that stays valid while the description is used (the reference decodes with stbi_load, gpu.cu:1743).
 #pragma once
@@ -31,6 +32,8 @@ struct SceneHolder {
     std::vector<rtc_image> images;
     std::vector<rtc_material> materials;
     std::vector<rtc_dir_light> dir_lights;
+    std::vector<rtc_omni_light> omni_lights;
+    std::vector<rtc_spot_light> spot_lights;
     std::vector<rtc_sphere> spheres;
     std::vector<rtc_quad> quads;
     std::vector<rtc_mesh> meshes;
@@ -49,6 +52,10 @@ struct SceneHolder {
         desc.num_materials = (uint32_t)materials.size();
         desc.dir_lights = dir_lights.data();
         desc.num_dir_lights = (uint32_t)dir_lights.size();
+        desc.omni_lights = omni_lights.data();
+        desc.num_omni_lights = (uint32_t)omni_lights.size();
+        desc.spot_lights = spot_lights.data();
+        desc.num_spot_lights = (uint32_t)spot_lights.size();
         desc.spheres = spheres.data();
         desc.num_spheres = (uint32_t)spheres.size();
         desc.quads = quads.data();
@@ -159,7 +166,17 @@ const rtc_scene_desc* from_sceneconfig(const SceneConfig& cfg, SceneHolder& out,
     };
 
     const auto& L = cfg.lightsCfg;
-    if (L.omniLightCount) out.skipped.push_back("omni lights");
+    // lightsCfg -> light list: omni, directional, spot (load_scene, gpu.cu:504-523)
+    for (int i = 0; i < L.omniLightCount; ++i) {
+        const auto& o = L.omniLights[i];
+        rtc_omni_light l{};
+        put3(l.position, o.position);
+        l.radius = o.radius;
+        putc3(l.color, o.rgb);
+        l.intensity = o.intensity;
+        l.invisible = o.invisible ? 1 : 0;
+        out.omni_lights.push_back(l);
+    }
     for (int i = 0; i < L.dirLightCount; ++i) {
         const auto& d = L.dirLights[i];
         rtc_dir_light l{};
@@ -171,7 +188,19 @@ const rtc_scene_desc* from_sceneconfig(const SceneConfig& cfg, SceneHolder& out,
         l.invisible = d.invisible ? 1 : 0;
         out.dir_lights.push_back(l);
     }
-    if (L.spotLightCount) out.skipped.push_back("spot lights");
+    for (int i = 0; i < L.spotLightCount; ++i) {
+        const auto& sp = L.spotLights[i];
+        rtc_spot_light l{};
+        put3(l.position, sp.position);
+        put3(l.direction, sp.direction);
+        l.cutoff = sp.cutoff;
+        l.falloff = sp.falloff;
+        l.intensity = sp.intensity;
+        l.radius = sp.radius;
+        putc3(l.color, sp.rgb);
+        l.invisible = sp.invisible ? 1 : 0;
+        out.spot_lights.push_back(l);
+    }
 
     const auto& P = cfg.primitivesCfg;
     for (int i = 0; i < P.spherePrimitiveCount; ++i) {

@@ -34,6 +34,8 @@
 #include "primitives/triangle.cuh"
 #include "lights/light.cuh"
 #include "lights/directional_light.cuh"
+#include "lights/omni_light.cuh"
+#include "lights/spot_light.cuh"
 #include "cameras/camera.cuh"
 #include "cameras/perspective_camera.cuh"
 
@@ -231,7 +233,7 @@ void* refh_scene_create(const rtc_scene_desc* d, int bvh_kind) {
     ref_scene* s = new ref_scene();
     s->cam_desc = d->camera;
     s->bg = d->background;
-    uint64_t total = (uint64_t)d->num_dir_lights + d->num_spheres + d->num_quads;
+    uint64_t total = (uint64_t)d->num_omni_lights + d->num_dir_lights + d->num_spot_lights + d->num_spheres + d->num_quads;
     for (uint32_t m = 0; m < d->num_meshes; ++m) total += d->meshes[m].num_triangles;
     s->names.assign(total + 1, 0);
     size_t k = 0;
@@ -240,10 +242,25 @@ void* refh_scene_create(const rtc_scene_desc* d, int bvh_kind) {
     auto mat_of = [&](int idx) -> material* {
         return (idx >= 0 && (uint32_t)idx < d->num_materials) ? mats[idx] : nullptr;
     };
+    // lights in load_scene's order: omni, directional, spot (gpu.cu:504-523)
+    for (uint32_t i = 0; i < d->num_omni_lights; ++i, ++k) {
+        const rtc_omni_light& L = d->omni_lights[i];
+        auto* h = new omni_light(v3(L.position), L.radius, L.intensity, color(L.color[0], L.color[1], L.color[2]),
+                                 &s->names[k], L.invisible != 0);
+        s->objects.push_back(h);
+        s->lights.add(h);
+    }
     for (uint32_t i = 0; i < d->num_dir_lights; ++i, ++k) {
         const rtc_dir_light& L = d->dir_lights[i];
         auto* h = new directional_light(v3(L.position), v3(L.u), v3(L.v), L.intensity,
                                         color(L.color[0], L.color[1], L.color[2]), &s->names[k], L.invisible != 0);
+        s->objects.push_back(h);
+        s->lights.add(h);
+    }
+    for (uint32_t i = 0; i < d->num_spot_lights; ++i, ++k) {
+        const rtc_spot_light& L = d->spot_lights[i];
+        auto* h = new spot_light(v3(L.position), v3(L.direction), L.cutoff, L.falloff, L.intensity, L.radius,
+                                 color(L.color[0], L.color[1], L.color[2]), &s->names[k], L.invisible != 0);
         s->objects.push_back(h);
         s->lights.add(h);
     }
@@ -411,7 +428,8 @@ int refh_get_int(uint32_t seed, int lo, int hi, int64_t n, int32_t* out) {
 
 // The reference's multi-draw helpers as this (g++) build evaluates them; 3 floats per call:
 // which = 0 random_in_unit_disk, 1 random_in_unit_sphere, 2 random_cosine_direction,
-//         3 directional_light::random for light (0,0,0), u=(1,0,0), v=(0,1,0) seen from the origin.
+//         3 directional_light::random for light (0,0,0), u=(1,0,0), v=(0,1,0) seen from the origin,
+//         4 omni_light::random for a light at (0.3,-0.2,0.1), radius 0.5, seen from (1.3,0.7,-2.1).
 int refh_sampler_draws(int which, uint32_t seed, int64_t n, float* out) {
     thrust::minstd_rand rng(seed);
     directional_light L(point3(0, 0, 0), vector3(1, 0, 0), vector3(0, 1, 0), 1.0f, color(1, 1, 1));
@@ -422,6 +440,11 @@ int refh_sampler_draws(int which, uint32_t seed, int64_t n, float* out) {
         case 1: p = random_in_unit_sphere(rng); break;
         case 2: p = random_cosine_direction(rng); break;
         case 3: p = L.random(point3(0, 0, 0), rng); break;
+        case 4: {   // omni_light::random for a light at (0.3, -0.2, 0.1), radius 0.5, seen from (1.3, 0.7, -2.1)
+            static omni_light O(point3(0.3f, -0.2f, 0.1f), 0.5f, 1.0f, color(1, 1, 1));
+            p = O.random(point3(1.3f, 0.7f, -2.1f), rng);
+        } break;
+        case 5: p = random_to_sphere(rng, 0.5f, 4.0f); break;
         default: g_err = "bad sampler"; return 1;
         }
         out[3 * k] = p.x; out[3 * k + 1] = p.y; out[3 * k + 2] = p.z;

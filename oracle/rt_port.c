@@ -41,6 +41,7 @@ static inline float f_cos(float x) { return g_trig ? (float)cos((double)x) : cos
 static inline float f_sin(float x) { return g_trig ? (float)sin((double)x) : sinf(x); }
 static inline float f_acos(float x) { return g_trig ? (float)acos((double)x) : acosf(x); }
 static inline float f_atan2(float y, float x) { return g_trig ? (float)atan2((double)y, (double)x) : atan2f(y, x); }
+static inline float f_pow(float x, float y) { return g_trig ? (float)pow((double)x, (double)y) : powf(x, y); }
 
 /* ---------------------------------------------------------------------------------------------- */
 /* vectors: glm semantics (func_geometric.inl), misc/vector3.cuh                                  */
@@ -116,6 +117,7 @@ typedef struct {
     int mat;          /* material index (lights: index into the appended light materials) */
     int light;        /* light index for K_LIGHT */
     int invisible;
+    int sphere_light; /* omni / spot light: a sphere (a = center, rad) */
     v3 a, b, c;       /* sphere: a=center, r in rad;  quad/light: a=Q|P, b=u, c=v;  tri: a=v0, b=v0v1, c=v0v2 */
     float rad;
     v3 normal, w;     /* planar */
@@ -126,7 +128,12 @@ typedef struct {
 } prim_t;
 
 typedef struct { int kind; float col[3]; float inv_scale; int even, odd, image; } tex_t;
-typedef struct { int kind; int tex; float fuzz, ior, intensity; int directional; } mat_t;
+/* kind MAT_SPOT (4): diffuse_spot_light (materials/diffuse_spot_light.cuh), cone in dir/cos_cutoff/falloff */
+enum { MAT_SPOT = 4 };
+typedef struct {
+    int kind; int tex; float fuzz, ior, intensity; int directional;
+    v3 dir; float cos_cutoff, falloff; int invisible;
+} mat_t;
 typedef struct { float lo[3], hi[3]; int left, right, first, count; } node_t;
 
 typedef struct {
@@ -194,13 +201,15 @@ void* port_scene_create(const rtc_scene_desc* d) {
     if (!s || !d) { snprintf(g_err, sizeof g_err, "bad argument"); free(s); return NULL; }
     int ntri = 0;
     for (uint32_t m = 0; m < d->num_meshes; ++m) ntri += (int)d->meshes[m].num_triangles;
-    s->nprims = (int)(d->num_dir_lights + d->num_spheres + d->num_quads) + ntri;
+    const int n_omni = (int)d->num_omni_lights, n_dir = (int)d->num_dir_lights, n_spot = (int)d->num_spot_lights;
+    const int n_lights = n_omni + n_dir + n_spot;   /* light list: omni, directional, spot (gpu.cu:504-523) */
+    s->nprims = n_lights + (int)(d->num_spheres + d->num_quads) + ntri;
     s->prims = (prim_t*)calloc((size_t)s->nprims + 1, sizeof(prim_t));
-    s->ntex = (int)d->num_textures + (int)d->num_dir_lights;
+    s->ntex = (int)d->num_textures + n_lights;
     s->tex = (tex_t*)calloc((size_t)s->ntex + 1, sizeof(tex_t));
-    s->nmat = (int)d->num_materials + (int)d->num_dir_lights;
+    s->nmat = (int)d->num_materials + n_lights;
     s->mat = (mat_t*)calloc((size_t)s->nmat + 1, sizeof(mat_t));
-    s->nlights = (int)d->num_dir_lights;
+    s->nlights = n_lights;
     s->lights = (int*)calloc((size_t)s->nlights + 1, sizeof(int));
     for (uint32_t i = 0; i < d->num_textures; ++i) {
         const rtc_texture* t = &d->textures[i];
@@ -221,24 +230,57 @@ void* port_scene_create(const rtc_scene_desc* d) {
     s->cam = d->camera;
     s->bg = d->background;
     int k = 0;
+    /* omni and spot lights: spheres (omni_light.cuh / spot_light.cuh) */
+    for (int j = 0; j < n_omni + n_spot; ++j) {
+        const int is_spot = j >= n_omni, li = is_spot ? n_omni + n_dir + (j - n_omni) : j;
+        const float* pos = is_spot ? d->spot_lights[j - n_omni].position : d->omni_lights[j].position;
+        const float radius = is_spot ? d->spot_lights[j - n_omni].radius : d->omni_lights[j].radius;
+        const float* col = is_spot ? d->spot_lights[j - n_omni].color : d->omni_lights[j].color;
+        const float inten = is_spot ? d->spot_lights[j - n_omni].intensity : d->omni_lights[j].intensity;
+        prim_t* p = &s->prims[li];
+        p->kind = K_LIGHT; p->light = li; p->sphere_light = 1;
+        p->invisible = is_spot ? d->spot_lights[j - n_omni].invisible : d->omni_lights[j].invisible;
+        p->a = Vp(pos); p->rad = radius;
+        int ti = (int)d->num_textures + li, mi = (int)d->num_materials + li;
+        s->tex[ti].kind = RTC_TEX_SOLID; memcpy(s->tex[ti].col, col, 12);
+        s->mat[mi].tex = ti; s->mat[mi].intensity = inten;
+        if (is_spot) {
+            const rtc_spot_light* L = &d->spot_lights[j - n_omni];
+            /* diffuse_spot_light(solid(color), pos, dir, cos(degrees_to_radians(cutoff)), falloff, ...) */
+            float rad = L->cutoff * PI_F / 180.0f;   /* degrees_to_radians with the float M_PI */
+            s->mat[mi].kind = MAT_SPOT; s->mat[mi].directional = 1;
+            s->mat[mi].dir = Vp(L->direction); s->mat[mi].cos_cutoff = cosf(rad); s->mat[mi].falloff = L->falloff;
+            s->mat[mi].invisible = L->invisible;
+        } else {
+            /* m_mat = new diffuse_light(m_color, intensity, false, invisible) (omni_light.cuh:16) */
+            s->mat[mi].kind = RTC_MAT_DIFFUSE_LIGHT; s->mat[mi].directional = 0;
+        }
+        p->mat = mi;
+        s->lights[li] = li;
+        float r = fabsf(radius);
+        for (int q = 0; q < 3; ++q) { p->lo[q] = FLT_MAX; p->hi[q] = -FLT_MAX; }
+        box_grow(p->lo, p->hi, vsub(p->a, V(r, r, r))); box_grow(p->lo, p->hi, vadd(p->a, V(r, r, r)));
+    }
+    k = n_omni;
     for (uint32_t i = 0; i < d->num_dir_lights; ++i, ++k) {
         const rtc_dir_light* L = &d->dir_lights[i];
         prim_t* p = &s->prims[k];
-        p->kind = K_LIGHT; p->light = (int)i; p->invisible = L->invisible;
+        p->kind = K_LIGHT; p->light = k; p->invisible = L->invisible;
         p->a = Vp(L->position); p->b = Vp(L->u); p->c = Vp(L->v);
         planar_init(p);
-        int ti = (int)d->num_textures + (int)i, mi = (int)d->num_materials + (int)i;
+        int ti = (int)d->num_textures + k, mi = (int)d->num_materials + k;
         s->tex[ti].kind = RTC_TEX_SOLID; memcpy(s->tex[ti].col, L->color, 12);
         /* m_mat = new diffuse_light(m_color, intensity, true, invisible) (directional_light.cuh:48) */
         s->mat[mi].kind = RTC_MAT_DIFFUSE_LIGHT; s->mat[mi].tex = ti; s->mat[mi].intensity = L->intensity;
         s->mat[mi].directional = 1;
         p->mat = mi;
-        s->lights[i] = k;
+        s->lights[k] = k;
         v3 hu = vscale(0.5f, p->b), hv = vscale(0.5f, p->c);
         for (int q = 0; q < 3; ++q) { p->lo[q] = FLT_MAX; p->hi[q] = -FLT_MAX; }
         box_grow(p->lo, p->hi, vsub(vsub(p->a, hu), hv)); box_grow(p->lo, p->hi, vadd(vsub(p->a, hu), hv));
         box_grow(p->lo, p->hi, vsub(vadd(p->a, hu), hv)); box_grow(p->lo, p->hi, vadd(vadd(p->a, hu), hv));
     }
+    k = n_lights;   /* the spot lights sit after the directional ones */
     for (uint32_t i = 0; i < d->num_spheres; ++i, ++k) {
         const rtc_sphere* S = &d->spheres[i];
         prim_t* p = &s->prims[k];
@@ -383,8 +425,12 @@ static int prim_t_test(const prim_t* p, v3 o, v3 d, float tmin, float tmax, int 
     case K_SPHERE: return exact ? sphere_t_exact(p, o, d, tmin, tmax, t) : sphere_t(p, o, d, tmin, tmax, t);
     case K_QUAD: return planar_t(p, o, d, tmin, tmax, 0, t, &a, &b);
     case K_LIGHT:
-        if (!planar_t(p, o, d, tmin, tmax, 1, t, &a, &b)) return 0;
-        return !(p->invisible && hide);   /* directional_light.cuh:106 */
+        if (p->sphere_light) {   /* omni_light::hit (omni_light.cuh:55-83) */
+            if (!(exact ? sphere_t_exact(p, o, d, tmin, tmax, t) : sphere_t(p, o, d, tmin, tmax, t))) return 0;
+        } else if (!planar_t(p, o, d, tmin, tmax, 1, t, &a, &b)) {
+            return 0;
+        }
+        return !(p->invisible && hide);   /* directional_light.cuh:106, omni_light.cuh:76-80 */
     default: return tri_t(p, o, d, tmin, tmax, t, &a, &b);
     }
 }
@@ -441,6 +487,10 @@ static void finalize(const scene_t* s, int pi, float t, v3 o, v3 d, hit_t* h) {
         float sc = phi / (2 * PI_F), tc = theta / PI_F;
         sc = fmodf(sc * 1.0f, 1.0f); tc = fmodf(tc * 1.0f, 1.0f);
         h->u = 1.0f * sc + 0.0f; h->v = 1.0f * tc + 0.0f;
+    } else if (p->kind == K_LIGHT && p->sphere_light) {
+        h->p = vat(o, d, t);
+        face(h, d, vdivs(vsub(h->p, p->a), p->rad));
+        h->u = 0.0f; h->v = 0.0f;   /* solid texture: uv unused */
     } else if (p->kind == K_QUAD || p->kind == K_LIGHT) {
         v3 ip = vat(o, d, t), pl = vsub(ip, p->a);
         float a = vdot(p->w, vcross(pl, p->c)), b = vdot(p->w, vcross(p->b, pl));
@@ -521,6 +571,12 @@ static rgb_t background(const scene_t* s, v3 dir) {
 static float light_pdf(const scene_t* s, int li, v3 o, v3 v) {
     const prim_t* p = &s->prims[s->lights[li]];
     float t, a, b;
+    if (p->sphere_light) {   /* omni_light::pdf_value (omni_light.cuh:104-115) */
+        if (!sphere_t(p, o, v, 0.00001f, INFINITY, &t)) return 0;
+        float ctm = sqrtf(1 - p->rad * p->rad / vlensq(vsub(p->a, o)));
+        float solid_angle = 2 * PI_F * (1 - ctm);   /* M_PI is a float literal (misc/constants.cuh:35) */
+        return 1.0f / solid_angle;
+    }
     if (!planar_t(p, o, v, 0.00001f, INFINITY, 1, &t, &a, &b)) return 0;
     v3 nrm = vdot(v, p->normal) < 0.0f ? p->normal : vneg(p->normal);
     float distance_squared = t * t * vlensq(v);
@@ -558,6 +614,29 @@ static inline v3 scatter_origin(int clean, v3 p, v3 n, v3 dir) {
     return V(offset_coord(p.x, side.x), offset_coord(p.y, side.y), offset_coord(p.z, side.z));
 }
 
+/* omni_light::random (omni_light.cuh:117-124) with random_to_sphere (gpu_randomizer.cuh:82-93): the
+   direction toward a sphere light of centre c and radius r from o (two draws) */
+static v3 sphere_light_random(v3 c, float r, v3 o, rng_t* rng) {
+    v3 dl = vsub(c, o);
+    float dsq = vlensq(dl);
+    onb_t lb = build_from_w(dl);
+    float r1 = U(rng), r2 = U(rng);
+    float z = 1 + r2 * (sqrtf(1 - r * r / dsq) - 1);
+    float phi = 2 * PI_F * r1;   /* float M_PI (misc/constants.cuh:35) */
+    float x = f_cos(phi) * sqrtf(1 - z * z), y = f_sin(phi) * sqrtf(1 - z * z);
+    return onb_local(&lb, V(x, y, z));
+}
+
+/* the same sampler for the known-answer test: light (0.3,-0.2,0.1), radius 0.5, seen from (1.3,0.7,-2.1) */
+int port_sphere_light_draws(uint32_t seed, int64_t n, float* out) {
+    rng_t rng; minstd_seed(&rng, seed);
+    for (int64_t k = 0; k < n; ++k) {
+        v3 p = sphere_light_random(V(0.3f, -0.2f, 0.1f), 0.5f, V(1.3f, 0.7f, -2.1f), &rng);
+        out[3 * k] = p.x; out[3 * k + 1] = p.y; out[3 * k + 2] = p.z;
+    }
+    return 0;
+}
+
 /* camera::ray_color (camera.cuh:149-264) for one sample; returns radiance, counts closest-hit calls */
 static rgb_t ray_color(const scene_t* s, v3 o, v3 d, int max_depth, rng_t* rng, int order, int clean, uint64_t* rays) {
     rgb_t res = {0, 0, 0}, att = {1, 1, 1};
@@ -578,13 +657,27 @@ static rgb_t ray_color(const scene_t* s, v3 o, v3 d, int max_depth, rng_t* rng, 
         if (m->kind == RTC_MAT_DIFFUSE_LIGHT) {   /* diffuse_light::emitted (diffuse_light.cuh:45-67) */
             if (m->directional && !h.front) alpha0 = 1;
             else { rgb_t tv = tex_value(s, m->tex, h.u, h.v, h.p); em.r = tv.r * m->intensity; em.g = tv.g * m->intensity; em.b = tv.b * m->intensity; }
+        } else if (m->kind == MAT_SPOT) {   /* diffuse_spot_light::emitted (diffuse_spot_light.cuh:33-49) */
+            if (!h.front) {
+                alpha0 = 1;
+                if (!m->invisible) { em.r = em.g = em.b = 1.0f; }   /* color(1,1,1,0) */
+            } else {
+                float cos_theta = vdot(vunit(d), vunit(m->dir));
+                if (cos_theta < m->cos_cutoff) {
+                    em.r = em.g = em.b = 1.0f;
+                } else {
+                    float k2 = m->intensity * f_pow(cos_theta, m->falloff);
+                    rgb_t tv = tex_value(s, m->tex, h.u, h.v, h.p);
+                    em.r = tv.r * k2; em.g = tv.g * k2; em.b = tv.b * k2;
+                }
+            }
         }
         if (alpha0) {   /* invisible re-hit (camera.cuh:177-183) */
             float t2; int p2;
             (*rays)++;
             if (closest(s, o, d, h.t + 0.001f, FLT_MAX, hide, clean, &t2, &p2)) { finalize(s, p2, t2, o, d, &h); m = &s->mat[h.mat]; }
         }
-        if (m->kind == RTC_MAT_DIFFUSE_LIGHT) {
+        if (m->kind == RTC_MAT_DIFFUSE_LIGHT || m->kind == MAT_SPOT) {
             res.r += att.r * em.r; res.g += att.g * em.g; res.b += att.b * em.b;
             break;
         }
@@ -631,10 +724,14 @@ static rgb_t ray_color(const scene_t* s, v3 o, v3 d, int max_depth, rng_t* rng, 
             else {
                 if (s->nlights > 1) (void)U(rng);   /* get_int(rng, 0, n-1) == 0 */
                 const prim_t* L = &s->prims[s->lights[0]];
-                float ru, rv;
-                draw2(rng, order, &ru, &rv);
-                v3 pp = vadd(vadd(L->a, vscale(ru - 0.5f, L->b)), vscale(rv - 0.5f, L->c));
-                dir = vsub(pp, h.p);
+                if (L->sphere_light) {
+                    dir = sphere_light_random(L->a, L->rad, h.p, rng);
+                } else {
+                    float ru, rv;
+                    draw2(rng, order, &ru, &rv);
+                    v3 pp = vadd(vadd(L->a, vscale(ru - 0.5f, L->b)), vscale(rv - 0.5f, L->c));
+                    dir = vsub(pp, h.p);
+                }
             }
         } else {
             float r1 = U(rng), r2 = U(rng);   /* random_cosine_direction (gpu_randomizer.cuh:121-133) */

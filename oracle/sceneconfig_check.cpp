@@ -82,6 +82,29 @@ int main() {
     cfg.lightsCfg.dirLights = lights;
     cfg.lightsCfg.dirLightCount = 1;
 
+    static omniLightConfig omnis[1];
+    omnis[0].position = point3(100.0f, 500.0f, 200.0f);
+    omnis[0].radius = 20.0f;
+    omnis[0].intensity = 2.0f;
+    omnis[0].rgb = color(4.0f, 3.0f, 2.0f);
+    omnis[0].name = "SphereLight1";
+    omnis[0].invisible = false;
+    cfg.lightsCfg.omniLights = omnis;
+    cfg.lightsCfg.omniLightCount = 1;
+
+    static spotLightConfig spots[1];
+    spots[0].position = point3(400.0f, 500.0f, 300.0f);
+    spots[0].direction = vector3(0.0f, -1.0f, 0.2f);
+    spots[0].cutoff = 30.0f;
+    spots[0].falloff = 3.0f;
+    spots[0].intensity = 5.0f;
+    spots[0].radius = 10.0f;
+    spots[0].rgb = color(6.0f, 6.0f, 5.0f);
+    spots[0].name = "SpotLight1";
+    spots[0].invisible = true;
+    cfg.lightsCfg.spotLights = spots;
+    cfg.lightsCfg.spotLightCount = 1;
+
     static quadPrimitiveConfig quads[6];
     const float qv[6][9] = {{555, 0, 0, 0, 555, 0, 0, 0, 555},     {0, 0, 0, 0, 555, 0, 0, 0, 555},
                             {0, 0, 0, 555, 0, 0, 0, 0, 555},       {555, 555, 555, -555, 0, 0, 0, 0, -555},
@@ -158,6 +181,24 @@ int main() {
         arr3("v", l.v);
         arr3("color", l.color);
         std::printf("\"intensity\": %.9g, \"invisible\": %d}", l.intensity, l.invisible);
+    }
+    std::printf("], \"omni_lights\": [");
+    for (uint32_t i = 0; i < d->num_omni_lights; ++i) {
+        const rtc_omni_light& l = d->omni_lights[i];
+        std::printf("%s{", i ? ", " : "");
+        arr3("position", l.position);
+        arr3("color", l.color);
+        std::printf("\"radius\": %.9g, \"intensity\": %.9g, \"invisible\": %d}", l.radius, l.intensity, l.invisible);
+    }
+    std::printf("], \"spot_lights\": [");
+    for (uint32_t i = 0; i < d->num_spot_lights; ++i) {
+        const rtc_spot_light& l = d->spot_lights[i];
+        std::printf("%s{", i ? ", " : "");
+        arr3("position", l.position);
+        arr3("direction", l.direction);
+        arr3("color", l.color);
+        std::printf("\"cutoff\": %.9g, \"falloff\": %.9g, \"radius\": %.9g, \"intensity\": %.9g, \"invisible\": %d}",
+                    l.cutoff, l.falloff, l.radius, l.intensity, l.invisible);
     }
     std::printf("], \"spheres\": [");
     for (uint32_t i = 0; i < d->num_spheres; ++i) {

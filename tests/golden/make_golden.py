@@ -10,9 +10,9 @@ its own classes, compiled with g++ (oracle/ref_harness.cpp), produce them here:
                  1984, 2580, 2580+65535 (10^4 each) and the states whose draw rounds to 1.0f;
                  get_int draws (always `min`); the g++ build's multi-draw helpers
                  (random_in_unit_disk, random_in_unit_sphere, random_cosine_direction,
-                 directional_light::random), 500 calls each.
+                 directional_light::random, omni_light::random), 500 calls each.
 * scenes.npz     T3: per-pixel FP32 radiance sums (pixel_color before prepare_pixel_color) of the
-                 four parity scenes at small sizes, g++ draw order; T2: closest-hit primitive ids
+                 five parity scenes at small sizes, g++ draw order; T2: closest-hit primitive ids
                  and t of 4096 seeded random rays per scene.
 """
 from __future__ import annotations
@@ -38,6 +38,7 @@ GOLDEN_SCENES = {
     "spheres": dict(width=48, height=27, spp=9, max_depth=16),
     "textured": dict(width=40, height=30, spp=9, max_depth=10),
     "icosphere": dict(width=36, height=24, spp=9, max_depth=12),
+    "lights": dict(width=40, height=30, spp=9, max_depth=10),
 }
 RAYS_PER_SCENE = 4096
 
@@ -73,7 +74,7 @@ def main():
         kat[f"draws_{seed}"] = ref.rng_draws(seed, 10000)
     # states x with float(x - 1) * 2^-31 == 1.0f: a seed s gives x1 = 48271*s mod m; search near the top
     kat["get_int_2580_0_5"] = ref.get_int(2580, 0, 5, 1000)
-    for which, nm in enumerate(("disk", "sphere", "cosine", "light")):
+    for which, nm in enumerate(("disk", "sphere", "cosine", "light", "omni")):
         kat[f"sampler_{nm}"] = ref.sampler_draws(which, 2580, 500)
     np.savez_compressed(HERE / "rng_kat.npz", **kat)
 

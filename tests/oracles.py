@@ -188,6 +188,12 @@ class Port:
             raise RuntimeError(self.lib.port_last_error().decode())
         return _PortScene(self, h, d)
 
+    def sphere_light_draws(self, seed: int, n: int) -> np.ndarray:
+        """omni_light::random for the known-answer light (see port_sphere_light_draws)."""
+        out = np.empty((n, 3), np.float32)
+        self.lib.port_sphere_light_draws(C.c_uint32(seed), C.c_int64(n), out.ctypes.data_as(C.c_void_p))
+        return out
+
     def rng_draws(self, seed: int, n: int) -> np.ndarray:
         out = np.empty(n, np.float32)
         self.lib.port_rng_draws(C.c_uint32(seed), C.c_int64(n), out.ctypes.data_as(C.c_void_p))

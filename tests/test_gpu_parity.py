@@ -34,6 +34,7 @@ SCENES = [
     ("spheres", dict(width=64, height=36, spp=9, max_depth=16)),
     ("textured", dict(width=64, height=48, spp=9, max_depth=10)),
     ("icosphere", dict(width=60, height=40, spp=9, max_depth=12)),
+    ("lights", dict(width=48, height=36, spp=9, max_depth=10)),   # omni, directional and spot lights
 ]
 
 
@@ -147,7 +148,7 @@ def test_compat_parity_vs_reference_gpu(ctx, refgpu, name, kw):
     assert np.all(np.abs(qa - qb) <= 0.05 * np.maximum(np.abs(qb), 1e-3 * mb)), (qa, qb)
 
 
-@pytest.mark.parametrize("name", ["cornell", "spheres", "icosphere", "textured"])
+@pytest.mark.parametrize("name", ["cornell", "spheres", "icosphere", "textured", "lights"])
 def test_closest_hit_identity(ctx, refcpu, name):
     from golden.make_golden import golden_rays
     mk, _ = configs.SCENES[name]
@@ -265,7 +266,7 @@ def test_long_chain_split(ctx, monkeypatch, order):
 
 
 
-@pytest.mark.parametrize("name", ["cornell", "spheres", "icosphere", "textured", "meshes6"])
+@pytest.mark.parametrize("name", ["cornell", "spheres", "icosphere", "textured", "lights", "meshes6"])
 def test_wide_bvh_hit_identity(ctx, name):
     """Closest hits through the 8-wide quantised nodes equal the binary walk's on random rays, including
     rays with a zero direction component and all-zero directions (which miss in both walks)."""

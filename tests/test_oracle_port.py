@@ -67,6 +67,11 @@ def test_sampler_host_order(kat, which, name):
     assert np.array_equal(rep, kat[f"sampler_{name}"])
 
 
+def test_sphere_light_sampler_bitexact(port, kat):
+    """omni_light::random (random_to_sphere with the reference's float M_PI) reproduced bit for bit."""
+    assert np.array_equal(port.sphere_light_draws(2580, 500), kat["sampler_omni"])
+
+
 def test_sampler_cosine_within_ulp(kat):
     rep = oracles.sampler_reproduction(2, 2580, 500, 1)
     ref = kat["sampler_cosine"]

@@ -39,6 +39,17 @@ def test_objects_in_load_scene_order_and_unresolved_skipped(desc):
     assert "boxes" in d["skipped"]
 
 
+def test_omni_and_spot_lights(desc):
+    o, = desc["omni_lights"]
+    assert o["position"] == [100.0, 500.0, 200.0] and o["radius"] == 20.0 and o["intensity"] == 2.0
+    assert o["color"] == [4.0, 3.0, 2.0] and o["invisible"] == 0
+    s, = desc["spot_lights"]
+    assert s["position"] == [400.0, 500.0, 300.0] and s["direction"] == pytest.approx([0.0, -1.0, 0.2], abs=1e-7)
+    assert s["cutoff"] == 30.0 and s["falloff"] == 3.0 and s["radius"] == 10.0 and s["intensity"] == 5.0
+    assert s["color"] == [6.0, 6.0, 5.0] and s["invisible"] == 1
+    assert not any("light" in k for k in desc["skipped"])
+
+
 def test_directional_light_and_camera(desc):
     L = desc["dir_lights"][0]
     assert L["position"] == [278.0, 554.0, 332.0] and L["u"] == [-130.0, 0.0, 0.0] and L["v"] == [0.0, 0.0, -105.0]
