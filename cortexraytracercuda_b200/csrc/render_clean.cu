@@ -49,6 +49,7 @@ __global__ void __launch_bounds__(128) rtc_render_clean(DevScene S, DevParams P,
         }
         }
         out[pixel_index] = make_float4(tr, tg, tb, 1.0f);
+        if (P.rgb8) quantize_pixel(make_float4(tr, tg, tb, 1.0f), P.spp, P.width, P.height, pixel_index, P.rgb8);
     }
     if (counters) {
         unsigned long long r = pc.rays, p = paths, n = pc.nodes, q = pc.prims;

@@ -15,7 +15,6 @@
 //   rtc_render_compat<ORDER>  one thread per pixel, all samples of the pixel in sequence
 //                             (the render kernel, core/src/gpu.cu:761-790), writes the FP32 sum;
 //   rtc_trace_closest         closest hit of arbitrary rays (hit-identity tests);
-//   rtc_quantize              prepare_pixel_color + 8-bit quantisation + row flip
 //                             (color.cuh:289-309, gpu.cu:792-799, 2098-2107).
 #include "rtc_kernels.h"
 #include "rtc_path.cuh"
@@ -72,6 +71,7 @@ __global__ void __launch_bounds__(128) rtc_render_compat(DevScene S, DevParams P
             }
         }
         out[pixel_index] = make_float4(pr, pg, pb, 1.0f);
+        if (P.rgb8) quantize_pixel(make_float4(pr, pg, pb, 1.0f), P.spp, P.width, P.height, pixel_index, P.rgb8);
     }
     flush_counters(counters, pc.rays, paths, pc.nodes, pc.prims);
     if (status) atomicOr(status_word, status);
@@ -105,25 +105,6 @@ __global__ void __launch_bounds__(128) rtc_trace_closest(DevScene S, const float
     if (status) atomicOr(status_word, status);
 }
 
-// prepare_pixel_color (color.cuh:289-309): NaN -> 0, * (1/spp), sqrt; then
-// int(255.99 * clamp(c, 0, 0.999)) (gpu.cu:792-799) and the PNG row flip (gpu.cu:2098-2107).
-__global__ void rtc_quantize(const float4* __restrict__ sum, uint8_t* __restrict__ rgb8, int width, int height,
-                             int spp) {
-    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= (int64_t)width * height) return;
-    int i = (int)(p % width), j = (int)(p / width);
-    float4 c = sum[p];
-    float ch[3] = {c.x, c.y, c.z};
-    uint8_t* o = rgb8 + ((size_t)(height - j - 1) * width + i) * 3;
-    for (int k = 0; k < 3; ++k) {
-        float x = ch[k] != ch[k] ? 0.0f : ch[k];
-        if (spp > 0) x *= 1.0f / (float)spp;
-        x = sqrtf(x);
-        float cl = x < 0.0f ? 0.0f : (x > 0.999f ? 0.999f : x);
-        int q = (int)(255.99f * cl);
-        o[k] = (uint8_t)q;
-    }
-}
 #endif  // RTC_FLAVOR == 1
 
 }  // namespace rtc
@@ -153,11 +134,4 @@ cudaError_t rtc_launch_trace_closest(const DevScene& S, const float* rays, uint3
     return cudaGetLastError();
 }
 
-cudaError_t rtc_launch_quantize(const float4* sum, uint8_t* rgb8, int width, int height, int spp, cudaStream_t st) {
-    int64_t n = (int64_t)width * height;
-    if (n == 0) return cudaSuccess;
-    const int threads = 256;
-    rtc_quantize<<<(unsigned)((n + threads - 1) / threads), threads, 0, st>>>(sum, rgb8, width, height, spp);
-    return cudaGetLastError();
-}
 #endif  // RTC_FLAVOR == 1

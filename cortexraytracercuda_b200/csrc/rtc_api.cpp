@@ -665,6 +665,7 @@ DevParams rtc_dev_params(const rtc_render_params* p) {
     P.draw_order = p->draw_order;
     P.num_pixels = (int64_t)p->width * p->height;
     P.groups = (p->mode == RTC_MODE_CLEAN && (p->flags & RTC_FLAG_SAMPLE_GROUPS)) ? std::min(8, p->spp) : 1;
+    P.rgb8 = nullptr;
     return P;
 }
 
@@ -783,8 +784,9 @@ rtc::WfOneFn wf_one_fn(const rtc_render_params* p) {
 rtc_status run_wavefront(const DevScene& S, const rtc_render_params* p, const WfBuffers& B, uint32_t* d_status,
                          float4* d_out, unsigned long long* d_counters, cudaStream_t st, int num_sms,
                          const WfPoller& poll, cudaEvent_t* phase, WfRun& run, WfTimer* timer = nullptr,
-                         void* groups = nullptr) {
-    const DevParams P = dev_params(p);
+                         void* groups = nullptr, uint8_t* d_rgb8 = nullptr) {
+    DevParams P = dev_params(p);
+    P.rgb8 = d_rgb8;   // quantised output written as each pixel finishes
     const bool clean = p->mode == RTC_MODE_CLEAN;
     const WfOneFn fn = wf_one_fn(p);
     WfOneArgs J;
@@ -934,7 +936,7 @@ rtc_status run_wavefront(const DevScene& S, const rtc_render_params* p, const Wf
 }
 
 rtc_status launch_wavefront(rtc_context* c, const rtc_scene* s, const rtc_render_params* p, float4* d_out,
-                            unsigned long long* d_counters, cudaStream_t st) {
+                            unsigned long long* d_counters, cudaStream_t st, uint8_t* d_rgb8) {
     const int64_t units = (int64_t)p->width * p->height * dev_params(p).groups;
     const uint32_t slots = (uint32_t)std::min<int64_t>(units, WF_MAX_SLOTS);
     WfBuffers B;
@@ -960,7 +962,7 @@ rtc_status launch_wavefront(rtc_context* c, const rtc_scene* s, const rtc_render
     timer.pool = &c->kev;
     const bool timed = (p->flags & RTC_FLAG_KERNEL_TIMING) != 0;
     r = run_wavefront(rtc_scene_view(s, p), p, B, c->d_status, d_out, d_counters, st, c->num_sms, poll,
-                      c->phase_ev, run, timed ? &timer : nullptr, c->d_groups);
+                      c->phase_ev, run, timed ? &timer : nullptr, c->d_groups, d_rgb8);
     if (r != RTC_OK) return r;
     c->kev_ext = c->kev_shade = 0;
     c->kev_pairs.clear();
@@ -1002,14 +1004,17 @@ rtc_status rtc_run_wavefront_sync(const rtc_scene* s, const rtc_render_params* p
 
 namespace {
 
+// d_rgb8 (may be null): the quantised, row-flipped RGB8 image, written by the render kernels as each
+// pixel finishes (prepare_pixel_color + the output loop fused into the accumulation).
 rtc_status launch(rtc_context* c, const rtc_scene* s, const rtc_render_params* p, float4* d_out,
-                  unsigned long long* d_counters, cudaStream_t st) {
-    if (p->engine != RTC_ENGINE_MEGAKERNEL) return launch_wavefront(c, s, p, d_out, d_counters, st);
+                  unsigned long long* d_counters, cudaStream_t st, uint8_t* d_rgb8) {
+    if (p->engine != RTC_ENGINE_MEGAKERNEL) return launch_wavefront(c, s, p, d_out, d_counters, st, d_rgb8);
     c->last = rtc_render_stats{};
     c->last.engine = RTC_ENGINE_MEGAKERNEL;
     c->last.launches = 1;
     c->last_timed = false;
     DevParams P = dev_params(p);
+    P.rgb8 = d_rgb8;
     const DevScene S = rtc_scene_view(s, p);
     cudaError_t e =
         p->mode == RTC_MODE_CLEAN ? rtc_launch_render_clean(S, P, d_out, d_counters, c->d_status, p->block_size, st)
@@ -1057,12 +1062,9 @@ extern "C" rtc_status rtc_render(rtc_context* c, const rtc_scene* s, const rtc_r
         c->rgb8_cap = npix * 3;
     }
     RTC_CUDA(cudaMemsetAsync(c->d_status, 0, 4, c->stream));
-    r = launch(c, s, p, c->d_out, nullptr, c->stream);
+    r = launch(c, s, p, c->d_out, nullptr, c->stream, rgb8 ? c->d_rgb8 : nullptr);
     if (r != RTC_OK) return r;
-    if (rgb8) {
-        RTC_CUDA(rtc_launch_quantize(c->d_out, c->d_rgb8, p->width, p->height, p->spp, c->stream));
-        RTC_CUDA(cudaMemcpyAsync(rgb8, c->d_rgb8, npix * 3, cudaMemcpyDeviceToHost, c->stream));
-    }
+    if (rgb8) RTC_CUDA(cudaMemcpyAsync(rgb8, c->d_rgb8, npix * 3, cudaMemcpyDeviceToHost, c->stream));
     if (radiance_sum)
         RTC_CUDA(cudaMemcpyAsync(radiance_sum, c->d_out, npix * sizeof(float4), cudaMemcpyDeviceToHost, c->stream));
     RTC_CUDA(cudaStreamSynchronize(c->stream));
@@ -1078,10 +1080,7 @@ extern "C" rtc_status rtc_render_device(rtc_context* c, const rtc_scene* s, cons
     if (r != RTC_OK) return r;
     cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
     RTC_CUDA(cudaSetDevice(c->device));
-    r = launch(c, s, p, (float4*)d_radiance_sum, d_counters, st);
-    if (r != RTC_OK) return r;
-    if (d_rgb8) RTC_CUDA(rtc_launch_quantize((const float4*)d_radiance_sum, d_rgb8, p->width, p->height, p->spp, st));
-    return RTC_OK;
+    return launch(c, s, p, (float4*)d_radiance_sum, d_counters, st, d_rgb8);
 }
 
 extern "C" rtc_status rtc_get_render_stats(rtc_context* c, rtc_render_stats* out) {

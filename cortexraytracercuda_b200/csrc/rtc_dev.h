@@ -113,6 +113,7 @@ struct DevParams {
     int draw_order;    // 0 device (left to right), 1 host (right to left)
     int64_t num_pixels;
     int groups;        // sample groups per pixel (clean mode, RTC_FLAG_SAMPLE_GROUPS), else 1
+    uint8_t* rgb8;     // non-null: each finished pixel is also written quantised here (quantize_pixel)
 };
 
 // Wavefront path slots (SoA, one slot = one pixel in flight) and the two slot queues.

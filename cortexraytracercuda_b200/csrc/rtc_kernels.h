@@ -55,8 +55,7 @@ cudaError_t rtc_launch_render_clean(const rtc::DevScene& S, const rtc::DevParams
                                     unsigned long long* counters, uint32_t* status, int block, cudaStream_t st);
 cudaError_t rtc_launch_trace_closest(const rtc::DevScene& S, const float* rays, uint32_t n, int depth,
                                      int max_depth, int32_t* prim, float* t, uint32_t* status, cudaStream_t st);
-cudaError_t rtc_launch_quantize(const float4* sum, uint8_t* rgb8, int width, int height, int spp,
-                                cudaStream_t st);
+
 
 // clean-mode wavefront (wavefront_clean.cu)
 cudaError_t rtc_wf_one_clean(rtc::WfOp op, const rtc::WfOneArgs& a, const rtc::WfBuffers& B, const rtc::WfLaunch& L);

@@ -640,4 +640,20 @@ __device__ __forceinline__ float lights_pdf_value(const DevScene& S, V3 o, V3 v)
     return sum;
 }
 
+// prepare_pixel_color (color.cuh:289-309) and the output loop (gpu.cu:792-799, 2098-2107) for one pixel:
+// NaN -> 0, * (1/spp), sqrt, int(255.99 * clamp(c, 0, 0.999)), written to the row-flipped RGB8 image.
+// `p` is the frame-buffer index j*W + i with j counted from the bottom.
+__device__ __forceinline__ void quantize_pixel(float4 c, int spp, int width, int height, int64_t p, uint8_t* rgb8) {
+    const int i = (int)(p % width), j = (int)(p / width);
+    const float ch[3] = {c.x, c.y, c.z};
+    uint8_t* o = rgb8 + ((size_t)(height - j - 1) * width + i) * 3;
+    for (int k = 0; k < 3; ++k) {
+        float x = ch[k] != ch[k] ? 0.0f : ch[k];
+        if (spp > 0) x *= 1.0f / (float)spp;
+        x = sqrtf(x);
+        const float cl = x < 0.0f ? 0.0f : (x > 0.999f ? 0.999f : x);
+        o[k] = (uint8_t)(int)(255.99f * cl);
+    }
+}
+
 }  // namespace rtc

@@ -227,6 +227,7 @@ __device__ __forceinline__ void wf_group_done(const J& jobs, uint32_t job, uint3
     const DevParams& P = jobs.params(job);
     if (P.groups <= 1) {
         jobs.output(job)[pixel] = make_float4(ps.x, ps.y, ps.z, 1.0f);
+        if (P.rgb8) quantize_pixel(make_float4(ps.x, ps.y, ps.z, 1.0f), P.spp, P.width, P.height, pixel, P.rgb8);
         jobs.pixel_done(job);
         return;
     }
@@ -243,6 +244,7 @@ __device__ __forceinline__ void wf_group_done(const J& jobs, uint32_t job, uint3
         t.z += v.z;
     }
     jobs.output(job)[pixel] = make_float4(t.x, t.y, t.z, 1.0f);
+    if (P.rgb8) quantize_pixel(make_float4(t.x, t.y, t.z, 1.0f), P.spp, P.width, P.height, pixel, P.rgb8);
     jobs.pixel_done(job);
 }
 

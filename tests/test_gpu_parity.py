@@ -284,3 +284,29 @@ def test_wide_bvh_hit_identity(ctx, name):
     assert np.array_equal(ta.view(np.uint32), tb.view(np.uint32))
     assert int((a != b).sum()) <= max(3, int(0.001 * len(rays)))   # exact-t ties only
     ds.close()
+
+
+def _quantize(rad, spp):
+    """prepare_pixel_color (color.cuh:289-309) + 8-bit quantisation and row flip (gpu.cu:792-799,
+    2098-2107) in float32 numpy, the host restatement of the fused output step."""
+    x = rad[..., :3].astype(np.float32).copy()
+    x[np.isnan(x)] = 0.0
+    x = x * (np.float32(1.0) / np.float32(spp))
+    x = np.sqrt(x)
+    x = np.clip(x, np.float32(0.0), np.float32(0.999))
+    q = (np.float32(255.99) * x).astype(np.int32).astype(np.uint8)
+    return q[::-1]
+
+
+@pytest.mark.parametrize("engine,mode,flags", [(ENGINE_WAVEFRONT, MODE_COMPAT, 0), (ENGINE_MEGAKERNEL, MODE_COMPAT, 0),
+                                               (ENGINE_WAVEFRONT, MODE_CLEAN, 4), (ENGINE_MEGAKERNEL, MODE_CLEAN, 0)])
+def test_fused_rgb8_output(ctx, engine, mode, flags):
+    """The RGB8 image is written by the render kernels as each pixel finishes (no separate pass); it
+    equals the quantised, row-flipped radiance sums the same call returns."""
+    scene, params = _params("textured", dict(width=64, height=48, spp=9, max_depth=10), DRAW_ORDER_DEVICE, engine)
+    params.mode, params.flags = mode, flags
+    ds = DeviceScene(ctx, scene)
+    rad, rgb = ds.render(params, want_rgb8=True)
+    ds.close()
+    assert rgb.shape == (48, 64, 3)
+    assert np.array_equal(rgb, _quantize(rad, params.spp))
