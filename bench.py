@@ -62,6 +62,10 @@ FALLBACK_HBM_GBS = 6650.0
 NODE_BYTES = 64          # BVH2 node: two child boxes + two child links (4 x float4)
 NODE8_BYTES = 96         # 8-wide node: header, quantised child boxes (8-bit), eight child links (6 x float4)
 PRIM_BYTES = {"spheres": 16, "cornell": 48, "meshes": 48}   # dominant primitive record of each workload
+# algorithmic FP32 operations per visit (the fixed constants of the roofline's flop count): a binary node's
+# two slab tests, and the dominant primitive test of each workload (sphere 20, triangle 30)
+NODE_FLOPS = 24
+PRIM_FLOPS = {"spheres": 20, "cornell": 30, "meshes": 30}
 STATE_BYTES = 32 + 16 + 2 * 48   # ray read + hit write + path state read/write per traversal
 EXTEND_STATE_BYTES = 4 + 32 + 4 + 8   # queue entry + ray (origin, direction) + depth word read, hit record write
 
@@ -715,6 +719,22 @@ def main():
                 "alg_bytes_per_launch": int(alg_bytes), "kernel_ms": round(kernel_ms, 3),
                 "per_launch": {"rays": rays, "paths": paths, "node_visits": nodes, "prim_tests": prims},
                 "bytes_per_ray": round(alg_bytes / max(rays, 1), 1)}
+    # the issue side of the same kernel: algorithmic FP32 flops over the FP32 SIMT peak at the sampled clock
+    # (SMs x 128 lanes x 2 flops x f_SM)
+    import torch as _t
+    sms = _t.cuda.get_device_properties(local).multi_processor_count
+    mhz = clk.get("sm_mhz") or clk.get("sm_max_mhz") or 1965.0
+    fp32_peak = sms * 128 * 2 * mhz * 1e6 / 1e12
+    if wavefront:
+        flops = ext_nodes * NODE_FLOPS + ext_prims * PRIM_FLOPS[args.config]
+        t_s = ext_ms / 1e3
+    else:
+        flops = nodes * NODE_FLOPS + prims * PRIM_FLOPS[args.config]
+        t_s = kernel_ms / 1e3
+    roof["flops"] = {"achieved": round(flops / t_s / 1e12, 3), "peak": round(fp32_peak, 1), "unit": "TFLOP/s",
+                     "frac": round(flops / t_s / 1e12 / fp32_peak, 4),
+                     "peak_source": f"FP32 SIMT: {sms} SMs x 128 x 2 x {mhz:.0f} MHz",
+                     "per_visit": {"node": NODE_FLOPS, "prim": PRIM_FLOPS[args.config]}}
     prof = ROOT / "profiles" / f"traffic_{'wf_extend' if wavefront else 'megakernel'}_{args.config}.json"
     if prof.exists():
         try:
