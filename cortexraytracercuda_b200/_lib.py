@@ -10,7 +10,8 @@ import os
 from pathlib import Path
 
 from .scene import (rtc_batch_params, rtc_job, rtc_obj_mesh, rtc_render_params, rtc_render_stats, rtc_request, rtc_request_info,
-                    rtc_scene_desc, rtc_scene_info, rtc_scene_options, rtc_server_config, rtc_server_stats)
+                    rtc_scene_desc, rtc_scene_info, rtc_scene_options, rtc_server_config, rtc_server_stats,
+                    IMAGE_LOADER, rtc_scene_file_info)
 
 LIB_PATH = Path(__file__).resolve().parent / "librtc_b200.so"
 
@@ -49,6 +50,11 @@ PROTOTYPES = {
     "rtc_launchGPU": (C.c_int, [C.POINTER(rtc_scene_desc), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                 C.c_char_p, C.c_int]),
     "rtc_load_obj": (C.c_int, [C.c_char_p, C.POINTER(rtc_obj_mesh)]),
+    "rtc_scene_file_load": (C.c_int, [C.c_char_p, C.c_uint32, IMAGE_LOADER, C.c_void_p, C.POINTER(C.c_void_p)]),
+    "rtc_scene_file_desc": (C.POINTER(rtc_scene_desc), [_P]),
+    "rtc_scene_file_get_info": (C.c_int, [_P, C.POINTER(rtc_scene_file_info)]),
+    "rtc_scene_file_skipped": (C.c_char_p, [_P, C.c_uint32]),
+    "rtc_scene_file_free": (None, [_P]),
     "rtc_free_obj": (None, [C.POINTER(rtc_obj_mesh)]),
     "rtc_write_png": (C.c_int, [C.c_char_p, _P, C.c_int, C.c_int]),
 }

@@ -46,6 +46,7 @@ SOURCES = [
     ("rtc_batch.cpp", "rtc_batch", "cxx", []),
     ("rtc_server.cpp", "rtc_server", "cxx", []),
     ("rtc_obj.cpp", "rtc_obj", "cxx", []),
+    ("rtc_scene_file.cpp", "rtc_scene_file", "cxx", []),
     ("bvh_device.cu", "bvh_device", "nvcc", []),
     ("bvh_build.cpp", "bvh_build", "cxx", []),
 ]

@@ -27,6 +27,11 @@ from .scene import (MODE_COMPAT, DRAW_ORDER_DEVICE, REQ_DONE, REQ_FAILED, Camera
                     rtc_server_config, rtc_server_stats)
 
 
+def _desc(scene):
+    """A Scene's packed description, or a SceneFile as it is (both have .ptr())."""
+    return scene if hasattr(scene, "ptr") and not isinstance(scene, Scene) else SceneDesc(scene)
+
+
 class Context:
     """One CUDA device + stream (rtc_context)."""
 
@@ -90,7 +95,7 @@ class DeviceScene:
 
     def __init__(self, ctx: Context, scene: Scene, bvh_builder: int = 0):
         self.ctx = ctx
-        self.desc = SceneDesc(scene)
+        self.desc = _desc(scene)
         h = C.c_void_p()
         if not ctx.handle:
             raise RtcError(1, "context is closed")
@@ -198,7 +203,7 @@ class RenderServer:
             pass
 
     def add_scene(self, scene: Scene) -> int:
-        desc = SceneDesc(scene)
+        desc = _desc(scene)
         sid = C.c_uint32()
         check(self.lib.rtc_server_add_scene(self.handle, desc.ptr(), C.byref(sid)))
         return sid.value

@@ -421,3 +421,135 @@ def load_obj(path):
     finally:
         lib.rtc_free_obj(C.byref(m))
     return v, f, n, t
+
+
+# ---- the reference's .scene files ------------------------------------------------------------------
+SCENE_FILE_REFERENCE_CAPACITY = 1   # the reference's table capacities (list length mod 256; glass sized from `dielectric`)
+
+
+class rtc_scene_file_info(C.Structure):
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("spp", C.c_int32), ("max_depth", C.c_int32),
+                ("num_skipped", C.c_uint32)]
+
+
+IMAGE_LOADER = C.CFUNCTYPE(C.c_void_p, C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_void_p)
+
+
+def decode_png(path) -> np.ndarray | None:
+    """RGB8 pixels (H, W, 3) of an 8-bit non-interlaced PNG (greyscale, RGB, palette, with or without
+    alpha; alpha dropped), or None for anything else."""
+    import struct
+    import zlib
+    try:
+        data = open(path, "rb").read()
+    except OSError:
+        return None
+    if data[:8] != b"\x89PNG\r\n\x1a\n":
+        return None
+    pos, idat, plte, hdr = 8, b"", None, None
+    while pos + 8 <= len(data):
+        n, kind = struct.unpack(">I4s", data[pos:pos + 8])
+        body = data[pos + 8:pos + 8 + n]
+        if kind == b"IHDR":
+            hdr = struct.unpack(">IIBBBBB", body)
+        elif kind == b"PLTE":
+            plte = np.frombuffer(body, np.uint8).reshape(-1, 3)
+        elif kind == b"IDAT":
+            idat += body
+        pos += 12 + n
+    if hdr is None:
+        return None
+    w, h, depth, ctype, _, _, interlace = hdr
+    ch = {0: 1, 2: 3, 3: 1, 4: 2, 6: 4}.get(ctype)
+    if depth != 8 or interlace or ch is None:
+        return None
+    raw = np.frombuffer(zlib.decompress(idat), np.uint8).reshape(h, 1 + w * ch)
+    out = np.zeros((h, w * ch), np.int32)
+    for y in range(h):   # PNG row filters (0 none, 1 sub, 2 up, 3 average, 4 Paeth)
+        f, row = raw[y, 0], raw[y, 1:].astype(np.int32)
+        prev = out[y - 1] if y else np.zeros(w * ch, np.int32)
+        cur = np.zeros(w * ch, np.int32)
+        for x in range(w * ch):
+            a = cur[x - ch] if x >= ch else 0
+            b = prev[x]
+            c = prev[x - ch] if x >= ch else 0
+            if f == 0:
+                pr = 0
+            elif f == 1:
+                pr = a
+            elif f == 2:
+                pr = b
+            elif f == 3:
+                pr = (a + b) // 2
+            else:
+                p = a + b - c
+                pa, pb, pc = abs(p - a), abs(p - b), abs(p - c)
+                pr = a if pa <= pb and pa <= pc else (b if pb <= pc else c)
+            cur[x] = (row[x] + pr) & 255
+        out[y] = cur
+    px = out.astype(np.uint8).reshape(h, w, ch)
+    if ctype == 3:
+        return plte[px[..., 0]] if plte is not None else None
+    if ch in (1, 2):
+        return np.repeat(px[..., :1], 3, axis=2)
+    return np.ascontiguousarray(px[..., :3])
+
+
+def _png_loader(path, w, h, user):
+    px = decode_png(path.decode())
+    if px is None:
+        return None
+    libc = C.CDLL(None)
+    libc.malloc.restype = C.c_void_p
+    libc.malloc.argtypes = [C.c_size_t]
+    buf = libc.malloc(px.nbytes)
+    if not buf:
+        return None
+    C.memmove(buf, px.ctypes.data, px.nbytes)
+    w[0], h[0] = px.shape[1], px.shape[0]
+    return buf
+
+
+_PNG_LOADER = IMAGE_LOADER(_png_loader)
+
+
+class SceneFile:
+    """A reference `.scene` file read by the library (rtc_scene_file_load): usable wherever a Scene is
+    (DeviceScene, RenderServer.add_scene).  Image textures are decoded with decode_png (PNG only)."""
+
+    def __init__(self, path, flags: int = 0, decode_images: bool = True):
+        from . import _lib
+        self.lib = _lib.load()
+        h = C.c_void_p()
+        _lib.check(self.lib.rtc_scene_file_load(str(path).encode(), flags, _PNG_LOADER if decode_images else IMAGE_LOADER(),
+                                                None, C.byref(h)))
+        self.handle = h
+        info = rtc_scene_file_info()
+        _lib.check(self.lib.rtc_scene_file_get_info(h, C.byref(info)))
+        self.info = {k: getattr(info, k) for k, _ in rtc_scene_file_info._fields_}
+        self.skipped = [self.lib.rtc_scene_file_skipped(h, i).decode() for i in range(info.num_skipped)]
+
+    def ptr(self):
+        return self.lib.rtc_scene_file_desc(self.handle)
+
+    @property
+    def desc(self) -> rtc_scene_desc:
+        return self.ptr().contents
+
+    def params(self, **kw) -> RenderParams:
+        """RenderParams from the file's image section (width, height, samplesPerPixel, maxDepth)."""
+        i = self.info
+        base = {k: v for k, v in (("width", i["width"]), ("height", i["height"]), ("spp", i["spp"]),
+                                  ("max_depth", i["max_depth"])) if v > 0}
+        return RenderParams(**{**base, **kw})
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.rtc_scene_file_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

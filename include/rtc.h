@@ -224,6 +224,41 @@ typedef struct rtc_obj_mesh {
 rtc_status rtc_load_obj(const char* path, rtc_obj_mesh* mesh);
 void rtc_free_obj(rtc_obj_mesh* mesh);
 
+/* The reference's `.scene` files (libconfig syntax), read the way core/src/scenes/scene_loader.cpp reads
+ * them into a sceneConfig and converted as rtc_sceneconfig.hpp converts one: image, camera, lights
+ * (directional, omni, spot), solid / checker / image textures, lambertian / metal / glass materials,
+ * spheres, quads and OBJ meshes (read with rtc_load_obj).  Values follow libconfig's typing as the
+ * reference reads it (no AutoConvert): a float setting written as an integer (`radius = 1;`) keeps the
+ * loader's default, and colours of three integers are 0-255 values.  Where scene_loader throws (a setting
+ * handed to the builder with the wrong type, a nameless texture or material, a primitive without a
+ * material) loading fails with RTC_ERR_BAD_SCENE, as does a syntax error (the message names the line).
+ * Relative paths resolve against the scene file's directory, then the working directory.  What the
+ * render path does not cover (other primitives, materials and textures, transforms, groups) is listed by
+ * rtc_scene_file_skipped.  Replaces scene_loader::loadSceneFromFile (scene_loader.cpp:19-120) followed
+ * by the scene_builder getters a caller of launchGPU passes on. */
+typedef struct rtc_scene_file rtc_scene_file;
+/* Image decoder for image textures: returns malloc'ed RGB8 pixels (width*height*3, top row first) that
+ * the scene file frees with free(), or NULL.  Without one, image textures are skipped. */
+typedef uint8_t* (*rtc_image_loader)(const char* path, int* width, int* height, void* user);
+/* The reference's table capacities.  scene_loader counts each list into a uint8_t (scene_loader.cpp:
+ * 124-204, 220-229, 280-282), so a kind holds (list length mod 256) entries, and it sizes the dielectric
+ * table from a `dielectric` key while filling it from `glass` (scene_loader.cpp:191, 1092), so glass
+ * materials, and the objects using them, are dropped unless a `dielectric` list makes room.  By default
+ * every entry is kept; this flag reproduces the reference. */
+#define RTC_SCENE_FILE_REFERENCE_CAPACITY 1
+typedef struct rtc_scene_file_info {
+    int32_t width, height;     /* image.width / image.height (scene_builder's 400 x 225 when absent)  */
+    int32_t spp, max_depth;    /* image.samplesPerPixel / image.maxDepth (50 / 100 when absent)      */
+    uint32_t num_skipped;      /* notes readable with rtc_scene_file_skipped                          */
+} rtc_scene_file_info;
+rtc_status rtc_scene_file_load(const char* path, uint32_t flags, rtc_image_loader load_image, void* user,
+                               rtc_scene_file** out);
+/* The scene description (valid until rtc_scene_file_free), ready for rtc_scene_create. */
+const rtc_scene_desc* rtc_scene_file_desc(const rtc_scene_file* file);
+rtc_status rtc_scene_file_get_info(const rtc_scene_file* file, rtc_scene_file_info* info);
+const char* rtc_scene_file_skipped(const rtc_scene_file* file, uint32_t index);
+void rtc_scene_file_free(rtc_scene_file* file);
+
 /* ------------------------------------------------------------------------------------------------ */
 /* render parameters                                                                                 */
 /* ------------------------------------------------------------------------------------------------ */

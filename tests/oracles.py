@@ -14,7 +14,7 @@ from pathlib import Path
 
 import numpy as np
 
-from cortexraytracercuda_b200.scene import RenderParams, Scene, SceneDesc
+from cortexraytracercuda_b200.scene import RenderParams, Scene, SceneDesc, SceneFile
 
 ORACLE = Path(__file__).resolve().parent.parent / "oracle"
 
@@ -43,7 +43,7 @@ class RefCpu(_Base):
     prefix = "refh_"
 
     def scene(self, scene: Scene, bvh_kind: int = -1):
-        d = SceneDesc(scene)
+        d = scene if isinstance(scene, SceneFile) else SceneDesc(scene)
         h = self.lib.refh_scene_create(d.ptr(), C.c_int(bvh_kind))
         if not h:
             raise RuntimeError(self.error())
@@ -121,7 +121,7 @@ class RefGpu(_Base):
 
     def scene(self, scene: Scene):
         self.setup()
-        d = SceneDesc(scene)
+        d = scene if isinstance(scene, SceneFile) else SceneDesc(scene)
         h = self.lib.refg_scene_create(d.ptr())
         if not h:
             raise RuntimeError(self.error())
@@ -182,7 +182,7 @@ class Port:
         self.lib.port_set_trig(C.c_int(mode))
 
     def scene(self, scene: Scene):
-        d = SceneDesc(scene)
+        d = scene if isinstance(scene, SceneFile) else SceneDesc(scene)
         h = self.lib.port_scene_create(d.ptr())
         if not h:
             raise RuntimeError(self.lib.port_last_error().decode())
@@ -251,7 +251,7 @@ class Fp64:
                pix: np.ndarray | None = None, threads: int = 0) -> np.ndarray:
         """Radiance sums (n, 3) float64 of the given frame-buffer pixels (all pixels by default)."""
         import os
-        d = SceneDesc(scene)
+        d = scene if isinstance(scene, SceneFile) else SceneDesc(scene)
         h = self.lib.f64_scene_create(d.ptr())
         try:
             if pix is None:
