@@ -481,3 +481,24 @@ def test_scene_file_renders_like_the_reference_cpu(tmp_path, refcpu):
     ref, _ = refcpu.scene(f).render_pixels(p, pix)
     st = oracles.parity_stats(ours, ref)
     assert st["frac_exact"] >= 0.999, st
+
+
+def test_reference_scene_files(ref_loader):
+    """Every `.scene` file the reference ships (data/scenes), read by both readers from the reference's
+    root directory: identical descriptions (its OBJ and image paths, written relative to a build
+    directory, are missing on both sides from there)."""
+    ref = Path(os.environ.get("REF", "/root/reference"))
+    files = sorted((ref / "data" / "scenes").glob("*.scene"))
+    if not files:
+        pytest.skip("the reference's scene files are not available")
+    cwd = os.getcwd()
+    try:
+        os.chdir(ref)
+        for path in files:
+            rel = path.relative_to(ref)
+            r = subprocess.run([str(ref_loader), str(rel)], cwd=ref, capture_output=True, text=True, timeout=120)
+            assert r.returncode == 0, path.name
+            mine = SceneFile(rel, flags=SCENE_FILE_REFERENCE_CAPACITY, decode_images=False)
+            _same(json.loads(r.stdout.strip().splitlines()[-1]), _desc_json(mine), path.name)
+    finally:
+        os.chdir(cwd)
