@@ -185,6 +185,71 @@ def cornell(light_intensity=1.0) -> Scene:
     return s
 
 
+def _rot_inv(deg):
+    """rt::rotate's inverse matrix (rotations by -x, -y, -z degrees about x, then y, then z), in double."""
+    m = np.eye(3)
+    for ax, a in enumerate(deg):
+        c, s_ = np.cos(np.radians(-a)), np.sin(np.radians(-a))
+        r = np.eye(3)
+        i, j = [(1, 2), (0, 2), (0, 1)][ax]
+        r[i, i], r[j, j] = c, c
+        r[i, j], r[j, i] = (-s_, s_) if ax != 1 else (s_, -s_)
+        m = m @ r
+    return m
+
+
+def placed(s: Scene, at, rotate=None, scale=None) -> int:
+    """A transform that puts the object's origin at world point `at`.  The reference applies translate
+    inside rotate and scale (world = s * R(p + t)), so t = R_inv(at / s)."""
+    sc = np.ones(3) if scale is None else np.asarray(scale, float)
+    t = np.asarray(at, float) / sc
+    if rotate is not None:
+        t = _rot_inv(rotate) @ t
+    return s.transform(translate=tuple(float(x) for x in t), rotate=rotate, scale=scale)
+
+
+def transforms_scene(seed=DEFAULT_SEED, multi_axis=True) -> Scene:
+    """The Cornell room with the reference's own box primitives under transforms (the two boxes of
+    cornell_box.scene, turned about y), a scaled glass sphere, a turned metal quad and an untransformed
+    box; with `multi_axis`, also a box and a small displaced icosphere turned about two and three axes
+    and scaled.  The reference culls a multi-axis rotation by corners mapped with its forward matrix,
+    which is not where its inverse-mapped rays find the object, so those two objects differ at their
+    edges from the reference's own build; the kernel and the C restatement agree on them."""
+    s = Scene(name="xforms")
+    red = s.lambertian((0.65, 0.05, 0.05))
+    green = s.lambertian((0.12, 0.45, 0.15))
+    white = s.lambertian((0.73, 0.73, 0.73))
+    blue = s.lambertian((0.2, 0.3, 0.75))
+    s.dir_light((278.0, 554.0, 332.0), (-130.0, 0.0, 0.0), (0.0, 0.0, -105.0), (15.0, 15.0, 15.0),
+                intensity=1.0, invisible=True)
+    s.quad((555, 0, 0), (0, 555, 0), (0, 0, 555), green)
+    s.quad((0, 0, 0), (0, 555, 0), (0, 0, 555), red)
+    s.quad((0, 0, 0), (555, 0, 0), (0, 0, 555), white)
+    s.quad((555, 555, 555), (-555, 0, 0), (0, 0, -555), white)
+    s.quad((0, 0, 555), (555, 0, 0), (0, 555, 0), white)
+    s.quad((-60, -60, 0), (120, 0, 0), (0, 120, 0), s.metal((0.85, 0.85, 0.9), 0.05),
+           transform=placed(s, (450, 300, 520), rotate=(0.0, 25.0, 0.0)))
+    s.sphere((0, 0, 0), 1.0, s.dielectric(1.5), transform=placed(s, (150, 380, 250), scale=(60, 45, 60)))
+    s.box((0, 0, 0), (165, 330, 165), white, transform=placed(s, (347.5, 165.0, 377.5), rotate=(0, -15, 0)))
+    s.box((0, 0, 0), (165, 165, 165), white, transform=placed(s, (212.5, 82.5, 147.5), rotate=(0, 18, 0)))
+    s.box((90, 470, 470), (60, 60, 60), red)
+    if multi_axis:
+        s.box((0, 0, 0), (70, 70, 70), blue, transform=placed(s, (440, 60, 110), rotate=(30, 40, 0), scale=(1.0, 1.2, 1.0)))
+        v, f = displaced_icosphere(2, 0.1, seed)
+        s.mesh(v, f, s.metal((0.9, 0.8, 0.5), 0.2),
+               transform=placed(s, (300, 430, 200), rotate=(20, 35, 10), scale=(55, 55, 55)))
+    s.camera = Camera(look_from=(278, 278, -800), look_at=(278, 278, 0), up=(0, 1, 0), vfov=40.0, aspect=1.0,
+                      aperture=0.0, focus=100.0)
+    s.set_background_constant((0.0, 0.0, 0.0))
+    return s
+
+
+def transforms_params(**kw) -> RenderParams:
+    p = dict(width=64, height=64, spp=16, max_depth=8)
+    p.update(kw)
+    return RenderParams(**p)
+
+
 def cornell_params(**kw) -> RenderParams:
     p = dict(width=256, height=256, spp=16, max_depth=8)
     p.update(kw)
@@ -388,4 +453,8 @@ SCENES = {
     "textured": (textured, lambda **kw: RenderParams(**{**dict(width=160, height=120, spp=16, max_depth=10), **kw})),
     "icosphere": (icosphere_scene, lambda **kw: RenderParams(**{**dict(width=150, height=100, spp=16, max_depth=12), **kw})),
     "lights": (lights_scene, lambda **kw: RenderParams(**{**dict(width=120, height=90, spp=16, max_depth=10), **kw})),
+    # boxes and transforms; "xforms" leaves out the multi-axis rotations the reference clips (see
+    # transforms_scene), so the reference's own build renders it exactly
+    "xforms": (lambda seed=DEFAULT_SEED: transforms_scene(seed, multi_axis=False), transforms_params),
+    "xforms_multi": (transforms_scene, transforms_params),
 }

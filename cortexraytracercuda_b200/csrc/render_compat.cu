@@ -79,8 +79,9 @@ __global__ void __launch_bounds__(128) rtc_render_compat(DevScene S, DevParams P
 
 #if RTC_FLAVOR == 1
 __device__ __forceinline__ int32_t item_gid(const DevScene& S, uint32_t it) {
-    uint32_t kind = it >> 30, idx = it & 0x3fffffffu;
+    uint32_t kind = it >> ITEM_KIND_SHIFT, idx = it & ITEM_INDEX_MASK;
     switch (kind) {
+    case ITEM_XPRIM: return __ldg(S.xprim + idx).w;
     case ITEM_SPHERE: return __ldg(S.sph_aux + idx).y;
     case ITEM_QUAD: return __float_as_int(__ldg(S.quad + 5 * (size_t)idx + 2).w);
     case ITEM_LIGHT: return __float_as_int(__ldg(S.light + 6 * (size_t)idx + 2).w);

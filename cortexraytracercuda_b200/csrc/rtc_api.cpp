@@ -153,6 +153,81 @@ Aabb box_of(const V3* pts, int n) {
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
+// glm::rotate(m, angle, axis) for a coordinate axis (glm/ext/matrix_transform.inl:18-46), in float and
+// in the same operation order; the axis is a unit vector, which normalize leaves unchanged.  `m` is
+// column-major (m[column][row]).
+void glm_rotate_axis(float m[4][4], float angle, int ax) {
+    const float c = std::cos(angle), s = std::sin(angle);
+    float axis[3] = {0.0f, 0.0f, 0.0f};
+    axis[ax] = 1.0f;
+    const float temp[3] = {(1.0f - c) * axis[0], (1.0f - c) * axis[1], (1.0f - c) * axis[2]};
+    float R[3][3];
+    R[0][0] = c + temp[0] * axis[0];
+    R[0][1] = temp[0] * axis[1] + s * axis[2];
+    R[0][2] = temp[0] * axis[2] - s * axis[1];
+    R[1][0] = temp[1] * axis[0] - s * axis[2];
+    R[1][1] = c + temp[1] * axis[1];
+    R[1][2] = temp[1] * axis[2] + s * axis[0];
+    R[2][0] = temp[2] * axis[0] + s * axis[1];
+    R[2][1] = temp[2] * axis[1] - s * axis[0];
+    R[2][2] = c + temp[2] * axis[2];
+    float out[3][4];
+    for (int j = 0; j < 3; ++j)
+        for (int i = 0; i < 4; ++i) out[j][i] = (m[0][i] * R[j][0] + m[1][i] * R[j][1]) + m[2][i] * R[j][2];
+    for (int j = 0; j < 3; ++j)
+        for (int i = 0; i < 4; ++i) m[j][i] = out[j][i];
+}
+
+// rt::rotate's matrix (rotate.cuh hit()): identity, then glm::rotate about x, y and z by
+// degrees_to_radians(sign * angle) = sign * angle * M_PI / 180.0f with the reference's float M_PI.
+void rotate_matrix(const float deg[3], float sign, float m[4][4]) {
+    for (int j = 0; j < 4; ++j)
+        for (int i = 0; i < 4; ++i) m[j][i] = i == j ? 1.0f : 0.0f;
+    for (int ax = 0; ax < 3; ++ax) glm_rotate_axis(m, (sign * deg[ax]) * 3.14159265358979323846f / 180.0f, ax);
+}
+
+// Device transform record (rtc_dev.h `xf`): 8 float4.
+void put_transform(const rtc_transform& T, std::vector<float4>& xf) {
+    float inv[4][4], fwd[4][4];
+    rotate_matrix(T.rotate, -1.0f, inv);
+    rotate_matrix(T.rotate, 1.0f, fwd);
+    xf.push_back(make_float4(T.translate[0], T.translate[1], T.translate[2], ibits((int32_t)(T.flags & 7u))));
+    xf.push_back(make_float4(T.scale[0], T.scale[1], T.scale[2], 0.0f));
+    for (int j = 0; j < 3; ++j) xf.push_back(make_float4(inv[j][0], inv[j][1], inv[j][2], 0.0f));
+    for (int j = 0; j < 3; ++j) xf.push_back(make_float4(fwd[j][0], fwd[j][1], fwd[j][2], 0.0f));
+}
+
+// World-space bounds of an object-space box seen through transform T: the corners mapped by the exact
+// inverse of the ray's path into object space (o -> o / s -> R_inv o -> o - t), i.e. x -> s * R_inv^T
+// (x + t), in double, padded for the float rounding of that path.
+Aabb transform_box(const rtc_transform& T, const Aabb& b) {
+    float inv[4][4];
+    rotate_matrix(T.rotate, -1.0f, inv);
+    double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    double mag = 0.0;
+    for (int c = 0; c < 8; ++c) {
+        double p[3] = {(c & 1) ? b.hi[0] : b.lo[0], (c & 2) ? b.hi[1] : b.lo[1], (c & 4) ? b.hi[2] : b.lo[2]};
+        if (T.flags & RTC_XF_TRANSLATE)
+            for (int k = 0; k < 3; ++k) p[k] += T.translate[k];
+        mag = std::max({mag, std::fabs(p[0]), std::fabs(p[1]), std::fabs(p[2])});
+        if (T.flags & RTC_XF_ROTATE) {
+            // R_inv^T p: row k of the transpose is column k of R_inv
+            double q[3];
+            for (int k = 0; k < 3; ++k) q[k] = inv[k][0] * p[0] + inv[k][1] * p[1] + inv[k][2] * p[2];
+            for (int k = 0; k < 3; ++k) p[k] = q[k];
+        }
+        if (T.flags & RTC_XF_SCALE)
+            for (int k = 0; k < 3; ++k) p[k] *= T.scale[k];
+        for (int k = 0; k < 3; ++k) { lo[k] = std::min(lo[k], p[k]); hi[k] = std::max(hi[k], p[k]); }
+    }
+    double smax = 1.0;
+    if (T.flags & RTC_XF_SCALE) smax = std::max({std::fabs((double)T.scale[0]), std::fabs((double)T.scale[1]), std::fabs((double)T.scale[2])});
+    const double e = 4e-6 * mag * smax + 1e-6;
+    Aabb r;
+    for (int k = 0; k < 3; ++k) { r.lo[k] = (float)(lo[k] - e); r.hi[k] = (float)(hi[k] + e); }
+    return r;
+}
+
 }  // namespace
 
 // perspective_camera::initialize (perspective_camera.cuh:41-108), operation by operation.
@@ -249,10 +324,32 @@ rtc_status rtc_build_host_scene(const rtc_scene_desc* d, HostScene& H, uint32_t 
             !std::isfinite(L.intensity) || !std::isfinite(L.cutoff) || !std::isfinite(L.falloff))
             return bad("spot light " + std::to_string(i) + " is invalid");
     }
+    // transforms (1-based references, 0 = none) and boxes
+    if ((d->num_transforms && !d->transforms) || (d->num_boxes && !d->boxes)) return bad("count > 0 with a null array");
+    for (uint32_t i = 0; i < d->num_transforms; ++i) {
+        const rtc_transform& T = d->transforms[i];
+        if ((T.flags & ~7u) || !finite3(T.translate) || !finite3(T.rotate) || !finite3(T.scale))
+            return bad("transform " + std::to_string(i) + " is invalid");
+    }
+    auto xf_ok = [&](const uint32_t* refs, uint32_t n) {
+        if (!refs) return true;
+        for (uint32_t i = 0; i < n; ++i)
+            if (refs[i] > d->num_transforms) return false;
+        return true;
+    };
+    if (!xf_ok(d->sphere_transforms, d->num_spheres) || !xf_ok(d->quad_transforms, d->num_quads) ||
+        !xf_ok(d->mesh_transforms, d->num_meshes))
+        return bad("transform reference out of range");
+    for (uint32_t i = 0; i < d->num_boxes; ++i) {
+        const rtc_box& B = d->boxes[i];
+        if (!mat_ok(B.material) || !finite3(B.center) || !finite3(B.size) || B.transform > d->num_transforms)
+            return bad("box " + std::to_string(i) + " is invalid");
+    }
+    auto xf_of = [](const uint32_t* refs, uint32_t i) -> int32_t { return refs ? (int32_t)refs[i] - 1 : -1; };
     // the light list: omni lights, directional lights, spot lights (load_scene, gpu.cu:504-523)
     const uint32_t n_omni = d->num_omni_lights, n_dir = d->num_dir_lights, n_spot = d->num_spot_lights;
     const uint32_t nlights = n_omni + n_dir + n_spot;
-    const uint64_t nprims = (uint64_t)nlights + d->num_spheres + d->num_quads + ntri;
+    const uint64_t nprims = (uint64_t)nlights + d->num_spheres + d->num_quads + 6ull * d->num_boxes + ntri;
     if (nprims == 0) return bad("scene has no primitives");
     if (nprims >= (1ull << 26)) return bad("scene has too many primitives (max 2^26)");
     if (d->background.kind < 0 || d->background.kind > 2) return bad("unknown background kind");
@@ -260,8 +357,10 @@ rtc_status rtc_build_host_scene(const rtc_scene_desc* d, HostScene& H, uint32_t 
         (!d->background.env_rgb || d->background.env_width <= 0 || d->background.env_height <= 0))
         return bad("environment map missing");
 
-    // ---- primitives in global order: lights, spheres, quads, triangles ------------------------
-    struct PrimRef { uint8_t kind; uint32_t src; };   // src: index within its own kind (mesh tris flattened)
+    // ---- primitives in global order: lights, spheres, quads, boxes, triangles -------------------
+    // kind ITEM_XPRIM: a transformed sphere / quad / triangle or a box face; `inner` is then its own kind
+    // (XPRIM_RECT for a face: src = box, face 0-5) and `xf` its transform (-1 for an untransformed box).
+    struct PrimRef { uint8_t kind; uint8_t inner; uint8_t face; uint32_t src; int32_t xf; };
     std::vector<PrimRef> prims;
     prims.reserve(nprims);
     BvhInput bin;
@@ -273,7 +372,7 @@ rtc_status rtc_build_host_scene(const rtc_scene_desc* d, HostScene& H, uint32_t 
     };
     for (uint32_t i = 0; i < n_omni; ++i) {
         bin.boxes.push_back(sphere_light_box(d->omni_lights[i].position, d->omni_lights[i].radius));
-        prims.push_back({ITEM_LIGHT, i});
+        prims.push_back({ITEM_LIGHT, 0, 0, i, -1});
     }
     for (uint32_t i = 0; i < d->num_dir_lights; ++i) {
         const rtc_dir_light& L = d->dir_lights[i];
@@ -281,25 +380,62 @@ rtc_status rtc_build_host_scene(const rtc_scene_desc* d, HostScene& H, uint32_t 
         V3 hu = mul(0.5f, U), hv = mul(0.5f, Vv);
         V3 c[4] = {sub(sub(P, hu), hv), add(sub(P, hu), hv), sub(add(P, hu), hv), add(add(P, hu), hv)};
         bin.boxes.push_back(box_of(c, 4));
-        prims.push_back({ITEM_LIGHT, n_omni + i});
+        prims.push_back({ITEM_LIGHT, 0, 0, n_omni + i, -1});
     }
     for (uint32_t i = 0; i < n_spot; ++i) {
         bin.boxes.push_back(sphere_light_box(d->spot_lights[i].position, d->spot_lights[i].radius));
-        prims.push_back({ITEM_LIGHT, n_omni + n_dir + i});
+        prims.push_back({ITEM_LIGHT, 0, 0, n_omni + n_dir + i, -1});
     }
     for (uint32_t i = 0; i < d->num_spheres; ++i) {
         const rtc_sphere& S = d->spheres[i];
         float r = std::fabs(S.radius);
         V3 c[2] = {v3(S.center[0] - r, S.center[1] - r, S.center[2] - r), v3(S.center[0] + r, S.center[1] + r, S.center[2] + r)};
-        bin.boxes.push_back(box_of(c, 2));
-        prims.push_back({ITEM_SPHERE, i});
+        const int32_t xi = xf_of(d->sphere_transforms, i);
+        bin.boxes.push_back(xi >= 0 ? transform_box(d->transforms[xi], box_of(c, 2)) : box_of(c, 2));
+        if (xi >= 0) prims.push_back({ITEM_XPRIM, ITEM_SPHERE, 0, i, xi});
+        else prims.push_back({ITEM_SPHERE, 0, 0, i, -1});
     }
     for (uint32_t i = 0; i < d->num_quads; ++i) {
         const rtc_quad& Q = d->quads[i];
         V3 q = v3(Q.q), u = v3(Q.u), v = v3(Q.v);
         V3 c[4] = {q, add(q, u), add(q, v), add(add(q, u), v)};
-        bin.boxes.push_back(box_of(c, 4));
-        prims.push_back({ITEM_QUAD, i});
+        const int32_t xi = xf_of(d->quad_transforms, i);
+        bin.boxes.push_back(xi >= 0 ? transform_box(d->transforms[xi], box_of(c, 4)) : box_of(c, 4));
+        if (xi >= 0) prims.push_back({ITEM_XPRIM, ITEM_QUAD, 0, i, xi});
+        else prims.push_back({ITEM_QUAD, 0, 0, i, -1});
+    }
+    // box faces (box.cuh:40-52): pmin = center - size / 2, pmax = pmin + size; faces front (z = pmax.z),
+    // back (z = pmin.z, flipped), top (y = pmax.y), bottom (flipped), right (x = pmax.x), left (flipped)
+    auto box_face = [&](const rtc_box& B, int face, float r0[4], float r1[4]) {
+        float lo[3], hi[3];
+        for (int k = 0; k < 3; ++k) {
+            lo[k] = B.center[k] - (B.size[k] / 2.0f);
+            hi[k] = lo[k] + B.size[k];
+        }
+        const int axis = face / 2;                    // 0 xy, 1 xz, 2 yz
+        const bool low = (face & 1) != 0;
+        const int a = axis == 2 ? 1 : 0, b = axis == 0 ? 1 : 2, n = axis == 0 ? 2 : axis == 1 ? 1 : 0;
+        r0[0] = lo[a]; r0[1] = hi[a]; r0[2] = lo[b]; r0[3] = hi[b];
+        r1[0] = low ? lo[n] : hi[n];
+        r1[1] = ibits(axis);
+        r1[2] = low ? 1.0f : 0.0f;
+        r1[3] = ibits(B.material);
+    };
+    for (uint32_t i = 0; i < d->num_boxes; ++i) {
+        const rtc_box& B = d->boxes[i];
+        const int32_t xi = (int32_t)B.transform - 1;
+        for (int f = 0; f < 6; ++f) {
+            float r0[4], r1[4];
+            box_face(B, f, r0, r1);
+            const int axis = f / 2, a = axis == 2 ? 1 : 0, b = axis == 0 ? 1 : 2, n = axis == 0 ? 2 : axis == 1 ? 1 : 0;
+            V3 c[2];
+            float p0[3], p1[3];
+            p0[a] = r0[0]; p1[a] = r0[1]; p0[b] = r0[2]; p1[b] = r0[3]; p0[n] = p1[n] = r1[0];
+            c[0] = v3(p0[0], p0[1], p0[2]);
+            c[1] = v3(p1[0], p1[1], p1[2]);
+            bin.boxes.push_back(xi >= 0 ? transform_box(d->transforms[xi], box_of(c, 2)) : box_of(c, 2));
+            prims.push_back({ITEM_XPRIM, (uint8_t)XPRIM_RECT, (uint8_t)f, i, xi});
+        }
     }
     std::vector<uint32_t> tri_mesh;   // mesh of each flattened triangle
     std::vector<uint32_t> tri_face;
@@ -316,8 +452,10 @@ rtc_status rtc_build_host_scene(const rtc_scene_desc* d, HostScene& H, uint32_t 
                 V3 c[3] = {v3(M.vertices + 3 * ia), v3(M.vertices + 3 * ib), v3(M.vertices + 3 * ic)};
                 if (!finite3(M.vertices + 3 * ia) || !finite3(M.vertices + 3 * ib) || !finite3(M.vertices + 3 * ic))
                     return bad("mesh vertex is not finite");
-                bin.boxes.push_back(box_of(c, 3));
-                prims.push_back({ITEM_TRI, t});
+                const int32_t xi = xf_of(d->mesh_transforms, m);
+                bin.boxes.push_back(xi >= 0 ? transform_box(d->transforms[xi], box_of(c, 3)) : box_of(c, 3));
+                if (xi >= 0) prims.push_back({ITEM_XPRIM, ITEM_TRI, 0, t, xi});
+                else prims.push_back({ITEM_TRI, 0, 0, t, -1});
                 tri_mesh.push_back(m);
                 tri_face.push_back(f);
             }
@@ -395,10 +533,13 @@ rtc_status rtc_build_host_scene(const rtc_scene_desc* d, HostScene& H, uint32_t 
 
     // ---- per-kind arrays in leaf order ---------------------------------------------------------
     std::vector<uint32_t> items(bvh.order.size());
-    std::vector<float4> sph, tri, tri_n, tri_vn, quad, light(6 * (size_t)nlights);
+    std::vector<float4> sph, tri, tri_n, tri_vn, quad, light(6 * (size_t)nlights), rect, xf;
     std::vector<int2> sph_aux;
-    // global id bases: the lights come first, in light-list order (index = light id = global id)
-    const uint32_t base_sph = nlights, base_quad = base_sph + d->num_spheres, base_tri = base_quad + d->num_quads;
+    std::vector<int4> xprim;
+    // global id bases: the lights come first, in light-list order (index = light id = global id); one id
+    // per box
+    const uint32_t base_sph = nlights, base_quad = base_sph + d->num_spheres, base_box = base_quad + d->num_quads,
+                   base_tri = base_box + d->num_boxes;
     for (uint32_t i = 0; i < n_dir; ++i) {
         const rtc_dir_light& L = d->dir_lights[i];
         const uint32_t li = n_omni + i;
@@ -435,53 +576,78 @@ rtc_status rtc_build_host_scene(const rtc_scene_desc* d, HostScene& H, uint32_t 
         put_sphere_light(n_omni + n_dir + i, L.position, L.radius, L.direction, std::cos(rad), L.falloff, L.invisible,
                          L.color, L.intensity);
     }
+    auto pack_sphere = [&](uint32_t src) {
+        const rtc_sphere& S = d->spheres[src];
+        const uint32_t typed = (uint32_t)sph.size();
+        sph.push_back(make_float4(S.center[0], S.center[1], S.center[2], S.radius));
+        sph_aux.push_back(make_int2(S.material, (int)(base_sph + src)));
+        return typed;
+    };
+    auto pack_quad = [&](uint32_t src) {
+        const rtc_quad& Q = d->quads[src];
+        V3 q0 = v3(Q.q), u = v3(Q.u), v = v3(Q.v);
+        PlanarPre pp = planar_pre(q0, u, v);
+        const uint32_t typed = (uint32_t)(quad.size() / 5);
+        quad.push_back(make_float4(pp.normal.x, pp.normal.y, pp.normal.z, pp.D));
+        quad.push_back(make_float4(q0.x, q0.y, q0.z, ibits(Q.material)));
+        quad.push_back(make_float4(u.x, u.y, u.z, ibits((int32_t)(base_quad + src))));
+        quad.push_back(make_float4(v.x, v.y, v.z, 0.0f));
+        quad.push_back(make_float4(pp.w.x, pp.w.y, pp.w.z, 0.0f));
+        return typed;
+    };
+    auto pack_tri = [&](uint32_t src) {
+        const rtc_mesh& M = d->meshes[tri_mesh[src]];
+        uint32_t f = tri_face[src];
+        uint32_t ia = M.indices[3 * f], ib = M.indices[3 * f + 1], ic = M.indices[3 * f + 2];
+        V3 a = v3(M.vertices + 3 * ia), b = v3(M.vertices + 3 * ib), c = v3(M.vertices + 3 * ic);
+        // triangle::triangle (triangle.cuh:87-123): v0_v1, v0_v2, middle_normal
+        V3 e1 = sub(b, a), e2 = sub(c, a);
+        V3 mn = unit(cross(sub(a, b), sub(a, c)));
+        const uint32_t typed = (uint32_t)(tri.size() / 3);
+        int32_t smooth_slot = -1;
+        if (M.smooth && M.normals) {
+            smooth_slot = (int32_t)(tri_vn.size() / 3);
+            for (uint32_t vi : {ia, ib, ic}) {
+                V3 nn = unit(v3(M.normals + 3 * vi));
+                tri_vn.push_back(make_float4(nn.x, nn.y, nn.z, 0.0f));
+            }
+        }
+        tri.push_back(make_float4(a.x, a.y, a.z, ibits(M.material)));
+        tri.push_back(make_float4(e1.x, e1.y, e1.z, ibits((int32_t)(base_tri + src))));
+        tri.push_back(make_float4(e2.x, e2.y, e2.z, ibits(smooth_slot)));
+        tri_n.push_back(make_float4(mn.x, mn.y, mn.z, 0.0f));
+        return typed;
+    };
     for (size_t k = 0; k < bvh.order.size(); ++k) {
         const PrimRef& pr = prims[bvh.order[k]];
         uint32_t typed = 0;
         switch (pr.kind) {
         case ITEM_LIGHT: typed = pr.src; break;
-        case ITEM_SPHERE: {
-            const rtc_sphere& S = d->spheres[pr.src];
-            typed = (uint32_t)sph.size();
-            sph.push_back(make_float4(S.center[0], S.center[1], S.center[2], S.radius));
-            sph_aux.push_back(make_int2(S.material, (int)(base_sph + pr.src)));
-        } break;
-        case ITEM_QUAD: {
-            const rtc_quad& Q = d->quads[pr.src];
-            V3 q0 = v3(Q.q), u = v3(Q.u), v = v3(Q.v);
-            PlanarPre pp = planar_pre(q0, u, v);
-            typed = (uint32_t)(quad.size() / 5);
-            quad.push_back(make_float4(pp.normal.x, pp.normal.y, pp.normal.z, pp.D));
-            quad.push_back(make_float4(q0.x, q0.y, q0.z, ibits(Q.material)));
-            quad.push_back(make_float4(u.x, u.y, u.z, ibits((int32_t)(base_quad + pr.src))));
-            quad.push_back(make_float4(v.x, v.y, v.z, 0.0f));
-            quad.push_back(make_float4(pp.w.x, pp.w.y, pp.w.z, 0.0f));
-        } break;
-        default: {
-            const rtc_mesh& M = d->meshes[tri_mesh[pr.src]];
-            uint32_t f = tri_face[pr.src];
-            uint32_t ia = M.indices[3 * f], ib = M.indices[3 * f + 1], ic = M.indices[3 * f + 2];
-            V3 a = v3(M.vertices + 3 * ia), b = v3(M.vertices + 3 * ib), c = v3(M.vertices + 3 * ic);
-            // triangle::triangle (triangle.cuh:87-123): v0_v1, v0_v2, middle_normal
-            V3 e1 = sub(b, a), e2 = sub(c, a);
-            V3 mn = unit(cross(sub(a, b), sub(a, c)));
-            typed = (uint32_t)(tri.size() / 3);
-            int32_t smooth_slot = -1;
-            if (M.smooth && M.normals) {
-                smooth_slot = (int32_t)(tri_vn.size() / 3);
-                for (uint32_t vi : {ia, ib, ic}) {
-                    V3 nn = unit(v3(M.normals + 3 * vi));
-                    tri_vn.push_back(make_float4(nn.x, nn.y, nn.z, 0.0f));
-                }
+        case ITEM_SPHERE: typed = pack_sphere(pr.src); break;
+        case ITEM_QUAD: typed = pack_quad(pr.src); break;
+        case ITEM_TRI: typed = pack_tri(pr.src); break;
+        default: {   // ITEM_XPRIM
+            uint32_t inner = 0, gid = 0;
+            switch (pr.inner) {
+            case ITEM_SPHERE: inner = pack_sphere(pr.src); gid = base_sph + pr.src; break;
+            case ITEM_QUAD: inner = pack_quad(pr.src); gid = base_quad + pr.src; break;
+            case ITEM_TRI: inner = pack_tri(pr.src); gid = base_tri + pr.src; break;
+            default: {
+                float r0[4], r1[4];
+                box_face(d->boxes[pr.src], pr.face, r0, r1);
+                inner = (uint32_t)(rect.size() / 2);
+                rect.push_back(make_float4(r0[0], r0[1], r0[2], r0[3]));
+                rect.push_back(make_float4(r1[0], r1[1], r1[2], r1[3]));
+                gid = base_box + pr.src;
+            } break;
             }
-            tri.push_back(make_float4(a.x, a.y, a.z, ibits(M.material)));
-            tri.push_back(make_float4(e1.x, e1.y, e1.z, ibits((int32_t)(base_tri + pr.src))));
-            tri.push_back(make_float4(e2.x, e2.y, e2.z, ibits(smooth_slot)));
-            tri_n.push_back(make_float4(mn.x, mn.y, mn.z, 0.0f));
+            typed = (uint32_t)xprim.size();
+            xprim.push_back(make_int4(pr.xf, pr.inner, (int)inner, (int)gid));
         } break;
         }
-        items[k] = ((uint32_t)pr.kind << 30) | typed;
+        items[k] = ((uint32_t)pr.kind << ITEM_KIND_SHIFT) | typed;
     }
+    for (uint32_t i = 0; i < d->num_transforms; ++i) put_transform(d->transforms[i], xf);
 
     // ---- camera: perspective_camera::initialize (perspective_camera.cuh:41-108) -----------------
     DevCamera cam{};
@@ -513,6 +679,9 @@ rtc_status rtc_build_host_scene(const rtc_scene_desc* d, HostScene& H, uint32_t 
     size_t o_tf = add_chunk(tex_f.data(), tex_f.size() * 16);
     size_t o_img = add_chunk(img_i.data(), img_i.size() * 16);
     size_t o_imgb = add_chunk(img_bytes.data(), img_bytes.size());
+    size_t o_xprim = add_chunk(xprim.data(), xprim.size() * 16);
+    size_t o_xf = add_chunk(xf.data(), xf.size() * 16);
+    size_t o_rect = add_chunk(rect.data(), rect.size() * 16);
     size_t env_bytes = d->background.kind == RTC_BG_ENV_MAP
                            ? (size_t)d->background.env_width * d->background.env_height * 3 * sizeof(float) : 0;
     size_t o_env = add_chunk(env_bytes ? d->background.env_rgb : nullptr, env_bytes);
@@ -540,6 +709,12 @@ rtc_status rtc_build_host_scene(const rtc_scene_desc* d, HostScene& H, uint32_t 
     D.tex_f = (const float4*)off(o_tf);
     D.images = (const int4*)off(o_img);
     D.image_bytes = (const uint8_t*)off(o_imgb);
+    D.xprim = (const int4*)off(o_xprim);
+    D.xf = (const float4*)off(o_xf);
+    D.rect = (const float4*)off(o_rect);
+    D.num_xprim = (uint32_t)xprim.size();
+    D.num_xf = d->num_transforms;
+    D.num_rect = (uint32_t)(rect.size() / 2);
     D.num_nodes = bvh.num_nodes;
     D.num_nodes8 = bvh.num_nodes8;
     D.num_items = (uint32_t)items.size();
@@ -579,6 +754,7 @@ DevScene rtc_rebase_scene(const HostScene& H, uint8_t* base) {
     if (D.nodes8) rb(D.nodes8);
     rb(D.sph); rb(D.sph_aux); rb(D.tri); rb(D.tri_n); rb(D.tri_vn); rb(D.quad);
     rb(D.light); rb(D.mat_i); rb(D.mat_f); rb(D.tex_i); rb(D.tex_f); rb(D.images); rb(D.image_bytes);
+    rb(D.xprim); rb(D.xf); rb(D.rect);
     if (D.bg.env) rb(D.bg.env);
     return D;
 }

@@ -13,7 +13,13 @@
 //              child c's box on axis a is [p.a + qlo.a[c] * 2^e.a, p.a + qhi.a[c] * 2^e.a] (rounded outwards
 //              when built, so it encloses the child's exact box); slots at or past `children` are
 //              unused.  Same leaves and leaf order as `nodes`; renders use it when RTC_FLAG_WIDE_BVH is set.
-//   items      uint32 per leaf entry, leaf order: (kind << 30) | index into that kind's array.
+//   items      uint32 per leaf entry, leaf order: (kind << 29) | index into that kind's array.
+//   xprim      int4 per transformed primitive or box face (leaf order): (transform or -1, inner kind,
+//              inner index, global id).  The inner record sits in the sph / quad / tri / rect array.
+//   xf         8 x float4 per transform: (translate.xyz, flags) (scale.xyz, -) (inverse rotation columns
+//              0..2, xyz) (forward rotation columns 0..2, xyz), the glm matrices of rt::rotate
+//   rect       2 x float4 per box face: (a0, a1, b0, b1) (k, axis, flip, material); axis 0 = xy_rect
+//              (plane z = k), 1 = xz_rect (y = k), 2 = yz_rect (x = k)
 //   sph        float4 (center.xyz, radius)                      16 B / sphere  (leaf order)
 //   sph_aux    int2   (material, global id)
 //   tri        3 x float4: (v0.xyz, material bits) (v1-v0, gid bits) (v2-v0, smooth-normal slot or -1)
@@ -37,7 +43,12 @@
 
 namespace rtc {
 
-enum ItemKind : uint32_t { ITEM_SPHERE = 0, ITEM_QUAD = 1, ITEM_TRI = 2, ITEM_LIGHT = 3 };
+enum ItemKind : uint32_t { ITEM_SPHERE = 0, ITEM_QUAD = 1, ITEM_TRI = 2, ITEM_LIGHT = 3, ITEM_XPRIM = 4 };
+// Item word: (kind << ITEM_KIND_SHIFT) | index into that kind's array.
+constexpr uint32_t ITEM_KIND_SHIFT = 29;
+constexpr uint32_t ITEM_INDEX_MASK = (1u << ITEM_KIND_SHIFT) - 1u;
+// Inner kinds of an xprim: ITEM_SPHERE, ITEM_QUAD, ITEM_TRI, or a box face.
+constexpr int XPRIM_RECT = 5;
 // Material kinds past the public rtc_material_kind values: a spot light's diffuse_spot_light.
 constexpr int MAT_SPOT_LIGHT = 4;
 constexpr int LEAF_COUNT_BITS = 5;
@@ -91,6 +102,9 @@ struct DevScene {
     const float4* tex_f;
     const int4* images;
     const uint8_t* image_bytes;
+    const int4* xprim;
+    const float4* xf;
+    const float4* rect;
     uint32_t num_nodes;
     uint32_t num_nodes8;
     uint32_t num_items;
@@ -99,6 +113,7 @@ struct DevScene {
     uint32_t num_textures;
     uint32_t num_images;
     uint32_t num_sph, num_tri, num_quad;
+    uint32_t num_xprim, num_xf, num_rect;
     DevCamera cam;
     DevBackground bg;
 };

@@ -267,9 +267,21 @@ struct Dielectric { const char* name; float refraction; };
 struct DirLight { V3 position, u, v; float intensity; Col rgb; bool invisible; };
 struct OmniLight { V3 position; float radius, intensity; Col rgb; bool invisible; };
 struct SpotLight { V3 position, direction; float cutoff, falloff, intensity, radius; Col rgb; bool invisible; };
-struct SpherePrim { const char* materialName; V3 position; float radius; };
-struct QuadPrim { const char* materialName; V3 position, u, v; };
-struct ObjMesh { const char* filepath; const char* materialName; V3 position; bool use_mtl, use_smoothing; };
+// rt::transform (misc/transform.cuh): the parts a `transform` group sets
+struct Xf {
+    bool t = false, r = false, s = false;
+    V3 tv, rv, sv;
+    bool hasTranslate() const { return t; }
+    bool hasRotate() const { return r; }
+    bool hasScale() const { return s; }
+    V3 getTranslate() const { return tv; }
+    V3 getRotate() const { return rv; }
+    V3 getScale() const { return sv; }
+};
+struct SpherePrim { const char* materialName; V3 position; float radius; Xf transform; };
+struct QuadPrim { const char* materialName; V3 position, u, v; Xf transform; };
+struct BoxPrim { const char* materialName; V3 position, size; Xf transform; };
+struct ObjMesh { const char* filepath; const char* materialName; V3 position; bool use_mtl, use_smoothing; Xf transform; };
 
 struct Config {
     struct { std::vector<SolidTex> s; std::vector<ImageTex> im; std::vector<CheckerTex> ch;
@@ -284,11 +296,12 @@ struct Config {
              int dirLightCount = 0, omniLightCount = 0, spotLightCount = 0;
              const DirLight* dirLights = nullptr; const OmniLight* omniLights = nullptr;
              const SpotLight* spotLights = nullptr; } lightsCfg;
-    struct { std::vector<SpherePrim> s; std::vector<QuadPrim> q;
+    struct { std::vector<SpherePrim> s; std::vector<QuadPrim> q; std::vector<BoxPrim> b;
              int spherePrimitiveCount = 0, quadPrimitiveCount = 0, planePrimitiveCount = 0, boxPrimitiveCount = 0,
                  conePrimitiveCount = 0, cylinderPrimitiveCount = 0, diskPrimitiveCount = 0, torusPrimitiveCount = 0,
                  volumePrimitiveCount = 0;
-             const SpherePrim* spherePrimitives = nullptr; const QuadPrim* quadPrimitives = nullptr; } primitivesCfg;
+             const SpherePrim* spherePrimitives = nullptr; const QuadPrim* quadPrimitives = nullptr;
+             const BoxPrim* boxPrimitives = nullptr; } primitivesCfg;
     struct { std::vector<ObjMesh> o; int objMeshCount = 0; const ObjMesh* objMeshes = nullptr; } meshesCfg;
     struct { V3 lookFrom{0, 0, 10}, lookAt, upAxis{0, 1, 0}; float fov = 70, aspectRatio = 16.0f / 9.0f, aperture = 0,
              focus = 100; } cameraCfg;   // scene_builder's defaults (scene_builder.cpp:49)
@@ -311,6 +324,7 @@ struct Config {
         auto& P = primitivesCfg;
         P.spherePrimitives = P.s.data(); P.spherePrimitiveCount = (int)P.s.size();
         P.quadPrimitives = P.q.data(); P.quadPrimitiveCount = (int)P.q.size();
+        P.boxPrimitives = P.b.data(); P.boxPrimitiveCount = (int)P.b.size();
         meshesCfg.objMeshes = meshesCfg.o.data();
         meshesCfg.objMeshCount = (int)meshesCfg.o.size();
     }
@@ -394,6 +408,17 @@ V3 point(const Node* n) {
         if (look(n, k[i], w)) *a[i] = (float)w;
     }
     return v;
+}
+// scene_loader::getTransform (scene_loader.cpp:1692-1704): translate, rotate and scale read as vectors
+// (so `scale = 4.0;`, not a group, sets a zero scale, as in the reference)
+Xf transform_of(const Node& n) {
+    Xf x;
+    const Node* g = n.get("transform");
+    if (!g) return x;
+    if (g->get("translate")) { x.t = true; x.tv = point(g->get("translate")); }
+    if (g->get("rotate")) { x.r = true; x.rv = point(g->get("rotate")); }
+    if (g->get("scale")) { x.s = true; x.sv = point(g->get("scale")); }
+    return x;
 }
 // scene_loader::getColor (scene_loader.cpp:1622-1656): three non-negative integers are 0-255 values;
 // otherwise the float components (an integer component reads as 0)
@@ -631,9 +656,10 @@ rtc_status read_file(rtc_scene_file& F, const char* path, uint32_t flags, rtc_im
         for (const char* k : {"isotropic", "anisotropic", "orennayar", "phong"})
             if (count(M, k)) skip(std::string(k) + " materials");
     }
-    // primitives (scene_loader.cpp:122-174, 1138-1266): spheres and quads; one without a material throws
+    // primitives (scene_loader.cpp:122-174, 1138-1308): spheres, quads and boxes with their transforms;
+    // one without a material throws
     if (const Node* P2 = root.get("primitives")) {
-        bool transformed = false;
+        bool grouped = false, mapped = false;
         auto common = [&](const Node& n, std::string& mat) {
             look(&n, "material", mat);
             if (mat.empty()) throw SceneError{"line " + std::to_string(n.line) + ": Material name is empty"};
@@ -641,34 +667,45 @@ rtc_status read_file(rtc_scene_file& F, const char* path, uint32_t flags, rtc_im
             look(&n, "active", active);
             std::string group;
             look(&n, "group", group);
-            if (active && (n.get("transform") || !group.empty())) transformed = true;
+            if (active && !group.empty()) grouped = true;
+            if (active && n.get("uvmapping")) mapped = true;
             return active;
         };
-        const size_t cs = cap(P2, "spheres"), cq = cap(P2, "quads");
+        const size_t cs = cap(P2, "spheres"), cq = cap(P2, "quads"), cb = cap(P2, "boxes");
         each(P2, "spheres", [&](const Node& n) {
-            SpherePrim sp{nullptr, point(n.get("position")), 0.0f};
+            SpherePrim sp{nullptr, point(n.get("position")), 0.0f, {}};
             look(&n, "radius", sp.radius);
             std::string mat;
             if (!common(n, mat) || full(C.primitivesCfg.s.size(), cs, "sphere")) return;
             sp.materialName = C.keep(mat);
+            sp.transform = transform_of(n);
             C.primitivesCfg.s.push_back(sp);
         });
         each(P2, "quads", [&](const Node& n) {
-            QuadPrim q{nullptr, point(n.get("position")), point(n.get("u")), point(n.get("v"))};
+            QuadPrim q{nullptr, point(n.get("position")), point(n.get("u")), point(n.get("v")), {}};
             std::string mat;
             if (!common(n, mat) || full(C.primitivesCfg.q.size(), cq, "quad")) return;
             q.materialName = C.keep(mat);
+            q.transform = transform_of(n);
             C.primitivesCfg.q.push_back(q);
+        });
+        each(P2, "boxes", [&](const Node& n) {
+            BoxPrim b{nullptr, point(n.get("position")), point(n.get("size")), {}};
+            std::string mat;
+            if (!common(n, mat) || full(C.primitivesCfg.b.size(), cb, "box")) return;
+            b.materialName = C.keep(mat);
+            b.transform = transform_of(n);
+            C.primitivesCfg.b.push_back(b);
         });
         auto& PC = C.primitivesCfg;
         PC.planePrimitiveCount = (int)count(P2, "planes");
-        PC.boxPrimitiveCount = (int)count(P2, "boxes");
         PC.conePrimitiveCount = (int)count(P2, "cones");
         PC.cylinderPrimitiveCount = (int)count(P2, "cylinders");
         PC.diskPrimitiveCount = (int)count(P2, "disks");
         PC.torusPrimitiveCount = (int)count(P2, "toruses");
         PC.volumePrimitiveCount = (int)count(P2, "volumes");
-        if (transformed) skip("transforms and groups of primitives (placed untransformed)");
+        if (grouped) skip("groups of primitives (the reference's loadGroups reads none)");
+        if (mapped) skip("uv mappings of primitives (the render path uses the default mapping)");
     }
     // meshes (scene_loader.cpp:369-435): the first missing OBJ file ends the meshes
     if (const Node* MS = root.get("meshes")) {
@@ -690,8 +727,8 @@ rtc_status read_file(rtc_scene_file& F, const char* path, uint32_t flags, rtc_im
                 return;
             }
             if (!active || full(C.meshesCfg.o.size(), cm, "OBJ mesh")) return;
-            if (n.get("transform")) skip("transforms of OBJ meshes (placed at `position` only)");
-            C.meshesCfg.o.push_back(ObjMesh{C.keep(fp), C.keep(mat), point(n.get("position")), use_mtl, smooth});
+            C.meshesCfg.o.push_back(ObjMesh{C.keep(fp), C.keep(mat), point(n.get("position")), use_mtl, smooth,
+                                            transform_of(n)});
         });
     }
     if (root.get("groups")) skip("groups");

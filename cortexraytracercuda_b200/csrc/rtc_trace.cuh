@@ -222,7 +222,122 @@ __device__ __forceinline__ bool slab2(const float4 n0, const float4 n1, const fl
     return lin <= lout;
 }
 
+// ------------------------------------------------------------------------------------------------
+// transformed primitives and box faces
+// ------------------------------------------------------------------------------------------------
+// glm mat4 * vec4 (glm/detail/type_mat4x4.inl:560-571) for a rotation matrix, whose fourth column is
+// (0, 0, 0, 1): component i = (m0_i x + m1_i y) + (m2_i z + m3_i w), and m3_i w is +0 for i < 3.
+__device__ __forceinline__ V3 rot_apply(float4 m0, float4 m1, float4 m2, V3 v) {
+    return v3((m0.x * v.x + m1.x * v.y) + (m2.x * v.z + 0.0f), (m0.y * v.x + m1.y * v.y) + (m2.y * v.z + 0.0f),
+              (m0.z * v.x + m1.z * v.y) + (m2.z * v.z + 0.0f));
+}
+
+// World ray -> object space through scale, rotate, translate (scale.cuh, rotate.cuh, translate.cuh hit()).
+__device__ __forceinline__ void xf_to_object(const DevScene& S, int32_t xi, V3& o, V3& d) {
+    const float4* x = S.xf + 8 * (size_t)xi;
+    const float4 h0 = __ldg(x);
+    const uint32_t fl = __float_as_uint(h0.w);
+    if (fl & 4u) {
+        const float4 sc = __ldg(x + 1);
+        o = v3(o.x / sc.x, o.y / sc.y, o.z / sc.z);
+        d = v3(d.x / sc.x, d.y / sc.y, d.z / sc.z);
+    }
+    if (fl & 2u) {
+        const float4 m0 = __ldg(x + 2), m1 = __ldg(x + 3), m2 = __ldg(x + 4);
+        o = rot_apply(m0, m1, m2, o);
+        d = rot_apply(m0, m1, m2, d);
+    }
+    if (fl & 1u) o = v3(o.x - h0.x, o.y - h0.y, o.z - h0.z);
+}
+
+// Hit point and normal back to world space: translate (+t), rotate (forward matrix), scale (p * s,
+// normal unit_vector(n / s)).
+__device__ __forceinline__ void xf_to_world(const DevScene& S, int32_t xi, V3& p, V3& n) {
+    const float4* x = S.xf + 8 * (size_t)xi;
+    const float4 h0 = __ldg(x);
+    const uint32_t fl = __float_as_uint(h0.w);
+    if (fl & 1u) p = v3(p.x + h0.x, p.y + h0.y, p.z + h0.z);
+    if (fl & 2u) {
+        const float4 m0 = __ldg(x + 5), m1 = __ldg(x + 6), m2 = __ldg(x + 7);
+        p = rot_apply(m0, m1, m2, p);
+        n = rot_apply(m0, m1, m2, n);
+    }
+    if (fl & 4u) {
+        const float4 sc = __ldg(x + 1);
+        p = v3(p.x * sc.x, p.y * sc.y, p.z * sc.z);
+        n = unit(v3(n.x / sc.x, n.y / sc.y, n.z / sc.z));
+    }
+}
+
+// xy_rect / xz_rect / yz_rect::hit (aarect.cuh): t = (k - o_a) / d_a in [tmin, tmax] inclusive, then the
+// two in-plane coordinates inside the rectangle, bounds inclusive.
+__device__ __forceinline__ bool rect_t(float4 r0, float4 r1, V3 o, V3 d, float tmin, float tmax, float& t, float& a,
+                                       float& b) {
+    const int axis = __float_as_int(r1.y);
+    const float oa = axis == 0 ? o.z : axis == 1 ? o.y : o.x;
+    const float da = axis == 0 ? d.z : axis == 1 ? d.y : d.x;
+    t = (r1.x - oa) / da;
+    if (t < tmin || t > tmax) return false;
+    const float o0 = axis == 2 ? o.y : o.x, d0 = axis == 2 ? d.y : d.x;
+    const float o1 = axis == 0 ? o.y : o.z, d1 = axis == 0 ? d.y : d.z;
+    a = o0 + t * d0;
+    b = o1 + t * d1;
+    return !(a < r0.x || a > r0.y || b < r0.z || b > r0.w);
+}
+
 // Tests every item of one leaf against [tmin, best_t].  EXACT: clean mode's double-precision sphere test.
+// Transformed primitives and box faces (xprims) of a leaf, tested after its other items on the
+// object-space ray.  Kept out of test_leaf's main loop so that scenes without them keep that loop's
+// registers.
+template <bool EXACT>
+__device__ __forceinline__ void test_leaf_xprims(const DevScene& S, uint32_t first, uint32_t cnt, V3 o, V3 d,
+                                                 float tmin, float& best_t, uint32_t& best_item, uint32_t& status) {
+    for (uint32_t k = 0; k < cnt; ++k) {
+        const uint32_t it = ld_scene(S.items + first + k);
+        const uint32_t idx = it & ITEM_INDEX_MASK;
+        if ((it >> ITEM_KIND_SHIFT) != ITEM_XPRIM) continue;
+        if (idx >= S.num_xprim) { status |= STATUS_BAD_ITEM; continue; }
+        const int4 x = __ldg(S.xprim + idx);
+        V3 ro = o, rd = d;
+        if (x.x >= 0) {
+            if ((uint32_t)x.x >= S.num_xf) { status |= STATUS_BAD_ITEM; continue; }
+            xf_to_object(S, x.x, ro, rd);
+        }
+        const uint32_t in = (uint32_t)x.z;
+        float t;
+        bool h = false;
+        switch (x.y) {
+        case ITEM_SPHERE: {
+            if (in >= S.num_sph) { status |= STATUS_BAD_ITEM; break; }
+            const float4 sp = ld_scene(S.sph + in);
+            h = EXACT ? sphere_t_exact(sp, ro, rd, tmin, best_t, t) : sphere_t(sp, ro, rd, tmin, best_t, t);
+        } break;
+        case ITEM_QUAD: {
+            if (in >= S.num_quad) { status |= STATUS_BAD_ITEM; break; }
+            const float4* q = S.quad + 5 * (size_t)in;
+            float a, b;
+            h = planar_t(__ldg(q), __ldg(q + 1), __ldg(q + 2), __ldg(q + 3), __ldg(q + 4), ro, rd, tmin, best_t, false, t, a, b);
+        } break;
+        case ITEM_TRI: {
+            if (in >= S.num_tri) { status |= STATUS_BAD_ITEM; break; }
+            const float4* p = S.tri + 3 * (size_t)in;
+            float bu, bv;
+            h = tri_t(ld_scene(p), ld_scene(p + 1), ld_scene(p + 2), ro, rd, tmin, best_t, t, bu, bv);
+        } break;
+        case XPRIM_RECT: {
+            if (in >= S.num_rect) { status |= STATUS_BAD_ITEM; break; }
+            float a, b;
+            h = rect_t(__ldg(S.rect + 2 * (size_t)in), __ldg(S.rect + 2 * (size_t)in + 1), ro, rd, tmin, best_t, t, a, b);
+        } break;
+        default: status |= STATUS_BAD_ITEM; break;
+        }
+        if (h) {
+            best_t = t;
+            best_item = it;
+        }
+    }
+}
+
 template <bool EXACT>
 __device__ __forceinline__ void test_leaf(const DevScene& S, int32_t child, V3 o, V3 d, float tmin, float& best_t,
                                           uint32_t& best_item, bool hide_invisible, TraceStats& st,
@@ -230,9 +345,10 @@ __device__ __forceinline__ void test_leaf(const DevScene& S, int32_t child, V3 o
     uint32_t enc = (uint32_t)(~child);
     uint32_t first = enc >> LEAF_COUNT_BITS, cnt = enc & MAX_LEAF;
     if (first + cnt > S.num_items) { status |= STATUS_BAD_ITEM; return; }
+    bool xprims = false;
     for (uint32_t k = 0; k < cnt; ++k) {
         uint32_t it = ld_scene(S.items + first + k);
-        uint32_t kind = it >> 30, idx = it & 0x3fffffffu;
+        uint32_t kind = it >> ITEM_KIND_SHIFT, idx = it & ITEM_INDEX_MASK;
         float t;
         st.prims++;
         switch (kind) {
@@ -276,8 +392,11 @@ __device__ __forceinline__ void test_leaf(const DevScene& S, int32_t child, V3 o
             // (directional_light.cuh:106, omni_light.cuh:76-80)
             if (hitl && !(q3.w != 0.0f && hide_invisible)) { best_t = t; best_item = it; }
         } break;
+        case ITEM_XPRIM: xprims = true; break;
+        default: status |= STATUS_BAD_ITEM; break;
         }
     }
+    if (xprims) test_leaf_xprims<EXACT>(S, first, cnt, o, d, tmin, best_t, best_item, status);
 }
 
 // Direction component for the slab tests' reciprocal.  The slab distance is fma(lo, 1/d, -o/d); with a
@@ -457,10 +576,8 @@ __device__ __forceinline__ bool closest_hit(const DevScene& S, V3 o, V3 d, float
 // interval test (sphere.cuh:137-165, quad.cuh:122-132, directional_light.cuh:113-120,
 // triangle.cuh:160-184).
 template <bool FLOAT_TRIG>
-__device__ __forceinline__ void finalize_hit(const DevScene& S, uint32_t it, float t, V3 o, V3 d, Hit& h) {
-    uint32_t kind = it >> 30, idx = it & 0x3fffffffu;
-    h.t = t;
-    h.item = it;
+__device__ __forceinline__ void finalize_prim(const DevScene& S, uint32_t kind, uint32_t idx, float t, V3 o, V3 d,
+                                              Hit& h) {
     switch (kind) {
     case ITEM_SPHERE: {
         float4 s = __ldg(S.sph + idx);
@@ -541,6 +658,45 @@ __device__ __forceinline__ void finalize_hit(const DevScene& S, uint32_t it, flo
         h.v = 0.0f;
     } break;
     }
+}
+
+// A box face (aarect.cuh hit()): hit point r.at(t), the axis normal (negated by rt::flip_normals for the
+// low faces), front_face left at hit_record's default true, uv by get_xy/xz/yz_rect_uv with the default
+// mapping.
+__device__ __forceinline__ void finalize_rect(const DevScene& S, uint32_t idx, float t, V3 o, V3 d, Hit& h) {
+    const float4 r0 = __ldg(S.rect + 2 * (size_t)idx), r1 = __ldg(S.rect + 2 * (size_t)idx + 1);
+    const int axis = __float_as_int(r1.y);
+    const float o0 = axis == 2 ? o.y : o.x, d0 = axis == 2 ? d.y : d.x;
+    const float o1 = axis == 0 ? o.y : o.z, d1 = axis == 0 ? d.y : d.z;
+    const float a = o0 + t * d0, b = o1 + t * d1;
+    float su = (a - r0.x) / (r0.y - r0.x);
+    float sv = (b - r0.z) / (r0.w - r0.z);
+    su = fmodf(su * 1.0f, 1.0f);
+    sv = fmodf(sv * 1.0f, 1.0f);
+    h.u = 1.0f * su + 0.0f;
+    h.v = 1.0f * sv + 0.0f;
+    h.p = at(o, d, t);
+    const float sgn = r1.z != 0.0f ? -1.0f : 1.0f;
+    h.n = axis == 0 ? v3(0.0f, 0.0f, sgn) : axis == 1 ? v3(0.0f, sgn, 0.0f) : v3(sgn, 0.0f, 0.0f);
+    h.front = true;
+    h.mat = __float_as_int(r1.w);
+}
+
+template <bool FLOAT_TRIG>
+__device__ __forceinline__ void finalize_hit(const DevScene& S, uint32_t it, float t, V3 o, V3 d, Hit& h) {
+    const uint32_t kind = it >> ITEM_KIND_SHIFT, idx = it & ITEM_INDEX_MASK;
+    h.t = t;
+    h.item = it;
+    if (kind != ITEM_XPRIM) {
+        finalize_prim<FLOAT_TRIG>(S, kind, idx, t, o, d, h);
+        return;
+    }
+    // a transformed primitive or a box face: the inner hit in object space, then back to world space
+    const int4 x = __ldg(S.xprim + idx);
+    if (x.x >= 0) xf_to_object(S, x.x, o, d);
+    if (x.y == XPRIM_RECT) finalize_rect(S, (uint32_t)x.z, t, o, d, h);
+    else finalize_prim<FLOAT_TRIG>(S, (uint32_t)x.y, (uint32_t)x.z, t, o, d, h);
+    if (x.x >= 0) xf_to_world(S, x.x, h.p, h.n);
 }
 
 // ------------------------------------------------------------------------------------------------

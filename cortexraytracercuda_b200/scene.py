@@ -87,6 +87,17 @@ class rtc_background(C.Structure):
                 ("env_width", C.c_int32), ("env_height", C.c_int32)]
 
 
+XF_TRANSLATE, XF_ROTATE, XF_SCALE = 1, 2, 4
+
+
+class rtc_transform(C.Structure):
+    _fields_ = [("translate", F3), ("rotate", F3), ("scale", F3), ("flags", C.c_uint32)]
+
+
+class rtc_box(C.Structure):
+    _fields_ = [("center", F3), ("size", F3), ("material", C.c_int32), ("transform", C.c_uint32)]
+
+
 class rtc_scene_desc(C.Structure):
     _fields_ = [("textures", C.POINTER(rtc_texture)), ("num_textures", C.c_uint32),
                 ("images", C.POINTER(rtc_image)), ("num_images", C.c_uint32),
@@ -97,7 +108,11 @@ class rtc_scene_desc(C.Structure):
                 ("meshes", C.POINTER(rtc_mesh)), ("num_meshes", C.c_uint32),
                 ("camera", rtc_camera), ("background", rtc_background),
                 ("omni_lights", C.POINTER(rtc_omni_light)), ("num_omni_lights", C.c_uint32),
-                ("spot_lights", C.POINTER(rtc_spot_light)), ("num_spot_lights", C.c_uint32)]
+                ("spot_lights", C.POINTER(rtc_spot_light)), ("num_spot_lights", C.c_uint32),
+                ("transforms", C.POINTER(rtc_transform)), ("num_transforms", C.c_uint32),
+                ("sphere_transforms", C.POINTER(C.c_uint32)), ("quad_transforms", C.POINTER(C.c_uint32)),
+                ("mesh_transforms", C.POINTER(C.c_uint32)),
+                ("boxes", C.POINTER(rtc_box)), ("num_boxes", C.c_uint32)]
 
 
 class rtc_render_params(C.Structure):
@@ -231,6 +246,10 @@ class Scene:
     spheres: list = field(default_factory=list)
     quads: list = field(default_factory=list)
     meshes: list = field(default_factory=list)        # dicts with numpy arrays
+    boxes: list = field(default_factory=list)         # (center, size, material, transform ref)
+    transforms: list = field(default_factory=list)    # (translate, rotate, scale, flags)
+    sphere_transforms: dict = field(default_factory=dict)   # sphere index -> 1-based transform ref
+    quad_transforms: dict = field(default_factory=dict)
     camera: Camera = field(default_factory=Camera)
     background: dict = field(default_factory=lambda: {"kind": BG_CONSTANT, "color": (0.0, 0.0, 0.0)})
     name: str = "scene"
@@ -298,20 +317,37 @@ class Scene:
                                  float(radius), tuple(rgb), int(bool(invisible))))
         return len(self.spot_lights) - 1
 
-    def sphere(self, center, radius, mat) -> int:
+    def transform(self, translate=None, rotate=None, scale=None) -> int:
+        """An rt::translate / rotate / scale chain (rotate in degrees about x, y, z); returns the 1-based
+        reference that sphere(), quad(), box() and mesh() take as `transform` (0 = none)."""
+        flags = (XF_TRANSLATE if translate is not None else 0) | (XF_ROTATE if rotate is not None else 0) | \
+            (XF_SCALE if scale is not None else 0)
+        self.transforms.append((tuple(translate or (0, 0, 0)), tuple(rotate or (0, 0, 0)), tuple(scale or (1, 1, 1)), flags))
+        return len(self.transforms)
+
+    def sphere(self, center, radius, mat, transform=0) -> int:
         self.spheres.append((tuple(center), float(radius), int(mat)))
+        if transform:
+            self.sphere_transforms[len(self.spheres) - 1] = int(transform)
         return len(self.spheres) - 1
 
-    def quad(self, q, u, v, mat) -> int:
+    def quad(self, q, u, v, mat, transform=0) -> int:
         self.quads.append((tuple(q), tuple(u), tuple(v), int(mat)))
+        if transform:
+            self.quad_transforms[len(self.quads) - 1] = int(transform)
         return len(self.quads) - 1
 
-    def mesh(self, vertices, indices, mat, normals=None, uvs=None, smooth=False) -> int:
+    def box(self, center, size, mat, transform=0) -> int:
+        """An axis-aligned box of six rectangles (box.cuh), after the quads in the object order."""
+        self.boxes.append((tuple(center), tuple(size), int(mat), int(transform)))
+        return len(self.boxes) - 1
+
+    def mesh(self, vertices, indices, mat, normals=None, uvs=None, smooth=False, transform=0) -> int:
         m = {"vertices": np.ascontiguousarray(vertices, dtype=np.float32).reshape(-1, 3),
              "indices": np.ascontiguousarray(indices, dtype=np.uint32).reshape(-1, 3),
              "normals": None if normals is None else np.ascontiguousarray(normals, dtype=np.float32).reshape(-1, 3),
              "uvs": None if uvs is None else np.ascontiguousarray(uvs, dtype=np.float32).reshape(-1, 2),
-             "material": int(mat), "smooth": int(bool(smooth))}
+             "material": int(mat), "smooth": int(bool(smooth)), "transform": int(transform)}
         self.meshes.append(m)
         return len(self.meshes) - 1
 
@@ -335,7 +371,7 @@ class Scene:
 
     @property
     def num_primitives(self) -> int:
-        return len(self.dir_lights) + len(self.spheres) + len(self.quads) + self.num_triangles
+        return len(self.dir_lights) + len(self.spheres) + len(self.quads) + 6 * len(self.boxes) + self.num_triangles
 
     # C description --------------------------------------------------------------------------------
     def to_desc(self) -> "SceneDesc":
@@ -397,6 +433,21 @@ class SceneDesc:
                                    a[4], len(spheres), a[5], len(quads), a[6], len(meshes),
                                    rtc_camera(_f3(cam.look_from), _f3(cam.look_at), _f3(cam.up), cam.vfov, cam.aspect,
                                               cam.aperture, cam.focus), cbg, a[7], len(omnis), a[8], len(spots))
+        xfs = [rtc_transform(_f3(t), _f3(r), _f3(sc), fl) for (t, r, sc, fl) in s.transforms]
+        boxes = [rtc_box(_f3(c), _f3(sz), m, x) for (c, sz, m, x) in s.boxes]
+        refs = {}
+        for name, n, get in (("sphere", len(s.spheres), s.sphere_transforms.get),
+                             ("quad", len(s.quads), s.quad_transforms.get),
+                             ("mesh", len(s.meshes), lambda i: s.meshes[i].get("transform", 0))):
+            r = [int(get(i) or 0) for i in range(n)]
+            refs[name] = _carray(C.c_uint32, r) if any(r) else None
+        self.arrays += [_carray(rtc_transform, xfs), _carray(rtc_box, boxes)]
+        self.arrays += [r for r in refs.values() if r is not None]
+        self.desc.transforms, self.desc.num_transforms = self.arrays[9], len(xfs)
+        self.desc.boxes, self.desc.num_boxes = self.arrays[10], len(boxes)
+        for name, r in refs.items():
+            if r is not None:
+                setattr(self.desc, name + "_transforms", C.cast(r, C.POINTER(C.c_uint32)))
         self._keep = keep
         self.scene = s
 

@@ -165,6 +165,33 @@ typedef struct rtc_mesh {
     int32_t smooth;             /* barycentric normal interpolation (triangle.cuh:171-175)         */
 } rtc_mesh;
 
+/* Object transform, as scene_factory::applyTransform wraps a primitive (core/src/scene_factory.cuh:
+ * 710-725): rt::translate inside, then rt::rotate, then rt::scale outside (primitives/translate.cuh,
+ * rotate.cuh, scale.cuh).  A ray reaches the object through scale (o / s, d / s), rotate (the glm
+ * matrix of -x, -y, -z degrees about x, then y, then z) and translate (o - t); the hit point returns
+ * through translate (+ t), rotate (the matrix of +x, +y, +z degrees, which is not the inverse of the
+ * first when two axes turn, as in the reference) and scale (p * s, normal unit(n / s)).  Only the parts
+ * whose flag is set apply. */
+#define RTC_XF_TRANSLATE 1u
+#define RTC_XF_ROTATE 2u
+#define RTC_XF_SCALE 4u
+typedef struct rtc_transform {
+    float translate[3];
+    float rotate[3];            /* degrees about x, y, z                                           */
+    float scale[3];
+    uint32_t flags;             /* RTC_XF_* bits                                                   */
+} rtc_transform;
+
+/* Axis-aligned box of six rectangles, centre and size (core/src/primitives/box.cuh, aarect.cuh).  Its
+ * faces report the outward normal and front_face = true whatever side the ray comes from, as the
+ * reference's xy/xz/yz_rect do; the faces at the low coordinate go through rt::flip_normals. */
+typedef struct rtc_box {
+    float center[3];
+    float size[3];
+    int32_t material;
+    uint32_t transform;         /* 1-based index into rtc_scene_desc.transforms; 0 = none          */
+} rtc_box;
+
 /* Perspective camera (core/src/cameras/perspective_camera.cuh:41-117). */
 typedef struct rtc_camera {
     float look_from[3];
@@ -206,6 +233,14 @@ typedef struct rtc_scene_desc {
      * load_scene adds them (gpu.cu:504-523); that order also numbers them before the spheres. */
     const rtc_omni_light* omni_lights;  uint32_t num_omni_lights;
     const rtc_spot_light* spot_lights;  uint32_t num_spot_lights;
+    /* Transforms and boxes.  *_transforms give, per sphere / quad / mesh, a 1-based index into
+     * `transforms` (0 = none); each may be NULL when no object of that kind is transformed.  Boxes follow
+     * the quads in the object order, as load_scene adds them (gpu.cu:527-565). */
+    const rtc_transform* transforms;    uint32_t num_transforms;
+    const uint32_t* sphere_transforms;
+    const uint32_t* quad_transforms;
+    const uint32_t* mesh_transforms;
+    const rtc_box* boxes;               uint32_t num_boxes;
 } rtc_scene_desc;
 
 /* Triangle geometry read from a Wavefront OBJ file, laid out for rtc_mesh: per-vertex positions (and

@@ -11,9 +11,11 @@
 //     colours; odd lands in m_even as scene_factory does, scene_factory.cuh:619-629), image;
 //   * an object whose material does not resolve is skipped, as `if (mat)` skips it (gpu.cu:531).
 // OBJ meshes are read through an optional loader callback (with this library: rtc_load_obj).
-// Lights map to omni, directional and spot lights in the light list's order.  Primitives the B200 path
-// does not cover (planes, boxes, cones, cylinders, disks, tori, volumes) and transforms are reported in
-// `skipped`.
+// Lights map to omni, directional and spot lights in the light list's order.  Spheres, quads and boxes
+// keep their rt::transform as scene_factory::applyTransform applies it; OBJ meshes take their
+// `position` as a vertex offset and their transform too, where the reference's createObjMesh drops both
+// (scene_factory.cuh createObjMesh) and renders meshes[0] for every entry (gpu.cu:628).  Primitives the
+// B200 path does not cover (planes, cones, cylinders, disks, tori, volumes) are reported in `skipped`.
 // Image textures need decoded RGB8 pixels: pass `load_image(filepath, &w, &h)` returning a pointer
 // that stays valid while the description is used (the reference decodes with stbi_load, gpu.cu:1743).
 #pragma once
@@ -37,6 +39,9 @@ struct SceneHolder {
     std::vector<rtc_sphere> spheres;
     std::vector<rtc_quad> quads;
     std::vector<rtc_mesh> meshes;
+    std::vector<rtc_box> boxes;
+    std::vector<rtc_transform> transforms;
+    std::vector<uint32_t> sphere_transforms, quad_transforms, mesh_transforms;   // 1-based, 0 = none
     // geometry of the OBJ meshes (owned here; rtc_mesh points into it)
     std::vector<std::vector<float>> mesh_vertices, mesh_normals;
     std::vector<std::vector<uint32_t>> mesh_indices;
@@ -67,6 +72,13 @@ struct SceneHolder {
         }
         desc.meshes = meshes.data();
         desc.num_meshes = (uint32_t)meshes.size();
+        desc.boxes = boxes.data();
+        desc.num_boxes = (uint32_t)boxes.size();
+        desc.transforms = transforms.data();
+        desc.num_transforms = (uint32_t)transforms.size();
+        desc.sphere_transforms = transforms.empty() ? nullptr : sphere_transforms.data();
+        desc.quad_transforms = transforms.empty() ? nullptr : quad_transforms.data();
+        desc.mesh_transforms = transforms.empty() ? nullptr : mesh_transforms.data();
         return &desc;
     }
 };
@@ -83,6 +95,18 @@ inline bool same(const char* a, const char* b) { return a && b && std::strcmp(a,
 inline bool named(const char* a) { return a && a[0] != '\0'; }
 template <class V> void put3(float* dst, const V& v) { dst[0] = v.x; dst[1] = v.y; dst[2] = v.z; }
 template <class C> void putc3(float* dst, const C& c) { dst[0] = c.r(); dst[1] = c.g(); dst[2] = c.b(); }
+// An rt::transform (misc/transform.cuh) as a 1-based reference into out.transforms; 0 when it has no part.
+template <class T> uint32_t add_transform(const T& trs, SceneHolder& out) {
+    rtc_transform x{};
+    x.flags = (trs.hasTranslate() ? RTC_XF_TRANSLATE : 0u) | (trs.hasRotate() ? RTC_XF_ROTATE : 0u) |
+              (trs.hasScale() ? RTC_XF_SCALE : 0u);
+    if (!x.flags) return 0;
+    put3(x.translate, trs.getTranslate());
+    put3(x.rotate, trs.getRotate());
+    put3(x.scale, trs.getScale());
+    out.transforms.push_back(x);
+    return (uint32_t)out.transforms.size();
+}
 }  // namespace detail
 
 // Converts `cfg` (a reference sceneConfig) into `out`; returns out.finish().
@@ -212,6 +236,7 @@ const rtc_scene_desc* from_sceneconfig(const SceneConfig& cfg, SceneHolder& out,
         o.radius = s.radius;
         o.material = m;
         out.spheres.push_back(o);
+        out.sphere_transforms.push_back(add_transform(s.transform, out));   // scene_factory::createSphere
     }
     if (P.planePrimitiveCount) out.skipped.push_back("planes");
     for (int i = 0; i < P.quadPrimitiveCount; ++i) {
@@ -224,13 +249,25 @@ const rtc_scene_desc* from_sceneconfig(const SceneConfig& cfg, SceneHolder& out,
         put3(o.v, q.v);
         o.material = m;
         out.quads.push_back(o);
+        out.quad_transforms.push_back(add_transform(q.transform, out));
     }
-    if (P.boxPrimitiveCount) out.skipped.push_back("boxes");
+    // boxes after the quads (gpu.cu:556-565; scene_factory::createBox, box.cuh)
+    for (int i = 0; i < P.boxPrimitiveCount; ++i) {
+        const auto& b = P.boxPrimitives[i];
+        int m = fetch_material(b.materialName);
+        if (m < 0) continue;
+        rtc_box o{};
+        put3(o.center, b.position);
+        put3(o.size, b.size);
+        o.material = m;
+        o.transform = add_transform(b.transform, out);
+        out.boxes.push_back(o);
+    }
     if (P.conePrimitiveCount || P.cylinderPrimitiveCount || P.diskPrimitiveCount || P.torusPrimitiveCount ||
         P.volumePrimitiveCount)
         out.skipped.push_back("cones/cylinders/disks/tori/volumes");
-    // OBJ meshes (load_scene adds them after the quads, gpu.cu:612-635): geometry offset by `position`,
-    // one material for the whole mesh (use_mtl materials and transforms beyond the offset are reported)
+    // OBJ meshes (load_scene adds them after the boxes, gpu.cu:612-635): geometry offset by `position`,
+    // then the mesh's transform; one material for the whole mesh (use_mtl materials are reported)
     const auto& MS = cfg.meshesCfg;
     for (int i = 0; i < MS.objMeshCount; ++i) {
         const auto& m = MS.objMeshes[i];
@@ -260,6 +297,7 @@ const rtc_scene_desc* from_sceneconfig(const SceneConfig& cfg, SceneHolder& out,
         out.mesh_indices.push_back(std::move(idx));
         out.mesh_normals.push_back(r.smooth ? std::move(n) : std::vector<float>());
         out.meshes.push_back(r);
+        out.mesh_transforms.push_back(add_transform(m.transform, out));
     }
 
     const auto& C = cfg.cameraCfg;

@@ -32,6 +32,10 @@
 #include "primitives/sphere.cuh"
 #include "primitives/quad.cuh"
 #include "primitives/triangle.cuh"
+#include "primitives/box.cuh"
+#include "primitives/translate.cuh"
+#include "primitives/rotate.cuh"
+#include "primitives/scale.cuh"
 #include "lights/light.cuh"
 #include "lights/directional_light.cuh"
 #include "lights/omni_light.cuh"
@@ -171,6 +175,16 @@ struct ref_scene {
 
 static vector3 v3(const float* p) { return vector3(p[0], p[1], p[2]); }
 
+// scene_factory::applyTransform (scene_factory.cuh:710-725): translate inside, then rotate, then scale.
+static hittable* apply_transform(hittable* h, const rtc_scene_desc* d, uint32_t ref) {
+    if (!ref || ref > d->num_transforms) return h;
+    const rtc_transform& T = d->transforms[ref - 1];
+    if (T.flags & RTC_XF_TRANSLATE) h = new rt::translate(h, v3(T.translate));
+    if (T.flags & RTC_XF_ROTATE) h = new rt::rotate(h, v3(T.rotate));
+    if (T.flags & RTC_XF_SCALE) h = new rt::scale(h, v3(T.scale));
+    return h;
+}
+
 static texture* make_texture(ref_scene& s, const rtc_scene_desc* d, int idx, int depth) {
     if (idx < 0 || (uint32_t)idx >= d->num_textures || depth > 4) return nullptr;
     const rtc_texture& t = d->textures[idx];
@@ -233,7 +247,8 @@ void* refh_scene_create(const rtc_scene_desc* d, int bvh_kind) {
     ref_scene* s = new ref_scene();
     s->cam_desc = d->camera;
     s->bg = d->background;
-    uint64_t total = (uint64_t)d->num_omni_lights + d->num_dir_lights + d->num_spot_lights + d->num_spheres + d->num_quads;
+    uint64_t total = (uint64_t)d->num_omni_lights + d->num_dir_lights + d->num_spot_lights + d->num_spheres + d->num_quads +
+                     d->num_boxes;
     for (uint32_t m = 0; m < d->num_meshes; ++m) total += d->meshes[m].num_triangles;
     s->names.assign(total + 1, 0);
     size_t k = 0;
@@ -268,13 +283,23 @@ void* refh_scene_create(const rtc_scene_desc* d, int bvh_kind) {
         const rtc_sphere& S = d->spheres[i];
         material* m = mat_of(S.material);
         if (!m) { g_err = "sphere " + std::to_string(i) + ": bad material"; delete s; return nullptr; }
-        s->objects.push_back(new sphere(v3(S.center), S.radius, m, uvmapping(), &s->names[k]));
+        s->objects.push_back(apply_transform(new sphere(v3(S.center), S.radius, m, uvmapping(), &s->names[k]), d,
+                                             d->sphere_transforms ? d->sphere_transforms[i] : 0));
     }
     for (uint32_t i = 0; i < d->num_quads; ++i, ++k) {
         const rtc_quad& Q = d->quads[i];
         material* m = mat_of(Q.material);
         if (!m) { g_err = "quad " + std::to_string(i) + ": bad material"; delete s; return nullptr; }
-        s->objects.push_back(new quad(v3(Q.q), v3(Q.u), v3(Q.v), m, uvmapping(), &s->names[k]));
+        s->objects.push_back(apply_transform(new quad(v3(Q.q), v3(Q.u), v3(Q.v), m, uvmapping(), &s->names[k]), d,
+                                             d->quad_transforms ? d->quad_transforms[i] : 0));
+    }
+    // boxes after the quads (load_scene, gpu.cu:556-565): scene_factory::createBox
+    for (uint32_t i = 0; i < d->num_boxes; ++i, ++k) {
+        const rtc_box& B = d->boxes[i];
+        material* m = mat_of(B.material);
+        if (!m) { g_err = "box " + std::to_string(i) + ": bad material"; delete s; return nullptr; }
+        s->objects.push_back(apply_transform(new box(v3(B.center), v3(B.size), m, uvmapping(), &s->names[k]), d,
+                                             B.transform));
     }
     for (uint32_t mi = 0; mi < d->num_meshes; ++mi) {
         const rtc_mesh& M = d->meshes[mi];
@@ -302,7 +327,7 @@ void* refh_scene_create(const rtc_scene_desc* d, int bvh_kind) {
                 t = new tri_named(a, b, c, m, &s->names[k]);
             }
             t->setName(&s->names[k]);
-            s->objects.push_back(t);
+            s->objects.push_back(apply_transform(t, d, d->mesh_transforms ? d->mesh_transforms[mi] : 0));
         }
     }
     if (s->objects.empty()) { g_err = "empty scene"; delete s; return nullptr; }

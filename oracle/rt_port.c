@@ -110,7 +110,7 @@ static inline void draw3(rng_t* r, int order, float* a, float* b, float* c) {
 /* ---------------------------------------------------------------------------------------------- */
 /* scene                                                                                          */
 /* ---------------------------------------------------------------------------------------------- */
-enum { K_LIGHT = 0, K_SPHERE = 1, K_QUAD = 2, K_TRI = 3 };
+enum { K_LIGHT = 0, K_SPHERE = 1, K_QUAD = 2, K_TRI = 3, K_RECT = 4 };
 
 typedef struct {
     int kind;
@@ -125,7 +125,14 @@ typedef struct {
     v3 mid;           /* triangle middle_normal */
     int smooth; v3 vn[3];
     float lo[3], hi[3];
+    int xf;           /* transform index or -1 (rt::translate / rotate / scale around the primitive) */
+    int gid;          /* global object id (one per box) */
+    int axis, flip;   /* box face: 0 xy_rect, 1 xz_rect, 2 yz_rect; flip_normals on the low faces */
+    float r0, r1, s0, s1, k;   /* box face bounds in its two in-plane axes and its plane */
 } prim_t;
+
+/* rt::translate / rt::rotate / rt::scale (primitives/translate.cuh, rotate.cuh, scale.cuh) */
+typedef struct { v3 t, s; float inv[3][3], fwd[3][3]; unsigned flags; } xf_t;
 
 typedef struct { int kind; float col[3]; float inv_scale; int even, odd, image; } tex_t;
 /* kind MAT_SPOT (4): diffuse_spot_light (materials/diffuse_spot_light.cuh), cone in dir/cos_cutoff/falloff */
@@ -138,6 +145,7 @@ typedef struct { float lo[3], hi[3]; int left, right, first, count; } node_t;
 
 typedef struct {
     prim_t* prims; int nprims;
+    xf_t* xf; int nxf;
     int* order;           /* BVH leaf order */
     node_t* nodes; int nnodes;
     tex_t* tex; int ntex;
@@ -162,6 +170,72 @@ static void planar_init(prim_t* p) {
     p->D = vdot(p->normal, p->a);
     p->w = vdivs(n, vdot(n, n));
     p->area = vlen(n);
+}
+
+/* glm::rotate(m, angle, axis) for a coordinate axis (glm/ext/matrix_transform.inl:18-46), float, same
+ * operation order; m column-major m[column][row] */
+static void glm_rotate_axis(float m[4][4], float angle, int ax) {
+    const float c = cosf(angle), sn = sinf(angle);
+    float axis[3] = {0.0f, 0.0f, 0.0f}, R[3][3], out[3][4];
+    axis[ax] = 1.0f;
+    const float temp[3] = {(1.0f - c) * axis[0], (1.0f - c) * axis[1], (1.0f - c) * axis[2]};
+    R[0][0] = c + temp[0] * axis[0];
+    R[0][1] = temp[0] * axis[1] + sn * axis[2];
+    R[0][2] = temp[0] * axis[2] - sn * axis[1];
+    R[1][0] = temp[1] * axis[0] - sn * axis[2];
+    R[1][1] = c + temp[1] * axis[1];
+    R[1][2] = temp[1] * axis[2] + sn * axis[0];
+    R[2][0] = temp[2] * axis[0] + sn * axis[1];
+    R[2][1] = temp[2] * axis[1] - sn * axis[0];
+    R[2][2] = c + temp[2] * axis[2];
+    for (int j = 0; j < 3; ++j)
+        for (int i = 0; i < 4; ++i) out[j][i] = (m[0][i] * R[j][0] + m[1][i] * R[j][1]) + m[2][i] * R[j][2];
+    for (int j = 0; j < 3; ++j)
+        for (int i = 0; i < 4; ++i) m[j][i] = out[j][i];
+}
+/* rt::rotate's matrix: identity rotated about x, y, z by degrees_to_radians(sign * angle) (float M_PI) */
+static void rotate_matrix(const float deg[3], float sign, float out[3][3]) {
+    float m[4][4];
+    for (int j = 0; j < 4; ++j)
+        for (int i = 0; i < 4; ++i) m[j][i] = i == j ? 1.0f : 0.0f;
+    for (int ax = 0; ax < 3; ++ax) glm_rotate_axis(m, (sign * deg[ax]) * PI_F / 180.0f, ax);
+    for (int j = 0; j < 3; ++j)
+        for (int i = 0; i < 3; ++i) out[j][i] = m[j][i];
+}
+/* glm mat4 * vec4 for a rotation: (m0_i x + m1_i y) + (m2_i z + 0) */
+static v3 rot_apply(const float m[3][3], v3 v) {
+    return V((m[0][0] * v.x + m[1][0] * v.y) + (m[2][0] * v.z + 0.0f), (m[0][1] * v.x + m[1][1] * v.y) + (m[2][1] * v.z + 0.0f),
+             (m[0][2] * v.x + m[1][2] * v.y) + (m[2][2] * v.z + 0.0f));
+}
+/* world ray -> object space: scale (o / s, d / s), rotate (inverse matrix), translate (o - t) */
+static void xf_to_object(const xf_t* x, v3* o, v3* d) {
+    if (x->flags & 4u) { *o = V(o->x / x->s.x, o->y / x->s.y, o->z / x->s.z); *d = V(d->x / x->s.x, d->y / x->s.y, d->z / x->s.z); }
+    if (x->flags & 2u) { *o = rot_apply(x->inv, *o); *d = rot_apply(x->inv, *d); }
+    if (x->flags & 1u) *o = vsub(*o, x->t);
+}
+/* hit point / normal -> world: translate (+t), rotate (forward matrix), scale (p * s, unit(n / s)) */
+static void xf_to_world(const xf_t* x, v3* p, v3* n) {
+    if (x->flags & 1u) *p = vadd(*p, x->t);
+    if (x->flags & 2u) { *p = rot_apply(x->fwd, *p); *n = rot_apply(x->fwd, *n); }
+    if (x->flags & 4u) { *p = V(p->x * x->s.x, p->y * x->s.y, p->z * x->s.z); *n = vunit(V(n->x / x->s.x, n->y / x->s.y, n->z / x->s.z)); }
+}
+/* world bounds of an object-space box through x: corners mapped by s * R_inv^T (c + t), in double */
+static void xf_box(const xf_t* x, float* lo, float* hi) {
+    double L[3] = {INFINITY, INFINITY, INFINITY}, H[3] = {-INFINITY, -INFINITY, -INFINITY}, mag = 0.0, smax = 1.0;
+    for (int c = 0; c < 8; ++c) {
+        double p[3] = {(c & 1) ? hi[0] : lo[0], (c & 2) ? hi[1] : lo[1], (c & 4) ? hi[2] : lo[2]}, q[3];
+        if (x->flags & 1u) { p[0] += x->t.x; p[1] += x->t.y; p[2] += x->t.z; }
+        for (int k = 0; k < 3; ++k) if (fabs(p[k]) > mag) mag = fabs(p[k]);
+        if (x->flags & 2u) {
+            for (int k = 0; k < 3; ++k) q[k] = x->inv[k][0] * p[0] + x->inv[k][1] * p[1] + x->inv[k][2] * p[2];
+            for (int k = 0; k < 3; ++k) p[k] = q[k];
+        }
+        if (x->flags & 4u) { p[0] *= x->s.x; p[1] *= x->s.y; p[2] *= x->s.z; }
+        for (int k = 0; k < 3; ++k) { if (p[k] < L[k]) L[k] = p[k]; if (p[k] > H[k]) H[k] = p[k]; }
+    }
+    if (x->flags & 4u) smax = fmax(fabs(x->s.x), fmax(fabs(x->s.y), fabs(x->s.z)));
+    const double e = 4e-6 * mag * smax + 1e-6;
+    for (int k = 0; k < 3; ++k) { lo[k] = (float)(L[k] - e); hi[k] = (float)(H[k] + e); }
 }
 
 static int cmp_axis;
@@ -203,7 +277,7 @@ void* port_scene_create(const rtc_scene_desc* d) {
     for (uint32_t m = 0; m < d->num_meshes; ++m) ntri += (int)d->meshes[m].num_triangles;
     const int n_omni = (int)d->num_omni_lights, n_dir = (int)d->num_dir_lights, n_spot = (int)d->num_spot_lights;
     const int n_lights = n_omni + n_dir + n_spot;   /* light list: omni, directional, spot (gpu.cu:504-523) */
-    s->nprims = n_lights + (int)(d->num_spheres + d->num_quads) + ntri;
+    s->nprims = n_lights + (int)(d->num_spheres + d->num_quads) + 6 * (int)d->num_boxes + ntri;
     s->prims = (prim_t*)calloc((size_t)s->nprims + 1, sizeof(prim_t));
     s->ntex = (int)d->num_textures + n_lights;
     s->tex = (tex_t*)calloc((size_t)s->ntex + 1, sizeof(tex_t));
@@ -229,6 +303,16 @@ void* port_scene_create(const rtc_scene_desc* d) {
     for (int i = 0; i < s->nimg; ++i) s->img[i] = d->images[i];
     s->cam = d->camera;
     s->bg = d->background;
+    s->nxf = (int)d->num_transforms;
+    s->xf = (xf_t*)calloc((size_t)s->nxf + 1, sizeof(xf_t));
+    for (int i = 0; i < s->nxf; ++i) {
+        const rtc_transform* T = &d->transforms[i];
+        xf_t* x = &s->xf[i];
+        x->t = Vp(T->translate); x->s = Vp(T->scale); x->flags = T->flags & 7u;
+        rotate_matrix(T->rotate, -1.0f, x->inv);
+        rotate_matrix(T->rotate, 1.0f, x->fwd);
+    }
+    for (int i = 0; i < s->nprims; ++i) { s->prims[i].xf = -1; s->prims[i].gid = i; }
     int k = 0;
     /* omni and spot lights: spheres (omni_light.cuh / spot_light.cuh) */
     for (int j = 0; j < n_omni + n_spot; ++j) {
@@ -287,6 +371,7 @@ void* port_scene_create(const rtc_scene_desc* d) {
         p->kind = K_SPHERE; p->mat = S->material; p->a = Vp(S->center); p->rad = S->radius;
         float r = fabsf(S->radius);
         for (int q = 0; q < 3; ++q) { p->lo[q] = S->center[q] - r; p->hi[q] = S->center[q] + r; }
+        p->xf = d->sphere_transforms ? (int)d->sphere_transforms[i] - 1 : -1;
     }
     for (uint32_t i = 0; i < d->num_quads; ++i, ++k) {
         const rtc_quad* Q = &d->quads[i];
@@ -296,7 +381,28 @@ void* port_scene_create(const rtc_scene_desc* d) {
         for (int q = 0; q < 3; ++q) { p->lo[q] = FLT_MAX; p->hi[q] = -FLT_MAX; }
         box_grow(p->lo, p->hi, p->a); box_grow(p->lo, p->hi, vadd(p->a, p->b));
         box_grow(p->lo, p->hi, vadd(p->a, p->c)); box_grow(p->lo, p->hi, vadd(vadd(p->a, p->b), p->c));
+        p->xf = d->quad_transforms ? (int)d->quad_transforms[i] - 1 : -1;
     }
+    /* boxes (box.cuh:40-52): six faces, pmin = center - size / 2, pmax = pmin + size; face order front
+     * (z = pmax.z), back (z = pmin.z, flipped), top, bottom (flipped), right, left (flipped) */
+    const int box_gid0 = k;
+    for (uint32_t i = 0; i < d->num_boxes; ++i) {
+        const rtc_box* B = &d->boxes[i];
+        float lo[3], hi[3];
+        for (int q = 0; q < 3; ++q) { lo[q] = B->center[q] - (B->size[q] / 2.0f); hi[q] = lo[q] + B->size[q]; }
+        for (int f = 0; f < 6; ++f, ++k) {
+            prim_t* p = &s->prims[k];
+            const int axis = f / 2, low = f & 1;
+            const int a = axis == 2 ? 1 : 0, b = axis == 0 ? 1 : 2, n = axis == 0 ? 2 : axis == 1 ? 1 : 0;
+            p->kind = K_RECT; p->mat = B->material; p->axis = axis; p->flip = low;
+            p->r0 = lo[a]; p->r1 = hi[a]; p->s0 = lo[b]; p->s1 = hi[b]; p->k = low ? lo[n] : hi[n];
+            p->xf = (int)B->transform - 1;
+            p->gid = box_gid0 + (int)i;
+            for (int q = 0; q < 3; ++q) { p->lo[q] = lo[q]; p->hi[q] = hi[q]; }
+            p->lo[n] = p->hi[n] = p->k;
+        }
+    }
+    const int tri_gid_shift = 5 * (int)d->num_boxes;   /* one id per box, not per face */
     for (uint32_t m = 0; m < d->num_meshes; ++m) {
         const rtc_mesh* M = &d->meshes[m];
         for (uint32_t f = 0; f < M->num_triangles; ++f, ++k) {
@@ -314,8 +420,12 @@ void* port_scene_create(const rtc_scene_desc* d) {
             }
             for (int q = 0; q < 3; ++q) { p->lo[q] = FLT_MAX; p->hi[q] = -FLT_MAX; }
             box_grow(p->lo, p->hi, v0); box_grow(p->lo, p->hi, v1); box_grow(p->lo, p->hi, v2);
+            p->xf = d->mesh_transforms ? (int)d->mesh_transforms[m] - 1 : -1;
+            p->gid = k - tri_gid_shift;
         }
     }
+    for (int i = 0; i < s->nprims; ++i)
+        if (s->prims[i].xf >= 0) xf_box(&s->xf[s->prims[i].xf], s->prims[i].lo, s->prims[i].hi);
     for (int i = 0; i < s->nprims; ++i)   /* conservative padding */
         for (int q = 0; q < 3; ++q) {
             float e = 1e-4f * (fabsf(s->prims[i].lo[q]) + fabsf(s->prims[i].hi[q])) + 1e-5f;
@@ -332,7 +442,7 @@ void* port_scene_create(const rtc_scene_desc* d) {
 void port_scene_destroy(void* p) {
     scene_t* s = (scene_t*)p;
     if (!s) return;
-    free(s->prims); free(s->order); free(s->nodes); free(s->tex); free(s->mat); free(s->img); free(s->lights);
+    free(s->prims); free(s->order); free(s->nodes); free(s->tex); free(s->mat); free(s->img); free(s->lights); free(s->xf);
     free(s);
 }
 
@@ -419,9 +529,25 @@ static int tri_t(const prim_t* p, v3 o, v3 d, float tmin, float tmax, float* t, 
     return 1;
 }
 
+/* xy_rect / xz_rect / yz_rect::hit (aarect.cuh): inclusive interval and bounds */
+static int rect_t(const prim_t* p, v3 o, v3 d, float tmin, float tmax, float* t, float* al, float* be) {
+    const float oa = p->axis == 0 ? o.z : p->axis == 1 ? o.y : o.x, da = p->axis == 0 ? d.z : p->axis == 1 ? d.y : d.x;
+    const float tt = (p->k - oa) / da;
+    if (tt < tmin || tt > tmax) return 0;
+    const float o0 = p->axis == 2 ? o.y : o.x, d0 = p->axis == 2 ? d.y : d.x;
+    const float o1 = p->axis == 0 ? o.y : o.z, d1 = p->axis == 0 ? d.y : d.z;
+    const float a = o0 + tt * d0, b = o1 + tt * d1;
+    if (a < p->r0 || a > p->r1 || b < p->s0 || b > p->s1) return 0;
+    *t = tt; *al = a; *be = b;
+    return 1;
+}
+
+static int prim_t_test_xf(const scene_t* s, const prim_t* p, v3 o, v3 d, float tmin, float tmax, int hide, int exact,
+                          float* t);
 static int prim_t_test(const prim_t* p, v3 o, v3 d, float tmin, float tmax, int hide, int exact, float* t) {
     float a, b;
     switch (p->kind) {
+    case K_RECT: return rect_t(p, o, d, tmin, tmax, t, &a, &b);
     case K_SPHERE: return exact ? sphere_t_exact(p, o, d, tmin, tmax, t) : sphere_t(p, o, d, tmin, tmax, t);
     case K_QUAD: return planar_t(p, o, d, tmin, tmax, 0, t, &a, &b);
     case K_LIGHT:
@@ -433,6 +559,11 @@ static int prim_t_test(const prim_t* p, v3 o, v3 d, float tmin, float tmax, int 
         return !(p->invisible && hide);   /* directional_light.cuh:106, omni_light.cuh:76-80 */
     default: return tri_t(p, o, d, tmin, tmax, t, &a, &b);
     }
+}
+static int prim_t_test_xf(const scene_t* s, const prim_t* p, v3 o, v3 d, float tmin, float tmax, int hide, int exact,
+                          float* t) {
+    if (p->xf >= 0) xf_to_object(&s->xf[p->xf], &o, &d);
+    return prim_t_test(p, o, d, tmin, tmax, hide, exact, t);
 }
 
 /* aabb::hit semantics (aabb.cuh:141-166) on the port's own (padded) boxes */
@@ -461,7 +592,7 @@ static int closest(const scene_t* s, v3 o, v3 d, float tmin, float tmax, int hid
         if (n->left < 0) {
             for (int i = n->first; i < n->first + n->count; ++i) {
                 float t;
-                if (prim_t_test(&s->prims[s->order[i]], o, d, tmin, best_t, hide, exact, &t)) { best_t = t; best = s->order[i]; }
+                if (prim_t_test_xf(s, &s->prims[s->order[i]], o, d, tmin, best_t, hide, exact, &t)) { best_t = t; best = s->order[i]; }
             }
         } else {
             if (sp + 2 > 128) return 0;
@@ -477,7 +608,21 @@ static int closest(const scene_t* s, v3 o, v3 d, float tmin, float tmax, int hid
 static void finalize(const scene_t* s, int pi, float t, v3 o, v3 d, hit_t* h) {
     const prim_t* p = &s->prims[pi];
     h->t = t; h->prim = pi; h->mat = p->mat;
-    if (p->kind == K_SPHERE) {
+    if (p->xf >= 0) xf_to_object(&s->xf[p->xf], &o, &d);
+    if (p->kind == K_RECT) {
+        /* aarect hit(): r.at(t), the axis normal (flip_normals negates it), front_face stays true, uv by
+         * get_xy/xz/yz_rect_uv with the default mapping */
+        const float o0 = p->axis == 2 ? o.y : o.x, d0 = p->axis == 2 ? d.y : d.x;
+        const float o1 = p->axis == 0 ? o.y : o.z, d1 = p->axis == 0 ? d.y : d.z;
+        const float a = o0 + t * d0, b = o1 + t * d1;
+        float su = (a - p->r0) / (p->r1 - p->r0), sv = (b - p->s0) / (p->s1 - p->s0);
+        su = fmodf(su * 1.0f, 1.0f); sv = fmodf(sv * 1.0f, 1.0f);
+        h->u = 1.0f * su + 0.0f; h->v = 1.0f * sv + 0.0f;
+        h->p = vat(o, d, t);
+        const float sg = p->flip ? -1.0f : 1.0f;
+        h->n = p->axis == 0 ? V(0.0f, 0.0f, sg) : p->axis == 1 ? V(0.0f, sg, 0.0f) : V(sg, 0.0f, 0.0f);
+        h->front = 1;
+    } else if (p->kind == K_SPHERE) {
         h->p = vat(o, d, t);
         v3 outward = vdivs(vsub(h->p, p->a), p->rad);
         face(h, d, outward);
@@ -512,6 +657,7 @@ static void finalize(const scene_t* s, int pi, float t, v3 o, v3 d, hit_t* h) {
         face(h, d, normal);
         h->u = 0.0f; h->v = 0.0f;   /* get_triangle_uv over all-zero vertex uvs */
     }
+    if (p->xf >= 0) xf_to_world(&s->xf[p->xf], &h->p, &h->n);
 }
 
 /* ---------------------------------------------------------------------------------------------- */
@@ -873,7 +1019,7 @@ int port_trace_closest(void* sp, const float* rays, int64_t n, int depth, int ma
         const float* R = rays + 8 * k;
         float t; int pi;
         int h = closest(s, V(R[0], R[1], R[2]), V(R[4], R[5], R[6]), R[3], R[7], depth == max_depth, 0, &t, &pi);
-        if (prim) prim[k] = h ? pi : -1;
+        if (prim) prim[k] = h ? s->prims[pi].gid : -1;
         if (tout) tout[k] = h ? t : INFINITY;
     }
     return 0;

@@ -128,6 +128,11 @@ int main() {
     static boxPrimitiveConfig boxes[1];
     boxes[0].name = "box";
     boxes[0].materialName = "white";
+    boxes[0].position = point3(212.5f, 82.5f, 147.5f);
+    boxes[0].size = vector3(165.0f, 165.0f, 165.0f);
+    boxes[0].transform.setTranslate(vector3(10.0f, 0.0f, -5.0f));
+    boxes[0].transform.setRotate(vector3(0.0f, 18.0f, 0.0f));
+    spheres[0].transform.setScale(vector3(2.0f, 1.0f, 1.0f));
     cfg.primitivesCfg.quadPrimitives = quads;
     cfg.primitivesCfg.quadPrimitiveCount = 6;
     cfg.primitivesCfg.spherePrimitives = spheres;
@@ -216,6 +221,26 @@ int main() {
         arr3("v", q.v);
         std::printf("\"material\": %d}", q.material);
     }
+    std::printf("], \"boxes\": [");
+    for (uint32_t i = 0; i < d->num_boxes; ++i) {
+        const rtc_box& b = d->boxes[i];
+        std::printf("%s{", i ? ", " : "");
+        arr3("center", b.center);
+        arr3("size", b.size);
+        std::printf("\"material\": %d, \"transform\": %u}", b.material, b.transform);
+    }
+    std::printf("], \"transforms\": [");
+    for (uint32_t i = 0; i < d->num_transforms; ++i) {
+        const rtc_transform& x = d->transforms[i];
+        std::printf("%s{", i ? ", " : "");
+        arr3("translate", x.translate);
+        arr3("rotate", x.rotate);
+        arr3("scale", x.scale);
+        std::printf("\"flags\": %u}", x.flags);
+    }
+    std::printf("], \"sphere_transforms\": [");
+    for (uint32_t i = 0; d->sphere_transforms && i < d->num_spheres; ++i)
+        std::printf("%s%u", i ? ", " : "", d->sphere_transforms[i]);
     std::printf("], \"meshes\": [");
     for (uint32_t i = 0; i < d->num_meshes; ++i) {
         const rtc_mesh& m = d->meshes[i];

@@ -121,6 +121,30 @@ int main(int argc, char** argv) {
         arr("v", q.v, 3);
         std::printf("\"material\": %d}", q.material);
     }
+    std::printf("], \"boxes\": [");
+    for (uint32_t i = 0; i < d->num_boxes; ++i) {
+        const rtc_box& b = d->boxes[i];
+        std::printf("%s{", i ? ", " : "");
+        arr("center", b.center, 3);
+        arr("size", b.size, 3);
+        std::printf("\"material\": %d, \"transform\": %u}", b.material, b.transform);
+    }
+    std::printf("], \"transforms\": [");
+    for (uint32_t i = 0; i < d->num_transforms; ++i) {
+        const rtc_transform& x = d->transforms[i];
+        std::printf("%s{", i ? ", " : "");
+        arr("translate", x.translate, 3);
+        arr("rotate", x.rotate, 3);
+        arr("scale", x.scale, 3);
+        std::printf("\"flags\": %u}", x.flags);
+    }
+    auto refs = [&](const char* k, const uint32_t* r, uint32_t n) {
+        std::printf("], \"%s\": [", k);
+        for (uint32_t i = 0; r && i < n; ++i) std::printf("%s%u", i ? ", " : "", r[i]);
+    };
+    refs("sphere_transforms", d->sphere_transforms, d->num_spheres);
+    refs("quad_transforms", d->quad_transforms, d->num_quads);
+    refs("mesh_transforms", d->mesh_transforms, d->num_meshes);
     std::printf("], \"meshes\": [");
     for (uint32_t i = 0; i < d->num_meshes; ++i) {
         const rtc_mesh& m = d->meshes[i];

@@ -39,6 +39,7 @@ GOLDEN_SCENES = {
     "textured": dict(width=40, height=30, spp=9, max_depth=10),
     "icosphere": dict(width=36, height=24, spp=9, max_depth=12),
     "lights": dict(width=40, height=30, spp=9, max_depth=10),
+    "xforms": dict(width=40, height=40, spp=9, max_depth=8),   # boxes and transforms
 }
 RAYS_PER_SCENE = 4096
 

@@ -35,6 +35,7 @@ SCENES = [
     ("textured", dict(width=64, height=48, spp=9, max_depth=10)),
     ("icosphere", dict(width=60, height=40, spp=9, max_depth=12)),
     ("lights", dict(width=48, height=36, spp=9, max_depth=10)),   # omni, directional and spot lights
+    ("xforms", dict(width=48, height=48, spp=9, max_depth=8)),    # boxes, translate / rotate / scale
 ]
 
 
@@ -85,6 +86,19 @@ def test_kernel_bitexact_vs_port(ctx, port, name, kw, engine):
     st = oracles.parity_stats(ours.reshape(-1, 4), ref)
     print(name, order, engine, st)
     # exact-t ties between primitives may resolve differently in two different BVHs
+    assert st["frac_exact"] >= 0.999, st
+
+
+@pytest.mark.parametrize("engine", [ENGINE_MEGAKERNEL, ENGINE_WAVEFRONT])
+def test_multi_axis_transforms_bitexact_vs_port(ctx, port, engine):
+    """Boxes and a mesh turned about two and three axes and scaled: the forward matrix maps hit points
+    and normals back, as rt::rotate does; the kernel equals the C restatement pixel for pixel."""
+    scene, params = _params("xforms_multi", dict(width=48, height=48, spp=9, max_depth=8), DRAW_ORDER_HOST, engine)
+    ours, _ = DeviceScene(ctx, scene).render(params)
+    pix = np.arange(params.width * params.height, dtype=np.int64)
+    ref, _ = port.scene(scene).render_pixels(params, pix, trig=1)
+    st = oracles.parity_stats(ours.reshape(-1, 4), ref)
+    print("xforms_multi", engine, st)
     assert st["frac_exact"] >= 0.999, st
 
 

@@ -166,7 +166,8 @@ def test_sections_read_like_scene_loader(scene_dir):
     assert np.ctypeslib.as_array(m.vertices, shape=(9,)).tolist() == [0, 2, 0, 1, 2, 0, 0, 3, 0]
     metal = d.materials[m.material]
     assert metal.kind == MAT_METAL and metal.fuzz == 1.0
-    assert any("boxes" in s for s in f.skipped) and any("noise" in s for s in f.skipped)
+    assert d.num_boxes == 1 and list(d.boxes[0].size) == [1.0, 1.0, 1.0] and d.boxes[0].transform == 0
+    assert not any("boxes" in s for s in f.skipped) and any("noise" in s for s in f.skipped)
     assert any("phong" in s for s in f.skipped)
     f.close()
 
@@ -239,6 +240,10 @@ def _arr(p, n):
     return [float(p[i]) for i in range(n)]
 
 
+def _refs(p, n):
+    return [int(p[i]) for i in range(n)] if p else []
+
+
 def _desc_json(f):
     """The fields oracle/scenefile_check.cpp prints, from this library's description."""
     d, info = f.desc, f.info
@@ -261,6 +266,13 @@ def _desc_json(f):
                     for s in (d.spheres[i] for i in range(d.num_spheres))],
         "quads": [{"q": _arr(q.q, 3), "u": _arr(q.u, 3), "v": _arr(q.v, 3), "material": q.material}
                   for q in (d.quads[i] for i in range(d.num_quads))],
+        "boxes": [{"center": _arr(b.center, 3), "size": _arr(b.size, 3), "material": b.material,
+                   "transform": b.transform} for b in (d.boxes[i] for i in range(d.num_boxes))],
+        "transforms": [{"translate": _arr(x.translate, 3), "rotate": _arr(x.rotate, 3), "scale": _arr(x.scale, 3),
+                        "flags": x.flags} for x in (d.transforms[i] for i in range(d.num_transforms))],
+        "sphere_transforms": _refs(d.sphere_transforms, d.num_spheres),
+        "quad_transforms": _refs(d.quad_transforms, d.num_quads),
+        "mesh_transforms": _refs(d.mesh_transforms, d.num_meshes),
         "meshes": [{"vertices": _arr(m.vertices, 3 * m.num_vertices), "num_triangles": m.num_triangles,
                     "material": m.material, "smooth": m.smooth} for m in (d.meshes[i] for i in range(d.num_meshes))],
         "camera": {"look_from": _arr(d.camera.look_from, 3), "look_at": _arr(d.camera.look_at, 3),

@@ -36,7 +36,18 @@ def test_objects_in_load_scene_order_and_unresolved_skipped(desc):
     assert len(d["quads"]) == 5            # so is the quad with an unknown material
     assert [s["radius"] for s in d["spheres"]] == [90.0, 80.0, 60.0]
     assert any("missing" in s for s in d["skipped"]) and any("nosuchmaterial" in s for s in d["skipped"])
-    assert "boxes" in d["skipped"]
+    assert "boxes" not in d["skipped"]
+
+
+def test_boxes_and_transforms(desc):
+    """boxPrimitives become rtc_box (after the quads); each rt::transform becomes a 1-based reference
+    with the parts it has (scene_factory::applyTransform)."""
+    b, = desc["boxes"]
+    assert b["center"] == [212.5, 82.5, 147.5] and b["size"] == [165.0, 165.0, 165.0]
+    xs = desc["transforms"]
+    assert desc["sphere_transforms"] == [1, 0, 0] and b["transform"] == 2
+    assert xs[0]["flags"] == 4 and xs[0]["scale"] == [2.0, 1.0, 1.0]
+    assert xs[1]["flags"] == 3 and xs[1]["translate"] == [10.0, 0.0, -5.0] and xs[1]["rotate"] == [0.0, 18.0, 0.0]
 
 
 def test_omni_and_spot_lights(desc):
