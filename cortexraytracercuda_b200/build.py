@@ -40,6 +40,13 @@ SOURCES = [
     ("wavefront_compat.cu", "wavefront_compat_dev", "nvcc", ["--fmad=true", "-DRTC_FLAVOR=0"]),
     ("render_clean.cu", "render_clean", "nvcc", ["--fmad=true"]),
     ("wavefront_clean.cu", "wavefront_clean", "nvcc", ["--fmad=true"]),
+    # the same kernels with the xprim BVH walk (RTC_XP=1), for scenes with transformed primitives or boxes
+    ("render_compat.cu", "render_compat_host_x", "nvcc", ["--fmad=false", "-DRTC_FLAVOR=1", "-DRTC_XP=1"]),
+    ("render_compat.cu", "render_compat_dev_x", "nvcc", ["--fmad=true", "-DRTC_FLAVOR=0", "-DRTC_XP=1"]),
+    ("wavefront_compat.cu", "wavefront_compat_host_x", "nvcc", ["--fmad=false", "-DRTC_FLAVOR=1", "-DRTC_XP=1"]),
+    ("wavefront_compat.cu", "wavefront_compat_dev_x", "nvcc", ["--fmad=true", "-DRTC_FLAVOR=0", "-DRTC_XP=1"]),
+    ("render_clean.cu", "render_clean_x", "nvcc", ["--fmad=true", "-DRTC_XP=1"]),
+    ("wavefront_clean.cu", "wavefront_clean_x", "nvcc", ["--fmad=true", "-DRTC_XP=1"]),
     ("render_noalloc.cu", "render_noalloc", "nvcc", []),
     ("rtc_api.cpp", "rtc_api", "cxx", []),
     ("rtc_engine.cpp", "rtc_engine", "cxx", []),

@@ -8,6 +8,7 @@
 #include "rtc_path.cuh"
 
 namespace rtc {
+inline namespace RTC_XP_NS {
 
 __global__ void __launch_bounds__(128) rtc_render_clean(DevScene S, DevParams P, float4* __restrict__ out,
                                                         unsigned long long* counters, uint32_t* status_word) {
@@ -69,11 +70,12 @@ __global__ void __launch_bounds__(128) rtc_render_clean(DevScene S, DevParams P,
     if (status) atomicOr(status_word, status);
 }
 
+}  // namespace RTC_XP_NS
 }  // namespace rtc
 
 using namespace rtc;
 
-cudaError_t rtc_launch_render_clean(const DevScene& S, const DevParams& P, float4* out, unsigned long long* counters,
+cudaError_t RTC_XP_FN(rtc_launch_render_clean)(const DevScene& S, const DevParams& P, float4* out, unsigned long long* counters,
                                     uint32_t* status, int block, cudaStream_t st) {
     (void)block;
     const int threads = 128;

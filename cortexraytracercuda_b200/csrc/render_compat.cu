@@ -24,6 +24,7 @@
 #endif
 
 namespace rtc {
+inline namespace RTC_XP_NS {
 
 __device__ __forceinline__ void flush_counters(unsigned long long* counters, uint32_t rays, uint32_t paths,
                                                uint32_t nodes, uint32_t prims) {
@@ -108,6 +109,7 @@ __global__ void __launch_bounds__(128) rtc_trace_closest(DevScene S, const float
 
 #endif  // RTC_FLAVOR == 1
 
+}  // namespace RTC_XP_NS
 }  // namespace rtc
 
 using namespace rtc;
@@ -124,7 +126,7 @@ cudaError_t RTC_FLAVOR_FN(rtc_launch_render_compat)(const DevScene& S, const Dev
 
 #if RTC_FLAVOR == 1
 
-cudaError_t rtc_launch_trace_closest(const DevScene& S, const float* rays, uint32_t n, int depth, int max_depth,
+cudaError_t RTC_XP_FN(rtc_launch_trace_closest)(const DevScene& S, const float* rays, uint32_t n, int depth, int max_depth,
                                      int32_t* prim, float* t, uint32_t* status, cudaStream_t st) {
     if (n == 0) return cudaSuccess;
     const int threads = 128;

@@ -471,17 +471,32 @@ rtc_status rtc_build_host_scene(const rtc_scene_desc* d, HostScene& H, uint32_t 
     }
 
     // ---- BVH -----------------------------------------------------------------------------------
-    BvhOutput bvh;
+    // Transformed primitives and box faces (xprims) get a BVH of their own, walked after the main one by
+    // kernels built for it; the main BVH holds every other primitive (and may be empty).
+    std::vector<uint32_t> main_ids, x_ids;
+    BvhInput bin_x;
+    {
+        BvhInput bin_main;
+        for (uint32_t i = 0; i < (uint32_t)prims.size(); ++i) {
+            const bool x = prims[i].kind == ITEM_XPRIM;
+            (x ? x_ids : main_ids).push_back(i);
+            (x ? bin_x : bin_main).boxes.push_back(bin.boxes[i]);
+        }
+        bin = std::move(bin_main);
+    }
+    BvhOutput bvh, xbvh;
     const char* berr = nullptr;
     uint32_t builder = RTC_BVH_SAH;
-    if (bvh_builder != RTC_BVH_SAH) {
+    if (bvh_builder != RTC_BVH_SAH && !main_ids.empty()) {
         const int rc = build_bvh_device(bin, device, bvh_builder == RTC_BVH_DEVICE_LBVH ? BVH_DEVICE_LBVH : BVH_DEVICE_PLOC,
                                         bvh, &berr);
         if (rc == BVH_DEVICE_ERROR) return fail(RTC_ERR_CUDA, std::string("device BVH build: ") + (berr ? berr : "failed"));
         if (rc == BVH_DEVICE_OK) builder = bvh_builder;
         berr = nullptr;
     }
-    if (builder == RTC_BVH_SAH && !build_bvh(bin, 4, 0, bvh, &berr)) return bad(berr ? berr : "BVH build failed");
+    if (builder == RTC_BVH_SAH && !main_ids.empty() && !build_bvh(bin, 4, 0, bvh, &berr))
+        return bad(berr ? berr : "BVH build failed");
+    if (!x_ids.empty() && !build_bvh(bin_x, 4, 0, xbvh, &berr)) return bad(berr ? berr : "BVH build failed");
     auto t1 = std::chrono::steady_clock::now();
 
     // ---- materials / textures (directional lights get their own diffuse_light + solid texture) --
@@ -532,7 +547,7 @@ rtc_status rtc_build_host_scene(const rtc_scene_desc* d, HostScene& H, uint32_t 
     }
 
     // ---- per-kind arrays in leaf order ---------------------------------------------------------
-    std::vector<uint32_t> items(bvh.order.size());
+    std::vector<uint32_t> items(bvh.order.size()), xitems(xbvh.order.size());
     std::vector<float4> sph, tri, tri_n, tri_vn, quad, light(6 * (size_t)nlights), rect, xf;
     std::vector<int2> sph_aux;
     std::vector<int4> xprim;
@@ -618,8 +633,9 @@ rtc_status rtc_build_host_scene(const rtc_scene_desc* d, HostScene& H, uint32_t 
         tri_n.push_back(make_float4(mn.x, mn.y, mn.z, 0.0f));
         return typed;
     };
-    for (size_t k = 0; k < bvh.order.size(); ++k) {
-        const PrimRef& pr = prims[bvh.order[k]];
+    for (size_t k = 0; k < bvh.order.size() + xbvh.order.size(); ++k) {
+        const bool xk = k >= bvh.order.size();
+        const PrimRef& pr = xk ? prims[x_ids[xbvh.order[k - bvh.order.size()]]] : prims[main_ids[bvh.order[k]]];
         uint32_t typed = 0;
         switch (pr.kind) {
         case ITEM_LIGHT: typed = pr.src; break;
@@ -645,7 +661,7 @@ rtc_status rtc_build_host_scene(const rtc_scene_desc* d, HostScene& H, uint32_t 
             xprim.push_back(make_int4(pr.xf, pr.inner, (int)inner, (int)gid));
         } break;
         }
-        items[k] = ((uint32_t)pr.kind << ITEM_KIND_SHIFT) | typed;
+        (xk ? xitems[k - bvh.order.size()] : items[k]) = ((uint32_t)pr.kind << ITEM_KIND_SHIFT) | typed;
     }
     for (uint32_t i = 0; i < d->num_transforms; ++i) put_transform(d->transforms[i], xf);
 
@@ -682,6 +698,8 @@ rtc_status rtc_build_host_scene(const rtc_scene_desc* d, HostScene& H, uint32_t 
     size_t o_xprim = add_chunk(xprim.data(), xprim.size() * 16);
     size_t o_xf = add_chunk(xf.data(), xf.size() * 16);
     size_t o_rect = add_chunk(rect.data(), rect.size() * 16);
+    size_t o_xnodes = add_chunk(xbvh.nodes.data(), xbvh.nodes.size() * sizeof(float));
+    size_t o_xitems = add_chunk(xitems.data(), xitems.size() * 4);
     size_t env_bytes = d->background.kind == RTC_BG_ENV_MAP
                            ? (size_t)d->background.env_width * d->background.env_height * 3 * sizeof(float) : 0;
     size_t o_env = add_chunk(env_bytes ? d->background.env_rgb : nullptr, env_bytes);
@@ -715,6 +733,10 @@ rtc_status rtc_build_host_scene(const rtc_scene_desc* d, HostScene& H, uint32_t 
     D.num_xprim = (uint32_t)xprim.size();
     D.num_xf = d->num_transforms;
     D.num_rect = (uint32_t)(rect.size() / 2);
+    D.xnodes = xbvh.num_nodes ? (const float4*)off(o_xnodes) : nullptr;
+    D.xitems = xbvh.num_nodes ? (const uint32_t*)off(o_xitems) : nullptr;
+    D.num_xnodes = xbvh.num_nodes;
+    D.num_xitems = (uint32_t)xitems.size();
     D.num_nodes = bvh.num_nodes;
     D.num_nodes8 = bvh.num_nodes8;
     D.num_items = (uint32_t)items.size();
@@ -755,6 +777,7 @@ DevScene rtc_rebase_scene(const HostScene& H, uint8_t* base) {
     rb(D.sph); rb(D.sph_aux); rb(D.tri); rb(D.tri_n); rb(D.tri_vn); rb(D.quad);
     rb(D.light); rb(D.mat_i); rb(D.mat_f); rb(D.tex_i); rb(D.tex_f); rb(D.images); rb(D.image_bytes);
     rb(D.xprim); rb(D.xf); rb(D.rect);
+    if (D.xnodes) { rb(D.xnodes); rb(D.xitems); }
     if (D.bg.env) rb(D.bg.env);
     return D;
 }
@@ -952,9 +975,11 @@ struct WfTimer {
     }
 };
 
-rtc::WfOneFn wf_one_fn(const rtc_render_params* p) {
-    if (p->mode == RTC_MODE_CLEAN) return rtc_wf_one_clean;
-    return p->draw_order == RTC_DRAW_ORDER_HOST ? rtc_wf_one_compat_host : rtc_wf_one_compat_dev;
+// `xp`: the scene has transformed primitives or boxes (an xprim BVH), walked by the RTC_XP=1 kernels.
+rtc::WfOneFn wf_one_fn(const rtc_render_params* p, bool xp) {
+    if (p->mode == RTC_MODE_CLEAN) return xp ? rtc_wf_one_clean_x : rtc_wf_one_clean;
+    if (p->draw_order == RTC_DRAW_ORDER_HOST) return xp ? rtc_wf_one_compat_host_x : rtc_wf_one_compat_host;
+    return xp ? rtc_wf_one_compat_dev_x : rtc_wf_one_compat_dev;
 }
 
 rtc_status run_wavefront(const DevScene& S, const rtc_render_params* p, const WfBuffers& B, uint32_t* d_status,
@@ -964,7 +989,7 @@ rtc_status run_wavefront(const DevScene& S, const rtc_render_params* p, const Wf
     DevParams P = dev_params(p);
     P.rgb8 = d_rgb8;   // quantised output written as each pixel finishes
     const bool clean = p->mode == RTC_MODE_CLEAN;
-    const WfOneFn fn = wf_one_fn(p);
+    const WfOneFn fn = wf_one_fn(p, S.num_xnodes != 0);
     WfOneArgs J;
     J.S = S;
     J.P = P;
@@ -1192,11 +1217,11 @@ rtc_status launch(rtc_context* c, const rtc_scene* s, const rtc_render_params* p
     DevParams P = dev_params(p);
     P.rgb8 = d_rgb8;
     const DevScene S = rtc_scene_view(s, p);
-    cudaError_t e =
-        p->mode == RTC_MODE_CLEAN ? rtc_launch_render_clean(S, P, d_out, d_counters, c->d_status, p->block_size, st)
-        : p->draw_order == RTC_DRAW_ORDER_HOST
-            ? rtc_launch_render_compat_host(S, P, d_out, d_counters, c->d_status, p->block_size, st)
-            : rtc_launch_render_compat_dev(S, P, d_out, d_counters, c->d_status, p->block_size, st);
+    const bool xp = S.num_xnodes != 0;
+    auto fn = p->mode == RTC_MODE_CLEAN ? (xp ? rtc_launch_render_clean_x : rtc_launch_render_clean)
+              : p->draw_order == RTC_DRAW_ORDER_HOST ? (xp ? rtc_launch_render_compat_host_x : rtc_launch_render_compat_host)
+                                                     : (xp ? rtc_launch_render_compat_dev_x : rtc_launch_render_compat_dev);
+    cudaError_t e = fn(S, P, d_out, d_counters, c->d_status, p->block_size, st);
     if (e != cudaSuccess) return cuda_fail(e, "render launch");
     return RTC_OK;
 }
@@ -1302,7 +1327,9 @@ extern "C" rtc_status rtc_trace_closest_ex(rtc_context* c, const rtc_scene* s, c
         if (e == cudaSuccess) e = cudaMemsetAsync(c->d_status, 0, 4, c->stream);
         rtc_render_params vp{};
         vp.flags = flags;
-        if (e == cudaSuccess) e = rtc_launch_trace_closest(rtc_scene_view(s, &vp), d_rays, n, depth, max_depth, d_prim, d_t, c->d_status, c->stream);
+        const DevScene SV = rtc_scene_view(s, &vp);
+        auto tfn = SV.num_xnodes ? rtc_launch_trace_closest_x : rtc_launch_trace_closest;
+        if (e == cudaSuccess) e = tfn(SV, d_rays, n, depth, max_depth, d_prim, d_t, c->d_status, c->stream);
         if (e == cudaSuccess && prim) e = cudaMemcpyAsync(prim, d_prim, (size_t)n * 4, cudaMemcpyDeviceToHost, c->stream);
         if (e == cudaSuccess && t) e = cudaMemcpyAsync(t, d_t, (size_t)n * 4, cudaMemcpyDeviceToHost, c->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);

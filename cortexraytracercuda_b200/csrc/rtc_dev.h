@@ -16,6 +16,7 @@
 //   items      uint32 per leaf entry, leaf order: (kind << 29) | index into that kind's array.
 //   xprim      int4 per transformed primitive or box face (leaf order): (transform or -1, inner kind,
 //              inner index, global id).  The inner record sits in the sph / quad / tri / rect array.
+//              Xprims have their own BVH2 (`xnodes`, leaves into `xitems`), walked after the main one.
 //   xf         8 x float4 per transform: (translate.xyz, flags) (scale.xyz, -) (inverse rotation columns
 //              0..2, xyz) (forward rotation columns 0..2, xyz), the glm matrices of rt::rotate
 //   rect       2 x float4 per box face: (a0, a1, b0, b1) (k, axis, flip, material); axis 0 = xy_rect
@@ -40,6 +41,17 @@
 
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+// Kernels that walk the xprim BVH (transformed primitives and box faces) are compiled separately, with
+// RTC_XP=1, into the inline namespace rtc::xp1; without them the traversal carries none of that code.
+#ifndef RTC_XP
+#define RTC_XP 0
+#endif
+#if RTC_XP
+#define RTC_XP_NS xp1
+#else
+#define RTC_XP_NS xp0
+#endif
 
 namespace rtc {
 
@@ -105,6 +117,8 @@ struct DevScene {
     const int4* xprim;
     const float4* xf;
     const float4* rect;
+    const float4* xnodes;      // BVH2 over the xprims (null when there are none)
+    const uint32_t* xitems;
     uint32_t num_nodes;
     uint32_t num_nodes8;
     uint32_t num_items;
@@ -113,7 +127,7 @@ struct DevScene {
     uint32_t num_textures;
     uint32_t num_images;
     uint32_t num_sph, num_tri, num_quad;
-    uint32_t num_xprim, num_xf, num_rect;
+    uint32_t num_xprim, num_xf, num_rect, num_xnodes, num_xitems;
     DevCamera cam;
     DevBackground bg;
 };

@@ -49,8 +49,9 @@ rtc_status Engine::init(const EngineConfig& cfg, cudaStream_t st) {
         return rtc_set_error(RTC_ERR_INVALID_ARGUMENT, "slot count must be in 1..2^24");
     cfg_ = cfg;
     st_ = st;
-    if (cfg.mode == RTC_MODE_CLEAN) fn_ = rtc_wf_table_clean;
-    else fn_ = cfg.draw_order == RTC_DRAW_ORDER_HOST ? rtc_wf_table_compat_host : rtc_wf_table_compat_dev;
+    if (cfg.mode == RTC_MODE_CLEAN) { fn_ = rtc_wf_table_clean; fn_x_ = rtc_wf_table_clean_x; }
+    else if (cfg.draw_order == RTC_DRAW_ORDER_HOST) { fn_ = rtc_wf_table_compat_host; fn_x_ = rtc_wf_table_compat_host_x; }
+    else { fn_ = rtc_wf_table_compat_dev; fn_x_ = rtc_wf_table_compat_dev_x; }
     drain_ = cfg.drain ? cfg.drain : (uint32_t)cfg.num_sms * 512u;
     device_bytes_ = (size_t)cfg.slots * rtc_wf_slot_bytes() + 16 * 256 + (size_t)cfg.ring * sizeof(DevJob) +
                     sizeof(WfFeed) + (size_t)cfg.ring * sizeof(uint32_t) + 256;
@@ -90,6 +91,10 @@ rtc_status Engine::reset() {
 
 rtc_status Engine::admit(DevJob job, uint64_t tag, uint64_t* seq) {
     if (ring_free() == 0) return rtc_set_error(RTC_ERR_BUSY, "job ring is full");
+    if (job.S.num_xnodes && fn_ != fn_x_) {   // from now on the kernels that also walk xprim BVHs
+        fn_ = fn_x_;
+        drop_graph();
+    }
     const uint64_t s = hi_++;
     const uint32_t slot = (uint32_t)(s & (cfg_.ring - 1));
     const uint64_t npix = (uint64_t)job.P.num_pixels;

@@ -104,6 +104,7 @@ private:
     EngineConfig cfg_;
     cudaStream_t st_ = nullptr;
     WfTableFn fn_ = nullptr;
+    WfTableFn fn_x_ = nullptr;   // the RTC_XP=1 kernels: taken once a job's scene has an xprim BVH
     void* d_wf_ = nullptr;          // slot state (carve_wavefront layout)
     WfBuffers B_{};
     DevJob* d_jobs_ = nullptr;

@@ -12,10 +12,15 @@
 
 #define RTC_FLAVOR_CAT2(a, b) a##b
 #define RTC_FLAVOR_CAT(a, b) RTC_FLAVOR_CAT2(a, b)
+#if RTC_XP
+#define RTC_XP_FN(name) RTC_FLAVOR_CAT(name, _x)
+#else
+#define RTC_XP_FN(name) name
+#endif
 #if defined(RTC_FLAVOR) && RTC_FLAVOR == 0
-#define RTC_FLAVOR_FN(name) RTC_FLAVOR_CAT(name, _dev)
+#define RTC_FLAVOR_FN(name) RTC_XP_FN(RTC_FLAVOR_CAT(name, _dev))
 #elif defined(RTC_FLAVOR)
-#define RTC_FLAVOR_FN(name) RTC_FLAVOR_CAT(name, _host)
+#define RTC_FLAVOR_FN(name) RTC_XP_FN(RTC_FLAVOR_CAT(name, _host))
 #endif
 
 namespace rtc {
@@ -50,13 +55,21 @@ using WfTableFn = cudaError_t (*)(WfOp, const WfTableArgs&, const WfBuffers&, co
 
 RTC_DECLARE_COMPAT(_dev)
 RTC_DECLARE_COMPAT(_host)
+// `_x`: the variants built with RTC_XP=1, for scenes with transformed primitives or boxes
+RTC_DECLARE_COMPAT(_dev_x)
+RTC_DECLARE_COMPAT(_host_x)
 
-cudaError_t rtc_launch_render_clean(const rtc::DevScene& S, const rtc::DevParams& P, float4* out,
-                                    unsigned long long* counters, uint32_t* status, int block, cudaStream_t st);
-cudaError_t rtc_launch_trace_closest(const rtc::DevScene& S, const float* rays, uint32_t n, int depth,
-                                     int max_depth, int32_t* prim, float* t, uint32_t* status, cudaStream_t st);
-
-
-// clean-mode wavefront (wavefront_clean.cu)
-cudaError_t rtc_wf_one_clean(rtc::WfOp op, const rtc::WfOneArgs& a, const rtc::WfBuffers& B, const rtc::WfLaunch& L);
-cudaError_t rtc_wf_table_clean(rtc::WfOp op, const rtc::WfTableArgs& a, const rtc::WfBuffers& B, const rtc::WfLaunch& L);
+// clean mode (render_clean.cu, wavefront_clean.cu) and closest-hit queries (render_compat.cu)
+#define RTC_DECLARE_CLEAN(sfx)                                                                                      \
+    cudaError_t rtc_launch_render_clean##sfx(const rtc::DevScene& S, const rtc::DevParams& P, float4* out,         \
+                                             unsigned long long* counters, uint32_t* status, int block,             \
+                                             cudaStream_t st);                                                      \
+    cudaError_t rtc_launch_trace_closest##sfx(const rtc::DevScene& S, const float* rays, uint32_t n, int depth,    \
+                                              int max_depth, int32_t* prim, float* t, uint32_t* status,            \
+                                              cudaStream_t st);                                                     \
+    cudaError_t rtc_wf_one_clean##sfx(rtc::WfOp op, const rtc::WfOneArgs& a, const rtc::WfBuffers& B,             \
+                                      const rtc::WfLaunch& L);                                                      \
+    cudaError_t rtc_wf_table_clean##sfx(rtc::WfOp op, const rtc::WfTableArgs& a, const rtc::WfBuffers& B,         \
+                                        const rtc::WfLaunch& L);
+RTC_DECLARE_CLEAN()
+RTC_DECLARE_CLEAN(_x)

@@ -9,6 +9,7 @@
 #include "rtc_trace.cuh"
 
 namespace rtc {
+inline namespace RTC_XP_NS {
 
 // Multi-draw expressions: the reference builds vectors from several get_real() calls inside one
 // constructor call or overloaded-operator expression, whose evaluation order C++ leaves open.
@@ -352,4 +353,5 @@ __device__ __forceinline__ RGB trace_sample(const DevScene& S, Ray r, int max_de
     return result;
 }
 
+}  // namespace RTC_XP_NS
 }  // namespace rtc

@@ -11,6 +11,7 @@
 #include "rtc_math.cuh"
 
 namespace rtc {
+inline namespace RTC_XP_NS {
 
 // ------------------------------------------------------------------------------------------------
 // random numbers
@@ -286,17 +287,19 @@ __device__ __forceinline__ bool rect_t(float4 r0, float4 r1, V3 o, V3 d, float t
 }
 
 // Tests every item of one leaf against [tmin, best_t].  EXACT: clean mode's double-precision sphere test.
-// Transformed primitives and box faces (xprims) of a leaf, tested after its other items on the
-// object-space ray.  Kept out of test_leaf's main loop so that scenes without them keep that loop's
-// registers.
+// A leaf of the xprim BVH: transformed primitives and box faces, each tested on its object-space ray.
 template <bool EXACT>
-__device__ __forceinline__ void test_leaf_xprims(const DevScene& S, uint32_t first, uint32_t cnt, V3 o, V3 d,
-                                                 float tmin, float& best_t, uint32_t& best_item, uint32_t& status) {
+__device__ __forceinline__ void test_leaf_xprims(const DevScene& S, int32_t child, V3 o, V3 d, float tmin,
+                                                 float& best_t, uint32_t& best_item, TraceStats& st,
+                                                 uint32_t& status) {
+    const uint32_t enc = (uint32_t)(~child);
+    const uint32_t first = enc >> LEAF_COUNT_BITS, cnt = enc & MAX_LEAF;
+    if (first + cnt > S.num_xitems) { status |= STATUS_BAD_ITEM; return; }
     for (uint32_t k = 0; k < cnt; ++k) {
-        const uint32_t it = ld_scene(S.items + first + k);
+        const uint32_t it = ld_scene(S.xitems + first + k);
         const uint32_t idx = it & ITEM_INDEX_MASK;
-        if ((it >> ITEM_KIND_SHIFT) != ITEM_XPRIM) continue;
-        if (idx >= S.num_xprim) { status |= STATUS_BAD_ITEM; continue; }
+        st.prims++;
+        if ((it >> ITEM_KIND_SHIFT) != ITEM_XPRIM || idx >= S.num_xprim) { status |= STATUS_BAD_ITEM; continue; }
         const int4 x = __ldg(S.xprim + idx);
         V3 ro = o, rd = d;
         if (x.x >= 0) {
@@ -345,7 +348,6 @@ __device__ __forceinline__ void test_leaf(const DevScene& S, int32_t child, V3 o
     uint32_t enc = (uint32_t)(~child);
     uint32_t first = enc >> LEAF_COUNT_BITS, cnt = enc & MAX_LEAF;
     if (first + cnt > S.num_items) { status |= STATUS_BAD_ITEM; return; }
-    bool xprims = false;
     for (uint32_t k = 0; k < cnt; ++k) {
         uint32_t it = ld_scene(S.items + first + k);
         uint32_t kind = it >> ITEM_KIND_SHIFT, idx = it & ITEM_INDEX_MASK;
@@ -392,11 +394,9 @@ __device__ __forceinline__ void test_leaf(const DevScene& S, int32_t child, V3 o
             // (directional_light.cuh:106, omni_light.cuh:76-80)
             if (hitl && !(q3.w != 0.0f && hide_invisible)) { best_t = t; best_item = it; }
         } break;
-        case ITEM_XPRIM: xprims = true; break;
         default: status |= STATUS_BAD_ITEM; break;
         }
     }
-    if (xprims) test_leaf_xprims<EXACT>(S, first, cnt, o, d, tmin, best_t, best_item, status);
 }
 
 // Direction component for the slab tests' reciprocal.  The slab distance is fma(lo, 1/d, -o/d); with a
@@ -513,6 +513,44 @@ __device__ __forceinline__ bool closest_hit8(const DevScene& S, V3 o, V3 d, V3 i
     return best_item != 0xffffffffu;
 }
 
+// The xprim BVH (binary, `xnodes` / `xitems`) against [tmin, best_t]: updates best_t / best_item and
+// returns whether any hit is held.  Same node layout and walk as the binary traversal below.
+template <bool EXACT>
+__device__ __forceinline__ bool closest_hit_xprims(const DevScene& S, V3 o, V3 d, V3 inv, V3 oi, float tmin,
+                                                float& best_t, uint32_t& best_item, TraceStats& st,
+                                                uint32_t& status) {
+    int32_t stack[TRAVERSAL_STACK];
+    int sp = 0;
+    int32_t node = 0;
+    for (;;) {
+        const float4* np = S.xnodes + 4 * (size_t)node;
+        float4 n0 = ld_scene(np), n1 = ld_scene(np + 1), n2 = ld_scene(np + 2), n3 = ld_scene(np + 3);
+        st.nodes++;
+        int32_t cl = __float_as_int(n3.x), cr = __float_as_int(n3.y);
+        float tl, tr;
+        bool hr;
+        bool hl = slab2(n0, n1, n2, inv, oi, tmin, best_t, tl, tr, hr);
+        if (hl && cl < 0) { test_leaf_xprims<EXACT>(S, cl, o, d, tmin, best_t, best_item, st, status); hl = false; }
+        if (hr && cr < 0) { test_leaf_xprims<EXACT>(S, cr, o, d, tmin, best_t, best_item, st, status); hr = false; }
+        if (hl && hr) {
+            int32_t nearc = tl <= tr ? cl : cr;
+            int32_t farc = tl <= tr ? cr : cl;
+            if (sp >= TRAVERSAL_STACK) { status |= STATUS_STACK_OVERFLOW; break; }
+            stack[sp++] = farc;
+            node = nearc;
+        } else if (hl) {
+            node = cl;
+        } else if (hr) {
+            node = cr;
+        } else {
+            if (sp == 0) break;
+            node = stack[--sp];
+        }
+        if ((uint32_t)node >= S.num_xnodes) { status |= STATUS_BAD_ITEM; break; }
+    }
+    return best_item != 0xffffffffu;
+}
+
 // Closest hit in [tmin, tmax] over the whole scene (the reference's world.hit through the BVH).
 // EXACT: clean mode (double-precision sphere test).  WIDE: walk the 8-wide nodes when the scene
 // carries them (only the extend kernel is built with it, so the other kernels carry no code for it).
@@ -532,7 +570,11 @@ __device__ __forceinline__ bool closest_hit(const DevScene& S, V3 o, V3 d, float
     if constexpr (WIDE) {
         if (S.nodes8) {
             V3 oi8 = v3(o.x * inv.x, o.y * inv.y, o.z * inv.z);
-            return closest_hit8<EXACT>(S, o, d, inv, oi8, tmin, tmax, hide_invisible, t_out, item_out, st, status);
+            bool h = closest_hit8<EXACT>(S, o, d, inv, oi8, tmin, tmax, hide_invisible, t_out, item_out, st, status);
+#if RTC_XP
+            if (S.num_xnodes) h = closest_hit_xprims<EXACT>(S, o, d, inv, oi8, tmin, t_out, item_out, st, status);
+#endif
+            return h;
         }
     }
     V3 oi = v3(o.x * inv.x, o.y * inv.y, o.z * inv.z);
@@ -542,6 +584,9 @@ __device__ __forceinline__ bool closest_hit(const DevScene& S, V3 o, V3 d, float
     int sp = 0;
     int32_t node = 0;
     for (;;) {
+#if RTC_XP
+        if (S.num_nodes == 0) break;   // every primitive is transformed (xprim BVH only)
+#endif
         const float4* np = S.nodes + 4 * (size_t)node;
         float4 n0 = ld_scene(np), n1 = ld_scene(np + 1), n2 = ld_scene(np + 2), n3 = ld_scene(np + 3);
         st.nodes++;
@@ -569,6 +614,11 @@ __device__ __forceinline__ bool closest_hit(const DevScene& S, V3 o, V3 d, float
     }
     t_out = best_t;
     item_out = best_item;
+    // transformed primitives and box faces live in their own BVH, walked after the first one against the
+    // best hit so far; scenes without them skip it (and their traversal loop carries none of its registers)
+#if RTC_XP
+    if (S.num_xnodes) return closest_hit_xprims<EXACT>(S, o, d, inv, oi, tmin, t_out, item_out, st, status);
+#endif
     return best_item != 0xffffffffu;
 }
 
@@ -812,4 +862,5 @@ __device__ __forceinline__ void quantize_pixel(float4 c, int spp, int width, int
     }
 }
 
+}  // namespace RTC_XP_NS
 }  // namespace rtc

@@ -47,6 +47,7 @@
 #include "rtc_path.cuh"
 
 namespace rtc {
+inline namespace RTC_XP_NS {
 
 // Appends `slot` to queue `q` when `pred`; every active lane of the warp must call it together.
 __device__ __forceinline__ void wf_push(uint32_t* q, uint32_t* cnt, uint32_t slot, bool pred) {
@@ -639,4 +640,5 @@ cudaError_t wf_dispatch(WfOp op, const A& args, const WfBuffers& B, const WfLaun
     return cudaGetLastError();
 }
 
+}  // namespace RTC_XP_NS
 }  // namespace rtc
