@@ -749,7 +749,8 @@ rtc_status read_file(rtc_scene_file& F, const char* path, uint32_t flags, rtc_im
         rtc_free_obj(&m);
         return true;
     };
-    F.desc = rtc_adapter::from_sceneconfig(C, F.holder, load_image ? rtc_adapter::ImageLoader(img) : nullptr, obj);
+    F.desc = rtc_adapter::from_sceneconfig(C, F.holder, load_image ? rtc_adapter::ImageLoader(img) : nullptr, obj,
+                                           (flags & RTC_SCENE_FILE_REFERENCE_MESHES) ? rtc_adapter::REFERENCE_MESHES : 0u);
     for (const auto& s : F.holder.skipped) F.skipped.push_back(s);
     F.info.num_skipped = (uint32_t)F.skipped.size();
     return RTC_OK;

@@ -476,6 +476,7 @@ def load_obj(path):
 
 # ---- the reference's .scene files ------------------------------------------------------------------
 SCENE_FILE_REFERENCE_CAPACITY = 1   # the reference's table capacities (list length mod 256; glass sized from `dielectric`)
+SCENE_FILE_REFERENCE_MESHES = 2     # the reference's OBJ meshes (meshes[0]'s file for every entry, no position or transform)
 
 
 class rtc_scene_file_info(C.Structure):

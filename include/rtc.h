@@ -281,6 +281,11 @@ typedef uint8_t* (*rtc_image_loader)(const char* path, int* width, int* height, 
  * materials, and the objects using them, are dropped unless a `dielectric` list makes room.  By default
  * every entry is kept; this flag reproduces the reference. */
 #define RTC_SCENE_FILE_REFERENCE_CAPACITY 1
+/* The reference's OBJ meshes.  load_scene renders the first meshes entry's file (meshes[0]) for every
+ * entry (gpu.cu:626-631), each with its own material, and createObjMesh drops the entry's position and
+ * transform (scene_factory.cuh:373-385).  By default each entry renders its own file, offset by its
+ * position and transformed; this flag reproduces the reference. */
+#define RTC_SCENE_FILE_REFERENCE_MESHES 2
 typedef struct rtc_scene_file_info {
     int32_t width, height;     /* image.width / image.height (scene_builder's 400 x 225 when absent)  */
     int32_t spp, max_depth;    /* image.samplesPerPixel / image.maxDepth (50 / 100 when absent)      */

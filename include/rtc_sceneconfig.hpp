@@ -14,7 +14,8 @@
 // Lights map to omni, directional and spot lights in the light list's order.  Spheres, quads and boxes
 // keep their rt::transform as scene_factory::applyTransform applies it; OBJ meshes take their
 // `position` as a vertex offset and their transform too, where the reference's createObjMesh drops both
-// (scene_factory.cuh createObjMesh) and renders meshes[0] for every entry (gpu.cu:628).  Primitives the
+// (scene_factory.cuh createObjMesh) and renders meshes[0] for every entry (gpu.cu:628); the flag
+// REFERENCE_MESHES reproduces the reference there.  Primitives the
 // B200 path does not cover (planes, cones, cylinders, disks, tori, volumes) are reported in `skipped`.
 // Image textures need decoded RGB8 pixels: pass `load_image(filepath, &w, &h)` returning a pointer
 // that stays valid while the description is used (the reference decodes with stbi_load, gpu.cu:1743).
@@ -109,10 +110,16 @@ template <class T> uint32_t add_transform(const T& trs, SceneHolder& out) {
 }
 }  // namespace detail
 
+// from_sceneconfig flag: OBJ meshes as the reference's load_scene adds them.  Every objMeshes entry
+// renders the first entry's file, meshes[0] (gpu.cu:626-631), with its own material and smoothing, and
+// without its position or transform, which createObjMesh drops (scene_factory.cuh:373-385).  By default
+// each entry renders its own file, offset by its position and transformed.
+constexpr uint32_t REFERENCE_MESHES = 1u;
+
 // Converts `cfg` (a reference sceneConfig) into `out`; returns out.finish().
 template <class SceneConfig>
 const rtc_scene_desc* from_sceneconfig(const SceneConfig& cfg, SceneHolder& out, const ImageLoader& load_image = nullptr,
-                                       const ObjLoader& load_obj = nullptr) {
+                                       const ObjLoader& load_obj = nullptr, uint32_t flags = 0) {
     using namespace detail;
     const auto& T = cfg.texturesCfg;
     const auto& M = cfg.materialsCfg;
@@ -269,19 +276,22 @@ const rtc_scene_desc* from_sceneconfig(const SceneConfig& cfg, SceneHolder& out,
     // OBJ meshes (load_scene adds them after the boxes, gpu.cu:612-635): geometry offset by `position`,
     // then the mesh's transform; one material for the whole mesh (use_mtl materials are reported)
     const auto& MS = cfg.meshesCfg;
+    const bool ref_meshes = (flags & REFERENCE_MESHES) != 0;
     for (int i = 0; i < MS.objMeshCount; ++i) {
         const auto& m = MS.objMeshes[i];
-        if (!load_obj) { out.skipped.push_back(std::string("OBJ mesh without loader: ") + (m.filepath ? m.filepath : "")); continue; }
+        // with REFERENCE_MESHES the geometry is always meshes[0]'s file, placed as it is in the file
+        const auto& g = ref_meshes ? MS.objMeshes[0] : m;
+        if (!load_obj) { out.skipped.push_back(std::string("OBJ mesh without loader: ") + (g.filepath ? g.filepath : "")); continue; }
         const int mat = fetch_material(m.materialName);
         if (mat < 0) continue;
         std::vector<float> v, n;
         std::vector<uint32_t> idx;
-        if (!m.filepath || !load_obj(m.filepath, v, idx, n) || idx.empty()) {
-            out.skipped.push_back(std::string("OBJ mesh not loaded: ") + (m.filepath ? m.filepath : ""));
+        if (!g.filepath || !load_obj(g.filepath, v, idx, n) || idx.empty()) {
+            out.skipped.push_back(std::string("OBJ mesh not loaded: ") + (g.filepath ? g.filepath : ""));
             continue;
         }
-        float off[3];
-        put3(off, m.position);
+        float off[3] = {0.f, 0.f, 0.f};
+        if (!ref_meshes) put3(off, m.position);
         for (size_t k = 0; k < v.size(); k += 3) {
             v[k] += off[0];
             v[k + 1] += off[1];
@@ -297,7 +307,7 @@ const rtc_scene_desc* from_sceneconfig(const SceneConfig& cfg, SceneHolder& out,
         out.mesh_indices.push_back(std::move(idx));
         out.mesh_normals.push_back(r.smooth ? std::move(n) : std::vector<float>());
         out.meshes.push_back(r);
-        out.mesh_transforms.push_back(add_transform(m.transform, out));
+        out.mesh_transforms.push_back(ref_meshes ? 0u : add_transform(m.transform, out));
     }
 
     const auto& C = cfg.cameraCfg;

@@ -17,7 +17,7 @@ import numpy as np
 import pytest
 
 from cortexraytracercuda_b200._lib import RtcError
-from cortexraytracercuda_b200.scene import (DRAW_ORDER_HOST, MAT_DIELECTRIC, MAT_LAMBERTIAN, MAT_METAL, SCENE_FILE_REFERENCE_CAPACITY,
+from cortexraytracercuda_b200.scene import (DRAW_ORDER_HOST, MAT_DIELECTRIC, MAT_LAMBERTIAN, MAT_METAL, SCENE_FILE_REFERENCE_CAPACITY, SCENE_FILE_REFERENCE_MESHES,
                                             TEX_CHECKER, TEX_IMAGE, TEX_SOLID, SceneFile, decode_png)
 
 SCENE = r'''
@@ -400,6 +400,45 @@ meshes: { obj: ( { filepath = "tri.obj"; material = "grey"; },
     f = SceneFile(tmp_path / "m.scene")
     assert f.desc.num_meshes == 1 and f.desc.meshes[0].smooth == 1     # use_smoothing defaults to true
     assert any("obj file not found" in s for s in f.skipped)
+
+
+QUAD_OBJ = """v 0 0 0
+v 2 0 0
+v 2 2 0
+v 0 2 0
+f 1 2 3 4
+"""
+
+
+def test_reference_meshes_flag(tmp_path):
+    """RTC_SCENE_FILE_REFERENCE_MESHES: every entry renders meshes[0]'s file (gpu.cu:626-631) with its own
+    material, without its position or transform (scene_factory.cuh:373-385)."""
+    (tmp_path / "tri.obj").write_text(OBJ)
+    (tmp_path / "quad.obj").write_text(QUAD_OBJ)
+    (tmp_path / "m.scene").write_text('''
+materials: { lambertian: ( { name = "grey"; color = { r = 0.5; g = 0.5; b = 0.5; }; },
+                           { name = "red"; color = { r = 0.9; g = 0.1; b = 0.1; }; } ); };
+meshes: { obj: ( { filepath = "tri.obj"; material = "grey"; position = { x = 0.0; y = 3.0; z = 0.0; }; },
+                 { filepath = "quad.obj"; material = "red"; use_smoothing = false;
+                   position = { x = 1.0; y = 0.0; z = 0.0; };
+                   transform = { rotate = { x = 0.0; y = 45.0; z = 0.0; }; }; } ); };
+''')
+    tri = np.array([0, 0, 0, 1, 0, 0, 0, 1, 0], np.float32)
+    own = SceneFile(tmp_path / "m.scene")
+    d = own.desc
+    assert d.num_meshes == 2 and d.meshes[1].num_triangles == 2
+    assert np.array_equal(_arr(d.meshes[0].vertices, 9), tri + np.tile(np.float32([0, 3, 0]), 3))
+    assert d.mesh_transforms[1] != 0
+    ref = SceneFile(tmp_path / "m.scene", flags=SCENE_FILE_REFERENCE_MESHES)
+    r = ref.desc
+    assert r.num_meshes == 2
+    for i in range(2):
+        assert r.meshes[i].num_triangles == 1 and r.meshes[i].num_vertices == 3
+        assert np.array_equal(_arr(r.meshes[i].vertices, 9), tri)
+        assert not r.mesh_transforms or r.mesh_transforms[i] == 0
+    assert (r.meshes[0].smooth, r.meshes[1].smooth) == (1, 0)
+    assert r.meshes[0].material != r.meshes[1].material
+    assert [r.textures[r.materials[r.meshes[i].material].texture].color[0] for i in range(2)] == pytest.approx([0.5, 0.9])
 
 
 REFUSED = [
