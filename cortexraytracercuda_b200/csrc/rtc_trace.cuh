@@ -737,6 +737,11 @@ __device__ __forceinline__ void finalize_hit(const DevScene& S, uint32_t it, flo
     const uint32_t kind = it >> ITEM_KIND_SHIFT, idx = it & ITEM_INDEX_MASK;
     h.t = t;
     h.item = it;
+#if !RTC_XP
+    // only the RTC_XP=1 kernels walk the xprim BVH, so an item here is always a plain primitive; keeping
+    // the xprim branch out of these kernels keeps its registers out of the shade kernel
+    finalize_prim<FLOAT_TRIG>(S, kind, idx, t, o, d, h);
+#else
     if (kind != ITEM_XPRIM) {
         finalize_prim<FLOAT_TRIG>(S, kind, idx, t, o, d, h);
         return;
@@ -747,6 +752,7 @@ __device__ __forceinline__ void finalize_hit(const DevScene& S, uint32_t it, flo
     if (x.y == XPRIM_RECT) finalize_rect(S, (uint32_t)x.z, t, o, d, h);
     else finalize_prim<FLOAT_TRIG>(S, (uint32_t)x.y, (uint32_t)x.z, t, o, d, h);
     if (x.x >= 0) xf_to_world(S, x.x, h.p, h.n);
+#endif
 }
 
 // ------------------------------------------------------------------------------------------------
