@@ -79,9 +79,14 @@ def workload(name):
     return scene, params
 
 
+# what each measured scene adds to its BASELINE configuration, named in the bench line
+ADDED = {"spheres": " + hidden quad light of random_spheres.scene (the config names none)",
+         "meshes": " + hidden 8x4 quad light (the config names none)", "cornell": ""}
+
+
 def describe(name, params, scene):
     return {"workload": f"{name} {params.width}x{params.height} spp{params.spp} (traced {params.traced_spp}) "
-                        f"depth{params.max_depth}",
+                        f"depth{params.max_depth}{ADDED.get(name, '')}",
             "primitives": scene.num_primitives, "mode": "compat (reference RNG stream and quirks)",
             "l2": "flushed between steps (256 MiB write)", "seed": configs.DEFAULT_SEED}
 
@@ -578,6 +583,11 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.gpus != world:
+        # one process per GPU: --gpus N is launched by torchrun with N ranks; a mismatch would time and
+        # report a different number of replicas than asked for
+        sys.exit(f"bench.py: --gpus {args.gpus} but WORLD_SIZE={world}; launch N>1 with "
+                 f"python -m torch.distributed.run --nproc-per-node {args.gpus} bench.py --gpus {args.gpus}")
 
     if args.impl == "reference":
         run_reference_arm(args, rank, world)

@@ -18,7 +18,8 @@ sizes and value distributions follow the workloads the library is measured on:
                      noise of amplitude 0.15, four instances (metal, dielectric, lambertian, lambertian
                      checker) = 1,310,720 triangles; a checker ground quad with a 10-unit period; a
                      2048x1024 FP32 equirectangular environment map (sky gradient + Gaussian sun lobe);
-                     1920x1080, 128 spp, depth 16.
+                     1920x1080, 128 spp, depth 16; plus a hidden 8x4 quad light above the instances, for the
+                     same reason as in ``spheres``.
 * ``textured``     - spheres and quads with checker and image textures (parity of the texture paths).
 * batched workload (:func:`batch_workload`) - 64 heterogeneous scenes drawn from the seed: triangle
                      counts log-uniform in [1K, 500K] (instances of one displaced icosphere level) plus
@@ -296,8 +297,13 @@ def spheres_params(**kw) -> RenderParams:
     return RenderParams(**p)
 
 
-def meshes(level=7, seed=DEFAULT_SEED, env_size=(2048, 1024)) -> Scene:
+def meshes(level=7, seed=DEFAULT_SEED, env_size=(2048, 1024), light=True) -> Scene:
     s = Scene(name="meshes")
+    if light:
+        # a hidden quad light above the instances, so the lambertian mixture PDF has a light to sample
+        # (with an empty light list the reference's mixture PDF gives NaN / zero-direction bounces,
+        # hittable_list.cuh:191-215, which would cut half the diffuse paths short)
+        s.dir_light((0.0, 8.0, 1.0), (8.0, 0.0, 0.0), (0.0, 0.0, 4.0), (4.0, 4.0, 4.0), intensity=1.0, invisible=True)
     v, f = displaced_icosphere(level, 0.15, seed)
     mats = [s.metal((0.8, 0.85, 0.9), 0.05), s.dielectric(1.5), s.lambertian((0.7, 0.3, 0.2)),
             s.lambertian(s.checker_colors(0.25, (0.9, 0.9, 0.9), (0.1, 0.3, 0.6)))]

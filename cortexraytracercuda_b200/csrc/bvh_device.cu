@@ -35,6 +35,7 @@
 
 #include "bvh_build.h"
 #include "rtc_dev.h"
+#include "rtc_internal.h"
 
 namespace rtc {
 namespace {
@@ -388,7 +389,8 @@ int build_bvh_device(const BvhInput& in, int device, BvhDeviceMethod method, Bvh
 
     // Own non-blocking stream and stream-ordered allocations: a build never waits for (or stalls) work
     // that other threads have in flight on the device.
-    cudaError_t e = cudaSetDevice(device);
+    RtcDeviceScope dev(device);
+    cudaError_t e = dev.error();
     cudaStream_t st = nullptr;
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
     if (e != cudaSuccess) {

@@ -19,7 +19,11 @@
 //     call, the rest is fully rewritten; calls that overlap on the GPU (two streams, two threads)
 //     race on it;
 //   * the call returns when the frame is complete: it polls the queue counter with synchronous
-//     copies into a host variable (no pinned memory, no events).
+//     copies into a host variable (no pinned memory, no events); a call that fails part-way waits
+//     for its queued kernels before it returns;
+//   * it always runs the wavefront kernels, untimed: params->engine and RTC_FLAG_KERNEL_TIMING are
+//     ignored;
+//   * the caller's current device is the same after the call as before it.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -72,7 +76,8 @@ extern "C" rtc_status rtc_render_noalloc(const rtc_scene* scene, const rtc_rende
         return rtc_set_error(RTC_ERR_INVALID_ARGUMENT, m.c_str());
     }
     const int device = rtc_scene_device(scene);
-    cudaError_t e = cudaSetDevice(device);
+    RtcDeviceScope dev(device);   // the caller's current device is restored on return
+    cudaError_t e = dev.error();
     if (e != cudaSuccess) return rtc_set_error(RTC_ERR_CUDA, cudaGetErrorString(e));
     void* base = nullptr;
     r = scratch_address(device, &base);
@@ -86,7 +91,12 @@ extern "C" rtc_status rtc_render_noalloc(const rtc_scene* scene, const rtc_rende
     e = cudaMemsetAsync(d_status, 0, sizeof(uint32_t), st);
     if (e != cudaSuccess) return rtc_set_error(RTC_ERR_CUDA, cudaGetErrorString(e));
     r = rtc_run_wavefront_sync(scene, params, B, d_status, (float4*)d_radiance_sum, st);
-    if (r != RTC_OK) return r;
+    if (r != RTC_OK) {
+        // kernels of this call may still be queued on the stream and use the shared array: wait for
+        // them, so no work of a failed call outlives it (the error recorded above is kept)
+        cudaStreamSynchronize(st);
+        return r;
+    }
     uint32_t status = 0;
     e = cudaMemcpyAsync(&status, d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);

@@ -62,7 +62,8 @@ extern "C" rtc_status rtc_context_create(int device, rtc_context** out) {
     cudaDeviceProp prop;
     RTC_CUDA(cudaGetDeviceProperties(&prop, device));
     if (prop.major < 10) return fail(RTC_ERR_NO_DEVICE, std::string("device is not sm_100: ") + prop.name);
-    RTC_CUDA(cudaSetDevice(device));
+    RtcDeviceScope dev(device);
+    RTC_CUDA(dev.error());
     rtc_context* c = new (std::nothrow) rtc_context();
     if (!c) return fail(RTC_ERR_OOM, "host allocation failed");
     c->device = device;
@@ -81,7 +82,7 @@ extern "C" rtc_status rtc_context_create(int device, rtc_context** out) {
 
 extern "C" rtc_status rtc_context_destroy(rtc_context* c) {
     if (!c) return RTC_OK;
-    cudaSetDevice(c->device);
+    RtcDeviceScope dev(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     c->engine.reset();
     cudaFree(c->d_status);
@@ -799,7 +800,7 @@ extern "C" rtc_status rtc_scene_create_ex(rtc_context* ctx, const rtc_scene_desc
     if (!s) return fail(RTC_ERR_OOM, "host allocation failed");
     s->ctx = ctx;
     s->device = ctx->device;
-    cudaSetDevice(ctx->device);
+    RtcDeviceScope dev(ctx->device);
     const size_t total = H.slab.size();
     cudaError_t e = cudaMalloc(&s->d_slab, total);
     if (e != cudaSuccess) { delete s; return cuda_fail(e, "cudaMalloc(scene)"); }
@@ -818,7 +819,7 @@ extern "C" rtc_status rtc_scene_destroy(rtc_scene* s) {
     // A scene may outlive its context: only its own device id is used here (cudaFree synchronises
     // with the device before releasing the memory).
     if (!s) return RTC_OK;
-    cudaSetDevice(s->device);
+    RtcDeviceScope dev(s->device);
     cudaFree(s->d_slab);
     delete s;
     return RTC_OK;
@@ -913,6 +914,17 @@ size_t carve_wavefront(void* base, uint32_t slots, WfBuffers& B) {
     B.slots = slots;
     return (size_t)(p - (uint8_t*)base);
 }
+
+// Bytes carve_wavefront lays out for `slots` slots (each buffer rounded up to 256 bytes).
+constexpr size_t wavefront_bytes(size_t n) {
+    return 7 * ((n * 16 + 255) & ~(size_t)255) + ((n * 8 + 255) & ~(size_t)255) + 3 * ((n * 4 + 255) & ~(size_t)255) +
+           ((WF_CTR_N * 4 + 255) & ~(size_t)255);
+}
+// The allocation-free render's advertised cap fits its 64 MiB array behind a 256-byte status header
+// (render_noalloc.cu), so an image at or under RTC_NOALLOC_MAX_PIXELS never fails for lack of room.
+static_assert(256 + wavefront_bytes(RTC_NOALLOC_MAX_PIXELS) <= (size_t(64) << 20),
+              "RTC_NOALLOC_MAX_PIXELS slots do not fit the allocation-free render's static array");
+static_assert(wavefront_bytes(1) <= WF_SLOT_BYTES + 12 * 256, "wavefront layout grew past WF_SLOT_BYTES");
 
 rtc_status ensure_wavefront(rtc_context* c, uint32_t slots, WfBuffers& B) {
     if (c->wf_cap < slots) {
@@ -1246,7 +1258,8 @@ extern "C" rtc_status rtc_render(rtc_context* c, const rtc_scene* s, const rtc_r
     rtc_status r = check_params(p);
     if (r != RTC_OK) return r;
     std::lock_guard<std::mutex> lk(c->mu);
-    RTC_CUDA(cudaSetDevice(c->device));
+    RtcDeviceScope dev(c->device);
+    RTC_CUDA(dev.error());
     const size_t npix = (size_t)p->width * p->height;
     if (c->out_cap < npix) {
         cudaFree(c->d_out);
@@ -1280,7 +1293,8 @@ extern "C" rtc_status rtc_render_device(rtc_context* c, const rtc_scene* s, cons
     rtc_status r = check_params(p);
     if (r != RTC_OK) return r;
     cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
-    RTC_CUDA(cudaSetDevice(c->device));
+    RtcDeviceScope dev(c->device);
+    RTC_CUDA(dev.error());
     return launch(c, s, p, (float4*)d_radiance_sum, d_counters, st, d_rgb8);
 }
 
@@ -1313,7 +1327,8 @@ extern "C" rtc_status rtc_trace_closest_ex(rtc_context* c, const rtc_scene* s, c
     if (!c || !s || (n && !rays)) return fail(RTC_ERR_INVALID_ARGUMENT, "null argument");
     if (n == 0) return RTC_OK;
     std::lock_guard<std::mutex> lk(c->mu);
-    RTC_CUDA(cudaSetDevice(c->device));
+    RtcDeviceScope dev(c->device);
+    RTC_CUDA(dev.error());
     float* d_rays = nullptr;
     int32_t* d_prim = nullptr;
     float* d_t = nullptr;

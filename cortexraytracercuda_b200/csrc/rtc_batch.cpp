@@ -85,7 +85,8 @@ extern "C" rtc_status rtc_render_batch(rtc_context* c, const rtc_job* jobs, uint
     if (cfg.ring != next_pow2(cfg.ring)) return rtc_set_error(RTC_ERR_INVALID_ARGUMENT, "ring must be a power of two");
 
     std::lock_guard<std::mutex> lk(c->mu);
-    cudaError_t e = cudaSetDevice(c->device);
+    RtcDeviceScope dev(c->device);
+    cudaError_t e = dev.error();
     if (e != cudaSuccess) return cuda_err(e, "cudaSetDevice");
     cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
     const EngineConfig* have = c->engine ? &c->engine->config() : nullptr;

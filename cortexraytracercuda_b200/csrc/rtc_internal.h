@@ -8,6 +8,31 @@
 #include "../../include/rtc.h"
 #include "rtc_dev.h"
 
+// Makes `device` current for the lifetime of the object and gives the calling thread back its own
+// current device afterwards: a public entry point works on the device of its context, scene or server
+// without changing which device the caller's later CUDA calls go to.
+class RtcDeviceScope {
+public:
+    explicit RtcDeviceScope(int device) {
+        if (cudaGetDevice(&prev_) != cudaSuccess) prev_ = -1;
+        if (prev_ != device) {
+            err_ = cudaSetDevice(device);
+            changed_ = err_ == cudaSuccess && prev_ >= 0;
+        }
+    }
+    ~RtcDeviceScope() {
+        if (changed_) cudaSetDevice(prev_);
+    }
+    RtcDeviceScope(const RtcDeviceScope&) = delete;
+    RtcDeviceScope& operator=(const RtcDeviceScope&) = delete;
+    cudaError_t error() const { return err_; }
+
+private:
+    int prev_ = -1;
+    bool changed_ = false;
+    cudaError_t err_ = cudaSuccess;
+};
+
 // bytes of wavefront scratch per path slot, and the layout of `slots` slots starting at `base`
 size_t rtc_wf_slot_bytes();
 size_t rtc_carve_wavefront(void* base, uint32_t slots, rtc::WfBuffers& B);

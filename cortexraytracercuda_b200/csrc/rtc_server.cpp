@@ -359,7 +359,8 @@ extern "C" rtc_status rtc_server_create(const rtc_server_config* cfg, rtc_server
     cudaDeviceProp prop;
     if (cudaGetDeviceProperties(&prop, cfg->device) != cudaSuccess) return rtc_set_error(RTC_ERR_CUDA, "cudaGetDeviceProperties");
     if (prop.major < 10) return rtc_set_error(RTC_ERR_NO_DEVICE, (std::string("device is not sm_100: ") + prop.name).c_str());
-    if (cudaSetDevice(cfg->device) != cudaSuccess) return rtc_set_error(RTC_ERR_CUDA, "cudaSetDevice");
+    RtcDeviceScope dev(cfg->device);
+    if (dev.error() != cudaSuccess) return rtc_set_error(RTC_ERR_CUDA, "cudaSetDevice");
     std::unique_ptr<rtc_server> s(new (std::nothrow) rtc_server());
     if (!s) return rtc_set_error(RTC_ERR_OOM, "host allocation failed");
     s->cfg = *cfg;
@@ -410,7 +411,7 @@ extern "C" rtc_status rtc_server_destroy(rtc_server* s) {
         s->cv_done.notify_all();
     }
     if (s->th.joinable()) s->th.join();
-    cudaSetDevice(s->cfg.device);
+    RtcDeviceScope dev(s->cfg.device);
     for (auto& e : s->scenes)
         if (e->d_slab) cudaFreeAsync(e->d_slab, s->st);
     for (auto& kv : s->reqs) {

@@ -464,7 +464,9 @@ rtc_status rtc_get_render_stats(rtc_context* ctx, rtc_render_stats* stats);
  * (width*height float4, frame-buffer order) come from the caller; `stream` may be NULL (legacy
  * stream).  The first call on a device looks up the array's address; make it before any stream
  * capture.  All calls share the array, so calls that overlap on the GPU race.  Returns when the frame
- * is complete. */
+ * is complete; a call that fails part-way first waits for its queued kernels.  It always runs the
+ * wavefront engine untimed (params->engine and RTC_FLAG_KERNEL_TIMING are ignored), and the calling
+ * thread's current device is unchanged on return. */
 #define RTC_NOALLOC_MAX_PIXELS 508376u
 rtc_status rtc_render_noalloc(const rtc_scene* scene, const rtc_render_params* params, float* d_radiance_sum,
                               void* stream);

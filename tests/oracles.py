@@ -10,6 +10,7 @@ at build time; the built files then travel with the repository).
 from __future__ import annotations
 
 import ctypes as C
+import os
 from pathlib import Path
 
 import numpy as np
@@ -17,6 +18,9 @@ import numpy as np
 from cortexraytracercuda_b200.scene import RenderParams, Scene, SceneDesc, SceneFile
 
 ORACLE = Path(__file__).resolve().parent.parent / "oracle"
+# the reference tree (flarive/CortexRaytracerCuda), used only to build the reference-based checkers:
+# RTC_REFERENCE, else a checkout named `reference` beside this repository
+REFERENCE = Path(os.environ.get("RTC_REFERENCE", str(ORACLE.parent.parent / "reference")))
 
 
 def _load(path: Path):

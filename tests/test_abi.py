@@ -42,6 +42,11 @@ def test_every_declared_symbol_is_exported(lib):
     assert set(declared_functions()) <= set(_lib.PROTOTYPES)
 
 
+def test_noalloc_cap_matches_header():
+    m = re.search(r"#define\s+RTC_NOALLOC_MAX_PIXELS\s+(\d+)u?", HEADER.read_text())
+    assert m and int(m.group(1)) == _lib.NOALLOC_MAX_PIXELS
+
+
 def test_struct_sizes_match_header(lib):
     # the ctypes mirror and the C layout agree on the sizes the ABI depends on
     assert C.sizeof(rtc_render_params) == 10 * 4

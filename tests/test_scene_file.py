@@ -16,6 +16,8 @@ from pathlib import Path
 import numpy as np
 import pytest
 
+import oracles
+
 from cortexraytracercuda_b200._lib import RtcError
 from cortexraytracercuda_b200.scene import (DRAW_ORDER_HOST, MAT_DIELECTRIC, MAT_LAMBERTIAN, MAT_METAL, SCENE_FILE_REFERENCE_CAPACITY, SCENE_FILE_REFERENCE_MESHES,
                                             TEX_CHECKER, TEX_IMAGE, TEX_SOLID, SceneFile, decode_png)
@@ -218,7 +220,7 @@ REF_EXE = ROOT / "oracle" / "_ref" / "scenefile_check"
 
 @pytest.fixture(scope="module")
 def ref_loader():
-    ref = os.environ.get("REF", "/root/reference")
+    ref = str(oracles.REFERENCE)
     if (Path(ref) / "core" / "src" / "scenes" / "scene_loader.cpp").exists():
         subprocess.run(["make", "-s", "-C", str(ROOT / "oracle"), "scenefile", f"REF={ref}"], check=True,
                        capture_output=True)
@@ -538,7 +540,7 @@ def test_reference_scene_files(ref_loader):
     """Every `.scene` file the reference ships (data/scenes), read by both readers from the reference's
     root directory: identical descriptions (its OBJ and image paths, written relative to a build
     directory, are missing on both sides from there)."""
-    ref = Path(os.environ.get("REF", "/root/reference"))
+    ref = oracles.REFERENCE
     files = sorted((ref / "data" / "scenes").glob("*.scene"))
     if not files:
         pytest.skip("the reference's scene files are not available")

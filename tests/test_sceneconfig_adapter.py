@@ -9,13 +9,15 @@ from pathlib import Path
 
 import pytest
 
+import oracles
+
 ROOT = Path(__file__).resolve().parent.parent
 EXE = ROOT / "oracle" / "_ref" / "sceneconfig_check"
 
 
 @pytest.fixture(scope="module")
 def desc():
-    ref = os.environ.get("REF", "/root/reference")
+    ref = str(oracles.REFERENCE)
     if not (Path(ref) / "core" / "src" / "scenes" / "scene_config.h").exists() and not EXE.exists():
         pytest.skip("reference tree not available to compile the adapter check")
     if Path(ref).exists():
