@@ -54,6 +54,8 @@ struct DDesc {
     unsigned char** img_data; int* img_w; int* img_h; int nimg;
     rtc_camera cam;
     rtc_background bg;
+    const float* env;          // environment map (RTC_BG_ENV_MAP), device copy
+    unsigned char* dummy_px;   // the 1x1 bitmap the background texture's base class holds
 };
 
 struct DWorld {
@@ -62,6 +64,40 @@ struct DWorld {
     hittable** objects;
     int n;
     char* names;   // names[k] = name storage of primitive k
+    image_texture* bg_tex;   // sky gradient / environment map behind the camera's background hook, or null
+};
+
+// Sky gradient or FP32 environment map behind the camera's background-texture hook
+// (camera::ray_color's `if (background_texture)` branch, core/src/cameras/camera.cuh:164-168, which calls
+// background_texture->value(u, v, unit_dir)); the device twin of ref_harness.cpp's background_tex.  The
+// reference's GPU path never sets the hook (gpu.cu:729-742), so these backgrounds are parity-unpinned and
+// their formulas are the library's; the hook, the loop around it and everything it multiplies are the
+// reference's own code.
+class refg_background : public image_texture {
+public:
+    __host__ __device__ refg_background(unsigned char* dummy, const rtc_background& bg, const float* env)
+        : image_texture(bitmap_image(dummy, 1, 1, 3)), m_bg(bg), m_env(env) {}
+    __host__ __device__ color value(float, float, const point3& p) const override {
+        if (m_bg.kind == RTC_BG_SKY_GRADIENT) {
+            float a = 0.5f * (p.y + 1.0f);
+            float b = 1.0f - a;
+            return color(b * m_bg.color[0] + a * m_bg.top[0], b * m_bg.color[1] + a * m_bg.top[1],
+                         b * m_bg.color[2] + a * m_bg.top[2]);
+        }
+        // equirectangular lookup with get_spherical_uv's convention (uvmapping.cuh:144-158)
+        double theta = acos((double)-p.y);
+        double phi = atan2((double)-p.z, (double)p.x) + 3.14159265358979323846;
+        double u = phi / (2.0 * 3.14159265358979323846);
+        double v = theta / 3.14159265358979323846;
+        int W = m_bg.env_width, H = m_bg.env_height;
+        int x = (int)(u * W); x = x < 0 ? 0 : (x >= W ? W - 1 : x);
+        int y = (int)((1.0 - v) * H); y = y < 0 ? 0 : (y >= H ? H - 1 : y);
+        const float* px = m_env + 3 * ((size_t)y * W + x);
+        return color(px[0], px[1], px[2]);
+    }
+private:
+    rtc_background m_bg;
+    const float* m_env;
 };
 
 __device__ vector3 dv3(const float* p) { return vector3(p[0], p[1], p[2]); }
@@ -138,14 +174,14 @@ __global__ void refg_load_scene(DDesc d, DWorld* out, int* ok) {
     out->objects = objs;
     out->n = n;
     out->names = names;
+    out->bg_tex = d.bg.kind != RTC_BG_CONSTANT ? new refg_background(d.dummy_px, d.bg, d.env) : nullptr;
     *ok = 1;
 }
 
-// render kernel body (gpu.cu:761-790) without quantisation / printf
-__global__ void refg_render(DWorld* w, rtc_camera cd, rtc_background bg, rtc_render_params p, int sqrt_spp,
-                            const int64_t* pix, int64_t n, float* out) {
-    int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= n) return;
+// One pixel of the `render` kernel (gpu.cu:767-790): its FP32 pixel_color sum, before
+// prepare_pixel_color.  The camera is the reference's perspective_camera, initialised as load_scene does.
+__device__ color refg_pixel(DWorld* w, const rtc_camera& cd, const rtc_background& bg, const rtc_render_params& p,
+                            int sqrt_spp, int64_t pixel_index) {
     perspective_camera cam;
     cam.vfov = cd.vfov;
     cam.initialize(dv3(cd.look_from), dv3(cd.look_at), dv3(cd.up), p.width, cd.aspect, cd.vfov, cd.aperture, cd.focus,
@@ -153,7 +189,7 @@ __global__ void refg_render(DWorld* w, rtc_camera cd, rtc_background bg, rtc_ren
     cam.samples_per_pixel = p.spp;
     cam.max_depth = p.max_depth;
     cam.background_color = color(bg.color[0], bg.color[1], bg.color[2]);
-    int64_t pixel_index = pix[q];
+    if (w->bg_tex) { cam.background_texture = w->bg_tex; cam.background_iskybox = true; }
     int i = (int)(pixel_index % p.width), j = (int)(pixel_index / p.width);
     thrust::minstd_rand rng(p.seed + (uint32_t)pixel_index);
     thrust::uniform_real_distribution<float> uniform_dist(0.0f, 1.0f);
@@ -167,6 +203,31 @@ __global__ void refg_render(DWorld* w, rtc_camera cd, rtc_background bg, rtc_ren
             pixel_color += cam.ray_color(r, i, j, p.max_depth, p.max_depth, *w->world, *w->lights, rng);
         }
     }
+    return pixel_color;
+}
+
+// the render kernel body over a list of pixels (gpu.cu:761-790), without quantisation / printf
+__global__ void refg_render(DWorld* w, rtc_camera cd, rtc_background bg, rtc_render_params p, int sqrt_spp,
+                            const int64_t* pix, int64_t n, float* out) {
+    int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    const color pixel_color = refg_pixel(w, cd, bg, p, sqrt_spp, pix[q]);
+    out[4 * q + 0] = pixel_color.r();
+    out[4 * q + 1] = pixel_color.g();
+    out[4 * q + 2] = pixel_color.b();
+    out[4 * q + 3] = pixel_color.a();
+}
+
+// The whole frame in the reference's launch shape (gpu.cu:2072-2080): (W/16+1, H/16+1) blocks of 16x16
+// threads, thread (i, j) renders pixel j*W+i (gpu.cu:763-767).  Stores the FP32 sum where the reference
+// stores the quantised colour and prints it (the per-pixel printf is left out).
+__global__ void refg_render_frame(DWorld* w, rtc_camera cd, rtc_background bg, rtc_render_params p, int sqrt_spp,
+                                  float* out) {
+    int i = threadIdx.x + blockIdx.x * blockDim.x;
+    int j = threadIdx.y + blockIdx.y * blockDim.y;
+    if ((i >= p.width) || (j >= p.height)) return;
+    const int64_t q = (int64_t)j * p.width + i;
+    const color pixel_color = refg_pixel(w, cd, bg, p, sqrt_spp, q);
     out[4 * q + 0] = pixel_color.r();
     out[4 * q + 1] = pixel_color.g();
     out[4 * q + 2] = pixel_color.b();
@@ -258,9 +319,13 @@ int refg_setup(void) {
 
 void* refg_scene_create(const rtc_scene_desc* d) {
     if (!d) return nullptr;
-    if (d->background.kind != RTC_BG_CONSTANT) { g_err = "the reference's GPU path has a constant background only"; return nullptr; }
     GpuScene* s = new GpuScene();
     DDesc dd{};
+    dd.bg = d->background;
+    if (d->background.kind == RTC_BG_ENV_MAP)
+        dd.env = upload(d->background.env_rgb, (size_t)3 * d->background.env_width * d->background.env_height, s->allocs);
+    const unsigned char px[3] = {0, 0, 0};
+    dd.dummy_px = upload(px, 3, s->allocs);
     dd.tex = upload(d->textures, d->num_textures, s->allocs); dd.ntex = d->num_textures;
     dd.mat = upload(d->materials, d->num_materials, s->allocs); dd.nmat = d->num_materials;
     dd.lights = upload(d->dir_lights, d->num_dir_lights, s->allocs); dd.nlights = d->num_dir_lights;
@@ -332,6 +397,34 @@ int refg_render_pixels(void* p, const rtc_render_params* prm, const int64_t* pix
     bool ok = check(cudaDeviceSynchronize(), "refg_render");
     if (ok) ok = check(cudaMemcpy(out_rgba, dout, n * 16, cudaMemcpyDeviceToHost), "copy");
     cudaFree(dpix);
+    cudaFree(dout);
+    return ok ? 0 : 1;
+}
+
+// Renders the whole frame with refg_render_frame; `ms` receives the kernel's CUDA-event time (the
+// device-heap object graph is already built; allocation and copies are outside the events).
+// `out_rgba` (may be null) receives width*height float4 sums in frame-buffer order.
+int refg_render_frame_timed(void* p, const rtc_render_params* prm, float* out_rgba, float* ms) {
+    GpuScene* s = static_cast<GpuScene*>(p);
+    if (!s || !prm || !ms || prm->width <= 0 || prm->height <= 0) { g_err = "bad argument"; return 1; }
+    const int sqrt_spp = (int)std::sqrt((double)prm->spp);
+    const size_t npix = (size_t)prm->width * prm->height;
+    float* dout = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (!check(cudaMalloc(&dout, npix * 16), "malloc")) return 1;
+    bool ok = check(cudaEventCreate(&e0), "event") && check(cudaEventCreate(&e1), "event");
+    if (ok) {
+        const int tx = 16, ty = 16;   // gpu_cuda_renderer passes tx = ty = 16 (renderers/gpu_cuda_renderer.h:23-27)
+        dim3 blocks(prm->width / tx + 1, prm->height / ty + 1), threads(tx, ty);
+        cudaEventRecord(e0, 0);
+        refg_render_frame<<<blocks, threads>>>(s->d_world, s->cam, s->bg, *prm, sqrt_spp, dout);
+        cudaEventRecord(e1, 0);
+        ok = check(cudaGetLastError(), "refg_render_frame") && check(cudaDeviceSynchronize(), "refg_render_frame") &&
+             check(cudaEventElapsedTime(ms, e0, e1), "elapsed");
+    }
+    if (ok && out_rgba) ok = check(cudaMemcpy(out_rgba, dout, npix * 16, cudaMemcpyDeviceToHost), "copy");
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
     cudaFree(dout);
     return ok ? 0 : 1;
 }

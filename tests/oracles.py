@@ -160,6 +160,18 @@ class _RefGpuScene:
             raise RuntimeError(self.o.error())
         return out
 
+    def render_frame_timed(self, params: RenderParams, want_image: bool = False):
+        """The whole frame in the reference's launch shape (16x16 blocks, one thread per pixel); returns
+        (kernel milliseconds from CUDA events, (H, W, 4) sums or None)."""
+        ms = C.c_float(0.0)
+        img = np.empty((params.height, params.width, 4), np.float32) if want_image else None
+        p = params.to_c()
+        rc = self.o.lib.refg_render_frame_timed(self.h, C.byref(p), img.ctypes.data_as(C.c_void_p) if want_image else None,
+                                                C.byref(ms))
+        if rc:
+            raise RuntimeError(self.o.error())
+        return float(ms.value), img
+
     def trace_closest(self, rays: np.ndarray, depth: int, max_depth: int):
         rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
         prim = np.empty(rays.shape[0], np.int32)

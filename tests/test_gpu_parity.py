@@ -164,12 +164,14 @@ def test_compat_parity_vs_reference_gpu(ctx, refgpu, name, kw):
 
 @pytest.mark.parametrize("name", ["cornell", "spheres", "icosphere", "textured", "lights"])
 def test_closest_hit_identity(ctx, refcpu, name):
+    """T2: closest-hit primitive ids and distances against the reference's own BVH (bvh_node) on 10^6
+    seeded random rays per scene, for primary-ray visibility and for bounce rays."""
     from golden.make_golden import golden_rays
     mk, _ = configs.SCENES[name]
     scene = mk()
     ds = DeviceScene(ctx, scene)
     rs = refcpu.scene(scene)
-    rays = golden_rays(name, 20000, seed=7)
+    rays = golden_rays(name, 1000000, seed=7)
     for depth, max_depth in ((1, 1), (0, 8)):   # primary-ray visibility (invisible lights hidden) and bounce
         ours, t_ours = ds.trace_closest(rays, depth, max_depth)
         ref, t_ref = rs.trace_closest(rays, depth, max_depth)
