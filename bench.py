@@ -52,7 +52,8 @@ sys.path.insert(0, str(ROOT))
 from cortexraytracercuda_b200 import configs  # noqa: E402
 from cortexraytracercuda_b200.scene import (DRAW_ORDER_DEVICE, DRAW_ORDER_HOST, ENGINE_MEGAKERNEL,  # noqa: E402
                                             ENGINE_WAVEFRONT, FLAG_KERNEL_TIMING, FLAG_SAMPLE_GROUPS,
-                                            FLAG_WIDE_BVH, MODE_CLEAN, MODE_COMPAT, BVH_DEVICE, BVH_DEVICE_LBVH, BVH_SAH)
+                                            FLAG_WIDE_BVH, MODE_CLEAN, MODE_COMPAT, BVH_DEVICE, BVH_DEVICE_LBVH, BVH_SAH,
+                                            RenderParams)
 
 METRIC = "Mpaths/s"
 PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
@@ -192,6 +193,69 @@ def cpu_reference_rate(scene, params, target_s=10.0, max_pixels=None):
     return paths / dt / 1e6, rays / dt / 1e6, info
 
 
+# The reference's own GPU build timed on the same B200 (a second reported baseline, not a target): its
+# classes compiled by nvcc for sm_100a (oracle/_ref/libref_gpu.so), its render loop in its own launch
+# shape (16x16 blocks, one thread per pixel, gpu.cu:2072-2080), the per-pixel printf left out.
+REF_GPU_CASES = [
+    # (label, scene builder, parameters)
+    ("config 1: cornell 256x256 spp16 depth8", lambda: configs.cornell(), dict(width=256, height=256, spp=16, max_depth=8)),
+    ("config 2: spheres 1280x720 spp64 depth50 (the timed frame)", lambda: configs.spheres(),
+     dict(width=1280, height=720, spp=64, max_depth=50)),
+    ("P2: spheres 320x180 spp16 depth16, constant background", lambda: configs.spheres(sky=False),
+     dict(width=320, height=180, spp=16, max_depth=16)),
+    ("P3: textured 160x120 spp16 depth10", lambda: configs.textured(), dict(width=160, height=120, spp=16, max_depth=10)),
+    ("P4: icosphere (1,280 triangles x3) 150x100 spp16 depth12", lambda: configs.icosphere_scene(),
+     dict(width=150, height=100, spp=16, max_depth=12)),
+]
+
+
+def ref_gpu_baseline(ctx, stream, warmup=3, steps=3):
+    """Per case: the reference's own nvcc build (kernel time from CUDA events, one launch after one
+    untimed launch) against this library's default engine on the same scene and parameters (nvcc
+    flavour, scene resident, mean of `steps` event-timed launches after `warmup`).  None when the
+    reference's GPU build is not available."""
+    import torch
+    from cortexraytracercuda_b200.renderer import DeviceScene
+    sys.path.insert(0, str(ROOT / "tests"))
+    import oracles
+    ref = oracles.ref_gpu()
+    if ref is None:
+        return None
+    out = []
+    sp = stream.cuda_stream
+    for label, mk, kw in REF_GPU_CASES:
+        scene = mk()
+        p = RenderParams(**kw)
+        p.mode, p.draw_order, p.engine = MODE_COMPAT, DRAW_ORDER_DEVICE, ENGINE_WAVEFRONT
+        ds = DeviceScene(ctx, scene)
+        img = torch.empty((p.height, p.width, 4), dtype=torch.float32, device="cuda")
+        for _ in range(warmup):
+            ds.render_device(p, img.data_ptr(), stream=sp)
+        evs = []
+        for _ in range(steps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            ds.render_device(p, img.data_ptr(), stream=sp)
+            b.record(stream)
+            evs.append((a, b))
+        torch.cuda.synchronize()
+        ours_ms = float(np.mean([a.elapsed_time(b) for a, b in evs]))
+        ds.close()
+        rs = ref.scene(scene)
+        if p.width * p.height <= 65536:
+            rs.render_frame_timed(p)   # untimed first launch (module load, heap warm-up)
+        ref_ms, _ = rs.render_frame_timed(p)
+        del rs
+        paths = p.width * p.height * p.traced_spp
+        out.append({"case": label, "reference_gpu_ms": round(ref_ms, 2),
+                    "reference_gpu_mpaths_per_s": round(paths / ref_ms / 1e3, 3),
+                    "ours_ms": round(ours_ms, 3), "ours_mpaths_per_s": round(paths / ours_ms / 1e3, 3),
+                    "speedup": round(ref_ms / ours_ms, 2)})
+    return {"kind": "reference GPU build (oracle/_ref/libref_gpu.so: the reference's classes, nvcc -O3 sm_100a, "
+                    "device-heap object graph and bvh_node as load_scene builds them; its render loop in 16x16 "
+                    "blocks, per-pixel printf left out)", "cases": out}
+
+
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return
@@ -246,46 +310,80 @@ def replica_rate(units_per_rank, world, steps, total_ms):
     return units_per_rank * world * steps / (total_ms / 1e3) / 1e6
 
 
-def run_batched(args, rank, world, local):
-    """64 heterogeneous images per step: one rtc_render_batch call vs one plain launch per image."""
+def fp64_references(work, px_per_scene=128, mult=16, seed_offset=7919):
+    """Converged references for the RMSE of the batched workload: the double-precision clean-mode
+    estimator (oracle/fp64_clean.c) on a deterministic subsample of `px_per_scene` pixels of every image,
+    at `mult` x that image's spp, with a seed independent of the renders'.  Returns [(pixels, mean
+    radiance (n, 3))] per image, or None when the oracle is not built."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    import oracles
+    from concurrent.futures import ThreadPoolExecutor
+    f = oracles.fp64()
+    if f is None:
+        return None
+    workers = min(8, os.cpu_count() or 1)
+    threads = max(1, (os.cpu_count() or 1) // workers)
+
+    def one(k):
+        sc, p = work[k]
+        npx = p.width * p.height
+        pix = np.arange(0, npx, max(1, npx // px_per_scene), dtype=np.int64)[:px_per_scene]
+        out = f.render(sc, p.width, p.height, p.spp * mult, p.max_depth, (p.seed + seed_offset) & 0xFFFFFFFF, pix,
+                       threads=threads)
+        return pix, out / float(p.spp * mult)
+
+    with ThreadPoolExecutor(max_workers=workers) as ex:
+        return list(ex.map(one, range(len(work))))
+
+
+def relative_rmse(images, refs, params):
+    """sqrt(mean squared error) / sqrt(mean square) of the per-pixel mean radiance over the sampled pixels of
+    every image (linear RGB; a non-finite pixel counts as 0)."""
+    num = den = 0.0
+    for img, (pix, ref), p in zip(images, refs, params):
+        x = img.reshape(-1, 4)[pix, :3].astype(np.float64) / float(p.spp)
+        x = np.where(np.isfinite(x), x, 0.0)
+        num += float(((x - ref) ** 2).sum())
+        den += float((ref ** 2).sum())
+    return float(np.sqrt(num / max(den, 1e-30)))
+
+
+def batched_record(ctx, work, dss, mode, groups, warmup, steps, stream, flush, slots=0, drain=0, bvh="2",
+                   autotune=False, refs=None, launchgpu=False):
+    """One batch of all the workload's images per step (rtc_render_batch, CUDA-graph replay) against the
+    plain one-image-per-launch forms with every scene resident: the wavefront engine and the megakernel
+    (one thread per pixel, the reference's kernel shape), same mode and parameters.  Device time from CUDA
+    events on `stream`, L2 flushed between steps.  With `refs` (fp64_references), the relative RMSE of
+    each form's images against the converged references."""
     import torch
-    from cortexraytracercuda_b200.renderer import Context, DeviceScene, Job
-    dist = _init_dist(world, local)
-    mode, order = _mode_order(args)
-    ctx = Context(local)
-    work = configs.batch_workload(args.scenes)
-    t0 = time.perf_counter()
-    dss = [DeviceScene(ctx, sc) for sc, _ in work]
-    setup_s = time.perf_counter() - t0
+    from cortexraytracercuda_b200.renderer import Job
     params = []
-    for _, p in work:
-        p.mode, p.draw_order, p.engine = mode, order, ENGINE_WAVEFRONT
-        if args.groups:
+    for _, p0 in work:
+        p = p0.__class__(**p0.__dict__)
+        p.mode, p.draw_order, p.engine = mode, DRAW_ORDER_DEVICE, ENGINE_WAVEFRONT
+        if groups:
             p.flags |= FLAG_SAMPLE_GROUPS
-        if args.bvh == "8":
+        if bvh == "8":
             p.flags |= FLAG_WIDE_BVH
         params.append(p)
     outs = [torch.empty((p.height, p.width, 4), dtype=torch.float32, device="cuda") for p in params]
     plain_outs = [torch.empty_like(o) for o in outs]
+    mk_outs = [torch.empty_like(o) for o in outs]
     jobs = [Job(ds, p, o.data_ptr()) for ds, p, o in zip(dss, params, outs)]
     paths = sum(p.width * p.height * p.traced_spp for p in params)
     pixels = sum(p.width * p.height for p in params)
-    stream = torch.cuda.Stream()
-    torch.cuda.set_stream(stream)
     sp = stream.cuda_stream
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-
     tuned = None
-    if args.autotune:
-        from cortexraytracercuda_b200 import autotune
-        tuned = autotune.autotune_batch(ctx, jobs, repeats=1, stream=sp)
-        jobs = autotune.with_layout(jobs, tuned.layout)
-        args.slots, args.drain = tuned.slots, tuned.drain
+    if autotune:
+        from cortexraytracercuda_b200 import autotune as at
+        tuned = at.autotune_batch(ctx, jobs, repeats=1, stream=sp)
+        jobs = at.with_layout(jobs, tuned.layout)
+        slots, drain = tuned.slots, tuned.drain
         torch.cuda.synchronize()
 
     def batched():
-        ctx.render_batch(jobs, slots=args.slots, drain=args.drain, stream=sp,
-                         batch=tuned.batch if tuned else 0, block=tuned.block if tuned else 0)
+        ctx.render_batch(jobs, slots=slots, drain=drain, stream=sp, batch=tuned.batch if tuned else 0,
+                         block=tuned.block if tuned else 0)
 
     def plain():
         for ds, p, o in zip(dss, params, plain_outs):
@@ -294,12 +392,12 @@ def run_batched(args, rank, world, local):
     mk_params = [p.__class__(**{**p.__dict__, "engine": ENGINE_MEGAKERNEL}) for p in params]
 
     def plain_megakernel():
-        for ds, p, o in zip(dss, mk_params, plain_outs):
+        for ds, p, o in zip(dss, mk_params, mk_outs):
             ds.render_device(p, o.data_ptr(), stream=sp)
 
-    def timed(fn, steps):
+    def timed(fn, n):
         evs = []
-        for k in range(steps):
+        for k in range(n):
             flush.fill_(float(k))
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record(stream)
@@ -309,40 +407,20 @@ def run_batched(args, rank, world, local):
         torch.cuda.synchronize()
         return [a.elapsed_time(b) for a, b in evs]
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         batched()
     plain()
-    torch.cuda.synchronize()
-    clocks = ClockSampler(local)
-    clocks.start()
-    if world > 1:
-        dist.barrier()
-    stats = []
-    b_ms = timed(lambda: (batched(), stats.append(ctx.last_stats())), args.steps)
-    p_steps = max(1, min(args.steps, 2))
-    p_ms = timed(plain, p_steps)
     plain_megakernel()
-    m_ms = timed(plain_megakernel, 1)
-    clk = clocks.stop()
-    # the reference's per-call pattern (launchGPU builds and uploads its world for every image):
-    # rtc_scene_create + rtc_render with a host buffer + destroy, per image, one pass
-    t = time.perf_counter()
-    for (sc, _), p in zip(work, params):
-        host_img = np.empty((p.height, p.width, 4), np.float32)
-        d2 = DeviceScene(ctx, sc)
-        import ctypes as C
-        from cortexraytracercuda_b200._lib import check
-        pc = p.to_c()
-        check(ctx.lib.rtc_render(ctx.handle, d2.handle, C.byref(pc), host_img.ctypes.data, None))
-        d2.close()
-    l_s = time.perf_counter() - t
-    b_tot = _max_over_ranks(float(np.sum(b_ms)), world)
-    p_tot = _max_over_ranks(float(np.sum(p_ms)), world)
-    value = paths * world * args.steps / (b_tot / 1e3) / 1e6
-    plain_value = paths * world * p_steps / (p_tot / 1e3) / 1e6
-    # same images: bit-identical pixels and image-mean agreement of batched vs plain
-    plain()
     torch.cuda.synchronize()
+    stats = []
+    b_ms = timed(lambda: (batched(), stats.append(ctx.last_stats())), steps)
+    p_steps = max(1, min(steps, 2))
+    p_ms = timed(plain, p_steps)
+    m_ms = timed(plain_megakernel, 1)
+    value = paths * steps / (float(np.sum(b_ms)) / 1e3) / 1e6
+    plain_value = paths * p_steps / (float(np.sum(p_ms)) / 1e3) / 1e6
+    mk_value = paths / (m_ms[0] / 1e3) / 1e6
+    # the same images: bit-identical pixels and image-mean agreement of batched vs plain
     same, mean_dev = [], []
     for o, q in zip(outs, plain_outs):
         a, b = o[..., :3].double().nan_to_num(), q[..., :3].double().nan_to_num()
@@ -351,51 +429,106 @@ def run_batched(args, rank, world, local):
     # end to end: the batch with every image copied to pinned host memory
     host = [torch.empty(o.shape, dtype=torch.float32, pin_memory=True) for o in outs]
     e2e = []
-    for k in range(args.warmup + args.steps):
+    for k in range(warmup + steps):
         torch.cuda.synchronize()
         t = time.perf_counter()
         batched()
         for h, o in zip(host, outs):
             h.copy_(o, non_blocking=True)
         torch.cuda.synchronize()
-        if k >= args.warmup:
+        if k >= warmup:
             e2e.append(time.perf_counter() - t)
-    e2e_tot = _max_over_ranks(float(np.sum(e2e)), world)
     import ctypes as C
     from cortexraytracercuda_b200.scene import rtc_job
+    rec = {"value": round(value, 3), "unit": METRIC, "ms_per_step": round(float(np.mean(b_ms)), 3),
+           "steps": steps, "warmup": warmup,
+           "mode": ("clean, sample groups" if groups else "clean") if mode == MODE_CLEAN else "compat",
+           "workload": f"{len(work)} scenes, {pixels} pixels, {paths} paths per step",
+           "slots": slots or "default", "drain": drain or "default",
+           "plain_wavefront": {"value": round(plain_value, 3), "ms_per_step": round(float(np.mean(p_ms)), 3),
+                               "form": "one rtc_render_device per image, wavefront engine, scene resident"},
+           "plain_megakernel": {"value": round(mk_value, 3), "ms_per_step": round(m_ms[0], 3),
+                                "form": "one rtc_render_device per image, megakernel (one thread per pixel, the "
+                                        "reference's kernel shape), scene resident"},
+           "batched_over_plain_wavefront": round(value / plain_value, 3),
+           "batched_over_plain_megakernel": round(value / mk_value, 3),
+           "equal_to_plain_wavefront": {"bit_identical_pixels_min": round(min(same), 4),
+                                        "image_mean_rel_dev_max": round(max(mean_dev), 6)},
+           "gpu_launches": int(sum(st["launches"] for st in stats)),
+           "iterations": int(np.mean([st["iterations"] for st in stats])),
+           "e2e": {"value": round(paths * steps / float(np.sum(e2e)) / 1e6, 3), "unit": METRIC,
+                   "h2d_bytes_per_step": len(jobs) * C.sizeof(rtc_job), "d2h_bytes_per_step": pixels * 16}}
+    if refs is not None:
+        imgs = lambda lst: [o.cpu().numpy() for o in lst]   # noqa: E731
+        px = len(refs[0][0])
+        rec["rmse_vs_fp64"] = {
+            "batched": round(relative_rmse(imgs(outs), refs, params), 5),
+            "plain_wavefront": round(relative_rmse(imgs(plain_outs), refs, params), 5),
+            "plain_megakernel": round(relative_rmse(imgs(mk_outs), refs, params), 5),
+            "definition": f"relative RMSE of per-pixel mean linear RGB over {px} pixels of each of the {len(work)} "
+                          "images (every (W*H/px)-th pixel) against oracle/fp64_clean.c at 16x each image's spp, "
+                          "independent seed"}
+    if launchgpu:
+        # the reference's per-call pattern (launchGPU builds and uploads its world for every image):
+        # rtc_scene_create + rtc_render with a host buffer + destroy, per image, one pass
+        from cortexraytracercuda_b200._lib import check
+        from cortexraytracercuda_b200.renderer import DeviceScene
+        t = time.perf_counter()
+        for (sc, _), p in zip(work, params):
+            host_img = np.empty((p.height, p.width, 4), np.float32)
+            d2 = DeviceScene(ctx, sc)
+            pc = p.to_c()
+            check(ctx.lib.rtc_render(ctx.handle, d2.handle, C.byref(pc), host_img.ctypes.data, None))
+            d2.close()
+        l_s = time.perf_counter() - t
+        rec["plain_launchgpu"] = {"value": round(paths / l_s / 1e6, 3), "ms_per_step": round(l_s * 1e3, 1),
+                                  "form": "per image: rtc_scene_create (host BVH + upload) + rtc_render to a host "
+                                          "buffer + destroy, as launchGPU rebuilds its world per call"}
+        rec["batched_over_plain_launchgpu"] = round(value / (paths / l_s / 1e6), 3)
+    if tuned:
+        rec["autotune"] = {"chosen": {"slots": tuned.slots, "batch": tuned.batch, "drain": tuned.drain,
+                                      "layout": tuned.layout, "block": tuned.block},
+                           "search": "coordinate descent",
+                           "candidates_ms": [[c, round(ms, 1)] for c, ms in tuned.table]}
+    del outs, plain_outs, mk_outs
+    return rec
+
+
+def run_batched(args, rank, world, local):
+    """64 heterogeneous images per step: one rtc_render_batch call vs one plain launch per image."""
+    import torch
+    from cortexraytracercuda_b200.renderer import Context, DeviceScene
+    dist = _init_dist(world, local)
+    mode, _ = _mode_order(args)
+    ctx = Context(local)
+    work = configs.batch_workload(args.scenes)
+    t0 = time.perf_counter()
+    dss = [DeviceScene(ctx, sc) for sc, _ in work]
+    setup_s = time.perf_counter() - t0
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    refs = fp64_references(work) if args.rmse else None
+    clocks = ClockSampler(local)
+    clocks.start()
+    if world > 1:
+        dist.barrier()
+    rec = batched_record(ctx, work, dss, mode, args.groups, args.warmup, args.steps, stream, flush, args.slots,
+                         args.drain, args.bvh, args.autotune, refs, launchgpu=True)
+    clk = clocks.stop()
+    b_tot = _max_over_ranks(rec["ms_per_step"] * args.steps, world)
+    value = rec["value"] * world * (rec["ms_per_step"] * args.steps) / b_tot
     line = {"metric": METRIC, "value": round(value, 3), "unit": METRIC, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(b_tot / args.steps, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"batched: {len(work)} scenes, {pixels} pixels, {paths} paths per step",
-                       "triangles": int(sum(sc.num_triangles for sc, _ in work)),
-                       "mode": "compat" if mode == MODE_COMPAT else "clean",
-                       "slots": args.slots or "default", "drain": args.drain or "default",
+            "config": {"workload": f"batched: {rec['workload']}",
+                       "triangles": int(sum(sc.num_triangles for sc, _ in work)), "mode": rec["mode"],
+                       "slots": rec["slots"], "drain": rec["drain"],
                        "l2": "flushed between steps (256 MiB write)", "seed": configs.DEFAULT_SEED,
                        "parallelism": f"replicas x{world}"},
-            "plain": {"value": round(plain_value, 3), "unit": METRIC, "ms_per_step": round(p_tot / p_steps, 3),
-                      "form": "one rtc_render_device per image, wavefront engine, scene resident"},
-            "plain_megakernel": {"value": round(paths / (m_ms[0] / 1e3) / 1e6, 3), "unit": METRIC,
-                                 "ms_per_step": round(m_ms[0], 3),
-                                 "form": "one rtc_render_device per image, megakernel (one thread per pixel, "
-                                         "the reference's kernel shape), scene resident"},
-            "plain_launchgpu": {"value": round(paths / l_s / 1e6, 3), "unit": METRIC, "ms_per_step": round(l_s * 1e3, 1),
-                                "form": "per image: rtc_scene_create (host BVH + upload) + rtc_render to a host "
-                                        "buffer + destroy, as launchGPU rebuilds its world per call"},
-            "batched_over_plain": round(value / plain_value, 3),
-            "batched_over_plain_megakernel": round(value / (paths / (m_ms[0] / 1e3) / 1e6), 3),
-            "batched_over_plain_launchgpu": round(value / (paths / l_s / 1e6), 3),
-            "equal_to_plain": {"bit_identical_pixels_min": round(min(same), 4),
-                               "image_mean_rel_dev_max": round(max(mean_dev), 6)},
-            "gpu_launches": int(sum(st["launches"] for st in stats)),
-            "iterations": int(np.mean([st["iterations"] for st in stats])),
-            "e2e": {"value": round(paths * world * args.steps / e2e_tot / 1e6, 3), "unit": METRIC,
-                    "h2d_bytes_per_step": len(jobs) * C.sizeof(rtc_job), "d2h_bytes_per_step": pixels * 16},
+            **{k: v for k, v in rec.items() if k not in ("value", "ms_per_step", "steps", "warmup", "workload", "mode",
+                                                         "slots", "drain")},
             "setup_s": round(setup_s, 2), "clocks": clk, "roofline": None, "cpu_baseline": None}
-    if tuned:
-        line["autotune"] = {"chosen": {"slots": tuned.slots, "batch": tuned.batch, "drain": tuned.drain,
-                                       "layout": tuned.layout, "block": tuned.block},
-                            "search": "coordinate descent",
-                            "candidates_ms": [[c, round(ms, 1)] for c, ms in tuned.table]}
     if rank == 0:
         print(json.dumps(line), flush=True)
     for ds in dss:
@@ -416,22 +549,22 @@ def _percentiles(lat):
             "p99_ms": round(float(np.percentile(lat, 99)), 2), "mean_ms": round(float(lat.mean()), 2)}
 
 
-def run_served(args, rank, world, local):
-    """Poisson request streams through the render server vs a plain one-request-per-launch server."""
+def served_record(local, work, mode, groups, lambdas, requests, plain_requests, slots=0, seed_offset=0):
+    """Poisson request streams through the render server (continuous admission, resident scenes, LRU under
+    the HBM budget) against a plain server that renders one request per launch in arrival order, for each
+    rate in `lambdas` (1/s).  Latency = completion - submission; Mpaths/s over the stream's span."""
     import torch
     from cortexraytracercuda_b200.renderer import Context, DeviceScene, Job, RenderServer
-    dist = _init_dist(world, local)
-    mode, order = _mode_order(args)
-    work = configs.batch_workload(args.scenes)
-    gflags = FLAG_SAMPLE_GROUPS if args.groups else 0
-    srv = RenderServer(local, mode=mode, draw_order=order, slots=args.slots, flags=gflags)
+    order = DRAW_ORDER_DEVICE
+    gflags = FLAG_SAMPLE_GROUPS if groups else 0
+    srv = RenderServer(local, mode=mode, draw_order=order, slots=slots, flags=gflags)
     t0 = time.perf_counter()
     ids = [srv.add_scene(sc) for sc, _ in work]
     setup_s = time.perf_counter() - t0
     ctx = Context(local)
     dss = [DeviceScene(ctx, sc) for sc, _ in work]   # the plain server's resident scenes
     weights = _zipf_weights(len(work))
-    rng = np.random.default_rng(configs.DEFAULT_SEED + rank)
+    rng = np.random.default_rng(configs.DEFAULT_SEED + seed_offset)
     pools = {}
 
     def take(shape):
@@ -444,7 +577,7 @@ def run_served(args, rank, world, local):
         ang = rng.uniform(0.0, 2.0 * np.pi, n)
         return arr, sc, ang
 
-    def request(k, sc, ang):
+    def request(sc, ang):
         cam = configs.orbit_camera(work[sc][0].camera, float(ang))
         p = work[sc][1]
         rp = p.__class__(**{**p.__dict__, "mode": mode, "draw_order": order, "engine": ENGINE_WAVEFRONT,
@@ -453,15 +586,13 @@ def run_served(args, rank, world, local):
 
     # warm-up: every scene once (uploads), not timed
     for k in range(len(work)):
-        rp, cam = request(k, k, 0.0)
+        rp, cam = request(k, 0.0)
         out = take((rp.height, rp.width, 4))
         srv.wait(srv.submit(ids[k], rp, cam, out)[0])
         pools[(rp.height, rp.width, 4)].append(out)
     per_rate = {}
-    clocks = ClockSampler(local)
-    clocks.start()
-    for lam in [float(x) for x in args.lambdas.split(",")]:
-        arr, scs, angs = stream_of(lam, args.requests)
+    for lam in lambdas:
+        arr, scs, angs = stream_of(lam, requests)
         tickets = []
         lock = threading.Lock()
 
@@ -471,7 +602,7 @@ def run_served(args, rank, world, local):
                 dt = arr[k] - (time.perf_counter() - start)
                 if dt > 0:
                     time.sleep(dt)
-                rp, cam = request(k, scs[k], angs[k])
+                rp, cam = request(scs[k], angs[k])
                 with lock:
                     out = take((rp.height, rp.width, 4))
                 t, _ = srv.submit(ids[scs[k]], rp, cam, out)
@@ -500,7 +631,7 @@ def run_served(args, rank, world, local):
         served = {"requests": len(arr), **_percentiles(lat), "mpaths_per_s": round(total / ((last - first) / 1e3) / 1e6, 3),
                   "offered_mpaths_per_s": round(total / arr[-1] / 1e6, 3)}
         # plain comparison: one launch per request, in arrival order, same stream prefix
-        n_plain = min(args.plain_requests, len(arr))
+        n_plain = min(plain_requests, len(arr))
         plat, ptotal = [], 0
         start = time.perf_counter()
         busy_until = 0.0
@@ -508,7 +639,7 @@ def run_served(args, rank, world, local):
             now = time.perf_counter() - start
             if arr[q] > now:
                 time.sleep(arr[q] - now)
-            rp, cam = request(q, scs[q], angs[q])
+            rp, cam = request(scs[q], angs[q])
             out = torch.empty((rp.height, rp.width, 4), dtype=torch.float32, device="cuda")
             host = take((rp.height, rp.width, 4))
             ds = dss[int(scs[q])]
@@ -523,28 +654,42 @@ def run_served(args, rank, world, local):
                  "mpaths_per_s": round(ptotal / (busy_until - arr[0]) / 1e6, 3)}
         per_rate[str(int(lam))] = {"served": served, "plain": plain,
                                    "served_over_plain": round(served["mpaths_per_s"] / plain["mpaths_per_s"], 3)}
-    clk = clocks.stop()
     st = srv.stats()
-    top = per_rate[max(per_rate, key=lambda x: float(x))]
-    line = {"metric": METRIC, "value": top["served"]["mpaths_per_s"], "unit": METRIC, "n_gpus": world,
-            "steps": len(per_rate), "warmup": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"served: Poisson streams over {len(work)} batched scenes, Zipf s=1.1, "
-                                   f"orbit cameras, {args.requests} requests per rate",
-                       "mode": "compat" if mode == MODE_COMPAT else "clean", "slots": args.slots or "default",
-                       "sample_groups": bool(args.groups), "hbm_budget": "120 GB", "parallelism": f"replicas x{world}", "seed": configs.DEFAULT_SEED},
-            "rates": per_rate, "server": {k: st[k] for k in ("completed", "failed", "scene_uploads", "scene_evictions",
-                                                             "peak_resident_bytes", "iterations", "launches")},
-            "gpu_launches": int(st["launches"]),
-            "e2e": {"value": top["served"]["mpaths_per_s"], "unit": METRIC, "h2d_bytes_per_step": None,
-                    "d2h_bytes_per_step": None, "note": "requests in, radiance in pinned host buffers out"},
-            "setup_s": round(setup_s, 2), "clocks": clk, "roofline": None, "cpu_baseline": None}
-    if rank == 0:
-        print(json.dumps(line), flush=True)
+    rec = {"mode": ("clean, sample groups" if groups else "clean") if mode == MODE_CLEAN else "compat",
+           "workload": f"Poisson streams over {len(work)} batched scenes, Zipf s=1.1, orbit cameras, "
+                       f"{requests} requests per rate ({plain_requests} for the plain server)",
+           "rates": per_rate, "server": {k: st[k] for k in ("completed", "failed", "scene_uploads", "scene_evictions",
+                                                            "peak_resident_bytes", "iterations", "launches")},
+           "gpu_launches": int(st["launches"]), "setup_s": round(setup_s, 2), "hbm_budget": "120 GB"}
     srv.close()
     for ds in dss:
         ds.close()
     ctx.close()
+    return rec
+
+
+def run_served(args, rank, world, local):
+    """Poisson request streams through the render server vs a plain one-request-per-launch server."""
+    dist = _init_dist(world, local)
+    mode, _ = _mode_order(args)
+    work = configs.batch_workload(args.scenes)
+    clocks = ClockSampler(local)
+    clocks.start()
+    rec = served_record(local, work, mode, args.groups, [float(x) for x in args.lambdas.split(",")], args.requests,
+                        args.plain_requests, args.slots, seed_offset=rank)
+    clk = clocks.stop()
+    top = rec["rates"][max(rec["rates"], key=lambda x: float(x))]
+    line = {"metric": METRIC, "value": top["served"]["mpaths_per_s"], "unit": METRIC, "n_gpus": world,
+            "steps": len(rec["rates"]), "warmup": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"served: {rec['workload']}", "mode": rec["mode"], "slots": args.slots or "default",
+                       "hbm_budget": rec["hbm_budget"], "parallelism": f"replicas x{world}", "seed": configs.DEFAULT_SEED},
+            "rates": rec["rates"], "server": rec["server"], "gpu_launches": rec["gpu_launches"],
+            "e2e": {"value": top["served"]["mpaths_per_s"], "unit": METRIC, "h2d_bytes_per_step": None,
+                    "d2h_bytes_per_step": None, "note": "requests in, radiance in pinned host buffers out"},
+            "setup_s": rec["setup_s"], "clocks": clk, "roofline": None, "cpu_baseline": None}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
 
@@ -573,12 +718,19 @@ def main():
                     help="batched: pick slots / batch / drain / BVH layout with the autotuner before timing")
     ap.add_argument("--groups", action="store_true",
                     help="batched/served, clean mode: split pixels into sample groups (RTC_FLAG_SAMPLE_GROUPS)")
+    ap.add_argument("--no-batched", action="store_true", help="default line: skip the batched record")
+    ap.add_argument("--no-served", action="store_true", help="default line: skip the served record")
+    ap.add_argument("--no-ref-gpu", action="store_true", help="default line: skip the reference GPU build's timings")
+    ap.add_argument("--no-rmse", action="store_true", help="skip the RMSE against the fp64 oracle")
+    ap.add_argument("--served-requests", type=int, default=100, help="default line: served requests at 200/s")
+    ap.add_argument("--served-plain-requests", type=int, default=40)
     ap.add_argument("--lambdas", default="20,50,200,800", help="served: request rates (1/s)")
     ap.add_argument("--requests", type=int, default=300, help="served: requests per rate")
     ap.add_argument("--plain-requests", type=int, default=120, help="served: requests of the plain comparison")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    args.rmse = not args.no_rmse
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -769,9 +921,37 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, r, inf = cpu_reference_rate(scene, params, target_s=args.cpu_baseline_s)
         line["cpu_baseline"] = {"value": round(v, 4), "unit": METRIC, **inf, "mrays_per_s": round(r, 4)}
+    ds.close()
+    # ---- the batched and served forms (configs 4 and 5) and the reference's GPU build, one GPU only ----
+    if world == 1 and args.config == "spheres" and not args.small:
+        extra_clk = ClockSampler(local)
+        extra_clk.start()
+        if not args.no_batched:
+            work = configs.batch_workload(args.scenes)
+            t0 = time.perf_counter()
+            bdss = [DeviceScene(ctx, sc) for sc, _ in work]
+            setup_s = time.perf_counter() - t0
+            refs = None if args.no_rmse else fp64_references(work)
+            bsteps = max(1, min(args.steps, 3))
+            line["batched"] = {
+                "config": "batched: 64 seeded scenes (1K-500K triangles, 256^2..1024^2, spp 4/16/64, depth 8-32)",
+                "scene_setup_s": round(setup_s, 2),
+                "compat": batched_record(ctx, work, bdss, MODE_COMPAT, False, args.warmup, bsteps, stream, flush,
+                                         refs=refs),
+                "clean_groups": batched_record(ctx, work, bdss, MODE_CLEAN, True, args.warmup, bsteps, stream, flush,
+                                               refs=refs)}
+            for d in bdss:
+                d.close()
+            del bdss
+        if not args.no_served:
+            work = configs.batch_workload(args.scenes)
+            line["served"] = served_record(local, work, MODE_CLEAN, True, [200.0], args.served_requests,
+                                           args.served_plain_requests)
+        if not args.no_ref_gpu:
+            line["gpu_baseline"] = ref_gpu_baseline(ctx, stream)
+        line["clocks_extra_legs"] = extra_clk.stop()
     if rank == 0:
         print(json.dumps(line), flush=True)
-    ds.close()
     ctx.close()
     if world > 1:
         dist.destroy_process_group()

@@ -885,13 +885,14 @@ void rtc_carve_groups(void* base, const rtc_render_params* p, float4** part, uin
 
 namespace {
 
-// Bytes of wavefront scratch per path slot.
-constexpr size_t WF_SLOT_BYTES = 5 * sizeof(float4) + 2 * sizeof(uint4) + sizeof(float2) + 3 * sizeof(uint32_t);
+// Bytes of wavefront scratch per path slot (with the shade bins).
+constexpr size_t WF_SLOT_BYTES =
+    5 * sizeof(float4) + 2 * sizeof(uint4) + sizeof(float2) + 3 * sizeof(uint32_t) + WF_BINS * sizeof(uint32_t);
 constexpr uint32_t WF_MAX_SLOTS = 1u << 22;   // 4,194,304 slots = 432 MiB of path state
 
 // Lays out the wavefront buffers for `slots` path slots in one block of device memory at `base`
-// (the context's scratch, or the allocation-free entry point's static array).
-size_t carve_wavefront(void* base, uint32_t slots, WfBuffers& B) {
+// (the context's scratch, or the allocation-free entry point's static array, which has no bins).
+size_t carve_wavefront(void* base, uint32_t slots, WfBuffers& B, bool bins = true) {
     uint8_t* p = (uint8_t*)base;
     auto take = [&](size_t bytes) {
         uint8_t* r = p;
@@ -910,21 +911,22 @@ size_t carve_wavefront(void* base, uint32_t slots, WfBuffers& B) {
     B.queue[0] = (uint32_t*)take(n * 4);
     B.queue[1] = (uint32_t*)take(n * 4);
     B.queue[2] = (uint32_t*)take(n * 4);
+    B.bins = bins ? (uint32_t*)take(n * 4 * WF_BINS) : nullptr;
     B.ctr = (uint32_t*)take(WF_CTR_N * 4);
     B.slots = slots;
     return (size_t)(p - (uint8_t*)base);
 }
 
 // Bytes carve_wavefront lays out for `slots` slots (each buffer rounded up to 256 bytes).
-constexpr size_t wavefront_bytes(size_t n) {
+constexpr size_t wavefront_bytes(size_t n, bool bins) {
     return 7 * ((n * 16 + 255) & ~(size_t)255) + ((n * 8 + 255) & ~(size_t)255) + 3 * ((n * 4 + 255) & ~(size_t)255) +
-           ((WF_CTR_N * 4 + 255) & ~(size_t)255);
+           (bins ? ((n * 4 * WF_BINS + 255) & ~(size_t)255) : 0) + ((WF_CTR_N * 4 + 255) & ~(size_t)255);
 }
 // The allocation-free render's advertised cap fits its 64 MiB array behind a 256-byte status header
 // (render_noalloc.cu), so an image at or under RTC_NOALLOC_MAX_PIXELS never fails for lack of room.
-static_assert(256 + wavefront_bytes(RTC_NOALLOC_MAX_PIXELS) <= (size_t(64) << 20),
+static_assert(256 + wavefront_bytes(RTC_NOALLOC_MAX_PIXELS, false) <= (size_t(64) << 20),
               "RTC_NOALLOC_MAX_PIXELS slots do not fit the allocation-free render's static array");
-static_assert(wavefront_bytes(1) <= WF_SLOT_BYTES + 12 * 256, "wavefront layout grew past WF_SLOT_BYTES");
+static_assert(wavefront_bytes(1, true) <= WF_SLOT_BYTES + 13 * 256, "wavefront layout grew past WF_SLOT_BYTES");
 
 rtc_status ensure_wavefront(rtc_context* c, uint32_t slots, WfBuffers& B) {
     if (c->wf_cap < slots) {
@@ -943,7 +945,9 @@ rtc_status ensure_wavefront(rtc_context* c, uint32_t slots, WfBuffers& B) {
         for (cudaEvent_t& e : c->split_ev) RTC_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         RTC_CUDA(cudaStreamCreateWithFlags(&c->stream_long, cudaStreamNonBlocking));
     }
-    carve_wavefront(c->d_wf, slots, B);
+    // shade bins (material-sorted shading) unless RTC_WF_BINS=0
+    const char* eb = std::getenv("RTC_WF_BINS");
+    carve_wavefront(c->d_wf, slots, B, !(eb && std::atoi(eb) == 0));
     return RTC_OK;
 }
 
@@ -1200,7 +1204,9 @@ rtc_status launch_wavefront(rtc_context* c, const rtc_scene* s, const rtc_render
 
 // ---- internal helpers shared with render_noalloc.cu (rtc_internal.h) ----
 size_t rtc_wf_slot_bytes() { return WF_SLOT_BYTES; }
-size_t rtc_carve_wavefront(void* base, uint32_t slots, WfBuffers& B) { return carve_wavefront(base, slots, B); }
+size_t rtc_carve_wavefront(void* base, uint32_t slots, WfBuffers& B, bool bins) {
+    return carve_wavefront(base, slots, B, bins);
+}
 rtc_status rtc_set_error(rtc_status s, const char* msg) { return fail(s, msg); }
 rtc_status rtc_check_render_params(const rtc_render_params* p) { return check_params(p); }
 int rtc_scene_device(const rtc_scene* s) { return s->device; }

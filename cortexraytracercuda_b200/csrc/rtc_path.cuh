@@ -188,78 +188,12 @@ struct PathCounters {
     uint32_t rays, nodes, prims;
 };
 
-// One bounce of camera::ray_color (camera.cuh:153-227) AFTER the closest-hit query of the current ray:
-// `hit` tells whether world.hit found something at (t, item).  Updates the path's running radiance
-// `result`, its attenuation `att` and its ray; returns false when the path ends at this bounce.
-// All additions of the reference are kept, including the zero emission of non-emitting materials,
-// so NaN/Inf propagate exactly as in the reference.  The megakernel and the wavefront shade kernel
-// both call this, so the two engines are the same arithmetic.
+// material::scatter of the hit material (metal, dielectric or lambertian; lights are handled by the
+// caller): updates the attenuation and turns `r` into the scattered ray (camera.cuh:185-225).
 template <bool CLEAN, int ORDER, class R>
-__device__ __forceinline__ bool shade_bounce(const DevScene& S, Ray& r, bool hit, float t, uint32_t item, bool hide,
-                                             RGB& result, RGB& att, R& rng, PathCounters& pc, TraceStats& st,
-                                             uint32_t& status) {
-    if (!hit) {
-        RGB bg = background(S, r.d);
-        result.r += att.r * bg.r;
-        result.g += att.g * bg.g;
-        result.b += att.b * bg.b;
-        return false;
-    }
+__device__ __forceinline__ void scatter_bounce(const DevScene& S, Ray& r, const Hit& h, int4 mi, float4 mf, RGB& att,
+                                               R& rng, uint32_t& status) {
     constexpr bool FT = CLEAN || ORDER == 0;   // float trig in the nvcc flavour and in clean mode
-    Hit h;
-    finalize_hit<FT>(S, item, t, r.o, r.d, h);
-    if ((uint32_t)h.mat >= S.num_materials) { status |= STATUS_BAD_MATERIAL; return false; }
-    int4 mi = __ldg(S.mat_i + h.mat);
-    float4 mf = __ldg(S.mat_f + h.mat);
-    // emitted (diffuse_light.cuh:45-67; material::emitted returns (0,0,0) otherwise)
-    RGB em = rgb(0.f, 0.f, 0.f);
-    bool em_alpha0 = false;
-    if (mi.x == 3) {
-        if (mf.w != 0.0f && !h.front) {
-            em_alpha0 = true;   // RGBA(0,0,0,0): back face of a one-sided light
-        } else {
-            RGB tv = texture_value(S, mi.y, h.u, h.v, h.p, status);
-            em = rgb(tv.r * mf.z, tv.g * mf.z, tv.b * mf.z);
-        }
-    } else if (mi.x == MAT_SPOT_LIGHT) {
-        // diffuse_spot_light::emitted (diffuse_spot_light.cuh:33-49).  Back face: RGBA(0,0,0,0) when
-        // invisible, else RGBA(1,1,1,0) (both re-hit; the product with the attenuation adds 0 or 1);
-        // outside the cone RGBA(1,1,1,1); inside texture * (intensity * pow(cos, falloff)).
-        const float4* q = S.light + 6 * (size_t)mi.z;
-        const float4 sd = __ldg(q + 2), cone = __ldg(q + 3);
-        if (!h.front) {
-            em_alpha0 = true;
-            if (cone.w == 0.0f) em = rgb(1.f, 1.f, 1.f);
-        } else {
-            const float cos_theta = dot(unit(r.d), unit(v3(sd.x, sd.y, sd.z)));
-            if (cos_theta < cone.x) {
-                em = rgb(1.f, 1.f, 1.f);
-            } else {
-                const float attn = FT ? powf(cos_theta, cone.y) : (float)pow((double)cos_theta, (double)cone.y);
-                const float k = mf.z * attn;
-                RGB tv = texture_value(S, mi.y, h.u, h.v, h.p, status);
-                em = rgb(tv.r * k, tv.g * k, tv.b * k);
-            }
-        }
-    }
-    if (em_alpha0) {
-        // "invisible" re-hit from just behind the light (camera.cuh:177-183); rec is replaced only
-        // when the re-hit finds something, and `emitted` is not recomputed.
-        float t2;
-        uint32_t item2;
-        pc.rays++;
-        if (closest_hit<CLEAN>(S, r.o, r.d, h.t + 0.001f, 3.402823466e+38f, hide, t2, item2, st, status)) {
-            finalize_hit<FT>(S, item2, t2, r.o, r.d, h);
-            if ((uint32_t)h.mat >= S.num_materials) { status |= STATUS_BAD_MATERIAL; return false; }
-            mi = __ldg(S.mat_i + h.mat);
-            mf = __ldg(S.mat_f + h.mat);
-        }
-    }
-    result.r += att.r * em.r;
-    result.g += att.g * em.g;
-    result.b += att.b * em.b;
-    if (mi.x == 3 || mi.x == MAT_SPOT_LIGHT) return false;   // lights: material::scatter returns false
-
     if (mi.x == 1) {
         // metal::scatter (metal.cuh:57-64)
         RGB a = texture_value(S, mi.y, h.u, h.v, h.p, status);
@@ -270,7 +204,7 @@ __device__ __forceinline__ bool shade_bounce(const DevScene& S, Ray& r, bool hit
         att.r *= a.r;
         att.g *= a.g;
         att.b *= a.b;
-        return true;
+        return;
     }
     if (mi.x == 2) {
         // dielectric::scatter (dielectric.cuh:32-52) with Schlick (dielectric.cuh:57-63)
@@ -293,7 +227,7 @@ __device__ __forceinline__ bool shade_bounce(const DevScene& S, Ray& r, bool hit
         }
         r.d = do_reflect ? reflect(ud, h.n) : refract(ud, h.n, ratio);
         r.o = scatter_origin<CLEAN>(h.p, h.n, r.d);
-        return true;   // attenuation (1,1,1)
+        return;   // attenuation (1,1,1)
     }
     // lambertian::scatter (lambertian.cuh:63-131): attenuation from the texture, cosine_pdf(normal)
     RGB a = texture_value(S, mi.y, h.u, h.v, h.p, status);
@@ -330,7 +264,137 @@ __device__ __forceinline__ bool shade_bounce(const DevScene& S, Ray& r, bool hit
     att.b *= rcp * (a.b * spdf);
     r.o = scatter_origin<CLEAN>(h.p, h.n, dir);
     r.d = dir;
+}
+
+__device__ __forceinline__ bool is_light_material(int kind) { return kind == 3 || kind == MAT_SPOT_LIGHT; }
+
+// material::emitted of the hit (diffuse_light.cuh:45-67, diffuse_spot_light.cuh:33-49; other materials
+// emit (0,0,0)).  `alpha0` is set for an emission with alpha 0 - the back face of a one-sided light -
+// which makes camera::ray_color re-hit the scene from just behind it (camera.cuh:177-183).
+template <bool FT>
+__device__ __forceinline__ RGB emitted(const DevScene& S, const Ray& r, const Hit& h, int4 mi, float4 mf, bool& alpha0,
+                                       uint32_t& status) {
+    RGB em = rgb(0.f, 0.f, 0.f);
+    alpha0 = false;
+    if (mi.x == 3) {
+        if (mf.w != 0.0f && !h.front) {
+            alpha0 = true;   // RGBA(0,0,0,0): back face of a one-sided light
+        } else {
+            RGB tv = texture_value(S, mi.y, h.u, h.v, h.p, status);
+            em = rgb(tv.r * mf.z, tv.g * mf.z, tv.b * mf.z);
+        }
+    } else if (mi.x == MAT_SPOT_LIGHT) {
+        // diffuse_spot_light::emitted (diffuse_spot_light.cuh:33-49).  Back face: RGBA(0,0,0,0) when
+        // invisible, else RGBA(1,1,1,0) (both re-hit; the product with the attenuation adds 0 or 1);
+        // outside the cone RGBA(1,1,1,1); inside texture * (intensity * pow(cos, falloff)).
+        const float4* q = S.light + 6 * (size_t)mi.z;
+        const float4 sd = __ldg(q + 2), cone = __ldg(q + 3);
+        if (!h.front) {
+            alpha0 = true;
+            if (cone.w == 0.0f) em = rgb(1.f, 1.f, 1.f);
+        } else {
+            const float cos_theta = dot(unit(r.d), unit(v3(sd.x, sd.y, sd.z)));
+            if (cos_theta < cone.x) {
+                em = rgb(1.f, 1.f, 1.f);
+            } else {
+                const float attn = FT ? powf(cos_theta, cone.y) : (float)pow((double)cos_theta, (double)cone.y);
+                const float k = mf.z * attn;
+                RGB tv = texture_value(S, mi.y, h.u, h.v, h.p, status);
+                em = rgb(tv.r * k, tv.g * k, tv.b * k);
+            }
+        }
+    }
+    return em;
+}
+
+// One bounce of camera::ray_color (camera.cuh:153-227) AFTER the closest-hit query of the current ray:
+// `hit` tells whether world.hit found something at (t, item).  Updates the path's running radiance
+// `result`, its attenuation `att` and its ray; returns false when the path ends at this bounce.
+// All additions of the reference are kept, including the zero emission of non-emitting materials,
+// so NaN/Inf propagate exactly as in the reference.  The megakernel and the drain kernel call this;
+// the wavefront shade kernel calls the same pieces through shade_bounce_deferred.
+template <bool CLEAN, int ORDER, class R>
+__device__ __forceinline__ bool shade_bounce(const DevScene& S, Ray& r, bool hit, float t, uint32_t item, bool hide,
+                                             RGB& result, RGB& att, R& rng, PathCounters& pc, TraceStats& st,
+                                             uint32_t& status) {
+    if (!hit) {
+        RGB bg = background(S, r.d);
+        result.r += att.r * bg.r;
+        result.g += att.g * bg.g;
+        result.b += att.b * bg.b;
+        return false;
+    }
+    constexpr bool FT = CLEAN || ORDER == 0;   // float trig in the nvcc flavour and in clean mode
+    Hit h;
+    finalize_hit<FT>(S, item, t, r.o, r.d, h);
+    if ((uint32_t)h.mat >= S.num_materials) { status |= STATUS_BAD_MATERIAL; return false; }
+    int4 mi = __ldg(S.mat_i + h.mat);
+    float4 mf = __ldg(S.mat_f + h.mat);
+    bool em_alpha0;
+    const RGB em = emitted<FT>(S, r, h, mi, mf, em_alpha0, status);
+    if (em_alpha0) {
+        // "invisible" re-hit from just behind the light (camera.cuh:177-183); rec is replaced only
+        // when the re-hit finds something, and `emitted` is not recomputed.
+        float t2;
+        uint32_t item2;
+        pc.rays++;
+        if (closest_hit<CLEAN>(S, r.o, r.d, h.t + 0.001f, 3.402823466e+38f, hide, t2, item2, st, status)) {
+            finalize_hit<FT>(S, item2, t2, r.o, r.d, h);
+            if ((uint32_t)h.mat >= S.num_materials) { status |= STATUS_BAD_MATERIAL; return false; }
+            mi = __ldg(S.mat_i + h.mat);
+            mf = __ldg(S.mat_f + h.mat);
+        }
+    }
+    result.r += att.r * em.r;
+    result.g += att.g * em.g;
+    result.b += att.b * em.b;
+    if (is_light_material(mi.x)) return false;   // lights: material::scatter returns false
+    scatter_bounce<CLEAN, ORDER>(S, r, h, mi, mf, att, rng, status);
     return true;
+}
+
+// The same bounce with the invisible re-hit handed back to the caller instead of traced here, so the
+// wavefront shade kernel holds no traversal: the re-hit goes through the extend kernel like any other ray.
+//   BOUNCE_END    the path ends at this bounce;
+//   BOUNCE_NEXT   the path continues with the scattered ray (one depth level used);
+//   BOUNCE_REHIT  the hit was the back face of a one-sided light: its (zero-alpha) emission is added
+//                 and the same ray must be traced again from `rehit_tmin` = t + 0.001, at the same
+//                 depth; the next call passes `rehit` = true with that trace's result.
+// With `rehit`, a miss or a light leaves the path ending on the light (rec keeps the light's material,
+// whose scatter returns false), anything else scatters with no emission added - exactly camera.cuh:177-190.
+enum BounceOut { BOUNCE_END = 0, BOUNCE_NEXT = 1, BOUNCE_REHIT = 2 };
+template <bool CLEAN, int ORDER, class R>
+__device__ __forceinline__ int shade_bounce_deferred(const DevScene& S, Ray& r, bool hit, float t, uint32_t item,
+                                                     bool rehit, RGB& result, RGB& att, R& rng, uint32_t& status,
+                                                     float& rehit_tmin) {
+    constexpr bool FT = CLEAN || ORDER == 0;
+    if (!hit) {
+        if (rehit) return BOUNCE_END;
+        RGB bg = background(S, r.d);
+        result.r += att.r * bg.r;
+        result.g += att.g * bg.g;
+        result.b += att.b * bg.b;
+        return BOUNCE_END;
+    }
+    Hit h;
+    finalize_hit<FT>(S, item, t, r.o, r.d, h);
+    if ((uint32_t)h.mat >= S.num_materials) { status |= STATUS_BAD_MATERIAL; return BOUNCE_END; }
+    const int4 mi = __ldg(S.mat_i + h.mat);
+    const float4 mf = __ldg(S.mat_f + h.mat);
+    if (!rehit) {
+        bool em_alpha0;
+        const RGB em = emitted<FT>(S, r, h, mi, mf, em_alpha0, status);
+        result.r += att.r * em.r;
+        result.g += att.g * em.g;
+        result.b += att.b * em.b;
+        if (em_alpha0) {
+            rehit_tmin = h.t + 0.001f;
+            return BOUNCE_REHIT;
+        }
+    }
+    if (is_light_material(mi.x)) return BOUNCE_END;
+    scatter_bounce<CLEAN, ORDER>(S, r, h, mi, mf, att, rng, status);
+    return BOUNCE_NEXT;
 }
 
 // One camera sample: camera::ray_color (camera.cuh:149-264).  Returns the radiance of the sample.

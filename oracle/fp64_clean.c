@@ -18,7 +18,9 @@
  *   - solid / checker / image textures, constant / sky-gradient / equirectangular backgrounds.
  * All geometry and shading arithmetic is in double.  The random draws are the clean kernels' PCG32
  * draws (24-bit uniforms), so a sample starts on the same path as the kernel's and drifts away only
- * where rounding differs.  Closest hits are found by testing every primitive (small scenes only).
+ * where rounding differs.  Closest hits are found by testing every primitive, or, in scenes of more
+ * than BVH_MIN_PRIMS primitives, through a median-split bounding-volume tree of double-precision boxes
+ * (padded outward, so it finds the same closest hit; only exact-distance ties may resolve differently).
  *
  * Exported C API (ctypes, tests/oracles.py): f64_scene_create / f64_scene_destroy / f64_render.
  */
@@ -106,7 +108,19 @@ typedef struct {
     double bg[3], top[3];
     float* env;
     int env_w, env_h;
+    struct bvh_node* nodes;   /* NULL: brute force */
+    int* order;               /* leaf order of primitive indices */
 } scene_t;
+
+/* ---- bounding-volume tree (large scenes) ---------------------------------------------------------- */
+#define BVH_MIN_PRIMS 64
+#define BVH_LEAF 4
+typedef struct bvh_node {
+    double lo[3], hi[3];
+    int left, count;   /* count > 0: leaf of order[left .. left+count); else children left, left+1 */
+} bvh_node;
+
+static void bvh_create(scene_t* s);
 
 static void planar(prim_t* p, d3 q, d3 u, d3 v) {
     p->a = q;
@@ -233,12 +247,115 @@ void* f64_scene_create(const rtc_scene_desc* d) {
         s->env_w = d->background.env_width;
         s->env_h = d->background.env_height;
     }
+    bvh_create(s);
     return s;
+}
+
+static void prim_box(const prim_t* p, double lo[3], double hi[3]) {
+    d3 pts[4];
+    int n = 0;
+    if (p->kind == K_SPHERE) {
+        const double c[3] = {p->a.x, p->a.y, p->a.z};
+        for (int k = 0; k < 3; ++k) { lo[k] = c[k] - fabs(p->r); hi[k] = c[k] + fabs(p->r); }
+        return;
+    }
+    if (p->kind == K_TRI) {
+        pts[0] = p->a; pts[1] = add(p->a, p->b); pts[2] = add(p->a, p->c); n = 3;
+    } else if (p->kind == K_QUAD) {
+        pts[0] = p->a; pts[1] = add(p->a, p->b); pts[2] = add(p->a, p->c); pts[3] = add(pts[1], p->c); n = 4;
+    } else {   /* light: centred quad */
+        d3 h = add(mul(0.5, p->b), mul(0.5, p->c)), g = sub(mul(0.5, p->b), mul(0.5, p->c));
+        pts[0] = sub(p->a, h); pts[1] = add(p->a, h); pts[2] = sub(p->a, g); pts[3] = add(p->a, g); n = 4;
+    }
+    for (int k = 0; k < 3; ++k) { lo[k] = INFINITY; hi[k] = -INFINITY; }
+    for (int i = 0; i < n; ++i) {
+        const double v[3] = {pts[i].x, pts[i].y, pts[i].z};
+        for (int k = 0; k < 3; ++k) { if (v[k] < lo[k]) lo[k] = v[k]; if (v[k] > hi[k]) hi[k] = v[k]; }
+    }
+}
+
+typedef struct { double key; int idx; } keyed_t;
+static int cmp_keyed(const void* a, const void* b) {
+    const keyed_t *x = (const keyed_t*)a, *y = (const keyed_t*)b;
+    if (x->key != y->key) return x->key < y->key ? -1 : 1;
+    return x->idx < y->idx ? -1 : (x->idx > y->idx ? 1 : 0);
+}
+
+static int bvh_build(scene_t* s, double* lo, double* hi, double* cen, keyed_t* tmp, int first, int count, int* nn) {
+    const int me = (*nn)++;
+    bvh_node* nd = &s->nodes[me];
+    for (int k = 0; k < 3; ++k) { nd->lo[k] = INFINITY; nd->hi[k] = -INFINITY; }
+    double clo[3] = {INFINITY, INFINITY, INFINITY}, chi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int i = first; i < first + count; ++i) {
+        const int q = s->order[i];
+        for (int k = 0; k < 3; ++k) {
+            if (lo[3 * q + k] < nd->lo[k]) nd->lo[k] = lo[3 * q + k];
+            if (hi[3 * q + k] > nd->hi[k]) nd->hi[k] = hi[3 * q + k];
+            if (cen[3 * q + k] < clo[k]) clo[k] = cen[3 * q + k];
+            if (cen[3 * q + k] > chi[k]) chi[k] = cen[3 * q + k];
+        }
+    }
+    for (int k = 0; k < 3; ++k) {   /* outward padding: flat boxes and rounding of the slab test */
+        const double pad = 1e-9 * (fabs(nd->lo[k]) + fabs(nd->hi[k]) + 1.0);
+        nd->lo[k] -= pad;
+        nd->hi[k] += pad;
+    }
+    if (count <= BVH_LEAF) {
+        nd->left = first;
+        nd->count = count;
+        return me;
+    }
+    int axis = 0;
+    for (int k = 1; k < 3; ++k)
+        if (chi[k] - clo[k] > chi[axis] - clo[axis]) axis = k;
+    /* sort the span by centroid on the widest axis (scene creation may run on several threads at once,
+       so no global sort state) */
+    for (int i = 0; i < count; ++i) {
+        tmp[i].idx = s->order[first + i];
+        tmp[i].key = cen[3 * tmp[i].idx + axis];
+    }
+    qsort(tmp, (size_t)count, sizeof(keyed_t), cmp_keyed);
+    for (int i = 0; i < count; ++i) s->order[first + i] = tmp[i].idx;
+    const int half = count / 2;
+    nd->count = 0;
+    const int l = bvh_build(s, lo, hi, cen, tmp, first, half, nn);
+    const int r = bvh_build(s, lo, hi, cen, tmp, first + half, count - half, nn);
+    (void)l;
+    s->nodes[me].left = l;
+    s->nodes[me].count = -r;   /* children l and r */
+    return me;
+}
+
+static int g_bvh_min = BVH_MIN_PRIMS;
+/* Scenes created afterwards use the tree above `min_prims` primitives (a huge value: brute force always). */
+void f64_set_bvh_threshold(int min_prims) { g_bvh_min = min_prims; }
+
+static void bvh_create(scene_t* s) {
+    if (s->np <= g_bvh_min) return;
+    double* lo = (double*)malloc(sizeof(double) * 3 * (size_t)s->np);
+    double* hi = (double*)malloc(sizeof(double) * 3 * (size_t)s->np);
+    double* cen = (double*)malloc(sizeof(double) * 3 * (size_t)s->np);
+    s->order = (int*)malloc(sizeof(int) * (size_t)s->np);
+    s->nodes = (bvh_node*)calloc(2 * (size_t)s->np, sizeof(bvh_node));
+    for (int i = 0; i < s->np; ++i) {
+        prim_box(&s->prims[i], lo + 3 * i, hi + 3 * i);
+        for (int k = 0; k < 3; ++k) cen[3 * i + k] = 0.5 * (lo[3 * i + k] + hi[3 * i + k]);
+        s->order[i] = i;
+    }
+    keyed_t* tmp = (keyed_t*)malloc(sizeof(keyed_t) * (size_t)s->np);
+    int nn = 0;
+    bvh_build(s, lo, hi, cen, tmp, 0, s->np, &nn);
+    free(tmp);
+    free(lo);
+    free(hi);
+    free(cen);
 }
 
 void f64_scene_destroy(void* p) {
     scene_t* s = (scene_t*)p;
     if (!s) return;
+    free(s->nodes);
+    free(s->order);
     for (int i = 0; i < s->nimg; ++i) free((void*)s->img[i].px);
     free(s->img);
     free(s->prims);
@@ -308,14 +425,51 @@ static int prim_t_test(const prim_t* p, d3 o, d3 d, double tmin, double tmax, in
     }
 }
 
+static int slab(const bvh_node* nd, const double o[3], const double inv[3], double tmin, double tmax) {
+    for (int k = 0; k < 3; ++k) {
+        double t0 = (nd->lo[k] - o[k]) * inv[k], t1 = (nd->hi[k] - o[k]) * inv[k];
+        if (t0 > t1) { double x = t0; t0 = t1; t1 = x; }
+        if (t0 != t0) t0 = -INFINITY;   /* 0 * inf: the ray lies in the slab's plane */
+        if (t1 != t1) t1 = INFINITY;
+        if (t0 > tmin) tmin = t0;
+        if (t1 < tmax) tmax = t1;
+        if (tmax < tmin) return 0;
+    }
+    return 1;
+}
+
 static int closest(const scene_t* s, d3 o, d3 d, double tmin, double tmax, int hide, double* tout) {
     int best = -1;
     double bt = tmax, t;
-    for (int i = 0; i < s->np; ++i)
-        if (prim_t_test(&s->prims[i], o, d, tmin, bt, hide, &t)) {
-            bt = t;
-            best = i;
+    if (!s->nodes) {
+        for (int i = 0; i < s->np; ++i)
+            if (prim_t_test(&s->prims[i], o, d, tmin, bt, hide, &t)) {
+                bt = t;
+                best = i;
+            }
+        *tout = bt;
+        return best;
+    }
+    const double oo[3] = {o.x, o.y, o.z};
+    const double inv[3] = {1.0 / d.x, 1.0 / d.y, 1.0 / d.z};
+    int stack[128], sp = 0;
+    stack[sp++] = 0;
+    while (sp > 0) {
+        const bvh_node* nd = &s->nodes[stack[--sp]];
+        if (!slab(nd, oo, inv, tmin, bt)) continue;
+        if (nd->count > 0) {
+            for (int i = nd->left; i < nd->left + nd->count; ++i) {
+                const int q = s->order[i];
+                if (prim_t_test(&s->prims[q], o, d, tmin, bt, hide, &t)) {
+                    bt = t;
+                    best = q;
+                }
+            }
+        } else if (sp + 2 <= 128) {
+            stack[sp++] = -nd->count;
+            stack[sp++] = nd->left;
         }
+    }
     *tout = bt;
     return best;
 }

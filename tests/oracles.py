@@ -263,6 +263,10 @@ class Fp64:
         lib.f64_render.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint32, C.c_void_p,
                                    C.c_int64, C.c_void_p, C.c_int]
 
+    def set_bvh_threshold(self, min_prims: int):
+        """Scenes created afterwards search closest hits through a tree above `min_prims` primitives."""
+        self.lib.f64_set_bvh_threshold(C.c_int(min_prims))
+
     def render(self, scene: Scene, width: int, height: int, spp: int, max_depth: int, seed: int,
                pix: np.ndarray | None = None, threads: int = 0) -> np.ndarray:
         """Radiance sums (n, 3) float64 of the given frame-buffer pixels (all pixels by default)."""

@@ -87,3 +87,23 @@ def test_clean_kernel_converges_to_fp64(ctx, f64, name, mk, w, h, depth):
     print(name, "RMSE vs fp64", err, "noise floor", noise, "means", ga.mean(), ref.mean(), "stderr", se)
     assert err <= 1.2 * noise
     assert abs(ga.mean() - ref.mean()) <= 4.0 * se * np.sqrt(2.0) + 1e-9
+
+
+@pytest.mark.parametrize("name,mk", [("spheres", lambda: configs.spheres(grid=6)),
+                                     ("icosphere", lambda: configs.icosphere_scene(level=3))])
+def test_fp64_tree_finds_the_brute_force_hits(f64, name, mk):
+    """The fp64 oracle's bounding-volume tree (scenes of more than 64 primitives) changes how closest
+    hits are searched, not which are found: its image equals the brute-force search's except where an
+    exact-distance tie resolves to another primitive."""
+    scene = mk()
+    w, h, spp, depth = 24, 16, 4, 8
+    try:
+        f64.set_bvh_threshold(1 << 30)
+        brute = f64.render(scene, w, h, spp, depth, 5)
+        f64.set_bvh_threshold(64)
+        tree = f64.render(scene, w, h, spp, depth, 5)
+    finally:
+        f64.set_bvh_threshold(64)
+    same = float(np.mean(np.all(np.nan_to_num(brute, nan=-1.0) == np.nan_to_num(tree, nan=-1.0), axis=1)))
+    print(name, "identical pixels", same)
+    assert same >= 0.99
