@@ -16,7 +16,8 @@ sizes and value distributions follow the workloads the library is measured on:
                      for half the bounces, hittable_list.cuh:191-215).
 * ``meshes``       - an icosphere subdivided to 327,680 triangles, radially displaced by 3-octave value
                      noise of amplitude 0.15, four instances (metal, dielectric, lambertian, lambertian
-                     checker) = 1,310,720 triangles; a checker ground quad with a 10-unit period; a
+                     with an RGB8 image texture mapped through per-vertex texture coordinates) =
+                     1,310,720 triangles; a checker ground quad with a 10-unit period; a
                      2048x1024 FP32 equirectangular environment map (sky gradient + Gaussian sun lobe);
                      1920x1080, 128 spp, depth 16; plus a hidden 8x4 quad light above the instances, for the
                      same reason as in ``spheres``.
@@ -126,6 +127,16 @@ def displaced_icosphere(level: int, amplitude=0.15, seed=DEFAULT_SEED):
     v, f = icosphere(level)
     r = 1.0 + amplitude * value_noise(v, seed=seed)
     return (v * r[:, None]), f
+
+
+def sphere_uvs(vertices) -> np.ndarray:
+    """Per-vertex texture coordinates of a mesh around the origin: longitude and latitude of each vertex's
+    direction (u = 0.5 + atan2(z, x) / 2pi, v = 0.5 + asin(y) / pi), as float32 (n, 2)."""
+    d = np.asarray(vertices, np.float64)
+    d = d / np.linalg.norm(d, axis=1, keepdims=True)
+    u = 0.5 + np.arctan2(d[:, 2], d[:, 0]) / (2.0 * math.pi)
+    v = 0.5 + np.arcsin(np.clip(d[:, 1], -1.0, 1.0)) / math.pi
+    return np.stack([u, v], axis=1).astype(np.float32)
 
 
 def procedural_image(w: int, h: int, seed=DEFAULT_SEED):
@@ -306,10 +317,12 @@ def meshes(level=7, seed=DEFAULT_SEED, env_size=(2048, 1024), light=True) -> Sce
         s.dir_light((0.0, 8.0, 1.0), (8.0, 0.0, 0.0), (0.0, 0.0, 4.0), (4.0, 4.0, 4.0), intensity=1.0, invisible=True)
     v, f = displaced_icosphere(level, 0.15, seed)
     mats = [s.metal((0.8, 0.85, 0.9), 0.05), s.dielectric(1.5), s.lambertian((0.7, 0.3, 0.2)),
-            s.lambertian(s.checker_colors(0.25, (0.9, 0.9, 0.9), (0.1, 0.3, 0.6)))]
+            s.lambertian(s.image(procedural_image(512, 256, seed)))]
     xs = (-3.3, -1.1, 1.1, 3.3)
-    for x, m in zip(xs, mats):
-        s.mesh((v + np.array([x, 1.0, 0.0])).astype(np.float32), f, m)
+    uvs = sphere_uvs(v)
+    for k, (x, m) in enumerate(zip(xs, mats)):
+        # the fourth instance is image-textured through its per-vertex texture coordinates
+        s.mesh((v + np.array([x, 1.0, 0.0])).astype(np.float32), f, m, uvs=uvs if k == 3 else None)
     ground = s.lambertian(s.checker_colors(10.0, (0.2, 0.3, 0.1), (0.9, 0.9, 0.9)))
     s.quad((-200.0, -0.15, -200.0), (400.0, 0.0, 0.0), (0.0, 0.0, 400.0), ground)
     s.camera = Camera(look_from=(0.0, 2.5, 9.0), look_at=(0.0, 0.9, 0.0), up=(0, 1, 0), vfov=35.0,
@@ -356,6 +369,27 @@ def icosphere_scene(level=3, seed=DEFAULT_SEED) -> Scene:
     s.quad((-10.0, -0.2, -10.0), (20.0, 0.0, 0.0), (0.0, 0.0, 20.0), s.lambertian((0.5, 0.5, 0.5)))
     s.camera = Camera(look_from=(0.0, 2.5, 7.0), look_at=(0.0, 1.0, 0.0), up=(0, 1, 0), vfov=40.0, aspect=1.5,
                       aperture=0.05, focus=7.0)
+    s.set_background_constant((0.3, 0.35, 0.45))
+    return s
+
+
+def uv_mesh_scene(seed=DEFAULT_SEED) -> Scene:
+    """Image textures on triangle meshes through per-vertex texture coordinates: a displaced icosphere
+    with an RGB8 image mapped by longitude/latitude, a second one whose coordinates wrap several times
+    (values outside [0, 1) wrap as calculateTextureCoordinate does), and a metal mesh without texture
+    coordinates beside them; a floor and a quad light."""
+    s = Scene(name="uvmesh")
+    s.dir_light((0.0, 6.0, 0.0), (3.0, 0.0, 0.0), (0.0, 0.0, 3.0), (8.0, 8.0, 8.0), intensity=1.0, invisible=True)
+    v, f = displaced_icosphere(3, 0.15, seed)
+    img = s.image(procedural_image(64, 48, seed))
+    uvs = sphere_uvs(v)
+    s.mesh((v + np.array([-2.2, 1.0, 0.0])).astype(np.float32), f, s.lambertian(img), uvs=uvs)
+    s.mesh((v + np.array([0.0, 1.0, 0.0])).astype(np.float32), f, s.lambertian(img),
+           uvs=(uvs * np.float32(3.0) - np.float32(1.25)).astype(np.float32))
+    s.mesh((v + np.array([2.2, 1.0, 0.0])).astype(np.float32), f, s.metal((0.8, 0.8, 0.9), 0.1))
+    s.quad((-10.0, -0.2, -10.0), (20.0, 0.0, 0.0), (0.0, 0.0, 20.0), s.lambertian((0.5, 0.5, 0.5)))
+    s.camera = Camera(look_from=(0.0, 2.5, 7.0), look_at=(0.0, 1.0, 0.0), up=(0, 1, 0), vfov=40.0, aspect=1.5,
+                      aperture=0.0, focus=7.0)
     s.set_background_constant((0.3, 0.35, 0.45))
     return s
 
@@ -459,6 +493,7 @@ SCENES = {
     "textured": (textured, lambda **kw: RenderParams(**{**dict(width=160, height=120, spp=16, max_depth=10), **kw})),
     "icosphere": (icosphere_scene, lambda **kw: RenderParams(**{**dict(width=150, height=100, spp=16, max_depth=12), **kw})),
     "lights": (lights_scene, lambda **kw: RenderParams(**{**dict(width=120, height=90, spp=16, max_depth=10), **kw})),
+    "uvmesh": (uv_mesh_scene, lambda **kw: RenderParams(**{**dict(width=120, height=80, spp=16, max_depth=10), **kw})),
     # boxes and transforms; "xforms" leaves out the multi-axis rotations the reference clips (see
     # transforms_scene), so the reference's own build renders it exactly
     "xforms": (lambda seed=DEFAULT_SEED: transforms_scene(seed, multi_axis=False), transforms_params),

@@ -85,7 +85,7 @@ extern "C" rtc_status rtc_render_noalloc(const rtc_scene* scene, const rtc_rende
     cudaStream_t st = (cudaStream_t)stream;
     uint32_t* d_status = (uint32_t*)base;
     rtc::WfBuffers B;
-    if (NOALLOC_HEADER_BYTES + rtc_carve_wavefront((uint8_t*)base + NOALLOC_HEADER_BYTES, (uint32_t)npix, B, false) >
+    if (NOALLOC_HEADER_BYTES + rtc_carve_wavefront((uint8_t*)base + NOALLOC_HEADER_BYTES, (uint32_t)npix, B) >
         NOALLOC_SCRATCH_BYTES)
         return rtc_set_error(RTC_ERR_INVALID_ARGUMENT, "path state does not fit the static scratch");
     e = cudaMemsetAsync(d_status, 0, sizeof(uint32_t), st);

@@ -446,6 +446,9 @@ rtc_status rtc_build_host_scene(const rtc_scene_desc* d, HostScene& H, uint32_t 
         uint32_t t = 0;
         for (uint32_t m = 0; m < d->num_meshes; ++m) {
             const rtc_mesh& M = d->meshes[m];
+            if (M.uvs)
+                for (uint32_t k = 0; k < 2 * M.num_vertices; ++k)
+                    if (!std::isfinite(M.uvs[k])) return bad("mesh " + std::to_string(m) + " texture coordinate is not finite");
             for (uint32_t f = 0; f < M.num_triangles; ++f, ++t) {
                 uint32_t ia = M.indices[3 * f], ib = M.indices[3 * f + 1], ic = M.indices[3 * f + 2];
                 if (ia >= M.num_vertices || ib >= M.num_vertices || ic >= M.num_vertices)
@@ -549,7 +552,11 @@ rtc_status rtc_build_host_scene(const rtc_scene_desc* d, HostScene& H, uint32_t 
 
     // ---- per-kind arrays in leaf order ---------------------------------------------------------
     std::vector<uint32_t> items(bvh.order.size()), xitems(xbvh.order.size());
-    std::vector<float4> sph, tri, tri_n, tri_vn, quad, light(6 * (size_t)nlights), rect, xf;
+    std::vector<float4> sph, tri, tri_n, tri_vn, tri_uv, quad, light(6 * (size_t)nlights), rect, xf;
+    // per-vertex texture coordinates: when any mesh has them, every triangle gets a uv record (zeros
+    // for meshes without)
+    bool any_uv = false;
+    for (uint32_t m = 0; m < d->num_meshes; ++m) any_uv = any_uv || d->meshes[m].uvs != nullptr;
     std::vector<int2> sph_aux;
     std::vector<int4> xprim;
     // global id bases: the lights come first, in light-list order (index = light id = global id); one id
@@ -632,6 +639,12 @@ rtc_status rtc_build_host_scene(const rtc_scene_desc* d, HostScene& H, uint32_t 
         tri.push_back(make_float4(e1.x, e1.y, e1.z, ibits((int32_t)(base_tri + src))));
         tri.push_back(make_float4(e2.x, e2.y, e2.z, ibits(smooth_slot)));
         tri_n.push_back(make_float4(mn.x, mn.y, mn.z, 0.0f));
+        if (any_uv) {
+            const float* t = M.uvs;
+            auto uv = [t](uint32_t vi, int k) { return t ? t[2 * vi + k] : 0.0f; };
+            tri_uv.push_back(make_float4(uv(ia, 0), uv(ia, 1), uv(ib, 0), uv(ib, 1)));
+            tri_uv.push_back(make_float4(uv(ic, 0), uv(ic, 1), 0.0f, 0.0f));
+        }
         return typed;
     };
     for (size_t k = 0; k < bvh.order.size() + xbvh.order.size(); ++k) {
@@ -688,6 +701,7 @@ rtc_status rtc_build_host_scene(const rtc_scene_desc* d, HostScene& H, uint32_t 
     size_t o_tri = add_chunk(tri.data(), tri.size() * 16);
     size_t o_trin = add_chunk(tri_n.data(), tri_n.size() * 16);
     size_t o_trivn = add_chunk(tri_vn.data(), tri_vn.size() * 16);
+    size_t o_triuv = add_chunk(tri_uv.data(), tri_uv.size() * 16);
     size_t o_quad = add_chunk(quad.data(), quad.size() * 16);
     size_t o_light = add_chunk(light.data(), light.size() * 16);
     size_t o_mi = add_chunk(mat_i.data(), mat_i.size() * 16);
@@ -720,6 +734,7 @@ rtc_status rtc_build_host_scene(const rtc_scene_desc* d, HostScene& H, uint32_t 
     D.tri = (const float4*)off(o_tri);
     D.tri_n = (const float4*)off(o_trin);
     D.tri_vn = (const float4*)off(o_trivn);
+    D.tri_uv = tri_uv.empty() ? nullptr : (const float4*)off(o_triuv);
     D.quad = (const float4*)off(o_quad);
     D.light = (const float4*)off(o_light);
     D.mat_i = (const int4*)off(o_mi);
@@ -780,6 +795,7 @@ DevScene rtc_rebase_scene(const HostScene& H, uint8_t* base) {
     rb(D.xprim); rb(D.xf); rb(D.rect);
     if (D.xnodes) { rb(D.xnodes); rb(D.xitems); }
     if (D.bg.env) rb(D.bg.env);
+    if (D.tri_uv) rb(D.tri_uv);
     return D;
 }
 
@@ -885,14 +901,13 @@ void rtc_carve_groups(void* base, const rtc_render_params* p, float4** part, uin
 
 namespace {
 
-// Bytes of wavefront scratch per path slot (with the shade bins).
-constexpr size_t WF_SLOT_BYTES =
-    5 * sizeof(float4) + 2 * sizeof(uint4) + sizeof(float2) + 3 * sizeof(uint32_t) + WF_BINS * sizeof(uint32_t);
+// Bytes of wavefront scratch per path slot.
+constexpr size_t WF_SLOT_BYTES = 5 * sizeof(float4) + 2 * sizeof(uint4) + sizeof(float2) + 3 * sizeof(uint32_t);
 constexpr uint32_t WF_MAX_SLOTS = 1u << 22;   // 4,194,304 slots = 432 MiB of path state
 
 // Lays out the wavefront buffers for `slots` path slots in one block of device memory at `base`
-// (the context's scratch, or the allocation-free entry point's static array, which has no bins).
-size_t carve_wavefront(void* base, uint32_t slots, WfBuffers& B, bool bins = true) {
+// (the context's scratch, or the allocation-free entry point's static array).
+size_t carve_wavefront(void* base, uint32_t slots, WfBuffers& B) {
     uint8_t* p = (uint8_t*)base;
     auto take = [&](size_t bytes) {
         uint8_t* r = p;
@@ -911,22 +926,21 @@ size_t carve_wavefront(void* base, uint32_t slots, WfBuffers& B, bool bins = tru
     B.queue[0] = (uint32_t*)take(n * 4);
     B.queue[1] = (uint32_t*)take(n * 4);
     B.queue[2] = (uint32_t*)take(n * 4);
-    B.bins = bins ? (uint32_t*)take(n * 4 * WF_BINS) : nullptr;
     B.ctr = (uint32_t*)take(WF_CTR_N * 4);
     B.slots = slots;
     return (size_t)(p - (uint8_t*)base);
 }
 
 // Bytes carve_wavefront lays out for `slots` slots (each buffer rounded up to 256 bytes).
-constexpr size_t wavefront_bytes(size_t n, bool bins) {
+constexpr size_t wavefront_bytes(size_t n) {
     return 7 * ((n * 16 + 255) & ~(size_t)255) + ((n * 8 + 255) & ~(size_t)255) + 3 * ((n * 4 + 255) & ~(size_t)255) +
-           (bins ? ((n * 4 * WF_BINS + 255) & ~(size_t)255) : 0) + ((WF_CTR_N * 4 + 255) & ~(size_t)255);
+           ((WF_CTR_N * 4 + 255) & ~(size_t)255);
 }
 // The allocation-free render's advertised cap fits its 64 MiB array behind a 256-byte status header
 // (render_noalloc.cu), so an image at or under RTC_NOALLOC_MAX_PIXELS never fails for lack of room.
-static_assert(256 + wavefront_bytes(RTC_NOALLOC_MAX_PIXELS, false) <= (size_t(64) << 20),
+static_assert(256 + wavefront_bytes(RTC_NOALLOC_MAX_PIXELS) <= (size_t(64) << 20),
               "RTC_NOALLOC_MAX_PIXELS slots do not fit the allocation-free render's static array");
-static_assert(wavefront_bytes(1, true) <= WF_SLOT_BYTES + 13 * 256, "wavefront layout grew past WF_SLOT_BYTES");
+static_assert(wavefront_bytes(1) <= WF_SLOT_BYTES + 12 * 256, "wavefront layout grew past WF_SLOT_BYTES");
 
 rtc_status ensure_wavefront(rtc_context* c, uint32_t slots, WfBuffers& B) {
     if (c->wf_cap < slots) {
@@ -945,9 +959,7 @@ rtc_status ensure_wavefront(rtc_context* c, uint32_t slots, WfBuffers& B) {
         for (cudaEvent_t& e : c->split_ev) RTC_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         RTC_CUDA(cudaStreamCreateWithFlags(&c->stream_long, cudaStreamNonBlocking));
     }
-    // shade bins (material-sorted shading) unless RTC_WF_BINS=0
-    const char* eb = std::getenv("RTC_WF_BINS");
-    carve_wavefront(c->d_wf, slots, B, !(eb && std::atoi(eb) == 0));
+    carve_wavefront(c->d_wf, slots, B);
     return RTC_OK;
 }
 
@@ -1204,9 +1216,7 @@ rtc_status launch_wavefront(rtc_context* c, const rtc_scene* s, const rtc_render
 
 // ---- internal helpers shared with render_noalloc.cu (rtc_internal.h) ----
 size_t rtc_wf_slot_bytes() { return WF_SLOT_BYTES; }
-size_t rtc_carve_wavefront(void* base, uint32_t slots, WfBuffers& B, bool bins) {
-    return carve_wavefront(base, slots, B, bins);
-}
+size_t rtc_carve_wavefront(void* base, uint32_t slots, WfBuffers& B) { return carve_wavefront(base, slots, B); }
 rtc_status rtc_set_error(rtc_status s, const char* msg) { return fail(s, msg); }
 rtc_status rtc_check_render_params(const rtc_render_params* p) { return check_params(p); }
 int rtc_scene_device(const rtc_scene* s) { return s->device; }

@@ -27,6 +27,7 @@
 //                                                               48 B / triangle test (leaf order)
 //   tri_n      float4 (middle_normal.xyz, -)                    fetched once per final hit only
 //   tri_vn     3 x float4 vertex normals (unit_vector'd) for smooth triangles
+//   tri_uv     2 x float4 per triangle, only when a mesh has texture coordinates: (uv0.xy, uv1.xy) (uv2.xy, -)
 //   quad       5 x float4: (n.xyz, D) (Q.xyz, mat) (u.xyz, gid) (v.xyz, -) (w.xyz, -)
 //   light      6 x float4 per light, in light-list order (omni, directional, spot lights):
 //              directional (quad): (n.xyz, D) (P.xyz, mat) (u.xyz, gid) (v.xyz, invisible) (w.xyz, area)
@@ -106,6 +107,7 @@ struct DevScene {
     const float4* tri;
     const float4* tri_n;
     const float4* tri_vn;
+    const float4* tri_uv;      // null, or 2 x float4 per triangle: (uv0, uv1) (uv2, -) in leaf order
     const float4* quad;
     const float4* light;
     const int4* mat_i;
@@ -158,17 +160,9 @@ struct WfBuffers {
     uint4* pcg;        // clean mode: PCG32 state (lo, hi) and increment (lo, hi)
     float2* hit;       // t, item bits (0xffffffff = miss)
     uint32_t* queue[3];   // [0], [1]: the alternating slot queues; [2]: slots split off as long chains
-    uint32_t* bins;    // null, or WF_BINS arrays of `slots` entries: the extend kernel sorts the slots it
-                       // traced by the class of the hit's material (WfBin), so each shade warp runs one
-                       // material's code; without bins the shade kernel reads the queue in place
-    uint32_t* ctr;     // [0..2] queue sizes (rotating), [3] next pixel to fetch, [4] long-chain queue size,
-                       // [WF_BIN_CTR ..) the bin sizes, two sets used by alternate iterations (WfCtr)
+    uint32_t* ctr;     // [0..2] queue sizes (rotating), [3] next pixel to fetch, [4] long-chain queue size
     uint32_t slots;
 };
-
-// Material classes of the shade bins: what the traced ray found.
-enum WfBin { WF_BIN_MISS = 0, WF_BIN_LAMBERT = 1, WF_BIN_METAL = 2, WF_BIN_DIELECTRIC = 3, WF_BIN_OTHER = 4,
-             WF_BINS = 5 };
 
 constexpr uint32_t WF_IDLE = 0xffffffffu;
 constexpr int WF_MAX_DEPTH = 0xffff;
@@ -217,10 +211,8 @@ struct WfTableArgs {           // a ring of jobs
 };
 
 // Iteration k reads queue (k & 1) with size ctr[k % 3], appends to queue ((k+1) & 1) counted in
-// ctr[(k+1) % 3] and clears ctr[(k+2) % 3], which iteration k+1 appends to.  With bins, iteration k's
-// extend appends to bin set (k & 1), its shade reads that set and clears set ((k+1) & 1) for the next
-// extend (a split pass in place of iteration k clears it too).
-enum WfCtr { WF_NEXT_PIXEL = 3, WF_LONG = 4, WF_BIN_CTR = 5, WF_CTR_N = WF_BIN_CTR + 2 * WF_BINS };
+// ctr[(k+1) % 3] and clears ctr[(k+2) % 3], which iteration k+1 appends to.
+enum WfCtr { WF_NEXT_PIXEL = 3, WF_LONG = 4, WF_CTR_N = 5 };
 struct WfIter {
     int qin, cin, cout, czero;
 };

@@ -35,7 +35,7 @@ private:
 
 // bytes of wavefront scratch per path slot, and the layout of `slots` slots starting at `base`
 size_t rtc_wf_slot_bytes();
-size_t rtc_carve_wavefront(void* base, uint32_t slots, rtc::WfBuffers& B, bool bins = true);
+size_t rtc_carve_wavefront(void* base, uint32_t slots, rtc::WfBuffers& B);
 // records an error message for rtc_last_error_string() and returns `s`
 rtc_status rtc_set_error(rtc_status s, const char* msg);
 rtc_status rtc_check_render_params(const rtc_render_params* p);

@@ -740,12 +740,14 @@ rtc_status read_file(rtc_scene_file& F, const char* path, uint32_t flags, rtc_im
         if (px) F.pixels.emplace_back(px, std::free);
         return px;
     };
-    auto obj = [&](const char* fp, std::vector<float>& v, std::vector<uint32_t>& idx, std::vector<float>& nrm) -> bool {
+    auto obj = [&](const char* fp, std::vector<float>& v, std::vector<uint32_t>& idx, std::vector<float>& nrm,
+                   std::vector<float>& uv) -> bool {
         rtc_obj_mesh m{};
         if (rtc_load_obj(fp, &m) != RTC_OK) return false;
         v.assign(m.vertices, m.vertices + 3 * (size_t)m.num_vertices);
         idx.assign(m.indices, m.indices + 3 * (size_t)m.num_triangles);
         if (m.normals) nrm.assign(m.normals, m.normals + 3 * (size_t)m.num_vertices);
+        if (m.uvs) uv.assign(m.uvs, m.uvs + 2 * (size_t)m.num_vertices);
         rtc_free_obj(&m);
         return true;
     };

@@ -702,10 +702,32 @@ __device__ __forceinline__ void finalize_prim(const DevScene& S, uint32_t kind, 
             normal = add(add(mul(bu, v3(__ldg(vn + 1))), mul(bv, v3(__ldg(vn + 2)))), mul(bc, v3(__ldg(vn))));
         }
         set_face_normal(h, d, normal);
-        // triangles carry no texture coordinates here: get_triangle_uv over all-zero vertex uvs gives
-        // (0, 0) (uvmapping.cuh:415-447)
-        h.u = 0.0f;
-        h.v = 0.0f;
+        if (S.tri_uv) {
+            // get_triangle_uv (uvmapping.cuh:415-429) at this hit's point: get_barycenter's barycentrics
+            // (math_utils.cuh:73-86) over v0, v1 = v0 + e1, v2 = v0 + e2, then calculateTextureCoordinate
+            // (uvmapping.cuh:435-447) with its wrap into [0, 1).  The reference passes the hit record's
+            // previous hit point (triangle.cuh:162), which depends on the BVH's visit order; this uses
+            // the hit's own.
+            const V3 e1 = v3(a1.x, a1.y, a1.z), e2 = v3(a2.x, a2.y, a2.z), p2 = sub(h.p, v3(a0.x, a0.y, a0.z));
+            const float d00 = dot(e1, e1), d01 = dot(e1, e2), d11 = dot(e2, e2), d20 = dot(p2, e1), d21 = dot(p2, e2);
+            const float denom = d00 * d11 - d01 * d01;
+            const float bv = (d11 * d20 - d01 * d21) / denom;
+            const float bw = (d00 * d21 - d01 * d20) / denom;
+            const float bu = 1.0f - bv - bw;
+            const float4 t0 = __ldg(S.tri_uv + 2 * (size_t)idx), t1 = __ldg(S.tri_uv + 2 * (size_t)idx + 1);
+            float tu = bu * t0.x + bv * t0.z + (1.0f - bu - bv) * t1.x;
+            float tv = bu * t0.y + bv * t0.w + (1.0f - bu - bv) * t1.y;
+            tu = fmodf(tu, 1.0f);
+            tv = fmodf(tv, 1.0f);
+            if (tu < 0.0f) tu += 1.0f;
+            if (tv < 0.0f) tv += 1.0f;
+            h.u = tu;
+            h.v = tv;
+        } else {
+            // no mesh has texture coordinates: get_triangle_uv over all-zero vertex uvs gives (0, 0)
+            h.u = 0.0f;
+            h.v = 0.0f;
+        }
     } break;
     }
 }

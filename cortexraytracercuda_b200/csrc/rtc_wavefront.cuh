@@ -54,23 +54,6 @@ inline namespace RTC_XP_NS {
 // the shade kernel hands back to the extend kernel (camera.cuh:177-183).
 __device__ __forceinline__ float wf_tmin(float4 d) { return d.w > 0.0f ? d.w : 0.00001f; }
 
-// The shade bin of a traced ray: miss, or the class of the hit primitive's material (the record's
-// material field; transformed primitives and unknown materials go to WF_BIN_OTHER).
-__device__ __forceinline__ uint32_t wf_bin_of(const DevScene& S, bool hit, uint32_t it) {
-    if (!hit) return WF_BIN_MISS;
-    const uint32_t kind = it >> ITEM_KIND_SHIFT, idx = it & ITEM_INDEX_MASK;
-    int m;
-    switch (kind) {
-    case ITEM_SPHERE: m = __ldg(S.sph_aux + idx).x; break;
-    case ITEM_TRI: m = __float_as_int(__ldg(S.tri + 3 * (size_t)idx).w); break;
-    case ITEM_QUAD: m = __float_as_int(__ldg(S.quad + 5 * (size_t)idx + 1).w); break;
-    default: return WF_BIN_OTHER;   // lights, xprims
-    }
-    if ((uint32_t)m >= S.num_materials) return WF_BIN_OTHER;
-    const int k = __ldg(&S.mat_i[m].x);
-    return k == 0 ? WF_BIN_LAMBERT : k == 1 ? WF_BIN_METAL : k == 2 ? WF_BIN_DIELECTRIC : WF_BIN_OTHER;
-}
-
 // Appends `slot` to queue `q` when `pred`; every active lane of the warp must call it together.
 __device__ __forceinline__ void wf_push(uint32_t* q, uint32_t* cnt, uint32_t slot, bool pred) {
     const unsigned act = __activemask();
@@ -316,28 +299,20 @@ __global__ void RTC_EXTEND_BOUNDS wf_extend(J jobs, WfBuffers B, WfIter w, unsig
     const uint32_t n = B.ctr[w.cin];
     if (blockIdx.x == 0 && threadIdx.x == 0) B.ctr[w.czero] = 0u;
     const uint32_t* q = B.queue[w.qin];
-    uint32_t* bctr = B.ctr + WF_BIN_CTR + WF_BINS * w.qin;
     TraceStats st{0, 0};
     uint32_t status = 0, rays = 0;
     const uint32_t stride = gridDim.x * blockDim.x;
-    const uint32_t limit = B.bins ? (n + 31u) & ~31u : n;   // whole warps reach the bin appends together
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < limit; k += stride) {
-        uint32_t slot = 0, bin = WF_BINS;
-        if (k < n) {
-            slot = __ldcs(q + k);
-            const float4 o = __ldcs(B.ray_o + slot), d = __ldcs(B.ray_d + slot);
-            const uint32_t mw = __ldcs(&B.meta[slot].w);
-            const uint32_t job = wf_job(mw);
-            float t;
-            uint32_t item;
-            bool h = closest_hit<FLAVOR == 2, WIDE>(jobs.scene(job), v3(o), v3(d), wf_tmin(d), 3.402823466e+38f,
-                                              wf_depth(mw) == (uint32_t)jobs.params(job).max_depth, t, item, st, status);
-            B.hit[slot] = make_float2(t, __uint_as_float(h ? item : 0xffffffffu));
-            if (B.bins) bin = wf_bin_of(jobs.scene(job), h, item);
-            ++rays;
-        }
-        if (B.bins)
-            for (uint32_t c = 0; c < WF_BINS; ++c) wf_push(B.bins + (size_t)c * B.slots, bctr + c, slot, bin == c);
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
+        const uint32_t slot = __ldcs(q + k);
+        const float4 o = __ldcs(B.ray_o + slot), d = __ldcs(B.ray_d + slot);
+        const uint32_t mw = __ldcs(&B.meta[slot].w);
+        const uint32_t job = wf_job(mw);
+        float t;
+        uint32_t item;
+        bool h = closest_hit<FLAVOR == 2, WIDE>(jobs.scene(job), v3(o), v3(d), wf_tmin(d), 3.402823466e+38f,
+                                          wf_depth(mw) == (uint32_t)jobs.params(job).max_depth, t, item, st, status);
+        B.hit[slot] = make_float2(t, __uint_as_float(h ? item : 0xffffffffu));
+        ++rays;
     }
     if (COUNT && counters) {
         unsigned long long r = rays, nn = st.nodes, pp = st.prims;
@@ -458,18 +433,6 @@ __global__ void RTC_SHADE_BOUNDS wf_shade(J jobs, WfBuffers B, WfIter w, unsigne
     const uint32_t* q = B.queue[w.qin];
     uint32_t* qn = B.queue[w.qin ^ 1];
     uint32_t* cn = B.ctr + w.cout;
-    // with bins: the traced slots sorted by material class, read as one sequence bin after bin (the
-    // bins' ends in shared memory, so the lookup holds no registers across the shading)
-    __shared__ uint32_t bend[WF_BINS];
-    if (B.bins) {
-        if (threadIdx.x == 0) {
-            const uint32_t* bctr = B.ctr + WF_BIN_CTR + WF_BINS * w.qin;
-            uint32_t acc = 0;
-            for (int c = 0; c < WF_BINS; ++c) bend[c] = acc += bctr[c];
-        }
-        if (blockIdx.x == 0 && threadIdx.x < WF_BINS) B.ctr[WF_BIN_CTR + WF_BINS * (w.qin ^ 1) + threadIdx.x] = 0u;
-        __syncthreads();
-    }
     uint32_t status = 0, paths = 0;
     PathCounters pc{0, 0, 0};
     TraceStats st{0, 0};
@@ -479,13 +442,7 @@ __global__ void RTC_SHADE_BOUNDS wf_shade(J jobs, WfBuffers B, WfIter w, unsigne
         bool live = false;
         uint32_t slot = 0;
         if (k < n) {
-            if (B.bins) {
-                uint32_t c = 0, first = 0;
-                while (c + 1 < WF_BINS && k >= bend[c]) first = bend[c++];
-                slot = __ldcs(B.bins + (size_t)c * B.slots + (k - first));
-            } else {
-                slot = __ldcs(q + k);
-            }
+            slot = __ldcs(q + k);
             const float2 hv = __ldcs(B.hit + slot);
             live = wf_step<CLEAN, ORDER>(jobs, win, B, slot, hv.x, __float_as_uint(hv.y), pc, st, paths, status);
         }
@@ -543,7 +500,6 @@ template <bool CLEAN, class J>
 __global__ void __launch_bounds__(128) wf_split(J jobs, WfBuffers B, WfIter w, float k0, float threshold) {
     const uint32_t n = B.ctr[w.cin];
     if (blockIdx.x == 0 && threadIdx.x == 0) B.ctr[w.czero] = 0u;   // appended to by the next iteration
-    if (blockIdx.x == 0 && threadIdx.x < WF_BINS) B.ctr[WF_BIN_CTR + WF_BINS * (w.qin ^ 1) + threadIdx.x] = 0u;
     const uint32_t* q = B.queue[w.qin];
     uint32_t* qn = B.queue[w.qin ^ 1];
     uint32_t* cn = B.ctr + w.cout;

@@ -44,12 +44,14 @@ void launchGPU(const sceneConfig& cfg, int width, int height, int spp, int max_d
         return px;
     };
     // OBJ meshes: the library's reader (rtc_load_obj), in place of tinyobjloader (mesh_loader.cuh)
-    auto load_obj = [](const char* path, std::vector<float>& v, std::vector<uint32_t>& idx, std::vector<float>& n) {
+    auto load_obj = [](const char* path, std::vector<float>& v, std::vector<uint32_t>& idx, std::vector<float>& n,
+                       std::vector<float>& uv) {
         rtc_obj_mesh m;
         if (rtc_load_obj(path, &m) != RTC_OK) return false;
         v.assign(m.vertices, m.vertices + 3 * (size_t)m.num_vertices);
         idx.assign(m.indices, m.indices + 3 * (size_t)m.num_triangles);
         if (m.normals) n.assign(m.normals, m.normals + 3 * (size_t)m.num_vertices);
+        if (m.uvs) uv.assign(m.uvs, m.uvs + 2 * (size_t)m.num_vertices);
         rtc_free_obj(&m);
         return true;
     };

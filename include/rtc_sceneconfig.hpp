@@ -15,7 +15,8 @@
 // keep their rt::transform as scene_factory::applyTransform applies it; OBJ meshes take their
 // `position` as a vertex offset and their transform too, where the reference's createObjMesh drops both
 // (scene_factory.cuh createObjMesh) and renders meshes[0] for every entry (gpu.cu:628); the flag
-// REFERENCE_MESHES reproduces the reference there.  Primitives the
+// REFERENCE_MESHES reproduces the reference there, including its texture-coordinate read with a stride
+// of 3 (mesh_loader.cuh:370-371).  Primitives the
 // B200 path does not cover (planes, cones, cylinders, disks, tori, volumes) are reported in `skipped`.
 // Image textures need decoded RGB8 pixels: pass `load_image(filepath, &w, &h)` returning a pointer
 // that stays valid while the description is used (the reference decodes with stbi_load, gpu.cu:1743).
@@ -44,7 +45,7 @@ struct SceneHolder {
     std::vector<rtc_transform> transforms;
     std::vector<uint32_t> sphere_transforms, quad_transforms, mesh_transforms;   // 1-based, 0 = none
     // geometry of the OBJ meshes (owned here; rtc_mesh points into it)
-    std::vector<std::vector<float>> mesh_vertices, mesh_normals;
+    std::vector<std::vector<float>> mesh_vertices, mesh_normals, mesh_uvs;
     std::vector<std::vector<uint32_t>> mesh_indices;
     std::vector<std::string> skipped;
     rtc_scene_desc desc{};
@@ -70,6 +71,7 @@ struct SceneHolder {
             meshes[i].vertices = mesh_vertices[i].data();
             meshes[i].indices = mesh_indices[i].data();
             meshes[i].normals = mesh_normals[i].empty() ? nullptr : mesh_normals[i].data();
+            meshes[i].uvs = mesh_uvs[i].empty() ? nullptr : mesh_uvs[i].data();
         }
         desc.meshes = meshes.data();
         desc.num_meshes = (uint32_t)meshes.size();
@@ -85,11 +87,12 @@ struct SceneHolder {
 };
 
 using ImageLoader = std::function<const uint8_t*(const char* filepath, int* width, int* height)>;
-// Reads an OBJ file's triangles: positions (3 per vertex), indices (3 per triangle) and per-vertex
-// normals (3 per vertex, or left empty); returns false when the file cannot be read.  With this
-// library, a wrapper around rtc_load_obj / rtc_free_obj.
+// Reads an OBJ file's triangles: positions (3 per vertex), indices (3 per triangle), per-vertex
+// normals (3 per vertex, or left empty) and per-vertex texture coordinates (2 per vertex, or left
+// empty); returns false when the file cannot be read.  With this library, a wrapper around
+// rtc_load_obj / rtc_free_obj.
 using ObjLoader = std::function<bool(const char* filepath, std::vector<float>& vertices, std::vector<uint32_t>& indices,
-                                     std::vector<float>& normals)>;
+                                     std::vector<float>& normals, std::vector<float>& uvs)>;
 
 namespace detail {
 inline bool same(const char* a, const char* b) { return a && b && std::strcmp(a, b) == 0; }
@@ -284,9 +287,9 @@ const rtc_scene_desc* from_sceneconfig(const SceneConfig& cfg, SceneHolder& out,
         if (!load_obj) { out.skipped.push_back(std::string("OBJ mesh without loader: ") + (g.filepath ? g.filepath : "")); continue; }
         const int mat = fetch_material(m.materialName);
         if (mat < 0) continue;
-        std::vector<float> v, n;
+        std::vector<float> v, n, t;
         std::vector<uint32_t> idx;
-        if (!g.filepath || !load_obj(g.filepath, v, idx, n) || idx.empty()) {
+        if (!g.filepath || !load_obj(g.filepath, v, idx, n, t) || idx.empty()) {
             out.skipped.push_back(std::string("OBJ mesh not loaded: ") + (g.filepath ? g.filepath : ""));
             continue;
         }
@@ -306,6 +309,17 @@ const rtc_scene_desc* from_sceneconfig(const SceneConfig& cfg, SceneHolder& out,
         out.mesh_vertices.push_back(std::move(v));
         out.mesh_indices.push_back(std::move(idx));
         out.mesh_normals.push_back(r.smooth ? std::move(n) : std::vector<float>());
+        if (t.size() != 2 * (size_t)r.num_vertices) t.clear();
+        if (ref_meshes && !t.empty()) {
+            // mesh_loader reads texcoords[3 * idx + 0], [3 * idx + 1] from an array of 2 per vertex
+            // (mesh_loader.cuh:370-371); reads past its end - undefined memory there - give 0 here
+            std::vector<float> r3(t.size(), 0.0f);
+            for (size_t k = 0; k < r.num_vertices; ++k)
+                for (size_t c = 0; c < 2; ++c)
+                    if (3 * k + c < t.size()) r3[2 * k + c] = t[3 * k + c];
+            t.swap(r3);
+        }
+        out.mesh_uvs.push_back(std::move(t));
         out.meshes.push_back(r);
         out.mesh_transforms.push_back(ref_meshes ? 0u : add_transform(m.transform, out));
     }

@@ -88,6 +88,7 @@ typedef struct {
     int invisible;       /* lights */
     int smooth;
     d3 vn[3];
+    double uv[6];        /* triangle: per-vertex texture coordinates (zeros without) */
 } prim_t;
 typedef struct { int kind; double col[3]; double inv_scale; int even, odd, image; } tex_t;
 typedef struct { int kind; int tex; double fuzz, ior, intensity; int directional; } mat_t;
@@ -220,6 +221,13 @@ void* f64_scene_create(const rtc_scene_desc* d) {
                 p->vn[0] = unit(Dp(M->normals + 3 * ia));
                 p->vn[1] = unit(Dp(M->normals + 3 * ib));
                 p->vn[2] = unit(Dp(M->normals + 3 * ic));
+            }
+            if (M->uvs) {
+                const uint32_t vi[3] = {ia, ib, ic};
+                for (int q = 0; q < 3; ++q) {
+                    p->uv[2 * q] = M->uvs[2 * vi[q]];
+                    p->uv[2 * q + 1] = M->uvs[2 * vi[q] + 1];
+                }
             }
         }
     }
@@ -501,7 +509,16 @@ static void finalize(const scene_t* s, int pi, double t, d3 o, d3 d, hit_t* h) {
             double bu = dot(tv, pv) * inv, bv = dot(d, cross(tv, p->b)) * inv, bc = 1.0 - bu - bv;
             outward = add(add(mul(bu, p->vn[1]), mul(bv, p->vn[2])), mul(bc, p->vn[0]));
         }
-        h->u = h->v = 0.0;
+        /* get_triangle_uv at the hit point (barycentric interpolation of the vertex uvs, wrapped into
+           [0, 1): math_utils.cuh:73-86, uvmapping.cuh:415-447) */
+        d3 p2 = sub(h->p, p->a);
+        double d00 = dot(p->b, p->b), d01 = dot(p->b, p->c), d11 = dot(p->c, p->c);
+        double d20 = dot(p2, p->b), d21 = dot(p2, p->c), den = d00 * d11 - d01 * d01;
+        double bv = (d11 * d20 - d01 * d21) / den, bw = (d00 * d21 - d01 * d20) / den, bu = 1.0 - bv - bw;
+        double tu = fmod(bu * p->uv[0] + bv * p->uv[2] + bw * p->uv[4], 1.0);
+        double tv = fmod(bu * p->uv[1] + bv * p->uv[3] + bw * p->uv[5], 1.0);
+        h->u = tu < 0.0 ? tu + 1.0 : tu;
+        h->v = tv < 0.0 ? tv + 1.0 : tv;
     }
     h->front = dot(d, outward) < 0.0;
     h->n = h->front ? outward : neg(outward);

@@ -124,6 +124,7 @@ typedef struct {
     float D, area;
     v3 mid;           /* triangle middle_normal */
     int smooth; v3 vn[3];
+    float uv[6];      /* triangle: per-vertex texture coordinates (zeros without) */
     float lo[3], hi[3];
     int xf;           /* transform index or -1 (rt::translate / rotate / scale around the primitive) */
     int gid;          /* global object id (one per box) */
@@ -156,6 +157,7 @@ typedef struct {
     rtc_camera cam;
     rtc_background bg;
     float* env;
+    int any_uv;           /* a mesh has texture coordinates: triangles evaluate them at the hit */
 } scene_t;
 
 static void box_grow(float* lo, float* hi, v3 p) {
@@ -418,6 +420,11 @@ void* port_scene_create(const rtc_scene_desc* d) {
                 p->vn[0] = vunit(Vp(M->normals + 3 * ia)); p->vn[1] = vunit(Vp(M->normals + 3 * ib));
                 p->vn[2] = vunit(Vp(M->normals + 3 * ic));
             }
+            if (M->uvs) {
+                const uint32_t vi[3] = {ia, ib, ic};
+                for (int q = 0; q < 3; ++q) { p->uv[2 * q] = M->uvs[2 * vi[q]]; p->uv[2 * q + 1] = M->uvs[2 * vi[q] + 1]; }
+                s->any_uv = 1;
+            }
             for (int q = 0; q < 3; ++q) { p->lo[q] = FLT_MAX; p->hi[q] = -FLT_MAX; }
             box_grow(p->lo, p->hi, v0); box_grow(p->lo, p->hi, v1); box_grow(p->lo, p->hi, v2);
             p->xf = d->mesh_transforms ? (int)d->mesh_transforms[m] - 1 : -1;
@@ -655,7 +662,26 @@ static void finalize(const scene_t* s, int pi, float t, v3 o, v3 d, hit_t* h) {
             normal = vadd(vadd(vscale(bu, p->vn[1]), vscale(bv, p->vn[2])), vscale(bc, p->vn[0]));
         }
         face(h, d, normal);
-        h->u = 0.0f; h->v = 0.0f;   /* get_triangle_uv over all-zero vertex uvs */
+        if (s->any_uv) {
+            /* get_triangle_uv (uvmapping.cuh:415-429) at this hit's point: get_barycenter (math_utils.cuh:
+               73-86), then calculateTextureCoordinate with its wrap (uvmapping.cuh:435-447); the reference
+               passes the record's previous hit point (triangle.cuh:162), here the hit's own */
+            v3 p2 = vsub(h->p, p->a);
+            float d00 = vdot(p->b, p->b), d01 = vdot(p->b, p->c), d11 = vdot(p->c, p->c);
+            float d20 = vdot(p2, p->b), d21 = vdot(p2, p->c);
+            float denom = d00 * d11 - d01 * d01;
+            float bv = (d11 * d20 - d01 * d21) / denom;
+            float bw = (d00 * d21 - d01 * d20) / denom;
+            float bu = 1.0f - bv - bw;
+            float tu = bu * p->uv[0] + bv * p->uv[2] + (1.0f - bu - bv) * p->uv[4];
+            float tv = bu * p->uv[1] + bv * p->uv[3] + (1.0f - bu - bv) * p->uv[5];
+            tu = fmodf(tu, 1.0f); tv = fmodf(tv, 1.0f);
+            if (tu < 0.0f) tu += 1.0f;
+            if (tv < 0.0f) tv += 1.0f;
+            h->u = tu; h->v = tv;
+        } else {
+            h->u = 0.0f; h->v = 0.0f;   /* get_triangle_uv over all-zero vertex uvs */
+        }
     }
     if (p->xf >= 0) xf_to_world(&s->xf[p->xf], &h->p, &h->n);
 }

@@ -153,7 +153,8 @@ int main() {
     cfg.meshesCfg.objMeshes = objs;
     cfg.meshesCfg.objMeshCount = 2;
     // a stand-in for rtc_load_obj: one tetrahedron with normals for "tetra.obj", nothing else
-    auto load_obj = [](const char* path, std::vector<float>& v, std::vector<uint32_t>& idx, std::vector<float>& n) {
+    auto load_obj = [](const char* path, std::vector<float>& v, std::vector<uint32_t>& idx, std::vector<float>& n,
+                       std::vector<float>&) {
         if (std::strcmp(path, "tetra.obj") != 0) return false;
         v = {0, 0, 0, 1, 0, 0, 0, 1, 0, 0, 0, 1};
         idx = {0, 2, 1, 0, 1, 3, 0, 3, 2, 1, 2, 3};

@@ -24,7 +24,8 @@ static void arr(const char* k, const float* v, int n, bool comma = true) {
     std::printf("]%s", comma ? ", " : "");
 }
 
-static bool read_obj(const char* path, std::vector<float>& v, std::vector<uint32_t>& idx, std::vector<float>& n) {
+static bool read_obj(const char* path, std::vector<float>& v, std::vector<uint32_t>& idx, std::vector<float>& n,
+                     std::vector<float>&) {
     std::ifstream f(path);
     if (!f) return false;
     std::vector<float> vn;

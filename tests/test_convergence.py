@@ -33,6 +33,7 @@ CASES = [
     ("textured", _textured, 32, 24, 10),
     ("spheres", _small_spheres, 40, 24, 16),
     ("icosphere", _ico_scene, 36, 24, 12),
+    ("uvmesh", configs.uv_mesh_scene, 36, 24, 10),   # image textures through per-vertex texture coordinates
 ]
 
 

@@ -102,6 +102,21 @@ def test_multi_axis_transforms_bitexact_vs_port(ctx, port, engine):
     assert st["frac_exact"] >= 0.999, st
 
 
+@pytest.mark.parametrize("engine", [ENGINE_MEGAKERNEL, ENGINE_WAVEFRONT])
+def test_uv_mesh_bitexact_vs_port(ctx, port, engine):
+    """Image textures on triangle meshes through per-vertex texture coordinates (get_triangle_uv at the
+    hit point, wrapped into [0, 1)), in meshes with and without coordinates: every pixel identical to the
+    C restatement.  The reference itself evaluates a triangle's uv at the hit record's previous hit point
+    (triangle.cuh:162), which depends on its BVH's visit order, so its own build is not the oracle here."""
+    scene, params = _params("uvmesh", dict(width=60, height=40, spp=9, max_depth=10), DRAW_ORDER_HOST, engine)
+    ours, _ = DeviceScene(ctx, scene).render(params)
+    pix = np.arange(params.width * params.height, dtype=np.int64)
+    ref, _ = port.scene(scene).render_pixels(params, pix, trig=1)
+    st = oracles.parity_stats(ours.reshape(-1, 4), ref)
+    print("uvmesh", engine, st)
+    assert st["frac_exact"] >= 0.999, st
+
+
 @pytest.mark.parametrize("name,kw", SCENES)
 def test_compat_parity_vs_reference_cpu(ctx, refcpu, name, kw):
     scene, params = _params(name, kw, DRAW_ORDER_HOST)

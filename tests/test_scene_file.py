@@ -443,6 +443,36 @@ meshes: { obj: ( { filepath = "tri.obj"; material = "grey"; position = { x = 0.0
     assert [r.textures[r.materials[r.meshes[i].material].texture].color[0] for i in range(2)] == pytest.approx([0.5, 0.9])
 
 
+UV_OBJ = """v 0 0 0
+v 1 0 0
+v 1 1 0
+v 0 1 0
+vt 0.0 0.0
+vt 0.25 0.0
+vt 0.25 0.5
+vt 0.0 0.5
+f 1/1 2/2 3/3 4/4
+"""
+
+
+def test_obj_texture_coordinates(tmp_path):
+    """`vt` coordinates reach the mesh (2 per vertex); with RTC_SCENE_FILE_REFERENCE_MESHES they are read as
+    mesh_loader reads them, texcoords[3 * i] and [3 * i + 1] from the array of 2 per vertex
+    (mesh_loader.cuh:370-371), reads past its end giving 0."""
+    (tmp_path / "sq.obj").write_text(UV_OBJ)
+    (tmp_path / "m.scene").write_text(
+        'materials: { lambertian: ( { name = "grey"; color = { r = 0.5; g = 0.5; b = 0.5; }; } ); };\n'
+        'meshes: { obj: ( { filepath = "sq.obj"; material = "grey"; } ); };\n')
+    own_file = SceneFile(tmp_path / "m.scene")   # the description lives as long as its file object
+    own = own_file.desc
+    uv = np.array([0.0, 0.0, 0.25, 0.0, 0.25, 0.5, 0.0, 0.5], np.float32)
+    assert own.meshes[0].num_vertices == 4 and np.array_equal(_arr(own.meshes[0].uvs, 8), uv)
+    ref_file = SceneFile(tmp_path / "m.scene", flags=SCENE_FILE_REFERENCE_MESHES)
+    ref = ref_file.desc
+    strided = np.array([uv[0], uv[1], uv[3], uv[4], uv[6], uv[7], 0.0, 0.0], np.float32)
+    assert np.array_equal(_arr(ref.meshes[0].uvs, 8), strided)
+
+
 REFUSED = [
     ("camera: { aperture = 1; };", "aperture"),                   # an integer handed to a float setter
     ("camera: { aspectRatio = 1.5; };", "aspectRatio"),           # not a string
