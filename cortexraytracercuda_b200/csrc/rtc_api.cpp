@@ -261,7 +261,11 @@ const DevScene& rtc_scene_dev(const rtc_scene* s) { return s->dev; }
 DevScene rtc_scene_view(const rtc_scene* s, const rtc_render_params* p) {
     DevScene S = s->dev;
     if (!p || !(p->flags & RTC_FLAG_WIDE_BVH)) S.nodes8 = nullptr;
+    rtc_view_env_sampling(S, p);
     return S;
+}
+void rtc_view_env_sampling(DevScene& S, const rtc_render_params* p) {
+    if (!p || !(p->flags & RTC_FLAG_ENV_SAMPLING) || p->mode != RTC_MODE_CLEAN) S.bg.cdf = nullptr;
 }
 DevParams rtc_dev_params(const rtc_render_params* p);
 
@@ -718,6 +722,39 @@ rtc_status rtc_build_host_scene(const rtc_scene_desc* d, HostScene& H, uint32_t 
     size_t env_bytes = d->background.kind == RTC_BG_ENV_MAP
                            ? (size_t)d->background.env_width * d->background.env_height * 3 * sizeof(float) : 0;
     size_t o_env = add_chunk(env_bytes ? d->background.env_rgb : nullptr, env_bytes);
+    // environment-map sampling tables (image_pdf, pdf/image_pdf.cuh:32-78): per texel luminance
+    // (0.2126, 0.7152, 0.0722) x sin(theta) of its row's centre; the marginal CDF over rows, then each
+    // row's conditional CDF over columns (a row of zero weight gets a uniform one)
+    std::vector<float> env_cdf;
+    if (env_bytes) {
+        const int W = d->background.env_width, H = d->background.env_height;
+        const float* px = d->background.env_rgb;
+        env_cdf.assign((size_t)H + (size_t)W * H, 0.0f);
+        std::vector<double> row(H, 0.0);
+        double total = 0.0;
+        for (int y = 0; y < H; ++y) {
+            const double st = std::sin(3.14159265358979323846 * (1.0 - (y + 0.5) / H));
+            double acc = 0.0;
+            float* C = env_cdf.data() + H + (size_t)y * W;
+            for (int x = 0; x < W; ++x) {
+                const float* q = px + 3 * ((size_t)y * W + x);
+                acc += std::max(0.0, (0.2126 * q[0] + 0.7152 * q[1] + 0.0722 * q[2]) * st);
+                C[x] = (float)acc;
+            }
+            for (int x = 0; x < W; ++x) C[x] = acc > 0.0 ? (float)(C[x] / acc) : (float)(x + 1) / (float)W;
+            C[W - 1] = 1.0f;
+            row[y] = acc;
+            total += acc;
+        }
+        double acc = 0.0;
+        for (int y = 0; y < H; ++y) {
+            acc += row[y];
+            env_cdf[y] = total > 0.0 ? (float)(acc / total) : 0.0f;
+        }
+        if (total > 0.0) env_cdf[H - 1] = 1.0f;
+        else env_cdf.clear();   // a black map: nothing to sample
+    }
+    size_t o_envcdf = add_chunk(env_cdf.data(), env_cdf.size() * sizeof(float));
 
     // host image of the device slab; the DevScene's pointer fields hold byte offsets into it
     H.slab.assign(total, 0);
@@ -769,6 +806,10 @@ rtc_status rtc_build_host_scene(const rtc_scene_desc* d, HostScene& H, uint32_t 
     D.bg.env = env_bytes ? (const float*)off(o_env) : nullptr;
     D.bg.env_w = d->background.env_width;
     D.bg.env_h = d->background.env_height;
+    D.bg.cdf = env_cdf.empty() ? nullptr : (const float*)off(o_envcdf);
+    D.bg.pdf_scale = env_cdf.empty() ? 0.0f
+                                     : (float)((double)D.bg.env_w * D.bg.env_h /
+                                               (2.0 * 3.14159265358979323846 * 3.14159265358979323846));
     H.cam = d->camera;
     H.info = rtc_scene_info{};
     H.info.num_primitives = (uint32_t)nprims;
@@ -795,6 +836,7 @@ DevScene rtc_rebase_scene(const HostScene& H, uint8_t* base) {
     rb(D.xprim); rb(D.xf); rb(D.rect);
     if (D.xnodes) { rb(D.xnodes); rb(D.xitems); }
     if (D.bg.env) rb(D.bg.env);
+    if (D.bg.cdf) rb(D.bg.cdf);
     if (D.tri_uv) rb(D.tri_uv);
     return D;
 }

@@ -96,6 +96,11 @@ struct DevBackground {
     float top[3];
     const float* env;   // device, env_w*env_h*3
     int env_w, env_h;
+    // environment-map importance sampling (clean mode, RTC_FLAG_ENV_SAMPLING; null otherwise): the
+    // marginal CDF over rows (env_h floats, top row first) followed by each row's conditional CDF over
+    // its columns (env_w floats per row), of luminance x sin(theta); pdf_scale = W*H / (2 pi^2)
+    const float* cdf;
+    float pdf_scale;
 };
 
 struct DevScene {

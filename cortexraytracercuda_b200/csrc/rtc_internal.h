@@ -43,6 +43,9 @@ rtc_status rtc_check_render_params(const rtc_render_params* p);
 const rtc::DevScene& rtc_scene_dev(const rtc_scene* s);
 // the device view a render uses: the 8-wide nodes only when the params ask for RTC_FLAG_WIDE_BVH
 rtc::DevScene rtc_scene_view(const rtc_scene* s, const rtc_render_params* p);
+// drops the environment-map sampling tables from a view unless the render asks for them (clean mode,
+// RTC_FLAG_ENV_SAMPLING)
+void rtc_view_env_sampling(rtc::DevScene& S, const rtc_render_params* p);
 rtc::DevParams rtc_dev_params(const rtc_render_params* p);
 // scratch of an image rendered with sample groups (0 without), and its layout at `base`
 size_t rtc_group_bytes(const rtc_render_params* p);

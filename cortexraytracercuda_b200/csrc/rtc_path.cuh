@@ -234,7 +234,25 @@ __device__ __forceinline__ void scatter_bounce(const DevScene& S, Ray& r, const 
     Onb b = build_from_w(h.n);
     V3 dir;
     float pdf_val, spdf;
-    if (!CLEAN || S.num_lights > 0) {
+    if (CLEAN && S.bg.cdf) {
+        // with environment-map sampling: mixture_pdf(objects, background, 0.8) (camera.cuh:333-336),
+        // objects = the light/cosine mixture below (cosine alone without lights)
+        const bool lights = S.num_lights > 0;
+        const float pick = rng.uniform();
+        if (pick < 0.2f) {
+            const float r1 = rng.uniform(), r2 = rng.uniform();
+            dir = env_sample(S.bg, r1, r2);
+        } else if (lights && rng.uniform() < 0.5f) {
+            if (S.num_lights > 1) (void)rng.uniform();
+            dir = light_random<ORDER>(S, 0, h.p, rng);
+        } else {
+            dir = onb_local(b, random_cosine_direction<FT>(rng));
+        }
+        float cosv = dot(unit(dir), b.w) / 3.14159265358979323846f;
+        float cpdf = 0.0f > cosv ? 0.0f : cosv;
+        const float obj = lights ? 0.5f * lights_pdf_value(S, h.p, dir) + 0.5f * cpdf : cpdf;
+        pdf_val = 0.8f * obj + 0.2f * env_pdf(S.bg, dir);
+    } else if (!CLEAN || S.num_lights > 0) {
         // mixture_pdf(hittable_pdf(lights, p), cosine_pdf), proportion 0.5 (mixture_pdf.cuh:28-47)
         if (rng.uniform() < 0.5f) {
             if (S.num_lights == 0) {

@@ -207,6 +207,7 @@ rtc_status admit_queued(rtc_server* s) {
         }
         note_resident(s);
         J.S = E.dev;
+        rtc_view_env_sampling(J.S, &rp);
         if (!R.req.use_scene_camera && !rtc_make_camera(R.req.camera, J.S.cam)) {
             cudaFreeAsync(out, s->st);
             R.d_out = nullptr;

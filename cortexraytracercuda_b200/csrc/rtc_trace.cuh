@@ -844,6 +844,58 @@ __device__ __forceinline__ RGB background(const DevScene& S, V3 dir) {
     return rgb(__ldg(px), __ldg(px + 1), __ldg(px + 2));
 }
 
+// ---- environment-map importance sampling (clean mode, RTC_FLAG_ENV_SAMPLING) ---------------------
+// The distribution of image_pdf (pdf/image_pdf.cuh:32-145) done so that generate and value agree: a row
+// by the marginal CDF, a column by the row's conditional CDF (each by binary search, the CDFs inverted
+// continuously so the point is uniform inside its texel), the point (u, v) turned into a direction by
+// from_spherical_uv (uvmapping.cuh:194-200), whose inverse is the background lookup above
+// (get_spherical_uv, uvmapping.cuh:144-158).  Density over directions: texel probability x W x H /
+// (2 pi^2 sin(theta)).
+
+// first index in cdf[0, n) whose value exceeds r (n - 1 at most)
+__device__ __forceinline__ int env_search(const float* cdf, int n, float r) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(cdf + mid) > r) hi = mid;
+        else lo = mid + 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ V3 env_sample(const DevBackground& B, float r1, float r2) {
+    const int W = B.env_w, H = B.env_h;
+    const int y = env_search(B.cdf, H, r1);
+    const float m0 = y > 0 ? __ldg(B.cdf + y - 1) : 0.0f, m1 = __ldg(B.cdf + y);
+    const float fy = m1 > m0 ? fminf(fmaxf((r1 - m0) / (m1 - m0), 0.0f), 1.0f) : 0.5f;
+    const float* C = B.cdf + H + (size_t)y * W;
+    const int x = env_search(C, W, r2);
+    const float c0 = x > 0 ? __ldg(C + x - 1) : 0.0f, c1 = __ldg(C + x);
+    const float fx = c1 > c0 ? fminf(fmaxf((r2 - c0) / (c1 - c0), 0.0f), 1.0f) : 0.5f;
+    const float u = ((float)x + fx) / (float)W;
+    const float v = 1.0f - ((float)y + fy) / (float)H;
+    float st, ct, sa, ca;
+    sincosf(3.14159265358979323846f * v, &st, &ct);
+    sincosf(2.0f * 3.14159265358979323846f * u - 3.14159265358979323846f, &sa, &ca);
+    return v3(st * ca, -ct, -st * sa);
+}
+
+__device__ __forceinline__ float env_pdf(const DevBackground& B, V3 dir) {
+    const V3 ud = unit(dir);
+    const double theta = acos((double)-ud.y);
+    const double phi = atan2((double)-ud.z, (double)ud.x) + 3.14159265358979323846;
+    const int W = B.env_w, H = B.env_h;
+    int x = (int)(phi / (2.0 * 3.14159265358979323846) * W);
+    x = x < 0 ? 0 : (x >= W ? W - 1 : x);
+    int y = (int)((1.0 - theta / 3.14159265358979323846) * H);
+    y = y < 0 ? 0 : (y >= H ? H - 1 : y);
+    const float* C = B.cdf + H + (size_t)y * W;
+    const float pr = __ldg(B.cdf + y) - (y > 0 ? __ldg(B.cdf + y - 1) : 0.0f);
+    const float pc = __ldg(C + x) - (x > 0 ? __ldg(C + x - 1) : 0.0f);
+    const float st = sqrtf(fmaxf(0.0f, 1.0f - ud.y * ud.y));
+    return st > 0.0f ? pr * pc * B.pdf_scale / st : 0.0f;
+}
+
 // directional_light::pdf_value (directional_light.cuh:147-158) for light `li` seen from o along v;
 // omni_light::pdf_value / spot_light::pdf_value (omni_light.cuh:104-115): 1 / the solid angle of the
 // sphere, 2 * M_PI * (1 - cos_theta_max), all in float: the reference's M_PI is a float literal

@@ -25,6 +25,7 @@ ENGINE_AUTO, ENGINE_MEGAKERNEL, ENGINE_WAVEFRONT = 0, 1, 2
 FLAG_KERNEL_TIMING = 1
 FLAG_WIDE_BVH = 2
 FLAG_SAMPLE_GROUPS = 4
+FLAG_ENV_SAMPLING = 8   # clean mode: lambertian bounces also sample the environment map by luminance
 BVH_SAH = 0        # binned SAH on host threads (default)
 BVH_DEVICE = 1     # built on the device: Morton sort + PLOC clustering (near-SAH quality)
 BVH_DEVICE_LBVH = 2   # built on the device: Morton sort + linear BVH (fastest build)

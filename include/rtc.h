@@ -361,6 +361,14 @@ typedef struct rtc_render_params {
  * sum in the last bits (float addition is not associative).  Needs per-image scratch: not available to
  * rtc_render_noalloc.  Compat mode ignores it (a pixel's samples share one stream there). */
 #define RTC_FLAG_SAMPLE_GROUPS 4
+/* Clean mode with an environment-map background: lambertian bounces also sample the map in proportion
+ * to its luminance (x sin(theta)), with probability 0.2, mixed with their light and cosine sampling
+ * (the mixture_pdf(objects, background_pdf, 0.8) that camera.cuh:333-336 leaves commented out, with
+ * image_pdf's marginal and conditional CDFs, pdf/image_pdf.cuh:80-145).  The estimate stays unbiased
+ * (the cosine part covers the hemisphere) and converges to the same image with less noise where the
+ * map carries the light.  Compat mode ignores it (the reference's GPU path never samples its map,
+ * gpu.cu:729-742). */
+#define RTC_FLAG_ENV_SAMPLING 8
 
 /* ------------------------------------------------------------------------------------------------ */
 /* context and scenes                                                                                */
