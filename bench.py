@@ -71,6 +71,61 @@ STATE_BYTES = 32 + 16 + 2 * 48   # ray read + hit write + path state read/write 
 EXTEND_STATE_BYTES = 4 + 32 + 4 + 8   # queue entry + ray (origin, direction) + depth word read, hit record write
 
 
+# Path-state bytes the shade kernel moves per traced ray (its algorithmic traffic): queue entry, hit
+# record and the slot's meta, ray origin/direction, attenuation and sample radiance read (4+8+5x16), the
+# ray, attenuation, radiance and meta written back (4x16) and the survivor's queue entry (4).
+SHADE_STATE_BYTES = 4 + 8 + 5 * 16 + 4 * 16 + 4
+NCU_SUMMARY = ROOT / "profiles" / "ncu_wavefront_{config}.json"
+
+
+def kernel_bounds(config, peak, kstats, ext_rays, roof):
+    """What binds each wavefront kernel: the live per-frame times of this run (CUDA events) beside the
+    figures of one ncu --set full capture per kernel of the same frame (profiles/ncu_wavefront_<config>
+    .json): DRAM and L2 bytes per launch, issue-active and lanes active per instruction.  DRAM traffic is
+    far below the algorithmic bytes (the BVH, the scene and most of the path state stay in L1/L2), and
+    no kernel is near the DRAM or FP32 peak: the kernels are bound by memory latency and divergence."""
+    f = NCU_SUMMARY.with_name(NCU_SUMMARY.name.format(config=config))
+    prof = {}
+    if f.exists():
+        try:
+            prof = json.loads(f.read_text())
+        except Exception:
+            prof = {}
+    live = {"wf_extend": (float(np.mean([s["extend_ms"] for s in kstats])), int(np.mean([s["extend_launches"] for s in kstats]))),
+            "wf_shade": (float(np.mean([s["shade_ms"] for s in kstats])), int(np.mean([s["shade_launches"] for s in kstats]))),
+            "wf_finish": (float(np.mean([s["drain_ms"] for s in kstats])), 1)}
+    out = {}
+    for k, (ms, n) in live.items():
+        rec = {"ms_per_frame": round(ms, 3), "launches_per_frame": n, "avg_launch_us": round(1e3 * ms / max(n, 1), 2)}
+        p = prof.get(k)
+        if p:
+            avg_s = ms / 1e3 / max(n, 1) if k != "wf_finish" else ms / 1e3
+            rec.update({kk: p[kk] for kk in ("dram_bytes_per_launch", "l2_bytes_per_launch", "l1_hit_pct", "l2_hit_pct",
+                                              "issue_active_pct", "lanes_active_per_inst", "warps_active_pct",
+                                              "registers", "top_stalls") if kk in p})
+            if "dram_bytes_per_launch" in p and k != "wf_finish":
+                rec["dram_frac"] = round(p["dram_bytes_per_launch"] / avg_s / 1e9 / peak, 4)
+            if "l2_bytes_per_launch" in p and k != "wf_finish":
+                rec["l2_gbs"] = round(p["l2_bytes_per_launch"] / avg_s / 1e9, 1)
+        out[k] = rec
+    shade_ms = live["wf_shade"][0]
+    out["wf_shade"]["alg_bytes_per_frame"] = int(ext_rays * SHADE_STATE_BYTES)
+    out["wf_shade"]["alg_gbs"] = round(ext_rays * SHADE_STATE_BYTES / (shade_ms / 1e3) / 1e9, 1)
+    ext = out["wf_extend"]
+    res = {"bound": "latency",
+           "bound_why": "DRAM traffic per launch is a few percent of the algorithmic bytes and of the DRAM peak; "
+                        "FP32 issue is a few percent of peak; the kernels wait on dependent L1/L2 fetches "
+                        "(long_scoreboard) with about a third of the lanes active (divergent walks)",
+           "kernels": out}
+    if "dram_bytes_per_launch" in ext:
+        res["traffic"] = ext["dram_bytes_per_launch"]
+        res["dram_frac"] = ext.get("dram_frac")
+    if prof:
+        res["profile_source"] = f"profiles/{f.name} (ncu --set full, one launch per kernel, command in " \
+                                f"profiles/wavefront_kernels_{config}.md)"
+    return res
+
+
 def workload(name):
     mk, mp = configs.SCENES[name]
     scene = mk()
@@ -897,12 +952,8 @@ def main():
                      "frac": round(flops / t_s / 1e12 / fp32_peak, 4),
                      "peak_source": f"FP32 SIMT: {sms} SMs x 128 x 2 x {mhz:.0f} MHz",
                      "per_visit": {"node": NODE_FLOPS, "prim": PRIM_FLOPS[args.config]}}
-    prof = ROOT / "profiles" / f"traffic_{'wf_extend' if wavefront else 'megakernel'}_{args.config}.json"
-    if prof.exists():
-        try:
-            roof["traffic"] = json.loads(prof.read_text()).get("dram_bytes_per_launch")
-        except Exception:
-            pass
+    if wavefront:
+        roof.update(kernel_bounds(args.config, peak, kstats, ext_rays, roof))
 
     line = {"metric": METRIC, "value": round(value, 3), "unit": METRIC, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 3), "higher_is_better": True,

@@ -8,6 +8,7 @@
 #include <cstring>
 #include <mutex>
 #include <thread>
+#include <tuple>
 
 #include "rtc_dev.h"
 
@@ -402,6 +403,113 @@ bool build_bvh(const BvhInput& in, int max_leaf, int threads, BvhOutput& out, co
     }
     if (max_depth + 2 > (uint32_t)TRAVERSAL_STACK) { if (err) *err = "BVH too deep for the traversal stack"; return false; }
     return true;
+}
+
+// Collapses subtrees of at most `max_leaf` primitives into leaves where the SAH cost says a leaf is
+// cheaper (the host build's costs: 1 per node visit, 1 per primitive test, children weighted by their
+// box's area over the parent's), renumbering the nodes in depth-first order and the leaf slots so that
+// each new leaf's primitives are contiguous.  The root stays an inner node.  For trees built one
+// primitive per leaf (the device builds).
+void collapse_leaves(BvhOutput& t, int max_leaf) {
+    const uint32_t inner = t.num_nodes;
+    if (inner == 0) return;
+    auto link = [&](uint32_t node, int side) {
+        int32_t c;
+        std::memcpy(&c, &t.nodes[16 * (size_t)node + 12 + side], 4);
+        return c;
+    };
+    // a child's box and area, from its parent's record (L: x in [0,1], y in [2,3], z in [8,9]; R: 4-7, 10-11)
+    auto child_area = [&](uint32_t node, int side) {
+        const float* n = &t.nodes[16 * (size_t)node];
+        const float dx = side ? n[5] - n[4] : n[1] - n[0];
+        const float dy = side ? n[7] - n[6] : n[3] - n[2];
+        const float dz = side ? n[11] - n[10] : n[9] - n[8];
+        return 2.0 * ((double)dx * dy + (double)dy * dz + (double)dz * dx);
+    };
+    auto node_area = [&](uint32_t node) {
+        const float* n = &t.nodes[16 * (size_t)node];
+        const float dx = std::max(n[1], n[5]) - std::min(n[0], n[4]);
+        const float dy = std::max(n[3], n[7]) - std::min(n[2], n[6]);
+        const float dz = std::max(n[9], n[11]) - std::min(n[8], n[10]);
+        return 2.0 * ((double)dx * dy + (double)dy * dz + (double)dz * dx);
+    };
+    std::vector<uint32_t> count(inner, 0);
+    std::vector<double> cost(inner, 0.0);
+    std::vector<uint8_t> leaf(inner, 0);
+    // post-order over the inner nodes (explicit stack: device trees can be deep)
+    std::vector<std::pair<uint32_t, bool>> st{{0u, false}};
+    while (!st.empty()) {
+        auto [node, done] = st.back();
+        st.pop_back();
+        if (!done) {
+            st.push_back({node, true});
+            for (int side = 0; side < 2; ++side)
+                if (link(node, side) >= 0) st.push_back({(uint32_t)link(node, side), false});
+            continue;
+        }
+        uint32_t n = 0;
+        double split = 1.0;
+        const double a = std::max(node_area(node), 1e-30);
+        for (int side = 0; side < 2; ++side) {
+            const int32_t c = link(node, side);
+            const uint32_t cn = c < 0 ? ((uint32_t)~c & 31u) : count[c];
+            const double cc = c < 0 ? (double)cn : cost[c];
+            n += cn;
+            split += child_area(node, side) * cc / a;
+        }
+        count[node] = n;
+        leaf[node] = node != 0 && (int)n <= max_leaf && (double)n <= split;
+        cost[node] = leaf[node] ? (double)n : split;
+    }
+    // depth-first renumbering; collapsed subtrees become leaves of contiguous slots
+    std::vector<float> nodes;
+    std::vector<uint32_t> order;
+    nodes.reserve(t.nodes.size());
+    order.reserve(t.order.size());
+    uint32_t max_depth = 0, max_leaf_seen = 0;
+    auto gather = [&](int32_t c) {   // appends the primitives under link c to `order`
+        std::vector<int32_t> s{c};
+        while (!s.empty()) {
+            const int32_t x = s.back();
+            s.pop_back();
+            if (x < 0) {
+                const uint32_t first = (uint32_t)~x >> 5, cnt = (uint32_t)~x & 31u;
+                for (uint32_t k = 0; k < cnt; ++k) order.push_back(t.order[first + k]);
+            } else {
+                s.push_back(link((uint32_t)x, 1));
+                s.push_back(link((uint32_t)x, 0));
+            }
+        }
+    };
+    // (old node, depth, where its new index goes: a link slot in `nodes`, or -1 for the root)
+    std::vector<std::tuple<uint32_t, uint32_t, int64_t>> work{{0u, 1u, -1}};
+    while (!work.empty()) {
+        const auto [old, depth, slot] = work.back();
+        work.pop_back();
+        const uint32_t me = (uint32_t)(nodes.size() / 16);
+        if (slot >= 0) std::memcpy(&nodes[(size_t)slot], &me, 4);
+        nodes.insert(nodes.end(), t.nodes.begin() + 16 * (size_t)old, t.nodes.begin() + 16 * (size_t)old + 16);
+        for (int side = 1; side >= 0; --side) {
+            const int32_t c = link(old, side);
+            const size_t at = 16 * (size_t)me + 12 + side;
+            if (c >= 0 && !leaf[c]) {
+                work.push_back({(uint32_t)c, depth + 1, (int64_t)at});
+                continue;
+            }
+            const uint32_t first = (uint32_t)order.size();
+            gather(c);
+            const uint32_t cnt = (uint32_t)order.size() - first;
+            const int32_t enc = ~(int32_t)((first << 5) | cnt);
+            std::memcpy(&nodes[at], &enc, 4);
+            max_depth = std::max(max_depth, depth + 1);
+            max_leaf_seen = std::max(max_leaf_seen, cnt);
+        }
+    }
+    t.nodes.swap(nodes);
+    t.order.swap(order);
+    t.num_nodes = (uint32_t)(t.nodes.size() / 16);
+    t.max_depth = max_depth;
+    t.max_leaf_seen = max_leaf_seen;
 }
 
 }  // namespace rtc

@@ -36,6 +36,11 @@ struct BvhOutput {
 // Returns false (with a message) if the tree would not fit the traversal stack or the item encoding.
 bool build_bvh(const BvhInput& in, int max_leaf, int threads, BvhOutput& out, const char** err);
 
+// Merges subtrees of at most `max_leaf` primitives into single leaves where the SAH cost favours it
+// (bvh_build.cpp): renumbers the nodes depth-first and reorders `order` so each leaf is contiguous;
+// updates num_nodes, max_depth and max_leaf_seen.  For one-primitive-per-leaf trees.
+void collapse_leaves(BvhOutput& tree, int max_leaf);
+
 // BVH built on CUDA device `device` (bvh_device.cu) over Morton-sorted primitives, one primitive per
 // leaf, no 8-wide nodes: PLOC clustering (BVH_DEVICE_PLOC) or the linear BVH (BVH_DEVICE_LBVH).
 // BVH_DEVICE_TOO_DEEP and BVH_DEVICE_UNSUPPORTED leave the SAH build as the way out.
