@@ -311,6 +311,42 @@ def ref_gpu_baseline(ctx, stream, warmup=3, steps=3):
                     "blocks, per-pixel printf left out)", "cases": out}
 
 
+def cpu_reference_batched(work, every=8, target_s=12.0):
+    """The reference's own CPU code on a subsample of the batched workload: every `every`-th scene, a
+    deterministic pixel subsample of each image sized to about target_s in total, compat mode (its g++
+    build's draw order).  Returns the record (Mpaths/s over the rendered paths)."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    import oracles
+    ref = oracles.ref_cpu()
+    if ref is None:
+        return None
+    threads = os.cpu_count() or 1
+    picked = list(range(0, len(work), every))
+    per_scene = target_s / max(len(picked), 1)
+    paths = 0
+    secs = 0.0
+    px_total = 0
+    for k in picked:
+        sc, p0 = work[k]
+        p = p0.__class__(**{**p0.__dict__, "mode": MODE_COMPAT, "draw_order": DRAW_ORDER_HOST})
+        rs = ref.scene(sc)
+        npix = p.width * p.height
+        probe = np.arange(0, npix, max(1, npix // 512), dtype=np.int64)
+        t = time.perf_counter()
+        rs.render_pixels(p, probe, threads)
+        per_px = max(time.perf_counter() - t, 1e-6) / probe.size
+        stride = max(1, int(npix / max(1.0, per_scene / per_px)))
+        pix = np.arange(0, npix, stride, dtype=np.int64)
+        t = time.perf_counter()
+        rs.render_pixels(p, pix, threads)
+        secs += time.perf_counter() - t
+        paths += pix.size * p.traced_spp
+        px_total += pix.size
+    return {"value": round(paths / secs / 1e6, 4), "unit": METRIC, "kind": "reference", "cores": threads,
+            "sample": f"scenes 0, {every}, ... ({len(picked)} of {len(work)}), {px_total} pixels at each image's spp "
+                      f"and depth, compat mode, {secs:.1f} s"}
+
+
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return
@@ -331,6 +367,8 @@ def run_reference_arm(args, rank, world):
             "mrays_per_s": round(float(np.mean(rays_rates)), 4),
             "cpu_baseline": {"value": round(value, 4), "unit": METRIC, **info},
             "e2e": {"value": round(value, 4), "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if name == "spheres" and not args.no_batched:
+        line["batched"] = cpu_reference_batched(configs.batch_workload(args.scenes))
     print(json.dumps(line), flush=True)
 
 

@@ -327,52 +327,11 @@ __device__ __forceinline__ RGB emitted(const DevScene& S, const Ray& r, const Hi
 
 // One bounce of camera::ray_color (camera.cuh:153-227) AFTER the closest-hit query of the current ray:
 // `hit` tells whether world.hit found something at (t, item).  Updates the path's running radiance
-// `result`, its attenuation `att` and its ray; returns false when the path ends at this bounce.
-// All additions of the reference are kept, including the zero emission of non-emitting materials,
-// so NaN/Inf propagate exactly as in the reference.  The megakernel and the drain kernel call this;
-// the wavefront shade kernel calls the same pieces through shade_bounce_deferred.
-template <bool CLEAN, int ORDER, class R>
-__device__ __forceinline__ bool shade_bounce(const DevScene& S, Ray& r, bool hit, float t, uint32_t item, bool hide,
-                                             RGB& result, RGB& att, R& rng, PathCounters& pc, TraceStats& st,
-                                             uint32_t& status) {
-    if (!hit) {
-        RGB bg = background(S, r.d);
-        result.r += att.r * bg.r;
-        result.g += att.g * bg.g;
-        result.b += att.b * bg.b;
-        return false;
-    }
-    constexpr bool FT = CLEAN || ORDER == 0;   // float trig in the nvcc flavour and in clean mode
-    Hit h;
-    finalize_hit<FT>(S, item, t, r.o, r.d, h);
-    if ((uint32_t)h.mat >= S.num_materials) { status |= STATUS_BAD_MATERIAL; return false; }
-    int4 mi = __ldg(S.mat_i + h.mat);
-    float4 mf = __ldg(S.mat_f + h.mat);
-    bool em_alpha0;
-    const RGB em = emitted<FT>(S, r, h, mi, mf, em_alpha0, status);
-    if (em_alpha0) {
-        // "invisible" re-hit from just behind the light (camera.cuh:177-183); rec is replaced only
-        // when the re-hit finds something, and `emitted` is not recomputed.
-        float t2;
-        uint32_t item2;
-        pc.rays++;
-        if (closest_hit<CLEAN>(S, r.o, r.d, h.t + 0.001f, 3.402823466e+38f, hide, t2, item2, st, status)) {
-            finalize_hit<FT>(S, item2, t2, r.o, r.d, h);
-            if ((uint32_t)h.mat >= S.num_materials) { status |= STATUS_BAD_MATERIAL; return false; }
-            mi = __ldg(S.mat_i + h.mat);
-            mf = __ldg(S.mat_f + h.mat);
-        }
-    }
-    result.r += att.r * em.r;
-    result.g += att.g * em.g;
-    result.b += att.b * em.b;
-    if (is_light_material(mi.x)) return false;   // lights: material::scatter returns false
-    scatter_bounce<CLEAN, ORDER>(S, r, h, mi, mf, att, rng, status);
-    return true;
-}
-
-// The same bounce with the invisible re-hit handed back to the caller instead of traced here, so the
-// wavefront shade kernel holds no traversal: the re-hit goes through the extend kernel like any other ray.
+// `result`, its attenuation `att` and its ray.  All additions of the reference are kept, including the
+// zero emission of non-emitting materials, so NaN/Inf propagate exactly as in the reference.  The
+// "invisible" re-hit from behind a one-sided light (camera.cuh:177-183) is handed back to the caller
+// instead of traced here, so every engine has one trace call site: the wavefront sends the re-hit
+// through its extend kernel like any other ray, the megakernel and the drain loop around (trace_bounces).
 //   BOUNCE_END    the path ends at this bounce;
 //   BOUNCE_NEXT   the path continues with the scattered ray (one depth level used);
 //   BOUNCE_REHIT  the hit was the back face of a one-sided light: its (zero-alpha) emission is added
@@ -415,6 +374,34 @@ __device__ __forceinline__ int shade_bounce_deferred(const DevScene& S, Ray& r, 
     return BOUNCE_NEXT;
 }
 
+// camera::ray_color's loop (camera.cuh:155-226) from `depth` levels left down to the end of the path:
+// trace, then shade; a re-hit from behind a one-sided light traces the same ray again from `tmin` =
+// t + 0.001 at the same depth.  `tmin` starts at 1e-5 (SHADOW_ACNE_FIX), or at a pending re-hit's start.
+template <bool CLEAN, int ORDER, class R>
+__device__ __forceinline__ void trace_bounces(const DevScene& S, Ray& r, int depth, int max_depth, float tmin,
+                                              RGB& result, RGB& att, R& rng, PathCounters& pc, TraceStats& st,
+                                              uint32_t& status) {
+    bool rehit = tmin > 0.00001f;
+    for (; depth > 0; --depth) {
+        const bool hide = depth == max_depth;
+        float t, next_tmin = 0.0f;
+        uint32_t item;
+        pc.rays++;
+        const bool hit = closest_hit<CLEAN>(S, r.o, r.d, tmin, 3.402823466e+38f, hide, t, item, st, status);
+        const int out = shade_bounce_deferred<CLEAN, ORDER>(S, r, hit, t, item, rehit, result, att, rng, status,
+                                                            next_tmin);
+        if (out == BOUNCE_REHIT) {   // the same depth again
+            rehit = true;
+            tmin = next_tmin;
+            ++depth;
+            continue;
+        }
+        if (out != BOUNCE_NEXT) break;
+        rehit = false;
+        tmin = 0.00001f;
+    }
+}
+
 // One camera sample: camera::ray_color (camera.cuh:149-264).  Returns the radiance of the sample.
 template <bool CLEAN, int ORDER, class R>
 __device__ __forceinline__ RGB trace_sample(const DevScene& S, Ray r, int max_depth, R& rng, PathCounters& pc,
@@ -422,14 +409,7 @@ __device__ __forceinline__ RGB trace_sample(const DevScene& S, Ray r, int max_de
     RGB result = rgb(0.f, 0.f, 0.f);
     RGB att = rgb(1.f, 1.f, 1.f);
     TraceStats st{0, 0};
-    for (int depth = max_depth; depth > 0; --depth) {
-        const bool hide = depth == max_depth;
-        float t;
-        uint32_t item;
-        pc.rays++;
-        bool hit = closest_hit<CLEAN>(S, r.o, r.d, 0.00001f, 3.402823466e+38f, hide, t, item, st, status);
-        if (!shade_bounce<CLEAN, ORDER>(S, r, hit, t, item, hide, result, att, rng, pc, st, status)) break;
-    }
+    trace_bounces<CLEAN, ORDER>(S, r, max_depth, max_depth, 0.00001f, result, att, rng, pc, st, status);
     pc.nodes += st.nodes;
     pc.prims += st.prims;
     return result;

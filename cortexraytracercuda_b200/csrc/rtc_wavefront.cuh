@@ -5,7 +5,7 @@
 // thrust::minstd_rand per pixel, consumed by all samples, core/src/gpu.cu:770-790), so the radiance
 // is bit-identical to the megakernel's.  What changes is the shape of the work:
 //   extend  every queued slot runs only the closest-hit traversal of its current ray;
-//   shade   every queued slot runs one bounce of camera::ray_color (shade_bounce); a finished sample
+//   shade   every queued slot runs one bounce of camera::ray_color (shade_bounce_deferred); a finished sample
 //           adds into the pixel sum and the slot regenerates the next camera sample, a finished pixel
 //           is written out and the slot fetches the next pixel from a global counter;
 // and survivors are compacted into the next queue with one atomic per warp (ballot + popc + shfl).
@@ -333,7 +333,7 @@ __global__ void RTC_EXTEND_BOUNDS wf_extend(J jobs, WfBuffers B, WfIter w, unsig
     if (status) atomicOr(status_word, status);
 }
 
-// One shade step of a slot whose current ray has been traced: shade_bounce, then the slot's
+// One shade step of a slot whose current ray has been traced: shade_bounce_deferred, then the slot's
 // bookkeeping (next bounce / next sample / next pixel).  Returns true while the slot has a ray to trace.
 template <bool CLEAN, int ORDER, class J>
 __device__ __forceinline__ bool wf_step(const J& jobs, const WfWindow& win, const WfBuffers& B, uint32_t slot,
@@ -551,30 +551,13 @@ __global__ void RTC_FINISH_BOUNDS wf_finish(J jobs, WfBuffers B, WfIter w, unsig
         else rng.x = m.z;
         uint32_t pixel = m.x, sample = m.y, job = wf_job(m.w), grp = CLEAN ? m.z : 0u;
         int depth = (int)wf_depth(m.w);
-        float pending = d.w;   // > 0: the slot waits for its re-hit from behind a one-sided light
+        float tmin = wf_tmin(d);   // the slot may wait for its re-hit from behind a one-sided light
         // one pass of the loop finishes the current sample of the current pixel
         for (;;) {
             const DevScene& S = jobs.scene(job);
             const DevParams& P = jobs.params(job);
             // the rest of the current sample: camera::ray_color's loop from `depth` down
-            for (; depth > 0; --depth) {
-                const bool hide = depth == P.max_depth;
-                float t;
-                uint32_t item;
-                pc.rays++;
-                if (pending > 0.0f) {
-                    const float tmin = pending;
-                    pending = 0.0f;
-                    bool h = closest_hit<CLEAN>(S, r.o, r.d, tmin, 3.402823466e+38f, hide, t, item, st, status);
-                    float unused;
-                    if (shade_bounce_deferred<CLEAN, ORDER>(S, r, h, t, item, true, acc, att, rng, status, unused) !=
-                        BOUNCE_NEXT)
-                        break;
-                    continue;
-                }
-                bool h = closest_hit<CLEAN>(S, r.o, r.d, 0.00001f, 3.402823466e+38f, hide, t, item, st, status);
-                if (!shade_bounce<CLEAN, ORDER>(S, r, h, t, item, hide, acc, att, rng, pc, st, status)) break;
-            }
+            trace_bounces<CLEAN, ORDER>(S, r, depth, P.max_depth, tmin, acc, att, rng, pc, st, status);
             ++paths;
             if (!CLEAN || (isfinite(acc.r) && isfinite(acc.g) && isfinite(acc.b))) {
                 pr += acc.r;
@@ -586,6 +569,7 @@ __global__ void RTC_FINISH_BOUNDS wf_finish(J jobs, WfBuffers B, WfIter w, unsig
                 att = rgb(1.f, 1.f, 1.f);
                 acc = rgb(0.f, 0.f, 0.f);
                 depth = P.max_depth;
+                tmin = 0.00001f;
                 continue;
             }
             wf_group_done(jobs, job, pixel, grp, make_float4(pr, pg, pb, 0.0f));
@@ -606,6 +590,7 @@ __global__ void RTC_FINISH_BOUNDS wf_finish(J jobs, WfBuffers B, WfIter w, unsig
             grp = CLEAN ? m.z : 0u;
             job = wf_job(m.w);
             depth = (int)wf_depth(m.w);
+            tmin = wf_tmin(d2);
             if (status) break;
         }
     }

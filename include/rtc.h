@@ -158,7 +158,10 @@ typedef struct rtc_mesh {
     const float* vertices;      /* 3 floats per vertex                                             */
     const uint32_t* indices;    /* 3 per triangle                                                  */
     const float* normals;       /* optional, 3 floats per vertex; used when smooth != 0            */
-    const float* uvs;           /* optional, 2 floats per vertex                                   */
+    const float* uvs;           /* optional, 2 floats per vertex: texture coordinates, interpolated at
+                                   the hit with get_triangle_uv's barycentrics and wrapped into [0, 1)
+                                   (uvmapping.cuh:415-447; the reference evaluates them at the hit
+                                   record's previous hit point, triangle.cuh:162 - not reproduced)  */
     uint32_t num_vertices;
     uint32_t num_triangles;
     int32_t material;
