@@ -625,6 +625,34 @@ __device__ __forceinline__ bool closest_hit(const DevScene& S, V3 o, V3 d, float
 // Full hit record of the winning item: the part of each reference hit() that runs after the
 // interval test (sphere.cuh:137-165, quad.cuh:122-132, directional_light.cuh:113-120,
 // triangle.cuh:160-184).
+// fmod(x, 1) (the wraps of uvmapping.cuh): x - trunc(x) carries the sign of x and is exact - the
+// fractional part of a float is representable, and |x| >= 2^23 is an integer - so this equals fmodf(x,
+// 1.0f) for every x (NaN for infinities and NaN, zero of x's sign for integers) in three instructions
+// where fmodf's general algorithm inlines a loop into every kernel that finalises a hit.
+__device__ __forceinline__ float fmod1(float x) { return copysignf(x - truncf(x), x); }
+
+// get_triangle_uv (uvmapping.cuh:415-429) at a triangle hit's point: get_barycenter's barycentrics
+// (math_utils.cuh:73-86) over v0, v1 = v0 + e1, v2 = v0 + e2, then calculateTextureCoordinate
+// (uvmapping.cuh:435-447) with its wrap into [0, 1).  The reference passes the hit record's previous
+// hit point (triangle.cuh:162), which depends on the BVH's visit order; this uses the hit's own.
+__device__ __forceinline__ void tri_uv_at(const DevScene& S, uint32_t idx, float4 a0, float4 a1, float4 a2, Hit& h) {
+    const V3 e1 = v3(a1.x, a1.y, a1.z), e2 = v3(a2.x, a2.y, a2.z), p2 = sub(h.p, v3(a0.x, a0.y, a0.z));
+    const float d00 = dot(e1, e1), d01 = dot(e1, e2), d11 = dot(e2, e2), d20 = dot(p2, e1), d21 = dot(p2, e2);
+    const float denom = d00 * d11 - d01 * d01;
+    const float bv = (d11 * d20 - d01 * d21) / denom;
+    const float bw = (d00 * d21 - d01 * d20) / denom;
+    const float bu = 1.0f - bv - bw;
+    const float4 t0 = __ldg(S.tri_uv + 2 * (size_t)idx), t1 = __ldg(S.tri_uv + 2 * (size_t)idx + 1);
+    float tu = bu * t0.x + bv * t0.z + (1.0f - bu - bv) * t1.x;
+    float tv = bu * t0.y + bv * t0.w + (1.0f - bu - bv) * t1.y;
+    tu = fmod1(tu);
+    tv = fmod1(tv);
+    if (tu < 0.0f) tu += 1.0f;
+    if (tv < 0.0f) tv += 1.0f;
+    h.u = tu;
+    h.v = tv;
+}
+
 template <bool FLOAT_TRIG>
 __device__ __forceinline__ void finalize_prim(const DevScene& S, uint32_t kind, uint32_t idx, float t, V3 o, V3 d,
                                               Hit& h) {
@@ -648,8 +676,8 @@ __device__ __forceinline__ void finalize_prim(const DevScene& S, uint32_t kind, 
         }
         float sc = phi / (2.0f * 3.14159265358979323846f);
         float tc = theta / 3.14159265358979323846f;
-        sc = fmodf(sc * 1.0f, 1.0f);
-        tc = fmodf(tc * 1.0f, 1.0f);
+        sc = fmod1(sc * 1.0f);
+        tc = fmod1(tc * 1.0f);
         h.u = 1.0f * sc + 0.0f;
         h.v = 1.0f * tc + 0.0f;
     } break;
@@ -703,26 +731,7 @@ __device__ __forceinline__ void finalize_prim(const DevScene& S, uint32_t kind, 
         }
         set_face_normal(h, d, normal);
         if (S.tri_uv) {
-            // get_triangle_uv (uvmapping.cuh:415-429) at this hit's point: get_barycenter's barycentrics
-            // (math_utils.cuh:73-86) over v0, v1 = v0 + e1, v2 = v0 + e2, then calculateTextureCoordinate
-            // (uvmapping.cuh:435-447) with its wrap into [0, 1).  The reference passes the hit record's
-            // previous hit point (triangle.cuh:162), which depends on the BVH's visit order; this uses
-            // the hit's own.
-            const V3 e1 = v3(a1.x, a1.y, a1.z), e2 = v3(a2.x, a2.y, a2.z), p2 = sub(h.p, v3(a0.x, a0.y, a0.z));
-            const float d00 = dot(e1, e1), d01 = dot(e1, e2), d11 = dot(e2, e2), d20 = dot(p2, e1), d21 = dot(p2, e2);
-            const float denom = d00 * d11 - d01 * d01;
-            const float bv = (d11 * d20 - d01 * d21) / denom;
-            const float bw = (d00 * d21 - d01 * d20) / denom;
-            const float bu = 1.0f - bv - bw;
-            const float4 t0 = __ldg(S.tri_uv + 2 * (size_t)idx), t1 = __ldg(S.tri_uv + 2 * (size_t)idx + 1);
-            float tu = bu * t0.x + bv * t0.z + (1.0f - bu - bv) * t1.x;
-            float tv = bu * t0.y + bv * t0.w + (1.0f - bu - bv) * t1.y;
-            tu = fmodf(tu, 1.0f);
-            tv = fmodf(tv, 1.0f);
-            if (tu < 0.0f) tu += 1.0f;
-            if (tv < 0.0f) tv += 1.0f;
-            h.u = tu;
-            h.v = tv;
+            tri_uv_at(S, idx, a0, a1, a2, h);
         } else {
             // no mesh has texture coordinates: get_triangle_uv over all-zero vertex uvs gives (0, 0)
             h.u = 0.0f;
@@ -743,8 +752,8 @@ __device__ __forceinline__ void finalize_rect(const DevScene& S, uint32_t idx, f
     const float a = o0 + t * d0, b = o1 + t * d1;
     float su = (a - r0.x) / (r0.y - r0.x);
     float sv = (b - r0.z) / (r0.w - r0.z);
-    su = fmodf(su * 1.0f, 1.0f);
-    sv = fmodf(sv * 1.0f, 1.0f);
+    su = fmod1(su * 1.0f);
+    sv = fmod1(sv * 1.0f);
     h.u = 1.0f * su + 0.0f;
     h.v = 1.0f * sv + 0.0f;
     h.p = at(o, d, t);

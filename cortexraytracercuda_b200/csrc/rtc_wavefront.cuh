@@ -32,7 +32,10 @@
 #else
 #define RTC_EXTEND_BOUNDS __launch_bounds__(RTC_ITER_BLOCK_MAX)
 #endif
-#ifdef RTC_SHADE_MINB
+#if defined(RTC_SHADE_MAXNREG)
+// a register cap at any value (__maxnreg__ cannot be combined with launch bounds)
+#define RTC_SHADE_BOUNDS __maxnreg__(RTC_SHADE_MAXNREG)
+#elif defined(RTC_SHADE_MINB)
 #define RTC_SHADE_BOUNDS __launch_bounds__(RTC_ITER_BLOCK_MAX, RTC_SHADE_MINB)
 #else
 #define RTC_SHADE_BOUNDS __launch_bounds__(RTC_ITER_BLOCK_MAX)

@@ -33,7 +33,8 @@ def test_device_bvh_closest_hit_identity(ctx, name, builder):
     dev = DeviceScene(ctx, scene, builder)
     info = dev.info()
     assert info["bvh_builder"] == builder and sah.info()["bvh_builder"] == BVH_SAH
-    assert info["num_nodes"] == info["num_primitives"] - 1 and info["max_leaf_size"] == 1
+    # one primitive per leaf, then subtrees of up to 4 merged where the SAH cost favours a leaf
+    assert info["num_nodes"] <= info["num_primitives"] - 1 and 1 <= info["max_leaf_size"] <= 4
     rays = golden_rays(name, 50000, seed=19)
     for depth, max_depth in ((1, 1), (0, 8)):
         a, ta = sah.trace_closest(rays, depth, max_depth)
@@ -123,7 +124,8 @@ def test_ploc_identical_boxes(ctx):
     s.sphere((0.0, -100.5, -1.0), 100.0, mat)
     ds = DeviceScene(ctx, s, BVH_DEVICE)
     info = ds.info()
-    assert info["bvh_builder"] == BVH_DEVICE and info["num_nodes"] == 5000
+    # PLOC built it (no SAH fallback); the leaf collapse then merges the coincident spheres in fours
+    assert info["bvh_builder"] == BVH_DEVICE and info["num_nodes"] <= 5000 and info["max_leaf_size"] <= 4
     rays = np.zeros((64, 8), np.float32)
     rays[:, 2] = 3.0
     rays[:, 3] = 1e-4
