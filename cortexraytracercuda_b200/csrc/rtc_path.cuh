@@ -191,12 +191,12 @@ struct PathCounters {
 // material::scatter of the hit material (metal, dielectric or lambertian; lights are handled by the
 // caller): updates the attenuation and turns `r` into the scattered ray (camera.cuh:185-225).
 template <bool CLEAN, int ORDER, class R>
-__device__ __forceinline__ void scatter_bounce(const DevScene& S, Ray& r, const Hit& h, int4 mi, float4 mf, RGB& att,
+__device__ __forceinline__ void scatter_bounce(const DevScene& S, Ray& r, Hit& h, int4 mi, float4 mf, RGB& att,
                                                R& rng, uint32_t& status) {
     constexpr bool FT = CLEAN || ORDER == 0;   // float trig in the nvcc flavour and in clean mode
     if (mi.x == 1) {
         // metal::scatter (metal.cuh:57-64)
-        RGB a = texture_value(S, mi.y, h.u, h.v, h.p, status);
+        RGB a = texture_value<FT>(S, mi.y, h, status);
         V3 refl = reflect(unit(r.d), h.n);
         V3 rs = random_in_unit_sphere<ORDER>(rng);
         r.d = add(refl, mul(mf.x, rs));
@@ -230,7 +230,7 @@ __device__ __forceinline__ void scatter_bounce(const DevScene& S, Ray& r, const 
         return;   // attenuation (1,1,1)
     }
     // lambertian::scatter (lambertian.cuh:63-131): attenuation from the texture, cosine_pdf(normal)
-    RGB a = texture_value(S, mi.y, h.u, h.v, h.p, status);
+    RGB a = texture_value<FT>(S, mi.y, h, status);
     Onb b = build_from_w(h.n);
     V3 dir;
     float pdf_val, spdf;
@@ -290,7 +290,7 @@ __device__ __forceinline__ bool is_light_material(int kind) { return kind == 3 |
 // emit (0,0,0)).  `alpha0` is set for an emission with alpha 0 - the back face of a one-sided light -
 // which makes camera::ray_color re-hit the scene from just behind it (camera.cuh:177-183).
 template <bool FT>
-__device__ __forceinline__ RGB emitted(const DevScene& S, const Ray& r, const Hit& h, int4 mi, float4 mf, bool& alpha0,
+__device__ __forceinline__ RGB emitted(const DevScene& S, const Ray& r, Hit& h, int4 mi, float4 mf, bool& alpha0,
                                        uint32_t& status) {
     RGB em = rgb(0.f, 0.f, 0.f);
     alpha0 = false;
@@ -298,7 +298,7 @@ __device__ __forceinline__ RGB emitted(const DevScene& S, const Ray& r, const Hi
         if (mf.w != 0.0f && !h.front) {
             alpha0 = true;   // RGBA(0,0,0,0): back face of a one-sided light
         } else {
-            RGB tv = texture_value(S, mi.y, h.u, h.v, h.p, status);
+            RGB tv = texture_value<FT>(S, mi.y, h, status);
             em = rgb(tv.r * mf.z, tv.g * mf.z, tv.b * mf.z);
         }
     } else if (mi.x == MAT_SPOT_LIGHT) {
@@ -317,7 +317,7 @@ __device__ __forceinline__ RGB emitted(const DevScene& S, const Ray& r, const Hi
             } else {
                 const float attn = FT ? powf(cos_theta, cone.y) : (float)pow((double)cos_theta, (double)cone.y);
                 const float k = mf.z * attn;
-                RGB tv = texture_value(S, mi.y, h.u, h.v, h.p, status);
+                RGB tv = texture_value<FT>(S, mi.y, h, status);
                 em = rgb(tv.r * k, tv.g * k, tv.b * k);
             }
         }

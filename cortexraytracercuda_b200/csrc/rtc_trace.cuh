@@ -94,6 +94,7 @@ struct Hit {
     V3 n;              // normal, facing the ray
     float u, v;
     bool front;
+    bool sphere_uv;    // a sphere hit whose u, v are not computed yet (hit_uv computes them on first use)
     int mat;
 };
 
@@ -653,7 +654,38 @@ __device__ __forceinline__ void tri_uv_at(const DevScene& S, uint32_t idx, float
     h.v = tv;
 }
 
+// get_sphere_uv (uvmapping.cuh:204-228) with the default mapping (repeat 1, scale 1, offset 0) of a
+// sphere hit's outward normal, computed the first time a texture reads the uv (only image textures do;
+// the reference computes it on every sphere hit, sphere.cuh:141-150, to the same values).  Float
+// acos/atan2 for the nvcc flavour, double-evaluated for the g++ flavour (closest to glibc).
 template <bool FLOAT_TRIG>
+__device__ __forceinline__ void hit_uv(const DevScene& S, Hit& h, V3 outward) {
+    h.sphere_uv = false;
+    float theta, phi;
+    if (FLOAT_TRIG) {
+        theta = acosf(-outward.y);
+        phi = atan2f(-outward.z, outward.x) + 3.14159265358979323846f;
+    } else {
+        theta = (float)acos((double)(-outward.y));
+        phi = (float)atan2((double)(-outward.z), (double)outward.x) + 3.14159265358979323846f;
+    }
+    float sc = phi / (2.0f * 3.14159265358979323846f);
+    float tc = theta / 3.14159265358979323846f;
+    sc = fmod1(sc * 1.0f);
+    tc = fmod1(tc * 1.0f);
+    h.u = 1.0f * sc + 0.0f;
+    h.v = 1.0f * tc + 0.0f;
+}
+// The pending uv of a world-space sphere hit: its outward normal again, (p - c) / r with the same
+// operands and roundings as finalize_prim's.
+template <bool FLOAT_TRIG>
+__device__ __forceinline__ void hit_uv(const DevScene& S, Hit& h) {
+    if (!h.sphere_uv) return;
+    const float4 s = __ldg(S.sph + (h.item & ITEM_INDEX_MASK));
+    hit_uv<FLOAT_TRIG>(S, h, divs(sub(h.p, v3(s.x, s.y, s.z)), s.w));
+}
+
+template <bool FLOAT_TRIG, bool EAGER_UV = false>
 __device__ __forceinline__ void finalize_prim(const DevScene& S, uint32_t kind, uint32_t idx, float t, V3 o, V3 d,
                                               Hit& h) {
     switch (kind) {
@@ -664,22 +696,11 @@ __device__ __forceinline__ void finalize_prim(const DevScene& S, uint32_t kind, 
         V3 c = v3(s.x, s.y, s.z);
         V3 outward = divs(sub(h.p, c), s.w);
         set_face_normal(h, d, outward);
-        // get_sphere_uv (uvmapping.cuh:204-228) with the default mapping (repeat 1, scale 1, offset 0);
-        // float acos/atan2 for the nvcc flavour, double-evaluated for the g++ flavour (closest to glibc)
-        float theta, phi;
-        if (FLOAT_TRIG) {
-            theta = acosf(-outward.y);
-            phi = atan2f(-outward.z, outward.x) + 3.14159265358979323846f;
-        } else {
-            theta = (float)acos((double)(-outward.y));
-            phi = (float)atan2((double)(-outward.z), (double)outward.x) + 3.14159265358979323846f;
-        }
-        float sc = phi / (2.0f * 3.14159265358979323846f);
-        float tc = theta / 3.14159265358979323846f;
-        sc = fmod1(sc * 1.0f);
-        tc = fmod1(tc * 1.0f);
-        h.u = 1.0f * sc + 0.0f;
-        h.v = 1.0f * tc + 0.0f;
+        // the uv (get_sphere_uv) only feeds image textures: a hit in world space computes it when a
+        // texture reads it (hit_uv, from the same hit point and record); a transformed sphere's hit
+        // (object space here) computes it now
+        h.sphere_uv = true;
+        if (EAGER_UV) hit_uv<FLOAT_TRIG>(S, h, outward);
     } break;
     case ITEM_QUAD:
     case ITEM_LIGHT: {
@@ -768,6 +789,7 @@ __device__ __forceinline__ void finalize_hit(const DevScene& S, uint32_t it, flo
     const uint32_t kind = it >> ITEM_KIND_SHIFT, idx = it & ITEM_INDEX_MASK;
     h.t = t;
     h.item = it;
+    h.sphere_uv = false;
 #if !RTC_XP
     // only the RTC_XP=1 kernels walk the xprim BVH, so an item here is always a plain primitive; keeping
     // the xprim branch out of these kernels keeps its registers out of the shade kernel
@@ -781,7 +803,7 @@ __device__ __forceinline__ void finalize_hit(const DevScene& S, uint32_t it, flo
     const int4 x = __ldg(S.xprim + idx);
     if (x.x >= 0) xf_to_object(S, x.x, o, d);
     if (x.y == XPRIM_RECT) finalize_rect(S, (uint32_t)x.z, t, o, d, h);
-    else finalize_prim<FLOAT_TRIG>(S, (uint32_t)x.y, (uint32_t)x.z, t, o, d, h);
+    else finalize_prim<FLOAT_TRIG, true>(S, (uint32_t)x.y, (uint32_t)x.z, t, o, d, h);
     if (x.x >= 0) xf_to_world(S, x.x, h.p, h.n);
 #endif
 }
@@ -796,7 +818,9 @@ __device__ __forceinline__ RGB rgb(float r, float g, float b) { RGB c; c.r = r; 
 
 // texture::value dispatch: solid (solid_color_texture.cuh:34), checker (checker_texture.cuh:33-41),
 // image (image_texture.cuh:54-70 + bitmap_image::pixel_data, bitmap_image.cuh:74-91).
-__device__ __forceinline__ RGB texture_value(const DevScene& S, int tex, float u, float v, V3 p, uint32_t& status) {
+template <bool FLOAT_TRIG>
+__device__ __forceinline__ RGB texture_value(const DevScene& S, int tex, Hit& h, uint32_t& status) {
+    const V3 p = h.p;
     for (int guard = 0; guard < 8; ++guard) {
         if ((uint32_t)tex >= S.num_textures) { status |= STATUS_BAD_TEXTURE; return rgb(0.f, 0.f, 0.f); }
         int4 ti = __ldg(S.tex_i + tex);
@@ -815,6 +839,8 @@ __device__ __forceinline__ RGB texture_value(const DevScene& S, int tex, float u
         int4 im = __ldg(S.images + ti.w);
         int W = im.y, H = im.z;
         if (H <= 0) return rgb(0.f, 1.f, 1.f);
+        hit_uv<FLOAT_TRIG>(S, h);
+        const float u = h.u, v = h.v;
         float uu = u < 0.0f ? 0.0f : (u > 1.0f ? 1.0f : u);
         float vc = v < 0.0f ? 0.0f : (v > 1.0f ? 1.0f : v);
         float vv = 1.0f - vc;
