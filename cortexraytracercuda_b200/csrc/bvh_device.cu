@@ -38,6 +38,12 @@
 #include "rtc_dev.h"
 #include "rtc_internal.h"
 
+// Largest leaf of the device-built trees after the SAH collapse (a build-time knob; 1 keeps one
+// primitive per leaf, as the builders make them).
+#ifndef RTC_DEVICE_LEAF_MAX
+#define RTC_DEVICE_LEAF_MAX 4
+#endif
+
 namespace rtc {
 namespace {
 
@@ -463,9 +469,9 @@ int build_bvh_device(const BvhInput& in, int device, BvhDeviceMethod method, Bvh
         out.max_leaf_seen = 1;
         out.nodes8.clear();
         out.num_nodes8 = 0;
-        // one primitive per leaf so far: merge small subtrees into leaves of up to 4 where the SAH cost
-        // favours it, as the host build's leaves are (fewer node visits per ray)
-        collapse_leaves(out, 4);
+        // one primitive per leaf so far: merge small subtrees into leaves of up to RTC_DEVICE_LEAF_MAX (4)
+        // where the SAH cost favours it, as the host build's leaves are (fewer node visits per ray)
+        if (RTC_DEVICE_LEAF_MAX > 1) collapse_leaves(out, RTC_DEVICE_LEAF_MAX);
         if (out.max_depth + 2 > (uint32_t)TRAVERSAL_STACK) {
             what = "device BVH too deep for the traversal stack";
             rc = BVH_DEVICE_TOO_DEEP;
