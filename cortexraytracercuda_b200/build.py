@@ -55,7 +55,6 @@ SOURCES = [
     ("rtc_obj.cpp", "rtc_obj", "cxx", []),
     ("rtc_scene_file.cpp", "rtc_scene_file", "cxx", []),
     ("bvh_device.cu", "bvh_device", "nvcc", []),
-    ("wavefront_order.cu", "wavefront_order", "nvcc", []),
     ("bvh_build.cpp", "bvh_build", "cxx", []),
 ]
 HEADERS = ["rtc_dev.h", "rtc_math.cuh", "rtc_trace.cuh", "rtc_path.cuh", "rtc_wavefront.cuh", "rtc_kernels.h",

@@ -12,10 +12,10 @@
 //   4. bottom-up boxes: every leaf walks towards the root; the first thread to reach a node stops, the
 //      second (both children now known) writes the node's 64-byte record and goes on - no thread ever
 //      waits for another.
-// The tree comes out with one primitive per leaf in sorted order; a host pass (collapse_leaves) then
-// merges subtrees of up to 4 primitives into leaves where the SAH cost favours it.  Quality is below
-// the SAH build's (more node visits per ray); the build is a few milliseconds where the host build of
-// a million triangles takes a second.
+// The tree comes out with one primitive per leaf in sorted order (a host pass, collapse_leaves, can
+// merge small subtrees into leaves by SAH cost; see RTC_DEVICE_LEAF_MAX).  Quality is below the SAH
+// build's (more node visits per ray); the build is a few milliseconds where the host build of a million
+// triangles takes a second.
 //
 // The default device method replaces steps 3-4 with PLOC (Meister and Bittner, "Parallel Locally-Ordered
 // Clustering for Bounding Volume Hierarchy Construction", IEEE TVCG 2018): starting from the sorted
@@ -38,10 +38,12 @@
 #include "rtc_dev.h"
 #include "rtc_internal.h"
 
-// Largest leaf of the device-built trees after the SAH collapse (a build-time knob; 1 keeps one
-// primitive per leaf, as the builders make them).
+// Largest leaf of the device-built trees after the SAH collapse (a build-time knob).  The default, 1,
+// keeps one primitive per leaf as the builders make them: on the meshes frame (1.31 M triangles, PLOC)
+// leaves of up to 4 cut node visits by 5% (15.04 -> 14.26 G) but the frame measured 1% slower (361 against
+// 366 Mpaths/s); the gap to the SAH tree (395 Mpaths/s, 12.61 G visits) is in its upper levels.
 #ifndef RTC_DEVICE_LEAF_MAX
-#define RTC_DEVICE_LEAF_MAX 4
+#define RTC_DEVICE_LEAF_MAX 1
 #endif
 
 namespace rtc {
@@ -469,8 +471,8 @@ int build_bvh_device(const BvhInput& in, int device, BvhDeviceMethod method, Bvh
         out.max_leaf_seen = 1;
         out.nodes8.clear();
         out.num_nodes8 = 0;
-        // one primitive per leaf so far: merge small subtrees into leaves of up to RTC_DEVICE_LEAF_MAX (4)
-        // where the SAH cost favours it, as the host build's leaves are (fewer node visits per ray)
+        // one primitive per leaf so far: with RTC_DEVICE_LEAF_MAX > 1, merge small subtrees into leaves of
+        // up to that many where the SAH cost favours it, as the host build's leaves are
         if (RTC_DEVICE_LEAF_MAX > 1) collapse_leaves(out, RTC_DEVICE_LEAF_MAX);
         if (out.max_depth + 2 > (uint32_t)TRAVERSAL_STACK) {
             what = "device BVH too deep for the traversal stack";

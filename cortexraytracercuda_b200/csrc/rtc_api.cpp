@@ -92,7 +92,6 @@ extern "C" rtc_status rtc_context_destroy(rtc_context* c) {
     cudaFree(c->d_wf);
     cudaFree(c->d_groups);
     cudaFree(c->d_batch_groups);
-    cudaFree(c->d_order);
     if (c->h_poll) cudaFreeHost(c->h_poll);
     for (cudaEvent_t& e : c->poll_ev)
         if (e) cudaEventDestroy(e);
@@ -993,14 +992,6 @@ rtc_status ensure_wavefront(rtc_context* c, uint32_t slots, WfBuffers& B) {
         size_t bytes = (size_t)slots * WF_SLOT_BYTES + 16 * 256;
         RTC_CUDA(cudaMalloc(&c->d_wf, bytes));
         c->wf_cap = slots;
-        const size_t ob = rtc_drain_order_temp_bytes(slots);
-        if (ob > c->order_cap) {
-            cudaFree(c->d_order);
-            c->d_order = nullptr;
-            c->order_cap = 0;
-            RTC_CUDA(cudaMalloc(&c->d_order, ob));
-            c->order_cap = ob;
-        }
     }
     if (!c->h_poll) {
         RTC_CUDA(cudaMallocHost(&c->h_poll, 2 * sizeof(uint32_t)));
@@ -1064,8 +1055,7 @@ rtc::WfOneFn wf_one_fn(const rtc_render_params* p, bool xp) {
 rtc_status run_wavefront(const DevScene& S, const rtc_render_params* p, const WfBuffers& B, uint32_t* d_status,
                          float4* d_out, unsigned long long* d_counters, cudaStream_t st, int num_sms,
                          const WfPoller& poll, cudaEvent_t* phase, WfRun& run, WfTimer* timer = nullptr,
-                         void* groups = nullptr, uint8_t* d_rgb8 = nullptr, void* order_temp = nullptr,
-                         size_t order_bytes = 0) {
+                         void* groups = nullptr, uint8_t* d_rgb8 = nullptr) {
     DevParams P = dev_params(p);
     P.rgb8 = d_rgb8;   // quantised output written as each pixel finishes
     const bool clean = p->mode == RTC_MODE_CLEAN;
@@ -1207,13 +1197,6 @@ rtc_status run_wavefront(const DevScene& S, const rtc_render_params* p, const Wf
     if (phase) RTC_CUDA(cudaEventRecord(phase[1], st));
     if (run.drained) {
         L.w = wf_iter(it);
-        // pixels with similar remaining work in the same warps (off with RTC_WF_DRAIN_ORDER=0); the queue
-        // only shrinks, so the count observed one batch late bounds it
-        const char* eo = std::getenv("RTC_WF_DRAIN_ORDER");
-        if (order_temp && !run.split && P.groups <= 1 && !(eo && std::atoi(eo) == 0)) {
-            e = rtc_drain_order(B, L.w, left, order_temp, order_bytes, st);
-            if (e != cudaSuccess) return cuda_fail(e, "drain ordering");
-        }
         L.grid = (int)std::max<uint32_t>(1u, (drain + 127u) / 128u);
         e = fn(WF_OP_FINISH, J, B, L);
         if (e != cudaSuccess) return cuda_fail(e, "wavefront finish");
@@ -1250,7 +1233,7 @@ rtc_status launch_wavefront(rtc_context* c, const rtc_scene* s, const rtc_render
     timer.pool = &c->kev;
     const bool timed = (p->flags & RTC_FLAG_KERNEL_TIMING) != 0;
     r = run_wavefront(rtc_scene_view(s, p), p, B, c->d_status, d_out, d_counters, st, c->num_sms, poll,
-                      c->phase_ev, run, timed ? &timer : nullptr, c->d_groups, d_rgb8, c->d_order, c->order_cap);
+                      c->phase_ev, run, timed ? &timer : nullptr, c->d_groups, d_rgb8);
     if (r != RTC_OK) return r;
     c->kev_ext = c->kev_shade = 0;
     c->kev_pairs.clear();

@@ -53,11 +53,6 @@ void rtc_carve_groups(void* base, const rtc_render_params* p, float4** part, uin
 // perspective_camera::initialize; false for a degenerate camera
 bool rtc_make_camera(const rtc_camera& c, rtc::DevCamera& out);
 int rtc_scene_device(const rtc_scene* s);
-// orders the drain queue of a single-image wavefront by sample index (wavefront_order.cu): scratch bytes
-// for up to max_n entries, and the ordering of the (at most n_max) entries of iteration w's queue
-size_t rtc_drain_order_temp_bytes(uint32_t max_n);
-cudaError_t rtc_drain_order(const rtc::WfBuffers& B, const rtc::WfIter& w, uint32_t n_max, void* temp,
-                            size_t temp_bytes, cudaStream_t st);
 // runs the wavefront engine on caller-provided buffers with synchronous queue polling: no device or
 // pinned allocations, no events
 rtc_status rtc_run_wavefront_sync(const rtc_scene* s, const rtc_render_params* p, const rtc::WfBuffers& B,

@@ -29,8 +29,6 @@ struct rtc_context {
     size_t groups_cap = 0;
     void* d_batch_groups = nullptr;    // the same for the images of a batch
     size_t batch_groups_cap = 0;
-    void* d_order = nullptr;           // sort scratch of the drain queue's ordering (rtc_drain_order)
-    size_t order_cap = 0;
     uint32_t* h_poll = nullptr;       // pinned: queue sizes read back between batches
     cudaEvent_t poll_ev[2] = {nullptr, nullptr};
     cudaEvent_t phase_ev[3] = {nullptr, nullptr, nullptr};   // render start, drain start, render end

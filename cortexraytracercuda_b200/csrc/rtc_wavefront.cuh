@@ -344,8 +344,11 @@ __device__ __forceinline__ bool wf_step(const J& jobs, const WfWindow& win, cons
                                         uint32_t& status) {
     uint4 m = __ldcs(B.meta + slot);
     const uint32_t job = wf_job(m.w);
-    const DevScene& S = jobs.scene(job);
-    const DevParams& P = jobs.params(job);
+    // local copies: a job record in the ring is read once here; through a reference it would be
+    // re-read after each store to the path state below, which the compiler cannot prove does not alias
+    // it (a single image's record is in kernel parameters either way)
+    const DevScene S = jobs.scene(job);
+    const DevParams P = jobs.params(job);
     const float4 o = __ldcs(B.ray_o + slot), d = __ldcs(B.ray_d + slot), a4 = __ldcs(B.att + slot),
                  c4 = __ldcs(B.acc + slot);
     Ray r;
