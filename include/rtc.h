@@ -501,7 +501,8 @@ typedef struct rtc_job {
 } rtc_job;
 
 typedef struct rtc_batch_params {
-    uint32_t slots;    /* path slots (pixels in flight); 0: min(total pixels, 2^22)                      */
+    uint32_t slots;    /* path slots (pixels in flight); 0: min(total work units, 2^22), with 2^20 in
+                          place of 2^22 when the first job is clean mode with RTC_FLAG_SAMPLE_GROUPS    */
     uint32_t ring;     /* job ring capacity, a power of two <= 65536; 0: 1024.  Larger batches are
                           admitted as earlier images complete.                                            */
     int32_t batch;     /* (extend, shade) iterations between two host polls; 0: 12.  A multiple of 6 is
