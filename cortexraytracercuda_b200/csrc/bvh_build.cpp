@@ -260,22 +260,34 @@ bool build_bvh(const BvhInput& in, int max_leaf, int threads, BvhOutput& out, co
     out.num_nodes = (uint32_t)(out.nodes.size() / 16);
     out.max_depth = max_depth;
 
-    // 8-wide collapse of the same tree, with quantised child boxes.  A wide node starts with its binary
-    // node's two children and repeatedly opens the inner child of largest surface area in place (left
-    // child where it was, right child just after it), so children stay in left-to-right order and the
-    // leaves are met in exactly the binary flattening's order: both layouts share one leaf order (items
-    // array).  Each node stores its box's low corner p, one power-of-two step 2^e per axis with
-    // 255 * 2^e >= the box's extent, and per child and axis an 8-bit low bound floor((lo - p) / 2^e)
-    // and high bound ceil((hi - p) / 2^e): p + q * 2^e encloses the child's box exactly (checked in
-    // double below), so the quantised test never loses a hit the binary nodes find.
+    // 8-wide collapse of the same tree: quantised child boxes, slots in octant order, links by base
+    // index (the compressed wide layout of Ylitie, Karras and Laine, HPG 2017, restated for this
+    // tree's leaves).
+    //  * Children: a wide node starts with its binary node's two children and repeatedly opens the
+    //    inner child of largest surface area, up to eight.
+    //  * Slots: bit k of slot s means the high side of axis k.  Each child goes to the slot whose
+    //    diagonal direction (+-1, +-1, +-1) best matches the offset of its box centre from the node's
+    //    (greedy assignment, largest dot product first).  A ray whose direction has sign bits `oct`
+    //    visits slot j ^ oct at step j: the child at the corner the ray enters from comes first.
+    //  * Links: inner children get consecutive node indices in slot order (node = base + rank).  Leaf
+    //    children's item ranges are copied, in slot order, to consecutive entries of a second item
+    //    list (`items8`, entries = positions in `order`), so a leaf is (item base + offset, count).
+    //    One byte per slot: 0x80 | rank for an inner child, (count - 1) << 5 | offset for a leaf; the
+    //    node's valid mask marks the slots in use.
+    //  * Boxes: the node's low corner p, one power-of-two step 2^e per axis with 255 * 2^e >= the
+    //    box's extent, and per child and axis 8-bit bounds floor((lo - p) / 2^e) and
+    //    ceil((hi - p) / 2^e): p + q * 2^e encloses the child's box (checked in double below), so the
+    //    quantised test never loses a hit the binary nodes find.
     out.nodes8.clear();
-    auto alloc8 = [&]() {
-        out.nodes8.resize(out.nodes8.size() + NODE8_FLOATS, 0.0f);
-        return (int32_t)(out.nodes8.size() / NODE8_FLOATS - 1);
+    out.items8.clear();
+    auto alloc8 = [&](int count) {
+        const int32_t first = (int32_t)(out.nodes8.size() / NODE8_FLOATS);
+        out.nodes8.resize(out.nodes8.size() + (size_t)count * NODE8_FLOATS, 0.0f);
+        return first;
     };
-    std::vector<int32_t> leaf_enc;
+    // the binary flattening's leaf encoding of each binary leaf (replayed in its DFS left-first order)
+    std::vector<int32_t> leaf_of(B.nodes.size(), 0);
     {
-        // the binary flattening assigned leaf encodings in DFS left-first order: replay it
         std::vector<int32_t> st;
         if (root >= 0) st.push_back(root);
         uint32_t first = 0;
@@ -284,7 +296,7 @@ bool build_bvh(const BvhInput& in, int max_leaf, int threads, BvhOutput& out, co
             st.pop_back();
             const BNode& bn = B.nodes[b];
             if (bn.leaf) {
-                leaf_enc.push_back((int32_t)~((first << LEAF_COUNT_BITS) | bn.count));
+                leaf_of[b] = (int32_t)~((first << LEAF_COUNT_BITS) | bn.count);
                 first += bn.count;
             } else {
                 st.push_back(bn.right);
@@ -292,69 +304,105 @@ bool build_bvh(const BvhInput& in, int max_leaf, int threads, BvhOutput& out, co
             }
         }
     }
-    std::vector<int32_t> leaf_of(B.nodes.size(), 0);
-    {
-        std::vector<int32_t> st;
-        if (root >= 0) st.push_back(root);
-        size_t k = 0;
-        while (!st.empty()) {
-            int32_t b = st.back();
-            st.pop_back();
-            const BNode& bn = B.nodes[b];
-            if (bn.leaf) {
-                leaf_of[b] = leaf_enc[k++];
-            } else {
-                st.push_back(bn.right);
-                st.push_back(bn.left);
-            }
-        }
-    }
-    bool quant_ok = true;
-    // writes node `slot` from `n` children (binary node ids) and their links
-    auto put8 = [&](int32_t slot, const int32_t* ch, int n, const int32_t* link) {
-        float* f = &out.nodes8[NODE8_FLOATS * (size_t)slot];
+    struct Work8 { int32_t bnode; int32_t slot; uint32_t depth; };
+    bool wide_ok = true;
+    // writes wide node `at` from `n` children (binary node ids); inner children are queued on `kids`
+    auto put8 = [&](int32_t at, const int32_t* ch, int n, uint32_t depth, std::vector<Work8>& kids) {
         Aabb nb;
         for (int k = 0; k < 3; ++k) { nb.lo[k] = INFINITY; nb.hi[k] = -INFINITY; }
         for (int i = 0; i < n; ++i) grow(nb, B.nodes[ch[i]].box);
-        uint32_t hdr = (uint32_t)n << 24;
-        uint8_t q[3][2][8] = {};   // axis, (low, high), child
+        // slot assignment
+        double score[8][8];
+        for (int i = 0; i < n; ++i) {
+            const Aabb& c = B.nodes[ch[i]].box;
+            double off[3];
+            for (int k = 0; k < 3; ++k)
+                off[k] = 0.5 * ((double)c.lo[k] + (double)c.hi[k]) - 0.5 * ((double)nb.lo[k] + (double)nb.hi[k]);
+            for (int sl = 0; sl < 8; ++sl)
+                score[i][sl] = ((sl & 1) ? off[0] : -off[0]) + ((sl & 2) ? off[1] : -off[1]) +
+                               ((sl & 4) ? off[2] : -off[2]);
+        }
+        int child_in[8] = {-1, -1, -1, -1, -1, -1, -1, -1};
+        bool placed[8] = {};
+        for (int round = 0; round < n; ++round) {
+            int bi = -1, bs = -1;
+            double best = -INFINITY;
+            for (int i = 0; i < n; ++i) {
+                if (placed[i]) continue;
+                for (int sl = 0; sl < 8; ++sl)
+                    if (child_in[sl] < 0 && score[i][sl] > best) { best = score[i][sl]; bi = i; bs = sl; }
+            }
+            placed[bi] = true;
+            child_in[bs] = bi;
+        }
+        // links
+        int inner = 0;
+        for (int sl = 0; sl < 8; ++sl)
+            if (child_in[sl] >= 0 && !B.nodes[ch[child_in[sl]]].leaf) ++inner;
+        const int32_t base = inner ? alloc8(inner) : 0;
+        const uint32_t item_base = (uint32_t)out.items8.size();
+        uint32_t valid = 0, meta[2] = {0u, 0u};
+        int rank = 0;
+        for (int sl = 0; sl < 8; ++sl) {
+            if (child_in[sl] < 0) continue;
+            const int32_t b = ch[child_in[sl]];
+            valid |= 1u << sl;
+            uint32_t byte;
+            if (B.nodes[b].leaf) {
+                const uint32_t enc = (uint32_t)~leaf_of[b];
+                const uint32_t first = enc >> LEAF_COUNT_BITS, cnt = enc & MAX_LEAF;
+                const uint32_t off = (uint32_t)out.items8.size() - item_base;
+                if (cnt < 1 || cnt > 4 || off > 31) wide_ok = false;
+                byte = ((cnt - 1u) & 3u) << 5 | (off & 31u);
+                for (uint32_t i = 0; i < cnt; ++i) out.items8.push_back(first + i);
+            } else {
+                byte = 0x80u | (uint32_t)rank;
+                kids.push_back({b, base + rank, depth + 1});
+                ++rank;
+            }
+            meta[sl >> 2] |= byte << (8 * (sl & 3));
+        }
+        // quantised boxes
+        uint32_t hdr = valid << 24;
+        uint8_t q[3][2][8] = {};   // axis, (low, high), slot
         for (int k = 0; k < 3; ++k) {
             const double ext = (double)nb.hi[k] - (double)nb.lo[k];
             int e = -126;
             while (e < 127 && std::ldexp(255.0, e) < ext) ++e;
             const double step = std::ldexp(1.0, e);
             hdr |= (uint32_t)(e + 127) << (8 * k);
-            for (int i = 0; i < n; ++i) {
-                const Aabb& c = B.nodes[ch[i]].box;
+            for (int sl = 0; sl < 8; ++sl) {
+                if (child_in[sl] < 0) continue;
+                const Aabb& c = B.nodes[ch[child_in[sl]]].box;
                 const double ql = std::floor(((double)c.lo[k] - (double)nb.lo[k]) / step);
                 const double qh = std::ceil(((double)c.hi[k] - (double)nb.lo[k]) / step);
                 const double l = std::min(std::max(ql, 0.0), 255.0), h = std::min(std::max(qh, 0.0), 255.0);
                 if ((double)nb.lo[k] + l * step > (double)c.lo[k] || (double)nb.lo[k] + h * step < (double)c.hi[k])
-                    quant_ok = false;
-                q[k][0][i] = (uint8_t)l;
-                q[k][1][i] = (uint8_t)h;
+                    wide_ok = false;
+                q[k][0][sl] = (uint8_t)l;
+                q[k][1][sl] = (uint8_t)h;
             }
         }
+        float* f = &out.nodes8[NODE8_FLOATS * (size_t)at];   // after alloc8: nodes8 may have moved
         f[0] = nb.lo[0];
         f[1] = nb.lo[1];
         f[2] = nb.lo[2];
         std::memcpy(&f[3], &hdr, 4);
-        for (int k = 0; k < 3; ++k) {   // float4 1 + k: low bytes of children 0-7, then high bytes
-            std::memcpy(&f[4 + 4 * k], q[k][0], 8);
-            std::memcpy(&f[6 + 4 * k], q[k][1], 8);
-        }
-        for (int i = 0; i < 8; ++i) {
-            const int32_t l = i < n ? link[i] : (int32_t)~0u;
-            std::memcpy(&f[16 + i], &l, 4);
+        std::memcpy(&f[4], &base, 4);
+        std::memcpy(&f[5], &item_base, 4);
+        std::memcpy(&f[6], &meta[0], 4);
+        std::memcpy(&f[7], &meta[1], 4);
+        for (int k = 0; k < 3; ++k) {   // float4 2 + k: low bytes of slots 0-7, then high bytes
+            std::memcpy(&f[8 + 4 * k], q[k][0], 8);
+            std::memcpy(&f[10 + 4 * k], q[k][1], 8);
         }
     };
-    struct Work8 { int32_t bnode; int32_t slot; uint32_t depth; };
-    std::vector<Work8> w8;
+    std::vector<Work8> w8, kids;
     uint32_t depth8 = 1;
-    int32_t r8 = alloc8();
+    const int32_t r8 = alloc8(1);
     if (root >= 0) {
         if (B.nodes[root].leaf) {
-            put8(r8, &root, 1, &leaf_of[root]);
+            put8(r8, &root, 1, 1, kids);
         } else {
             w8.push_back({root, r8, 1});
         }
@@ -380,25 +428,16 @@ bool build_bvh(const BvhInput& in, int max_leaf, int threads, BvhOutput& out, co
             ch[best + 1] = o.right;
             ++n;
         }
-        // inner children get their node index now and are expanded later, in order
-        int32_t link[8];
-        std::vector<Work8> kids;
-        for (int i = 0; i < n; ++i) {
-            const BNode& c = B.nodes[ch[i]];
-            if (c.leaf) {
-                link[i] = leaf_of[ch[i]];
-            } else {
-                link[i] = alloc8();
-                kids.push_back({ch[i], link[i], w.depth + 1});
-            }
-        }
-        put8(w.slot, ch, n, link);
+        kids.clear();
+        put8(w.slot, ch, n, w.depth, kids);
+        // depth first, first slot next: a node's subtree sits close to it in memory
         for (auto it = kids.rbegin(); it != kids.rend(); ++it) w8.push_back(*it);
     }
     out.num_nodes8 = (uint32_t)(out.nodes8.size() / NODE8_FLOATS);
-    // the 8-wide walk holds at most 7 entries per level plus the children of the deepest node
-    if (!quant_ok || 7 * depth8 + 8 > (uint32_t)TRAVERSAL_STACK8) {
+    // the walk keeps at most one pending group per level; nodes are addressed with 24 bits on its stack
+    if (!wide_ok || depth8 + 1 > (uint32_t)TRAVERSAL_STACK8 || out.num_nodes8 >= (1u << 24)) {
         out.nodes8.clear();   // renders use the binary nodes
+        out.items8.clear();
         out.num_nodes8 = 0;
     }
     if (max_depth + 2 > (uint32_t)TRAVERSAL_STACK) { if (err) *err = "BVH too deep for the traversal stack"; return false; }

@@ -24,8 +24,8 @@ struct BvhInput {
 struct BvhOutput {
     std::vector<float> nodes;      // 16 floats per node (4 x float4), see rtc_dev.h
     std::vector<float> nodes8;     // the same tree collapsed to 8-wide nodes with quantised child boxes:
-                                   // NODE8_FLOATS (6 x float4) per node, see rtc_dev.h; same leaves, same
-                                   // leaf order
+                                   // NODE8_FLOATS (5 x float4) per node, see rtc_dev.h; same leaves
+    std::vector<uint32_t> items8;  // the 8-wide nodes' leaf ranges: per entry, a position in `order`
     std::vector<uint32_t> order;   // primitive index per leaf slot, leaf order
     uint32_t num_nodes = 0;
     uint32_t num_nodes8 = 0;

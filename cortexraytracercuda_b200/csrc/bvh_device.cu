@@ -470,6 +470,7 @@ int build_bvh_device(const BvhInput& in, int device, BvhDeviceMethod method, Bvh
         }
         out.max_leaf_seen = 1;
         out.nodes8.clear();
+        out.items8.clear();
         out.num_nodes8 = 0;
         // one primitive per leaf so far: with RTC_DEVICE_LEAF_MAX > 1, merge small subtrees into leaves of
         // up to that many where the SAH cost favours it, as the host build's leaves are

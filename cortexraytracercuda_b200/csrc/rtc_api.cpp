@@ -682,6 +682,9 @@ rtc_status rtc_build_host_scene(const rtc_scene_desc* d, HostScene& H, uint32_t 
         (xk ? xitems[k - bvh.order.size()] : items[k]) = ((uint32_t)pr.kind << ITEM_KIND_SHIFT) | typed;
     }
     for (uint32_t i = 0; i < d->num_transforms; ++i) put_transform(d->transforms[i], xf);
+    // the 8-wide nodes' leaf items: the same item words, regrouped per wide node
+    std::vector<uint32_t> items8(bvh.items8.size());
+    for (size_t k = 0; k < items8.size(); ++k) items8[k] = items[bvh.items8[k]];
 
     // ---- camera: perspective_camera::initialize (perspective_camera.cuh:41-108) -----------------
     DevCamera cam{};
@@ -700,6 +703,7 @@ rtc_status rtc_build_host_scene(const rtc_scene_desc* d, HostScene& H, uint32_t 
     size_t o_nodes = add_chunk(bvh.nodes.data(), bvh.nodes.size() * sizeof(float));
     size_t o_nodes8 = add_chunk(bvh.nodes8.data(), bvh.nodes8.size() * sizeof(float));
     size_t o_items = add_chunk(items.data(), items.size() * 4);
+    size_t o_items8 = add_chunk(items8.data(), items8.size() * 4);
     size_t o_sph = add_chunk(sph.data(), sph.size() * 16);
     size_t o_sphx = add_chunk(sph_aux.data(), sph_aux.size() * 8);
     size_t o_tri = add_chunk(tri.data(), tri.size() * 16);
@@ -766,6 +770,7 @@ rtc_status rtc_build_host_scene(const rtc_scene_desc* d, HostScene& H, uint32_t 
     D.nodes = (const float4*)off(o_nodes);
     D.nodes8 = bvh.num_nodes8 ? (const float4*)off(o_nodes8) : nullptr;
     D.items = (const uint32_t*)off(o_items);
+    D.items8 = bvh.num_nodes8 ? (const uint32_t*)off(o_items8) : nullptr;
     D.sph = (const float4*)off(o_sph);
     D.sph_aux = (const int2*)off(o_sphx);
     D.tri = (const float4*)off(o_tri);
@@ -830,7 +835,7 @@ DevScene rtc_rebase_scene(const HostScene& H, uint8_t* base) {
     };
     rb(D.nodes);
     rb(D.items);
-    if (D.nodes8) rb(D.nodes8);
+    if (D.nodes8) { rb(D.nodes8); rb(D.items8); }
     rb(D.sph); rb(D.sph_aux); rb(D.tri); rb(D.tri_n); rb(D.tri_vn); rb(D.quad);
     rb(D.light); rb(D.mat_i); rb(D.mat_f); rb(D.tex_i); rb(D.tex_f); rb(D.images); rb(D.image_bytes);
     rb(D.xprim); rb(D.xf); rb(D.rect);

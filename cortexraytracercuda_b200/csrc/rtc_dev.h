@@ -6,13 +6,18 @@
 //                n0 = (L.lo.x, L.hi.x, L.lo.y, L.hi.y)   n1 = (R.lo.x, R.hi.x, R.lo.y, R.hi.y)
 //                n2 = (L.lo.z, L.hi.z, R.lo.z, R.hi.z)   n3 = (child L, child R, -, -) as int bits
 //              child >= 0: inner node index; child < 0: leaf, ~child = (first_item << 5) | count.
-//   nodes8     the same tree collapsed to 8-wide nodes with quantised child boxes, 6 x float4 = 96 B:
-//                (p.xyz, header)  header = (e.x+127) | (e.y+127) << 8 | (e.z+127) << 16 | children << 24
+//   nodes8     the same tree collapsed to 8-wide nodes with quantised child boxes, 5 x float4 = 80 B:
+//                (p.xyz, header)  header = (e.x+127) | (e.y+127) << 8 | (e.z+127) << 16 | valid << 24
+//                (child base, item base, link bytes of slots 0-3, link bytes of slots 4-7) as int bits
 //                (qlo.x[0..7] bytes, qhi.x[0..7] bytes) (same for y) (same for z)
-//                (child[0..3] as int bits) (child[4..7] as int bits)
-//              child c's box on axis a is [p.a + qlo.a[c] * 2^e.a, p.a + qhi.a[c] * 2^e.a] (rounded outwards
-//              when built, so it encloses the child's exact box); slots at or past `children` are
-//              unused.  Same leaves and leaf order as `nodes`; renders use it when RTC_FLAG_WIDE_BVH is set.
+//              slot s's box on axis a is [p.a + qlo.a[s] * 2^e.a, p.a + qhi.a[s] * 2^e.a] (rounded outwards
+//              when built, so it encloses the child's exact box); `valid` has a bit per slot in use.
+//              Bit k of s is the high side of axis k (children placed by the direction of their centre
+//              from the node's).  Link byte: 0x80 | r for an inner child, node = child base + r (a node's
+//              inner children are consecutive); (count - 1) << 5 | offset for a leaf, whose items are
+//              items8[item base + offset ...] (count 1-4).  Renders use it when RTC_FLAG_WIDE_BVH is set.
+//   items8     uint32 per 8-wide leaf entry: the same item words as `items`, regrouped so that the leaves
+//              of one wide node are consecutive.
 //   items      uint32 per leaf entry, leaf order: (kind << 29) | index into that kind's array.
 //   xprim      int4 per transformed primitive or box face (leaf order): (transform or -1, inner kind,
 //              inner index, global id).  The inner record sits in the sph / quad / tri / rect array.
@@ -67,8 +72,8 @@ constexpr int MAT_SPOT_LIGHT = 4;
 constexpr int LEAF_COUNT_BITS = 5;
 constexpr int MAX_LEAF = 31;
 constexpr int TRAVERSAL_STACK = 64;
-constexpr int TRAVERSAL_STACK8 = 128;  // 8-wide: up to 7 entries per level, leaves included
-constexpr int NODE8_FLOATS = 24;       // 6 x float4 per 8-wide node
+constexpr int TRAVERSAL_STACK8 = 64;   // 8-wide: one pending group (node, slots left) per level
+constexpr int NODE8_FLOATS = 20;       // 5 x float4 per 8-wide node
 
 // kernel status word bits (device -> host)
 enum StatusBits : uint32_t {
@@ -107,6 +112,7 @@ struct DevScene {
     const float4* nodes;
     const float4* nodes8;      // null: binary traversal
     const uint32_t* items;
+    const uint32_t* items8;    // the 8-wide nodes' leaf items (with nodes8)
     const float4* sph;
     const int2* sph_aux;
     const float4* tri;

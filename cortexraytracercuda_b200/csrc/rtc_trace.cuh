@@ -342,15 +342,15 @@ __device__ __forceinline__ void test_leaf_xprims(const DevScene& S, int32_t chil
     }
 }
 
+// Items [first, first + cnt) of an item list (`items`, or `items8` for the 8-wide nodes; both hold
+// num_items entries) against [tmin, best_t].
 template <bool EXACT>
-__device__ __forceinline__ void test_leaf(const DevScene& S, int32_t child, V3 o, V3 d, float tmin, float& best_t,
-                                          uint32_t& best_item, bool hide_invisible, TraceStats& st,
-                                          uint32_t& status) {
-    uint32_t enc = (uint32_t)(~child);
-    uint32_t first = enc >> LEAF_COUNT_BITS, cnt = enc & MAX_LEAF;
+__device__ __forceinline__ void test_items(const DevScene& S, const uint32_t* items, uint32_t first, uint32_t cnt,
+                                           V3 o, V3 d, float tmin, float& best_t, uint32_t& best_item,
+                                           bool hide_invisible, TraceStats& st, uint32_t& status) {
     if (first + cnt > S.num_items) { status |= STATUS_BAD_ITEM; return; }
     for (uint32_t k = 0; k < cnt; ++k) {
-        uint32_t it = ld_scene(S.items + first + k);
+        uint32_t it = ld_scene(items + first + k);
         uint32_t kind = it >> ITEM_KIND_SHIFT, idx = it & ITEM_INDEX_MASK;
         float t;
         st.prims++;
@@ -400,6 +400,16 @@ __device__ __forceinline__ void test_leaf(const DevScene& S, int32_t child, V3 o
     }
 }
 
+// A binary leaf: child = ~((first << LEAF_COUNT_BITS) | count) over `items`.
+template <bool EXACT>
+__device__ __forceinline__ void test_leaf(const DevScene& S, int32_t child, V3 o, V3 d, float tmin, float& best_t,
+                                          uint32_t& best_item, bool hide_invisible, TraceStats& st,
+                                          uint32_t& status) {
+    const uint32_t enc = (uint32_t)(~child);
+    test_items<EXACT>(S, S.items, enc >> LEAF_COUNT_BITS, enc & MAX_LEAF, o, d, tmin, best_t, best_item,
+                      hide_invisible, st, status);
+}
+
 // Direction component for the slab tests' reciprocal.  The slab distance is fma(lo, 1/d, -o/d); with a
 // zero component the two infinite products cancel to NaN or collapse to -inf by the SIGNS of lo and o,
 // not by whether o lies between the slab's planes, so a box whose slab holds the origin could be culled
@@ -409,105 +419,115 @@ __device__ __forceinline__ void test_leaf(const DevScene& S, int32_t child, V3 o
 // are unchanged, so every other ray walks the tree exactly as before.
 __device__ __forceinline__ float slab_dir(float x) { return fabsf(x) < 1e-20f ? copysignf(1e-20f, x) : x; }
 
-__device__ __forceinline__ void cswap(uint32_t& a, uint32_t& b) {
-    const uint32_t lo = min(a, b), hi = max(a, b);
-    a = lo;
-    b = hi;
-}
-
 // Byte `c` (0-3) of `w` as a float: the byte becomes the low mantissa byte of 2^23, and subtracting
 // 2^23 leaves exactly its value (two full-rate instructions instead of an integer-to-float conversion).
 __device__ __forceinline__ float byte_f(uint32_t w, int c) {
     return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7650u | (uint32_t)c)) - 8388608.0f;
 }
 
-// Link of child `c` (0-7) from the node's two link words, by selects (no indexed register array).
-__device__ __forceinline__ int32_t child8(const float4& a, const float4& b, uint32_t c) {
-    const float4& v = c < 4u ? a : b;
-    const uint32_t k = c & 3u;
-    return __float_as_int(k < 2u ? (k == 0u ? v.x : v.y) : (k == 2u ? v.z : v.w));
+// An 8-wide node's link word (child base, item base, link bytes 0-3, link bytes 4-7).
+__device__ __forceinline__ int4 ld_links(const float4* p) {
+    const float4 v = ld_scene(p);
+    return make_int4(__float_as_int(v.x), __float_as_int(v.y), __float_as_int(v.z), __float_as_int(v.w));
 }
 
-// Closest hit through the 8-wide nodes with quantised child boxes.  A visit loads one 96-byte node and
-// tests its children's boxes: on each axis the child bound p + q * 2^e gives the distance
-// fma(q, 2^e / d, (p - o) / d), the same rounding model as the binary slab (the step is a power of two,
-// so 2^e / d is exact).  Hit children are sorted by entry distance (key = distance bits with the child
-// slot in the three low bits; distances are >= tmin > 0, so the bits order like the floats, and clearing
-// the low bits rounds down, which keeps the culling conservative) with a 19-comparator network and
-// pushed far to near.  Leaves travel through the stack too, so the leaf test is inlined once; an entry
-// farther than the current best hit is dropped when popped.
+// Bits of an 8-bit mask moved from position s to position s ^ oct.
+__device__ __forceinline__ uint32_t octant_order(uint32_t h, uint32_t oct) {
+    if (oct & 1u) h = ((h & 0x55u) << 1) | ((h >> 1) & 0x55u);
+    if (oct & 2u) h = ((h & 0x33u) << 2) | ((h >> 2) & 0x33u);
+    if (oct & 4u) h = ((h & 0x0fu) << 4) | ((h >> 4) & 0x0fu);
+    return h;
+}
+
+// Closest hit through the 8-wide nodes (compressed wide layout, after Ylitie, Karras and Laine, HPG
+// 2017).  A visit loads one 80-byte node and tests its children's quantised boxes: on each axis the
+// bound p + q * 2^e gives the distance fma(q, 2^e / d, (p - o) / d), the same rounding model as the
+// binary slab (the step is a power of two, so 2^e / d is exact).  The ray's direction signs pick, per
+// axis, which of a child's two bounds is its entry and which its exit plane, so a child costs six
+// distances and no min/max per axis.  The hit children form a group: (node, mask of hit slots), the
+// mask in visiting order (bit j = slot j ^ oct, near corner first).  The walk takes the group's next
+// child: a leaf is tested in place; for an inner child the rest of the group is pushed as one 32-bit
+// entry (node << 8 | mask) and the child's own group replaces it.  No sort, no distances on the stack:
+// at most one entry per level.
 template <bool EXACT>
 __device__ __forceinline__ bool closest_hit8(const DevScene& S, V3 o, V3 d, V3 inv, V3 oi, float tmin, float tmax,
                                              bool hide_invisible, float& t_out, uint32_t& item_out,
                                              TraceStats& st, uint32_t& status) {
     float best_t = tmax;
     uint32_t best_item = 0xffffffffu;
-    int2 stk[TRAVERSAL_STACK8];   // (child reference, entry distance bits)
+    // direction sign bits; slab_dir keeps the sign of a zero component, so inv has it too
+    const uint32_t oct = (inv.x < 0.0f ? 1u : 0u) | (inv.y < 0.0f ? 2u : 0u) | (inv.z < 0.0f ? 4u : 0u);
+    uint32_t stk[TRAVERSAL_STACK8];
     int sp = 0;
-    int32_t ref = 0;   // the root node
+    uint32_t node = 0;       // the current group: its node, the slots still to take (visiting order)
+    uint32_t hits = 0;       // and the node's links (child base, item base, link bytes)
+    int4 links = make_int4(0, 0, 0, 0);
+    int32_t visit = 0;       // node to visit at the top of the next pass, -1: none
     // A walk visits each node and leaf at most once; more visits than that mean malformed links, and
     // the walk stops with STATUS_TIMEOUT instead of running on.
     const uint32_t visit_limit = 2u * (S.num_nodes8 + S.num_items) + 64u;
     uint32_t visits = 0;
     for (;;) {
         if (++visits > visit_limit) { status |= STATUS_TIMEOUT; break; }
-        if (ref >= 0) {
-            if ((uint32_t)ref >= S.num_nodes8) { status |= STATUS_BAD_ITEM; break; }
-            const float4* np = S.nodes8 + 6 * (size_t)ref;
-            const float4 h = ld_scene(np), qx = ld_scene(np + 1), qy = ld_scene(np + 2), qz = ld_scene(np + 3);
-            const float4 la = ld_scene(np + 4), lb = ld_scene(np + 5);
+        if (visit >= 0) {
+            if ((uint32_t)visit >= S.num_nodes8) { status |= STATUS_BAD_ITEM; break; }
+            node = (uint32_t)visit;
+            visit = -1;
+            const float4* np = S.nodes8 + 5 * (size_t)node;
+            const float4 h = ld_scene(np), qx = ld_scene(np + 2), qy = ld_scene(np + 3), qz = ld_scene(np + 4);
+            links = ld_links(np + 1);
             st.nodes++;
             const uint32_t hdr = __float_as_uint(h.w);
-            const uint32_t n = hdr >> 24;
             const float ax = __uint_as_float((hdr & 0xffu) << 23) * inv.x;
             const float ay = __uint_as_float(((hdr >> 8) & 0xffu) << 23) * inv.y;
             const float az = __uint_as_float(((hdr >> 16) & 0xffu) << 23) * inv.z;
             const float bx = __fmaf_rn(h.x, inv.x, -oi.x), by = __fmaf_rn(h.y, inv.y, -oi.y),
                         bz = __fmaf_rn(h.z, inv.z, -oi.z);
-            uint32_t key[8];
+            // entry (n) and exit (f) bound words per axis: the low bounds are the entry planes where the
+            // direction is positive, the high bounds where it is negative
+            const uint32_t nx0 = __float_as_uint((oct & 1u) ? qx.z : qx.x), nx1 = __float_as_uint((oct & 1u) ? qx.w : qx.y);
+            const uint32_t fx0 = __float_as_uint((oct & 1u) ? qx.x : qx.z), fx1 = __float_as_uint((oct & 1u) ? qx.y : qx.w);
+            const uint32_t ny0 = __float_as_uint((oct & 2u) ? qy.z : qy.x), ny1 = __float_as_uint((oct & 2u) ? qy.w : qy.y);
+            const uint32_t fy0 = __float_as_uint((oct & 2u) ? qy.x : qy.z), fy1 = __float_as_uint((oct & 2u) ? qy.y : qy.w);
+            const uint32_t nz0 = __float_as_uint((oct & 4u) ? qz.z : qz.x), nz1 = __float_as_uint((oct & 4u) ? qz.w : qz.y);
+            const uint32_t fz0 = __float_as_uint((oct & 4u) ? qz.x : qz.z), fz1 = __float_as_uint((oct & 4u) ? qz.y : qz.w);
+            uint32_t hs = 0;
 #pragma unroll
             for (int c = 0; c < 8; ++c) {
                 const int b = c & 3;
-                const uint32_t wlx = __float_as_uint(c < 4 ? qx.x : qx.y), whx = __float_as_uint(c < 4 ? qx.z : qx.w);
-                const uint32_t wly = __float_as_uint(c < 4 ? qy.x : qy.y), why = __float_as_uint(c < 4 ? qy.z : qy.w);
-                const uint32_t wlz = __float_as_uint(c < 4 ? qz.x : qz.y), whz = __float_as_uint(c < 4 ? qz.z : qz.w);
-                const float x0 = __fmaf_rn(byte_f(wlx, b), ax, bx), x1 = __fmaf_rn(byte_f(whx, b), ax, bx);
-                const float y0 = __fmaf_rn(byte_f(wly, b), ay, by), y1 = __fmaf_rn(byte_f(why, b), ay, by);
-                const float z0 = __fmaf_rn(byte_f(wlz, b), az, bz), z1 = __fmaf_rn(byte_f(whz, b), az, bz);
-                const float tn = fmaxf(fmaxf(fminf(x0, x1), fminf(y0, y1)), fmaxf(fminf(z0, z1), tmin));
-                const float tf = fminf(fminf(fmaxf(x0, x1), fmaxf(y0, y1)), fminf(fmaxf(z0, z1), best_t));
-                key[c] = ((uint32_t)c < n && tn <= tf) ? ((__float_as_uint(tn) & ~7u) | (uint32_t)c) : 0xffffffffu;
+                const float tnx = __fmaf_rn(byte_f(c < 4 ? nx0 : nx1, b), ax, bx);
+                const float tfx = __fmaf_rn(byte_f(c < 4 ? fx0 : fx1, b), ax, bx);
+                const float tny = __fmaf_rn(byte_f(c < 4 ? ny0 : ny1, b), ay, by);
+                const float tfy = __fmaf_rn(byte_f(c < 4 ? fy0 : fy1, b), ay, by);
+                const float tnz = __fmaf_rn(byte_f(c < 4 ? nz0 : nz1, b), az, bz);
+                const float tfz = __fmaf_rn(byte_f(c < 4 ? fz0 : fz1, b), az, bz);
+                const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin));
+                const float tf = fminf(fminf(tfx, tfy), fminf(tfz, best_t));
+                hs |= (tn <= tf ? 1u : 0u) << c;
             }
-            cswap(key[0], key[1]); cswap(key[2], key[3]); cswap(key[4], key[5]); cswap(key[6], key[7]);
-            cswap(key[0], key[2]); cswap(key[1], key[3]); cswap(key[4], key[6]); cswap(key[5], key[7]);
-            cswap(key[1], key[2]); cswap(key[5], key[6]);
-            cswap(key[0], key[4]); cswap(key[1], key[5]); cswap(key[2], key[6]); cswap(key[3], key[7]);
-            cswap(key[2], key[4]); cswap(key[3], key[5]);
-            cswap(key[1], key[2]); cswap(key[3], key[4]); cswap(key[5], key[6]);
-            // push far to near: the nearest child ends on top
-#pragma unroll
-            for (int q = 7; q >= 0; --q) {
-                const uint32_t k = key[q];
-                if (k == 0xffffffffu) continue;
+            hits = octant_order(hs & (hdr >> 24), oct);
+        }
+        if (hits == 0u) {
+            if (sp == 0) break;
+            const uint32_t e = stk[--sp];
+            node = e >> 8;
+            hits = e & 0xffu;
+            links = ld_links(S.nodes8 + 5 * (size_t)node + 1);
+        }
+        // the group's next child
+        const uint32_t slot = (uint32_t)(__ffs(hits) - 1) ^ oct;
+        hits &= hits - 1u;
+        const uint32_t lb = ((uint32_t)(slot < 4u ? links.z : links.w) >> (8u * (slot & 3u))) & 0xffu;
+        if (lb & 0x80u) {
+            if (hits) {
                 if (sp >= TRAVERSAL_STACK8) { status |= STATUS_STACK_OVERFLOW; break; }
-                stk[sp] = make_int2(child8(la, lb, k & 7u), (int)(k & ~7u));
-                ++sp;
+                stk[sp++] = (node << 8) | hits;
             }
-            if (status & STATUS_STACK_OVERFLOW) break;
+            visit = links.x + (int32_t)(lb & 7u);
         } else {
-            test_leaf<EXACT>(S, ref, o, d, tmin, best_t, best_item, hide_invisible, st, status);
+            test_items<EXACT>(S, S.items8, (uint32_t)links.y + (lb & 31u), ((lb >> 5) & 3u) + 1u, o, d, tmin, best_t,
+                              best_item, hide_invisible, st, status);
         }
-        // next entry that is still nearer than the best hit
-        bool found = false;
-        while (sp > 0) {
-            const int2 e = stk[--sp];
-            if (__int_as_float(e.y) <= best_t) {
-                ref = e.x;
-                found = true;
-                break;
-            }
-        }
-        if (!found) break;
     }
     t_out = best_t;
     item_out = best_item;
