@@ -205,9 +205,68 @@ struct TraceStats {
     uint32_t nodes, prims;
 };
 
+// Packed pairs of floats for the box tests (sm_100's f32x2 arithmetic: one instruction, two lanes, each
+// rounded as the scalar instruction rounds it) and three-input min / max (sm_100).  RTC_WIDE_PACKED=0 /
+// RTC_BINARY_PACKED=0 build the scalar form of the same arithmetic for the 8-wide / binary nodes.
+#ifndef RTC_WIDE_PACKED
+#define RTC_WIDE_PACKED 1
+#endif
+#ifndef RTC_BINARY_PACKED
+#define RTC_BINARY_PACKED 1
+#endif
+typedef unsigned long long F2;
+__device__ __forceinline__ F2 f2(float lo, float hi) {
+    F2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void split_f2(F2 v, float& lo, float& hi) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ F2 fma_f2(F2 a, F2 b, F2 c) {
+    F2 d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+// bytes c and c + 1 (c = 0 or 2) of `w` as a pair of floats, as byte_f does for one
+__device__ __forceinline__ F2 bytes_f2(uint32_t w, int c) {
+    const F2 two23 = 0x4B0000004B000000ull;
+    const F2 v = f2(__uint_as_float(__byte_perm(w, 0x4B000000u, 0x7650u | (uint32_t)c)),
+                    __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7650u | (uint32_t)(c + 1))));
+    F2 d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(v), "l"(two23));
+    return d;
+}
+__device__ __forceinline__ float fmax3(float a, float b, float c) {
+    float d;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+__device__ __forceinline__ float fmin3(float a, float b, float c) {
+    float d;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+
 __device__ __forceinline__ bool slab2(const float4 n0, const float4 n1, const float4 n2, V3 inv, V3 oi,
                                       float tmin, float tmax, float& tl, float& tr, bool& hr) {
     // t = lo*inv - o*inv, one FMA per bound; boxes are padded on the host so rounding never culls.
+#if RTC_BINARY_PACKED
+    // each float4 holds a child's (lo, hi) pairs, so one f32x2 FMA gives both planes of an axis
+    const F2 ix = f2(inv.x, inv.x), iy = f2(inv.y, inv.y), iz = f2(inv.z, inv.z);
+    const F2 ox = f2(-oi.x, -oi.x), oy = f2(-oi.y, -oi.y), oz = f2(-oi.z, -oi.z);
+    float l0x, l1x, l0y, l1y, l0z, l1z, r0x, r1x, r0y, r1y, r0z, r1z;
+    split_f2(fma_f2(f2(n0.x, n0.y), ix, ox), l0x, l1x);
+    split_f2(fma_f2(f2(n0.z, n0.w), iy, oy), l0y, l1y);
+    split_f2(fma_f2(f2(n2.x, n2.y), iz, oz), l0z, l1z);
+    split_f2(fma_f2(f2(n1.x, n1.y), ix, ox), r0x, r1x);
+    split_f2(fma_f2(f2(n1.z, n1.w), iy, oy), r0y, r1y);
+    split_f2(fma_f2(f2(n2.z, n2.w), iz, oz), r0z, r1z);
+    const float lin = fmax3(fminf(l0x, l1x), fminf(l0y, l1y), fmaxf(fminf(l0z, l1z), tmin));
+    const float lout = fmin3(fmaxf(l0x, l1x), fmaxf(l0y, l1y), fminf(fmaxf(l0z, l1z), tmax));
+    const float rin = fmax3(fminf(r0x, r1x), fminf(r0y, r1y), fmaxf(fminf(r0z, r1z), tmin));
+    const float rout = fmin3(fmaxf(r0x, r1x), fmaxf(r0y, r1y), fminf(fmaxf(r0z, r1z), tmax));
+#else
     float l0x = __fmaf_rn(n0.x, inv.x, -oi.x), l1x = __fmaf_rn(n0.y, inv.x, -oi.x);
     float l0y = __fmaf_rn(n0.z, inv.y, -oi.y), l1y = __fmaf_rn(n0.w, inv.y, -oi.y);
     float l0z = __fmaf_rn(n2.x, inv.z, -oi.z), l1z = __fmaf_rn(n2.y, inv.z, -oi.z);
@@ -218,6 +277,7 @@ __device__ __forceinline__ bool slab2(const float4 n0, const float4 n1, const fl
     float lout = fminf(fminf(fmaxf(l0x, l1x), fmaxf(l0y, l1y)), fminf(fmaxf(l0z, l1z), tmax));
     float rin = fmaxf(fmaxf(fminf(r0x, r1x), fminf(r0y, r1y)), fmaxf(fminf(r0z, r1z), tmin));
     float rout = fminf(fminf(fmaxf(r0x, r1x), fmaxf(r0y, r1y)), fminf(fmaxf(r0z, r1z), tmax));
+#endif
     tl = lin;
     tr = rin;
     hr = rin <= rout;
@@ -492,6 +552,34 @@ __device__ __forceinline__ bool closest_hit8(const DevScene& S, V3 o, V3 d, V3 i
             const uint32_t nz0 = __float_as_uint((oct & 4u) ? qz.z : qz.x), nz1 = __float_as_uint((oct & 4u) ? qz.w : qz.y);
             const uint32_t fz0 = __float_as_uint((oct & 4u) ? qz.x : qz.z), fz1 = __float_as_uint((oct & 4u) ? qz.y : qz.w);
             uint32_t hs = 0;
+#if RTC_WIDE_PACKED
+            // two children per instruction: packed f32x2 subtract and FMA, the same roundings per lane
+            const F2 ax2 = f2(ax, ax), ay2 = f2(ay, ay), az2 = f2(az, az);
+            const F2 bx2 = f2(bx, bx), by2 = f2(by, by), bz2 = f2(bz, bz);
+#pragma unroll
+            for (int c = 0; c < 8; c += 2) {
+                const int b = c & 3;
+                const F2 tnx = fma_f2(bytes_f2(c < 4 ? nx0 : nx1, b), ax2, bx2);
+                const F2 tfx = fma_f2(bytes_f2(c < 4 ? fx0 : fx1, b), ax2, bx2);
+                const F2 tny = fma_f2(bytes_f2(c < 4 ? ny0 : ny1, b), ay2, by2);
+                const F2 tfy = fma_f2(bytes_f2(c < 4 ? fy0 : fy1, b), ay2, by2);
+                const F2 tnz = fma_f2(bytes_f2(c < 4 ? nz0 : nz1, b), az2, bz2);
+                const F2 tfz = fma_f2(bytes_f2(c < 4 ? fz0 : fz1, b), az2, bz2);
+                float nx[2], ny[2], nz[2], fx[2], fy[2], fz[2];
+                split_f2(tnx, nx[0], nx[1]);
+                split_f2(tny, ny[0], ny[1]);
+                split_f2(tnz, nz[0], nz[1]);
+                split_f2(tfx, fx[0], fx[1]);
+                split_f2(tfy, fy[0], fy[1]);
+                split_f2(tfz, fz[0], fz[1]);
+#pragma unroll
+                for (int k = 0; k < 2; ++k) {
+                    const float tn = fmax3(nx[k], ny[k], fmaxf(nz[k], tmin));
+                    const float tf = fmin3(fx[k], fy[k], fminf(fz[k], best_t));
+                    hs |= (tn <= tf ? 1u : 0u) << (c + k);
+                }
+            }
+#else
 #pragma unroll
             for (int c = 0; c < 8; ++c) {
                 const int b = c & 3;
@@ -505,6 +593,7 @@ __device__ __forceinline__ bool closest_hit8(const DevScene& S, V3 o, V3 d, V3 i
                 const float tf = fminf(fminf(tfx, tfy), fminf(tfz, best_t));
                 hs |= (tn <= tf ? 1u : 0u) << c;
             }
+#endif
             hits = octant_order(hs & (hdr >> 24), oct);
         }
         if (hits == 0u) {
