@@ -24,7 +24,8 @@
 // on a tie), merges mutual nearest neighbours into a new node, and compacts the survivors in order.
 // Merging by the surface-area distance gives trees close to a SAH build's.  Node indices count down from
 // the round's cluster count, so the last merge - the root - is node 0, and the numbering is
-// deterministic (a prefix sum orders each round's merges).
+// deterministic (a prefix sum orders each round's merges).  PLOC stops at RTC_PLOC_TOP clusters; the
+// host's binned SAH build joins those into the top of the tree (join_top).
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 #include <cub/device/device_select.cuh>
@@ -44,6 +45,13 @@
 // 366 Mpaths/s); the gap to the SAH tree (395 Mpaths/s, 12.61 G visits) is in its upper levels.
 #ifndef RTC_DEVICE_LEAF_MAX
 #define RTC_DEVICE_LEAF_MAX 1
+#endif
+// PLOC stops at this many clusters, and the host's binned SAH build joins them (a build-time knob; 1:
+// PLOC all the way to the root).  Meshes frame (1.31 M triangles), against 392.7-394.4 Mpaths/s with the
+// host SAH tree: PLOC to the root 367.8, joined at 4,096 clusters 381.1, at 32,768 380.6-383.4, at
+// 131,072 385.7; the join adds about 50 ms (32,768) to 140 ms (131,072) to a 200 ms scene create.
+#ifndef RTC_PLOC_TOP
+#define RTC_PLOC_TOP 131072
 #endif
 
 namespace rtc {
@@ -322,15 +330,49 @@ uint32_t tree_depth(const std::vector<float>& nodes, uint32_t inner) {
     return visited == inner ? deepest : 0;
 }
 
+// Joins the clusters PLOC left with the host's binned SAH build (one cluster per leaf) and writes its
+// k - 1 inner nodes into nodes [0, k - 2] of `nodes` (root 0), each leaf slot pointing at its cluster
+// (a PLOC node or a primitive leaf).  PLOC's nearest-neighbour merges make good lower levels; a tree's
+// upper levels, which every ray walks, come out better from the SAH split search.
+bool join_top(const std::vector<Cluster>& rest, std::vector<float>& nodes, const char** what) {
+    BvhInput tin;
+    tin.boxes.resize(rest.size());
+    for (size_t i = 0; i < rest.size(); ++i) tin.boxes[i] = rest[i].box;
+    BvhOutput top;
+    const char* terr = nullptr;
+    if (!build_bvh(tin, 1, 0, top, &terr) || top.num_nodes != rest.size() - 1) {
+        *what = terr ? terr : "device BVH build: the top-level join failed";
+        return false;
+    }
+    for (uint32_t t = 0; t < top.num_nodes; ++t) {
+        float* f = &top.nodes[16 * (size_t)t];
+        for (int side = 0; side < 2; ++side) {
+            int32_t c;
+            std::memcpy(&c, &f[12 + side], 4);
+            if (c < 0) {
+                const uint32_t first = (uint32_t)~c >> LEAF_COUNT_BITS;
+                c = rest[top.order[first]].id;
+                std::memcpy(&f[12 + side], &c, 4);
+            }
+        }
+        std::memcpy(&nodes[16 * (size_t)t], f, 16 * sizeof(float));
+    }
+    return true;
+}
+
 template <class T>
 cudaError_t dalloc(T** p, size_t n, cudaStream_t st) {
     return cudaMallocAsync((void**)p, std::max<size_t>(n, 1) * sizeof(T), st);
 }
 
-// PLOC rounds on `st` until one cluster is left; the nodes go to `nodes` (n - 1 records, root 0).
-// `h_count` is page-locked host memory for the per-round cluster count.
-cudaError_t ploc(const Aabb* d_boxes, const uint32_t* vals, uint32_t n, float4* d_nodes, uint32_t* d_error,
-                 uint32_t* h_count, cudaStream_t st, const char** what) {
+// PLOC rounds on `st` until at most `stop_at` clusters are left (at least 1); the nodes go to `nodes`.
+// A round with m clusters numbers its merges from m - 2 down, so nodes [0, m_final - 2] stay free for
+// the merges that remain: with stop_at = 1 they are all made here (n - 1 records, root 0); otherwise
+// the remaining clusters are copied to `rest` for the host to join.  `h_count` is page-locked host
+// memory for the per-round cluster count.
+cudaError_t ploc(const Aabb* d_boxes, const uint32_t* vals, uint32_t n, uint32_t stop_at, float4* d_nodes,
+                 uint32_t* d_error, uint32_t* h_count, std::vector<Cluster>& rest, cudaStream_t st,
+                 const char** what) {
     Cluster *cur = nullptr, *tmp = nullptr, *nxt = nullptr;
     uint32_t *nn = nullptr, *keep = nullptr, *fresh = nullptr, *rank = nullptr, *nsel = nullptr;
     void* temp = nullptr;
@@ -347,7 +389,7 @@ cudaError_t ploc(const Aabb* d_boxes, const uint32_t* vals, uint32_t n, float4* 
         k_ploc_init<<<(n + 255) / 256, 256, 0, st>>>(d_boxes, vals, n, cur);
         if ((e = cudaGetLastError())) break;
         uint32_t m = n;
-        for (int round = 0; m > 1; ++round) {
+        for (int round = 0; m > std::max(stop_at, 1u); ++round) {
             if (round >= PLOC_MAX_ROUNDS) {
                 *what = "device BVH build did not converge";
                 break;
@@ -369,6 +411,11 @@ cudaError_t ploc(const Aabb* d_boxes, const uint32_t* vals, uint32_t n, float4* 
             }
             m = *h_count;
             std::swap(cur, nxt);
+        }
+        if (e == cudaSuccess && !*what && m > 1) {
+            rest.resize(m);
+            if ((e = cudaMemcpyAsync(rest.data(), cur, m * sizeof(Cluster), cudaMemcpyDeviceToHost, st))) break;
+            e = cudaStreamSynchronize(st);
         }
     } while (false);
     for (void* p : {(void*)cur, (void*)tmp, (void*)nxt, (void*)nn, (void*)keep, (void*)fresh, (void*)rank,
@@ -417,6 +464,7 @@ int build_bvh_device(const BvhInput& in, int device, BvhDeviceMethod method, Bvh
     int rc = BVH_DEVICE_ERROR;
     const char* what = nullptr;
     uint32_t* h_info = nullptr;
+    std::vector<Cluster> rest;   // clusters PLOC leaves for the host's top-level join
     do {
         if ((e = dalloc(&d_boxes, n, st)) || (e = dalloc(&d_keys, n, st)) || (e = dalloc(&d_keys2, n, st)) ||
             (e = dalloc(&d_vals, n, st)) || (e = dalloc(&d_vals2, n, st)) || (e = dalloc(&d_flags, n, st)) ||
@@ -447,7 +495,7 @@ int build_bvh_device(const BvhInput& in, int device, BvhDeviceMethod method, Bvh
                                               d_nodes, d_info + 1, d_info);
             if ((e = cudaGetLastError())) break;
         } else {
-            e = ploc(d_boxes, vals, (uint32_t)n, d_nodes, d_info, h_info + 2, st, &what);
+            e = ploc(d_boxes, vals, (uint32_t)n, RTC_PLOC_TOP, d_nodes, d_info, h_info + 2, rest, st, &what);
             if (e == cudaSuccess && what) rc = BVH_DEVICE_TOO_DEEP;   // no tree: the SAH build takes over
             if (e != cudaSuccess || what) break;
         }
@@ -460,6 +508,10 @@ int build_bvh_device(const BvhInput& in, int device, BvhDeviceMethod method, Bvh
         if ((e = cudaStreamSynchronize(st))) break;
         if (h_info[0]) {
             what = "device BVH build produced an inconsistent tree";
+            break;
+        }
+        if (rest.size() > 1 && !join_top(rest, out.nodes, &what)) {
+            rc = BVH_DEVICE_TOO_DEEP;   // the SAH build takes over
             break;
         }
         out.num_nodes = (uint32_t)(n - 1);
