@@ -61,20 +61,20 @@ FALLBACK_HBM_GBS = 6650.0
 
 # bytes fetched per visit (ignoring caches) for the roofline's algorithmic traffic
 NODE_BYTES = 64          # BVH2 node: two child boxes + two child links (4 x float4)
-NODE8_BYTES = 96         # 8-wide node: header, quantised child boxes (8-bit), eight child links (6 x float4)
+NODE8_BYTES = 80         # 8-wide compressed node: origin, exponents, link bases, slot links, 8-bit child bounds (5 x float4)
 PRIM_BYTES = {"spheres": 16, "cornell": 48, "meshes": 48}   # dominant primitive record of each workload
 # algorithmic FP32 operations per visit (the fixed constants of the roofline's flop count): a binary node's
 # two slab tests, and the dominant primitive test of each workload (sphere 20, triangle 30)
 NODE_FLOPS = 24
 PRIM_FLOPS = {"spheres": 20, "cornell": 30, "meshes": 30}
 STATE_BYTES = 32 + 16 + 2 * 48   # ray read + hit write + path state read/write per traversal
-EXTEND_STATE_BYTES = 4 + 32 + 4 + 8   # queue entry + ray (origin, direction) + depth word read, hit record write
+EXTEND_STATE_BYTES = 4 + 32 + 8   # queue entry + the slot's ray sector (origin, direction, start, depth) read, hit write
 
 
-# Path-state bytes the shade kernel moves per traced ray (its algorithmic traffic): queue entry, hit
-# record and the slot's meta, ray origin/direction, attenuation and sample radiance read (4+8+5x16), the
-# ray, attenuation, radiance and meta written back (4x16) and the survivor's queue entry (4).
-SHADE_STATE_BYTES = 4 + 8 + 5 * 16 + 4 * 16 + 4
+# Path-state bytes the shade kernel moves per traced ray (its algorithmic traffic): the queue entry and
+# the slot's three 32-byte sectors read (ray, shade with the hit, pixel: 4 + 3 x 32), the ray and shade
+# sectors and the stream word written back (2 x 32 + 4), and the survivor's queue entry (4).
+SHADE_STATE_BYTES = 4 + 3 * 32 + 2 * 32 + 4 + 4
 NCU_SUMMARY = ROOT / "profiles" / "ncu_wavefront_{config}.json"
 
 

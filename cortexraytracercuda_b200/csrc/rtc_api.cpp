@@ -949,8 +949,8 @@ void rtc_carve_groups(void* base, const rtc_render_params* p, float4** part, uin
 namespace {
 
 // Bytes of wavefront scratch per path slot.
-constexpr size_t WF_SLOT_BYTES = 5 * sizeof(float4) + 2 * sizeof(uint4) + sizeof(float2) + 3 * sizeof(uint32_t);
-constexpr uint32_t WF_MAX_SLOTS = 1u << 22;   // 4,194,304 slots = 432 MiB of path state
+constexpr size_t WF_SLOT_BYTES = WF_REC_BYTES + 3 * sizeof(uint32_t);
+constexpr uint32_t WF_MAX_SLOTS = 1u << 22;   // 4,194,304 slots = 432 MiB of path state (108 B per slot)
 
 // Lays out the wavefront buffers for `slots` path slots in one block of device memory at `base`
 // (the context's scratch, or the allocation-free entry point's static array).
@@ -962,14 +962,7 @@ size_t carve_wavefront(void* base, uint32_t slots, WfBuffers& B) {
         return (void*)r;
     };
     const size_t n = slots;
-    B.ray_o = (float4*)take(n * 16);
-    B.ray_d = (float4*)take(n * 16);
-    B.att = (float4*)take(n * 16);
-    B.acc = (float4*)take(n * 16);
-    B.psum = (float4*)take(n * 16);
-    B.meta = (uint4*)take(n * 16);
-    B.pcg = (uint4*)take(n * 16);
-    B.hit = (float2*)take(n * 8);
+    B.rec = (uint32_t*)take(n * WF_REC_BYTES);
     B.queue[0] = (uint32_t*)take(n * 4);
     B.queue[1] = (uint32_t*)take(n * 4);
     B.queue[2] = (uint32_t*)take(n * 4);
@@ -980,7 +973,7 @@ size_t carve_wavefront(void* base, uint32_t slots, WfBuffers& B) {
 
 // Bytes carve_wavefront lays out for `slots` slots (each buffer rounded up to 256 bytes).
 constexpr size_t wavefront_bytes(size_t n) {
-    return 7 * ((n * 16 + 255) & ~(size_t)255) + ((n * 8 + 255) & ~(size_t)255) + 3 * ((n * 4 + 255) & ~(size_t)255) +
+    return ((n * WF_REC_BYTES + 255) & ~(size_t)255) + 3 * ((n * 4 + 255) & ~(size_t)255) +
            ((WF_CTR_N * 4 + 255) & ~(size_t)255);
 }
 // The allocation-free render's advertised cap fits its 64 MiB array behind a 256-byte status header

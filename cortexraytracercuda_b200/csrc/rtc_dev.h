@@ -158,20 +158,27 @@ struct DevParams {
     uint8_t* rgb8;     // non-null: each finished pixel is also written quantised here (quantize_pixel)
 };
 
-// Wavefront path slots (SoA, one slot = one pixel in flight) and the two slot queues.
+// Wavefront path slots (one slot = one pixel, or one sample group, in flight) and the slot queues.
+//
+// A slot's path state is one 96-byte record of three 32-byte sectors, each moved by a single 256-bit
+// load or store (the kernels reach slots through the queues, so neighbouring lanes touch unrelated
+// records: a sector per access is the least a scattered access can move):
+//   sector 0, ray:    origin.xyz, direction.xyz, the trace's start (0 for an ordinary ray, t + 0.001 for
+//                     the re-hit from behind a one-sided light, camera.cuh:177-183), and the depth word
+//                     (depth left in the low 16 bits | job slot in the high 16 bits, 0 for one image);
+//   sector 1, shade:  path attenuation rgb, radiance of the current sample rgb, and the closest hit the
+//                     extend kernel found (t, item bits; 0xffffffff = miss);
+//   sector 2, pixel:  pixel (0xffffffff = idle slot), sample index, the minstd state (compat) or the
+//                     sample group (clean), the PCG32 state's low word (clean), the pixel sum rgb, and
+//                     the PCG32 state's high word.  A clean-mode stream's increment is 2 s + 1 for sample
+//                     s (Pcg32::seed), so it is recomputed from the sample index, not stored.
+// The ray's time (perspective_camera::get_ray draws it) is not kept: no hit test reads it.
+constexpr uint32_t WF_REC_WORDS = 24;
+constexpr uint32_t WF_REC_BYTES = WF_REC_WORDS * 4;
 struct WfBuffers {
-    float4* ray_o;     // origin.xyz, time
-    float4* ray_d;     // direction.xyz, .w the trace's start: 0 for an ordinary ray, t + 0.001 for the
-                       // re-hit from behind a one-sided light (camera.cuh:177-183)
-    float4* att;       // path attenuation rgb
-    float4* acc;       // radiance of the current sample rgb
-    float4* psum;      // pixel sum rgb (pixel_color)
-    uint4* meta;       // x pixel (0xffffffff idle), y sample index, z minstd state,
-                       // w depth left (low 16 bits) | job slot (high 16 bits, 0 for a single image)
-    uint4* pcg;        // clean mode: PCG32 state (lo, hi) and increment (lo, hi)
-    float2* hit;       // t, item bits (0xffffffff = miss)
+    uint32_t* rec;        // slots x WF_REC_WORDS words, 256-byte aligned (so every sector is 32-byte aligned)
     uint32_t* queue[3];   // [0], [1]: the alternating slot queues; [2]: slots split off as long chains
-    uint32_t* ctr;     // [0..2] queue sizes (rotating), [3] next pixel to fetch, [4] long-chain queue size
+    uint32_t* ctr;        // [0..2] queue sizes (rotating), [3] next pixel to fetch, [4] long-chain queue size
     uint32_t slots;
 };
 

@@ -70,7 +70,8 @@ rtc_status Engine::init(const EngineConfig& cfg, cudaStream_t st) {
 
 rtc_status Engine::reset() {
     ENG_CUDA(cudaMemsetAsync(B_.ctr, 0, WF_CTR_N * sizeof(uint32_t), st_));
-    ENG_CUDA(cudaMemsetAsync(B_.meta, 0xff, (size_t)cfg_.slots * sizeof(uint4), st_));   // every slot idle
+    // every slot idle (pixel word 0xffffffff); the other words are written before they are read
+    ENG_CUDA(cudaMemsetAsync(B_.rec, 0xff, (size_t)cfg_.slots * WF_REC_BYTES, st_));
     ENG_CUDA(cudaMemsetAsync(d_prog_, 0, sizeof(WfFeed) + (size_t)cfg_.ring * sizeof(uint32_t), st_));
     ENG_CUDA(cudaMemsetAsync(d_status_, 0, sizeof(uint32_t), st_));
     ENG_CUDA(cudaStreamSynchronize(st_));

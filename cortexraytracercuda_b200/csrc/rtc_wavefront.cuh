@@ -52,11 +52,11 @@
 namespace rtc {
 inline namespace RTC_XP_NS {
 
-// Loads of the path-state arrays (queues, rays, hit records, slot state): a build-time choice of cache
-// policy - 0 streaming (ld.global.cs, evict first), 1 L2 only (ld.global.cg: the default), 2 the
-// default policy (L1 and L2).  Each slot's state is read once per iteration, so caching it in L1 only
-// evicts node records; on the spheres frame (1280x720, 64 spp) 1 measured 2.5% faster than 0 and 0.5%
-// faster than 2 (shade 26.0 ms against 27.4 and 26.3 ms).
+// Loads of the path state (queue entries and slot records): a build-time choice of cache policy - 0
+// streaming (ld.global.cs, evict first), 1 L2 only (ld.global.cg: the default), 2 the default policy
+// (L1 and L2).  Each slot's state is read once per iteration, so caching it in L1 only evicts node
+// records; on the spheres frame (1280x720, 64 spp) 1 measured 2.5% faster than 0 and 0.5% faster
+// than 2 (shade 26.0 ms against 27.4 and 26.3 ms).
 #ifndef RTC_STATE_LOAD
 #define RTC_STATE_LOAD 1
 #endif
@@ -71,10 +71,111 @@ __device__ __forceinline__ T ld_state(const T* p) {
 #endif
 }
 
-// A slot's ray direction carries in .w the start of its trace: 0 for an ordinary ray (tmin = 1e-5,
+// ---- slot records (WfBuffers::rec): three 32-byte sectors per slot, one 256-bit access each --------
+
+struct Sec {
+    uint32_t w[8];
+};
+constexpr int SEC_RAY = 0, SEC_SHADE = 1, SEC_PIXEL = 2;
+
+__device__ __forceinline__ uint32_t* wf_sec(const WfBuffers& B, uint32_t slot, int sec) {
+    return B.rec + (size_t)slot * WF_REC_WORDS + 8 * sec;
+}
+
+__device__ __forceinline__ Sec ld_sec(const uint32_t* p) {
+    Sec s;
+#if RTC_STATE_LOAD == 1
+    asm volatile("ld.global.cg.v8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+#elif RTC_STATE_LOAD == 2
+    asm volatile("ld.global.v8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+#else
+    asm volatile("ld.global.cs.v8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+#endif
+                 : "=r"(s.w[0]), "=r"(s.w[1]), "=r"(s.w[2]), "=r"(s.w[3]), "=r"(s.w[4]), "=r"(s.w[5]), "=r"(s.w[6]),
+                   "=r"(s.w[7])
+                 : "l"(p));
+    return s;
+}
+
+// A record load is a volatile asm without a memory clobber, and every store into the records is a
+// volatile asm with one: the loads keep their order against the stores (no volatile asm passes
+// another) without stopping the compiler from keeping scene data in registers across a load.
+__device__ __forceinline__ void st_word(uint32_t* p, uint32_t v) {
+    asm volatile("st.global.b32 [%0], %1;" : : "l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ uint32_t ld_word(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.global.cg.b32 %0, [%1];" : "=r"(v) : "l"(p));
+    return v;
+}
+
+__device__ __forceinline__ void st_sec(uint32_t* p, const Sec& s) {
+    asm volatile("st.global.v8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};"
+                 :
+                 : "l"(p), "r"(s.w[0]), "r"(s.w[1]), "r"(s.w[2]), "r"(s.w[3]), "r"(s.w[4]), "r"(s.w[5]), "r"(s.w[6]),
+                   "r"(s.w[7])
+                 : "memory");
+}
+
+// sector 0: origin, direction, the trace's start, the depth word
+__device__ __forceinline__ Sec ray_sec(V3 o, V3 d, float start, uint32_t mw) {
+    Sec s;
+    s.w[0] = __float_as_uint(o.x);
+    s.w[1] = __float_as_uint(o.y);
+    s.w[2] = __float_as_uint(o.z);
+    s.w[3] = __float_as_uint(d.x);
+    s.w[4] = __float_as_uint(d.y);
+    s.w[5] = __float_as_uint(d.z);
+    s.w[6] = __float_as_uint(start);
+    s.w[7] = mw;
+    return s;
+}
+__device__ __forceinline__ V3 sec_v3(const Sec& s, int k) {
+    return v3(__uint_as_float(s.w[k]), __uint_as_float(s.w[k + 1]), __uint_as_float(s.w[k + 2]));
+}
+__device__ __forceinline__ float sec_f(const Sec& s, int k) { return __uint_as_float(s.w[k]); }
+
+// sector 1: attenuation, sample radiance (the hit words are the extend kernel's to write)
+__device__ __forceinline__ Sec shade_sec(RGB att, RGB acc) {
+    Sec s;
+    s.w[0] = __float_as_uint(att.r);
+    s.w[1] = __float_as_uint(att.g);
+    s.w[2] = __float_as_uint(att.b);
+    s.w[3] = __float_as_uint(acc.r);
+    s.w[4] = __float_as_uint(acc.g);
+    s.w[5] = __float_as_uint(acc.b);
+    s.w[6] = 0u;
+    s.w[7] = 0xffffffffu;
+    return s;
+}
+
+// the closest hit (t, item bits) into sector 1's last two words
+__device__ __forceinline__ void st_hit(uint32_t* shade_sector, float t, uint32_t item) {
+    asm volatile("st.global.v2.b32 [%0], {%1, %2};" : : "l"(shade_sector + 6), "r"(__float_as_uint(t)), "r"(item)
+                 : "memory");
+}
+
+// sector 2: pixel, sample, minstd state / sample group, PCG32 state, pixel sum
+__device__ __forceinline__ Sec pixel_sec(uint32_t pixel, uint32_t sample, uint32_t aux, uint64_t pcg_state, float4 ps) {
+    Sec s;
+    s.w[0] = pixel;
+    s.w[1] = sample;
+    s.w[2] = aux;
+    s.w[3] = (uint32_t)pcg_state;
+    s.w[4] = __float_as_uint(ps.x);
+    s.w[5] = __float_as_uint(ps.y);
+    s.w[6] = __float_as_uint(ps.z);
+    s.w[7] = (uint32_t)(pcg_state >> 32);
+    return s;
+}
+__device__ __forceinline__ float4 sec_psum(const Sec& s) {
+    return make_float4(__uint_as_float(s.w[4]), __uint_as_float(s.w[5]), __uint_as_float(s.w[6]), 0.0f);
+}
+
+// A slot's ray sector carries the start of its trace: 0 for an ordinary ray (tmin = 1e-5,
 // SHADOW_ACNE_FIX, constants.cuh:27), or t + 0.001 for the re-hit from behind a one-sided light that
 // the shade kernel hands back to the extend kernel (camera.cuh:177-183).
-__device__ __forceinline__ float wf_tmin(float4 d) { return d.w > 0.0f ? d.w : 0.00001f; }
+__device__ __forceinline__ float wf_tmin(float start) { return start > 0.0f ? start : 0.00001f; }
 
 // Appends `slot` to queue `q` when `pred`; every active lane of the warp must call it together.
 __device__ __forceinline__ void wf_push(uint32_t* q, uint32_t* cnt, uint32_t slot, bool pred) {
@@ -100,13 +201,19 @@ struct WfRngT<true> {
 template <bool CLEAN>
 using WfRng = typename WfRngT<CLEAN>::type;
 
-__device__ __forceinline__ void pcg_load(Pcg32& r, uint4 v) {
-    r.state = ((uint64_t)v.y << 32) | v.x;
-    r.inc = ((uint64_t)v.w << 32) | v.z;
+// The stream of a slot from its pixel sector: compat keeps the minstd state in word 2; clean keeps the
+// PCG32 state in words 3 and 7, and the increment of sample s's stream is 2 s + 1 (Pcg32::seed).
+template <bool CLEAN>
+__device__ __forceinline__ void rng_load(const Sec& px, WfRng<CLEAN>& r) {
+    if constexpr (CLEAN) {
+        r.state = ((uint64_t)px.w[7] << 32) | px.w[3];
+        r.inc = ((uint64_t)px.w[1] << 1) | 1u;
+    } else {
+        r.x = px.w[2];
+    }
 }
-__device__ __forceinline__ uint4 pcg_store(const Pcg32& r) {
-    return make_uint4((uint32_t)r.state, (uint32_t)(r.state >> 32), (uint32_t)r.inc, (uint32_t)(r.inc >> 32));
-}
+
+
 
 // Starts sample `s` of pixel `pixel`: jitter and camera ray (perspective_camera::get_ray).
 // Compat: one shared stream per pixel, samples in stratum order (gpu.cu:776-786).
@@ -132,10 +239,15 @@ __device__ __forceinline__ void wf_start_sample(const DevScene& S, const DevPara
     }
 }
 
+// The pixel sector's stream words after `rng` has advanced (compat: word 2; clean: words 3 and 7).
 template <bool CLEAN>
-__device__ __forceinline__ void rng_save(const WfBuffers& B, uint32_t slot, const WfRng<CLEAN>& rng, uint4& m) {
-    if constexpr (CLEAN) B.pcg[slot] = pcg_store(rng);
-    else m.z = rng.x;
+__device__ __forceinline__ void rng_store(Sec& px, const WfRng<CLEAN>& rng) {
+    if constexpr (CLEAN) {
+        px.w[3] = (uint32_t)rng.state;
+        px.w[7] = (uint32_t)(rng.state >> 32);
+    } else {
+        px.w[2] = rng.x;
+    }
 }
 
 __device__ __forceinline__ uint32_t wf_samples(const DevParams& P, bool clean) {
@@ -224,7 +336,7 @@ __device__ __forceinline__ bool wf_fetch_pixel(const J& jobs, const WfWindow& wi
                                                uint32_t& status) {
     uint32_t job = 0, unit = 0;
     if (!jobs.claim(B, win, job, unit, status)) {
-        B.meta[slot] = make_uint4(WF_IDLE, 0u, 0u, 0u);
+        st_word(wf_sec(B, slot, SEC_PIXEL), WF_IDLE);
         return false;
     }
     const DevScene& S = jobs.scene(job);
@@ -236,14 +348,11 @@ __device__ __forceinline__ bool wf_fetch_pixel(const J& jobs, const WfWindow& wi
     if constexpr (!CLEAN) rng.seed(P.seed + pixel);
     Ray r;
     wf_start_sample<CLEAN, ORDER>(S, P, rng, pixel, s0, r);
-    B.ray_o[slot] = make_float4(r.o.x, r.o.y, r.o.z, r.time);
-    B.ray_d[slot] = make_float4(r.d.x, r.d.y, r.d.z, 0.f);
-    B.att[slot] = make_float4(1.f, 1.f, 1.f, 0.f);
-    B.acc[slot] = make_float4(0.f, 0.f, 0.f, 0.f);
-    B.psum[slot] = make_float4(0.f, 0.f, 0.f, 0.f);
-    uint4 m = make_uint4(pixel, s0, grp, wf_pack((uint32_t)P.max_depth, job));   // clean: z = group
-    rng_save<CLEAN>(B, slot, rng, m);
-    B.meta[slot] = m;
+    st_sec(wf_sec(B, slot, SEC_RAY), ray_sec(r.o, r.d, 0.0f, wf_pack((uint32_t)P.max_depth, job)));
+    st_sec(wf_sec(B, slot, SEC_SHADE), shade_sec(rgb(1.f, 1.f, 1.f), rgb(0.f, 0.f, 0.f)));
+    Sec px = pixel_sec(pixel, s0, grp, 0ull, make_float4(0.f, 0.f, 0.f, 0.f));   // clean: word 2 = group
+    rng_store<CLEAN>(px, rng);
+    st_sec(wf_sec(B, slot, SEC_PIXEL), px);
     return true;
 }
 
@@ -307,7 +416,7 @@ __global__ void __launch_bounds__(128) wf_admit(WfTable J, WfBuffers B, WfIter w
     for (uint32_t base = blockIdx.x * blockDim.x; base < B.slots; base += stride) {
         const uint32_t slot = base + threadIdx.x;
         bool live = false;
-        if (slot < B.slots && B.meta[slot].x == WF_IDLE) live = wf_fetch_pixel<CLEAN, ORDER>(J, win, B, slot, status);
+        if (slot < B.slots && ld_word(wf_sec(B, slot, SEC_PIXEL)) == WF_IDLE) live = wf_fetch_pixel<CLEAN, ORDER>(J, win, B, slot, status);
         wf_push(B.queue[w.qin], B.ctr + w.cin, slot, live);
     }
     if (status) atomicOr(status_word, status);
@@ -326,14 +435,15 @@ __global__ void RTC_EXTEND_BOUNDS wf_extend(J jobs, WfBuffers B, WfIter w, unsig
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
         const uint32_t slot = ld_state(q + k);
-        const float4 o = ld_state(B.ray_o + slot), d = ld_state(B.ray_d + slot);
-        const uint32_t mw = ld_state(&B.meta[slot].w);
+        const Sec R = ld_sec(wf_sec(B, slot, SEC_RAY));
+        const uint32_t mw = R.w[7];
         const uint32_t job = wf_job(mw);
         float t;
         uint32_t item;
-        bool h = closest_hit<FLAVOR == 2, WIDE>(jobs.scene(job), v3(o), v3(d), wf_tmin(d), 3.402823466e+38f,
-                                          wf_depth(mw) == (uint32_t)jobs.params(job).max_depth, t, item, st, status);
-        B.hit[slot] = make_float2(t, __uint_as_float(h ? item : 0xffffffffu));
+        bool h = closest_hit<FLAVOR == 2, WIDE>(jobs.scene(job), sec_v3(R, 0), sec_v3(R, 3), wf_tmin(sec_f(R, 6)),
+                                                3.402823466e+38f, wf_depth(mw) == (uint32_t)jobs.params(job).max_depth, t,
+                                                item, st, status);
+        st_hit(wf_sec(B, slot, SEC_SHADE), t, h ? item : 0xffffffffu);
         ++rays;
     }
     if (COUNT && counters) {
@@ -359,76 +469,75 @@ __global__ void RTC_EXTEND_BOUNDS wf_extend(J jobs, WfBuffers B, WfIter w, unsig
 // bookkeeping (next bounce / next sample / next pixel).  Returns true while the slot has a ray to trace.
 template <bool CLEAN, int ORDER, class J>
 __device__ __forceinline__ bool wf_step(const J& jobs, const WfWindow& win, const WfBuffers& B, uint32_t slot,
-                                        float t, uint32_t item, PathCounters& pc, TraceStats& st, uint32_t& paths,
-                                        uint32_t& status) {
-    uint4 m = ld_state(B.meta + slot);
-    const uint32_t job = wf_job(m.w);
+                                        const Sec& R, const Sec& SH, const Sec& PX, float t, uint32_t item,
+                                        PathCounters& pc, TraceStats& st, uint32_t& paths, uint32_t& status) {
+    const uint32_t job = wf_job(R.w[7]);
     // local copies: a job record in the ring is read once here; through a reference it would be
     // re-read after each store to the path state below, which the compiler cannot prove does not alias
     // it (a single image's record is in kernel parameters either way)
     const DevScene S = jobs.scene(job);
     const DevParams P = jobs.params(job);
-    const float4 o = ld_state(B.ray_o + slot), d = ld_state(B.ray_d + slot), a4 = ld_state(B.att + slot),
-                 c4 = ld_state(B.acc + slot);
     Ray r;
-    r.o = v3(o);
-    r.d = v3(d);
-    r.time = o.w;
-    RGB att = rgb(a4.x, a4.y, a4.z), acc = rgb(c4.x, c4.y, c4.z);
+    r.o = sec_v3(R, 0);
+    r.d = sec_v3(R, 3);
+    r.time = 0.0f;
+    RGB att = rgb(sec_f(SH, 0), sec_f(SH, 1), sec_f(SH, 2)), acc = rgb(sec_f(SH, 3), sec_f(SH, 4), sec_f(SH, 5));
     WfRng<CLEAN> rng;
-    if constexpr (CLEAN) pcg_load(rng, ld_state(B.pcg + slot));
-    else rng.x = m.z;
-    uint32_t depth = wf_depth(m.w);
+    rng_load<CLEAN>(PX, rng);   // of the pixel sector only the stream is kept past this point
+    uint32_t depth = wf_depth(R.w[7]);
     float rehit_tmin = 0.0f;
-    const int out = shade_bounce_deferred<CLEAN, ORDER>(S, r, item != 0xffffffffu, t, item, d.w > 0.0f, acc, att, rng,
-                                                        status, rehit_tmin);
+    const int out = shade_bounce_deferred<CLEAN, ORDER>(S, r, item != 0xffffffffu, t, item, sec_f(R, 6) > 0.0f, acc,
+                                                        att, rng, status, rehit_tmin);
+    uint32_t* rec_ray = wf_sec(B, slot, SEC_RAY);
+    uint32_t* rec_shade = wf_sec(B, slot, SEC_SHADE);
+    uint32_t* rec_px = wf_sec(B, slot, SEC_PIXEL);
     if (out == BOUNCE_REHIT) {
         // the same ray again from behind the light, at the same depth: only the radiance and the ray's
         // start change (no random draw has been made)
-        B.ray_d[slot] = make_float4(d.x, d.y, d.z, rehit_tmin);
-        B.acc[slot] = make_float4(acc.r, acc.g, acc.b, 0.f);
+        st_sec(rec_ray, ray_sec(r.o, r.d, rehit_tmin, R.w[7]));
+        st_sec(rec_shade, shade_sec(att, acc));
         return true;
     }
     const bool cont = out == BOUNCE_NEXT;
     if (cont) --depth;
     if (cont && depth > 0u) {
-        // the path continues: next bounce
-        B.ray_o[slot] = make_float4(r.o.x, r.o.y, r.o.z, r.time);
-        B.ray_d[slot] = make_float4(r.d.x, r.d.y, r.d.z, 0.f);
-        B.att[slot] = make_float4(att.r, att.g, att.b, 0.f);
-        B.acc[slot] = make_float4(acc.r, acc.g, acc.b, 0.f);
-        m.w = wf_pack(depth, job);
-        rng_save<CLEAN>(B, slot, rng, m);
-        B.meta[slot] = m;
+        // the path continues: next bounce (of the pixel sector only the stream words change)
+        st_sec(rec_ray, ray_sec(r.o, r.d, 0.0f, wf_pack(depth, job)));
+        st_sec(rec_shade, shade_sec(att, acc));
+        if constexpr (CLEAN) {
+            st_word(rec_px + 3, (uint32_t)rng.state);
+            st_word(rec_px + 7, (uint32_t)(rng.state >> 32));
+        } else {
+            st_word(rec_px + 2, rng.x);
+        }
         return true;
     }
-    // the sample is done: pixel_color += ray_color(...) (gpu.cu:787)
+    // the sample is done: pixel_color += ray_color(...) (gpu.cu:787).  The pixel sector is read again
+    // here (a quarter of the bounces end a sample) rather than held in registers through the bounce.
     ++paths;
-    float4 ps = ld_state(B.psum + slot);
+    const Sec px = ld_sec(rec_px);
+    float4 ps = sec_psum(px);
     if (!CLEAN || (isfinite(acc.r) && isfinite(acc.g) && isfinite(acc.b))) {
         ps.x += acc.r;
         ps.y += acc.g;
         ps.z += acc.b;
     }
-    const uint32_t s = m.y + 1u;
-    const uint32_t grp = CLEAN ? m.z : 0u;
+    const uint32_t pixel = px.w[0];
+    const uint32_t s = px.w[1] + 1u;
+    const uint32_t grp = CLEAN ? px.w[2] : 0u;
     if (s < (P.groups > 1 ? wf_group_end(P, grp, CLEAN) : wf_samples(P, CLEAN))) {
         // regenerate: the pixel's next sample on the same slot
         Ray nr;
-        wf_start_sample<CLEAN, ORDER>(S, P, rng, m.x, s, nr);
-        B.ray_o[slot] = make_float4(nr.o.x, nr.o.y, nr.o.z, nr.time);
-        B.ray_d[slot] = make_float4(nr.d.x, nr.d.y, nr.d.z, 0.f);
-        B.att[slot] = make_float4(1.f, 1.f, 1.f, 0.f);
-        B.acc[slot] = make_float4(0.f, 0.f, 0.f, 0.f);
-        B.psum[slot] = ps;
-        m.y = s;
-        m.w = wf_pack((uint32_t)P.max_depth, job);
-        rng_save<CLEAN>(B, slot, rng, m);
-        B.meta[slot] = m;
+        wf_start_sample<CLEAN, ORDER>(S, P, rng, pixel, s, nr);
+        st_sec(rec_ray, ray_sec(nr.o, nr.d, 0.0f, wf_pack((uint32_t)P.max_depth, job)));
+        st_sec(rec_shade, shade_sec(rgb(1.f, 1.f, 1.f), rgb(0.f, 0.f, 0.f)));
+        Sec npx = pixel_sec(pixel, s, px.w[2], 0ull, ps);
+        rng_store<CLEAN>(npx, rng);
+        st_sec(rec_px, npx);
         return true;
     }
     // the pixel (or its sample group) is done: write it and take the next work unit
-    wf_group_done(jobs, job, m.x, grp, ps);
+    wf_group_done(jobs, job, pixel, grp, ps);
     return wf_fetch_pixel<CLEAN, ORDER>(jobs, win, B, slot, status);
 }
 
@@ -468,8 +577,10 @@ __global__ void RTC_SHADE_BOUNDS wf_shade(J jobs, WfBuffers B, WfIter w, unsigne
         uint32_t slot = 0;
         if (k < n) {
             slot = ld_state(q + k);
-            const float2 hv = ld_state(B.hit + slot);
-            live = wf_step<CLEAN, ORDER>(jobs, win, B, slot, hv.x, __float_as_uint(hv.y), pc, st, paths, status);
+            const Sec R = ld_sec(wf_sec(B, slot, SEC_RAY));
+            const Sec SH = ld_sec(wf_sec(B, slot, SEC_SHADE));
+            const Sec PX = ld_sec(wf_sec(B, slot, SEC_PIXEL));
+            live = wf_step<CLEAN, ORDER>(jobs, win, B, slot, R, SH, PX, sec_f(SH, 6), SH.w[7], pc, st, paths, status);
         }
         wf_push(qn, cn, slot, live);
     }
@@ -497,16 +608,18 @@ __global__ void __launch_bounds__(RTC_ITER_BLOCK_MAX) wf_bounce(J jobs, WfBuffer
         bool live = false;
         uint32_t slot = 0;
         if (k < n) {
-            slot = q[k];
-            const float4 o = B.ray_o[slot], d = B.ray_d[slot];
-            const uint32_t mw = B.meta[slot].w;
+            slot = ld_state(q + k);
+            const Sec R = ld_sec(wf_sec(B, slot, SEC_RAY));
+            const Sec SH = ld_sec(wf_sec(B, slot, SEC_SHADE));
+            const Sec PX = ld_sec(wf_sec(B, slot, SEC_PIXEL));
+            const uint32_t mw = R.w[7];
             const uint32_t job = wf_job(mw);
             float t;
             uint32_t item;
             ++rays;
-            bool h = closest_hit<CLEAN>(jobs.scene(job), v3(o), v3(d), wf_tmin(d), 3.402823466e+38f,
-                                 wf_depth(mw) == (uint32_t)jobs.params(job).max_depth, t, item, st, status);
-            live = wf_step<CLEAN, ORDER>(jobs, win, B, slot, t, h ? item : 0xffffffffu, pc, st, paths, status);
+            bool h = closest_hit<CLEAN>(jobs.scene(job), sec_v3(R, 0), sec_v3(R, 3), wf_tmin(sec_f(R, 6)), 3.402823466e+38f,
+                                        wf_depth(mw) == (uint32_t)jobs.params(job).max_depth, t, item, st, status);
+            live = wf_step<CLEAN, ORDER>(jobs, win, B, slot, R, SH, PX, t, h ? item : 0xffffffffu, pc, st, paths, status);
         }
         wf_push(qn, cn, slot, live);
     }
@@ -535,9 +648,9 @@ __global__ void __launch_bounds__(128) wf_split(J jobs, WfBuffers B, WfIter w, f
         uint32_t slot = 0;
         if (k < n) {
             slot = q[k];
-            const uint4 m = B.meta[slot];
-            const uint32_t nsamp = wf_samples(jobs.params(wf_job(m.w)), CLEAN);
-            const float rem = (float)(nsamp - m.y - 1u) * (k0 / ((float)m.y + 1.0f));
+            const uint32_t mw = ld_word(wf_sec(B, slot, SEC_RAY) + 7), sample = ld_word(wf_sec(B, slot, SEC_PIXEL) + 1);
+            const uint32_t nsamp = wf_samples(jobs.params(wf_job(mw)), CLEAN);
+            const float rem = (float)(nsamp - sample - 1u) * (k0 / ((float)sample + 1.0f));
             longc = rem > threshold;
             keep = !longc;
         }
@@ -562,21 +675,21 @@ __global__ void RTC_FINISH_BOUNDS wf_finish(J jobs, WfBuffers B, WfIter w, unsig
     TraceStats st{0, 0};
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
-        const uint32_t slot = q[k];
-        uint4 m = B.meta[slot];
-        const float4 o = B.ray_o[slot], d = B.ray_d[slot], a4 = B.att[slot], c4 = B.acc[slot], p4 = B.psum[slot];
+        const uint32_t slot = ld_state(q + k);
+        const Sec R = ld_sec(wf_sec(B, slot, SEC_RAY)), SH = ld_sec(wf_sec(B, slot, SEC_SHADE)),
+                  PX = ld_sec(wf_sec(B, slot, SEC_PIXEL));
         Ray r;
-        r.o = v3(o);
-        r.d = v3(d);
-        r.time = o.w;
-        RGB att = rgb(a4.x, a4.y, a4.z), acc = rgb(c4.x, c4.y, c4.z);
+        r.o = sec_v3(R, 0);
+        r.d = sec_v3(R, 3);
+        r.time = 0.0f;
+        RGB att = rgb(sec_f(SH, 0), sec_f(SH, 1), sec_f(SH, 2)), acc = rgb(sec_f(SH, 3), sec_f(SH, 4), sec_f(SH, 5));
+        const float4 p4 = sec_psum(PX);
         float pr = p4.x, pg = p4.y, pb = p4.z;
         WfRng<CLEAN> rng;
-        if constexpr (CLEAN) pcg_load(rng, B.pcg[slot]);
-        else rng.x = m.z;
-        uint32_t pixel = m.x, sample = m.y, job = wf_job(m.w), grp = CLEAN ? m.z : 0u;
-        int depth = (int)wf_depth(m.w);
-        float tmin = wf_tmin(d);   // the slot may wait for its re-hit from behind a one-sided light
+        rng_load<CLEAN>(PX, rng);
+        uint32_t pixel = PX.w[0], sample = PX.w[1], job = wf_job(R.w[7]), grp = CLEAN ? PX.w[2] : 0u;
+        int depth = (int)wf_depth(R.w[7]);
+        float tmin = wf_tmin(sec_f(R, 6));   // the slot may wait for its re-hit from behind a one-sided light
         // one pass of the loop finishes the current sample of the current pixel
         for (;;) {
             const DevScene& S = jobs.scene(job);
@@ -600,22 +713,19 @@ __global__ void RTC_FINISH_BOUNDS wf_finish(J jobs, WfBuffers B, WfIter w, unsig
             wf_group_done(jobs, job, pixel, grp, make_float4(pr, pg, pb, 0.0f));
             // a slot that still has pixels to take (fewer slots than pixels) continues through memory
             if (!wf_fetch_pixel<CLEAN, ORDER>(jobs, win, B, slot, status)) break;
-            m = B.meta[slot];
-            const float4 o2 = B.ray_o[slot], d2 = B.ray_d[slot];
-            r.o = v3(o2);
-            r.d = v3(d2);
-            r.time = o2.w;
+            const Sec R2 = ld_sec(wf_sec(B, slot, SEC_RAY)), PX2 = ld_sec(wf_sec(B, slot, SEC_PIXEL));
+            r.o = sec_v3(R2, 0);
+            r.d = sec_v3(R2, 3);
             att = rgb(1.f, 1.f, 1.f);
             acc = rgb(0.f, 0.f, 0.f);
             pr = pg = pb = 0.f;
-            if constexpr (CLEAN) pcg_load(rng, B.pcg[slot]);
-            else rng.x = m.z;
-            pixel = m.x;
-            sample = m.y;
-            grp = CLEAN ? m.z : 0u;
-            job = wf_job(m.w);
-            depth = (int)wf_depth(m.w);
-            tmin = wf_tmin(d2);
+            rng_load<CLEAN>(PX2, rng);
+            pixel = PX2.w[0];
+            sample = PX2.w[1];
+            grp = CLEAN ? PX2.w[2] : 0u;
+            job = wf_job(R2.w[7]);
+            depth = (int)wf_depth(R2.w[7]);
+            tmin = wf_tmin(sec_f(R2, 6));
             if (status) break;
         }
     }
