@@ -816,7 +816,8 @@ def main():
     ap.add_argument("--no-ref-gpu", action="store_true", help="default line: skip the reference GPU build's timings")
     ap.add_argument("--no-rmse", action="store_true", help="skip the RMSE against the fp64 oracle")
     ap.add_argument("--served-requests", type=int, default=100, help="default line: served requests at 200/s")
-    ap.add_argument("--served-plain-requests", type=int, default=40)
+    ap.add_argument("--served-plain-requests", type=int, default=100,
+                    help="default line: requests of the plain server (the same stream prefix as the served form)")
     ap.add_argument("--lambdas", default="20,50,200,800", help="served: request rates (1/s)")
     ap.add_argument("--requests", type=int, default=300, help="served: requests per rate")
     ap.add_argument("--plain-requests", type=int, default=120, help="served: requests of the plain comparison")
@@ -1041,8 +1042,11 @@ def main():
             del bdss
         if not args.no_served:
             work = configs.batch_workload(args.scenes)
-            line["served"] = served_record(local, work, MODE_CLEAN, True, [200.0], args.served_requests,
-                                           args.served_plain_requests)
+            line["served"] = {
+                "compat": served_record(local, work, MODE_COMPAT, False, [200.0], args.served_requests,
+                                        args.served_plain_requests),
+                "clean_groups": served_record(local, work, MODE_CLEAN, True, [200.0], args.served_requests,
+                                              args.served_plain_requests)}
         if not args.no_ref_gpu:
             line["gpu_baseline"] = ref_gpu_baseline(ctx, stream)
         line["clocks_extra_legs"] = extra_clk.stop()
