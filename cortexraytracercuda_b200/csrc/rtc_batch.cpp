@@ -75,9 +75,10 @@ extern "C" rtc_status rtc_render_batch(rtc_context* c, const rtc_job* jobs, uint
     cfg.mode = jobs[0].params.mode;
     cfg.draw_order = cfg.mode == RTC_MODE_CLEAN ? RTC_DRAW_ORDER_DEVICE : jobs[0].params.draw_order;
     // Default slots: 2^22 when a slot runs all of a pixel's samples (the batch's tail is long pixels,
-    // and more slots in flight shorten it); 2^20 with sample groups, whose units are short: there a
-    // slot's path state (about 200 B) for 2^22 slots spills out of L2, and the shade kernel streams it
-    // from DRAM (64 scenes, clean mode: 614 Mpaths/s at 2^22, 720 at 2^20, 719 at 2^19 slots).
+    // and more slots in flight shorten it); 2^20 with sample groups, whose units are short: there the
+    // path state of 2^22 slots (108 B each: the 96-byte record and the queue entries) spills out of L2,
+    // and the shade kernel streams it from DRAM (64 scenes, clean mode, measured with the earlier
+    // 132-byte slots: 614 Mpaths/s at 2^22, 720 at 2^20, 719 at 2^19 slots).
     const bool grouped = jobs[0].params.mode == RTC_MODE_CLEAN && (jobs[0].params.flags & RTC_FLAG_SAMPLE_GROUPS);
     cfg.slots = bp && bp->slots ? bp->slots
                                 : (uint32_t)std::min<uint64_t>(total_pix, grouped ? 1u << 20 : 1u << 22);
