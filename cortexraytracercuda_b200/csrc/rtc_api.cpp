@@ -971,6 +971,18 @@ size_t carve_wavefront(void* base, uint32_t slots, WfBuffers& B) {
     return (size_t)(p - (uint8_t*)base);
 }
 
+}  // namespace
+
+int rtc_drain_every(int fallback) {
+    static const int every = [] {
+        const char* ev = std::getenv("RTC_WF_DRAIN_EVERY");
+        return ev ? std::max(0, std::atoi(ev)) : -1;
+    }();
+    return every >= 0 ? every : fallback;
+}
+
+namespace {
+
 // Bytes carve_wavefront lays out for `slots` slots (each buffer rounded up to 256 bytes).
 constexpr size_t wavefront_bytes(size_t n) {
     return ((n * WF_REC_BYTES + 255) & ~(size_t)255) + 3 * ((n * 4 + 255) & ~(size_t)255) +
@@ -1088,6 +1100,14 @@ rtc_status run_wavefront(const DevScene& S, const rtc_render_params* p, const Wf
     // drain threshold: below this many queued slots the finish kernel takes over
     uint32_t drain = (uint32_t)num_sms * 512u;
     if (const char* ev = std::getenv("RTC_WF_DRAIN")) drain = (uint32_t)std::strtoul(ev, nullptr, 10);
+    // Drain kernel: one thread per slot for its whole chain, or the compacting drain, whose live slots
+    // are repacked into full warps every 2 bounce steps.  A frame with fewer work units than the drain
+    // threshold runs almost whole in the drain, where its short chains leave the lanes idle: there the
+    // compacting drain pays (Cornell 256x256, 16 spp: drain 1.91 -> 1.52 ms).  In a larger frame the
+    // drain is bound by its longest chains' bounce latency, which packing does not shorten (spheres
+    // frame: 19.0 against 18.6-19.4 ms), and its barriers cost a DRAM-bound walk (meshes frame: 67.7
+    // against 98.9 ms), so it keeps the plain drain.
+    L.drain_every = rtc_drain_every(P.num_pixels * (int64_t)P.groups <= (int64_t)drain ? 2 : 0);
     // long-chain split: at iteration `split_at` (0: never), slots predicted to need more than
     // `split_thr` further iterations move to the drain kernel, running beside the bulk iterations
     uint64_t split_at = 0;
@@ -1195,7 +1215,8 @@ rtc_status run_wavefront(const DevScene& S, const rtc_render_params* p, const Wf
     if (phase) RTC_CUDA(cudaEventRecord(phase[1], st));
     if (run.drained) {
         L.w = wf_iter(it);
-        L.grid = (int)std::max<uint32_t>(1u, (drain + 127u) / 128u);
+        const uint32_t per_block = L.drain_every > 0 ? (uint32_t)rtc::WF_DRAIN_BLOCK : 128u;
+        L.grid = (int)std::max<uint32_t>(1u, (drain + per_block - 1u) / per_block);
         e = fn(WF_OP_FINISH, J, B, L);
         if (e != cudaSuccess) return cuda_fail(e, "wavefront finish");
     }

@@ -259,7 +259,9 @@ rtc_status Engine::finish() {
     L.counters = counters_;
     L.wide = cfg_.wide;
     L.st = st_;
-    L.grid = (int)std::max<uint32_t>(1u, (drain_ + 127u) / 128u);
+    L.drain_every = rtc_drain_every(0);   // the batch's drain is its tail of long chains: the plain drain
+    const uint32_t per_block = L.drain_every > 0 ? (uint32_t)WF_DRAIN_BLOCK : 128u;
+    L.grid = (int)std::max<uint32_t>(1u, (drain_ + per_block - 1u) / per_block);
     cudaError_t e = fn_(WF_OP_FINISH, A, B_, L);
     if (e != cudaSuccess) return cuda_err(e, "wavefront finish");
     ++launches_;

@@ -49,6 +49,9 @@ void rtc_view_env_sampling(rtc::DevScene& S, const rtc_render_params* p);
 rtc::DevParams rtc_dev_params(const rtc_render_params* p);
 // scratch of an image rendered with sample groups (0 without), and its layout at `base`
 size_t rtc_group_bytes(const rtc_render_params* p);
+// Drain kernel of the wavefront engines (WfLaunch::drain_every): RTC_WF_DRAIN_EVERY when set, else
+// `fallback`.
+int rtc_drain_every(int fallback);
 void rtc_carve_groups(void* base, const rtc_render_params* p, float4** part, uint32_t** gcnt);
 // perspective_camera::initialize; false for a degenerate camera
 bool rtc_make_camera(const rtc_camera& c, rtc::DevCamera& out);

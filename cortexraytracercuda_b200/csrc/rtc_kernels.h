@@ -24,6 +24,8 @@
 #endif
 
 namespace rtc {
+constexpr int WF_DRAIN_BLOCK = 256;   // threads per block of the compacting drain (wf_finish_packed)
+
 // Wavefront kernel launches.  One dispatcher per (mode, flavour) and job source; `op` picks the kernel.
 enum WfOp {
     WF_OP_INIT = 0, WF_OP_ADMIT = 1, WF_OP_EXTEND = 2, WF_OP_SHADE = 3, WF_OP_FINISH = 4, WF_OP_BOUNCE = 5,
@@ -38,6 +40,9 @@ struct WfLaunch {
     uint32_t* status;
     int grid;
     int block;                       // EXTEND / SHADE / BOUNCE: threads per block (0: 128; at most 512)
+    int drain_every;                 // FINISH: 0 the plain drain (128-thread blocks, one thread per slot);
+                                     // k > 0 the compacting drain (256-thread blocks, live slots repacked
+                                     // every k bounce steps)
     cudaStream_t st;
 };
 using WfOneFn = cudaError_t (*)(WfOp, const WfOneArgs&, const WfBuffers&, const WfLaunch&);

@@ -733,6 +733,195 @@ __global__ void RTC_FINISH_BOUNDS wf_finish(J jobs, WfBuffers B, WfIter w, unsig
     if (status) atomicOr(status_word, status);
 }
 
+// Compacting drain.  The plain drain above gives each remaining slot one thread for its whole chain,
+// so a warp runs as long as its longest chain while its other lanes idle (3.8 of 32 lanes active on
+// the spheres frame).  Here the chains advance one bounce per step, and every `every` steps the live
+// slots of a block move, through shared memory, to the block's lowest threads: the live chains stay
+// packed into full warps, and the warps left without a slot wait at the block barrier without
+// issuing.  Each slot computes exactly what the plain drain computes for it (the same bounce, sample
+// and pixel code in the same order); only which thread runs it changes.
+//
+// A block takes the queue entries b, b + G, b + 2G, ... (G blocks), so pixels that sit together in the
+// queue - neighbours, with similar chains - spread over all SMs; entries past G x WF_DRAIN_BLOCK are
+// taken in further rounds.
+constexpr int WF_DRAIN_WORDS = 23;   // a slot's state in the pool (WF_DRAIN_BLOCK: rtc_kernels.h)
+
+template <bool CLEAN>
+struct DrainSlot {
+    V3 o, d;
+    float tmin;            // 1e-5, or t + 0.001 for a pending re-hit from behind a one-sided light
+    RGB att, acc;
+    float pr, pg, pb;      // the pixel (or sample group) sum so far
+    WfRng<CLEAN> rng;
+    uint32_t pixel, sample, mw, grp, slot;
+};
+
+template <bool CLEAN>
+__device__ __forceinline__ void drain_load(const WfBuffers& B, uint32_t slot, DrainSlot<CLEAN>& x) {
+    const Sec R = ld_sec(wf_sec(B, slot, SEC_RAY)), SH = ld_sec(wf_sec(B, slot, SEC_SHADE)),
+              PX = ld_sec(wf_sec(B, slot, SEC_PIXEL));
+    x.o = sec_v3(R, 0);
+    x.d = sec_v3(R, 3);
+    x.tmin = wf_tmin(sec_f(R, 6));
+    x.mw = R.w[7];
+    x.att = rgb(sec_f(SH, 0), sec_f(SH, 1), sec_f(SH, 2));
+    x.acc = rgb(sec_f(SH, 3), sec_f(SH, 4), sec_f(SH, 5));
+    x.pr = sec_f(PX, 4);
+    x.pg = sec_f(PX, 5);
+    x.pb = sec_f(PX, 6);
+    rng_load<CLEAN>(PX, x.rng);
+    x.pixel = PX.w[0];
+    x.sample = PX.w[1];
+    x.grp = CLEAN ? PX.w[2] : 0u;
+    x.slot = slot;
+}
+
+// the slot's words in (or out of) the block's shared pool, column `i`
+template <bool CLEAN>
+__device__ __forceinline__ void drain_put(uint32_t (*pool)[WF_DRAIN_BLOCK], int i, const DrainSlot<CLEAN>& x) {
+    const float f[16] = {x.o.x, x.o.y, x.o.z, x.d.x, x.d.y, x.d.z, x.tmin, x.att.r, x.att.g, x.att.b,
+                         x.acc.r, x.acc.g, x.acc.b, x.pr, x.pg, x.pb};
+#pragma unroll
+    for (int k = 0; k < 16; ++k) pool[k][i] = __float_as_uint(f[k]);
+    pool[16][i] = x.pixel;
+    pool[17][i] = x.sample;
+    pool[18][i] = x.mw;
+    pool[19][i] = x.grp;
+    pool[20][i] = x.slot;
+    if constexpr (CLEAN) {
+        pool[21][i] = (uint32_t)x.rng.state;
+        pool[22][i] = (uint32_t)(x.rng.state >> 32);
+    } else {
+        pool[21][i] = x.rng.x;
+    }
+}
+template <bool CLEAN>
+__device__ __forceinline__ void drain_get(uint32_t (*pool)[WF_DRAIN_BLOCK], int i, DrainSlot<CLEAN>& x) {
+    float f[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) f[k] = __uint_as_float(pool[k][i]);
+    x.o = v3(f[0], f[1], f[2]);
+    x.d = v3(f[3], f[4], f[5]);
+    x.tmin = f[6];
+    x.att = rgb(f[7], f[8], f[9]);
+    x.acc = rgb(f[10], f[11], f[12]);
+    x.pr = f[13];
+    x.pg = f[14];
+    x.pb = f[15];
+    x.pixel = pool[16][i];
+    x.sample = pool[17][i];
+    x.mw = pool[18][i];
+    x.grp = pool[19][i];
+    x.slot = pool[20][i];
+    if constexpr (CLEAN) {
+        x.rng.state = ((uint64_t)pool[22][i] << 32) | pool[21][i];
+        x.rng.inc = ((uint64_t)x.sample << 1) | 1u;
+    } else {
+        x.rng.x = pool[21][i];
+    }
+}
+
+// One step of a slot: one pass of camera::ray_color's loop body (trace, then shade_bounce_deferred),
+// then the sample's and the pixel's bookkeeping when the sample ends - trace_bounces and the plain
+// drain's loop, one bounce at a time.  Returns false when the slot has no pixel left.
+template <bool CLEAN, int ORDER, class J>
+__device__ __forceinline__ bool drain_step(const J& jobs, const WfWindow& win, const WfBuffers& B, DrainSlot<CLEAN>& x,
+                                           PathCounters& pc, TraceStats& st, uint32_t& paths, uint32_t& status) {
+    const uint32_t job = wf_job(x.mw);
+    const DevScene& S = jobs.scene(job);
+    const DevParams& P = jobs.params(job);
+    uint32_t depth = wf_depth(x.mw);
+    Ray r;
+    r.o = x.o;
+    r.d = x.d;
+    r.time = 0.0f;
+    float t, next_tmin = 0.0f;
+    uint32_t item;
+    pc.rays++;
+    const bool hit = closest_hit<CLEAN>(S, r.o, r.d, x.tmin, 3.402823466e+38f, depth == (uint32_t)P.max_depth, t,
+                                        item, st, status);
+    const int out = shade_bounce_deferred<CLEAN, ORDER>(S, r, hit, t, item, x.tmin > 0.00001f, x.acc, x.att, x.rng,
+                                                        status, next_tmin);
+    if (out == BOUNCE_REHIT) {   // the same ray again from behind the light, at the same depth
+        x.tmin = next_tmin;
+        return true;
+    }
+    if (out == BOUNCE_NEXT && --depth > 0u) {
+        x.o = r.o;
+        x.d = r.d;
+        x.tmin = 0.00001f;
+        x.mw = wf_pack(depth, job);
+        return true;
+    }
+    // the sample is done: pixel_color += ray_color(...) (gpu.cu:787)
+    ++paths;
+    if (!CLEAN || (isfinite(x.acc.r) && isfinite(x.acc.g) && isfinite(x.acc.b))) {
+        x.pr += x.acc.r;
+        x.pg += x.acc.g;
+        x.pb += x.acc.b;
+    }
+    if (++x.sample < (P.groups > 1 ? wf_group_end(P, x.grp, CLEAN) : wf_samples(P, CLEAN))) {
+        wf_start_sample<CLEAN, ORDER>(S, P, x.rng, x.pixel, x.sample, r);
+        x.o = r.o;
+        x.d = r.d;
+        x.tmin = 0.00001f;
+        x.att = rgb(1.f, 1.f, 1.f);
+        x.acc = rgb(0.f, 0.f, 0.f);
+        x.mw = wf_pack((uint32_t)P.max_depth, job);
+        return true;
+    }
+    wf_group_done(jobs, job, x.pixel, x.grp, make_float4(x.pr, x.pg, x.pb, 0.0f));
+    // a slot that still has pixels to take (fewer slots than pixels) continues through memory
+    if (!wf_fetch_pixel<CLEAN, ORDER>(jobs, win, B, x.slot, status)) return false;
+    drain_load<CLEAN>(B, x.slot, x);
+    return status == 0u;
+}
+
+template <bool CLEAN, int ORDER, bool COUNT, class J>
+__global__ void __launch_bounds__(WF_DRAIN_BLOCK, 2) wf_finish_packed(J jobs, WfBuffers B, WfIter w, int every,
+                                                                  unsigned long long* counters, uint32_t* status_word) {
+    __shared__ uint32_t pool[WF_DRAIN_WORDS][WF_DRAIN_BLOCK];
+    __shared__ int warp_live[WF_DRAIN_BLOCK / 32];
+    const uint32_t n = B.ctr[w.cin];
+    const WfWindow win = jobs.window();
+    const uint32_t* q = B.queue[w.qin];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t G = gridDim.x;
+    uint32_t status = 0, paths = 0;
+    PathCounters pc{0, 0, 0};
+    TraceStats st{0, 0};
+    const int steps = every > 0 ? every : 1;
+    for (uint32_t round = 0; round < n; round += G * WF_DRAIN_BLOCK) {
+        DrainSlot<CLEAN> x;
+        const uint32_t k = round + blockIdx.x + G * (uint32_t)tid;
+        bool live = k < n;
+        if (live) drain_load<CLEAN>(B, ld_state(q + k), x);
+        for (;;) {
+            for (int s = 0; s < steps; ++s)
+                if (live) live = drain_step<CLEAN, ORDER>(jobs, win, B, x, pc, st, paths, status);
+            // compaction: the live slots move to threads 0 .. total-1, in thread order
+            const unsigned m = __ballot_sync(0xffffffffu, live);
+            __syncthreads();   // every thread is done with the pool's previous contents
+            if (lane == 0) warp_live[warp] = __popc(m);
+            __syncthreads();
+            int base = 0, total = 0;
+#pragma unroll
+            for (int v = 0; v < WF_DRAIN_BLOCK / 32; ++v) {
+                const int c = warp_live[v];
+                base += v < warp ? c : 0;
+                total += c;
+            }
+            if (total == 0) break;   // the same for every thread of the block
+            if (live) drain_put<CLEAN>(pool, base + __popc(m & ((1u << lane) - 1u)), x);
+            __syncthreads();
+            live = tid < total;
+            if (live) drain_get<CLEAN>(pool, tid, x);
+        }
+    }
+    wf_flush<COUNT>(counters, pc.rays, paths, st);
+    if (status) atomicOr(status_word, status);
+}
+
 // ---- launch dispatch (instantiated once per translation unit / flavour) ---------------------------
 
 template <bool CLEAN, int ORDER, int FLAVOR, class J, class A>
@@ -769,8 +958,15 @@ cudaError_t wf_dispatch(WfOp op, const A& args, const WfBuffers& B, const WfLaun
         else wf_shade<CLEAN, ORDER, false><<<L.grid, blk, 0, L.st>>>(jobs, B, L.w, nullptr, L.status);
         break;
     case WF_OP_FINISH:
-        if (c) wf_finish<CLEAN, ORDER, true><<<L.grid, 128, 0, L.st>>>(jobs, B, L.w, L.counters, L.status);
-        else wf_finish<CLEAN, ORDER, false><<<L.grid, 128, 0, L.st>>>(jobs, B, L.w, nullptr, L.status);
+        if (L.drain_every > 0) {
+            if (c) wf_finish_packed<CLEAN, ORDER, true><<<L.grid, WF_DRAIN_BLOCK, 0, L.st>>>(jobs, B, L.w, L.drain_every,
+                                                                                          L.counters, L.status);
+            else wf_finish_packed<CLEAN, ORDER, false><<<L.grid, WF_DRAIN_BLOCK, 0, L.st>>>(jobs, B, L.w, L.drain_every,
+                                                                                            nullptr, L.status);
+        } else {
+            if (c) wf_finish<CLEAN, ORDER, true><<<L.grid, 128, 0, L.st>>>(jobs, B, L.w, L.counters, L.status);
+            else wf_finish<CLEAN, ORDER, false><<<L.grid, 128, 0, L.st>>>(jobs, B, L.w, nullptr, L.status);
+        }
         break;
     case WF_OP_SPLIT:
         wf_split<CLEAN><<<L.grid, 128, 0, L.st>>>(jobs, B, L.w, L.k0, L.threshold);
