@@ -59,3 +59,30 @@ def test_desc_roundtrip_counts():
     d = SceneDesc(s).desc
     assert d.num_spheres == 3 and d.num_quads == 2 and d.num_images == 1 and d.num_dir_lights == 1
     assert d.images[0].width == 64 and d.images[0].height == 48
+
+
+def test_desc_packed_arrays_match_elementwise_construction():
+    """SceneDesc builds its sphere, material and texture arrays from numpy rows; each element's bytes
+    equal the ctypes structure built field by field."""
+    import ctypes as C
+
+    from cortexraytracercuda_b200.scene import (TEX_CHECKER, TEX_IMAGE, TEX_SOLID, rtc_material, rtc_sphere,
+                                                rtc_texture, F3)
+    for make in (configs.spheres, configs.cornell, configs.textured, configs.lights_scene):
+        s = make()
+        d = SceneDesc(s).desc
+        for k, (c, r, m) in enumerate(s.spheres):
+            assert bytes(d.spheres[k]) == bytes(rtc_sphere(F3(*map(float, c)), r, m))
+        for k, m in enumerate(s.materials):
+            assert bytes(d.materials[k]) == bytes(rtc_material(*m))
+        for k, t in enumerate(s.textures):
+            if t[0] == "solid":
+                ref = rtc_texture(TEX_SOLID, F3(*map(float, t[1])), 0.0, -1, -1, -1)
+            elif t[0] == "checker":
+                ref = rtc_texture(TEX_CHECKER, F3(0.0, 0.0, 0.0), t[1], t[2], t[3], -1)
+            else:
+                ref = rtc_texture(TEX_IMAGE, F3(0.0, 0.0, 0.0), 0.0, -1, -1, t[1])
+            assert bytes(d.textures[k]) == bytes(ref)
+        assert d.num_spheres == len(s.spheres) and d.num_materials == len(s.materials)
+        assert d.num_textures == len(s.textures)
+        assert C.sizeof(rtc_sphere) == 20
