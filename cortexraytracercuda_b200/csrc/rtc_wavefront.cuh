@@ -24,10 +24,14 @@
 // Launch bounds of the iteration kernels (extend, shade, fused bounce), which run with 128, 256 or 512
 // threads per block (WfLaunch::block, a batch autotuner knob).  Build-time knobs for occupancy sweeps:
 // RTC_EXTEND_MINB / RTC_SHADE_MINB ask for that many resident 512-thread blocks per SM (a register cap of
-// 65536 / (512 x blocks)).  Without them the compiler's own choice stands, which measured best (extend
-// 64 registers, shade 114); note that an explicit minimum of 1 is not the same as none.
+// 65536 / (512 x blocks)), RTC_EXTEND_MAXNREG and RTC_SHADE_MAXNREG cap the extend kernel and the ring's
+// shade kernel at any count.  Without them the compiler's own choice stands (extend 64 registers); note
+// that an explicit minimum of 1 is not the same as none.  The single-image shade kernel has its own cap,
+// RTC_SHADE_ONE_MAXNREG (see wf_shade).
 #define RTC_ITER_BLOCK_MAX 512
-#ifdef RTC_EXTEND_MINB
+#if defined(RTC_EXTEND_MAXNREG)
+#define RTC_EXTEND_BOUNDS __maxnreg__(RTC_EXTEND_MAXNREG)
+#elif defined(RTC_EXTEND_MINB)
 #define RTC_EXTEND_BOUNDS __launch_bounds__(RTC_ITER_BLOCK_MAX, RTC_EXTEND_MINB)
 #else
 #define RTC_EXTEND_BOUNDS __launch_bounds__(RTC_ITER_BLOCK_MAX)
@@ -560,8 +564,8 @@ __device__ __forceinline__ void wf_flush(unsigned long long* counters, uint32_t 
 }
 
 template <bool CLEAN, int ORDER, bool COUNT, class J>
-__global__ void RTC_SHADE_BOUNDS wf_shade(J jobs, WfBuffers B, WfIter w, unsigned long long* counters,
-                                                uint32_t* status_word) {
+__device__ __forceinline__ void wf_shade_pass(const J& jobs, const WfBuffers& B, WfIter w, unsigned long long* counters,
+                                              uint32_t* status_word) {
     const uint32_t n = B.ctr[w.cin];
     const WfWindow win = jobs.window();
     const uint32_t* q = B.queue[w.qin];
@@ -586,6 +590,27 @@ __global__ void RTC_SHADE_BOUNDS wf_shade(J jobs, WfBuffers B, WfIter w, unsigne
     }
     wf_flush<COUNT>(counters, pc.rays, paths, st);
     if (status) atomicOr(status_word, status);
+}
+
+// The shade kernels.  A single image's shade step is held to RTC_SHADE_ONE_MAXNREG registers (64 by
+// default): 8 blocks of 128 threads per SM, so its grid (8 blocks per SM) runs in one wave at more warps
+// than the compiler's own 85 registers allow (5 blocks per SM, and the grid's last 3 blocks per SM ran
+// alone afterwards).  It spills 32 bytes; on the spheres frame (1280x720, 64 spp) shade fell from 22.2 to
+// 17.9 ms per frame, where 80 and 72 registers (6 and 7 blocks, still two waves) measured 23.1 and
+// 22.2 ms.  The ring's shade step, which copies its job record, keeps the compiler's choice
+// (RTC_SHADE_BOUNDS): at 64 registers it would spill 256 bytes.
+#ifndef RTC_SHADE_ONE_MAXNREG
+#define RTC_SHADE_ONE_MAXNREG 64
+#endif
+template <bool CLEAN, int ORDER, bool COUNT>
+__global__ void __maxnreg__(RTC_SHADE_ONE_MAXNREG) wf_shade(WfOne jobs, WfBuffers B, WfIter w,
+                                                            unsigned long long* counters, uint32_t* status_word) {
+    wf_shade_pass<CLEAN, ORDER, COUNT>(jobs, B, w, counters, status_word);
+}
+template <bool CLEAN, int ORDER, bool COUNT>
+__global__ void RTC_SHADE_BOUNDS wf_shade_ring(WfTable jobs, WfBuffers B, WfIter w, unsigned long long* counters,
+                                               uint32_t* status_word) {
+    wf_shade_pass<CLEAN, ORDER, COUNT>(jobs, B, w, counters, status_word);
 }
 
 // Fused form of one iteration: trace + shade of every queued slot in one launch (each lane still does
@@ -954,8 +979,13 @@ cudaError_t wf_dispatch(WfOp op, const A& args, const WfBuffers& B, const WfLaun
         }
         break;
     case WF_OP_SHADE:
-        if (c) wf_shade<CLEAN, ORDER, true><<<L.grid, blk, 0, L.st>>>(jobs, B, L.w, L.counters, L.status);
-        else wf_shade<CLEAN, ORDER, false><<<L.grid, blk, 0, L.st>>>(jobs, B, L.w, nullptr, L.status);
+        if constexpr (std::is_same<J, WfOne>::value) {
+            if (c) wf_shade<CLEAN, ORDER, true><<<L.grid, blk, 0, L.st>>>(jobs, B, L.w, L.counters, L.status);
+            else wf_shade<CLEAN, ORDER, false><<<L.grid, blk, 0, L.st>>>(jobs, B, L.w, nullptr, L.status);
+        } else {
+            if (c) wf_shade_ring<CLEAN, ORDER, true><<<L.grid, blk, 0, L.st>>>(jobs, B, L.w, L.counters, L.status);
+            else wf_shade_ring<CLEAN, ORDER, false><<<L.grid, blk, 0, L.st>>>(jobs, B, L.w, nullptr, L.status);
+        }
         break;
     case WF_OP_FINISH:
         if (L.drain_every > 0) {
