@@ -24,10 +24,10 @@
 // Launch bounds of the iteration kernels (extend, shade, fused bounce), which run with 128, 256 or 512
 // threads per block (WfLaunch::block, a batch autotuner knob).  Build-time knobs for occupancy sweeps:
 // RTC_EXTEND_MINB / RTC_SHADE_MINB ask for that many resident 512-thread blocks per SM (a register cap of
-// 65536 / (512 x blocks)), RTC_EXTEND_MAXNREG and RTC_SHADE_MAXNREG cap the extend kernel and the ring's
-// shade kernel at any count.  Without them the compiler's own choice stands (extend 64 registers); note
-// that an explicit minimum of 1 is not the same as none.  The single-image shade kernel has its own cap,
-// RTC_SHADE_ONE_MAXNREG (see wf_shade).
+// 65536 / (512 x blocks)), RTC_EXTEND_MAXNREG caps the extend kernel at any count.  Without them the
+// compiler's own choice stands (extend 64 registers); note that an explicit minimum of 1 is not the same
+// as none.  The shade kernels are capped at 64 registers (RTC_SHADE_ONE_MAXNREG for a single image,
+// RTC_SHADE_MAXNREG for the ring; see wf_shade).
 #define RTC_ITER_BLOCK_MAX 512
 #if defined(RTC_EXTEND_MAXNREG)
 #define RTC_EXTEND_BOUNDS __maxnreg__(RTC_EXTEND_MAXNREG)
@@ -36,13 +36,14 @@
 #else
 #define RTC_EXTEND_BOUNDS __launch_bounds__(RTC_ITER_BLOCK_MAX)
 #endif
-#if defined(RTC_SHADE_MAXNREG)
-// a register cap at any value (__maxnreg__ cannot be combined with launch bounds)
-#define RTC_SHADE_BOUNDS __maxnreg__(RTC_SHADE_MAXNREG)
-#elif defined(RTC_SHADE_MINB)
+#if defined(RTC_SHADE_MINB)
 #define RTC_SHADE_BOUNDS __launch_bounds__(RTC_ITER_BLOCK_MAX, RTC_SHADE_MINB)
 #else
-#define RTC_SHADE_BOUNDS __launch_bounds__(RTC_ITER_BLOCK_MAX)
+// a register cap (__maxnreg__ cannot be combined with launch bounds); see wf_shade_ring
+#ifndef RTC_SHADE_MAXNREG
+#define RTC_SHADE_MAXNREG 64
+#endif
+#define RTC_SHADE_BOUNDS __maxnreg__(RTC_SHADE_MAXNREG)
 #endif
 #ifdef RTC_FINISH_MINB
 #define RTC_FINISH_BOUNDS __launch_bounds__(128, RTC_FINISH_MINB)
@@ -597,8 +598,10 @@ __device__ __forceinline__ void wf_shade_pass(const J& jobs, const WfBuffers& B,
 // than the compiler's own 85 registers allow (5 blocks per SM, and the grid's last 3 blocks per SM ran
 // alone afterwards).  It spills 32 bytes; on the spheres frame (1280x720, 64 spp) shade fell from 22.2 to
 // 17.9 ms per frame, where 80 and 72 registers (6 and 7 blocks, still two waves) measured 23.1 and
-// 22.2 ms.  The ring's shade step, which copies its job record, keeps the compiler's choice
-// (RTC_SHADE_BOUNDS): at 64 registers it would spill 256 bytes.
+// 22.2 ms.  The ring's shade step (batched and served renders), which copies its job record, takes 128
+// registers uncapped and spills 256 bytes at 64, yet 64 measured fastest there too: 64 scenes in compat
+// mode 846 -> 870 Mpaths/s, where 80 and 96 registers (164 and 92 bytes of spills, 6 and 5 blocks per
+// SM) measured 803 and 814.
 #ifndef RTC_SHADE_ONE_MAXNREG
 #define RTC_SHADE_ONE_MAXNREG 64
 #endif
