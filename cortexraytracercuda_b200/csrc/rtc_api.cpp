@@ -973,6 +973,14 @@ size_t carve_wavefront(void* base, uint32_t slots, WfBuffers& B) {
 
 }  // namespace
 
+bool rtc_dynamic_chunks(bool fallback) {
+    static const int v = [] {
+        const char* ev = std::getenv("RTC_WF_DYNAMIC");
+        return ev ? (std::atoi(ev) != 0 ? 1 : 0) : -1;
+    }();
+    return v >= 0 ? v != 0 : fallback;
+}
+
 int rtc_drain_every(int fallback) {
     static const int every = [] {
         const char* ev = std::getenv("RTC_WF_DRAIN_EVERY");
@@ -1108,6 +1116,12 @@ rtc_status run_wavefront(const DevScene& S, const rtc_render_params* p, const Wf
     // frame: 19.0 against 18.6-19.4 ms), and its barriers cost a DRAM-bound walk (meshes frame: 67.7
     // against 98.9 ms), so it keeps the plain drain.
     L.drain_every = rtc_drain_every(P.num_pixels * (int64_t)P.groups <= (int64_t)drain ? 2 : 0);
+    // Queue chunks handed out by a counter for scenes of 2^20 primitives or more, whose walks are long
+    // and uneven (meshes frame, 1.31 M triangles: extend 450.7 -> 405.5 ms, 436 -> 460-467 Mpaths/s);
+    // the fixed grid stride for smaller ones (spheres frame, 489 primitives: 945 against 840 Mpaths/s;
+    // the 64 batch scenes of up to 500 K triangles, one image per call: 631 against 608 in compat mode,
+    // 1,167 against 1,001 in clean mode with sample groups).
+    L.dynamic = rtc_dynamic_chunks(S.num_items >= (1u << 20));
     // long-chain split: at iteration `split_at` (0: never), slots predicted to need more than
     // `split_thr` further iterations move to the drain kernel, running beside the bulk iterations
     uint64_t split_at = 0;

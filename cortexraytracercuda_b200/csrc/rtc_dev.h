@@ -230,7 +230,8 @@ struct WfTableArgs {           // a ring of jobs
 
 // Iteration k reads queue (k & 1) with size ctr[k % 3], appends to queue ((k+1) & 1) counted in
 // ctr[(k+1) % 3] and clears ctr[(k+2) % 3], which iteration k+1 appends to.
-enum WfCtr { WF_NEXT_PIXEL = 3, WF_LONG = 4, WF_CTR_N = 5 };
+// [5], [6]: the next queue entry the extend / shade kernel hands out (each kernel clears the other's)
+enum WfCtr { WF_NEXT_PIXEL = 3, WF_LONG = 4, WF_FETCH_EXTEND = 5, WF_FETCH_SHADE = 6, WF_CTR_N = 7 };
 struct WfIter {
     int qin, cin, cout, czero;
 };

@@ -52,6 +52,9 @@ size_t rtc_group_bytes(const rtc_render_params* p);
 // Drain kernel of the wavefront engines (WfLaunch::drain_every): RTC_WF_DRAIN_EVERY when set, else
 // `fallback`.
 int rtc_drain_every(int fallback);
+// Queue distribution of the extend and shade kernels (WfLaunch::dynamic): RTC_WF_DYNAMIC when set, else
+// `fallback`.
+bool rtc_dynamic_chunks(bool fallback);
 void rtc_carve_groups(void* base, const rtc_render_params* p, float4** part, uint32_t** gcnt);
 // perspective_camera::initialize; false for a degenerate camera
 bool rtc_make_camera(const rtc_camera& c, rtc::DevCamera& out);

@@ -40,6 +40,8 @@ struct WfLaunch {
     uint32_t* status;
     int grid;
     int block;                       // EXTEND / SHADE / BOUNCE: threads per block (0: 128; at most 512)
+    bool dynamic;                    // EXTEND / SHADE: warps take chunks of the queue from a counter (WfChunks)
+                                     // instead of a fixed grid stride
     int drain_every;                 // FINISH: 0 the plain drain (128-thread blocks, one thread per slot);
                                      // k > 0 the compacting drain (256-thread blocks, live slots repacked
                                      // every k bounce steps)

@@ -182,6 +182,43 @@ __device__ __forceinline__ float4 sec_psum(const Sec& s) {
 // the shade kernel hands back to the extend kernel (camera.cuh:177-183).
 __device__ __forceinline__ float wf_tmin(float start) { return start > 0.0f ? start : 0.00001f; }
 
+// Work distribution of the iteration kernels, in chunks of 32 queue entries per warp:
+//   fixed    warp w of the grid takes chunks w, w + W, w + 2W, ... (W warps in the grid);
+//   dynamic  a warp takes the next chunk from a counter (one atomic by lane 0), and asks for its
+//            following chunk before it works on the current one, so the atomic's round trip overlaps
+//            the work.
+// Dynamic pays where walks are long and uneven (triangle meshes, a batch of many scenes): with the
+// fixed stride the warps that drew long walks ran alone at the end of each launch.  Where walks are
+// short (the 489-primitive spheres frame), the atomics on one counter cost more than the imbalance.
+// The choice is a template parameter, so the fixed form compiles to the plain grid-stride loop.  Every
+// lane of the warp must call it together.
+template <bool DYN>
+struct WfChunks {
+    uint32_t* ctr;
+    uint32_t next;
+    __device__ __forceinline__ explicit WfChunks(uint32_t* c) : ctr(c) {
+        uint32_t b = blockIdx.x * blockDim.x + (threadIdx.x & ~31u);
+        if constexpr (DYN) {
+            if ((threadIdx.x & 31) == 0) b = atomicAdd(ctr, 32u);
+            b = __shfl_sync(0xffffffffu, b, 0);
+        }
+        next = b;
+    }
+    // the current chunk's first entry, and the request for the one after it
+    __device__ __forceinline__ uint32_t take(uint32_t& pending) {
+        const uint32_t base = next;
+        pending = 0;
+        if constexpr (DYN) {
+            if ((threadIdx.x & 31) == 0) pending = atomicAdd(ctr, 32u);
+        }
+        return base;
+    }
+    __device__ __forceinline__ void advance(uint32_t pending) {
+        if constexpr (DYN) next = __shfl_sync(0xffffffffu, pending, 0);
+        else next += gridDim.x * blockDim.x;
+    }
+};
+
 // Appends `slot` to queue `q` when `pred`; every active lane of the warp must call it together.
 __device__ __forceinline__ void wf_push(uint32_t* q, uint32_t* cnt, uint32_t slot, bool pred) {
     const unsigned act = __activemask();
@@ -429,27 +466,38 @@ __global__ void __launch_bounds__(128) wf_admit(WfTable J, WfBuffers B, WfIter w
 
 // FLAVOR: 0 nvcc flavour, 1 g++ flavour, 2 clean mode (double-precision sphere test).
 // WIDE: the 8-wide node layout (RTC_FLAG_WIDE_BVH; the other kernels always walk the binary nodes).
-template <bool COUNT, int FLAVOR, class J, bool WIDE>
+template <bool COUNT, int FLAVOR, class J, bool WIDE, bool DYN>
 __global__ void RTC_EXTEND_BOUNDS wf_extend(J jobs, WfBuffers B, WfIter w, unsigned long long* counters,
                                                  uint32_t* status_word) {
     const uint32_t n = B.ctr[w.cin];
-    if (blockIdx.x == 0 && threadIdx.x == 0) B.ctr[w.czero] = 0u;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        B.ctr[w.czero] = 0u;
+        B.ctr[WF_FETCH_SHADE] = 0u;   // the shade kernel that follows hands out its entries from 0
+    }
     const uint32_t* q = B.queue[w.qin];
     TraceStats st{0, 0};
     uint32_t status = 0, rays = 0;
-    const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
-        const uint32_t slot = ld_state(q + k);
-        const Sec R = ld_sec(wf_sec(B, slot, SEC_RAY));
-        const uint32_t mw = R.w[7];
-        const uint32_t job = wf_job(mw);
-        float t;
-        uint32_t item;
-        bool h = closest_hit<FLAVOR == 2, WIDE>(jobs.scene(job), sec_v3(R, 0), sec_v3(R, 3), wf_tmin(sec_f(R, 6)),
-                                                3.402823466e+38f, wf_depth(mw) == (uint32_t)jobs.params(job).max_depth, t,
-                                                item, st, status);
-        st_hit(wf_sec(B, slot, SEC_SHADE), t, h ? item : 0xffffffffu);
-        ++rays;
+    WfChunks<DYN> chunks(B.ctr + WF_FETCH_EXTEND);
+    for (;;) {
+        uint32_t pending;
+        const uint32_t base = chunks.take(pending);
+        if (base >= n) break;   // the same for the whole warp
+        const uint32_t k = base + (threadIdx.x & 31u);
+        if (k < n) {
+            const uint32_t slot = ld_state(q + k);
+            const Sec R = ld_sec(wf_sec(B, slot, SEC_RAY));
+            const uint32_t mw = R.w[7];
+            const uint32_t job = wf_job(mw);
+            float t;
+            uint32_t item;
+            bool h = closest_hit<FLAVOR == 2, WIDE>(jobs.scene(job), sec_v3(R, 0), sec_v3(R, 3), wf_tmin(sec_f(R, 6)),
+                                                    3.402823466e+38f,
+                                                    wf_depth(mw) == (uint32_t)jobs.params(job).max_depth, t, item, st,
+                                                    status);
+            st_hit(wf_sec(B, slot, SEC_SHADE), t, h ? item : 0xffffffffu);
+            ++rays;
+        }
+        chunks.advance(pending);   // one call site: every lane of the warp takes part
     }
     if (COUNT && counters) {
         unsigned long long r = rays, nn = st.nodes, pp = st.prims;
@@ -564,7 +612,7 @@ __device__ __forceinline__ void wf_flush(unsigned long long* counters, uint32_t 
     }
 }
 
-template <bool CLEAN, int ORDER, bool COUNT, class J>
+template <bool CLEAN, int ORDER, bool COUNT, bool DYN, class J>
 __device__ __forceinline__ void wf_shade_pass(const J& jobs, const WfBuffers& B, WfIter w, unsigned long long* counters,
                                               uint32_t* status_word) {
     const uint32_t n = B.ctr[w.cin];
@@ -575,9 +623,13 @@ __device__ __forceinline__ void wf_shade_pass(const J& jobs, const WfBuffers& B,
     uint32_t status = 0, paths = 0;
     PathCounters pc{0, 0, 0};
     TraceStats st{0, 0};
-    const uint32_t stride = gridDim.x * blockDim.x;
-    const uint32_t limit = (n + 31u) & ~31u;   // whole warps iterate together so wf_push sees full warps
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < limit; k += stride) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) B.ctr[WF_FETCH_EXTEND] = 0u;   // for the next extend kernel
+    WfChunks<DYN> chunks(B.ctr + WF_FETCH_SHADE);
+    for (;;) {   // whole warps iterate together, so wf_push sees full warps
+        uint32_t pending;
+        const uint32_t base = chunks.take(pending);
+        if (base >= n) break;   // the same for the whole warp
+        const uint32_t k = base + (threadIdx.x & 31u);
         bool live = false;
         uint32_t slot = 0;
         if (k < n) {
@@ -588,6 +640,7 @@ __device__ __forceinline__ void wf_shade_pass(const J& jobs, const WfBuffers& B,
             live = wf_step<CLEAN, ORDER>(jobs, win, B, slot, R, SH, PX, sec_f(SH, 6), SH.w[7], pc, st, paths, status);
         }
         wf_push(qn, cn, slot, live);
+        chunks.advance(pending);
     }
     wf_flush<COUNT>(counters, pc.rays, paths, st);
     if (status) atomicOr(status_word, status);
@@ -605,15 +658,15 @@ __device__ __forceinline__ void wf_shade_pass(const J& jobs, const WfBuffers& B,
 #ifndef RTC_SHADE_ONE_MAXNREG
 #define RTC_SHADE_ONE_MAXNREG 64
 #endif
-template <bool CLEAN, int ORDER, bool COUNT>
+template <bool CLEAN, int ORDER, bool COUNT, bool DYN>
 __global__ void __maxnreg__(RTC_SHADE_ONE_MAXNREG) wf_shade(WfOne jobs, WfBuffers B, WfIter w,
                                                             unsigned long long* counters, uint32_t* status_word) {
-    wf_shade_pass<CLEAN, ORDER, COUNT>(jobs, B, w, counters, status_word);
+    wf_shade_pass<CLEAN, ORDER, COUNT, DYN>(jobs, B, w, counters, status_word);
 }
-template <bool CLEAN, int ORDER, bool COUNT>
+template <bool CLEAN, int ORDER, bool COUNT, bool DYN>
 __global__ void RTC_SHADE_BOUNDS wf_shade_ring(WfTable jobs, WfBuffers B, WfIter w, unsigned long long* counters,
                                                uint32_t* status_word) {
-    wf_shade_pass<CLEAN, ORDER, COUNT>(jobs, B, w, counters, status_word);
+    wf_shade_pass<CLEAN, ORDER, COUNT, DYN>(jobs, B, w, counters, status_word);
 }
 
 // Fused form of one iteration: trace + shade of every queued slot in one launch (each lane still does
@@ -952,6 +1005,29 @@ __global__ void __launch_bounds__(WF_DRAIN_BLOCK, 2) wf_finish_packed(J jobs, Wf
 
 // ---- launch dispatch (instantiated once per translation unit / flavour) ---------------------------
 
+template <int FLAVOR, class J, bool DYN>
+cudaError_t wf_launch_extend(const J& jobs, const WfBuffers& B, const WfLaunch& L, int blk, bool c) {
+    if (L.wide) {
+        if (c) wf_extend<true, FLAVOR, J, true, DYN><<<L.grid, blk, 0, L.st>>>(jobs, B, L.w, L.counters, L.status);
+        else wf_extend<false, FLAVOR, J, true, DYN><<<L.grid, blk, 0, L.st>>>(jobs, B, L.w, nullptr, L.status);
+    } else {
+        if (c) wf_extend<true, FLAVOR, J, false, DYN><<<L.grid, blk, 0, L.st>>>(jobs, B, L.w, L.counters, L.status);
+        else wf_extend<false, FLAVOR, J, false, DYN><<<L.grid, blk, 0, L.st>>>(jobs, B, L.w, nullptr, L.status);
+    }
+    return cudaGetLastError();
+}
+template <bool CLEAN, int ORDER, class J, bool DYN>
+cudaError_t wf_launch_shade(const J& jobs, const WfBuffers& B, const WfLaunch& L, int blk, bool c) {
+    if constexpr (std::is_same<J, WfOne>::value) {
+        if (c) wf_shade<CLEAN, ORDER, true, DYN><<<L.grid, blk, 0, L.st>>>(jobs, B, L.w, L.counters, L.status);
+        else wf_shade<CLEAN, ORDER, false, DYN><<<L.grid, blk, 0, L.st>>>(jobs, B, L.w, nullptr, L.status);
+    } else {
+        if (c) wf_shade_ring<CLEAN, ORDER, true, DYN><<<L.grid, blk, 0, L.st>>>(jobs, B, L.w, L.counters, L.status);
+        else wf_shade_ring<CLEAN, ORDER, false, DYN><<<L.grid, blk, 0, L.st>>>(jobs, B, L.w, nullptr, L.status);
+    }
+    return cudaGetLastError();
+}
+
 template <bool CLEAN, int ORDER, int FLAVOR, class J, class A>
 cudaError_t wf_dispatch(WfOp op, const A& args, const WfBuffers& B, const WfLaunch& L) {
     J jobs;
@@ -973,23 +1049,11 @@ cudaError_t wf_dispatch(WfOp op, const A& args, const WfBuffers& B, const WfLaun
         }
         break;
     case WF_OP_EXTEND:
-        if (L.wide) {
-            if (c) wf_extend<true, FLAVOR, J, true><<<L.grid, blk, 0, L.st>>>(jobs, B, L.w, L.counters, L.status);
-            else wf_extend<false, FLAVOR, J, true><<<L.grid, blk, 0, L.st>>>(jobs, B, L.w, nullptr, L.status);
-        } else {
-            if (c) wf_extend<true, FLAVOR, J, false><<<L.grid, blk, 0, L.st>>>(jobs, B, L.w, L.counters, L.status);
-            else wf_extend<false, FLAVOR, J, false><<<L.grid, blk, 0, L.st>>>(jobs, B, L.w, nullptr, L.status);
-        }
-        break;
+        if (L.dynamic) return wf_launch_extend<FLAVOR, J, true>(jobs, B, L, blk, c);
+        return wf_launch_extend<FLAVOR, J, false>(jobs, B, L, blk, c);
     case WF_OP_SHADE:
-        if constexpr (std::is_same<J, WfOne>::value) {
-            if (c) wf_shade<CLEAN, ORDER, true><<<L.grid, blk, 0, L.st>>>(jobs, B, L.w, L.counters, L.status);
-            else wf_shade<CLEAN, ORDER, false><<<L.grid, blk, 0, L.st>>>(jobs, B, L.w, nullptr, L.status);
-        } else {
-            if (c) wf_shade_ring<CLEAN, ORDER, true><<<L.grid, blk, 0, L.st>>>(jobs, B, L.w, L.counters, L.status);
-            else wf_shade_ring<CLEAN, ORDER, false><<<L.grid, blk, 0, L.st>>>(jobs, B, L.w, nullptr, L.status);
-        }
-        break;
+        if (L.dynamic) return wf_launch_shade<CLEAN, ORDER, J, true>(jobs, B, L, blk, c);
+        return wf_launch_shade<CLEAN, ORDER, J, false>(jobs, B, L, blk, c);
     case WF_OP_FINISH:
         if (L.drain_every > 0) {
             if (c) wf_finish_packed<CLEAN, ORDER, true><<<L.grid, WF_DRAIN_BLOCK, 0, L.st>>>(jobs, B, L.w, L.drain_every,
