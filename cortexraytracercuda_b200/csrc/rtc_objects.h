@@ -22,7 +22,7 @@ struct rtc_context {
     uint8_t* d_rgb8 = nullptr;
     size_t rgb8_cap = 0;
     int num_sms = 148;
-    // wavefront scratch: path slots (SoA) and the two slot queues
+    // wavefront scratch: path slot records and the slot queues (carve_wavefront)
     void* d_wf = nullptr;
     uint32_t wf_cap = 0;
     void* d_groups = nullptr;          // sample-group partial sums and counters (RTC_FLAG_SAMPLE_GROUPS)

@@ -68,8 +68,8 @@ __device__ __forceinline__ uint64_t mix64(uint64_t z) {   // splitmix64 finalise
 }
 
 // ------------------------------------------------------------------------------------------------
-// scene loads: read-only, kept in L1 with the evict_last priority so that streaming path state
-// (loaded with evict-first __ldcs in the wavefront kernels) does not push the BVH out of L1
+// scene loads: read-only, kept in L1 with the evict_last priority so that the path state the wavefront
+// kernels stream (their slot records, loaded L2-only) does not push the BVH out of L1
 // ------------------------------------------------------------------------------------------------
 __device__ __forceinline__ float4 ld_scene(const float4* p) {
     float4 r;
