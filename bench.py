@@ -135,7 +135,7 @@ def workload(name):
     return scene, params
 
 
-# what each measured scene adds to its BASELINE configuration, named in the bench line
+# what each measured scene adds to the workload as specified, named in the bench line
 ADDED = {"spheres": " + hidden quad light of random_spheres.scene (the config names none)",
          "meshes": " + hidden 8x4 quad light (the config names none)", "cornell": ""}
 
@@ -253,13 +253,13 @@ def cpu_reference_rate(scene, params, target_s=10.0, max_pixels=None):
 # shape (16x16 blocks, one thread per pixel, gpu.cu:2072-2080), the per-pixel printf left out.
 REF_GPU_CASES = [
     # (label, scene builder, parameters)
-    ("config 1: cornell 256x256 spp16 depth8", lambda: configs.cornell(), dict(width=256, height=256, spp=16, max_depth=8)),
-    ("config 2: spheres 1280x720 spp64 depth50 (the timed frame)", lambda: configs.spheres(),
+    ("cornell 256x256 spp16 depth8", lambda: configs.cornell(), dict(width=256, height=256, spp=16, max_depth=8)),
+    ("spheres 1280x720 spp64 depth50 (the timed frame)", lambda: configs.spheres(),
      dict(width=1280, height=720, spp=64, max_depth=50)),
-    ("P2: spheres 320x180 spp16 depth16, constant background", lambda: configs.spheres(sky=False),
+    ("spheres 320x180 spp16 depth16, constant background", lambda: configs.spheres(sky=False),
      dict(width=320, height=180, spp=16, max_depth=16)),
-    ("P3: textured 160x120 spp16 depth10", lambda: configs.textured(), dict(width=160, height=120, spp=16, max_depth=10)),
-    ("P4: icosphere (1,280 triangles x3) 150x100 spp16 depth12", lambda: configs.icosphere_scene(),
+    ("textured 160x120 spp16 depth10", lambda: configs.textured(), dict(width=160, height=120, spp=16, max_depth=10)),
+    ("icosphere (1,280 triangles x3) 150x100 spp16 depth12", lambda: configs.icosphere_scene(),
      dict(width=150, height=100, spp=16, max_depth=12)),
 ]
 
@@ -1024,7 +1024,7 @@ def main():
         v, r, inf = cpu_reference_rate(scene, params, target_s=args.cpu_baseline_s)
         line["cpu_baseline"] = {"value": round(v, 4), "unit": METRIC, **inf, "mrays_per_s": round(r, 4)}
     ds.close()
-    # ---- the batched and served forms (configs 4 and 5) and the reference's GPU build, one GPU only ----
+    # ---- the batched form (64 scenes), the served form (request streams) and the reference's GPU build, one GPU only ----
     if world == 1 and args.config == "spheres" and not args.small:
         extra_clk = ClockSampler(local)
         extra_clk.start()
